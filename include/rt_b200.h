@@ -1,0 +1,386 @@
+/* rt_b200.h — the C-ABI of the B200 path-tracing integrator.
+ *
+ * A scene goes in as plain tables that refer to each other by index (the reference's gpu::scene_desc,
+ * src/gpu/renderer.h:381-395 and its member types at renderer.h:43-377), linear pixels come out. Every entry point
+ * returns an rt_status; the reference's C++ API throws instead (renderer.h:518-526, 597-601) and the three exception
+ * classes map onto three status codes:
+ *   std::runtime_error   -> RT_ERR_RUNTIME  (a CUDA failure, an inconsistent scene)
+ *   std::invalid_argument-> RT_ERR_INVALID  (an option out of range)
+ *   std::logic_error     -> RT_ERR_LOGIC    (misuse: pixels() before a complete pass, a call on a dead session)
+ * rt_last_error_message() returns the message of the calling thread's last failure.
+ *
+ * All structs are plain data with fixed-width members and explicit padding, so that the layout is the same for C,
+ * C++, cgo, ctypes and JNI callers. No CUDA or torch type crosses this boundary.
+ */
+#ifndef RT_B200_H
+#define RT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RT_ABI_VERSION 1
+
+typedef enum rt_status
+{
+    RT_OK = 0,
+    RT_ERR_RUNTIME = 1,     /* std::runtime_error in the reference */
+    RT_ERR_INVALID = 2,     /* std::invalid_argument */
+    RT_ERR_LOGIC = 3,       /* std::logic_error */
+    RT_ERR_NO_DEVICE = 4,   /* no CUDA device: query_device's runtime_error */
+    RT_ERR_UNSUPPORTED = 5, /* a scene feature this build does not render (yet): a runtime_error in the reference */
+    RT_ERR_CAPACITY = 6,    /* a request beyond a stated limit (the HBM budget, a no-allocation scratch size) */
+    RT_ERR_TIMEOUT = 7      /* a bounded wait ran out */
+} rt_status;
+
+/* ---- the scene: renderer.h:30-395 as fixed-layout structs ---------------------------------------------------- */
+
+typedef struct rt_vec3
+{
+    double x, y, z;
+} rt_vec3;
+
+/* renderer.h:44-62 texture_kind / texture_desc */
+enum { RT_TEXTURE_SOLID = 0, RT_TEXTURE_CHECKER = 1, RT_TEXTURE_IMAGE = 2, RT_TEXTURE_NOISE = 3 };
+typedef struct rt_texture_desc
+{
+    int32_t kind;
+    int32_t even, odd;   /* checker: texture indices */
+    int32_t image;       /* image: index into images */
+    int32_t perlin;      /* noise: index into perlins */
+    int32_t pad0;
+    rt_vec3 rgb;         /* solid */
+    double inv_scale;    /* checker */
+    double scale;        /* noise */
+} rt_texture_desc;
+
+/* renderer.h:66-71 image_desc: width*height*3 linear floats, rows from the top */
+typedef struct rt_image_desc
+{
+    int32_t width, height;
+    const float* rgb;
+} rt_image_desc;
+
+/* renderer.h:82-88 perlin_desc */
+typedef struct rt_perlin_desc
+{
+    rt_vec3 random_vectors[256];
+    int32_t perm_x[256], perm_y[256], perm_z[256];
+} rt_perlin_desc;
+
+/* renderer.h:92-109 material_kind / material_desc */
+enum { RT_LAMBERTIAN = 0, RT_METAL = 1, RT_DIELECTRIC = 2, RT_DIFFUSE_LIGHT = 3, RT_ISOTROPIC = 4 };
+typedef struct rt_material_desc
+{
+    int32_t kind;
+    int32_t texture;          /* lambertian, diffuse_light, isotropic: index into textures */
+    rt_vec3 albedo;           /* metal */
+    double fuzz;              /* metal, at most 1 */
+    double refraction_index;  /* dielectric */
+} rt_material_desc;
+
+/* renderer.h:114-131 sphere_desc (world coordinates, instances baked) */
+typedef struct rt_sphere_desc
+{
+    rt_vec3 center;           /* at time 0 */
+    double radius;
+    int32_t material;
+    int32_t pad0;
+    rt_vec3 displacement;     /* motion over the shutter; exactly 0 for a sphere that stands still */
+    double uv_cos, uv_sin;    /* the turn of rotate_y instances, for texture coordinates */
+} rt_sphere_desc;
+
+/* renderer.h:134-141 quad_desc: points q + a*u + b*v, a, b in [0, 1]; front side u x v */
+typedef struct rt_quad_desc
+{
+    rt_vec3 q, u, v;
+    int32_t material;
+    int32_t pad0;
+} rt_quad_desc;
+
+/* renderer.h:146-162 medium_desc */
+enum { RT_BOUNDARY_SPHERE = 0, RT_BOUNDARY_CONVEX_QUADS = 1 };
+typedef struct rt_medium_desc
+{
+    int32_t boundary;
+    int32_t material;          /* isotropic */
+    rt_sphere_desc sphere;
+    const rt_quad_desc* quads;
+    int64_t quad_count;
+    double neg_inv_density;
+} rt_medium_desc;
+
+/* renderer.h:172-193 light_shape / light_desc: the books' lights list, instances baked */
+enum { RT_LIGHT_QUAD = 0, RT_LIGHT_SPHERE = 1 };
+typedef struct rt_light_desc
+{
+    int32_t kind;
+    int32_t pad0;
+    rt_quad_desc quad;
+    rt_vec3 center;
+    double radius;
+    double weight;             /* chance of aiming at it; the weights add up to 1 */
+} rt_light_desc;
+
+/* renderer.h:197-203 sampling_strategy */
+enum { RT_SAMPLING_UNIFORM = 0, RT_SAMPLING_MATERIAL = 1, RT_SAMPLING_LIGHTS = 2, RT_SAMPLING_MIXTURE = 3 };
+
+/* renderer.h:212-232 camera_desc, as the CPU's camera computed it from its settings (camera.ixx:138-182) */
+typedef struct rt_camera_desc
+{
+    int32_t image_width, image_height;
+    int32_t sqrt_spp;          /* a round of strata is sqrt_spp^2 passes */
+    int32_t max_depth;         /* rays per path, the camera ray included */
+    rt_vec3 center, pixel00_loc, pixel_delta_u, pixel_delta_v;
+    int32_t defocus;           /* rays start on the lens disk */
+    int32_t sampling;          /* RT_SAMPLING_*: effective_sampling of the requested strategy */
+    rt_vec3 defocus_disk_u, defocus_disk_v;
+    rt_vec3 sky_bottom, sky_top;
+} rt_camera_desc;
+
+/* renderer.h:239-266 light_combination, microfacet_kind / microfacet_desc, environment_desc */
+enum { RT_COMBINE_BSDF_ONLY = 0, RT_COMBINE_LIGHTS_ONLY = 1, RT_COMBINE_POWER_HEURISTIC = 2 };
+enum { RT_MICROFACET_NONE = 0, RT_MICROFACET_CONDUCTOR = 1, RT_MICROFACET_GLOSS = 2 };
+typedef struct rt_microfacet_desc
+{
+    int32_t kind;
+    int32_t pad0;
+    double roughness;          /* r in [0, 1]; the GGX width is alpha = r^2 */
+} rt_microfacet_desc;
+
+typedef struct rt_environment_desc
+{
+    rt_image_desc image;       /* equirectangular, +y up, row 0 = +y; finite and >= 0 */
+    double yaw_degrees;
+    double scale;
+} rt_environment_desc;
+
+/* Triangle meshes. The reference traces them only through OptiX (renderer.h:354-377); here they are traced by the
+ * same CUDA BVH as the spheres and quads. positions: 3 floats per vertex, world coordinates; indices: 3 per
+ * triangle; one scene material for the whole mesh. */
+typedef struct rt_mesh_desc
+{
+    const float* positions;
+    int64_t vertex_count;
+    const uint32_t* indices;
+    int64_t triangle_count;
+    int32_t material;
+    int32_t pad0;
+} rt_mesh_desc;
+
+/* renderer.h:381-395 scene_desc (+ quality_desc renderer.h:268-273, meshes traced by CUDA) */
+typedef struct rt_scene_desc
+{
+    const rt_sphere_desc* spheres;     int64_t sphere_count;
+    const rt_material_desc* materials; int64_t material_count;
+    rt_camera_desc camera;
+    const rt_texture_desc* textures;   int64_t texture_count;
+    const rt_image_desc* images;       int64_t image_count;
+    const rt_perlin_desc* perlins;     int64_t perlin_count;
+    const rt_quad_desc* quads;         int64_t quad_count;
+    const rt_medium_desc* media;       int64_t medium_count;
+    const rt_light_desc* lights;       int64_t light_count;
+    /* quality_desc */
+    int32_t combination;               /* RT_COMBINE_*: 0 renders with the books' strategies */
+    int32_t quality;                   /* nonzero: render with the NEE/MIS integrator (the reference's quality kernel) */
+    const rt_microfacet_desc* microfacets; int64_t microfacet_count; /* 0 or one per material */
+    const rt_environment_desc* environment;                          /* NULL: the camera's sky gradient */
+    const rt_mesh_desc* meshes;        int64_t mesh_count;
+} rt_scene_desc;
+
+/* ---- options and results: renderer.h:404-492, 530-562 -------------------------------------------------------- */
+
+enum { RT_FLOAT32 = 0, RT_FLOAT64 = 1 };
+
+typedef struct rt_render_options
+{
+    uint64_t seed;              /* round r draws with seed + r * 2^32 (renderer.h:564-566) */
+    int64_t passes;             /* 0: sqrt_spp^2; > 0: exactly that many */
+    int32_t arithmetic;         /* RT_FLOAT32 (the hot path); RT_FLOAT64 is refused: FP64 is used only where needed */
+    int32_t pad0;
+    double launch_seconds;      /* how long one launch is planned to take, (0, 0.5] */
+} rt_render_options;
+
+typedef struct rt_kernel_info
+{
+    char name[32];
+    int32_t registers;
+    int32_t local_bytes;
+    int32_t blocks_per_multiprocessor;
+    int32_t threads_per_block;
+    int32_t max_threads_per_multiprocessor;
+    int32_t multiprocessors;
+} rt_kernel_info;
+
+typedef struct rt_render_result
+{
+    double seconds;             /* render() end to end: validation, BVH, upload, all passes, download */
+    double kernel_seconds;      /* the passes alone, timed on the GPU */
+    uint64_t rays;              /* path segments: closest-hit queries, camera rays and bounces */
+    uint64_t shadow_rays;       /* NEE shadow queries, counted apart */
+    int64_t passes;
+    int32_t launches;
+    int32_t pad0;
+    rt_kernel_info kernel;
+} rt_render_result;
+
+typedef struct rt_device_info
+{
+    char name[256];
+    int32_t compute_capability_major, compute_capability_minor;
+    int32_t multiprocessors;
+    int32_t runtime_version, driver_version;
+    int32_t pad0;
+    double memory_gib;
+} rt_device_info;
+
+typedef struct rt_session_options
+{
+    uint64_t seed;
+    int32_t arithmetic;         /* RT_FLOAT32 */
+    int32_t pad0;
+    double launch_seconds;
+} rt_session_options;
+
+/* renderer.h:574-579 accumulation */
+typedef struct rt_accumulation
+{
+    int64_t passes;
+    int32_t rows;
+    int32_t pad0;
+} rt_accumulation;
+
+/* renderer.h:583-590 render_report */
+typedef struct rt_render_report
+{
+    rt_accumulation state;
+    int32_t launches;
+    int32_t pad0;
+    double gpu_seconds;
+    double longest_launch_seconds;
+} rt_render_report;
+
+/* ---- entry points ------------------------------------------------------------------------------------------ */
+
+/* The thread's last error message ("" after success). Replaces the what() of the reference's exceptions. */
+const char* rt_last_error_message(void);
+
+/* ABI version of the loaded library (RT_ABI_VERSION). */
+int32_t rt_abi_version(void);
+
+/* renderer.h:516 query_device(wait_mode): describes the first CUDA device and starts CUDA on it. */
+rt_status rt_query_device(rt_device_info* info);
+
+/* Selects the CUDA device this thread's later calls use (the reference renders on the first device only,
+ * renderer.h:512-518; one process per GPU calls this with its local rank). */
+rt_status rt_set_device(int32_t device);
+
+/* renderer.h:400 count_lamps: the quality integrator's lamps (quads and still spheres glowing one solid color). */
+rt_status rt_count_lamps(const rt_scene_desc* scene, int32_t* count);
+
+/* renderer.h:168 is_convex: whether quads bound one convex shape (a medium boundary the GPU can render). */
+rt_status rt_is_convex(const rt_quad_desc* quads, int64_t count, int32_t* convex);
+
+/* renderer.h:526 render(scene_desc, render_options) -> render_result. pixels: width*height*3 linear doubles, rows
+ * from the top (render_result::pixels, renderer.h:477-478); pixel_count must be width*height*3. */
+rt_status rt_render(const rt_scene_desc* scene, const rt_render_options* options, double* pixels,
+                    int64_t pixel_count, rt_render_result* result);
+
+/* A scene resident on the device: validated, its BVH built and uploaded once (the first half of the session
+ * constructor, renderer.h:596-601). Several sessions and serving requests may share one. */
+typedef struct rt_scene rt_scene;
+rt_status rt_scene_create(const rt_scene_desc* desc, rt_scene** scene);
+rt_status rt_scene_destroy(rt_scene* scene);
+/* Primitive and node counts and device bytes of the resident scene, for reports. */
+typedef struct rt_scene_stats
+{
+    int64_t spheres, quads, triangles, nodes, leaves, lamps, lights;
+    int64_t device_bytes;
+    int32_t depth;
+    int32_t max_leaf_size;
+} rt_scene_stats;
+rt_status rt_scene_stats_get(const rt_scene* scene, rt_scene_stats* stats);
+
+/* renderer.h:591-673 session: one view of a resident scene whose image gains passes on demand. */
+typedef struct rt_session rt_session;
+rt_status rt_session_create(rt_scene* scene, const rt_session_options* options, rt_session** session);
+rt_status rt_session_destroy(rt_session* session);
+/* set_camera (renderer.h:602): a new view; the image starts over. The strategy must stay the scene's. */
+rt_status rt_session_set_camera(rt_session* session, const rt_camera_desc* camera);
+rt_status rt_session_state(const rt_session* session, rt_accumulation* state);
+/* render_to({passes, 0}) (renderer.h:611): renders until the image has `passes` complete passes. */
+rt_status rt_session_render_to(rt_session* session, int64_t passes, rt_render_report* report);
+/* render_for(seconds, pass_limit) (renderer.h:618). */
+rt_status rt_session_render_for(rt_session* session, double seconds, int64_t pass_limit, rt_render_report* report);
+/* pixels() (renderer.h:623): sums / passes as doubles, width*height*3, rows from the top. */
+rt_status rt_session_pixels(const rt_session* session, double* pixels, int64_t pixel_count);
+/* rays(), shadow_rays(), kernel_seconds() (renderer.h:664-667), since the view was set */
+rt_status rt_session_counters(const rt_session* session, uint64_t* rays, uint64_t* shadow_rays,
+                              double* kernel_seconds);
+rt_status rt_session_kernel(const rt_session* session, rt_kernel_info* info);
+
+/* Device-resident variant for callers that keep the image on the GPU (a served frame, a display transform):
+ * the device address of the per-pixel sums (3 doubles per pixel, rows from the top) and of the pass count. */
+rt_status rt_session_device_sums(const rt_session* session, const double** sums, int64_t* passes);
+
+/* The counting build (no counterpart in the reference): while on, launches also count BVH node fetches and sphere,
+ * quad and triangle tests (closest-hit and shadow traversals together), the measured work behind the roofline's
+ * algorithmic bytes. Slower; off by default. counts: nodes, spheres, quads, triangles since the view was set. */
+rt_status rt_session_set_counting(rt_session* session, int32_t on);
+rt_status rt_session_fetch_counts(const rt_session* session, uint64_t counts[4]);
+
+/* ---- parity hooks (no counterpart in the reference's API: its GpuTests call device functions directly) ------ */
+
+/* Closest-hit queries for given rays on the device: the first hit's primitive in SOURCE index space (spheres
+ * 0..S-1, quads S..S+Q-1, triangles S+Q.. in mesh order; -1 for a miss) and its t, for the first-hit parity test
+ * (bvh.cuh:576-706 closest_hit; tracer_check_layout.h classes). Host arrays: origins and directions 3 floats each. */
+rt_status rt_scene_closest_hits(rt_scene* scene, const float* origins, const float* directions, int64_t count,
+                                int32_t* ids, float* ts);
+
+/* The deterministic camera rays of pass `pass` for every pixel of the scene's camera, as the kernel generates them
+ * (rows from the top), for the parity test: origins and directions, 3 floats each per pixel. */
+rt_status rt_scene_camera_rays(rt_scene* scene, uint64_t seed, int64_t pass, float* origins, float* directions,
+                               int64_t pixel_count);
+
+/* ---- built-in scenes (scenes.ixx:79-518, gpu_scenes*.ixx) ---------------------------------------------------- */
+
+/* A scene the library builds from its name, owning its tables. Names: "weekend" (cover, config 1), "cornell",
+ * "glass" (config 2 geometry), "cornell-mis" (glass under NEE+MIS), "materials", "quads", "furnace" (every pixel
+ * exactly 1: a closed white sky), "mesh-ggx" (config 3), "cover-N" (cover variant of about N random spheres, config
+ * 4, with its own seed). width, spp, depth override the scene's camera when > 0; scene_seed picks the scene's random
+ * content (the CPU's scene generator, mt19937_64 seeded as scenes.ixx's main thread). */
+typedef struct rt_builtin_params
+{
+    int32_t image_width;
+    int32_t image_height;       /* 0: from the scene's aspect ratio */
+    int32_t samples_per_pixel;  /* rounded to a square as camera.ixx:141 */
+    int32_t max_depth;
+    int32_t sampling;           /* -1: the scene's own; else RT_SAMPLING_* */
+    int32_t combination;        /* -1: the scene's own; else RT_COMBINE_* (nonzero turns on the NEE/MIS integrator) */
+    uint64_t scene_seed;
+    int32_t sphere_count;       /* cover-N: how many random spheres */
+    int32_t mesh_level;         /* mesh-ggx: icosphere subdivision level (8: 1,310,720 triangles) */
+    int32_t env_width;          /* mesh-ggx: environment map width (height = width / 2) */
+    int32_t pad0;
+    double orbit_azimuth;       /* when orbit != 0: camera orbits the look-at point (serving requests) */
+    double orbit_elevation;
+    int32_t orbit;
+    int32_t pad1;
+} rt_builtin_params;
+
+typedef struct rt_owned_scene rt_owned_scene;
+rt_status rt_builtin_scene(const char* name, const rt_builtin_params* params, rt_owned_scene** scene);
+const rt_scene_desc* rt_owned_scene_desc(const rt_owned_scene* scene);
+rt_status rt_owned_scene_destroy(rt_owned_scene* scene);
+/* A scene serialized once and fed to every renderer (the oracle, the reference build, this one). */
+rt_status rt_scene_save(const rt_scene_desc* scene, const char* path);
+rt_status rt_scene_load(const char* path, rt_owned_scene** scene);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RT_B200_H */

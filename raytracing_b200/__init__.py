@@ -1,0 +1,331 @@
+"""raytracing_b200: a B200-native path-tracing integrator behind the reference's scene API.
+
+The product is the C-ABI library `_lib/librt_b200.so` (include/rt_b200.h): a scene description in, linear pixels
+out, rendered by hand-written sm_100a kernels. This module is the thin Python face of that library, shaped like the
+reference's C++ interface (src/gpu/renderer.h): `render(scene, options)` and `Session` for a render that goes on,
+with the reference's exception classes mapped onto Python's (runtime_error -> RenderError, invalid_argument ->
+ValueError, logic_error -> LogicError). There is no CPU path: if the library is missing, importing works but every
+call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from ._abi import (RT_COMBINE_BSDF_ONLY, RT_COMBINE_LIGHTS_ONLY, RT_COMBINE_POWER_HEURISTIC, RT_SAMPLING_LIGHTS,
+                   RT_SAMPLING_MATERIAL, RT_SAMPLING_MIXTURE, RT_SAMPLING_UNIFORM)
+
+__all__ = ["RenderError", "LogicError", "NoDeviceError", "UnsupportedError", "CapacityError", "OwnedScene",
+           "builtin_scene", "load_scene", "query_device", "render", "Scene", "Session", "RenderResult",
+           "SAMPLING", "COMBINATION", "library_path"]
+
+SAMPLING = {"uniform": RT_SAMPLING_UNIFORM, "material": RT_SAMPLING_MATERIAL, "lights": RT_SAMPLING_LIGHTS,
+            "mixture": RT_SAMPLING_MIXTURE}
+COMBINATION = {"material": RT_COMBINE_BSDF_ONLY, "nee": RT_COMBINE_LIGHTS_ONLY, "mis": RT_COMBINE_POWER_HEURISTIC}
+
+
+class RenderError(RuntimeError):
+    """std::runtime_error in the reference: a CUDA failure or an inconsistent scene."""
+
+
+class LogicError(RuntimeError):
+    """std::logic_error in the reference: a call in the wrong state."""
+
+
+class NoDeviceError(RenderError):
+    """No CUDA device (query_device's runtime_error)."""
+
+
+class UnsupportedError(RenderError):
+    """A scene feature this build does not render."""
+
+
+class CapacityError(RenderError):
+    """A request beyond a stated limit."""
+
+
+def library_path() -> str:
+    return str(_abi.LIBRARY)
+
+
+def _lib():
+    return _abi.load()
+
+
+def _check(status: int) -> None:
+    if status == _abi.RT_OK:
+        return
+    message = _lib().rt_last_error_message().decode("utf-8", "replace")
+    if status == _abi.RT_ERR_INVALID:
+        raise ValueError(message)
+    if status == _abi.RT_ERR_LOGIC:
+        raise LogicError(message)
+    if status == _abi.RT_ERR_NO_DEVICE:
+        raise NoDeviceError(message)
+    if status == _abi.RT_ERR_UNSUPPORTED:
+        raise UnsupportedError(message)
+    if status == _abi.RT_ERR_CAPACITY:
+        raise CapacityError(message)
+    raise RenderError(message)
+
+
+class OwnedScene:
+    """A scene description owned by the library (built in, or loaded from a file)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._handle = handle
+
+    @property
+    def desc(self) -> "C._Pointer[_abi.SceneDesc]":
+        return _lib().rt_owned_scene_desc(self._handle)
+
+    @property
+    def camera(self) -> _abi.CameraDesc:
+        return self.desc.contents.camera
+
+    @property
+    def width(self) -> int:
+        return int(self.camera.image_width)
+
+    @property
+    def height(self) -> int:
+        return int(self.camera.image_height)
+
+    @property
+    def round_passes(self) -> int:
+        return int(self.camera.sqrt_spp) ** 2
+
+    def save(self, path: str) -> None:
+        _check(_lib().rt_scene_save(self.desc, str(path).encode()))
+
+    def count_lamps(self) -> int:
+        n = C.c_int32()
+        _check(_lib().rt_count_lamps(self.desc, C.byref(n)))
+        return int(n.value)
+
+    def close(self) -> None:
+        if self._handle:
+            _lib().rt_owned_scene_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def builtin_scene(name: str, width: int = 0, height: int = 0, spp: int = 0, depth: int = 0,
+                  sampling: Optional[str] = None, combination: Optional[str] = None, scene_seed: int = 0,
+                  sphere_count: int = 0, mesh_level: int = 0, env_width: int = 0,
+                  orbit: Optional[tuple[float, float]] = None) -> OwnedScene:
+    """A scene the library builds by name ("weekend", "cornell", "glass", "cornell-mis", "materials", "quads",
+    "furnace", "cover-N"): the reference's scene code, flattened as its GPU translator flattens it."""
+    p = _abi.BuiltinParams()
+    p.image_width = width
+    p.image_height = height
+    p.samples_per_pixel = spp
+    p.max_depth = depth
+    p.sampling = SAMPLING[sampling] if sampling else -1
+    p.combination = COMBINATION[combination] if combination else -1
+    p.scene_seed = scene_seed
+    p.sphere_count = sphere_count
+    p.mesh_level = mesh_level
+    p.env_width = env_width
+    if orbit is not None:
+        p.orbit = 1
+        p.orbit_azimuth, p.orbit_elevation = orbit
+    handle = C.c_void_p()
+    _check(_lib().rt_builtin_scene(name.encode(), C.byref(p), C.byref(handle)))
+    return OwnedScene(handle)
+
+
+def load_scene(path: str) -> OwnedScene:
+    handle = C.c_void_p()
+    _check(_lib().rt_scene_load(str(path).encode(), C.byref(handle)))
+    return OwnedScene(handle)
+
+
+def set_device(device: int) -> None:
+    """The CUDA device this thread's later calls use (one process per GPU passes its local rank)."""
+    _check(_lib().rt_set_device(device))
+
+
+def query_device() -> dict:
+    info = _abi.DeviceInfo()
+    _check(_lib().rt_query_device(C.byref(info)))
+    return {"name": info.name.decode(), "compute_capability": (info.compute_capability_major,
+                                                                  info.compute_capability_minor),
+            "multiprocessors": info.multiprocessors, "memory_gib": info.memory_gib,
+            "runtime_version": info.runtime_version, "driver_version": info.driver_version}
+
+
+def _kernel_dict(k: _abi.KernelInfo) -> dict:
+    return {"name": k.name.decode(), "registers": k.registers, "local_bytes": k.local_bytes,
+            "blocks_per_multiprocessor": k.blocks_per_multiprocessor, "threads_per_block": k.threads_per_block,
+            "max_threads_per_multiprocessor": k.max_threads_per_multiprocessor,
+            "multiprocessors": k.multiprocessors}
+
+
+@dataclass
+class RenderResult:
+    """render_result of renderer.h:475-492: pixels are height x width x 3 linear doubles, rows from the top."""
+    pixels: np.ndarray
+    seconds: float
+    kernel_seconds: float
+    rays: int
+    shadow_rays: int
+    passes: int
+    launches: int
+    kernel: dict
+
+
+def _desc_of(scene) -> "C._Pointer[_abi.SceneDesc]":
+    return scene.desc if isinstance(scene, OwnedScene) else scene
+
+
+def render(scene, seed: int = 0, passes: int = 0, launch_seconds: float = 0.05,
+           out: Optional[np.ndarray] = None) -> RenderResult:
+    """renderer.h:526 render(): the whole job through the C-ABI, host tables in, host pixels out."""
+    desc = _desc_of(scene)
+    cam = desc.contents.camera
+    h, w = int(cam.image_height), int(cam.image_width)
+    pixels = out if out is not None else np.empty((h, w, 3), dtype=np.float64)
+    if pixels.shape != (h, w, 3) or pixels.dtype != np.float64 or not pixels.flags.c_contiguous:
+        raise ValueError("out must be a C-contiguous float64 array of shape (height, width, 3)")
+    o = _abi.RenderOptions(seed=seed, passes=passes, arithmetic=_abi.RT_FLOAT32, launch_seconds=launch_seconds)
+    r = _abi.RenderResult()
+    _check(_lib().rt_render(desc, C.byref(o), pixels.ctypes.data_as(C.POINTER(C.c_double)), pixels.size,
+                            C.byref(r)))
+    return RenderResult(pixels, r.seconds, r.kernel_seconds, r.rays, r.shadow_rays, r.passes, r.launches,
+                        _kernel_dict(r.kernel))
+
+
+class Scene:
+    """A scene resident on the device: validated, its BVH built and uploaded once."""
+
+    def __init__(self, scene):
+        self._owner = scene  # keeps an OwnedScene's tables alive while this lives
+        handle = C.c_void_p()
+        _check(_lib().rt_scene_create(_desc_of(scene), C.byref(handle)))
+        self._handle = handle
+        desc = _desc_of(scene).contents
+        self.width = int(desc.camera.image_width)
+        self.height = int(desc.camera.image_height)
+
+    def stats(self) -> dict:
+        s = _abi.SceneStats()
+        _check(_lib().rt_scene_stats_get(self._handle, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in _abi.SceneStats._fields_}
+
+    def closest_hits(self, origins: np.ndarray, directions: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, dtype=np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        ids = np.empty(n, dtype=np.int32)
+        ts = np.empty(n, dtype=np.float32)
+        _check(_lib().rt_scene_closest_hits(self._handle, o.ctypes.data_as(C.POINTER(C.c_float)),
+                                            d.ctypes.data_as(C.POINTER(C.c_float)), n,
+                                            ids.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            ts.ctypes.data_as(C.POINTER(C.c_float))))
+        return ids, ts
+
+    def camera_rays(self, seed: int, pass_index: int) -> tuple[np.ndarray, np.ndarray]:
+        n = self.width * self.height
+        o = np.empty((n, 3), dtype=np.float32)
+        d = np.empty((n, 3), dtype=np.float32)
+        _check(_lib().rt_scene_camera_rays(self._handle, seed, pass_index, o.ctypes.data_as(C.POINTER(C.c_float)),
+                                           d.ctypes.data_as(C.POINTER(C.c_float)), n))
+        return o, d
+
+    def close(self) -> None:
+        if self._handle:
+            _lib().rt_scene_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Session:
+    """renderer.h:591-673 session: one view whose image gains passes on demand; its sums stay on the device."""
+
+    def __init__(self, scene: Scene, seed: int = 0, launch_seconds: float = 0.05):
+        self._scene = scene
+        o = _abi.SessionOptions(seed=seed, arithmetic=_abi.RT_FLOAT32, launch_seconds=launch_seconds)
+        handle = C.c_void_p()
+        _check(_lib().rt_session_create(scene._handle, C.byref(o), C.byref(handle)))
+        self._handle = handle
+        self.width = scene.width
+        self.height = scene.height
+
+    def set_camera(self, camera: _abi.CameraDesc) -> None:
+        _check(_lib().rt_session_set_camera(self._handle, C.byref(camera)))
+        self.width = int(camera.image_width)
+        self.height = int(camera.image_height)
+
+    def state(self) -> int:
+        a = _abi.Accumulation()
+        _check(_lib().rt_session_state(self._handle, C.byref(a)))
+        return int(a.passes)
+
+    def render_to(self, passes: int) -> dict:
+        r = _abi.RenderReport()
+        _check(_lib().rt_session_render_to(self._handle, passes, C.byref(r)))
+        return {"passes": r.state.passes, "launches": r.launches, "gpu_seconds": r.gpu_seconds,
+                "longest_launch_seconds": r.longest_launch_seconds}
+
+    def render_for(self, seconds: float, pass_limit: int) -> dict:
+        r = _abi.RenderReport()
+        _check(_lib().rt_session_render_for(self._handle, seconds, pass_limit, C.byref(r)))
+        return {"passes": r.state.passes, "launches": r.launches, "gpu_seconds": r.gpu_seconds,
+                "longest_launch_seconds": r.longest_launch_seconds}
+
+    def pixels(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        px = out if out is not None else np.empty((self.height, self.width, 3), dtype=np.float64)
+        _check(_lib().rt_session_pixels(self._handle, px.ctypes.data_as(C.POINTER(C.c_double)), px.size))
+        return px
+
+    def counters(self) -> dict:
+        rays = C.c_uint64()
+        shadow = C.c_uint64()
+        seconds = C.c_double()
+        _check(_lib().rt_session_counters(self._handle, C.byref(rays), C.byref(shadow), C.byref(seconds)))
+        return {"rays": rays.value, "shadow_rays": shadow.value, "kernel_seconds": seconds.value}
+
+    def kernel(self) -> dict:
+        k = _abi.KernelInfo()
+        _check(_lib().rt_session_kernel(self._handle, C.byref(k)))
+        return _kernel_dict(k)
+
+    def set_counting(self, on: bool) -> None:
+        _check(_lib().rt_session_set_counting(self._handle, 1 if on else 0))
+
+    def fetch_counts(self) -> dict:
+        v = (C.c_uint64 * 4)()
+        _check(_lib().rt_session_fetch_counts(self._handle, C.byref(v)))
+        return {"nodes": v[0], "spheres": v[1], "quads": v[2], "triangles": v[3]}
+
+    def device_sums(self) -> tuple[int, int]:
+        ptr = C.c_void_p()
+        passes = C.c_int64()
+        _check(_lib().rt_session_device_sums(self._handle, C.byref(ptr), C.byref(passes)))
+        return int(ptr.value or 0), int(passes.value)
+
+    def close(self) -> None:
+        if self._handle:
+            _lib().rt_session_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,285 @@
+// Binned SAH builder (Wald, "On fast Construction of SAH-based Bounding Volume Hierarchies", RT 2007): primitives
+// are binned by their box centroids on each axis, the split of least surface-area cost is taken, and recursion stops
+// at a leaf when a leaf is cheaper than any split (or the range is down to one primitive).
+#include "bvh_builder.h"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <stdexcept>
+#include <string>
+
+namespace rtb
+{
+float round_down(double x)
+{
+    const auto r = static_cast<float>(x);
+    return static_cast<double>(r) <= x ? r : std::nextafter(r, -std::numeric_limits<float>::infinity());
+}
+
+float round_up(double x)
+{
+    const auto r = static_cast<float>(x);
+    return static_cast<double>(r) >= x ? r : std::nextafter(r, std::numeric_limits<float>::infinity());
+}
+
+namespace
+{
+constexpr double inf = std::numeric_limits<double>::infinity();
+
+struct box
+{
+    double lo[3] = {inf, inf, inf};
+    double hi[3] = {-inf, -inf, -inf};
+    void grow(const box& b)
+    {
+        for (int a = 0; a < 3; ++a)
+        {
+            lo[a] = std::min(lo[a], b.lo[a]);
+            hi[a] = std::max(hi[a], b.hi[a]);
+        }
+    }
+    void grow(const double* p)
+    {
+        for (int a = 0; a < 3; ++a)
+        {
+            lo[a] = std::min(lo[a], p[a]);
+            hi[a] = std::max(hi[a], p[a]);
+        }
+    }
+    double area() const
+    {
+        const double dx = std::max(0.0, hi[0] - lo[0]);
+        const double dy = std::max(0.0, hi[1] - lo[1]);
+        const double dz = std::max(0.0, hi[2] - lo[2]);
+        return 2 * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
+class builder
+{
+public:
+    builder(std::vector<build_prim>& prims, const bvh_options& options, bvh_result& out)
+        : prims_(prims), options_(options), out_(out), index_(prims.size()), centroid_(prims.size() * 3),
+          bin_of_(prims.size())
+    {
+        for (size_t i = 0; i < prims.size(); ++i)
+        {
+            index_[i] = static_cast<int32_t>(i);
+            for (int a = 0; a < 3; ++a)
+            {
+                centroid_[3 * i + a] = 0.5 * (prims[i].lo[a] + prims[i].hi[a]);
+            }
+        }
+    }
+
+    void run()
+    {
+        const int n = static_cast<int>(prims_.size());
+        if (n == 0)
+        {
+            return;
+        }
+        box bounds;
+        const int32_t root = build(0, n, 1, bounds);
+        if (root < 0)
+        {
+            // A scene that is one leaf: a root node whose second child is the empty leaf, boxed at +infinity so that
+            // no ray enters it
+            bvh_node node{};
+            set_child(node, 0, root, bounds);
+            box far;
+            for (int a = 0; a < 3; ++a)
+            {
+                far.lo[a] = far.hi[a] = inf;
+            }
+            set_child(node, 1, leaf_link(0, 0, 0), far);
+            out_.nodes.insert(out_.nodes.begin(), node);
+        }
+    }
+
+private:
+    std::vector<build_prim>& prims_;
+    const bvh_options& options_;
+    bvh_result& out_;
+    std::vector<int32_t> index_;
+    std::vector<double> centroid_;
+    std::vector<int32_t> bin_of_;
+
+    static void set_child(bvh_node& node, int c, int32_t link, const box& b)
+    {
+        node.x[2 * c] = round_down(b.lo[0]);
+        node.x[2 * c + 1] = round_up(b.hi[0]);
+        node.y[2 * c] = round_down(b.lo[1]);
+        node.y[2 * c + 1] = round_up(b.hi[1]);
+        node.z[2 * c] = round_down(b.lo[2]);
+        node.z[2 * c + 1] = round_up(b.hi[2]);
+        node.link[c] = link;
+    }
+
+    box prim_box(int32_t i) const
+    {
+        box b;
+        for (int a = 0; a < 3; ++a)
+        {
+            b.lo[a] = prims_[static_cast<size_t>(i)].lo[a];
+            b.hi[a] = prims_[static_cast<size_t>(i)].hi[a];
+        }
+        return b;
+    }
+
+    int32_t make_leaf(int begin, int end)
+    {
+        const int32_t kind = prims_[static_cast<size_t>(index_[static_cast<size_t>(begin)])].kind;
+        std::vector<int32_t>& order = out_.order[kind];
+        const auto start = static_cast<int32_t>(order.size());
+        if (start >= (1 << (31 - leaf_start_shift)))
+        {
+            throw std::runtime_error("too many primitives of one kind for the leaf encoding (2^26)");
+        }
+        for (int i = begin; i < end; ++i)
+        {
+            order.push_back(prims_[static_cast<size_t>(index_[static_cast<size_t>(i)])].source);
+        }
+        ++out_.leaves;
+        return leaf_link(start, end - begin, kind);
+    }
+
+    // Returns the subtree's link: an inner node's index, or a leaf
+    int32_t build(int begin, int end, int depth, box& bounds)
+    {
+        bounds = box{};
+        box centroids;
+        bool one_kind = true;
+        const int32_t first_kind = prims_[static_cast<size_t>(index_[static_cast<size_t>(begin)])].kind;
+        for (int i = begin; i < end; ++i)
+        {
+            const int32_t p = index_[static_cast<size_t>(i)];
+            bounds.grow(prim_box(p));
+            centroids.grow(&centroid_[3 * static_cast<size_t>(p)]);
+            one_kind = one_kind && prims_[static_cast<size_t>(p)].kind == first_kind;
+        }
+        out_.depth = std::max(out_.depth, depth);
+        const int n = end - begin;
+        const int max_leaf = std::clamp(options_.max_leaf_size, 1, max_leaf_size);
+        if (n == 1)
+        {
+            return make_leaf(begin, end);
+        }
+
+        int split = -1;
+        if (!one_kind && n <= max_leaf)
+        {
+            // Few enough for one leaf but of several kinds: split off the first kind (stable, as bvh.cuh:404-410)
+            auto middle = std::stable_partition(index_.begin() + begin, index_.begin() + end, [&](int32_t p) {
+                return prims_[static_cast<size_t>(p)].kind == first_kind;
+            });
+            split = static_cast<int>(middle - index_.begin());
+        }
+        else
+        {
+            double best_cost = inf;
+            int best_axis = -1;
+            int best_bin = -1;
+            const int bins = std::clamp(options_.bins, 2, 256);
+            std::vector<box> bin_box(static_cast<size_t>(bins));
+            std::vector<int> bin_count(static_cast<size_t>(bins));
+            std::vector<double> right_area(static_cast<size_t>(bins));
+            std::vector<int> right_count(static_cast<size_t>(bins));
+            for (int axis = 0; axis < 3; ++axis)
+            {
+                const double lo = centroids.lo[axis];
+                const double extent = centroids.hi[axis] - lo;
+                if (!(extent > 0))
+                {
+                    continue;
+                }
+                std::fill(bin_box.begin(), bin_box.end(), box{});
+                std::fill(bin_count.begin(), bin_count.end(), 0);
+                const double scale = bins / extent;
+                for (int i = begin; i < end; ++i)
+                {
+                    const int32_t p = index_[static_cast<size_t>(i)];
+                    const int b = std::min(bins - 1, static_cast<int>((centroid_[3 * static_cast<size_t>(p) + axis] - lo) * scale));
+                    bin_box[static_cast<size_t>(b)].grow(prim_box(p));
+                    ++bin_count[static_cast<size_t>(b)];
+                }
+                box acc;
+                int count = 0;
+                for (int b = bins - 1; b > 0; --b)
+                {
+                    acc.grow(bin_box[static_cast<size_t>(b)]);
+                    count += bin_count[static_cast<size_t>(b)];
+                    right_area[static_cast<size_t>(b)] = acc.area();
+                    right_count[static_cast<size_t>(b)] = count;
+                }
+                acc = box{};
+                count = 0;
+                for (int b = 0; b < bins - 1; ++b)
+                {
+                    acc.grow(bin_box[static_cast<size_t>(b)]);
+                    count += bin_count[static_cast<size_t>(b)];
+                    const int rc = right_count[static_cast<size_t>(b + 1)];
+                    if (count == 0 || rc == 0)
+                    {
+                        continue;
+                    }
+                    const double cost = acc.area() * count + right_area[static_cast<size_t>(b + 1)] * rc;
+                    if (cost < best_cost)
+                    {
+                        best_cost = cost;
+                        best_axis = axis;
+                        best_bin = b;
+                    }
+                }
+            }
+            const double parent_area = bounds.area();
+            const double split_cost =
+                best_axis >= 0 && parent_area > 0 ? options_.node_cost + best_cost / parent_area : inf;
+            if (one_kind && n <= max_leaf && static_cast<double>(n) <= split_cost)
+            {
+                return make_leaf(begin, end);
+            }
+            if (best_axis >= 0)
+            {
+                const double lo = centroids.lo[best_axis];
+                const double scale = bins / (centroids.hi[best_axis] - lo);
+                auto middle = std::partition(index_.begin() + begin, index_.begin() + end, [&](int32_t p) {
+                    const int b = std::min(bins - 1, static_cast<int>((centroid_[3 * static_cast<size_t>(p) + best_axis] - lo) * scale));
+                    return b <= best_bin;
+                });
+                split = static_cast<int>(middle - index_.begin());
+            }
+            if (split <= begin || split >= end)
+            {
+                // All centroids in one place: halve the range by index
+                split = begin + n / 2;
+            }
+        }
+        if (depth + 1 > max_bvh_depth)
+        {
+            throw std::runtime_error("the BVH is deeper than the traversal stack (" + std::to_string(max_bvh_depth) +
+                                     " levels)");
+        }
+        const auto index = static_cast<int32_t>(out_.nodes.size());
+        out_.nodes.push_back(bvh_node{});
+        box left_box;
+        box right_box;
+        const int32_t left = build(begin, split, depth + 1, left_box);
+        const int32_t right = build(split, end, depth + 1, right_box);
+        bvh_node& node = out_.nodes[static_cast<size_t>(index)];
+        set_child(node, 0, left, left_box);
+        set_child(node, 1, right, right_box);
+        return index;
+    }
+};
+} // namespace
+
+bvh_result build_bvh(std::vector<build_prim> prims, const bvh_options& options)
+{
+    bvh_result out;
+    builder b(prims, options, out);
+    b.run();
+    return out;
+}
+} // namespace rtb

@@ -1,0 +1,153 @@
+// Plain data shared by the host code that builds a resident scene and the kernels that render it. Everything the
+// kernels read per ray is 16-byte aligned and fetched with 128-bit loads; a BVH node is 64 bytes (4 loads) and holds
+// the boxes of BOTH of its children, so one node fetch decides the whole step of the traversal (Aila and Laine,
+// "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009) where the reference's 32-byte node holds its own
+// box and a step reads two nodes (src/gpu/bvh.cuh:29-38, 680-693).
+#pragma once
+
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define RTB_HD __host__ __device__
+#else
+#define RTB_HD
+#endif
+
+namespace rtb
+{
+struct f3
+{
+    float x, y, z;
+};
+
+// A node: the boxes of its two children, laid out per axis so that the slab test of both children reads each axis
+// once: x = (lo0, hi0, lo1, hi1), likewise y and z. link[c] >= 0 is an inner node's index; link[c] < 0 is a leaf,
+// encoded in the link itself (see leaf_link), so a leaf needs no fetch of its own.
+struct alignas(64) bvh_node
+{
+    float x[4];
+    float y[4];
+    float z[4];
+    int32_t link[2];
+    int32_t pad[2];
+};
+static_assert(sizeof(bvh_node) == 64, "a node is four 16-byte loads");
+
+// Primitive kinds; a leaf holds primitives of one kind, contiguous in that kind's array
+enum prim_kind : int32_t
+{
+    kind_sphere = 0,
+    kind_quad = 1,
+    kind_triangle = 2,
+};
+
+constexpr int leaf_count_bits = 3; // at most 7 primitives in a leaf; 0 is the empty leaf
+constexpr int max_leaf_size = 7;
+constexpr int leaf_start_shift = 5;
+constexpr int max_bvh_depth = 64; // the traversal stack's size
+
+// ~link = start << 5 | count << 2 | kind
+RTB_HD inline int32_t leaf_link(int32_t start, int32_t count, int32_t kind)
+{
+    return ~((start << leaf_start_shift) | (count << 2) | kind);
+}
+RTB_HD inline int32_t leaf_kind(int32_t link) { return (~link) & 3; }
+RTB_HD inline int32_t leaf_count(int32_t link) { return ((~link) >> 2) & 7; }
+RTB_HD inline int32_t leaf_start(int32_t link) { return (~link) >> leaf_start_shift; }
+
+// A sphere: center and radius, one 16-byte load. A negative radius marks a sphere whose quadratic is solved in FP64
+// (its radius is large next to the distances rays travel to it, so FP32 cancels: the radius-1000 ground).
+struct alignas(16) sphere4
+{
+    float cx, cy, cz, r;
+};
+
+// A quad as hit_quad reads it (src/gpu/quad.cuh:19-46): a corner, the unit normal u x v, and the dual basis of (u, v)
+// in its plane, alpha_axis = v x w and beta_axis = w x u with w = n / |n|^2, 48 bytes: three 16-byte loads.
+struct alignas(16) quad12
+{
+    float qx, qy, qz, nx;
+    float ny, nz, ax, ay;
+    float az, bx, by, bz;
+};
+
+// A triangle: a vertex and two edges, 48 bytes (the last float is unused), three 16-byte loads
+struct alignas(16) triangle12
+{
+    float ax, ay, az, e1x;
+    float e1y, e1z, e2x, e2y;
+    float e2z, pad0, pad1, pad2;
+};
+
+// A material as the shading reads it (src/gpu/material.cuh:18-26)
+struct alignas(16) material8
+{
+    float r, g, b; // albedo, emission, or a metal's albedo (F0 for a GGX conductor)
+    int32_t kind;  // RT_LAMBERTIAN ...
+    float fuzz;
+    float ior;
+    int32_t lobe;  // 0 the books' material; 1 GGX conductor; 2 gloss coat (the quality integrator's side entry)
+    float alpha;   // GGX width r^2
+};
+
+// A shape of the books' lights list (src/gpu/lights.cuh:18-45): what lights_pdf_value and lights_random read
+struct alignas(16) light24
+{
+    quad12 quad;     // RT_LIGHT_QUAD: the hit test of the density
+    float ux, uy, uz, area;
+    float vx, vy, vz, cdf;
+    float cx, cy, cz, radius; // RT_LIGHT_SPHERE
+    float weight;
+    int32_t kind;
+    int32_t twin;    // the global id of the world's primitive with exactly these numbers, or -1
+    int32_t pad;
+};
+
+// A lamp of the NEE/MIS integrator's light set (src/gpu/lamps.cuh:34-47)
+struct alignas(16) emitter20
+{
+    float cx, cy, cz, size; // quad: corner, area; sphere: center, radius
+    float ux, uy, uz;
+    int32_t kind;
+    float vx, vy, vz;
+    int32_t primitive; // its global id
+    float nx, ny, nz, pad0;
+    float er, eg, eb, pad1;
+};
+
+// The camera (src/gpu/camera.cuh:33-50), pixel grid relative to the center computed in double on the host
+struct camera_params
+{
+    int32_t width, height, sqrt_spp, max_depth;
+    float recip_sqrt_spp;
+    f3 center;
+    f3 center_to_pixel00;
+    f3 delta_u, delta_v;
+    int32_t defocus;
+    f3 disk_u, disk_v;
+    f3 sky_bottom, sky_top;
+    int32_t sampling;
+};
+
+// The resident scene as the kernels see it
+struct scene_view
+{
+    const bvh_node* nodes;
+    const sphere4* spheres;     // global ids [0, quad_base)
+    const quad12* quads;        // [quad_base, triangle_base)
+    const triangle12* triangles;// [triangle_base, ...)
+    int32_t quad_base;
+    int32_t triangle_base;
+    int32_t node_count;
+    int32_t prim_count;
+    const int32_t* prim_material; // by global id
+    const material8* materials;
+    const light24* lights;
+    int32_t light_count;
+    int32_t lamp_count;
+    const emitter20* lamps;
+    const int32_t* lamp_of;     // by global id, -1: no lamp
+    float light_pmf;
+    int32_t combination;
+};
+} // namespace rtb

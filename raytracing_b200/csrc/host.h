@@ -1,0 +1,189 @@
+// The host runtime behind the C-ABI: errors, device memory, the resident scene and the session.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "device_types.h"
+#include "kernels.cuh"
+#include "rt_b200.h"
+
+namespace rtb
+{
+// An error with the status the C-ABI returns for it (the reference's exception classes, renderer.h:518-526)
+struct rt_error : std::runtime_error
+{
+    rt_status status;
+    rt_error(rt_status s, const std::string& message) : std::runtime_error(message), status(s) {}
+};
+
+[[noreturn]] void fail(rt_status status, const std::string& message);
+void check(cudaError_t e, const char* what);
+
+// Device memory owned by one object, freed with it
+template <class T>
+class device_array
+{
+public:
+    device_array() = default;
+    explicit device_array(size_t count) { allocate(count); }
+    ~device_array() { release(); }
+    device_array(const device_array&) = delete;
+    device_array& operator=(const device_array&) = delete;
+    device_array(device_array&& o) noexcept : data_(o.data_), count_(o.count_)
+    {
+        o.data_ = nullptr;
+        o.count_ = 0;
+    }
+    device_array& operator=(device_array&& o) noexcept
+    {
+        if (this != &o)
+        {
+            release();
+            data_ = o.data_;
+            count_ = o.count_;
+            o.data_ = nullptr;
+            o.count_ = 0;
+        }
+        return *this;
+    }
+
+    void allocate(size_t count)
+    {
+        release();
+        if (count > 0)
+        {
+            check(cudaMalloc(reinterpret_cast<void**>(&data_), count * sizeof(T)), "allocating device memory");
+        }
+        count_ = count;
+    }
+    void upload(const std::vector<T>& host)
+    {
+        allocate(host.size());
+        if (!host.empty())
+        {
+            check(cudaMemcpy(data_, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "copying to the device");
+        }
+    }
+    void release()
+    {
+        if (data_)
+        {
+            cudaFree(data_);
+        }
+        data_ = nullptr;
+        count_ = 0;
+    }
+    T* data() const { return data_; }
+    size_t size() const { return count_; }
+    size_t bytes() const { return count_ * sizeof(T); }
+
+private:
+    T* data_ = nullptr;
+    size_t count_ = 0;
+};
+
+// Checks a scene's tables before anything is built (the reference's validate, renderer.cu:688-900); throws rt_error
+void validate(const rt_scene_desc& desc);
+
+// The camera in the kernels' form: the pixel grid relative to the center subtracted in double (renderer.cu:512-532)
+camera_params to_camera(const rt_camera_desc& desc);
+
+// A scene on the device: its BVH, primitives, materials, lights and lamps, uploaded once
+class resident_scene
+{
+public:
+    explicit resident_scene(const rt_scene_desc& desc);
+
+    const scene_view& view() const { return view_; }
+    const rt_camera_desc& camera() const { return camera_; }
+    bool quality() const { return quality_; }
+    const int32_t* prim_source() const { return prim_source_.data(); }
+    const rt_scene_stats& stats() const { return stats_; }
+    int device() const { return device_; }
+
+private:
+    int device_ = 0;
+    rt_camera_desc camera_{};
+    bool quality_ = false;
+    scene_view view_{};
+    rt_scene_stats stats_{};
+    device_array<bvh_node> nodes_;
+    device_array<sphere4> spheres_;
+    device_array<quad12> quads_;
+    device_array<triangle12> triangles_;
+    device_array<int32_t> prim_material_;
+    device_array<int32_t> prim_source_;
+    device_array<material8> materials_;
+    device_array<light24> lights_;
+    device_array<emitter20> lamps_;
+    device_array<int32_t> lamp_of_;
+};
+
+// One view of a resident scene whose image gains passes on demand (renderer.h:591-673)
+class session
+{
+public:
+    session(std::shared_ptr<resident_scene> scene, const rt_session_options& options);
+    ~session();
+    session(const session&) = delete;
+    session& operator=(const session&) = delete;
+
+    void set_camera(const rt_camera_desc& camera);
+    rt_accumulation state() const { return {passes_, 0, 0}; }
+    rt_render_report render_to(int64_t target);
+    rt_render_report render_for(double seconds, int64_t pass_limit);
+    void pixels(double* out, int64_t count) const;
+    uint64_t rays() const;
+    uint64_t shadow_rays() const;
+    double kernel_seconds() const { return kernel_seconds_; }
+    rt_kernel_info kernel() const;
+    const double* device_sums() const { return sums_.data(); }
+    // The counting build: launches that also count node fetches and primitive tests (slower; for the roofline)
+    void set_counting(bool on) { counting_ = on; }
+    void fetch_counts(uint64_t out[4]) const;
+    const rt_camera_desc& camera() const { return camera_; }
+
+private:
+    std::shared_ptr<resident_scene> scene_;
+    rt_session_options options_;
+    rt_camera_desc camera_{};
+    camera_params cam_{};
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t start_ = nullptr;
+    cudaEvent_t stop_ = nullptr;
+    device_array<double> sums_;
+    device_array<double> partials_;
+    device_array<unsigned long long> counters_; // [0] work, [1] rays, [2] shadow rays, [3..6] the counting build's
+    bool counting_ = false;
+    int64_t passes_ = 0;
+    double kernel_seconds_ = 0;
+    double samples_per_second_ = 0;
+    int grid_ = 0;
+    int tiles_x_ = 0;
+    int padded_pixels_ = 0;
+    int64_t max_partial_entries_ = 0;
+
+    // Renders passes [passes_, end) in one launch and its reduction; returns its GPU seconds
+    double launch(int64_t end);
+    int64_t plan(int64_t target, double budget_seconds) const;
+};
+
+constexpr int pass_chunk = 16; // passes per work item; chunk boundaries are absolute multiples of it
+} // namespace rtb
+
+// The C-ABI's opaque handles
+struct rt_scene
+{
+    std::shared_ptr<rtb::resident_scene> scene;
+};
+
+struct rt_session
+{
+    std::unique_ptr<rtb::session> session;
+};

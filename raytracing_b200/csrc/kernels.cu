@@ -1,0 +1,1278 @@
+// The path-tracing kernels for sm_100a.
+//
+// One persistent kernel renders a launch: a grid of (multiprocessors x resident blocks) threads, each of which takes
+// work items (a pixel and a chunk of its passes) from a global counter, traces their samples one after another, and
+// starts the next sample the moment one ends (path regeneration), so a warp's lanes stay busy however uneven the
+// paths are. The lanes that need new work in an iteration claim it together: a ballot over the warp, one atomicAdd
+// by its leader for the whole batch, and each lane's item from the prefix count of the ballot below it. Each item's
+// sum goes to its own slot of a partials buffer, and a second kernel adds the slots to the pixels' sums in chunk
+// order, so the image does not depend on which thread rendered what.
+//
+// The estimators are the reference's: the books' strategies (src/gpu/camera.cuh:304-437 diffuse_bounce, trace_ray;
+// material.cuh:84-126 scatter; lights.cuh:49-227 the lights list) and the quality kernel's NEE with MIS
+// (quality_path.cuh:61-188, light_sampler.cuh:40-103, lamps.cuh:81-146, mis.cuh:30-62). What differs is the B200 form:
+// a 64-byte node holding both children's boxes, counter-based random numbers that depend only on (seed, pixel,
+// pass, depth, dimension), work items instead of one thread per pixel, and FP64 only for a large sphere's quadratic
+// and for the per-pixel sums.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.cuh"
+#include "rt_b200.h"
+
+namespace rtb
+{
+namespace
+{
+// ---- float3 arithmetic --------------------------------------------------------------------------------------
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float t, float3 v) { return make_float3(t * v.x, t * v.y, t * v.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float3 b) { return make_float3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross(float3 u, float3 v)
+{
+    return make_float3(u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x);
+}
+__device__ __forceinline__ float length_squared(float3 v) { return dot(v, v); }
+__device__ __forceinline__ float3 unit_vector(float3 v) { return rsqrtf(length_squared(v)) * v; }
+__device__ __forceinline__ float3 reflect(float3 v, float3 n) { return v - (2.0f * dot(v, n)) * n; }
+__device__ __forceinline__ float3 refract(float3 uv, float3 n, float etai_over_etat) // vec3.cuh refract
+{
+    const float cos_theta = fminf(dot(-uv, n), 1.0f);
+    const float3 perp = etai_over_etat * (uv + cos_theta * n);
+    const float3 parallel = (-sqrtf(fabsf(1.0f - length_squared(perp)))) * n;
+    return perp + parallel;
+}
+__device__ __forceinline__ float3 f3v(const f3& v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ float largest_channel(float3 c) { return fmaxf(fmaxf(c.x, c.y), c.z); }
+constexpr float pi_f = 3.14159265358979323846f;
+constexpr float inverse_pi_f = 0.318309886183790671538f;
+constexpr float uniform_sphere_density = 0.0795774715459476678844f; // 1 / (4 pi)
+constexpr float infinity_f = __builtin_huge_valf();
+
+// ---- counter-based random numbers ------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror and Shaw, "Parallel Random Numbers: As Easy as 1, 2, 3", SC 2011): ten rounds of
+// two 32x32->64 multiplies and a Feistel-like mix, keyed by the seed. The counter is (pixel, pass in the round,
+// depth << 4 | block, job): every number a sample draws is a pure function of the seed and where it is used, so a
+// seed fixes every image, whatever thread, launch or batch renders it.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+{
+#pragma unroll
+    for (int round = 0; round < 10; ++round)
+    {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// 24 random bits as a float in [0, 1 - 2^-24]: every value k / 2^24 exactly, as random_real<float> (random.cuh:79-93)
+__device__ __forceinline__ float to_unit(uint32_t x) { return static_cast<float>(x >> 8) * 0x1p-24f; }
+
+struct sampler
+{
+    uint2 key;
+    uint32_t pixel;
+    uint32_t pass;
+    uint32_t job;
+
+    // Four numbers for dimension block `block` of the vertex at depth `depth` (0: the camera ray)
+    __device__ __forceinline__ float4 draw(int depth, int block) const
+    {
+        const uint4 r = philox4x32_10(make_uint4(pixel, pass, (static_cast<uint32_t>(depth) << 4) | block, job), key);
+        return make_float4(to_unit(r.x), to_unit(r.y), to_unit(r.z), to_unit(r.w));
+    }
+};
+
+// The fixed dimension blocks of a vertex: block 0 the material's own sample (direction u0 u1, lobe or mixture
+// choice u2, the lights list's pick u3), block 1 the books' lights-list point, block 2 the NEE light sample
+constexpr int block_material = 0;
+constexpr int block_lights = 1;
+constexpr int block_nee = 2;
+
+// ---- sampling of directions (random.cuh:95-140, material.cuh:55-64) --------------------------------------------
+__device__ __forceinline__ float3 random_unit_vector(float u, float v)
+{
+    float s, c;
+    sincospif(2.0f * v, &s, &c);
+    const float r = 2.0f * sqrtf(u * (1.0f - u));
+    return make_float3(r * c, r * s, 1.0f - 2.0f * u);
+}
+
+__device__ __forceinline__ float3 random_cosine_direction(float r1, float r2)
+{
+    float s, c;
+    sincospif(2.0f * r1, &s, &c);
+    const float sin_theta = sqrtf(r2);
+    return make_float3(c * sin_theta, s * sin_theta, sqrtf(1.0f - r2));
+}
+
+// v given in a basis whose z axis is the unit vector n, in world coordinates: the branchless orthonormal basis of
+// Duff, Burgess, Christensen, Hery, Kensler, Liani and Villemin, "Building an Orthonormal Basis, Revisited" (JCGT 2017)
+__device__ __forceinline__ float3 around(float3 n, float3 v)
+{
+    const float sign = copysignf(1.0f, n.z);
+    const float a = -1.0f / (sign + n.z);
+    const float b = n.x * n.y * a;
+    const float3 x_axis = make_float3(1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x);
+    const float3 y_axis = make_float3(b, sign + n.y * n.y * a, -n.y);
+    return v.x * x_axis + v.y * y_axis + v.z * n;
+}
+
+__device__ __forceinline__ float cosine_density(float3 unit_normal, float3 direction) // pdf.cuh:21-26
+{
+    const float cosine = dot(unit_normal, direction) * rsqrtf(length_squared(direction));
+    return cosine > 0.0f ? cosine * inverse_pi_f : 0.0f;
+}
+
+// Schlick's reflectance (material.cuh:67-76)
+__device__ __forceinline__ float reflectance(float cosine, float ri)
+{
+    float r0 = (1.0f - ri) / (1.0f + ri);
+    r0 = r0 * r0;
+    const float x = 1.0f - cosine;
+    const float x2 = x * x;
+    return r0 + (1.0f - r0) * (x2 * x2 * x);
+}
+
+// ---- primitive tests ------------------------------------------------------------------------------------------
+// 1 / x, never infinite (bvh.cuh:475-488): |x| below 2^-80 moves out to +-2^-80
+__device__ __forceinline__ float safe_inverse(float x)
+{
+    const float tiny = 0x1p-80f;
+    return 1.0f / (fabsf(x) > tiny ? x : copysignf(tiny, x));
+}
+
+// The two roots of the line with a sphere, as (h/a) -+ sqrt(r^2 - |l|^2)/sqrt(a) with l the vector from the line's
+// closest point to the center (sphere.cuh:70-97, after Haines et al., Ray Tracing Gems ch. 7): nothing larger than
+// r^2 is subtracted, and the three squares go into r^2 through fused multiply-adds.
+__device__ __forceinline__ bool sphere_roots(float4 s, float3 o, float3 d, float inverse_a, float& near, float& far)
+{
+    if (s.w >= 0.0f)
+    {
+        const float3 oc = make_float3(s.x - o.x, s.y - o.y, s.z - o.z);
+        const float h_over_a = dot(d, oc) * inverse_a;
+        const float3 l = oc - h_over_a * d;
+        const float disc = fmaf(-l.x, l.x, fmaf(-l.y, l.y, fmaf(-l.z, l.z, s.w * s.w)));
+        if (disc < 0.0f)
+        {
+            return false;
+        }
+        const float half_chord = sqrtf(disc * inverse_a);
+        near = h_over_a - half_chord;
+        far = h_over_a + half_chord;
+        return true;
+    }
+    // A large sphere (negative radius): the same quadratic in FP64, where FP32's 24 bits cancel on its scale
+    const double r = -static_cast<double>(s.w);
+    const double ox = static_cast<double>(s.x) - o.x;
+    const double oy = static_cast<double>(s.y) - o.y;
+    const double oz = static_cast<double>(s.z) - o.z;
+    const double dx = d.x, dy = d.y, dz = d.z;
+    const double ia = 1.0 / (dx * dx + dy * dy + dz * dz);
+    const double hoa = (dx * ox + dy * oy + dz * oz) * ia;
+    const double lx = ox - hoa * dx, ly = oy - hoa * dy, lz = oz - hoa * dz;
+    const double disc = fma(-lx, lx, fma(-ly, ly, fma(-lz, lz, r * r)));
+    if (disc < 0.0)
+    {
+        return false;
+    }
+    const double half_chord = sqrt(disc * ia);
+    near = static_cast<float>(hoa - half_chord);
+    far = static_cast<float>(hoa + half_chord);
+    return true;
+}
+
+// hit_sphere (sphere.cuh:99-117): the nearest root in (t_min, t_max); far_only for the sphere the ray leaves inward
+__device__ __forceinline__ bool hit_sphere(float4 s, float3 o, float3 d, float inverse_a, float t_min, float t_max,
+                                           bool far_only, float& t, bool& entering)
+{
+    float near, far;
+    if (!sphere_roots(s, o, d, inverse_a, near, far))
+    {
+        return false;
+    }
+    t = near;
+    entering = !far_only && t > t_min;
+    if (!entering)
+    {
+        t = far;
+    }
+    return t_min < t && t < t_max;
+}
+
+struct quad_v
+{
+    float3 q, n, a, b;
+};
+
+__device__ __forceinline__ quad_v load_quad(const quad12* quads, int i)
+{
+    const float4* p = reinterpret_cast<const float4*>(quads + i);
+    const float4 a = __ldg(p);
+    const float4 b = __ldg(p + 1);
+    const float4 c = __ldg(p + 2);
+    return {make_float3(a.x, a.y, a.z), make_float3(a.w, b.x, b.y), make_float3(b.z, b.w, c.x),
+            make_float3(c.y, c.z, c.w)};
+}
+
+// hit_quad (quad.cuh:60-84): t in [t_min, t_max] and alpha, beta in [0, 1], closed; the corner taken relative to the
+// origin first. NaNs fail every comparison (a degenerate quad stays invisible).
+__device__ __forceinline__ bool hit_quad(const quad_v& s, float3 o, float3 d, float t_min, float t_max, float& t,
+                                         bool& front)
+{
+    const float denominator = dot(s.n, d);
+    if (!(fabsf(denominator) >= 1e-8f))
+    {
+        return false;
+    }
+    const float3 origin_to_q = s.q - o;
+    t = dot(s.n, origin_to_q) / denominator;
+    if (!(t_min <= t && t <= t_max))
+    {
+        return false;
+    }
+    const float3 p = t * d - origin_to_q;
+    const float alpha = dot(p, s.a);
+    const float beta = dot(p, s.b);
+    if (!(0.0f <= alpha && alpha <= 1.0f && 0.0f <= beta && beta <= 1.0f))
+    {
+        return false;
+    }
+    front = denominator < 0.0f;
+    return true;
+}
+
+struct triangle_v
+{
+    float3 a, e1, e2;
+};
+
+__device__ __forceinline__ triangle_v load_triangle(const triangle12* tris, int i)
+{
+    const float4* p = reinterpret_cast<const float4*>(tris + i);
+    const float4 a = __ldg(p);
+    const float4 b = __ldg(p + 1);
+    const float4 c = __ldg(p + 2);
+    return {make_float3(a.x, a.y, a.z), make_float3(a.w, b.x, b.y), make_float3(b.z, b.w, c.x)};
+}
+
+// Möller and Trumbore, "Fast, Minimum Storage Ray/Triangle Intersection" (JGT 1997): barycentrics closed, t open.
+// The front is the side e1 x e2 points to.
+__device__ __forceinline__ bool hit_triangle(const triangle_v& tr, float3 o, float3 d, float t_min, float t_max,
+                                             float& t, bool& front)
+{
+    const float3 pv = cross(d, tr.e2);
+    const float det = dot(tr.e1, pv);
+    if (!(fabsf(det) > 1e-30f))
+    {
+        return false;
+    }
+    const float inv = 1.0f / det;
+    const float3 tv = o - tr.a;
+    const float beta = dot(tv, pv) * inv;
+    if (!(beta >= 0.0f && beta <= 1.0f))
+    {
+        return false;
+    }
+    const float3 qv = cross(tv, tr.e1);
+    const float gamma = dot(d, qv) * inv;
+    if (!(gamma >= 0.0f && beta + gamma <= 1.0f))
+    {
+        return false;
+    }
+    t = dot(tr.e2, qv) * inv;
+    if (!(t_min < t && t < t_max))
+    {
+        return false;
+    }
+    front = det > 0.0f; // det = -d . (e1 x e2)
+    return true;
+}
+
+// ---- traversal ------------------------------------------------------------------------------------------------
+struct hit_info
+{
+    int id;     // global id, -1 for none
+    float t;
+    bool front; // the near root of a sphere, the front of a quad or a triangle
+};
+
+constexpr float t_min = 0.001f;
+
+// What one traversal fetched, for the counting build (the roofline's algorithmic bytes); compiled away otherwise
+struct fetch_counts
+{
+    uint32_t nodes = 0;
+    uint32_t spheres = 0;
+    uint32_t quads = 0;
+    uint32_t triangles = 0;
+};
+
+// The closest hit in (t_min, t_max) (SHADOW = false; the CPU's world.hit, bvh.cuh:576-706), or whether anything lies
+// there (SHADOW = true; shadow.cuh:26-109 occluded, `skip` not tested). The self-intersection rules of the primitive
+// the ray leaves, `from`: a quad or a triangle is never hit again (a line meets a plane once); a sphere left outward
+// is never hit again, and left inward only at its far root (bvh.cuh:539-575).
+template <bool SHADOW, bool COUNT = false>
+__device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d, float t_max, int from, bool inward,
+                                         int skip, hit_info& hit, fetch_counts* counts = nullptr)
+{
+    hit.id = -1;
+    hit.t = t_max;
+    hit.front = false;
+    if (S.node_count == 0)
+    {
+        return false;
+    }
+    const float inverse_a = 1.0f / length_squared(d);
+    const float3 inv = make_float3(safe_inverse(d.x), safe_inverse(d.y), safe_inverse(d.z));
+    const float3 os = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+    int2 stack[max_bvh_depth];
+    int sp = 0;
+    int link = 0;
+    while (true)
+    {
+        if (link >= 0)
+        {
+            const float4* np = reinterpret_cast<const float4*>(S.nodes + link);
+            const float4 nx = __ldg(np);
+            const float4 ny = __ldg(np + 1);
+            const float4 nz = __ldg(np + 2);
+            const int2 nl = __ldg(reinterpret_cast<const int2*>(np + 3));
+            if (COUNT)
+            {
+                ++counts->nodes;
+            }
+            const float a0 = fmaf(nx.x, inv.x, -os.x), a1 = fmaf(nx.y, inv.x, -os.x);
+            const float b0 = fmaf(ny.x, inv.y, -os.y), b1 = fmaf(ny.y, inv.y, -os.y);
+            const float c0 = fmaf(nz.x, inv.z, -os.z), c1 = fmaf(nz.y, inv.z, -os.z);
+            const float enter0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), t_min));
+            const float exit0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
+            const float a2 = fmaf(nx.z, inv.x, -os.x), a3 = fmaf(nx.w, inv.x, -os.x);
+            const float b2 = fmaf(ny.z, inv.y, -os.y), b3 = fmaf(ny.w, inv.y, -os.y);
+            const float c2 = fmaf(nz.z, inv.z, -os.z), c3 = fmaf(nz.w, inv.z, -os.z);
+            const float enter1 = fmaxf(fmaxf(fminf(a2, a3), fminf(b2, b3)), fmaxf(fminf(c2, c3), t_min));
+            const float exit1 = fminf(fminf(fmaxf(a2, a3), fmaxf(b2, b3)), fminf(fmaxf(c2, c3), hit.t));
+            const bool h0 = enter0 <= exit0;
+            const bool h1 = enter1 <= exit1;
+            if (h0 && h1)
+            {
+                const bool second_first = enter1 < enter0;
+                link = second_first ? nl.y : nl.x;
+                stack[sp++] = make_int2(second_first ? nl.x : nl.y, __float_as_int(second_first ? enter0 : enter1));
+                continue;
+            }
+            if (h0 || h1)
+            {
+                link = h0 ? nl.x : nl.y;
+                continue;
+            }
+        }
+        else
+        {
+            const int kind = leaf_kind(link);
+            const int count = leaf_count(link);
+            const int start = leaf_start(link);
+            if (COUNT)
+            {
+                (kind == kind_sphere ? counts->spheres : kind == kind_quad ? counts->quads : counts->triangles) +=
+                    count;
+            }
+            if (kind == kind_sphere)
+            {
+                for (int i = start; i < start + count; ++i)
+                {
+                    const int id = i; // spheres' global ids are their indices
+                    const bool own = id == from;
+                    if ((own && !inward) || id == skip)
+                    {
+                        continue;
+                    }
+                    const float4 s = __ldg(reinterpret_cast<const float4*>(S.spheres + i));
+                    float t;
+                    bool entering;
+                    if (hit_sphere(s, o, d, inverse_a, t_min, hit.t, own, t, entering))
+                    {
+                        if (SHADOW)
+                        {
+                            return true;
+                        }
+                        hit = {id, t, entering};
+                    }
+                }
+            }
+            else if (kind == kind_quad)
+            {
+                for (int i = start; i < start + count; ++i)
+                {
+                    const int id = S.quad_base + i;
+                    if (id == from || id == skip)
+                    {
+                        continue;
+                    }
+                    const quad_v q = load_quad(S.quads, i);
+                    float t;
+                    bool front;
+                    if (hit_quad(q, o, d, t_min, hit.t, t, front))
+                    {
+                        if (SHADOW)
+                        {
+                            return true;
+                        }
+                        hit = {id, t, front};
+                    }
+                }
+            }
+            else
+            {
+                for (int i = start; i < start + count; ++i)
+                {
+                    const int id = S.triangle_base + i;
+                    if (id == from || id == skip)
+                    {
+                        continue;
+                    }
+                    const triangle_v tr = load_triangle(S.triangles, i);
+                    float t;
+                    bool front;
+                    if (hit_triangle(tr, o, d, t_min, hit.t, t, front))
+                    {
+                        if (SHADOW)
+                        {
+                            return true;
+                        }
+                        hit = {id, t, front};
+                    }
+                }
+            }
+        }
+        // Nowhere to descend: the next entry of the stack that the ray enters before the closest hit so far
+        bool found = false;
+        while (sp > 0)
+        {
+            const int2 e = stack[--sp];
+            if (SHADOW || __int_as_float(e.y) < hit.t)
+            {
+                link = e.x;
+                found = true;
+                break;
+            }
+        }
+        if (!found)
+        {
+            break;
+        }
+    }
+    return hit.id >= 0;
+}
+
+// ---- the books' lights list (lights.cuh:49-227) ---------------------------------------------------------------
+__device__ __forceinline__ quad_v light_quad(const light24& l)
+{
+    return {make_float3(l.quad.qx, l.quad.qy, l.quad.qz), make_float3(l.quad.nx, l.quad.ny, l.quad.nz),
+            make_float3(l.quad.ax, l.quad.ay, l.quad.az), make_float3(l.quad.bx, l.quad.by, l.quad.bz)};
+}
+
+__device__ __forceinline__ float one_minus_cos_theta_max(float radius, float distance_squared)
+{
+    const float sin_squared = radius * radius / distance_squared;
+    return sin_squared / (1.0f + sqrtf(1.0f - sin_squared));
+}
+
+// |center - origin|^2 with its multiply-adds written out, so that the density and the sampler decide alike
+__device__ __forceinline__ float sphere_distance_squared(float3 v)
+{
+    return fmaf(v.z, v.z, fmaf(v.x, v.x, __fmul_rn(v.y, v.y)));
+}
+
+__device__ float lights_pdf_value(const scene_view& S, float3 origin, float3 direction, int from)
+{
+    float sum = 0.0f;
+    for (int k = 0; k < S.light_count; ++k)
+    {
+        const light24& l = S.lights[k];
+        const bool own = from >= 0 && l.twin == from;
+        if (l.kind == RT_LIGHT_QUAD)
+        {
+            if (own)
+            {
+                continue;
+            }
+            float t;
+            bool front;
+            if (!hit_quad(light_quad(l), origin, direction, t_min, infinity_f, t, front))
+            {
+                continue;
+            }
+            const float len2 = length_squared(direction);
+            const float distance_squared = t * t * len2;
+            const float3 n = make_float3(l.quad.nx, l.quad.ny, l.quad.nz);
+            const float cosine = fabsf(dot(direction, n)) * rsqrtf(len2);
+            sum += l.weight * (distance_squared / (cosine * l.area));
+        }
+        else
+        {
+            const float3 c = make_float3(l.cx, l.cy, l.cz);
+            const float3 to_center = c - origin;
+            const float distance_squared = sphere_distance_squared(to_center);
+            if (distance_squared < l.radius * l.radius)
+            {
+                sum += l.weight * uniform_sphere_density;
+                continue;
+            }
+            if (own && !(dot(direction, to_center) > 0.0f))
+            {
+                continue;
+            }
+            float t;
+            bool entering;
+            if (!hit_sphere(make_float4(c.x, c.y, c.z, l.radius), origin, direction, 1.0f / length_squared(direction),
+                            t_min, infinity_f, own, t, entering))
+            {
+                continue;
+            }
+            sum += l.weight * (1.0f / (2.0f * pi_f * one_minus_cos_theta_max(l.radius, distance_squared)));
+        }
+    }
+    return sum;
+}
+
+// lights_random: the running sums pick a light with `pick`; (a, b) draw its point or direction
+__device__ float3 lights_random(const scene_view& S, float3 origin, float pick, float a, float b)
+{
+    int k = 0;
+    while (k < S.light_count - 1 && !(pick < S.lights[k].cdf))
+    {
+        ++k;
+    }
+    const light24& l = S.lights[k];
+    if (l.kind == RT_LIGHT_QUAD)
+    {
+        const float3 q = make_float3(l.quad.qx, l.quad.qy, l.quad.qz);
+        return unit_vector((q - origin) + a * make_float3(l.ux, l.uy, l.uz) + b * make_float3(l.vx, l.vy, l.vz));
+    }
+    const float3 to_center = make_float3(l.cx, l.cy, l.cz) - origin;
+    const float distance_squared = sphere_distance_squared(to_center);
+    if (distance_squared < l.radius * l.radius)
+    {
+        return random_unit_vector(a, b);
+    }
+    const float one_minus_cos_max = one_minus_cos_theta_max(l.radius, distance_squared);
+    float s, c;
+    sincospif(2.0f * a, &s, &c);
+    const float one_minus_z = b * one_minus_cos_max;
+    const float sin_theta = sqrtf(one_minus_z * (2.0f - one_minus_z));
+    return around(rsqrtf(distance_squared) * to_center,
+                  make_float3(c * sin_theta, s * sin_theta, 1.0f - one_minus_z));
+}
+
+// ---- the NEE/MIS integrator's lamps and weights (lamps.cuh, light_sampler.cuh, mis.cuh) ------------------------
+__device__ __forceinline__ float power_weight(float self, float other)
+{
+    if (!(self > 0.0f))
+    {
+        return 0.0f;
+    }
+    const float r = other / self;
+    const float w = 1.0f / fmaf(r, r, 1.0f);
+    return w == w ? w : 0.0f;
+}
+
+__device__ __forceinline__ float light_weight(int c, float p_light, float p_bsdf)
+{
+    return c == RT_COMBINE_POWER_HEURISTIC ? power_weight(p_light, p_bsdf) : 1.0f;
+}
+
+__device__ __forceinline__ float bsdf_weight(int c, float p_bsdf, float p_light)
+{
+    if (c == RT_COMBINE_BSDF_ONLY || !(p_bsdf > 0.0f) || !(p_light > 0.0f))
+    {
+        return 1.0f;
+    }
+    return c == RT_COMBINE_POWER_HEURISTIC ? power_weight(p_bsdf, p_light) : 0.0f;
+}
+
+struct lamp_sample
+{
+    float3 wi;
+    float distance;
+    float pdf;
+};
+
+// sample_lamp (lamps.cuh:81-131): two numbers; false for the back of a quad or a point inside a sphere
+__device__ bool sample_lamp(const emitter20& e, float3 x, float a, float b, lamp_sample& out)
+{
+    const float3 corner = make_float3(e.cx, e.cy, e.cz);
+    if (e.kind == RT_LIGHT_QUAD)
+    {
+        const float3 to = (corner - x) + a * make_float3(e.ux, e.uy, e.uz) + b * make_float3(e.vx, e.vy, e.vz);
+        const float distance_squared = length_squared(to);
+        const float inverse_distance = rsqrtf(distance_squared);
+        out.wi = inverse_distance * to;
+        out.distance = distance_squared * inverse_distance;
+        const float cos_light = -dot(out.wi, make_float3(e.nx, e.ny, e.nz));
+        if (!(cos_light > 0.0f))
+        {
+            return false;
+        }
+        out.pdf = distance_squared / (cos_light * e.size);
+        return true;
+    }
+    const float3 to_center = corner - x;
+    const float distance_squared = sphere_distance_squared(to_center);
+    const float radius_squared = e.size * e.size;
+    if (!(distance_squared > radius_squared))
+    {
+        return false;
+    }
+    const float one_minus_cos_max = one_minus_cos_theta_max(e.size, distance_squared);
+    float s, c;
+    sincospif(2.0f * a, &s, &c);
+    const float one_minus_z = b * one_minus_cos_max;
+    const float sin_squared = one_minus_z * (2.0f - one_minus_z);
+    const float sin_theta = sqrtf(sin_squared);
+    const float cos_theta = 1.0f - one_minus_z;
+    const float inverse_distance = rsqrtf(distance_squared);
+    out.wi = around(inverse_distance * to_center, make_float3(c * sin_theta, s * sin_theta, cos_theta));
+    const float distance = distance_squared * inverse_distance;
+    out.distance = distance * cos_theta - sqrtf(fmaxf(0.0f, fmaf(-distance_squared, sin_squared, radius_squared)));
+    out.pdf = 1.0f / (2.0f * pi_f * one_minus_cos_max);
+    return true;
+}
+
+// lamp_pdf (lamps.cuh:136-146), for a ray from x that hit lamp e at `distance`
+__device__ float lamp_pdf(const emitter20& e, float3 x, float3 unit_dir, float distance)
+{
+    if (e.kind == RT_LIGHT_QUAD)
+    {
+        const float cos_light = -dot(unit_dir, make_float3(e.nx, e.ny, e.nz));
+        return cos_light > 0.0f ? distance * distance / (cos_light * e.size) : 0.0f;
+    }
+    const float distance_squared = sphere_distance_squared(make_float3(e.cx, e.cy, e.cz) - x);
+    return distance_squared > e.size * e.size
+               ? 1.0f / (2.0f * pi_f * one_minus_cos_theta_max(e.size, distance_squared))
+               : 0.0f;
+}
+
+// ---- the camera (camera.cuh:53-107) -----------------------------------------------------------------------------
+__device__ __forceinline__ void camera_ray(const camera_params& cam, int i, int j, int s_i, int s_j, float4 u,
+                                           float3& origin, float3& direction)
+{
+    const float dx = (static_cast<float>(s_i) + u.x) * cam.recip_sqrt_spp - 0.5f;
+    const float dy = (static_cast<float>(s_j) + u.y) * cam.recip_sqrt_spp - 0.5f;
+    const float3 to_sample = f3v(cam.center_to_pixel00) + (static_cast<float>(i) + dx) * f3v(cam.delta_u) +
+                             (static_cast<float>(j) + dy) * f3v(cam.delta_v);
+    origin = f3v(cam.center);
+    direction = to_sample;
+    if (cam.defocus)
+    {
+        // A uniform point of the unit disk: r = sqrt(u), angle 2 pi v (random.cuh:110-120)
+        const float r = sqrtf(u.z);
+        float s, c;
+        sincospif(2.0f * u.w, &s, &c);
+        const float3 lens = (r * c) * f3v(cam.disk_u) + (r * s) * f3v(cam.disk_v);
+        origin = origin + lens;
+        direction = to_sample - lens;
+    }
+}
+
+__device__ __forceinline__ float3 sky(const camera_params& cam, float3 direction)
+{
+    const float a = 0.5f * (unit_vector(direction).y + 1.0f);
+    return (1.0f - a) * f3v(cam.sky_bottom) + a * f3v(cam.sky_top);
+}
+
+__device__ __forceinline__ double without_nan(float x) { return static_cast<double>(x == x ? x : 0.0f); }
+
+// ---- one path: its state between segments ----------------------------------------------------------------------
+struct path_state
+{
+    float3 o, d;
+    float3 throughput;
+    float3 radiance; // the NEE/MIS integrator's light found so far
+    float bsdf_pdf;  // the density of d at a vertex that took a light sample; 0 otherwise
+    int rays_left;
+    int depth;       // rays traced so far in this sample (the next vertex's depth in the RNG counter)
+    int from;
+    bool inward;
+};
+
+// The hit as the shading needs it: point, outward normal, material, the hit's side
+struct surface
+{
+    float3 p;
+    float3 outward;
+    float3 normal;
+    int material;
+};
+
+__device__ __forceinline__ surface surface_at(const scene_view& S, const path_state& ps, const hit_info& h)
+{
+    surface s;
+    s.material = __ldg(S.prim_material + h.id);
+    if (h.id < S.quad_base)
+    {
+        const float4 sp = __ldg(reinterpret_cast<const float4*>(S.spheres + h.id));
+        s.p = ps.o + h.t * ps.d;
+        s.outward = (1.0f / fabsf(sp.w)) * (s.p - make_float3(sp.x, sp.y, sp.z));
+    }
+    else if (h.id < S.triangle_base)
+    {
+        // The quad's point as the CPU computes it, t * d rounded, then the sum (camera.cuh:175-195 at_unfused)
+        const quad_v q = load_quad(S.quads, h.id - S.quad_base);
+        s.p = make_float3(__fadd_rn(ps.o.x, __fmul_rn(h.t, ps.d.x)), __fadd_rn(ps.o.y, __fmul_rn(h.t, ps.d.y)),
+                          __fadd_rn(ps.o.z, __fmul_rn(h.t, ps.d.z)));
+        s.outward = q.n;
+    }
+    else
+    {
+        const triangle_v tr = load_triangle(S.triangles, h.id - S.triangle_base);
+        s.p = ps.o + h.t * ps.d;
+        s.outward = unit_vector(cross(tr.e1, tr.e2));
+    }
+    s.normal = h.front ? s.outward : -s.outward;
+    return s;
+}
+
+enum class step_result
+{
+    go_on,
+    done,
+};
+
+// One segment of a books' path (camera.cuh:364-437 trace_ray with diffuse_bounce 304-359 and scatter
+// material.cuh:84-126), after its closest hit
+__device__ __forceinline__ step_result shade_books(const scene_view& S, const camera_params& cam, const sampler& rng,
+                                                   path_state& ps, const hit_info& h, float3& sample)
+{
+    if (h.id < 0)
+    {
+        sample = ps.throughput * sky(cam, ps.d);
+        return step_result::done;
+    }
+    const surface s = surface_at(S, ps, h);
+    const material8 m = S.materials[s.material];
+    const float3 albedo = make_float3(m.r, m.g, m.b);
+    float3 direction;
+    if (m.kind == RT_DIFFUSE_LIGHT)
+    {
+        sample = h.front ? ps.throughput * albedo : make_float3(0.0f, 0.0f, 0.0f);
+        return step_result::done;
+    }
+    const float4 u = rng.draw(ps.depth, block_material);
+    if (m.kind == RT_LAMBERTIAN)
+    {
+        int strategy = cam.sampling;
+        if (strategy == RT_SAMPLING_MATERIAL)
+        {
+            direction = around(s.normal, random_cosine_direction(u.x, u.y));
+            if (!(dot(s.normal, direction) > 0.0f))
+            {
+                sample = make_float3(0.0f, 0.0f, 0.0f);
+                return step_result::done;
+            }
+            ps.throughput = ps.throughput * albedo;
+        }
+        else
+        {
+            bool toward_lights = strategy == RT_SAMPLING_LIGHTS;
+            if (strategy == RT_SAMPLING_MIXTURE)
+            {
+                toward_lights = u.z < 0.5f;
+            }
+            if (toward_lights)
+            {
+                const float4 v = rng.draw(ps.depth, block_lights);
+                direction = lights_random(S, s.p, u.w, v.x, v.y);
+            }
+            else
+            {
+                direction = strategy == RT_SAMPLING_UNIFORM ? random_unit_vector(u.x, u.y)
+                                                            : around(s.normal, random_cosine_direction(u.x, u.y));
+            }
+            const float p_scatter = cosine_density(s.normal, direction);
+            float p = uniform_sphere_density;
+            if (strategy != RT_SAMPLING_UNIFORM)
+            {
+                const float p_lights = lights_pdf_value(S, s.p, direction, h.id);
+                p = strategy == RT_SAMPLING_LIGHTS ? p_lights : 0.5f * p_lights + 0.5f * p_scatter;
+            }
+            if (!(p > 0.0f) || !(p_scatter > 0.0f))
+            {
+                sample = make_float3(0.0f, 0.0f, 0.0f);
+                return step_result::done;
+            }
+            ps.throughput = (p_scatter / p) * (ps.throughput * albedo);
+        }
+    }
+    else if (m.kind == RT_METAL)
+    {
+        direction = unit_vector(reflect(ps.d, s.normal)) + m.fuzz * random_unit_vector(u.x, u.y);
+        if (dot(direction, s.normal) <= 0.0f)
+        {
+            sample = make_float3(0.0f, 0.0f, 0.0f);
+            return step_result::done;
+        }
+        ps.throughput = ps.throughput * albedo;
+    }
+    else // dielectric
+    {
+        const float ri = h.front ? 1.0f / m.ior : m.ior;
+        const float3 ud = unit_vector(ps.d);
+        const float cos_theta = fminf(dot(-ud, s.normal), 1.0f);
+        const float sin_theta = sqrtf(1.0f - cos_theta * cos_theta);
+        const bool cannot_refract = ri * sin_theta > 1.0f;
+        direction = cannot_refract || reflectance(cos_theta, ri) > u.z ? reflect(ud, s.normal)
+                                                                       : refract(ud, s.normal, ri);
+    }
+    if (--ps.rays_left == 0)
+    {
+        sample = make_float3(0.0f, 0.0f, 0.0f);
+        return step_result::done;
+    }
+    ps.o = s.p;
+    ps.d = direction;
+    ps.from = h.id;
+    ps.inward = dot(direction, s.outward) < 0.0f;
+    return step_result::go_on;
+}
+
+// One segment of an NEE/MIS path (quality_path.cuh:83-188), after its closest hit. The shadow ray is traced here.
+template <bool COUNT>
+__device__ __forceinline__ step_result shade_quality(const scene_view& S, const camera_params& cam,
+                                                     const sampler& rng, path_state& ps, const hit_info& h,
+                                                     float3& sample, uint32_t& shadow_rays, fetch_counts* counts)
+{
+    if (h.id < 0)
+    {
+        // The sky: no light sample draws it, so it counts in full
+        sample = ps.radiance + ps.throughput * sky(cam, ps.d);
+        return step_result::done;
+    }
+    const surface s = surface_at(S, ps, h);
+    const material8 m = S.materials[s.material];
+    const float3 albedo = make_float3(m.r, m.g, m.b);
+    if (m.kind == RT_DIFFUSE_LIGHT)
+    {
+        float w = 1.0f;
+        if (ps.bsdf_pdf > 0.0f)
+        {
+            const int k = S.lamp_count > 0 ? __ldg(S.lamp_of + h.id) : -1;
+            float p_light = 0.0f;
+            if (k >= 0)
+            {
+                const float distance = h.t * sqrtf(length_squared(ps.d));
+                p_light = S.light_pmf * lamp_pdf(S.lamps[k], ps.o, unit_vector(ps.d), distance);
+            }
+            w = bsdf_weight(S.combination, ps.bsdf_pdf, p_light);
+        }
+        sample = ps.radiance + w * (h.front ? ps.throughput * albedo : make_float3(0.0f, 0.0f, 0.0f));
+        return step_result::done;
+    }
+    const bool delta = m.kind == RT_METAL || m.kind == RT_DIELECTRIC;
+    const bool nee = S.combination != RT_COMBINE_BSDF_ONLY && ps.rays_left > 1 && !delta && S.lamp_count > 0 &&
+                     largest_channel(ps.throughput) > 0.0f;
+    bool lit = false;
+    float3 contribution = make_float3(0.0f, 0.0f, 0.0f);
+    lamp_sample ls;
+    int skip = -1;
+    if (nee)
+    {
+        const float4 v = rng.draw(ps.depth, block_nee);
+        int k = static_cast<int>(v.x * static_cast<float>(S.lamp_count));
+        k = k < S.lamp_count ? k : S.lamp_count - 1;
+        const emitter20 e = S.lamps[k];
+        if (sample_lamp(e, s.p, v.y, v.z, ls))
+        {
+            const float p_light = S.light_pmf * ls.pdf;
+            const float p_bsdf = m.kind == RT_LAMBERTIAN ? cosine_density(s.normal, ls.wi) : uniform_sphere_density;
+            const float3 f = p_bsdf * albedo;
+            if (p_light > 0.0f && largest_channel(f) > 0.0f)
+            {
+                contribution = (light_weight(S.combination, p_light, p_bsdf) / p_light) *
+                               (ps.throughput * (f * make_float3(e.er, e.eg, e.eb)));
+                const float sum = contribution.x + contribution.y + contribution.z;
+                lit = sum > 0.0f && sum < infinity_f;
+                skip = e.primitive;
+            }
+        }
+    }
+    // The material's own sample: the path's next ray
+    const float4 u = rng.draw(ps.depth, block_material);
+    float3 wi;
+    float3 weight = albedo;
+    float pdf = 0.0f;
+    bool scattered = true;
+    if (m.kind == RT_LAMBERTIAN)
+    {
+        wi = around(s.normal, random_cosine_direction(u.x, u.y));
+        scattered = dot(s.normal, wi) > 0.0f;
+        pdf = cosine_density(s.normal, wi);
+    }
+    else if (m.kind == RT_METAL)
+    {
+        wi = unit_vector(reflect(ps.d, s.normal)) + m.fuzz * random_unit_vector(u.x, u.y);
+        scattered = dot(wi, s.normal) > 0.0f;
+    }
+    else if (m.kind == RT_DIELECTRIC)
+    {
+        const float ri = h.front ? 1.0f / m.ior : m.ior;
+        const float3 ud = unit_vector(ps.d);
+        const float cos_theta = fminf(dot(-ud, s.normal), 1.0f);
+        const float sin_theta = sqrtf(1.0f - cos_theta * cos_theta);
+        wi = ri * sin_theta > 1.0f || reflectance(cos_theta, ri) > u.z ? reflect(ud, s.normal)
+                                                                       : refract(ud, s.normal, ri);
+        weight = make_float3(1.0f, 1.0f, 1.0f);
+    }
+    else // isotropic
+    {
+        wi = random_unit_vector(u.x, u.y);
+        pdf = uniform_sphere_density;
+    }
+    if (lit)
+    {
+        ++shadow_rays;
+        hit_info blocker;
+        const bool blocked = traverse<true, COUNT>(S, s.p, ls.wi, ls.distance, h.id, dot(ls.wi, s.outward) < 0.0f,
+                                                   skip, blocker, counts);
+        if (!blocked)
+        {
+            ps.radiance = ps.radiance + contribution;
+        }
+    }
+    if (!scattered)
+    {
+        sample = ps.radiance;
+        return step_result::done;
+    }
+    ps.throughput = ps.throughput * weight;
+    ps.bsdf_pdf = nee ? pdf : 0.0f;
+    if (S.combination != RT_COMBINE_BSDF_ONLY && ps.throughput.x == 0.0f && ps.throughput.y == 0.0f &&
+        ps.throughput.z == 0.0f)
+    {
+        sample = ps.radiance;
+        return step_result::done;
+    }
+    if (--ps.rays_left == 0)
+    {
+        sample = ps.radiance;
+        return step_result::done;
+    }
+    ps.o = s.p;
+    ps.d = wi;
+    ps.from = h.id;
+    ps.inward = dot(wi, s.outward) < 0.0f;
+    return step_result::go_on;
+}
+
+// ---- the persistent render kernel ------------------------------------------------------------------------------
+template <bool QUALITY, bool COUNT>
+__global__ void __launch_bounds__(render_block) render_kernel(const __grid_constant__ launch_params P)
+{
+    __shared__ unsigned long long block_rays;
+    __shared__ unsigned long long block_shadow_rays;
+    if (threadIdx.x == 0)
+    {
+        block_rays = 0;
+        block_shadow_rays = 0;
+    }
+    __syncthreads();
+
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lanes_below = (1u << lane) - 1u;
+    const camera_params& cam = P.cam;
+
+    uint32_t rays = 0;
+    uint32_t shadow_rays = 0;
+    fetch_counts counts;
+    bool need = true;
+    bool start = false;
+    int px = 0, py = 0;
+    int64_t pass = 0, pass_end = 0;
+    int64_t slot = 0;
+    double acc_r = 0.0, acc_g = 0.0, acc_b = 0.0;
+    sampler rng{};
+    rng.job = P.job;
+    path_state ps{};
+
+    while (true)
+    {
+        // Claim work for the lanes that need it: one atomic per warp
+        const unsigned active = __activemask();
+        const unsigned needing = __ballot_sync(active, need);
+        if (needing != 0u)
+        {
+            const int leader = __ffs(static_cast<int>(needing)) - 1;
+            unsigned long long base = 0;
+            if (static_cast<int>(lane) == leader)
+            {
+                base = atomicAdd(P.work_counter, static_cast<unsigned long long>(__popc(needing)));
+            }
+            base = __shfl_sync(active, base, leader);
+            if (need)
+            {
+                const unsigned long long item = base + static_cast<unsigned long long>(__popc(needing & lanes_below));
+                if (item >= static_cast<unsigned long long>(P.total_items))
+                {
+                    break; // no work left for this lane
+                }
+                const int64_t k = static_cast<int64_t>(item / static_cast<unsigned long long>(P.padded_pixels));
+                const int q = static_cast<int>(item % static_cast<unsigned long long>(P.padded_pixels));
+                const int tile = q >> 5;
+                const int l = q & 31;
+                px = (tile % P.tiles_x) * 8 + (l & 7);
+                py = (tile / P.tiles_x) * 4 + (l >> 3);
+                if (px >= cam.width || py >= cam.height)
+                {
+                    continue; // a lane of a tile that hangs over the image's edge: nothing to render
+                }
+                const int64_t chunk_first = (P.first_chunk + k) * P.chunk;
+                pass = chunk_first > P.pass_begin ? chunk_first : P.pass_begin;
+                const int64_t chunk_end = chunk_first + P.chunk;
+                pass_end = chunk_end < P.pass_end ? chunk_end : P.pass_end;
+                slot = k * P.padded_pixels + q;
+                acc_r = acc_g = acc_b = 0.0;
+                rng.pixel = static_cast<uint32_t>(py) * static_cast<uint32_t>(cam.width) + static_cast<uint32_t>(px);
+                need = false;
+                start = true;
+            }
+        }
+        if (start)
+        {
+            // A new sample: pass n is pass n % k^2 of round n / k^2, whose numbers come from seed + round * 2^32
+            const int64_t round = pass / P.round_passes;
+            const int in_round = static_cast<int>(pass - round * P.round_passes);
+            const uint64_t key = P.seed + (static_cast<uint64_t>(round) << 32);
+            rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
+            rng.pass = static_cast<uint32_t>(in_round);
+            const float4 u = rng.draw(0, 0);
+            camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
+            ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
+            ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
+            ps.bsdf_pdf = 0.0f;
+            ps.rays_left = cam.max_depth;
+            ps.depth = 0;
+            ps.from = -1;
+            ps.inward = false;
+            start = false;
+        }
+
+        // One segment: the closest hit, then the vertex's shading
+        hit_info h;
+        traverse<false, COUNT>(P.scene, ps.o, ps.d, infinity_f, ps.from, ps.inward, -1, h, &counts);
+        ++rays;
+        ++ps.depth;
+        float3 sample;
+        const step_result r = QUALITY ? shade_quality<COUNT>(P.scene, cam, rng, ps, h, sample, shadow_rays, &counts)
+                                      : shade_books(P.scene, cam, rng, ps, h, sample);
+        if (r == step_result::done)
+        {
+            acc_r += without_nan(sample.x);
+            acc_g += without_nan(sample.y);
+            acc_b += without_nan(sample.z);
+            if (++pass == pass_end)
+            {
+                double* out = P.partials + 3 * slot;
+                out[0] = acc_r;
+                out[1] = acc_g;
+                out[2] = acc_b;
+                need = true;
+            }
+            else
+            {
+                start = true;
+            }
+        }
+    }
+    if (COUNT)
+    {
+        atomicAdd(P.counters + 2, static_cast<unsigned long long>(counts.nodes));
+        atomicAdd(P.counters + 3, static_cast<unsigned long long>(counts.spheres));
+        atomicAdd(P.counters + 4, static_cast<unsigned long long>(counts.quads));
+        atomicAdd(P.counters + 5, static_cast<unsigned long long>(counts.triangles));
+    }
+    atomicAdd(&block_rays, static_cast<unsigned long long>(rays));
+    if (QUALITY)
+    {
+        atomicAdd(&block_shadow_rays, static_cast<unsigned long long>(shadow_rays));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        atomicAdd(P.counters, block_rays);
+        if (QUALITY)
+        {
+            atomicAdd(P.counters + 1, block_shadow_rays);
+        }
+    }
+}
+
+// Adds each pixel's chunk partials to its sums, in chunk order (the sums are plain doubles in HBM, 24 bytes a pixel)
+__global__ void reduce_kernel(const reduce_params P)
+{
+    const int x = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = static_cast<int>(blockIdx.y);
+    if (x >= P.width || y >= P.height)
+    {
+        return;
+    }
+    const int q = ((y >> 2) * P.tiles_x + (x >> 3)) * 32 + ((y & 3) << 3) + (x & 7);
+    double* sum = P.sums + 3 * (static_cast<int64_t>(y) * P.width + x);
+    double r = sum[0], g = sum[1], b = sum[2];
+    for (int k = 0; k < P.chunks; ++k)
+    {
+        const double* part = P.partials + 3 * (static_cast<int64_t>(k) * P.padded_pixels + q);
+        r += part[0];
+        g += part[1];
+        b += part[2];
+    }
+    sum[0] = r;
+    sum[1] = g;
+    sum[2] = b;
+}
+
+__global__ void closest_hits_kernel(const scene_view S, const float* origins, const float* directions, int64_t count,
+                                    const int32_t* prim_source, int32_t* ids, float* ts)
+{
+    const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count)
+    {
+        return;
+    }
+    const float3 o = make_float3(origins[3 * i], origins[3 * i + 1], origins[3 * i + 2]);
+    const float3 d = make_float3(directions[3 * i], directions[3 * i + 1], directions[3 * i + 2]);
+    hit_info h;
+    traverse<false>(S, o, d, infinity_f, -1, false, -1, h);
+    ids[i] = h.id >= 0 ? prim_source[h.id] : -1;
+    ts[i] = h.id >= 0 ? h.t : infinity_f;
+}
+
+__global__ void camera_rays_kernel(const camera_params cam, uint64_t seed, int64_t pass, int32_t round_passes,
+                                   float* origins, float* directions)
+{
+    const int x = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = static_cast<int>(blockIdx.y);
+    if (x >= cam.width || y >= cam.height)
+    {
+        return;
+    }
+    const int64_t round = pass / round_passes;
+    const int in_round = static_cast<int>(pass - round * round_passes);
+    const uint64_t key = seed + (static_cast<uint64_t>(round) << 32);
+    sampler rng{make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32)),
+                static_cast<uint32_t>(y) * static_cast<uint32_t>(cam.width) + static_cast<uint32_t>(x),
+                static_cast<uint32_t>(in_round), 0u};
+    float3 o, d;
+    camera_ray(cam, x, y, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, rng.draw(0, 0), o, d);
+    const int64_t i = static_cast<int64_t>(y) * cam.width + x;
+    origins[3 * i] = o.x;
+    origins[3 * i + 1] = o.y;
+    origins[3 * i + 2] = o.z;
+    directions[3 * i] = d.x;
+    directions[3 * i + 1] = d.y;
+    directions[3 * i + 2] = d.z;
+}
+} // namespace
+
+cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream)
+{
+    if (quality)
+    {
+        if (counting)
+        {
+            render_kernel<true, true><<<grid, render_block, 0, stream>>>(p);
+        }
+        else
+        {
+            render_kernel<true, false><<<grid, render_block, 0, stream>>>(p);
+        }
+    }
+    else
+    {
+        if (counting)
+        {
+            render_kernel<false, true><<<grid, render_block, 0, stream>>>(p);
+        }
+        else
+        {
+            render_kernel<false, false><<<grid, render_block, 0, stream>>>(p);
+        }
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream)
+{
+    const dim3 block(128, 1);
+    const dim3 grid(static_cast<unsigned>((p.width + 127) / 128), static_cast<unsigned>(p.height));
+    reduce_kernel<<<grid, block, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t render_attributes(bool quality, kernel_attributes& out)
+{
+    cudaFuncAttributes a{};
+    cudaError_t e = quality ? cudaFuncGetAttributes(&a, render_kernel<true, false>)
+                            : cudaFuncGetAttributes(&a, render_kernel<false, false>);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    int device = 0;
+    e = cudaGetDevice(&device);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    int blocks = 0;
+    e = quality ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<true, false>, render_block, 0)
+                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<false, false>, render_block, 0);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    cudaDeviceProp prop{};
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    out.registers = a.numRegs;
+    out.local_bytes = static_cast<int>(a.localSizeBytes);
+    out.blocks_per_sm = blocks;
+    out.threads_per_block = render_block;
+    out.max_threads_per_sm = prop.maxThreadsPerMultiProcessor;
+    out.multiprocessors = prop.multiProcessorCount;
+    return cudaSuccess;
+}
+
+cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,
+                                const int32_t* prim_source, int32_t* ids, float* ts, cudaStream_t stream)
+{
+    if (count <= 0)
+    {
+        return cudaSuccess;
+    }
+    const int block = 128;
+    const auto grid = static_cast<unsigned>((count + block - 1) / block);
+    closest_hits_kernel<<<grid, block, 0, stream>>>(s, origins, directions, count, prim_source, ids, ts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_camera_rays(const camera_params& cam, uint64_t seed, int64_t pass, int32_t round_passes,
+                               float* origins, float* directions, cudaStream_t stream)
+{
+    const dim3 block(128, 1);
+    const dim3 grid(static_cast<unsigned>((cam.width + 127) / 128), static_cast<unsigned>(cam.height));
+    camera_rays_kernel<<<grid, block, 0, stream>>>(cam, seed, pass, round_passes, origins, directions);
+    return cudaGetLastError();
+}
+} // namespace rtb

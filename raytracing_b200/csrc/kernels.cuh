@@ -1,0 +1,69 @@
+// The launch interface between the host code (session.cpp) and the kernels (kernels.cu).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "device_types.h"
+
+namespace rtb
+{
+// One launch of the persistent render kernel: passes [pass_begin, pass_end) of every pixel of one view, cut into
+// work items (pixel, chunk of passes). Chunks are aligned to absolute multiples of `chunk` passes, so an image of N
+// passes is the same bit for bit however its passes were grouped into launches, as long as launches start and end
+// on chunk boundaries.
+struct launch_params
+{
+    scene_view scene;
+    camera_params cam;
+    uint64_t seed;          // round r of strata draws with seed + r * 2^32 (renderer.h:564-584)
+    int64_t pass_begin;
+    int64_t pass_end;
+    int64_t first_chunk;    // pass_begin / chunk
+    int32_t chunk;          // passes per work item
+    int32_t chunks;         // work items per pixel in this launch
+    int32_t tiles_x;        // the image in tiles of 8 x 4 pixels, a warp's worth
+    int32_t padded_pixels;  // tiles * 32
+    int64_t total_items;    // chunks * padded_pixels
+    int32_t round_passes;   // sqrt_spp^2
+    uint32_t job;           // a request's id in the RNG counter (0 for a plain render)
+    unsigned long long* work_counter;
+    double* partials;       // chunks * padded_pixels * 3
+    unsigned long long* counters; // [0] path segments, [1] shadow rays; the counting build also [2] node fetches,
+                                  // [3] sphere, [4] quad, [5] triangle tests
+};
+
+struct reduce_params
+{
+    const double* partials;
+    double* sums;           // width * height * 3
+    int32_t width, height;
+    int32_t tiles_x;
+    int32_t padded_pixels;
+    int32_t chunks;
+};
+
+// The kernels' static properties for kernel_info
+struct kernel_attributes
+{
+    int registers;
+    int local_bytes;
+    int blocks_per_sm;
+    int threads_per_block;
+    int max_threads_per_sm;
+    int multiprocessors;
+};
+
+constexpr int render_block = 128;
+
+cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream);
+cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream);
+cudaError_t render_attributes(bool quality, kernel_attributes& out);
+
+// Parity hooks: closest hits of given rays (source ids through prim_source), and the camera rays of one pass
+cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,
+                                const int32_t* prim_source, int32_t* ids, float* ts, cudaStream_t stream);
+cudaError_t launch_camera_rays(const camera_params& cam, uint64_t seed, int64_t pass, int32_t round_passes,
+                               float* origins, float* directions, cudaStream_t stream);
+} // namespace rtb

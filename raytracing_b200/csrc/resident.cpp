@@ -1,0 +1,591 @@
+// A scene made resident on the device: checked, its BVH built, every table converted to the kernels' 16-byte-aligned
+// form and copied once (the session constructor's first half in the reference, renderer.cu:1080-1199).
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <string>
+
+#include "bvh_builder.h"
+#include "host.h"
+
+namespace rtb
+{
+void fail(rt_status status, const std::string& message) { throw rt_error(status, message); }
+
+void check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess)
+    {
+        const rt_status s =
+            e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? RT_ERR_NO_DEVICE : RT_ERR_RUNTIME;
+        fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+namespace
+{
+bool finite(const rt_vec3& v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); }
+rt_vec3 sub(rt_vec3 a, rt_vec3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+rt_vec3 cross(rt_vec3 u, rt_vec3 v) { return {u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x}; }
+double dot(rt_vec3 a, rt_vec3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+rt_vec3 scale(double s, rt_vec3 v) { return {s * v.x, s * v.y, s * v.z}; }
+f3 to_f3(rt_vec3 v) { return {static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z)}; }
+
+std::string index_error(const char* table, int64_t i, const char* field, int64_t value)
+{
+    return std::string(table) + "[" + std::to_string(i) + "]." + field + " = " + std::to_string(value) +
+           " is out of range";
+}
+
+// make_quad (quad.cuh:40-52): the normal and the dual basis in double, rounded once
+quad12 make_quad(const rt_quad_desc& d)
+{
+    const rt_vec3 n = cross(d.u, d.v);
+    const rt_vec3 normal = scale(1 / std::sqrt(dot(n, n)), n);
+    const rt_vec3 w = scale(1 / dot(n, n), n);
+    const rt_vec3 a = cross(d.v, w);
+    const rt_vec3 b = cross(w, d.u);
+    quad12 q{};
+    q.qx = static_cast<float>(d.q.x);
+    q.qy = static_cast<float>(d.q.y);
+    q.qz = static_cast<float>(d.q.z);
+    q.nx = static_cast<float>(normal.x);
+    q.ny = static_cast<float>(normal.y);
+    q.nz = static_cast<float>(normal.z);
+    q.ax = static_cast<float>(a.x);
+    q.ay = static_cast<float>(a.y);
+    q.az = static_cast<float>(a.z);
+    q.bx = static_cast<float>(b.x);
+    q.by = static_cast<float>(b.y);
+    q.bz = static_cast<float>(b.z);
+    return q;
+}
+
+// A sphere whose quadratic is solved in FP64: radius large next to the spacing of floats at its center, where the
+// l-vector form's r^2 - |l|^2 is a difference of numbers near r^2 (the radius-1000 ground)
+constexpr double fp64_radius = 128;
+
+// quad_box (bvh.cuh:145-187): the corners widened by 1e-6 of the largest coordinate, and to 0.0001 at least
+build_prim quad_prim(const rt_quad_desc& d, int32_t source)
+{
+    const rt_vec3 c[4] = {d.q,
+                          {d.q.x + d.u.x, d.q.y + d.u.y, d.q.z + d.u.z},
+                          {d.q.x + d.v.x, d.q.y + d.v.y, d.q.z + d.v.z},
+                          {d.q.x + d.u.x + d.v.x, d.q.y + d.u.y + d.v.y, d.q.z + d.u.z + d.v.z}};
+    build_prim p{};
+    double largest = 0;
+    for (int a = 0; a < 3; ++a)
+    {
+        p.lo[a] = std::numeric_limits<double>::infinity();
+        p.hi[a] = -std::numeric_limits<double>::infinity();
+    }
+    for (const rt_vec3& v : c)
+    {
+        const double xyz[3] = {v.x, v.y, v.z};
+        for (int a = 0; a < 3; ++a)
+        {
+            p.lo[a] = std::min(p.lo[a], xyz[a]);
+            p.hi[a] = std::max(p.hi[a], xyz[a]);
+            largest = std::max(largest, std::fabs(xyz[a]));
+        }
+    }
+    const double margin = 1e-6 * (1 + largest);
+    for (int a = 0; a < 3; ++a)
+    {
+        p.lo[a] -= margin;
+        p.hi[a] += margin;
+        if (p.hi[a] - p.lo[a] < 0.0001)
+        {
+            p.lo[a] -= 0.00005;
+            p.hi[a] += 0.00005;
+        }
+    }
+    p.kind = kind_quad;
+    p.source = source;
+    return p;
+}
+} // namespace
+
+void validate(const rt_scene_desc& d)
+{
+    const rt_camera_desc& c = d.camera;
+    if (c.image_width < 1 || c.image_height < 1)
+    {
+        fail(RT_ERR_RUNTIME, "the camera's image must be at least 1 x 1 pixels");
+    }
+    if (static_cast<int64_t>(c.image_width) * c.image_height >= (int64_t{1} << 31))
+    {
+        fail(RT_ERR_RUNTIME, "the image has more than 2^31 pixels");
+    }
+    if (c.sqrt_spp < 1 || c.sqrt_spp > 46340)
+    {
+        fail(RT_ERR_RUNTIME, "camera.sqrt_spp must be in [1, 46340]");
+    }
+    if (c.max_depth < 0)
+    {
+        fail(RT_ERR_RUNTIME, "camera.max_depth must not be negative");
+    }
+    if (c.sampling < RT_SAMPLING_UNIFORM || c.sampling > RT_SAMPLING_MIXTURE)
+    {
+        fail(RT_ERR_RUNTIME, "camera.sampling is not a strategy");
+    }
+    if (!finite(c.center) || !finite(c.pixel00_loc) || !finite(c.pixel_delta_u) || !finite(c.pixel_delta_v) ||
+        !finite(c.defocus_disk_u) || !finite(c.defocus_disk_v) || !finite(c.sky_bottom) || !finite(c.sky_top))
+    {
+        fail(RT_ERR_RUNTIME, "the camera has a coordinate that is not a finite number");
+    }
+    if ((d.sphere_count > 0 && !d.spheres) || (d.quad_count > 0 && !d.quads) ||
+        (d.material_count > 0 && !d.materials) || (d.texture_count > 0 && !d.textures) ||
+        (d.light_count > 0 && !d.lights) || (d.mesh_count > 0 && !d.meshes))
+    {
+        fail(RT_ERR_RUNTIME, "a table has a count but no data");
+    }
+    for (int64_t i = 0; i < d.material_count; ++i)
+    {
+        const rt_material_desc& m = d.materials[i];
+        if (m.kind < RT_LAMBERTIAN || m.kind > RT_ISOTROPIC)
+        {
+            fail(RT_ERR_RUNTIME, "materials[" + std::to_string(i) + "] has no valid kind");
+        }
+        if (m.kind == RT_LAMBERTIAN || m.kind == RT_DIFFUSE_LIGHT || m.kind == RT_ISOTROPIC)
+        {
+            if (m.texture < 0 || m.texture >= d.texture_count)
+            {
+                fail(RT_ERR_RUNTIME, index_error("materials", i, "texture", m.texture));
+            }
+            if (d.textures[m.texture].kind != RT_TEXTURE_SOLID)
+            {
+                fail(RT_ERR_UNSUPPORTED, "materials[" + std::to_string(i) +
+                                             "]: textures other than one solid color are not rendered by this build");
+            }
+            if (!finite(d.textures[m.texture].rgb))
+            {
+                fail(RT_ERR_RUNTIME, "textures[" + std::to_string(m.texture) + "] is not finite");
+            }
+        }
+        if (m.kind == RT_ISOTROPIC)
+        {
+            fail(RT_ERR_UNSUPPORTED, "isotropic materials (smoke and fog) are not rendered by this build");
+        }
+        if (m.kind == RT_METAL && (!finite(m.albedo) || !(m.fuzz >= 0)))
+        {
+            fail(RT_ERR_RUNTIME, "materials[" + std::to_string(i) + "]: a metal needs a finite albedo and fuzz >= 0");
+        }
+        if (m.kind == RT_DIELECTRIC && !(m.refraction_index > 0 && std::isfinite(m.refraction_index)))
+        {
+            fail(RT_ERR_RUNTIME, "materials[" + std::to_string(i) + "]: refraction_index must be positive");
+        }
+    }
+    for (int64_t i = 0; i < d.sphere_count; ++i)
+    {
+        const rt_sphere_desc& s = d.spheres[i];
+        if (s.material < 0 || s.material >= d.material_count)
+        {
+            fail(RT_ERR_RUNTIME, index_error("spheres", i, "material", s.material));
+        }
+        if (!finite(s.center) || !(s.radius >= 0 && std::isfinite(s.radius)))
+        {
+            fail(RT_ERR_RUNTIME, "spheres[" + std::to_string(i) + "] is not a finite sphere");
+        }
+        if (s.displacement.x != 0 || s.displacement.y != 0 || s.displacement.z != 0)
+        {
+            fail(RT_ERR_UNSUPPORTED, "moving spheres (motion blur) are not rendered by this build");
+        }
+    }
+    for (int64_t i = 0; i < d.quad_count; ++i)
+    {
+        const rt_quad_desc& q = d.quads[i];
+        if (q.material < 0 || q.material >= d.material_count)
+        {
+            fail(RT_ERR_RUNTIME, index_error("quads", i, "material", q.material));
+        }
+        if (!finite(q.q) || !finite(q.u) || !finite(q.v))
+        {
+            fail(RT_ERR_RUNTIME, "quads[" + std::to_string(i) + "] is not finite");
+        }
+    }
+    for (int64_t m = 0; m < d.mesh_count; ++m)
+    {
+        const rt_mesh_desc& mesh = d.meshes[m];
+        if (mesh.material < 0 || mesh.material >= d.material_count)
+        {
+            fail(RT_ERR_RUNTIME, index_error("meshes", m, "material", mesh.material));
+        }
+        if ((mesh.triangle_count > 0 && (!mesh.indices || !mesh.positions)) || mesh.triangle_count < 0 ||
+            mesh.vertex_count < 0)
+        {
+            fail(RT_ERR_RUNTIME, "meshes[" + std::to_string(m) + "] has a count but no data");
+        }
+        for (int64_t k = 0; k < mesh.triangle_count * 3; ++k)
+        {
+            if (mesh.indices[k] >= static_cast<uint64_t>(mesh.vertex_count))
+            {
+                fail(RT_ERR_RUNTIME, index_error("meshes.indices", k, "vertex", mesh.indices[k]));
+            }
+        }
+    }
+    if (d.medium_count > 0)
+    {
+        fail(RT_ERR_UNSUPPORTED, "volumes of smoke (media) are not rendered by this build");
+    }
+    for (int64_t i = 0; i < d.light_count; ++i)
+    {
+        const rt_light_desc& l = d.lights[i];
+        if (l.kind != RT_LIGHT_QUAD && l.kind != RT_LIGHT_SPHERE)
+        {
+            fail(RT_ERR_RUNTIME, "lights[" + std::to_string(i) + "] has no valid kind");
+        }
+        if (!(l.weight >= 0 && std::isfinite(l.weight)))
+        {
+            fail(RT_ERR_RUNTIME, "lights[" + std::to_string(i) + "].weight must be finite and >= 0");
+        }
+        if (l.kind == RT_LIGHT_SPHERE && !(l.radius > 0))
+        {
+            fail(RT_ERR_RUNTIME, "lights[" + std::to_string(i) + "] is a sphere without size");
+        }
+    }
+    const bool aims = c.sampling == RT_SAMPLING_LIGHTS || c.sampling == RT_SAMPLING_MIXTURE;
+    if (aims && d.light_count == 0)
+    {
+        fail(RT_ERR_RUNTIME, "the lights and mixture strategies need a lights list to aim at");
+    }
+    if (d.combination < RT_COMBINE_BSDF_ONLY || d.combination > RT_COMBINE_POWER_HEURISTIC)
+    {
+        fail(RT_ERR_RUNTIME, "combination is not a light combination");
+    }
+    if (d.quality && c.sampling != RT_SAMPLING_MATERIAL)
+    {
+        fail(RT_ERR_INVALID, "the NEE/MIS integrator samples as the material scatters: camera.sampling must be material");
+    }
+    if (d.microfacet_count != 0 && d.microfacet_count != d.material_count)
+    {
+        fail(RT_ERR_RUNTIME, "microfacets: none, or one per material");
+    }
+    for (int64_t i = 0; i < d.microfacet_count; ++i)
+    {
+        if (d.microfacets[i].kind != RT_MICROFACET_NONE)
+        {
+            fail(RT_ERR_UNSUPPORTED, "GGX microfacet side entries are not rendered by this build yet");
+        }
+    }
+    if (d.environment)
+    {
+        fail(RT_ERR_UNSUPPORTED, "environment maps are not rendered by this build yet");
+    }
+}
+
+camera_params to_camera(const rt_camera_desc& d)
+{
+    camera_params c{};
+    c.width = d.image_width;
+    c.height = d.image_height;
+    c.sqrt_spp = d.sqrt_spp;
+    c.max_depth = d.max_depth;
+    c.recip_sqrt_spp = static_cast<float>(1.0 / d.sqrt_spp);
+    c.center = to_f3(d.center);
+    c.center_to_pixel00 = to_f3(sub(d.pixel00_loc, d.center));
+    c.delta_u = to_f3(d.pixel_delta_u);
+    c.delta_v = to_f3(d.pixel_delta_v);
+    c.defocus = d.defocus;
+    c.disk_u = to_f3(d.defocus_disk_u);
+    c.disk_v = to_f3(d.defocus_disk_v);
+    c.sky_bottom = to_f3(d.sky_bottom);
+    c.sky_top = to_f3(d.sky_top);
+    c.sampling = d.sampling;
+    return c;
+}
+
+resident_scene::resident_scene(const rt_scene_desc& d)
+{
+    validate(d);
+    check(cudaGetDevice(&device_), "selecting the CUDA device");
+    camera_ = d.camera;
+    quality_ = d.quality != 0;
+
+    // The primitives' boxes for the builder
+    std::vector<build_prim> prims;
+    std::vector<sphere4> source_spheres;
+    for (int64_t i = 0; i < d.sphere_count; ++i)
+    {
+        const rt_sphere_desc& s = d.spheres[i];
+        sphere4 v{static_cast<float>(s.center.x), static_cast<float>(s.center.y), static_cast<float>(s.center.z),
+                  static_cast<float>(s.radius)};
+        // sphere_box (bvh.cuh:140-152): the float sphere's extent, each bound one double step outward
+        build_prim p{};
+        const double c[3] = {v.cx, v.cy, v.cz};
+        for (int a = 0; a < 3; ++a)
+        {
+            p.lo[a] = std::nextafter(c[a] - static_cast<double>(v.r), -std::numeric_limits<double>::infinity());
+            p.hi[a] = std::nextafter(c[a] + static_cast<double>(v.r), std::numeric_limits<double>::infinity());
+        }
+        p.kind = kind_sphere;
+        p.source = static_cast<int32_t>(i);
+        prims.push_back(p);
+        if (s.radius >= fp64_radius)
+        {
+            v.r = -v.r;
+        }
+        source_spheres.push_back(v);
+    }
+    std::vector<quad12> source_quads;
+    for (int64_t i = 0; i < d.quad_count; ++i)
+    {
+        prims.push_back(quad_prim(d.quads[i], static_cast<int32_t>(i)));
+        source_quads.push_back(make_quad(d.quads[i]));
+    }
+    std::vector<triangle12> source_triangles;
+    std::vector<int32_t> triangle_material;
+    for (int64_t m = 0; m < d.mesh_count; ++m)
+    {
+        const rt_mesh_desc& mesh = d.meshes[m];
+        for (int64_t t = 0; t < mesh.triangle_count; ++t)
+        {
+            const float* a = mesh.positions + 3 * mesh.indices[3 * t];
+            const float* b = mesh.positions + 3 * mesh.indices[3 * t + 1];
+            const float* c = mesh.positions + 3 * mesh.indices[3 * t + 2];
+            triangle12 tr{};
+            tr.ax = a[0];
+            tr.ay = a[1];
+            tr.az = a[2];
+            tr.e1x = b[0] - a[0];
+            tr.e1y = b[1] - a[1];
+            tr.e1z = b[2] - a[2];
+            tr.e2x = c[0] - a[0];
+            tr.e2y = c[1] - a[1];
+            tr.e2z = c[2] - a[2];
+            build_prim p{};
+            double largest = 0;
+            for (int axis = 0; axis < 3; ++axis)
+            {
+                p.lo[axis] = std::min({static_cast<double>(a[axis]), static_cast<double>(b[axis]), static_cast<double>(c[axis])});
+                p.hi[axis] = std::max({static_cast<double>(a[axis]), static_cast<double>(b[axis]), static_cast<double>(c[axis])});
+                largest = std::max({largest, std::fabs(p.lo[axis]), std::fabs(p.hi[axis])});
+            }
+            const double margin = 1e-6 * (1 + largest);
+            for (int axis = 0; axis < 3; ++axis)
+            {
+                p.lo[axis] -= margin;
+                p.hi[axis] += margin;
+            }
+            p.kind = kind_triangle;
+            p.source = static_cast<int32_t>(source_triangles.size());
+            prims.push_back(p);
+            source_triangles.push_back(tr);
+            triangle_material.push_back(mesh.material);
+        }
+    }
+
+    bvh_options options;
+    options.max_leaf_size = prims.size() <= 8 ? 7 : (source_triangles.empty() ? 1 : 4);
+    const bvh_result tree = build_bvh(std::move(prims), options);
+
+    // Each kind's array in leaf order; global ids: spheres, then quads, then triangles
+    const auto S = static_cast<int32_t>(d.sphere_count);
+    const auto Q = static_cast<int32_t>(d.quad_count);
+    const auto T = static_cast<int32_t>(source_triangles.size());
+    std::vector<sphere4> spheres(tree.order[kind_sphere].size());
+    std::vector<quad12> quads(tree.order[kind_quad].size());
+    std::vector<triangle12> triangles(tree.order[kind_triangle].size());
+    std::vector<int32_t> prim_material(static_cast<size_t>(S + Q + T));
+    std::vector<int32_t> prim_source(static_cast<size_t>(S + Q + T));
+    std::vector<int32_t> sphere_gid(static_cast<size_t>(S));
+    std::vector<int32_t> quad_gid(static_cast<size_t>(Q));
+    for (size_t k = 0; k < spheres.size(); ++k)
+    {
+        const int32_t src = tree.order[kind_sphere][k];
+        spheres[k] = source_spheres[static_cast<size_t>(src)];
+        prim_material[k] = d.spheres[src].material;
+        prim_source[k] = src;
+        sphere_gid[static_cast<size_t>(src)] = static_cast<int32_t>(k);
+    }
+    for (size_t k = 0; k < quads.size(); ++k)
+    {
+        const int32_t src = tree.order[kind_quad][k];
+        quads[k] = source_quads[static_cast<size_t>(src)];
+        prim_material[static_cast<size_t>(S) + k] = d.quads[src].material;
+        prim_source[static_cast<size_t>(S) + k] = S + src;
+        quad_gid[static_cast<size_t>(src)] = S + static_cast<int32_t>(k);
+    }
+    for (size_t k = 0; k < triangles.size(); ++k)
+    {
+        const int32_t src = tree.order[kind_triangle][k];
+        triangles[k] = source_triangles[static_cast<size_t>(src)];
+        prim_material[static_cast<size_t>(S + Q) + k] = triangle_material[static_cast<size_t>(src)];
+        prim_source[static_cast<size_t>(S + Q) + k] = S + Q + src;
+    }
+
+    // Materials: a solid texture becomes the material's color (renderer.cu:551-600)
+    std::vector<material8> materials;
+    for (int64_t i = 0; i < d.material_count; ++i)
+    {
+        const rt_material_desc& m = d.materials[i];
+        material8 v{};
+        v.kind = m.kind;
+        const rt_vec3 color = m.kind == RT_METAL || m.kind == RT_DIELECTRIC ? m.albedo : d.textures[m.texture].rgb;
+        v.r = static_cast<float>(color.x);
+        v.g = static_cast<float>(color.y);
+        v.b = static_cast<float>(color.z);
+        v.fuzz = static_cast<float>(std::min(m.fuzz, 1.0));
+        v.ior = static_cast<float>(m.refraction_index);
+        materials.push_back(v);
+    }
+
+    // The books' lights list, with each light's twin (renderer.cu:968-1033): only the lights and mixture strategies
+    // read it
+    std::vector<light24> lights;
+    if (d.camera.sampling == RT_SAMPLING_LIGHTS || d.camera.sampling == RT_SAMPLING_MIXTURE)
+    {
+        double cdf = 0;
+        for (int64_t i = 0; i < d.light_count; ++i)
+        {
+            const rt_light_desc& l = d.lights[i];
+            cdf += l.weight;
+            light24 v{};
+            v.twin = -1;
+            if (l.kind == RT_LIGHT_QUAD)
+            {
+                v.quad = make_quad(l.quad);
+                const rt_vec3 n = cross(l.quad.u, l.quad.v);
+                v.ux = static_cast<float>(l.quad.u.x);
+                v.uy = static_cast<float>(l.quad.u.y);
+                v.uz = static_cast<float>(l.quad.u.z);
+                v.area = static_cast<float>(std::sqrt(dot(n, n)));
+                v.vx = static_cast<float>(l.quad.v.x);
+                v.vy = static_cast<float>(l.quad.v.y);
+                v.vz = static_cast<float>(l.quad.v.z);
+                for (int64_t q = 0; q < d.quad_count; ++q)
+                {
+                    const rt_quad_desc& w = d.quads[q];
+                    if (w.q.x == l.quad.q.x && w.q.y == l.quad.q.y && w.q.z == l.quad.q.z && w.u.x == l.quad.u.x &&
+                        w.u.y == l.quad.u.y && w.u.z == l.quad.u.z && w.v.x == l.quad.v.x && w.v.y == l.quad.v.y &&
+                        w.v.z == l.quad.v.z)
+                    {
+                        v.twin = quad_gid[static_cast<size_t>(q)];
+                        break;
+                    }
+                }
+            }
+            else
+            {
+                v.cx = static_cast<float>(l.center.x);
+                v.cy = static_cast<float>(l.center.y);
+                v.cz = static_cast<float>(l.center.z);
+                v.radius = static_cast<float>(l.radius);
+                for (int64_t s = 0; s < d.sphere_count; ++s)
+                {
+                    const rt_sphere_desc& w = d.spheres[s];
+                    if (w.center.x == l.center.x && w.center.y == l.center.y && w.center.z == l.center.z &&
+                        w.radius == l.radius)
+                    {
+                        v.twin = sphere_gid[static_cast<size_t>(s)];
+                        break;
+                    }
+                }
+            }
+            v.cdf = static_cast<float>(cdf);
+            v.weight = static_cast<float>(l.weight);
+            v.kind = l.kind;
+            lights.push_back(v);
+        }
+    }
+
+    // The NEE/MIS integrator's lamps: still spheres, then quads, glowing one solid color (lamp_table.cu)
+    std::vector<emitter20> lamps;
+    std::vector<int32_t> lamp_of(static_cast<size_t>(S + Q + T), -1);
+    const auto glows = [&](int32_t material) { return d.materials[material].kind == RT_DIFFUSE_LIGHT; };
+    const auto radiance = [&](int32_t material) { return d.textures[d.materials[material].texture].rgb; };
+    for (int64_t i = 0; i < d.sphere_count; ++i)
+    {
+        const rt_sphere_desc& s = d.spheres[i];
+        if (glows(s.material))
+        {
+            emitter20 e{};
+            e.cx = static_cast<float>(s.center.x);
+            e.cy = static_cast<float>(s.center.y);
+            e.cz = static_cast<float>(s.center.z);
+            e.size = static_cast<float>(s.radius);
+            e.kind = RT_LIGHT_SPHERE;
+            e.primitive = sphere_gid[static_cast<size_t>(i)];
+            const rt_vec3 r = radiance(s.material);
+            e.er = static_cast<float>(r.x);
+            e.eg = static_cast<float>(r.y);
+            e.eb = static_cast<float>(r.z);
+            lamp_of[static_cast<size_t>(e.primitive)] = static_cast<int32_t>(lamps.size());
+            lamps.push_back(e);
+        }
+    }
+    for (int64_t i = 0; i < d.quad_count; ++i)
+    {
+        const rt_quad_desc& q = d.quads[i];
+        if (glows(q.material))
+        {
+            const quad12 made = make_quad(q);
+            const rt_vec3 n = cross(q.u, q.v);
+            emitter20 e{};
+            e.cx = static_cast<float>(q.q.x);
+            e.cy = static_cast<float>(q.q.y);
+            e.cz = static_cast<float>(q.q.z);
+            e.size = static_cast<float>(std::sqrt(dot(n, n)));
+            e.ux = static_cast<float>(q.u.x);
+            e.uy = static_cast<float>(q.u.y);
+            e.uz = static_cast<float>(q.u.z);
+            e.kind = RT_LIGHT_QUAD;
+            e.vx = static_cast<float>(q.v.x);
+            e.vy = static_cast<float>(q.v.y);
+            e.vz = static_cast<float>(q.v.z);
+            e.primitive = quad_gid[static_cast<size_t>(i)];
+            e.nx = made.nx;
+            e.ny = made.ny;
+            e.nz = made.nz;
+            const rt_vec3 r = radiance(q.material);
+            e.er = static_cast<float>(r.x);
+            e.eg = static_cast<float>(r.y);
+            e.eb = static_cast<float>(r.z);
+            lamp_of[static_cast<size_t>(e.primitive)] = static_cast<int32_t>(lamps.size());
+            lamps.push_back(e);
+        }
+    }
+
+    nodes_.upload(tree.nodes);
+    spheres_.upload(spheres);
+    quads_.upload(quads);
+    triangles_.upload(triangles);
+    prim_material_.upload(prim_material);
+    prim_source_.upload(prim_source);
+    materials_.upload(materials);
+    lights_.upload(lights);
+    lamps_.upload(lamps);
+    lamp_of_.upload(lamp_of);
+
+    view_.nodes = nodes_.data();
+    view_.spheres = spheres_.data();
+    view_.quads = quads_.data();
+    view_.triangles = triangles_.data();
+    view_.quad_base = S;
+    view_.triangle_base = S + Q;
+    view_.node_count = static_cast<int32_t>(tree.nodes.size());
+    view_.prim_count = S + Q + T;
+    view_.prim_material = prim_material_.data();
+    view_.materials = materials_.data();
+    view_.lights = lights_.data();
+    view_.light_count = static_cast<int32_t>(lights.size());
+    view_.lamp_count = quality_ ? static_cast<int32_t>(lamps.size()) : 0;
+    view_.lamps = lamps_.data();
+    view_.lamp_of = lamp_of_.data();
+    view_.light_pmf = lamps.empty() ? 0.0f : static_cast<float>(1.0 / static_cast<double>(lamps.size()));
+    view_.combination = quality_ ? d.combination : RT_COMBINE_BSDF_ONLY;
+
+    stats_.spheres = S;
+    stats_.quads = Q;
+    stats_.triangles = T;
+    stats_.nodes = static_cast<int64_t>(tree.nodes.size());
+    stats_.leaves = tree.leaves;
+    stats_.lamps = static_cast<int64_t>(lamps.size());
+    stats_.lights = static_cast<int64_t>(lights.size());
+    stats_.device_bytes = static_cast<int64_t>(nodes_.bytes() + spheres_.bytes() + quads_.bytes() + triangles_.bytes() +
+                                               prim_material_.bytes() + prim_source_.bytes() + materials_.bytes() +
+                                               lights_.bytes() + lamps_.bytes() + lamp_of_.bytes());
+    stats_.depth = tree.depth;
+    stats_.max_leaf_size = options.max_leaf_size;
+}
+} // namespace rtb

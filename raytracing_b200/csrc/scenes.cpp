@@ -1,0 +1,834 @@
+// Built-in scenes, restated from the reference's scene code (src/scenes.ixx:79-518 and src/gpu_scenes.ixx) and
+// flattened the way its GPU translator flattens a CPU world (src/gpu_scene.ixx:89-168 placement, 670-745 lights):
+// instances are baked into world coordinates, the lights list is flattened with weights 1/n multiplied down nested
+// lists, and the camera is the frame the CPU's camera computes from its settings (src/camera.ixx:138-182).
+//
+// The scenes' random content is drawn once here, with std::mt19937_64 default-seeded as the CPU program's main thread
+// is (src/random.ixx:9-25, scenes.ixx:74-76) and std::uniform_real_distribution: that is implementation-defined
+// across standard libraries, so the cover scene built here is libstdc++'s, and every renderer (the oracle, the
+// reference's own GPU build, this one) is fed the same serialized tables.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numbers>
+#include <random>
+#include <string>
+
+#include "scene_store.h"
+
+namespace rtb
+{
+namespace
+{
+rt_vec3 v3(double x, double y, double z) { return {x, y, z}; }
+rt_vec3 add(rt_vec3 a, rt_vec3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+rt_vec3 sub(rt_vec3 a, rt_vec3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+rt_vec3 mul(double t, rt_vec3 v) { return {t * v.x, t * v.y, t * v.z}; }
+rt_vec3 hadamard(rt_vec3 a, rt_vec3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+rt_vec3 divide(rt_vec3 v, double t) { return mul(1 / t, v); } // vec3.ixx: v / t = (1 / t) * v
+double dot(rt_vec3 a, rt_vec3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+rt_vec3 cross(rt_vec3 u, rt_vec3 v)
+{
+    return {u.y * v.z - u.z * v.y, u.z * v.x - u.x * v.z, u.x * v.y - u.y * v.x};
+}
+double length(rt_vec3 v) { return std::sqrt(dot(v, v)); }
+rt_vec3 unit_vector(rt_vec3 v) { return divide(v, length(v)); }
+double degrees_to_radians(double d) { return d * std::numbers::pi / 180.0; }
+
+// The main thread's generator of the CPU program (random.ixx:9-25): default-constructed, never reseeded while scenes
+// are built. scene_seed != 0 reseeds it, for the batched jobs' cover variants that each have their own seed.
+class scene_random
+{
+public:
+    explicit scene_random(uint64_t seed)
+    {
+        if (seed != 0)
+        {
+            engine_.seed(seed);
+        }
+    }
+    double next() { return std::uniform_real_distribution<double>(0.0, 1.0)(engine_); }
+    double next(double lo, double hi) { return lo + (hi - lo) * next(); }
+    rt_vec3 vec() // vec3::random(): brace-initialized, so drawn x, y, z in order
+    {
+        const double x = next();
+        const double y = next();
+        const double z = next();
+        return {x, y, z};
+    }
+    rt_vec3 vec(double lo, double hi)
+    {
+        const double x = next(lo, hi);
+        const double y = next(lo, hi);
+        const double z = next(lo, hi);
+        return {x, y, z};
+    }
+
+private:
+    std::mt19937_64 engine_;
+};
+
+// gpu_scene.ixx:89-130 placement: a turn about y (rotate_y::to_world), then a shift
+struct placement
+{
+    double cos_theta = 1;
+    double sin_theta = 0;
+    rt_vec3 offset{0, 0, 0};
+
+    rt_vec3 turn(rt_vec3 v) const
+    {
+        return {cos_theta * v.x + sin_theta * v.z, v.y, -sin_theta * v.x + cos_theta * v.z};
+    }
+    rt_vec3 place(rt_vec3 p) const { return add(turn(p), offset); }
+    placement translated(rt_vec3 by) const { return {cos_theta, sin_theta, place(by)}; }
+    placement rotated_y(double degrees) const
+    {
+        const double s = std::sin(degrees_to_radians(degrees));
+        const double c = std::cos(degrees_to_radians(degrees));
+        return {cos_theta * c - sin_theta * s, sin_theta * c + cos_theta * s, offset};
+    }
+};
+
+// quad.ixx:118-140 box(): six faces whose u x v points out of the box
+void box_faces(rt_vec3 a, rt_vec3 b, std::vector<rt_quad_desc>& out, int material, const placement& where)
+{
+    const rt_vec3 mn{std::fmin(a.x, b.x), std::fmin(a.y, b.y), std::fmin(a.z, b.z)};
+    const rt_vec3 mx{std::fmax(a.x, b.x), std::fmax(a.y, b.y), std::fmax(a.z, b.z)};
+    const rt_vec3 dx{mx.x - mn.x, 0, 0};
+    const rt_vec3 dy{0, mx.y - mn.y, 0};
+    const rt_vec3 dz{0, 0, mx.z - mn.z};
+    const rt_vec3 neg_dx = mul(-1, dx);
+    const rt_vec3 neg_dz = mul(-1, dz);
+    const rt_vec3 faces[6][3] = {
+        {{mn.x, mn.y, mx.z}, dx, dy},     // front (z = max)
+        {{mx.x, mn.y, mx.z}, neg_dz, dy}, // right (x = max)
+        {{mx.x, mn.y, mn.z}, neg_dx, dy}, // back (z = min)
+        {{mn.x, mn.y, mn.z}, dz, dy},     // left (x = min)
+        {{mn.x, mx.y, mx.z}, dx, neg_dz}, // top (y = max)
+        {{mn.x, mn.y, mn.z}, dx, dz},     // bottom (y = min)
+    };
+    for (const auto& f : faces)
+    {
+        rt_quad_desc q{};
+        q.q = where.place(f[0]);
+        q.u = where.turn(f[1]);
+        q.v = where.turn(f[2]);
+        q.material = material;
+        out.push_back(q);
+    }
+}
+
+rt_quad_desc make_quad(rt_vec3 q, rt_vec3 u, rt_vec3 v, int material)
+{
+    rt_quad_desc d{};
+    d.q = q;
+    d.u = u;
+    d.v = v;
+    d.material = material;
+    return d;
+}
+
+rt_sphere_desc make_sphere(rt_vec3 center, double radius, int material)
+{
+    rt_sphere_desc s{};
+    s.center = center;
+    s.radius = std::fmax(0.0, radius);
+    s.material = material;
+    s.uv_cos = 1;
+    s.uv_sin = 0;
+    return s;
+}
+
+rt_light_desc quad_light(const rt_quad_desc& q, double weight)
+{
+    rt_light_desc l{};
+    l.kind = RT_LIGHT_QUAD;
+    l.quad = q;
+    l.quad.material = 0;
+    l.weight = weight;
+    return l;
+}
+
+rt_light_desc sphere_light(rt_vec3 center, double radius, double weight)
+{
+    rt_light_desc l{};
+    l.kind = RT_LIGHT_SPHERE;
+    l.center = center;
+    l.radius = radius;
+    l.weight = weight;
+    return l;
+}
+
+// camera.ixx:23-31 daylight_sky
+constexpr rt_vec3 daylight_bottom{1.0, 1.0, 1.0};
+constexpr rt_vec3 daylight_top{0.5, 0.7, 1.0};
+
+// scenes.ixx:130-142 cover_camera
+camera_settings cover_camera()
+{
+    camera_settings c;
+    c.aspect_ratio = 16.0 / 9.0;
+    c.image_width = 1920;
+    c.samples_per_pixel = 500;
+    c.max_depth = 50;
+    c.vfov = 20;
+    c.lookfrom = v3(13, 2, 3);
+    c.lookat = v3(0, 0, 0);
+    c.defocus_angle = 0.6;
+    c.focus_dist = 10.0;
+    c.sky_bottom = daylight_bottom;
+    c.sky_top = daylight_top;
+    return c;
+}
+
+// scenes.ixx:348-357 cornell_camera
+camera_settings cornell_camera()
+{
+    camera_settings c;
+    c.aspect_ratio = 1.0;
+    c.image_width = 1080;
+    c.samples_per_pixel = 1000;
+    c.max_depth = 50;
+    c.vfov = 40;
+    c.lookfrom = v3(278, 278, -800);
+    c.lookat = v3(278, 278, 0);
+    return c;
+}
+
+// scenes.ixx:79-127 random_spheres(false): the first book's cover. grid_half: the grid runs a, b in [-grid_half,
+// grid_half) (11 in the book); the small spheres keep the book's placement and material draws.
+void cover_world(scene_store& s, scene_random& rng, int grid_half)
+{
+    s.spheres.push_back(make_sphere(v3(0, -1000, 0), 1000, s.lambertian(v3(0.5, 0.5, 0.5))));
+    for (int a = -grid_half; a < grid_half; ++a)
+    {
+        for (int b = -grid_half; b < grid_half; ++b)
+        {
+            const double choose_mat = rng.next();
+            const double cx = a + 0.9 * rng.next();
+            const double cz = b + 0.9 * rng.next();
+            const rt_vec3 center{cx, 0.2, cz};
+            if (length(sub(center, v3(4, 0.2, 0))) <= 0.9)
+            {
+                continue;
+            }
+            int material;
+            if (choose_mat < 0.8)
+            {
+                const rt_vec3 c1 = rng.vec();
+                const rt_vec3 c2 = rng.vec();
+                material = s.lambertian(hadamard(c1, c2));
+            }
+            else if (choose_mat < 0.95)
+            {
+                const rt_vec3 albedo = rng.vec(0.5, 1);
+                material = s.metal(albedo, rng.next(0, 0.5));
+            }
+            else
+            {
+                material = s.dielectric(1.5);
+            }
+            s.spheres.push_back(make_sphere(center, 0.2, material));
+        }
+    }
+    s.spheres.push_back(make_sphere(v3(0, 1, 0), 1.0, s.dielectric(1.5)));
+    s.spheres.push_back(make_sphere(v3(-4, 1, 0), 1.0, s.lambertian(v3(0.4, 0.2, 0.1))));
+    s.spheres.push_back(make_sphere(v3(4, 1, 0), 1.0, s.metal(v3(0.7, 0.6, 0.5), 0.0)));
+}
+
+// scenes.ixx:294-305 add_cornell_walls
+void cornell_walls(scene_store& s)
+{
+    const int red = s.lambertian(v3(0.65, 0.05, 0.05));
+    const int white = s.lambertian(v3(0.73, 0.73, 0.73));
+    const int green = s.lambertian(v3(0.12, 0.45, 0.15));
+    s.quads.push_back(make_quad(v3(555, 0, 0), v3(0, 555, 0), v3(0, 0, 555), green));
+    s.quads.push_back(make_quad(v3(0, 0, 0), v3(0, 555, 0), v3(0, 0, 555), red));
+    s.quads.push_back(make_quad(v3(0, 0, 0), v3(555, 0, 0), v3(0, 0, 555), white));
+    s.quads.push_back(make_quad(v3(555, 555, 555), v3(-555, 0, 0), v3(0, 0, -555), white));
+    s.quads.push_back(make_quad(v3(0, 0, 555), v3(555, 0, 0), v3(0, 555, 0), white));
+}
+
+// scenes.ixx:331-335 cornell_lamp
+rt_quad_desc cornell_lamp(int material)
+{
+    return make_quad(v3(343, 554, 332), v3(-130, 0, 0), v3(0, 0, -105), material);
+}
+
+// scenes.ixx:310-322 tall_block / short_block: box, rotate_y, translate
+void tall_block(scene_store& s, int material)
+{
+    const placement where = placement{}.translated(v3(265, 0, 295)).rotated_y(15);
+    box_faces(v3(0, 0, 0), v3(165, 330, 165), s.quads, material, where);
+}
+
+void short_block(scene_store& s, int material)
+{
+    const placement where = placement{}.translated(v3(130, 0, 65)).rotated_y(-18);
+    box_faces(v3(0, 0, 0), v3(165, 165, 165), s.quads, material, where);
+}
+
+// Applies the overrides of rt_builtin_params to the scene's camera settings and computes the frame
+void set_camera(scene_store& s, camera_settings c, const rt_builtin_params& p, bool has_lights)
+{
+    if (p.image_width > 0)
+    {
+        c.image_width = p.image_width;
+    }
+    if (p.samples_per_pixel > 0)
+    {
+        c.samples_per_pixel = p.samples_per_pixel;
+    }
+    if (p.max_depth > 0)
+    {
+        c.max_depth = p.max_depth;
+    }
+    if (p.sampling >= 0)
+    {
+        c.sampling = p.sampling;
+    }
+    if (p.orbit != 0)
+    {
+        // A random orbit camera for served requests: the look-at point fixed, the distance kept
+        const rt_vec3 to = sub(c.lookfrom, c.lookat);
+        const double r = length(to);
+        const double az = p.orbit_azimuth;
+        const double el = p.orbit_elevation;
+        c.lookfrom = add(c.lookat, v3(r * std::cos(el) * std::sin(az), r * std::sin(el), r * std::cos(el) * std::cos(az)));
+    }
+    // camera.ixx:56-62 effective_sampling: lights and mixture need a lights list
+    const bool aims = c.sampling == RT_SAMPLING_LIGHTS || c.sampling == RT_SAMPLING_MIXTURE;
+    if (aims && !has_lights)
+    {
+        c.sampling = RT_SAMPLING_MATERIAL;
+    }
+    s.camera = camera_frame(c, p.image_height);
+}
+} // namespace
+
+int scene_store::add_solid_texture(rt_vec3 rgb)
+{
+    rt_texture_desc t{};
+    t.kind = RT_TEXTURE_SOLID;
+    t.even = t.odd = t.image = t.perlin = -1;
+    t.rgb = rgb;
+    t.inv_scale = 1;
+    t.scale = 1;
+    textures.push_back(t);
+    return static_cast<int>(textures.size()) - 1;
+}
+
+int scene_store::lambertian(rt_vec3 albedo)
+{
+    rt_material_desc m{};
+    m.kind = RT_LAMBERTIAN;
+    m.texture = add_solid_texture(albedo);
+    m.refraction_index = 1;
+    return add_material(m);
+}
+
+int scene_store::metal(rt_vec3 albedo, double fuzz)
+{
+    rt_material_desc m{};
+    m.kind = RT_METAL;
+    m.texture = -1;
+    m.albedo = albedo;
+    m.fuzz = std::min(fuzz, 1.0); // material.ixx:44 caps it
+    m.refraction_index = 1;
+    return add_material(m);
+}
+
+int scene_store::dielectric(double refraction_index)
+{
+    rt_material_desc m{};
+    m.kind = RT_DIELECTRIC;
+    m.texture = -1;
+    m.refraction_index = refraction_index;
+    return add_material(m);
+}
+
+int scene_store::diffuse_light(rt_vec3 emit)
+{
+    rt_material_desc m{};
+    m.kind = RT_DIFFUSE_LIGHT;
+    m.texture = add_solid_texture(emit);
+    m.refraction_index = 1;
+    return add_material(m);
+}
+
+const rt_scene_desc& scene_store::finish()
+{
+    desc = rt_scene_desc{};
+    desc.spheres = spheres.data();
+    desc.sphere_count = static_cast<int64_t>(spheres.size());
+    desc.materials = materials.data();
+    desc.material_count = static_cast<int64_t>(materials.size());
+    desc.camera = camera;
+    desc.textures = textures.data();
+    desc.texture_count = static_cast<int64_t>(textures.size());
+    for (size_t i = 0; i < images.size(); ++i)
+    {
+        images[i].rgb = image_pixels[i].data();
+    }
+    desc.images = images.data();
+    desc.image_count = static_cast<int64_t>(images.size());
+    desc.perlins = perlins.data();
+    desc.perlin_count = static_cast<int64_t>(perlins.size());
+    desc.quads = quads.data();
+    desc.quad_count = static_cast<int64_t>(quads.size());
+    media_desc.clear();
+    for (medium_store& m : media)
+    {
+        m.desc.quads = m.quads.data();
+        m.desc.quad_count = static_cast<int64_t>(m.quads.size());
+        media_desc.push_back(m.desc);
+    }
+    desc.media = media_desc.data();
+    desc.medium_count = static_cast<int64_t>(media_desc.size());
+    desc.lights = lights.data();
+    desc.light_count = static_cast<int64_t>(lights.size());
+    desc.combination = combination;
+    desc.quality = quality;
+    desc.microfacets = microfacets.data();
+    desc.microfacet_count = static_cast<int64_t>(microfacets.size());
+    if (has_environment)
+    {
+        environment.image.rgb = environment_pixels.data();
+        desc.environment = &environment;
+    }
+    mesh_desc.clear();
+    for (const mesh_store& m : meshes)
+    {
+        rt_mesh_desc d{};
+        d.positions = m.positions.data();
+        d.vertex_count = static_cast<int64_t>(m.positions.size() / 3);
+        d.indices = m.indices.data();
+        d.triangle_count = static_cast<int64_t>(m.indices.size() / 3);
+        d.material = m.material;
+        mesh_desc.push_back(d);
+    }
+    desc.meshes = mesh_desc.data();
+    desc.mesh_count = static_cast<int64_t>(mesh_desc.size());
+    return desc;
+}
+
+std::unique_ptr<scene_store> scene_store::copy_of(const rt_scene_desc& d)
+{
+    auto s = std::make_unique<scene_store>();
+    s->spheres.assign(d.spheres, d.spheres + d.sphere_count);
+    s->materials.assign(d.materials, d.materials + d.material_count);
+    s->camera = d.camera;
+    s->textures.assign(d.textures, d.textures + d.texture_count);
+    for (int64_t i = 0; i < d.image_count; ++i)
+    {
+        const rt_image_desc& im = d.images[i];
+        s->images.push_back(im);
+        s->image_pixels.emplace_back(im.rgb, im.rgb + static_cast<size_t>(im.width) * im.height * 3);
+    }
+    s->perlins.assign(d.perlins, d.perlins + d.perlin_count);
+    s->quads.assign(d.quads, d.quads + d.quad_count);
+    for (int64_t i = 0; i < d.medium_count; ++i)
+    {
+        medium_store m;
+        m.desc = d.media[i];
+        m.quads.assign(d.media[i].quads, d.media[i].quads + d.media[i].quad_count);
+        s->media.push_back(std::move(m));
+    }
+    s->lights.assign(d.lights, d.lights + d.light_count);
+    s->combination = d.combination;
+    s->quality = d.quality;
+    s->microfacets.assign(d.microfacets, d.microfacets + d.microfacet_count);
+    if (d.environment)
+    {
+        s->has_environment = true;
+        s->environment = *d.environment;
+        const rt_image_desc& im = d.environment->image;
+        s->environment_pixels.assign(im.rgb, im.rgb + static_cast<size_t>(im.width) * im.height * 3);
+    }
+    for (int64_t i = 0; i < d.mesh_count; ++i)
+    {
+        mesh_store m;
+        m.positions.assign(d.meshes[i].positions, d.meshes[i].positions + d.meshes[i].vertex_count * 3);
+        m.indices.assign(d.meshes[i].indices, d.meshes[i].indices + d.meshes[i].triangle_count * 3);
+        m.material = d.meshes[i].material;
+        s->meshes.push_back(std::move(m));
+    }
+    s->finish();
+    return s;
+}
+
+// camera.ixx:138-182: the viewport on the focus plane, the pixel grid and the lens disk
+rt_camera_desc camera_frame(const camera_settings& s, int height_override)
+{
+    rt_camera_desc c{};
+    c.image_width = s.image_width;
+    c.image_height =
+        height_override > 0 ? height_override : std::max(1, static_cast<int>(s.image_width / s.aspect_ratio));
+    c.sqrt_spp = std::max(1, static_cast<int>(std::lround(std::sqrt(s.samples_per_pixel))));
+    c.max_depth = s.max_depth;
+    c.center = s.lookfrom;
+    const double h = std::tan(degrees_to_radians(s.vfov) / 2);
+    const double viewport_height = 2 * h * s.focus_dist;
+    const double viewport_width = viewport_height * (static_cast<double>(c.image_width) / c.image_height);
+    const rt_vec3 w = unit_vector(sub(s.lookfrom, s.lookat));
+    const rt_vec3 u = unit_vector(cross(s.vup, w));
+    const rt_vec3 v = cross(w, u);
+    const rt_vec3 viewport_u = mul(viewport_width, u);
+    const rt_vec3 viewport_v = mul(viewport_height, mul(-1, v));
+    c.pixel_delta_u = divide(viewport_u, c.image_width);
+    c.pixel_delta_v = divide(viewport_v, c.image_height);
+    const rt_vec3 upper_left =
+        sub(sub(sub(c.center, mul(s.focus_dist, w)), divide(viewport_u, 2)), divide(viewport_v, 2));
+    c.pixel00_loc = add(upper_left, mul(0.5, add(c.pixel_delta_u, c.pixel_delta_v)));
+    const double defocus_radius = s.focus_dist * std::tan(degrees_to_radians(s.defocus_angle / 2));
+    c.defocus = s.defocus_angle > 0 ? 1 : 0;
+    c.defocus_disk_u = mul(defocus_radius, u);
+    c.defocus_disk_v = mul(defocus_radius, v);
+    c.sky_bottom = s.sky_bottom;
+    c.sky_top = s.sky_top;
+    c.sampling = s.sampling;
+    return c;
+}
+
+rt_status build_builtin(const std::string& name, const rt_builtin_params& p, std::unique_ptr<scene_store>& out,
+                        std::string& error)
+{
+    auto s = std::make_unique<scene_store>();
+    scene_random rng(p.scene_seed);
+    if (name == "weekend")
+    {
+        cover_world(*s, rng, 11);
+        set_camera(*s, cover_camera(), p, false);
+    }
+    else if (name.rfind("cover-", 0) == 0 || name == "cover")
+    {
+        // A cover variant of about N random spheres (a square grid of side round(sqrt(N)) centered like the book's
+        // 22 x 22), the camera pulled back in proportion to the grid
+        int n = p.sphere_count > 0 ? p.sphere_count : 484;
+        if (name.size() > 6)
+        {
+            n = std::atoi(name.c_str() + 6);
+        }
+        if (n < 1 || n > 4000000)
+        {
+            error = "cover-N: N must be in [1, 4000000]";
+            return RT_ERR_INVALID;
+        }
+        const int side = std::max(2, static_cast<int>(std::lround(std::sqrt(static_cast<double>(n)))));
+        const int half = (side + 1) / 2;
+        cover_world(*s, rng, half);
+        camera_settings c = cover_camera();
+        const double scale = std::max(1.0, half / 11.0);
+        c.lookfrom = mul(scale, c.lookfrom);
+        c.focus_dist = 10.0 * scale;
+        set_camera(*s, c, p, false);
+    }
+    else if (name == "materials")
+    {
+        // scenes.ixx:149-171
+        const int ground = s->lambertian(v3(0.8, 0.8, 0.0));
+        const int center = s->lambertian(v3(0.1, 0.2, 0.5));
+        const int left = s->dielectric(1.50);
+        const int bubble = s->dielectric(1.00 / 1.50);
+        const int right = s->metal(v3(0.8, 0.6, 0.2), 1.0);
+        s->spheres.push_back(make_sphere(v3(0.0, -100.5, -1.0), 100.0, ground));
+        s->spheres.push_back(make_sphere(v3(0.0, 0.0, -1.2), 0.5, center));
+        s->spheres.push_back(make_sphere(v3(-1.0, 0.0, -1.0), 0.5, left));
+        s->spheres.push_back(make_sphere(v3(-1.0, 0.0, -1.0), 0.4, bubble));
+        s->spheres.push_back(make_sphere(v3(1.0, 0.0, -1.0), 0.5, right));
+        camera_settings c = cover_camera();
+        c.lookfrom = v3(-2, 2, 1);
+        c.lookat = v3(0, 0, -1);
+        c.defocus_angle = 10.0;
+        c.focus_dist = 3.4;
+        set_camera(*s, c, p, false);
+    }
+    else if (name == "quads")
+    {
+        // scenes.ixx:224-249
+        const int left_red = s->lambertian(v3(1.0, 0.2, 0.2));
+        const int back_green = s->lambertian(v3(0.2, 1.0, 0.2));
+        const int right_blue = s->lambertian(v3(0.2, 0.2, 1.0));
+        const int upper_orange = s->lambertian(v3(1.0, 0.5, 0.0));
+        const int lower_teal = s->lambertian(v3(0.2, 0.8, 0.8));
+        s->quads.push_back(make_quad(v3(-3, -2, 5), v3(0, 0, -4), v3(0, 4, 0), left_red));
+        s->quads.push_back(make_quad(v3(-2, -2, 0), v3(4, 0, 0), v3(0, 4, 0), back_green));
+        s->quads.push_back(make_quad(v3(3, -2, 1), v3(0, 0, 4), v3(0, 4, 0), right_blue));
+        s->quads.push_back(make_quad(v3(-2, 3, 1), v3(4, 0, 0), v3(0, 0, 4), upper_orange));
+        s->quads.push_back(make_quad(v3(-2, -3, 5), v3(4, 0, 0), v3(0, 0, -4), lower_teal));
+        camera_settings c;
+        c.aspect_ratio = 1.0;
+        c.image_width = 1080;
+        c.samples_per_pixel = 500;
+        c.max_depth = 50;
+        c.vfov = 80;
+        c.lookfrom = v3(0, 0, 9);
+        c.lookat = v3(0, 0, 0);
+        c.sky_bottom = daylight_bottom;
+        c.sky_top = daylight_top;
+        set_camera(*s, c, p, false);
+    }
+    else if (name == "cornell")
+    {
+        // scenes.ixx:360-374: two white blocks, the lamp in the lights list
+        cornell_walls(*s);
+        s->quads.push_back(cornell_lamp(s->diffuse_light(v3(15, 15, 15))));
+        const int white = s->lambertian(v3(0.73, 0.73, 0.73));
+        tall_block(*s, white);
+        short_block(*s, white);
+        s->lights.push_back(quad_light(cornell_lamp(0), 1.0));
+        set_camera(*s, cornell_camera(), p, true);
+    }
+    else if (name == "glass" || name == "cornell-mis")
+    {
+        // scenes.ixx:484-501: the Cornell box with a glass ball instead of the short block; the lights list holds
+        // the lamp and the ball (weights 1/2 each, hittable_list::random)
+        cornell_walls(*s);
+        s->quads.push_back(cornell_lamp(s->diffuse_light(v3(15, 15, 15))));
+        tall_block(*s, s->lambertian(v3(0.73, 0.73, 0.73)));
+        s->spheres.push_back(make_sphere(v3(190, 90, 190), 90, s->dielectric(1.5)));
+        s->lights.push_back(quad_light(cornell_lamp(0), 0.5));
+        s->lights.push_back(sphere_light(v3(190, 90, 190), 90, 0.5));
+        rt_builtin_params q = p;
+        if (name == "cornell-mis")
+        {
+            // The quality integrator's -p mis: light samples at every vertex, power-heuristic MIS; its light set is
+            // the lamps (lamps.cuh:1-8: the ball doesn't glow), and its strategy is the material's
+            s->quality = 1;
+            s->combination = RT_COMBINE_POWER_HEURISTIC;
+            q.sampling = RT_SAMPLING_MATERIAL;
+        }
+        set_camera(*s, cornell_camera(), q, true);
+    }
+    else if (name == "furnace")
+    {
+        // gpu_scenes.ixx:33-55: a white sphere under a white sky, every pixel exactly 1 under -p material
+        s->spheres.push_back(make_sphere(v3(0, 0, 0), 1.0, s->lambertian(v3(1, 1, 1))));
+        camera_settings c;
+        c.aspect_ratio = 16.0 / 9.0;
+        c.image_width = 480;
+        c.samples_per_pixel = 64;
+        c.max_depth = 10;
+        c.sampling = RT_SAMPLING_MATERIAL;
+        c.vfov = 30;
+        c.lookfrom = v3(0, 0, 6);
+        c.lookat = v3(0, 0, 0);
+        c.sky_bottom = v3(1, 1, 1);
+        c.sky_top = v3(1, 1, 1);
+        set_camera(*s, c, p, false);
+    }
+    else
+    {
+        error = "unknown built-in scene '" + name + "'";
+        return RT_ERR_INVALID;
+    }
+    if (p.combination >= 0)
+    {
+        // A combination asks for the NEE/MIS integrator (the reference's quality kernel, -p material/nee/mis), which
+        // samples bounces as the material scatters
+        s->combination = p.combination;
+        s->quality = 1;
+        s->camera.sampling = RT_SAMPLING_MATERIAL;
+    }
+    s->finish();
+    out = std::move(s);
+    return RT_OK;
+}
+
+// ---- serialization: a little-endian binary file of the tables ---------------------------------------------------
+
+namespace
+{
+constexpr char magic[8] = {'R', 'T', 'B', '2', 'S', 'C', 'N', '1'};
+
+struct writer
+{
+    FILE* f;
+    bool ok = true;
+    void bytes(const void* p, size_t n)
+    {
+        if (n > 0 && std::fwrite(p, 1, n, f) != n)
+        {
+            ok = false;
+        }
+    }
+    template <class T>
+    void value(const T& v) { bytes(&v, sizeof(T)); }
+    template <class T>
+    void array(const T* p, int64_t n)
+    {
+        value(n);
+        bytes(p, sizeof(T) * static_cast<size_t>(n));
+    }
+};
+
+struct reader
+{
+    FILE* f;
+    bool ok = true;
+    void bytes(void* p, size_t n)
+    {
+        if (n > 0 && std::fread(p, 1, n, f) != n)
+        {
+            ok = false;
+        }
+    }
+    template <class T>
+    void value(T& v) { bytes(&v, sizeof(T)); }
+    template <class T>
+    void array(std::vector<T>& out)
+    {
+        int64_t n = 0;
+        value(n);
+        if (!ok || n < 0 || n > (int64_t{1} << 34))
+        {
+            ok = false;
+            return;
+        }
+        out.resize(static_cast<size_t>(n));
+        bytes(out.data(), sizeof(T) * static_cast<size_t>(n));
+    }
+};
+} // namespace
+
+rt_status save_scene(const rt_scene_desc& d, const std::string& path, std::string& error)
+{
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f)
+    {
+        error = "cannot open '" + path + "' for writing";
+        return RT_ERR_RUNTIME;
+    }
+    writer w{f};
+    w.bytes(magic, sizeof(magic));
+    w.array(d.spheres, d.sphere_count);
+    w.array(d.materials, d.material_count);
+    w.value(d.camera);
+    w.array(d.textures, d.texture_count);
+    w.value(d.image_count);
+    for (int64_t i = 0; i < d.image_count; ++i)
+    {
+        w.value(d.images[i].width);
+        w.value(d.images[i].height);
+        w.array(d.images[i].rgb, int64_t{d.images[i].width} * d.images[i].height * 3);
+    }
+    w.array(d.perlins, d.perlin_count);
+    w.array(d.quads, d.quad_count);
+    w.value(d.medium_count);
+    for (int64_t i = 0; i < d.medium_count; ++i)
+    {
+        w.value(d.media[i]);
+        w.array(d.media[i].quads, d.media[i].quad_count);
+    }
+    w.array(d.lights, d.light_count);
+    w.value(d.combination);
+    w.value(d.quality);
+    w.array(d.microfacets, d.microfacet_count);
+    const int32_t has_env = d.environment ? 1 : 0;
+    w.value(has_env);
+    if (d.environment)
+    {
+        w.value(d.environment->yaw_degrees);
+        w.value(d.environment->scale);
+        w.value(d.environment->image.width);
+        w.value(d.environment->image.height);
+        w.array(d.environment->image.rgb,
+                int64_t{d.environment->image.width} * d.environment->image.height * 3);
+    }
+    w.value(d.mesh_count);
+    for (int64_t i = 0; i < d.mesh_count; ++i)
+    {
+        w.value(d.meshes[i].material);
+        w.array(d.meshes[i].positions, d.meshes[i].vertex_count * 3);
+        w.array(d.meshes[i].indices, d.meshes[i].triangle_count * 3);
+    }
+    const bool ok = w.ok && std::fclose(f) == 0;
+    if (!ok)
+    {
+        error = "writing '" + path + "' failed";
+        return RT_ERR_RUNTIME;
+    }
+    return RT_OK;
+}
+
+rt_status load_scene(const std::string& path, std::unique_ptr<scene_store>& out, std::string& error)
+{
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f)
+    {
+        error = "cannot open '" + path + "'";
+        return RT_ERR_RUNTIME;
+    }
+    auto s = std::make_unique<scene_store>();
+    reader r{f};
+    char head[8] = {};
+    r.bytes(head, sizeof(head));
+    if (!r.ok || std::memcmp(head, magic, sizeof(magic)) != 0)
+    {
+        std::fclose(f);
+        error = "'" + path + "' is not a scene file";
+        return RT_ERR_RUNTIME;
+    }
+    r.array(s->spheres);
+    r.array(s->materials);
+    r.value(s->camera);
+    r.array(s->textures);
+    int64_t images = 0;
+    r.value(images);
+    for (int64_t i = 0; r.ok && i < images && i < 65536; ++i)
+    {
+        rt_image_desc im{};
+        r.value(im.width);
+        r.value(im.height);
+        s->image_pixels.emplace_back();
+        r.array(s->image_pixels.back());
+        s->images.push_back(im);
+    }
+    r.array(s->perlins);
+    r.array(s->quads);
+    int64_t media = 0;
+    r.value(media);
+    for (int64_t i = 0; r.ok && i < media && i < 65536; ++i)
+    {
+        medium_store m;
+        r.value(m.desc);
+        r.array(m.quads);
+        s->media.push_back(std::move(m));
+    }
+    r.array(s->lights);
+    r.value(s->combination);
+    r.value(s->quality);
+    r.array(s->microfacets);
+    int32_t has_env = 0;
+    r.value(has_env);
+    if (r.ok && has_env)
+    {
+        s->has_environment = true;
+        r.value(s->environment.yaw_degrees);
+        r.value(s->environment.scale);
+        r.value(s->environment.image.width);
+        r.value(s->environment.image.height);
+        r.array(s->environment_pixels);
+    }
+    int64_t meshes = 0;
+    r.value(meshes);
+    for (int64_t i = 0; r.ok && i < meshes && i < 65536; ++i)
+    {
+        mesh_store m;
+        r.value(m.material);
+        r.array(m.positions);
+        r.array(m.indices);
+        s->meshes.push_back(std::move(m));
+    }
+    std::fclose(f);
+    if (!r.ok)
+    {
+        error = "'" + path + "' is truncated or damaged";
+        return RT_ERR_RUNTIME;
+    }
+    s->finish();
+    out = std::move(s);
+    return RT_OK;
+}
+} // namespace rtb

@@ -1,0 +1,287 @@
+// A session: one view of a resident scene, its image's sums kept on the device and grown by launches of the
+// persistent kernel (renderer.h:591-673; the launch loop of renderer.cu:1315-1334, 1924-1971).
+//
+// Launch planning. The reference plans ~50 ms launches from measured row times and renders a pass in bands of rows
+// when one pass is too long for a launch (renderer.cu:179-308), because Windows stops long kernels. Here a launch is
+// a range of whole passes for every pixel, cut into (pixel, chunk) work items that the persistent threads pull, so a
+// launch's length is set by its number of passes alone: the first launch is one chunk (a probe of the speed), and
+// each later one as many chunks as fit launch_seconds at the last measured speed. A launch may span rounds of
+// strata: every sample finds its round, and so its seed, from its own absolute pass.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "host.h"
+
+namespace rtb
+{
+namespace
+{
+constexpr double max_launch_seconds = 0.5;              // renderer.h:413
+constexpr size_t partial_budget_bytes = size_t{1} << 30; // a launch's chunk partials: at most 1 GiB
+} // namespace
+
+session::session(std::shared_ptr<resident_scene> scene, const rt_session_options& options)
+    : scene_(std::move(scene)), options_(options)
+{
+    if (options_.arithmetic != RT_FLOAT32)
+    {
+        fail(RT_ERR_INVALID, "this integrator computes in float32, with FP64 only for large spheres and the sums");
+    }
+    if (!(options_.launch_seconds > 0 && options_.launch_seconds <= max_launch_seconds))
+    {
+        fail(RT_ERR_INVALID, "launch_seconds must be in (0, 0.5]");
+    }
+    check(cudaSetDevice(scene_->device()), "selecting the scene's device");
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a CUDA stream");
+    check(cudaEventCreate(&start_), "creating a CUDA event");
+    check(cudaEventCreate(&stop_), "creating a CUDA event");
+    kernel_attributes a{};
+    check(render_attributes(scene_->quality(), a), "querying the render kernel");
+    grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
+    counters_.allocate(7);
+    set_camera(scene_->camera());
+}
+
+session::~session()
+{
+    partials_.release();
+    sums_.release();
+    counters_.release();
+    if (start_)
+    {
+        cudaEventDestroy(start_);
+    }
+    if (stop_)
+    {
+        cudaEventDestroy(stop_);
+    }
+    if (stream_)
+    {
+        cudaStreamDestroy(stream_);
+    }
+}
+
+void session::set_camera(const rt_camera_desc& camera)
+{
+    if (camera.sampling != scene_->camera().sampling)
+    {
+        fail(RT_ERR_INVALID, "a new view must keep the scene's sampling strategy");
+    }
+    rt_scene_desc probe{};
+    probe.camera = camera;
+    probe.light_count = camera.sampling == RT_SAMPLING_LIGHTS || camera.sampling == RT_SAMPLING_MIXTURE ? 1 : 0;
+    rt_light_desc dummy{};
+    dummy.kind = RT_LIGHT_QUAD;
+    probe.lights = &dummy;
+    validate(probe);
+    camera_ = camera;
+    cam_ = to_camera(camera);
+    tiles_x_ = (camera.image_width + 7) / 8;
+    const int tiles_y = (camera.image_height + 3) / 4;
+    padded_pixels_ = tiles_x_ * tiles_y * 32;
+    max_partial_entries_ = static_cast<int64_t>(partial_budget_bytes / (3 * sizeof(double)));
+    const size_t pixels = static_cast<size_t>(camera.image_width) * static_cast<size_t>(camera.image_height);
+    sums_.allocate(pixels * 3);
+    check(cudaMemsetAsync(sums_.data(), 0, sums_.bytes(), stream_), "clearing the sums");
+    check(cudaMemsetAsync(counters_.data(), 0, counters_.bytes(), stream_), "clearing the counters");
+    check(cudaStreamSynchronize(stream_), "clearing the sums");
+    passes_ = 0;
+    kernel_seconds_ = 0;
+    samples_per_second_ = 0;
+}
+
+int64_t session::plan(int64_t target, double budget_seconds) const
+{
+    const int64_t next_chunk = (passes_ / pass_chunk + 1) * pass_chunk;
+    int64_t end;
+    if (samples_per_second_ <= 0)
+    {
+        end = next_chunk; // the probe: one chunk
+    }
+    else
+    {
+        const double pixels = static_cast<double>(camera_.image_width) * camera_.image_height;
+        const double passes = std::floor(budget_seconds * samples_per_second_ / pixels);
+        end = passes_ + std::max<int64_t>(1, static_cast<int64_t>(std::min(passes, 1e12)));
+        if (end > next_chunk)
+        {
+            end = end / pass_chunk * pass_chunk; // whole chunks
+        }
+    }
+    // At most what the partials buffer holds
+    const int64_t max_chunks = std::max<int64_t>(1, max_partial_entries_ / padded_pixels_);
+    end = std::min(end, (passes_ / pass_chunk + max_chunks) * pass_chunk);
+    return std::min(end, target);
+}
+
+double session::launch(int64_t end)
+{
+    const int64_t first_chunk = passes_ / pass_chunk;
+    const int64_t chunks = (end + pass_chunk - 1) / pass_chunk - first_chunk;
+    const size_t needed = static_cast<size_t>(chunks) * static_cast<size_t>(padded_pixels_) * 3;
+    if (partials_.size() < needed)
+    {
+        partials_.allocate(needed);
+    }
+    launch_params p{};
+    p.scene = scene_->view();
+    p.cam = cam_;
+    p.seed = options_.seed;
+    p.pass_begin = passes_;
+    p.pass_end = end;
+    p.first_chunk = first_chunk;
+    p.chunk = pass_chunk;
+    p.chunks = static_cast<int32_t>(chunks);
+    p.tiles_x = tiles_x_;
+    p.padded_pixels = padded_pixels_;
+    p.total_items = chunks * padded_pixels_;
+    p.round_passes = camera_.sqrt_spp * camera_.sqrt_spp;
+    p.job = 0;
+    p.work_counter = counters_.data();
+    p.partials = partials_.data();
+    p.counters = counters_.data() + 1;
+
+    reduce_params r{};
+    r.partials = partials_.data();
+    r.sums = sums_.data();
+    r.width = camera_.image_width;
+    r.height = camera_.image_height;
+    r.tiles_x = tiles_x_;
+    r.padded_pixels = padded_pixels_;
+    r.chunks = p.chunks;
+
+    check(cudaMemsetAsync(counters_.data(), 0, sizeof(unsigned long long), stream_), "resetting the work counter");
+    check(cudaEventRecord(start_, stream_), "recording a CUDA event");
+    check(launch_render(p, scene_->quality(), counting_, grid_, stream_), "launching the render kernel");
+    check(launch_reduce(r, stream_), "launching the reduction");
+    check(cudaEventRecord(stop_, stream_), "recording a CUDA event");
+    check(cudaEventSynchronize(stop_), "rendering on the GPU");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, start_, stop_), "timing the GPU");
+    const double seconds = std::max(1e-6, ms / 1000.0);
+    const double samples = static_cast<double>(camera_.image_width) * camera_.image_height * static_cast<double>(end - passes_);
+    samples_per_second_ = samples / seconds;
+    passes_ = end;
+    kernel_seconds_ += seconds;
+    return seconds;
+}
+
+rt_render_report session::render_to(int64_t target)
+{
+    if (target < passes_)
+    {
+        fail(RT_ERR_INVALID, "the target is behind the image");
+    }
+    rt_render_report report{};
+    if (camera_.max_depth == 0)
+    {
+        passes_ = target; // a path of no rays: every sample is 0, and no launch is needed
+    }
+    while (passes_ < target)
+    {
+        const double t = launch(plan(target, options_.launch_seconds));
+        ++report.launches;
+        report.gpu_seconds += t;
+        report.longest_launch_seconds = std::max(report.longest_launch_seconds, t);
+    }
+    report.state = state();
+    return report;
+}
+
+rt_render_report session::render_for(double seconds, int64_t pass_limit)
+{
+    if (!(seconds >= 0 && seconds <= 3600))
+    {
+        fail(RT_ERR_INVALID, "seconds must be in [0, 3600]");
+    }
+    if (pass_limit < 0)
+    {
+        fail(RT_ERR_INVALID, "pass_limit must not be negative");
+    }
+    rt_render_report report{};
+    if (camera_.max_depth == 0)
+    {
+        passes_ = std::max(passes_, std::min<int64_t>(pass_limit, passes_ + 1));
+    }
+    while (passes_ < pass_limit)
+    {
+        const double left = seconds - report.gpu_seconds;
+        if (passes_ > 0 && report.launches > 0 && left < 0.25 * std::min(seconds, options_.launch_seconds))
+        {
+            break;
+        }
+        const double budget = std::max(1e-4, std::min(options_.launch_seconds, left));
+        const double t = launch(plan(pass_limit, budget));
+        ++report.launches;
+        report.gpu_seconds += t;
+        report.longest_launch_seconds = std::max(report.longest_launch_seconds, t);
+        if (report.gpu_seconds >= seconds && passes_ > 0)
+        {
+            break;
+        }
+    }
+    report.state = state();
+    return report;
+}
+
+void session::pixels(double* out, int64_t count) const
+{
+    const int64_t n = static_cast<int64_t>(camera_.image_width) * camera_.image_height * 3;
+    if (count != n)
+    {
+        fail(RT_ERR_INVALID, "pixels: the buffer must hold width * height * 3 doubles");
+    }
+    if (passes_ == 0)
+    {
+        fail(RT_ERR_LOGIC, "pixels: the image has no complete pass");
+    }
+    check(cudaMemcpyAsync(out, sums_.data(), static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+          "copying the image");
+    check(cudaStreamSynchronize(stream_), "copying the image");
+    const double scale = 1.0 / static_cast<double>(passes_);
+    for (int64_t i = 0; i < n; ++i)
+    {
+        out[i] *= scale;
+    }
+}
+
+uint64_t session::rays() const
+{
+    unsigned long long v = 0;
+    check(cudaMemcpy(&v, counters_.data() + 1, sizeof(v), cudaMemcpyDeviceToHost), "reading the ray count");
+    return v;
+}
+
+void session::fetch_counts(uint64_t out[4]) const
+{
+    unsigned long long v[4] = {};
+    check(cudaMemcpy(v, counters_.data() + 3, sizeof(v), cudaMemcpyDeviceToHost), "reading the fetch counts");
+    for (int i = 0; i < 4; ++i)
+    {
+        out[i] = v[i];
+    }
+}
+
+uint64_t session::shadow_rays() const
+{
+    unsigned long long v = 0;
+    check(cudaMemcpy(&v, counters_.data() + 2, sizeof(v), cudaMemcpyDeviceToHost), "reading the ray count");
+    return v;
+}
+
+rt_kernel_info session::kernel() const
+{
+    kernel_attributes a{};
+    check(render_attributes(scene_->quality(), a), "querying the render kernel");
+    rt_kernel_info info{};
+    std::snprintf(info.name, sizeof(info.name), "%s", scene_->quality() ? "persistent nee-mis" : "persistent books");
+    info.registers = a.registers;
+    info.local_bytes = a.local_bytes;
+    info.blocks_per_multiprocessor = a.blocks_per_sm;
+    info.threads_per_block = a.threads_per_block;
+    info.max_threads_per_multiprocessor = a.max_threads_per_sm;
+    info.multiprocessors = a.multiprocessors;
+    return info;
+}
+} // namespace rtb
