@@ -317,10 +317,100 @@ struct fetch_counts
     uint32_t triangles = 0;
 };
 
+// The leaf's primitives against the ray, shrinking hit.t; true at the first hit for a shadow ray
+template <bool SHADOW, bool COUNT>
+__device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 o, float3 d, float inverse_a, int from,
+                                          bool inward, int skip, hit_info& hit, fetch_counts* counts)
+{
+    const int kind = leaf_kind(link);
+    const int count = leaf_count(link);
+    const int start = leaf_start(link);
+    if (COUNT)
+    {
+        (kind == kind_sphere ? counts->spheres : kind == kind_quad ? counts->quads : counts->triangles) += count;
+    }
+    if (kind == kind_sphere)
+    {
+        for (int i = start; i < start + count; ++i)
+        {
+            const int id = i; // spheres' global ids are their indices
+            const bool own = id == from;
+            if ((own && !inward) || id == skip)
+            {
+                continue;
+            }
+            const float4 s = __ldg(reinterpret_cast<const float4*>(S.spheres + i));
+            float t;
+            bool entering;
+            if (hit_sphere(s, o, d, inverse_a, t_min, hit.t, own, t, entering))
+            {
+                if (SHADOW)
+                {
+                    return true;
+                }
+                hit = {id, t, entering};
+            }
+        }
+    }
+    else if (kind == kind_quad)
+    {
+        for (int i = start; i < start + count; ++i)
+        {
+            const int id = S.quad_base + i;
+            if (id == from || id == skip)
+            {
+                continue;
+            }
+            const quad_v q = load_quad(S.quads, i);
+            float t;
+            bool front;
+            if (hit_quad(q, o, d, t_min, hit.t, t, front))
+            {
+                if (SHADOW)
+                {
+                    return true;
+                }
+                hit = {id, t, front};
+            }
+        }
+    }
+    else
+    {
+        for (int i = start; i < start + count; ++i)
+        {
+            const int id = S.triangle_base + i;
+            if (id == from || id == skip)
+            {
+                continue;
+            }
+            const triangle_v tr = load_triangle(S.triangles, i);
+            float t;
+            bool front;
+            if (hit_triangle(tr, o, d, t_min, hit.t, t, front))
+            {
+                if (SHADOW)
+                {
+                    return true;
+                }
+                hit = {id, t, front};
+            }
+        }
+    }
+    return false;
+}
+
+// No more nodes to visit (a leaf link never takes this value: its kind field would be 3)
+constexpr int traversal_done = static_cast<int>(0x80000000u);
+
 // The closest hit in (t_min, t_max) (SHADOW = false; the CPU's world.hit, bvh.cuh:576-706), or whether anything lies
 // there (SHADOW = true; shadow.cuh:26-109 occluded, `skip` not tested). The self-intersection rules of the primitive
 // the ray leaves, `from`: a quad or a triangle is never hit again (a line meets a plane once); a sphere left outward
 // is never hit again, and left inward only at its far root (bvh.cuh:539-575).
+//
+// The loop is Aila and Laine's speculative while-while (HPG 2009): a lane descends through inner nodes, sets aside the
+// first leaf it meets and keeps descending, and the warp leaves the node loop together once every lane holds a leaf;
+// then the leaf loop tests them. Node steps and leaf tests so run with the warp's lanes side by side, where a single
+// loop would run a node step for some lanes and a leaf test for the others one after the other.
 template <bool SHADOW, bool COUNT = false>
 __device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d, float t_max, int from, bool inward,
                                          int skip, hit_info& hit, fetch_counts* counts = nullptr)
@@ -337,10 +427,23 @@ __device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d
     const float3 os = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
     int2 stack[max_bvh_depth];
     int sp = 0;
+    // The next stack entry the ray enters before the closest hit so far, or traversal_done
+    const auto pop = [&]() -> int {
+        while (sp > 0)
+        {
+            const int2 e = stack[--sp];
+            if (SHADOW || __int_as_float(e.y) < hit.t)
+            {
+                return e.x;
+            }
+        }
+        return traversal_done;
+    };
     int link = 0;
-    while (true)
+    int leaf = 0; // a leaf set aside (leaf links are negative; 0: none)
+    while (link != traversal_done)
     {
-        if (link >= 0)
+        while (link >= 0)
         {
             const float4* np = reinterpret_cast<const float4*>(S.nodes + link);
             const float4 nx = __ldg(np);
@@ -368,107 +471,38 @@ __device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d
                 const bool second_first = enter1 < enter0;
                 link = second_first ? nl.y : nl.x;
                 stack[sp++] = make_int2(second_first ? nl.x : nl.y, __float_as_int(second_first ? enter0 : enter1));
-                continue;
             }
-            if (h0 || h1)
+            else if (h0 || h1)
             {
                 link = h0 ? nl.x : nl.y;
-                continue;
-            }
-        }
-        else
-        {
-            const int kind = leaf_kind(link);
-            const int count = leaf_count(link);
-            const int start = leaf_start(link);
-            if (COUNT)
-            {
-                (kind == kind_sphere ? counts->spheres : kind == kind_quad ? counts->quads : counts->triangles) +=
-                    count;
-            }
-            if (kind == kind_sphere)
-            {
-                for (int i = start; i < start + count; ++i)
-                {
-                    const int id = i; // spheres' global ids are their indices
-                    const bool own = id == from;
-                    if ((own && !inward) || id == skip)
-                    {
-                        continue;
-                    }
-                    const float4 s = __ldg(reinterpret_cast<const float4*>(S.spheres + i));
-                    float t;
-                    bool entering;
-                    if (hit_sphere(s, o, d, inverse_a, t_min, hit.t, own, t, entering))
-                    {
-                        if (SHADOW)
-                        {
-                            return true;
-                        }
-                        hit = {id, t, entering};
-                    }
-                }
-            }
-            else if (kind == kind_quad)
-            {
-                for (int i = start; i < start + count; ++i)
-                {
-                    const int id = S.quad_base + i;
-                    if (id == from || id == skip)
-                    {
-                        continue;
-                    }
-                    const quad_v q = load_quad(S.quads, i);
-                    float t;
-                    bool front;
-                    if (hit_quad(q, o, d, t_min, hit.t, t, front))
-                    {
-                        if (SHADOW)
-                        {
-                            return true;
-                        }
-                        hit = {id, t, front};
-                    }
-                }
             }
             else
             {
-                for (int i = start; i < start + count; ++i)
-                {
-                    const int id = S.triangle_base + i;
-                    if (id == from || id == skip)
-                    {
-                        continue;
-                    }
-                    const triangle_v tr = load_triangle(S.triangles, i);
-                    float t;
-                    bool front;
-                    if (hit_triangle(tr, o, d, t_min, hit.t, t, front))
-                    {
-                        if (SHADOW)
-                        {
-                            return true;
-                        }
-                        hit = {id, t, front};
-                    }
-                }
+                link = pop();
             }
-        }
-        // Nowhere to descend: the next entry of the stack that the ray enters before the closest hit so far
-        bool found = false;
-        while (sp > 0)
-        {
-            const int2 e = stack[--sp];
-            if (SHADOW || __int_as_float(e.y) < hit.t)
+            // A leaf: set it aside and go on descending, unless one is already waiting
+            if (link < 0 && link != traversal_done && leaf == 0)
             {
-                link = e.x;
-                found = true;
-                break;
+                leaf = link;
+                link = pop();
+            }
+            if (!__any_sync(__activemask(), leaf == 0))
+            {
+                break; // every lane of the warp holds a leaf: test them together
             }
         }
-        if (!found)
+        while (leaf < 0)
         {
-            break;
+            if (test_leaf<SHADOW, COUNT>(S, leaf, o, d, inverse_a, from, inward, skip, hit, counts))
+            {
+                return true;
+            }
+            leaf = 0;
+            if (link < 0 && link != traversal_done)
+            {
+                leaf = link;
+                link = pop();
+            }
         }
     }
     return hit.id >= 0;
@@ -974,8 +1008,14 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
 }
 
 // ---- the persistent render kernel ------------------------------------------------------------------------------
+// The render kernel's resident blocks per multiprocessor, which caps its registers at 64: 8 blocks of 128 threads
+// measured fastest on every workload against 5 (96 registers) and 6 (80), for the latency it hides
+#ifndef RTB_MIN_BLOCKS
+#define RTB_MIN_BLOCKS 8
+#endif
+
 template <bool QUALITY, bool COUNT>
-__global__ void __launch_bounds__(render_block) render_kernel(const __grid_constant__ launch_params P)
+__global__ void __launch_bounds__(render_block, RTB_MIN_BLOCKS) render_kernel(const __grid_constant__ launch_params P)
 {
     __shared__ unsigned long long block_rays;
     __shared__ unsigned long long block_shadow_rays;

@@ -61,6 +61,11 @@ quad12 make_quad(const rt_quad_desc& d)
     return q;
 }
 
+// The largest leaf of a scene of spheres and quads with more than 8 primitives (one leaf holds them all below)
+#ifndef RTB_LEAF_SIZE
+#define RTB_LEAF_SIZE 1
+#endif
+
 // A sphere whose quadratic is solved in FP64: radius large next to the spacing of floats at its center, where the
 // l-vector form's r^2 - |l|^2 is a difference of numbers near r^2 (the radius-1000 ground)
 constexpr double fp64_radius = 128;
@@ -376,7 +381,7 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     }
 
     bvh_options options;
-    options.max_leaf_size = prims.size() <= 8 ? 7 : (source_triangles.empty() ? 1 : 4);
+    options.max_leaf_size = prims.size() <= 8 ? 7 : (source_triangles.empty() ? RTB_LEAF_SIZE : 4);
     const bvh_result tree = build_bvh(std::move(prims), options);
 
     // Each kind's array in leaf order; global ids: spheres, then quads, then triangles

@@ -101,13 +101,12 @@ int64_t session::plan(int64_t target, double budget_seconds) const
     }
     else
     {
+        // As many whole chunks as fit the budget, at least one: a launch ends on a chunk boundary (or at the target),
+        // so every chunk's partial is summed from the same samples in the same order however the launches fall
         const double pixels = static_cast<double>(camera_.image_width) * camera_.image_height;
         const double passes = std::floor(budget_seconds * samples_per_second_ / pixels);
-        end = passes_ + std::max<int64_t>(1, static_cast<int64_t>(std::min(passes, 1e12)));
-        if (end > next_chunk)
-        {
-            end = end / pass_chunk * pass_chunk; // whole chunks
-        }
+        end = passes_ + static_cast<int64_t>(std::min(passes, 1e12));
+        end = std::max(next_chunk, end / pass_chunk * pass_chunk);
     }
     // At most what the partials buffer holds
     const int64_t max_chunks = std::max<int64_t>(1, max_partial_entries_ / padded_pixels_);

@@ -63,7 +63,9 @@ def test_first_hit_ids_match_oracle(rt, oracle, name, width):
         assert np.allclose(ts[both], ref_ts[both], rtol=2e-4, atol=1e-5)
         bad = ~same
         # a mismatch is a tie when both found a hit at the same distance (1e-6 relative, plus float rounding of t)
-        tie = bad & (ids >= 0) & (ref_ids >= 0) & (np.abs(ts - ref_ts) <= 1e-5 * np.maximum(ref_ts, 1e-3))
+        both_hit = (ids >= 0) & (ref_ids >= 0)
+        gap = np.where(both_hit, np.abs(np.where(both_hit, ts, 0) - np.where(both_hit, ref_ts, 0)), np.inf)
+        tie = bad & both_hit & (gap <= 1e-5 * np.maximum(ref_ts, 1e-3))
         mismatches += int(np.count_nonzero(bad & ~tie))
     assert mismatches / total <= 1e-4, (mismatches, total)
 
