@@ -322,6 +322,22 @@ rt_status rt_session_counters(const rt_session* session, uint64_t* rays, uint64_
                               double* kernel_seconds);
 rt_status rt_session_kernel(const rt_session* session, rt_kernel_info* info);
 
+/* Renders passes [pass_begin, pass_end) of `camera`'s view of a resident scene and ADDS the samples' sums into
+ * device_sums (width*height*3 doubles of device memory the caller owns, rows from the top; zero it to start an
+ * image), allocating no device memory at all. This entry point has no counterpart in the reference. It is for
+ * callers that cannot call cudaMalloc: a program that owns all of its device memory through its own pool (an engine
+ * or a server that reserves its HBM at start-up and hands out pre-sized buffers only), or a thread that must not
+ * block on the allocator, which can synchronize the device. The render kernel's scratch (work and ray counters, the
+ * per-chunk partial sums) comes from a fixed 64 MiB array in the library's device image instead: an image may have
+ * at most 2,796,192 pixels once padded to 8x4 tiles (about 1920x1440), larger ones return RT_ERR_CAPACITY. Every GPU
+ * that loads the library holds that array until the process exits. The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress) with that device current, so make that first call before any stream capture. Every
+ * call shares the array and leaves its contents behind; calls are synchronous, and two calls that overlap on the GPU
+ * (from two host threads) race. Passes are rendered in the same chunks as a session's, so the sums equal a
+ * session's render of the same seed and passes bit for bit. rays / shadow_rays (may be NULL): this call's counts. */
+rt_status rt_render_passes_no_alloc(rt_scene* scene, const rt_camera_desc* camera, uint64_t seed, int64_t pass_begin,
+                                    int64_t pass_end, double* device_sums, uint64_t* rays, uint64_t* shadow_rays);
+
 /* Device-resident variant for callers that keep the image on the GPU (a served frame, a display transform):
  * the device address of the per-pixel sums (3 doubles per pixel, rows from the top) and of the pass count. */
 rt_status rt_session_device_sums(const rt_session* session, const double** sums, int64_t* passes);

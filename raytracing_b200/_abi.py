@@ -174,6 +174,8 @@ ENTRY_POINTS = [
                                       C.POINTER(C.c_double)]),
     ("rt_session_kernel", C.c_int, [C.c_void_p, C.POINTER(KernelInfo)]),
     ("rt_session_device_sums", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
+    ("rt_render_passes_no_alloc", C.c_int, [C.c_void_p, C.POINTER(CameraDesc), C.c_uint64, C.c_int64, C.c_int64,
+                                            C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     ("rt_session_set_counting", C.c_int, [C.c_void_p, C.c_int32]),
     ("rt_session_fetch_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64 * 4)]),
     ("rt_scene_closest_hits", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64,

@@ -64,6 +64,8 @@ rt_session_options session_options_of(const rt_render_options& o)
 }
 } // namespace
 
+void rtb::remember_error(const char* message) { last_error = message; }
+
 extern "C" {
 
 const char* rt_last_error_message(void) { return last_error.c_str(); }

@@ -24,6 +24,8 @@ struct rt_error : std::runtime_error
 
 [[noreturn]] void fail(rt_status status, const std::string& message);
 void check(cudaError_t e, const char* what);
+// Keeps a message for rt_last_error_message() on this thread
+void remember_error(const char* message);
 
 // Device memory owned by one object, freed with it
 template <class T>
