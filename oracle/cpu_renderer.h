@@ -592,6 +592,9 @@ struct material
     color albedo;            // lambertian, diffuse_light, isotropic: the solid texture's color; metal: its albedo
     double fuzz = 0;
     double refraction_index = 1;
+    int lobe = RT_MICROFACET_NONE; // the quality integrator's GGX side entry (renderer.h:249-261)
+    double roughness = 0;
+    double alpha = 0;              // r^2, rounded to float as the GPU's
 };
 
 inline double reflectance(double cosine, double refraction_index) // material.ixx:101-107 (Schlick)
@@ -662,6 +665,12 @@ inline bool make_scene(const rt_scene_desc& d, scene& s, const char** error)
         mm.kind = m.kind;
         mm.fuzz = std::min(m.fuzz, 1.0);
         mm.refraction_index = m.refraction_index;
+        if (i < d.microfacet_count)
+        {
+            mm.lobe = d.microfacets[i].kind;
+            mm.roughness = d.microfacets[i].roughness;
+            mm.alpha = static_cast<float>(d.microfacets[i].roughness * d.microfacets[i].roughness);
+        }
         if (m.kind == RT_METAL)
         {
             mm.albedo = from(m.albedo);

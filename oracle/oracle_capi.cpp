@@ -66,7 +66,7 @@ int oracle_render(const rt_scene_desc* desc, uint64_t seed, int64_t passes, int3
     }
     row_begin = std::max(0, row_begin);
     const bool quality = desc->quality != 0;
-    const oracle::quality_scene q = oracle::make_quality(s, desc->combination);
+    const oracle::quality_scene q = oracle::make_quality(s, *desc);
     const unsigned thread_count = threads > 0 ? static_cast<unsigned>(threads)
                                               : std::max(1u, std::thread::hardware_concurrency());
     std::atomic<int> next_row{row_begin};
@@ -198,4 +198,12 @@ int oracle_thresholds(int32_t tested_tiles, double* whole_image, double* all_til
 }
 
 int32_t oracle_sizeof_compare_result(void) { return static_cast<int32_t>(sizeof(oracle::compare_result)); }
+
+// Turquin's energy table by the oracle's own quadrature: 32 x 32 doubles, [j * 32 + i] for r = j/31, sqrt(mu) = i/31
+int oracle_ggx_energy_table(double* out)
+{
+    const std::vector<double> t = oracle::ggx_energy_table();
+    std::copy(t.begin(), t.end(), out);
+    return 0;
+}
 }

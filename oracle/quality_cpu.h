@@ -8,6 +8,7 @@
 #pragma once
 
 #include "cpu_renderer.h"
+#include "ggx_env_cpu.h"
 
 namespace oracle
 {
@@ -145,6 +146,11 @@ struct quality_scene
     std::vector<int> lamp_of; // by source id, -1 for none
     int combination;
     double light_pmf;
+    bool has_environment = false;
+    environment env;
+    std::vector<double> energy; // Turquin's table, when a GGX conductor is in the scene
+
+    int light_count() const { return static_cast<int>(lamps.size()) + (has_environment && env.sampled() ? 1 : 0); }
 };
 
 // Anything in (0.001, t_max) along r, the lamp `skip` aside (shadow.cuh:26-109 occluded)? The CPU's BVH search with
@@ -154,6 +160,63 @@ inline bool occluded(const scene& s, const ray& r, double t_max, int skip)
     return s.geometry.hit_except(r, interval{0.001, t_max}, skip).has_value();
 }
 
+// The lobes of bsdf.cuh:30-99 on the CPU
+enum class lobe_kind
+{
+    lambertian,
+    isotropic,
+    conductor,
+    gloss,
+    smooth_conductor,
+    books_delta,
+};
+
+inline lobe_kind lobe_of(const material& m)
+{
+    if (m.lobe == RT_MICROFACET_CONDUCTOR)
+    {
+        return m.alpha >= min_ggx_alpha ? lobe_kind::conductor : lobe_kind::smooth_conductor;
+    }
+    if (m.lobe == RT_MICROFACET_GLOSS)
+    {
+        return lobe_kind::gloss;
+    }
+    if (m.kind == RT_LAMBERTIAN)
+    {
+        return lobe_kind::lambertian;
+    }
+    if (m.kind == RT_ISOTROPIC)
+    {
+        return lobe_kind::isotropic;
+    }
+    return lobe_kind::books_delta;
+}
+
+// eval_bsdf (bsdf.cuh:178-201): f * |cos| for a light sample's unit direction wi, and the lobe's density of it
+inline color eval_lobe(const quality_scene& q, lobe_kind k, const material& m, const vec3& n, const vec3& wo,
+                       const vec3& wi, double& pdf)
+{
+    switch (k)
+    {
+    case lobe_kind::lambertian:
+        pdf = cosine_density(n, wi);
+        return pdf * m.albedo;
+    case lobe_kind::isotropic:
+        pdf = uniform_sphere_density;
+        return uniform_sphere_density * m.albedo;
+    case lobe_kind::conductor:
+    {
+        const color single = ggx_eval(n, wo, wi, m.alpha, m.albedo, pdf);
+        return ggx_compensation(q.energy, m.albedo, dot(n, wo), m.roughness) * single;
+    }
+    case lobe_kind::gloss:
+        return gloss_eval(n, wo, wi, m.alpha, m.albedo, pdf);
+    default:
+        pdf = 0;
+        return {0, 0, 0};
+    }
+}
+
 // quality_path.cuh:83-188 trace_quality_ray, one whole sample
 inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
 {
@@ -161,15 +224,30 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
     color radiance{0, 0, 0};
     color throughput{1, 1, 1};
     double bsdf_pdf = 0;
+    bool specular = true;
     int rays_left = s.camera.max_depth;
+    const int lights = q.light_count();
     while (true)
     {
         const auto rec = s.geometry.hit(r, interval{0.001, infinity});
         ++n.rays;
         if (!rec)
         {
-            // the sky: no light sample could have drawn it (no environment map in the light set)
-            return radiance + throughput * s.sky(r.direction);
+            // background.cuh:44-61: the environment (filtered after the camera and delta vertices; the nearest texel
+            // and its density otherwise), or the camera's sky
+            if (!q.has_environment)
+            {
+                return radiance + throughput * s.sky(r.direction);
+            }
+            if (specular)
+            {
+                return radiance + throughput * q.env.radiance_filtered(r.direction);
+            }
+            double density;
+            const color le = q.env.radiance(r.direction, density);
+            const double p_light = q.env.sampled() ? q.light_pmf * density : 0.0;
+            const double w = bsdf_pdf > 0 ? bsdf_weight(q.combination, bsdf_pdf, p_light) : 1.0;
+            return radiance + w * (throughput * le);
         }
         const material& m = s.materials[static_cast<size_t>(rec->material)];
         if (m.kind == RT_DIFFUSE_LIGHT)
@@ -188,42 +266,57 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
             const color c = rec->front_face ? m.albedo : color{0, 0, 0};
             return radiance + w * (throughput * c);
         }
-        const bool delta = m.kind == RT_METAL || m.kind == RT_DIELECTRIC;
-        const bool nee = q.combination != RT_COMBINE_BSDF_ONLY && rays_left > 1 && !delta && !q.lamps.empty() &&
+        const lobe_kind lobe = lobe_of(m);
+        const bool delta = lobe == lobe_kind::books_delta || lobe == lobe_kind::smooth_conductor;
+        const vec3 wo = -unit_vector(r.direction);
+        const bool nee = q.combination != RT_COMBINE_BSDF_ONLY && rays_left > 1 && !delta && lights > 0 &&
                          largest_channel(throughput) > 0;
         bool lit = false;
         color contribution{0, 0, 0};
-        lamp_sample ls;
+        vec3 light_dir;
+        double light_distance = infinity;
         int skip = -1;
         if (nee)
         {
-            // light_sampler.cuh:40-75 sample_light, then quality_path.cuh:52-79 light_contribution
+            // light_sampler.cuh:40-75 sample_light: one number picks a light, the lamps first, the map last
             const double xi = g.next();
-            int k = static_cast<int>(xi * static_cast<double>(q.lamps.size()));
-            k = std::min(k, static_cast<int>(q.lamps.size()) - 1);
-            const lamp& e = q.lamps[static_cast<size_t>(k)];
-            if (sample_lamp(e, rec->p, g, ls))
+            int k = static_cast<int>(xi * lights);
+            k = std::min(k, lights - 1);
+            bool drawn = false;
+            color le;
+            double p_light = 0;
+            if (k < static_cast<int>(q.lamps.size()))
             {
-                const double p_light = q.light_pmf * ls.pdf;
+                const lamp& e = q.lamps[static_cast<size_t>(k)];
+                lamp_sample ls;
+                if (sample_lamp(e, rec->p, g, ls))
+                {
+                    drawn = true;
+                    light_dir = ls.wi;
+                    light_distance = ls.distance;
+                    le = e.radiance;
+                    p_light = q.light_pmf * ls.pdf;
+                    skip = e.primitive;
+                }
+            }
+            else
+            {
+                double density;
+                if (q.env.sample(g, light_dir, le, density))
+                {
+                    drawn = true;
+                    p_light = q.light_pmf * density;
+                }
+            }
+            if (drawn)
+            {
                 double p_bsdf;
-                color f;
-                if (m.kind == RT_LAMBERTIAN)
-                {
-                    p_bsdf = cosine_density(rec->normal, ls.wi);
-                    f = p_bsdf * m.albedo;
-                }
-                else // isotropic
-                {
-                    p_bsdf = uniform_sphere_density;
-                    f = uniform_sphere_density * m.albedo;
-                }
+                const color f = eval_lobe(q, lobe, m, rec->normal, wo, light_dir, p_bsdf);
                 if (p_light > 0 && largest_channel(f) > 0)
                 {
-                    contribution = (light_weight(q.combination, p_light, p_bsdf) / p_light) *
-                                   (throughput * (f * e.radiance));
+                    contribution = (light_weight(q.combination, p_light, p_bsdf) / p_light) * (throughput * (f * le));
                     const double sum = contribution.x + contribution.y + contribution.z;
                     lit = sum > 0 && sum < infinity;
-                    skip = e.primitive;
                 }
             }
         }
@@ -232,9 +325,9 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
         color weight{1, 1, 1};
         double pdf = 0;
         bool scattered = true;
-        switch (m.kind)
+        switch (lobe)
         {
-        case RT_LAMBERTIAN:
+        case lobe_kind::lambertian:
         {
             const onb uvw{rec->normal};
             wi = uvw.transform(random_cosine_direction(g));
@@ -243,34 +336,78 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
             pdf = cosine_density(rec->normal, wi);
             break;
         }
-        case RT_ISOTROPIC:
+        case lobe_kind::isotropic:
             wi = random_unit_vector(g);
             weight = m.albedo;
             pdf = uniform_sphere_density;
             break;
-        case RT_METAL:
+        case lobe_kind::conductor:
         {
-            wi = unit_vector(reflect(r.direction, rec->normal)) + m.fuzz * random_unit_vector(g);
-            scattered = dot(wi, rec->normal) > 0;
-            weight = m.albedo;
+            const double u1 = g.next();
+            const double u2 = g.next();
+            scattered = ggx_sample(rec->normal, wo, m.alpha, m.albedo, u1, u2, wi, weight, pdf);
+            if (scattered)
+            {
+                weight = weight * ggx_compensation(q.energy, m.albedo, dot(rec->normal, wo), m.roughness);
+            }
             break;
         }
-        default: // dielectric
+        case lobe_kind::smooth_conductor:
+            scattered = dot(rec->normal, wo) > 0;
+            wi = unit_vector(reflect(-wo, rec->normal));
+            weight = schlick(m.albedo, dot(rec->normal, wo));
+            break;
+        case lobe_kind::gloss:
         {
-            const double ri = rec->front_face ? (1.0 / m.refraction_index) : m.refraction_index;
-            const vec3 ud = unit_vector(r.direction);
-            const double cos_theta = std::fmin(dot(-ud, rec->normal), 1.0);
-            const double sin_theta = std::sqrt(1.0 - cos_theta * cos_theta);
-            wi = ri * sin_theta > 1.0 || reflectance(cos_theta, ri) > g.next() ? reflect(ud, rec->normal)
-                                                                                : refract(ud, rec->normal, ri);
+            // ggx.cuh:300-324: the coat or the base, half the time each, then the mixture's weight and density
+            if (g.next() < 0.5)
+            {
+                const double u1 = g.next();
+                const double u2 = g.next();
+                color coat_weight;
+                double coat_pdf;
+                scattered = ggx_sample(rec->normal, wo, m.alpha, color{gloss_coat_f0, gloss_coat_f0, gloss_coat_f0},
+                                       u1, u2, wi, coat_weight, coat_pdf);
+            }
+            else
+            {
+                const onb uvw{rec->normal};
+                wi = uvw.transform(random_cosine_direction(g));
+                scattered = dot(rec->normal, wi) > 0;
+            }
+            if (scattered)
+            {
+                const color f = gloss_eval(rec->normal, wo, wi, m.alpha, m.albedo, pdf);
+                scattered = pdf > 0;
+                if (scattered)
+                {
+                    weight = (1 / pdf) * f;
+                }
+            }
             break;
         }
+        default: // the books' metal and glass
+            if (m.kind == RT_METAL)
+            {
+                wi = unit_vector(reflect(r.direction, rec->normal)) + m.fuzz * random_unit_vector(g);
+                scattered = dot(wi, rec->normal) > 0;
+                weight = m.albedo;
+            }
+            else
+            {
+                const double ri = rec->front_face ? (1.0 / m.refraction_index) : m.refraction_index;
+                const vec3 ud = unit_vector(r.direction);
+                const double cos_theta = std::fmin(dot(-ud, rec->normal), 1.0);
+                const double sin_theta = std::sqrt(1.0 - cos_theta * cos_theta);
+                wi = ri * sin_theta > 1.0 || reflectance(cos_theta, ri) > g.next() ? reflect(ud, rec->normal)
+                                                                                    : refract(ud, rec->normal, ri);
+            }
+            break;
         }
         if (lit)
         {
             ++n.shadow_rays;
-            const bool blocked = occluded(s, ray{rec->p, ls.wi, r.time}, ls.distance, skip);
-            if (!blocked)
+            if (!occluded(s, ray{rec->p, light_dir, r.time}, light_distance, skip))
             {
                 radiance += contribution;
             }
@@ -281,6 +418,7 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
         }
         throughput = throughput * weight;
         bsdf_pdf = nee ? pdf : 0;
+        specular = delta;
         if (q.combination != RT_COMBINE_BSDF_ONLY && throughput.x == 0 && throughput.y == 0 && throughput.z == 0)
         {
             return radiance;
@@ -293,16 +431,29 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
     }
 }
 
-inline quality_scene make_quality(const scene& s, int combination)
+inline quality_scene make_quality(const scene& s, const rt_scene_desc& d)
 {
-    quality_scene q{s, build_lamps(s), {}, combination, 0};
+    quality_scene q{s, build_lamps(s), {}, d.combination, 0, false, environment{}, {}};
     const size_t ids = s.geometry.spheres.size() + s.geometry.quads.size() + s.geometry.triangles.size();
     q.lamp_of.assign(ids, -1);
     for (size_t k = 0; k < q.lamps.size(); ++k)
     {
         q.lamp_of[static_cast<size_t>(q.lamps[k].primitive)] = static_cast<int>(k);
     }
-    q.light_pmf = q.lamps.empty() ? 0.0 : 1.0 / static_cast<double>(q.lamps.size());
+    if (d.environment)
+    {
+        q.has_environment = true;
+        q.env = make_environment(*d.environment);
+    }
+    const int n = q.light_count();
+    q.light_pmf = n == 0 ? 0.0 : 1.0 / n;
+    for (const material& m : s.materials)
+    {
+        if (m.lobe == RT_MICROFACET_CONDUCTOR && q.energy.empty())
+        {
+            q.energy = ggx_energy_table();
+        }
+    }
     return q;
 }
 } // namespace oracle

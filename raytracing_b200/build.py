@@ -29,12 +29,14 @@ def nvcc() -> str:
 
 
 def _common_flags() -> list[str]:
-    return ["-std=c++20", "-O3", "-Xcompiler", "-fPIC", "-I", str(REPO / "include"), "-I", str(CSRC)]
+    return ["-std=c++20", "-O3", "-Xcompiler", "-fPIC", "-I", str(REPO / "include"), "-I", str(CSRC), "-I",
+            str(BUILD)]
 
 
 def _compile(source: Path) -> Path:
     obj = BUILD / (source.name + ".o")
-    deps = [source] + sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [REPO / "include" / "rt_b200.h"]
+    deps = [source] + sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + [REPO / "include" / "rt_b200.h",
+                                                                               BUILD / "ggx_energy_table.h"]
     if obj.exists() and obj.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return obj
     cmd = [nvcc()] + _common_flags()
@@ -49,10 +51,26 @@ def _compile(source: Path) -> Path:
     return obj
 
 
+def _generate_tables() -> None:
+    """Runs the build-time generators (csrc/gen): the GGX energy table, compiled into the library as constant data."""
+    source = CSRC / "gen" / "ggx_energy_gen.cpp"
+    header = BUILD / "ggx_energy_table.h"
+    if header.exists() and header.stat().st_mtime >= source.stat().st_mtime:
+        return
+    exe = BUILD / "ggx_energy_gen"
+    compiler = shutil.which("g++") or "c++"
+    result = subprocess.run([compiler, "-O2", "-std=c++20", "-pthread", str(source), "-o", str(exe)],
+                            capture_output=True, text=True)
+    if result.returncode != 0:
+        raise RuntimeError(f"compiling {source.name} failed:\n{result.stderr}")
+    subprocess.run([str(exe), str(header)], check=True)
+
+
 def build(verbose: bool = False) -> Path:
     """Compiles and links the library if any source is newer than it; returns its path."""
     BUILD.mkdir(exist_ok=True)
     OUT.mkdir(exist_ok=True)
+    _generate_tables()
     sources = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
     with concurrent.futures.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
         objects = list(pool.map(_compile, sources))

@@ -41,18 +41,18 @@ enum prim_kind : int32_t
     kind_triangle = 2,
 };
 
-constexpr int leaf_count_bits = 3; // at most 7 primitives in a leaf; 0 is the empty leaf
-constexpr int max_leaf_size = 7;
-constexpr int leaf_start_shift = 5;
+constexpr int leaf_count_bits = 4; // at most 15 primitives in a leaf; 0 is the empty leaf
+constexpr int max_leaf_size = 15;
+constexpr int leaf_start_shift = 6;
 constexpr int max_bvh_depth = 64; // the traversal stack's size
 
-// ~link = start << 5 | count << 2 | kind
+// ~link = start << 6 | count << 2 | kind
 RTB_HD inline int32_t leaf_link(int32_t start, int32_t count, int32_t kind)
 {
     return ~((start << leaf_start_shift) | (count << 2) | kind);
 }
 RTB_HD inline int32_t leaf_kind(int32_t link) { return (~link) & 3; }
-RTB_HD inline int32_t leaf_count(int32_t link) { return ((~link) >> 2) & 7; }
+RTB_HD inline int32_t leaf_count(int32_t link) { return ((~link) >> 2) & 15; }
 RTB_HD inline int32_t leaf_start(int32_t link) { return (~link) >> leaf_start_shift; }
 
 // A sphere: center and radius, one 16-byte load. A negative radius marks a sphere whose quadratic is solved in FP64
@@ -79,15 +79,43 @@ struct alignas(16) triangle12
     float e2z, pad0, pad1, pad2;
 };
 
-// A material as the shading reads it (src/gpu/material.cuh:18-26)
-struct alignas(16) material8
+// A material as the shading reads it (src/gpu/material.cuh:18-26), with the NEE/MIS integrator's GGX side entry
+// (renderer.h:249-261): 48 bytes, three 16-byte loads
+struct alignas(16) material12
 {
-    float r, g, b; // albedo, emission, or a metal's albedo (F0 for a GGX conductor)
-    int32_t kind;  // RT_LAMBERTIAN ...
+    float r, g, b;   // albedo, emission, or a metal's albedo (F0 for a GGX conductor)
+    int32_t kind;    // RT_LAMBERTIAN ...
     float fuzz;
     float ior;
-    int32_t lobe;  // 0 the books' material; 1 GGX conductor; 2 gloss coat (the quality integrator's side entry)
-    float alpha;   // GGX width r^2
+    int32_t lobe;    // RT_MICROFACET_NONE, _CONDUCTOR (the material is a metal of fuzz 0), _GLOSS (a lambertian)
+    float alpha;     // the GGX width r^2
+    float roughness; // r: the energy table's axis
+    float pad0, pad1, pad2;
+};
+
+// The environment map (src/gpu/environment_data.h): texels with their sampling density, the alias table's bins, the
+// rows' cosines, and the yaw
+struct alignas(16) env_texel
+{
+    float r, g, b, pdf; // radiance; the density Y/S per steradian of the cell's directions
+};
+
+struct alignas(8) alias_bin
+{
+    float q;       // the chance of the bin's own cell, on the 2^-24 grid
+    int32_t alias; // the cell that takes the rest
+};
+
+struct environment_view
+{
+    const env_texel* texels;
+    const alias_bin* bins;
+    const float* row_cos;    // height + 1
+    int32_t width, height;
+    int32_t log2_bins;
+    int32_t sampled;         // the map has light (S > 0) and an alias table: it is a light of the NEE set
+    float cos_yaw, sin_yaw;
+    float scale;
 };
 
 // A shape of the books' lights list (src/gpu/lights.cuh:18-45): what lights_pdf_value and lights_random read
@@ -141,13 +169,15 @@ struct scene_view
     int32_t node_count;
     int32_t prim_count;
     const int32_t* prim_material; // by global id
-    const material8* materials;
+    const material12* materials;
     const light24* lights;
     int32_t light_count;
     int32_t lamp_count;
     const emitter20* lamps;
     const int32_t* lamp_of;     // by global id, -1: no lamp
-    float light_pmf;
+    float light_pmf;         // 1 / (lamps + the map if it is sampled)
     int32_t combination;
+    int32_t has_environment; // misses see the map (the NEE/MIS integrator only), not the camera's sky
+    environment_view env;
 };
 } // namespace rtb

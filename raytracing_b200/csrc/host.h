@@ -121,11 +121,26 @@ private:
     device_array<triangle12> triangles_;
     device_array<int32_t> prim_material_;
     device_array<int32_t> prim_source_;
-    device_array<material8> materials_;
+    device_array<material12> materials_;
     device_array<light24> lights_;
     device_array<emitter20> lamps_;
     device_array<int32_t> lamp_of_;
+    device_array<env_texel> env_texels_;
+    device_array<alias_bin> env_bins_;
+    device_array<float> env_row_cos_;
 };
+
+// The environment map's tables (environment_table.cu:81-226 build_environment): texels with their densities Y/S,
+// Vose's alias table over the cells (coins on the 2^-24 grid, error diffusion), the rows' cosines
+struct environment_tables
+{
+    int width = 0, height = 0, log2_bins = 0;
+    double total = 0;
+    std::vector<env_texel> texels;
+    std::vector<alias_bin> bins;
+    std::vector<float> row_cos;
+};
+environment_tables build_environment(const rt_environment_desc& env);
 
 // One view of a resident scene whose image gains passes on demand (renderer.h:591-673)
 class session

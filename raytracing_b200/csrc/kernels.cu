@@ -18,6 +18,7 @@
 
 #include <cstdint>
 
+#include "ggx_energy_table.h"
 #include "kernels.cuh"
 #include "rt_b200.h"
 
@@ -84,16 +85,23 @@ struct sampler
     uint32_t pass;
     uint32_t job;
 
-    // Four numbers for dimension block `block` of the vertex at depth `depth` (0: the camera ray)
+    // Four 32-bit numbers for dimension block `block` of the vertex at depth `depth` (0: the camera ray)
+    __device__ __forceinline__ uint4 draw_bits(int depth, int block) const
+    {
+        return philox4x32_10(make_uint4(pixel, pass, (static_cast<uint32_t>(depth) << 4) | block, job), key);
+    }
+
+    // The same as uniform floats
     __device__ __forceinline__ float4 draw(int depth, int block) const
     {
-        const uint4 r = philox4x32_10(make_uint4(pixel, pass, (static_cast<uint32_t>(depth) << 4) | block, job), key);
+        const uint4 r = draw_bits(depth, block);
         return make_float4(to_unit(r.x), to_unit(r.y), to_unit(r.z), to_unit(r.w));
     }
 };
 
 // The fixed dimension blocks of a vertex: block 0 the material's own sample (direction u0 u1, lobe or mixture
-// choice u2, the lights list's pick u3), block 1 the books' lights-list point, block 2 the NEE light sample
+// choice u2, the lights list's pick u3), block 1 the books' lights-list point, blocks 2-3 the NEE light sample (the
+// pick, a lamp's point or the map's bin bits, coin and cell position)
 constexpr int block_material = 0;
 constexpr int block_lights = 1;
 constexpr int block_nee = 2;
@@ -733,6 +741,7 @@ struct path_state
     float3 throughput;
     float3 radiance; // the NEE/MIS integrator's light found so far
     float bsdf_pdf;  // the density of d at a vertex that took a light sample; 0 otherwise
+    bool specular;   // d left the camera or a delta vertex: an escape sees the map filtered
     int rays_left;
     int depth;       // rays traced so far in this sample (the next vertex's depth in the RNG counter)
     int from;
@@ -793,7 +802,7 @@ __device__ __forceinline__ step_result shade_books(const scene_view& S, const ca
         return step_result::done;
     }
     const surface s = surface_at(S, ps, h);
-    const material8 m = S.materials[s.material];
+    const material12 m = S.materials[s.material];
     const float3 albedo = make_float3(m.r, m.g, m.b);
     float3 direction;
     if (m.kind == RT_DIFFUSE_LIGHT)
@@ -879,7 +888,280 @@ __device__ __forceinline__ step_result shade_books(const scene_view& S, const ca
     return step_result::go_on;
 }
 
-// One segment of an NEE/MIS path (quality_path.cuh:83-188), after its closest hit. The shadow ray is traced here.
+// ---- GGX (ggx.cuh: Walter et al. 2007, Heitz 2014 and 2018, Dupuy & Benyoub 2023, Turquin 2019) --------------
+constexpr float min_ggx_alpha = 1e-3f; // below it, the perfect mirror with Schlick's F (ggx.cuh:37)
+
+__constant__ float ggx_energy_table[32 * 32] = {RTB_GGX_ENERGY_TABLE};
+
+__device__ __forceinline__ float smith_a(float c, float alpha2) { return sqrtf(fmaf(c * c, 1.0f - alpha2, alpha2)); }
+
+// D(h) = alpha^2 / (pi (alpha^2 c^2 + sin^2)^2), sin^2 from |n x h|^2 (exact near the peak)
+__device__ __forceinline__ float ggx_d(float3 n, float3 h, float alpha2)
+{
+    const float c = dot(n, h);
+    if (!(c > 0.0f))
+    {
+        return 0.0f;
+    }
+    const float3 s = cross(n, h);
+    const float d = fmaf(alpha2 * c, c, dot(s, s));
+    return alpha2 * inverse_pi_f / (d * d);
+}
+
+__device__ __forceinline__ float3 schlick(float3 f0, float cosine)
+{
+    const float x = fmaxf(0.0f, 1.0f - cosine);
+    const float x2 = x * x;
+    const float x5 = x2 * x2 * x;
+    return make_float3(fmaf(1.0f - f0.x, x5, f0.x), fmaf(1.0f - f0.y, x5, f0.y), fmaf(1.0f - f0.z, x5, f0.z));
+}
+
+// f * cos(theta_l) = F D cl / (2 (cl A_v + cv A_l)) and the visible-normal density D / (2 (cv + A_v))
+__device__ float3 ggx_eval(float3 n, float3 v, float3 l, float alpha, float3 f0, float& pdf)
+{
+    pdf = 0.0f;
+    const float cv = dot(n, v);
+    const float cl = dot(n, l);
+    const float3 sum = v + l;
+    const float len2 = length_squared(sum);
+    if (!(cv > 0.0f) || !(cl > 0.0f) || !(len2 > 0.0f))
+    {
+        return make_float3(0.0f, 0.0f, 0.0f);
+    }
+    const float3 h = rsqrtf(len2) * sum;
+    const float alpha2 = alpha * alpha;
+    const float d = ggx_d(n, h, alpha2);
+    const float av = smith_a(cv, alpha2);
+    const float al = smith_a(cl, alpha2);
+    pdf = d / (2.0f * (cv + av));
+    return (d * cl / (2.0f * (cl * av + cv * al))) * schlick(f0, dot(v, h));
+}
+
+// A direction by the visible normals with spherical caps: u1 the azimuth, u2 the height in the cap; weight
+// F G2/G1 (at most F); false: absorbed
+__device__ bool ggx_sample(float3 n, float3 v, float alpha, float3 f0, float u1, float u2, float3& l, float3& weight,
+                           float& pdf)
+{
+    const float cv = dot(n, v);
+    if (!(cv > 0.0f))
+    {
+        return false;
+    }
+    const float3 vs = unit_vector(alpha * (v - cv * n) + cv * n);
+    const float zs = dot(n, vs);
+    const float z = fmaf(1.0f - u2, 1.0f + zs, -zs);
+    const float sin_theta = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    float s, c;
+    sincospif(2.0f * u1, &s, &c);
+    const float3 cap = around(n, make_float3(sin_theta * c, sin_theta * s, z));
+    const float3 hs = cap + vs;
+    const float hn = dot(n, hs);
+    const float3 m = alpha * (hs - hn * n) + fmaxf(0.0f, hn) * n;
+    const float m2 = length_squared(m);
+    if (!(m2 > 0.0f))
+    {
+        return false;
+    }
+    const float3 h = rsqrtf(m2) * m;
+    const float vh = dot(v, h);
+    l = (2.0f * vh) * h - v;
+    const float cl = dot(n, l);
+    if (!(cl > 0.0f) || !(vh > 0.0f))
+    {
+        return false;
+    }
+    const float alpha2 = alpha * alpha;
+    const float av = smith_a(cv, alpha2);
+    const float al = smith_a(cl, alpha2);
+    weight = (cl * (cv + av) / (cl * av + cv * al)) * schlick(f0, vh);
+    pdf = ggx_d(n, h, alpha2) / (2.0f * (cv + av));
+    return true;
+}
+
+// Turquin's factor 1 + F0 (1 - E) / E, E from the energy table (bilinear; nodes sqrt(mu) = i/31, r = j/31)
+__device__ float3 ggx_compensation(float3 f0, float cos_v, float roughness)
+{
+    constexpr int last = 31;
+    const float x = sqrtf(fminf(fmaxf(cos_v, 0.0f), 1.0f)) * static_cast<float>(last);
+    const float y = fminf(fmaxf(roughness, 0.0f), 1.0f) * static_cast<float>(last);
+    const int i = min(static_cast<int>(x), last - 1);
+    const int j = min(static_cast<int>(y), last - 1);
+    const float fx = x - static_cast<float>(i);
+    const float fy = y - static_cast<float>(j);
+    const float* row = ggx_energy_table + j * 32 + i;
+    const float below = (1.0f - fx) * row[0] + fx * row[1];
+    const float above = (1.0f - fx) * row[32] + fx * row[33];
+    const float e = fminf((1.0f - fy) * below + fy * above, 1.0f);
+    const float lost = (1.0f - e) / e;
+    return make_float3(fmaf(f0.x, lost, 1.0f), fmaf(f0.y, lost, 1.0f), fmaf(f0.z, lost, 1.0f));
+}
+
+constexpr float gloss_coat_f0 = 0.04f;
+constexpr float gloss_diffuse_scale = 0.37200738f; // 28 / (23 pi) * (1 - 0.04)
+
+__device__ __forceinline__ float gloss_crossing(float c)
+{
+    const float x = 1.0f - 0.5f * c;
+    const float x2 = x * x;
+    return 1.0f - x2 * x2 * x;
+}
+
+// The coat over a matte base of color rho: GGX with F0 0.04 plus the coupled diffuse term; pdf the half-and-half
+// mixture of the two lobes' densities
+__device__ float3 gloss_eval(float3 n, float3 v, float3 l, float alpha, float3 rho, float& pdf)
+{
+    pdf = 0.0f;
+    const float cv = dot(n, v);
+    const float cl = dot(n, l);
+    if (!(cv > 0.0f) || !(cl > 0.0f))
+    {
+        return make_float3(0.0f, 0.0f, 0.0f);
+    }
+    float coat_pdf;
+    const float3 coat = ggx_eval(n, v, l, alpha, make_float3(gloss_coat_f0, gloss_coat_f0, gloss_coat_f0), coat_pdf);
+    pdf = 0.5f * (coat_pdf + cl * inverse_pi_f);
+    const float base = gloss_diffuse_scale * (gloss_crossing(cl) * gloss_crossing(cv)) * cl;
+    return coat + base * rho;
+}
+
+// ---- the environment map (environment.cuh, background.cuh) ---------------------------------------------------
+__device__ __forceinline__ float3 to_map(const environment_view& e, float3 d)
+{
+    return make_float3(e.cos_yaw * d.x + e.sin_yaw * d.z, d.y, -e.sin_yaw * d.x + e.cos_yaw * d.z);
+}
+
+__device__ __forceinline__ float3 from_map(const environment_view& e, float3 d)
+{
+    return make_float3(e.cos_yaw * d.x - e.sin_yaw * d.z, d.y, e.sin_yaw * d.x + e.cos_yaw * d.z);
+}
+
+// u = 0.5 + atan2(z, x) / (2 pi) across, t = atan2(sqrt(x^2 + z^2), y) / pi down: +y up, seen from inside
+__device__ __forceinline__ void map_coordinates(float3 m, float& u, float& t)
+{
+    u = 0.5f + atan2f(m.z, m.x) * (0.5f * inverse_pi_f);
+    t = atan2f(sqrtf(m.x * m.x + m.z * m.z), m.y) * inverse_pi_f;
+}
+
+__device__ __forceinline__ int clamp_index(int k, int n) { return k < 0 ? 0 : (k < n ? k : n - 1); }
+
+// The one map from a direction to its cell, used by escapes and light samples alike
+__device__ __forceinline__ int env_cell(const environment_view& e, float3 world)
+{
+    float u, t;
+    map_coordinates(to_map(e, world), u, t);
+    const int i = clamp_index(static_cast<int>(u * static_cast<float>(e.width)), e.width);
+    const int j = clamp_index(static_cast<int>(t * static_cast<float>(e.height)), e.height);
+    return j * e.width + i;
+}
+
+__device__ __forceinline__ float3 env_radiance(const environment_view& e, float3 dir, float& pdf)
+{
+    const env_texel texel = e.texels[env_cell(e, dir)];
+    pdf = texel.pdf;
+    return e.scale * make_float3(texel.r, texel.g, texel.b);
+}
+
+__device__ float3 env_radiance_filtered(const environment_view& e, float3 dir)
+{
+    float u, t;
+    map_coordinates(to_map(e, dir), u, t);
+    const float x = u * static_cast<float>(e.width) - 0.5f;
+    const float y = t * static_cast<float>(e.height) - 0.5f;
+    const float x0 = floorf(x);
+    const float y0 = floorf(y);
+    const float fx = x - x0;
+    const float fy = y - y0;
+    const int i = static_cast<int>(x0);
+    const int i0 = i < 0 ? i + e.width : i;
+    const int i1 = i0 + 1 < e.width ? i0 + 1 : 0;
+    const int j = static_cast<int>(y0);
+    const int j0 = clamp_index(j, e.height) * e.width;
+    const int j1 = clamp_index(j + 1, e.height) * e.width;
+    const auto texel = [&](int k) {
+        const env_texel t4 = e.texels[k];
+        return make_float3(t4.r, t4.g, t4.b);
+    };
+    const float3 a = texel(j0 + i0);
+    const float3 b = texel(j0 + i1);
+    const float3 c = texel(j1 + i0);
+    const float3 d = texel(j1 + i1);
+    const float3 top = a + fx * (b - a);
+    const float3 bottom = c + fx * (d - c);
+    return e.scale * (top + fy * (bottom - top));
+}
+
+// A cell from the alias table (the bin from the top bits of `bits`, then its coin), then a direction uniform over
+// the cell's solid angle; the radiance and density of the cell the direction lands in
+__device__ bool sample_environment(const environment_view& e, uint32_t bits, float coin, float s_theta, float s_phi,
+                                   float3& wi, float3& le, float& pdf)
+{
+    const int bin = static_cast<int>(bits >> (32 - e.log2_bins));
+    const alias_bin b = e.bins[bin];
+    const int cell = coin < b.q ? bin : b.alias;
+    const int j = cell / e.width;
+    const int i = cell - j * e.width;
+    const float top = e.row_cos[j];
+    const float bottom = e.row_cos[j + 1];
+    const float cos_theta = top - s_theta * (top - bottom);
+    const float sin_theta = sqrtf(fmaxf(0.0f, (1.0f - cos_theta) * (1.0f + cos_theta)));
+    float sp, cp;
+    sincospif(2.0f * (static_cast<float>(i) + s_phi) / static_cast<float>(e.width) - 1.0f, &sp, &cp);
+    wi = from_map(e, make_float3(sin_theta * cp, cos_theta, sin_theta * sp));
+    le = env_radiance(e, wi, pdf);
+    return pdf > 0.0f;
+}
+
+// ---- the NEE/MIS step (quality_path.cuh:83-188, bsdf.cuh:30-201, light_sampler.cuh:40-103) -------------------
+enum lobe_id : int
+{
+    lobe_lambertian,
+    lobe_isotropic,
+    lobe_conductor,
+    lobe_gloss,
+    lobe_smooth_conductor, // from here on: delta lobes (no density)
+    lobe_books_delta,
+};
+
+__device__ __forceinline__ int lobe_of(const material12& m)
+{
+    if (m.lobe == RT_MICROFACET_CONDUCTOR)
+    {
+        return m.alpha >= min_ggx_alpha ? lobe_conductor : lobe_smooth_conductor;
+    }
+    if (m.lobe == RT_MICROFACET_GLOSS)
+    {
+        return lobe_gloss;
+    }
+    return m.kind == RT_LAMBERTIAN ? lobe_lambertian : m.kind == RT_ISOTROPIC ? lobe_isotropic : lobe_books_delta;
+}
+
+// eval_bsdf: f * |cos| of a light sample's unit direction, and the lobe's density of it (0 for delta lobes)
+__device__ float3 eval_lobe(int lobe, const material12& m, float3 albedo, float3 n, float3 wo, float3 wi, float& pdf)
+{
+    if (lobe == lobe_lambertian)
+    {
+        pdf = cosine_density(n, wi);
+        return pdf * albedo;
+    }
+    if (lobe == lobe_isotropic)
+    {
+        pdf = uniform_sphere_density;
+        return uniform_sphere_density * albedo;
+    }
+    if (lobe == lobe_conductor)
+    {
+        const float3 single = ggx_eval(n, wo, wi, m.alpha, albedo, pdf);
+        return ggx_compensation(albedo, dot(n, wo), m.roughness) * single;
+    }
+    if (lobe == lobe_gloss)
+    {
+        return gloss_eval(n, wo, wi, m.alpha, albedo, pdf);
+    }
+    pdf = 0.0f;
+    return make_float3(0.0f, 0.0f, 0.0f);
+}
+
+// One segment of an NEE/MIS path after its closest hit; the shadow ray is traced here
 template <bool COUNT>
 __device__ __forceinline__ step_result shade_quality(const scene_view& S, const camera_params& cam,
                                                      const sampler& rng, path_state& ps, const hit_info& h,
@@ -887,12 +1169,27 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
 {
     if (h.id < 0)
     {
-        // The sky: no light sample draws it, so it counts in full
-        sample = ps.radiance + ps.throughput * sky(cam, ps.d);
+        // The environment (filtered after the camera and delta vertices, the nearest texel with its density
+        // otherwise), or the camera's sky
+        if (!S.has_environment)
+        {
+            sample = ps.radiance + ps.throughput * sky(cam, ps.d);
+            return step_result::done;
+        }
+        if (ps.specular)
+        {
+            sample = ps.radiance + ps.throughput * env_radiance_filtered(S.env, ps.d);
+            return step_result::done;
+        }
+        float density;
+        const float3 le = env_radiance(S.env, ps.d, density);
+        const float p_light = S.env.sampled ? S.light_pmf * density : 0.0f;
+        const float w = ps.bsdf_pdf > 0.0f ? bsdf_weight(S.combination, ps.bsdf_pdf, p_light) : 1.0f;
+        sample = ps.radiance + w * (ps.throughput * le);
         return step_result::done;
     }
     const surface s = surface_at(S, ps, h);
-    const material8 m = S.materials[s.material];
+    const material12 m = S.materials[s.material];
     const float3 albedo = make_float3(m.r, m.g, m.b);
     if (m.kind == RT_DIFFUSE_LIGHT)
     {
@@ -911,52 +1208,124 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
         sample = ps.radiance + w * (h.front ? ps.throughput * albedo : make_float3(0.0f, 0.0f, 0.0f));
         return step_result::done;
     }
-    const bool delta = m.kind == RT_METAL || m.kind == RT_DIELECTRIC;
-    const bool nee = S.combination != RT_COMBINE_BSDF_ONLY && ps.rays_left > 1 && !delta && S.lamp_count > 0 &&
+    const int lobe = lobe_of(m);
+    const bool delta = lobe >= lobe_smooth_conductor;
+    const float3 wo = -unit_vector(ps.d);
+    const int lights = S.lamp_count + (S.env.sampled ? 1 : 0);
+    const bool nee = S.combination != RT_COMBINE_BSDF_ONLY && ps.rays_left > 1 && !delta && lights > 0 &&
                      largest_channel(ps.throughput) > 0.0f;
     bool lit = false;
     float3 contribution = make_float3(0.0f, 0.0f, 0.0f);
-    lamp_sample ls;
+    float3 light_dir = make_float3(0.0f, 0.0f, 0.0f);
+    float light_distance = infinity_f;
     int skip = -1;
     if (nee)
     {
-        const float4 v = rng.draw(ps.depth, block_nee);
-        int k = static_cast<int>(v.x * static_cast<float>(S.lamp_count));
-        k = k < S.lamp_count ? k : S.lamp_count - 1;
-        const emitter20 e = S.lamps[k];
-        if (sample_lamp(e, s.p, v.y, v.z, ls))
+        // One number picks a light, the lamps first and the map last (light_sampler.cuh:40-75)
+        const uint4 bits = rng.draw_bits(ps.depth, block_nee);
+        const float pick = to_unit(bits.x);
+        int k = static_cast<int>(pick * static_cast<float>(lights));
+        k = k < lights ? k : lights - 1;
+        bool drawn = false;
+        float3 le;
+        float p_light = 0.0f;
+        if (k < S.lamp_count)
         {
-            const float p_light = S.light_pmf * ls.pdf;
-            const float p_bsdf = m.kind == RT_LAMBERTIAN ? cosine_density(s.normal, ls.wi) : uniform_sphere_density;
-            const float3 f = p_bsdf * albedo;
+            const emitter20 e = S.lamps[k];
+            lamp_sample ls;
+            if (sample_lamp(e, s.p, to_unit(bits.y), to_unit(bits.z), ls))
+            {
+                drawn = true;
+                light_dir = ls.wi;
+                light_distance = ls.distance;
+                le = make_float3(e.er, e.eg, e.eb);
+                p_light = S.light_pmf * ls.pdf;
+                skip = e.primitive;
+            }
+        }
+        else
+        {
+            float density;
+            const float s_phi = rng.draw(ps.depth, block_nee + 1).x;
+            if (sample_environment(S.env, bits.y, to_unit(bits.z), to_unit(bits.w), s_phi, light_dir, le, density))
+            {
+                drawn = true;
+                p_light = S.light_pmf * density;
+            }
+        }
+        if (drawn)
+        {
+            float p_bsdf;
+            const float3 f = eval_lobe(lobe, m, albedo, s.normal, wo, light_dir, p_bsdf);
             if (p_light > 0.0f && largest_channel(f) > 0.0f)
             {
-                contribution = (light_weight(S.combination, p_light, p_bsdf) / p_light) *
-                               (ps.throughput * (f * make_float3(e.er, e.eg, e.eb)));
+                contribution =
+                    (light_weight(S.combination, p_light, p_bsdf) / p_light) * (ps.throughput * (f * le));
                 const float sum = contribution.x + contribution.y + contribution.z;
                 lit = sum > 0.0f && sum < infinity_f;
-                skip = e.primitive;
             }
         }
     }
     // The material's own sample: the path's next ray
     const float4 u = rng.draw(ps.depth, block_material);
-    float3 wi;
+    float3 wi = make_float3(0.0f, 0.0f, 0.0f);
     float3 weight = albedo;
     float pdf = 0.0f;
     bool scattered = true;
-    if (m.kind == RT_LAMBERTIAN)
+    if (lobe == lobe_lambertian)
     {
         wi = around(s.normal, random_cosine_direction(u.x, u.y));
         scattered = dot(s.normal, wi) > 0.0f;
         pdf = cosine_density(s.normal, wi);
+    }
+    else if (lobe == lobe_isotropic)
+    {
+        wi = random_unit_vector(u.x, u.y);
+        pdf = uniform_sphere_density;
+    }
+    else if (lobe == lobe_conductor)
+    {
+        scattered = ggx_sample(s.normal, wo, m.alpha, albedo, u.x, u.y, wi, weight, pdf);
+        if (scattered)
+        {
+            weight = weight * ggx_compensation(albedo, dot(s.normal, wo), m.roughness);
+        }
+    }
+    else if (lobe == lobe_gloss)
+    {
+        // The coat or the base, half the time each, then the mixture's weight and density (ggx.cuh:300-324)
+        if (u.z < 0.5f)
+        {
+            float3 coat_weight;
+            float coat_pdf;
+            scattered = ggx_sample(s.normal, wo, m.alpha, make_float3(gloss_coat_f0, gloss_coat_f0, gloss_coat_f0),
+                                   u.x, u.y, wi, coat_weight, coat_pdf);
+        }
+        else
+        {
+            wi = around(s.normal, random_cosine_direction(u.x, u.y));
+            scattered = dot(s.normal, wi) > 0.0f;
+        }
+        if (scattered)
+        {
+            const float3 f = gloss_eval(s.normal, wo, wi, m.alpha, albedo, pdf);
+            scattered = pdf > 0.0f;
+            weight = (1.0f / pdf) * f;
+        }
+    }
+    else if (lobe == lobe_smooth_conductor)
+    {
+        // The mirror with Schlick's F: no random number (bsdf.cuh:153-166)
+        scattered = dot(s.normal, wo) > 0.0f;
+        wi = unit_vector(reflect(-wo, s.normal));
+        weight = schlick(albedo, dot(s.normal, wo));
     }
     else if (m.kind == RT_METAL)
     {
         wi = unit_vector(reflect(ps.d, s.normal)) + m.fuzz * random_unit_vector(u.x, u.y);
         scattered = dot(wi, s.normal) > 0.0f;
     }
-    else if (m.kind == RT_DIELECTRIC)
+    else // dielectric
     {
         const float ri = h.front ? 1.0f / m.ior : m.ior;
         const float3 ud = unit_vector(ps.d);
@@ -966,17 +1335,12 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
                                                                        : refract(ud, s.normal, ri);
         weight = make_float3(1.0f, 1.0f, 1.0f);
     }
-    else // isotropic
-    {
-        wi = random_unit_vector(u.x, u.y);
-        pdf = uniform_sphere_density;
-    }
     if (lit)
     {
         ++shadow_rays;
         hit_info blocker;
-        const bool blocked = traverse<true, COUNT>(S, s.p, ls.wi, ls.distance, h.id, dot(ls.wi, s.outward) < 0.0f,
-                                                   skip, blocker, counts);
+        const bool blocked = traverse<true, COUNT>(S, s.p, light_dir, light_distance, h.id,
+                                                   dot(light_dir, s.outward) < 0.0f, skip, blocker, counts);
         if (!blocked)
         {
             ps.radiance = ps.radiance + contribution;
@@ -989,6 +1353,7 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
     }
     ps.throughput = ps.throughput * weight;
     ps.bsdf_pdf = nee ? pdf : 0.0f;
+    ps.specular = delta;
     if (S.combination != RT_COMBINE_BSDF_ONLY && ps.throughput.x == 0.0f && ps.throughput.y == 0.0f &&
         ps.throughput.z == 0.0f)
     {
@@ -1008,14 +1373,19 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
 }
 
 // ---- the persistent render kernel ------------------------------------------------------------------------------
-// The render kernel's resident blocks per multiprocessor, which caps its registers at 64: 8 blocks of 128 threads
-// measured fastest on every workload against 5 (96 registers) and 6 (80), for the latency it hides
+// The render kernel's resident blocks per multiprocessor, which caps its registers: the books' integrator at 64 (8
+// blocks of 128 threads measured fastest against 5 and 6 blocks, for the latency they hide), the NEE/MIS integrator,
+// whose GGX and environment code spills heavily at 64, at 80 (6 blocks)
 #ifndef RTB_MIN_BLOCKS
 #define RTB_MIN_BLOCKS 8
 #endif
+#ifndef RTB_MIN_BLOCKS_QUALITY
+#define RTB_MIN_BLOCKS_QUALITY 6
+#endif
 
 template <bool QUALITY, bool COUNT>
-__global__ void __launch_bounds__(render_block, RTB_MIN_BLOCKS) render_kernel(const __grid_constant__ launch_params P)
+__global__ void __launch_bounds__(render_block, QUALITY ? RTB_MIN_BLOCKS_QUALITY : RTB_MIN_BLOCKS)
+    render_kernel(const __grid_constant__ launch_params P)
 {
     __shared__ unsigned long long block_rays;
     __shared__ unsigned long long block_shadow_rays;
@@ -1098,6 +1468,7 @@ __global__ void __launch_bounds__(render_block, RTB_MIN_BLOCKS) render_kernel(co
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
             ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
             ps.bsdf_pdf = 0.0f;
+            ps.specular = true;
             ps.rays_left = cam.max_depth;
             ps.depth = 0;
             ps.from = -1;

@@ -61,7 +61,12 @@ quad12 make_quad(const rt_quad_desc& d)
     return q;
 }
 
-// The largest leaf of a scene of spheres and quads with more than 8 primitives (one leaf holds them all below)
+// A scene of at most RTB_SMALL_SCENE primitives gets one leaf per primitive kind (a test of all of them beats a
+// tree walk there, as the reference found for up to 8 shapes, renderer.cu:75-82); a larger scene of spheres and quads
+// gets leaves of at most RTB_LEAF_SIZE
+#ifndef RTB_SMALL_SCENE
+#define RTB_SMALL_SCENE 16
+#endif
 #ifndef RTB_LEAF_SIZE
 #define RTB_LEAF_SIZE 1
 #endif
@@ -266,16 +271,58 @@ void validate(const rt_scene_desc& d)
     {
         fail(RT_ERR_RUNTIME, "microfacets: none, or one per material");
     }
+    bool side_entries = false;
     for (int64_t i = 0; i < d.microfacet_count; ++i)
     {
-        if (d.microfacets[i].kind != RT_MICROFACET_NONE)
+        const rt_microfacet_desc& f = d.microfacets[i];
+        if (f.kind == RT_MICROFACET_NONE)
         {
-            fail(RT_ERR_UNSUPPORTED, "GGX microfacet side entries are not rendered by this build yet");
+            continue;
+        }
+        side_entries = true;
+        const std::string where = "microfacets[" + std::to_string(i) + "]";
+        if (f.kind != RT_MICROFACET_CONDUCTOR && f.kind != RT_MICROFACET_GLOSS)
+        {
+            fail(RT_ERR_RUNTIME, where + " has no valid kind");
+        }
+        if (!(f.roughness >= 0 && f.roughness <= 1))
+        {
+            fail(RT_ERR_RUNTIME, where + ".roughness must be in [0, 1]");
+        }
+        // renderer.h:249-261: a conductor completes a metal of fuzz 0, a coat a lambertian, whose alpha is >= 1e-3
+        const rt_material_desc& m = d.materials[i];
+        if (f.kind == RT_MICROFACET_CONDUCTOR && !(m.kind == RT_METAL && m.fuzz == 0))
+        {
+            fail(RT_ERR_RUNTIME, where + ": a conductor's material must be a metal of fuzz 0");
+        }
+        if (f.kind == RT_MICROFACET_GLOSS && (m.kind != RT_LAMBERTIAN || f.roughness * f.roughness < 1e-3))
+        {
+            fail(RT_ERR_RUNTIME, where + ": a coat's material must be a lambertian, with roughness^2 >= 1e-3");
         }
     }
     if (d.environment)
     {
-        fail(RT_ERR_UNSUPPORTED, "environment maps are not rendered by this build yet");
+        const rt_environment_desc& e = *d.environment;
+        if (e.image.width < 1 || e.image.height < 1 || e.image.width > 2048 || e.image.height > 1024 || !e.image.rgb)
+        {
+            fail(RT_ERR_RUNTIME, "an environment map has 1x1 to 2048x1024 texels");
+        }
+        if (!std::isfinite(e.yaw_degrees) || !(std::isfinite(e.scale) && e.scale >= 0))
+        {
+            fail(RT_ERR_INVALID, "an environment map's yaw and scale must be finite, the scale >= 0");
+        }
+        const int64_t n = int64_t{e.image.width} * e.image.height * 3;
+        for (int64_t k = 0; k < n; ++k)
+        {
+            if (!(std::isfinite(e.image.rgb[k]) && e.image.rgb[k] >= 0))
+            {
+                fail(RT_ERR_RUNTIME, "an environment map's texels must be finite and >= 0");
+            }
+        }
+    }
+    if ((side_entries || d.environment) && !d.quality)
+    {
+        fail(RT_ERR_INVALID, "GGX side entries and environment maps need the NEE/MIS integrator (quality)");
     }
 }
 
@@ -381,7 +428,8 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     }
 
     bvh_options options;
-    options.max_leaf_size = prims.size() <= 8 ? 7 : (source_triangles.empty() ? RTB_LEAF_SIZE : 4);
+    options.max_leaf_size = prims.size() <= RTB_SMALL_SCENE ? max_leaf_size
+                                                            : (source_triangles.empty() ? RTB_LEAF_SIZE : 4);
     const bvh_result tree = build_bvh(std::move(prims), options);
 
     // Each kind's array in leaf order; global ids: spheres, then quads, then triangles
@@ -420,11 +468,11 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     }
 
     // Materials: a solid texture becomes the material's color (renderer.cu:551-600)
-    std::vector<material8> materials;
+    std::vector<material12> materials;
     for (int64_t i = 0; i < d.material_count; ++i)
     {
         const rt_material_desc& m = d.materials[i];
-        material8 v{};
+        material12 v{};
         v.kind = m.kind;
         const rt_vec3 color = m.kind == RT_METAL || m.kind == RT_DIELECTRIC ? m.albedo : d.textures[m.texture].rgb;
         v.r = static_cast<float>(color.x);
@@ -432,6 +480,12 @@ resident_scene::resident_scene(const rt_scene_desc& d)
         v.b = static_cast<float>(color.z);
         v.fuzz = static_cast<float>(std::min(m.fuzz, 1.0));
         v.ior = static_cast<float>(m.refraction_index);
+        if (i < d.microfacet_count)
+        {
+            v.lobe = d.microfacets[i].kind;
+            v.roughness = static_cast<float>(d.microfacets[i].roughness);
+            v.alpha = static_cast<float>(d.microfacets[i].roughness * d.microfacets[i].roughness);
+        }
         materials.push_back(v);
     }
 
@@ -551,6 +605,27 @@ resident_scene::resident_scene(const rt_scene_desc& d)
         }
     }
 
+    // The environment map's tables (the NEE/MIS integrator's sky and light)
+    environment_view env{};
+    if (d.environment)
+    {
+        const environment_tables t = build_environment(*d.environment);
+        env_texels_.upload(t.texels);
+        env_bins_.upload(t.bins);
+        env_row_cos_.upload(t.row_cos);
+        env.texels = env_texels_.data();
+        env.bins = env_bins_.data();
+        env.row_cos = env_row_cos_.data();
+        env.width = t.width;
+        env.height = t.height;
+        env.log2_bins = t.log2_bins;
+        env.sampled = t.total > 0 ? 1 : 0;
+        const double yaw = d.environment->yaw_degrees * 3.14159265358979323846 / 180;
+        env.cos_yaw = static_cast<float>(std::cos(yaw));
+        env.sin_yaw = static_cast<float>(std::sin(yaw));
+        env.scale = static_cast<float>(d.environment->scale);
+    }
+
     nodes_.upload(tree.nodes);
     spheres_.upload(spheres);
     quads_.upload(quads);
@@ -577,8 +652,11 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     view_.lamp_count = quality_ ? static_cast<int32_t>(lamps.size()) : 0;
     view_.lamps = lamps_.data();
     view_.lamp_of = lamp_of_.data();
-    view_.light_pmf = lamps.empty() ? 0.0f : static_cast<float>(1.0 / static_cast<double>(lamps.size()));
+    const size_t light_set = lamps.size() + (env.sampled ? 1 : 0);
+    view_.light_pmf = light_set == 0 ? 0.0f : static_cast<float>(1.0 / static_cast<double>(light_set));
     view_.combination = quality_ ? d.combination : RT_COMBINE_BSDF_ONLY;
+    view_.has_environment = d.environment ? 1 : 0;
+    view_.env = env;
 
     stats_.spheres = S;
     stats_.quads = Q;
@@ -589,7 +667,8 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     stats_.lights = static_cast<int64_t>(lights.size());
     stats_.device_bytes = static_cast<int64_t>(nodes_.bytes() + spheres_.bytes() + quads_.bytes() + triangles_.bytes() +
                                                prim_material_.bytes() + prim_source_.bytes() + materials_.bytes() +
-                                               lights_.bytes() + lamps_.bytes() + lamp_of_.bytes());
+                                               lights_.bytes() + lamps_.bytes() + lamp_of_.bytes() +
+                                               env_texels_.bytes() + env_bins_.bytes() + env_row_cos_.bytes());
     stats_.depth = tree.depth;
     stats_.max_leaf_size = options.max_leaf_size;
 }

@@ -8,12 +8,14 @@
 // across standard libraries, so the cover scene built here is libstdc++'s, and every renderer (the oracle, the
 // reference's own GPU build, this one) is fed the same serialized tables.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <numbers>
 #include <random>
 #include <string>
+#include <unordered_map>
 
 #include "scene_store.h"
 
@@ -267,6 +269,175 @@ void short_block(scene_store& s, int material)
 {
     const placement where = placement{}.translated(v3(130, 0, 65)).rotated_y(-18);
     box_faces(v3(0, 0, 0), v3(165, 165, 165), s.quads, material, where);
+}
+
+// perlin.ixx: 256 random unit gradients and three Fisher-Yates permutations of 0..255, drawn from the scene's
+// generator in that order; noise() blends the 8 lattice corners' dot products with Hermite weights; turbulence() sums
+// `depth` octaves, each twice as fine and half as strong, and takes the absolute value
+class perlin_noise
+{
+public:
+    explicit perlin_noise(scene_random& rng)
+    {
+        for (rt_vec3& v : gradients_)
+        {
+            v = unit_vector(rng.vec(-1, 1));
+        }
+        permute(perm_x_, rng);
+        permute(perm_y_, rng);
+        permute(perm_z_, rng);
+    }
+
+    double noise(rt_vec3 p) const
+    {
+        const double fx = std::floor(p.x), fy = std::floor(p.y), fz = std::floor(p.z);
+        const int i = static_cast<int>(fx), j = static_cast<int>(fy), k = static_cast<int>(fz);
+        const double u = p.x - fx, v = p.y - fy, w = p.z - fz;
+        const double uu = u * u * (3 - 2 * u), vv = v * v * (3 - 2 * v), ww = w * w * (3 - 2 * w);
+        double accum = 0;
+        for (int di = 0; di < 2; ++di)
+        {
+            for (int dj = 0; dj < 2; ++dj)
+            {
+                for (int dk = 0; dk < 2; ++dk)
+                {
+                    const rt_vec3& g = gradients_[static_cast<size_t>(perm_x_[(i + di) & 255] ^ perm_y_[(j + dj) & 255] ^
+                                                                      perm_z_[(k + dk) & 255])];
+                    const rt_vec3 offset{u - di, v - dj, w - dk};
+                    accum += (di * uu + (1 - di) * (1 - uu)) * (dj * vv + (1 - dj) * (1 - vv)) *
+                             (dk * ww + (1 - dk) * (1 - ww)) * dot(g, offset);
+                }
+            }
+        }
+        return accum;
+    }
+
+    double turbulence(rt_vec3 p, int depth) const
+    {
+        double accum = 0;
+        double weight = 1;
+        for (int layer = 0; layer < depth; ++layer)
+        {
+            accum += weight * noise(p);
+            weight *= 0.5;
+            p = mul(2, p);
+        }
+        return std::fabs(accum);
+    }
+
+private:
+    std::array<rt_vec3, 256> gradients_;
+    std::array<int, 256> perm_x_, perm_y_, perm_z_;
+
+    static void permute(std::array<int, 256>& perm, scene_random& rng)
+    {
+        for (int i = 0; i < 256; ++i)
+        {
+            perm[static_cast<size_t>(i)] = i;
+        }
+        for (int i = 255; i > 0; --i)
+        {
+            const int target = static_cast<int>(rng.next(0, i + 1)); // random_int(0, i)
+            std::swap(perm[static_cast<size_t>(i)], perm[static_cast<size_t>(target)]);
+        }
+    }
+};
+
+// meshes.ixx:159-230 icosphere(level): the icosahedron, its faces turned counter-clockwise seen from outside, each
+// triangle cut into four `level` times with the edge midpoints pushed onto the unit sphere (shared between the two
+// triangles of an edge): V = 10 * 4^k + 2 vertices and T = 20 * 4^k triangles
+void icosphere(int level, std::vector<rt_vec3>& points, std::vector<std::array<uint32_t, 3>>& faces)
+{
+    const double phi = (1 + std::sqrt(5.0)) / 2;
+    points = {{-1, phi, 0}, {1, phi, 0},  {-1, -phi, 0}, {1, -phi, 0}, {0, -1, phi},  {0, 1, phi},
+              {0, -1, -phi}, {0, 1, -phi}, {phi, 0, -1},  {phi, 0, 1},  {-phi, 0, -1}, {-phi, 0, 1}};
+    for (rt_vec3& p : points)
+    {
+        p = unit_vector(p);
+    }
+    faces = {{0, 11, 5}, {0, 5, 1},  {0, 1, 7},   {0, 7, 10}, {0, 10, 11}, {1, 5, 9},  {5, 11, 4},
+             {11, 10, 2}, {10, 7, 6}, {7, 1, 8},   {3, 9, 4},  {3, 4, 2},   {3, 2, 6},  {3, 6, 8},
+             {3, 8, 9},  {4, 9, 5},  {2, 4, 11},  {6, 2, 10}, {8, 6, 7},   {9, 8, 1}};
+    for (auto& f : faces)
+    {
+        if (dot(cross(sub(points[f[1]], points[f[0]]), sub(points[f[2]], points[f[0]])), points[f[0]]) < 0)
+        {
+            std::swap(f[1], f[2]);
+        }
+    }
+    for (int k = 0; k < level; ++k)
+    {
+        std::unordered_map<uint64_t, uint32_t> midpoints;
+        midpoints.reserve(faces.size() * 3 / 2);
+        const auto midpoint = [&](uint32_t a, uint32_t b) {
+            const uint64_t key = (uint64_t{std::min(a, b)} << 32) | std::max(a, b);
+            const auto [it, added] = midpoints.try_emplace(key, static_cast<uint32_t>(points.size()));
+            if (added)
+            {
+                points.push_back(unit_vector(add(points[a], points[b])));
+            }
+            return it->second;
+        };
+        std::vector<std::array<uint32_t, 3>> finer;
+        finer.reserve(faces.size() * 4);
+        for (const auto& f : faces)
+        {
+            const uint32_t ab = midpoint(f[0], f[1]);
+            const uint32_t bc = midpoint(f[1], f[2]);
+            const uint32_t ca = midpoint(f[2], f[0]);
+            finer.push_back({f[0], ab, ca});
+            finer.push_back({f[1], bc, ab});
+            finer.push_back({f[2], ca, bc});
+            finer.push_back({ab, bc, ca});
+        }
+        faces = std::move(finer);
+    }
+}
+
+// A synthetic equirectangular sky, +y up, row 0 at the top: the daylight gradient of camera.ixx:21-31 by the
+// direction's height, plus a sun disc of angular diameter sun_degrees at radiance sun_radiance, its coverage of each
+// texel measured by 8 x 8 sub-samples (so the sun's light is spread over the texels it really covers)
+void sky_with_sun(int width, int height, rt_vec3 sun_dir, double sun_degrees, double sun_radiance,
+                  std::vector<float>& rgb)
+{
+    rgb.assign(static_cast<size_t>(width) * height * 3, 0.0f);
+    const double cos_sun = std::cos(degrees_to_radians(sun_degrees / 2));
+    const auto direction = [&](double u, double t) {
+        const double ph = 2 * std::numbers::pi * (u - 0.5);
+        const double th = std::numbers::pi * t;
+        return rt_vec3{std::sin(th) * std::cos(ph), std::cos(th), std::sin(th) * std::sin(ph)};
+    };
+    // the texel size in angle, to find the texels near the sun
+    const double texel_radians = std::numbers::pi / height;
+    for (int j = 0; j < height; ++j)
+    {
+        for (int i = 0; i < width; ++i)
+        {
+            const rt_vec3 d = direction((i + 0.5) / width, (j + 0.5) / height);
+            const double a = 0.5 * (d.y + 1.0);
+            float* out = rgb.data() + 3 * (static_cast<size_t>(j) * width + i);
+            out[0] = static_cast<float>((1 - a) * 1.0 + a * 0.5);
+            out[1] = static_cast<float>((1 - a) * 1.0 + a * 0.7);
+            out[2] = static_cast<float>((1 - a) * 1.0 + a * 1.0);
+            if (std::acos(std::clamp(dot(d, sun_dir), -1.0, 1.0)) > degrees_to_radians(sun_degrees) + 4 * texel_radians)
+            {
+                continue;
+            }
+            int inside = 0;
+            for (int sj = 0; sj < 8; ++sj)
+            {
+                for (int si = 0; si < 8; ++si)
+                {
+                    const rt_vec3 s = direction((i + (si + 0.5) / 8) / width, (j + (sj + 0.5) / 8) / height);
+                    inside += dot(s, sun_dir) >= cos_sun ? 1 : 0;
+                }
+            }
+            const auto sun = static_cast<float>(sun_radiance * inside / 64.0);
+            out[0] += sun;
+            out[1] += sun;
+            out[2] += sun;
+        }
+    }
 }
 
 // Applies the overrides of rt_builtin_params to the scene's camera settings and computes the frame
@@ -617,6 +788,112 @@ rt_status build_builtin(const std::string& name, const rt_builtin_params& p, std
         c.sky_bottom = v3(1, 1, 1);
         c.sky_top = v3(1, 1, 1);
         set_camera(*s, c, p, false);
+    }
+    else if (name == "env-furnace" || name == "ggx-furnace")
+    {
+        // gpu_scenes_environments.ixx:96-110 env-furnace: the white furnace's sphere and camera under a constant map
+        // of radiance 1, every pixel exactly 1 under the material's own sampling. ggx-furnace (gpu_scenes.ixx:66-67,
+        // one sphere): a white GGX conductor (F0 = 1, roughness sqrt(0.3), alpha 0.3) whose centre keeps, with
+        // Turquin's compensation, all of the light (docs/quality.md:136-144)
+        int material;
+        if (name == "env-furnace")
+        {
+            material = s->lambertian(v3(1, 1, 1));
+        }
+        else
+        {
+            material = s->metal(v3(1, 1, 1), 0.0);
+        }
+        s->spheres.push_back(make_sphere(v3(0, 0, 0), 1.0, material));
+        if (name == "ggx-furnace")
+        {
+            s->microfacets.assign(s->materials.size(), rt_microfacet_desc{});
+            s->microfacets[static_cast<size_t>(material)] = {RT_MICROFACET_CONDUCTOR, 0, std::sqrt(0.3)};
+        }
+        const int w = p.env_width > 0 ? p.env_width : 64;
+        s->has_environment = true;
+        s->environment_pixels.assign(static_cast<size_t>(w) * (w / 2) * 3, 1.0f);
+        s->environment.image.width = w;
+        s->environment.image.height = w / 2;
+        s->environment.scale = 1;
+        s->quality = 1;
+        s->combination = RT_COMBINE_BSDF_ONLY;
+        camera_settings c;
+        c.aspect_ratio = 16.0 / 9.0;
+        c.image_width = 480;
+        c.samples_per_pixel = 64;
+        c.max_depth = 10;
+        c.sampling = RT_SAMPLING_MATERIAL;
+        c.vfov = 30;
+        c.lookfrom = v3(0, 0, 6);
+        c.lookat = v3(0, 0, 0);
+        rt_builtin_params q = p;
+        q.sampling = RT_SAMPLING_MATERIAL;
+        set_camera(*s, c, q, false);
+    }
+    else if (name == "mesh-ggx")
+    {
+        // A triangle mesh under an HDR sky: an icosphere of level 8 (1,310,720 triangles) displaced along its normal by
+        // 0.15 x 4-octave Perlin turbulence, a rough GGX metal (r = 0.3, F0 (0.95, 0.64, 0.54)), standing on a plane
+        // under a glossy coat (rho 0.73, r = 0.2); lit by a 1024 x 512 sky gradient with a 0.5-degree sun of radiance
+        // 5e4, 48 degrees high, sampled by its brightness. The NEE/MIS integrator, power heuristic.
+        const int level = p.mesh_level > 0 ? std::min(p.mesh_level, 9) : 8;
+        std::vector<rt_vec3> points;
+        std::vector<std::array<uint32_t, 3>> faces;
+        icosphere(level, points, faces);
+        const perlin_noise noise(rng);
+        const rt_vec3 center{0, 1.3, 0};
+        mesh_store mesh;
+        mesh.positions.reserve(points.size() * 3);
+        for (const rt_vec3& v : points)
+        {
+            const double r = 1 + 0.15 * noise.turbulence(mul(2.0, v), 4);
+            mesh.positions.push_back(static_cast<float>(center.x + r * v.x));
+            mesh.positions.push_back(static_cast<float>(center.y + r * v.y));
+            mesh.positions.push_back(static_cast<float>(center.z + r * v.z));
+        }
+        mesh.indices.reserve(faces.size() * 3);
+        for (const auto& f : faces)
+        {
+            mesh.indices.insert(mesh.indices.end(), {f[0], f[1], f[2]});
+        }
+        const int metal = s->metal(v3(0.95, 0.64, 0.54), 0.0);
+        const int plane = s->lambertian(v3(0.73, 0.73, 0.73));
+        mesh.material = metal;
+        s->meshes.push_back(std::move(mesh));
+        s->quads.push_back(make_quad(v3(-100, 0, -100), v3(0, 0, 200), v3(200, 0, 0), plane));
+        s->microfacets.resize(s->materials.size());
+        for (rt_microfacet_desc& f : s->microfacets)
+        {
+            f = rt_microfacet_desc{};
+        }
+        s->microfacets[static_cast<size_t>(metal)] = {RT_MICROFACET_CONDUCTOR, 0, 0.3};
+        s->microfacets[static_cast<size_t>(plane)] = {RT_MICROFACET_GLOSS, 0, 0.2};
+        const int env_width = p.env_width > 0 ? p.env_width : 1024;
+        const double elevation = degrees_to_radians(48);
+        const double azimuth = degrees_to_radians(35);
+        const rt_vec3 sun{std::cos(elevation) * std::sin(azimuth), std::sin(elevation),
+                          std::cos(elevation) * std::cos(azimuth)};
+        s->has_environment = true;
+        sky_with_sun(env_width, env_width / 2, sun, 0.5, 5e4, s->environment_pixels);
+        s->environment.image.width = env_width;
+        s->environment.image.height = env_width / 2;
+        s->environment.yaw_degrees = 0;
+        s->environment.scale = 1;
+        s->quality = 1;
+        s->combination = RT_COMBINE_POWER_HEURISTIC;
+        camera_settings c;
+        c.aspect_ratio = 16.0 / 9.0;
+        c.image_width = 1920;
+        c.samples_per_pixel = 256;
+        c.max_depth = 16;
+        c.sampling = RT_SAMPLING_MATERIAL;
+        c.vfov = 30;
+        c.lookfrom = v3(0, 2, 9);
+        c.lookat = v3(0, 1.1, 0);
+        rt_builtin_params q = p;
+        q.sampling = RT_SAMPLING_MATERIAL;
+        set_camera(*s, c, q, false);
     }
     else
     {

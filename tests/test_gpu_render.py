@@ -152,3 +152,44 @@ def test_counting_build_counts_fetches(rt):
     assert counts["nodes"] > rays  # every segment fetches at least the root
     assert counts["spheres"] > rays
     assert counts["quads"] == 0 and counts["triangles"] == 0
+
+
+def test_env_furnace_is_exactly_one(rt):
+    s = rt.builtin_scene("env-furnace", width=480, spp=64)
+    r = rt.render(s, seed=5)
+    assert np.all(r.pixels == 1.0), (r.pixels.min(), r.pixels.max())
+    assert r.kernel["name"] == "persistent nee-mis"
+
+
+def test_ggx_furnace_keeps_the_light(rt):
+    s = rt.builtin_scene("ggx-furnace", width=320, spp=256)
+    r = rt.render(s, seed=6)
+    h, w = s.height, s.width
+    centre = r.pixels[h // 2 - 3:h // 2 + 3, w // 2 - 3:w // 2 + 3].mean(axis=2).ravel()
+    se = centre.std(ddof=1) / np.sqrt(centre.size)
+    assert abs(centre.mean() - 1.0) < 0.005 + 4 * se, (centre.mean(), se)
+
+
+def test_mesh_first_hits_match_oracle(rt, oracle):
+    s = rt.builtin_scene("mesh-ggx", width=320, spp=16, mesh_level=5, env_width=256)
+    scene = rt.Scene(s)
+    assert scene.stats()["triangles"] == 20 * 4 ** 5
+    o, d = scene.camera_rays(seed=4, pass_index=3)
+    ids, ts = scene.closest_hits(o, d)
+    ref_ids, ref_ts = oracle.closest_hits(s.desc, o.astype(np.float64), d.astype(np.float64), brute_force=False)
+    same = ids == ref_ids
+    both_hit = (ids >= 0) & (ref_ids >= 0)
+    gap = np.where(both_hit, np.abs(np.where(both_hit, ts, 0) - np.where(both_hit, ref_ts, 0)), np.inf)
+    tie = ~same & both_hit & (gap <= 1e-5 * np.maximum(ref_ts, 1e-3))
+    assert np.count_nonzero(~same & ~tie) / ids.size <= 1e-4
+    assert np.allclose(ts[same & (ids >= 0)], ref_ts[same & (ids >= 0)], rtol=2e-4, atol=1e-5)
+
+
+def test_mesh_ggx_image_matches_oracle(rt, oracle):
+    """Config 3 reduced: the displaced icosphere (level 4), GGX metal, glossy-coat plane, the sun-lit sky sampled
+    by its alias table, NEE with power-heuristic MIS."""
+    r, g, cstats = _compare_with_rerun(rt, oracle, "mesh-ggx", 64, [(11, 12), (13, 14)], width=128, spp=64,
+                                       mesh_level=4, env_width=256)
+    assert g.shadow_rays > 0
+    per_sample = g.pixels[..., 0].size * 64
+    assert g.rays / per_sample == pytest.approx(cstats["rays"] / per_sample, rel=0.03)
