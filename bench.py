@@ -49,6 +49,12 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--extra", action="store_true", help="also measure the NEE/MIS integrator on the same scene")
+    p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
+    p.add_argument("--served", action="store_true", help="also measure the served request stream")
+    p.add_argument("--served-rate", type=float, default=200.0)
+    p.add_argument("--served-window", type=float, default=0.25, help="seconds of arrivals (a bounded sample)")
+    p.add_argument("--served-step", type=float, default=0.02, help="GPU seconds a server step aims at")
+    p.add_argument("--served-limit", type=float, default=300.0, help="wall seconds after which serving stops")
     return p.parse_args()
 
 
@@ -151,6 +157,162 @@ def cpu_baseline(scene, args, threads: int) -> dict:
     return {"value": value, "unit": UNIT, "cores": stats["threads"], "kind": "port",
             "sample": f"rows {begin}-{begin + rows - 1} of {scene.width}x{h} at {args.spp} spp "
                       f"({stats['rays']} segments in {stats['seconds']:.2f} s)"}
+
+
+def log_uniform(rng, lo: float, hi: float) -> float:
+    return float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+
+
+def batched_jobs(rt, count: int = 64, seed: int = 2024):
+    """The batched workload: `count` cover-scene variants, job j with seed j; W and H each log-uniform in
+    [64, 1024], spp log-uniform in [16, 1024] (whole passes), N log-uniform in [50, 2000] spheres."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for j in range(count):
+        w = int(round(log_uniform(rng, 64, 1024)))
+        h = int(round(log_uniform(rng, 64, 1024)))
+        spp = int(round(log_uniform(rng, 16, 1024)))
+        n = int(round(log_uniform(rng, 50, 2000)))
+        jobs.append((rt.builtin_scene(f"cover-{n}", width=w, height=h, spp=spp, scene_seed=j), j, spp))
+    return jobs
+
+
+def batched_measurement(rt, torch) -> dict:
+    """64 jobs in one batched render (one persistent launch per step, replayed as a CUDA graph) against the plain
+    form (one render per job), on the same jobs and seeds; every job's image compared bit for bit."""
+    jobs = batched_jobs(rt)
+    rt.batch_render(jobs[:4])  # warm-up (graph capture, module load)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b = rt.batch_render(jobs)
+    batch_wall = time.perf_counter() - t0
+    plain_kernel = 0.0
+    plain_wall = 0.0
+    plain_rays = 0
+    identical = 0
+    max_diff = 0.0
+    for (scene, seed, passes), img in zip(jobs, b.images):
+        t0 = time.perf_counter()
+        r = rt.render(scene, seed=seed, passes=passes)
+        plain_wall += time.perf_counter() - t0
+        plain_kernel += r.kernel_seconds
+        plain_rays += r.rays
+        identical += int(np.array_equal(r.pixels, img))
+        max_diff = max(max_diff, float(np.abs(r.pixels - img).max()))
+    pixels = sum(s.width * s.height for s, _, _ in jobs)
+    samples = sum(s.width * s.height * p for s, _, p in jobs)
+    return {"workload": "64 cover-scene variants (50-2000 spheres, W,H log-uniform 64-1024, spp log-uniform "
+                        "16-1024, seeds 0-63), mixture of sizes in one persistent launch per step",
+            "pixels": pixels, "samples": samples, "segments": b.rays,
+            "batched_segments_per_s": b.rays / b.gpu_seconds, "batched_gpu_s": b.gpu_seconds,
+            "batched_e2e_segments_per_s": b.rays / batch_wall, "batched_e2e_s": batch_wall,
+            "batched_setup_s": b.setup_seconds, "batched_steps": b.steps, "batched_launches": b.launches,
+            "graph": b.graph,
+            "plain_segments_per_s": plain_rays / plain_kernel, "plain_gpu_s": plain_kernel,
+            "plain_e2e_segments_per_s": plain_rays / plain_wall, "plain_e2e_s": plain_wall,
+            "speedup_gpu": (b.rays / b.gpu_seconds) / (plain_rays / plain_kernel),
+            "speedup_e2e": plain_wall / batch_wall,
+            "jobs_bit_identical_to_plain": f"{identical}/{len(jobs)}", "max_abs_difference": max_diff}
+
+
+SERVED_RESOLUTIONS = [((256, 256), 4), ((512, 512), 3), ((1920, 1080), 2), ((3840, 2160), 1)]
+SERVED_SCENES = ["weekend", "glass", "mesh-ggx"]
+
+
+def served_requests(rt, rate: float, window: float, seed: int = 7):
+    """The served stream: Poisson arrivals at `rate` per second over `window` seconds; each request a scene from
+    {cover (weekend), cornell glass, mesh+GGX} uniform, an orbit camera (azimuth U(0, 360), elevation U(5, 40)
+    degrees), a resolution from {256^2, 512^2, 1920x1080, 3840x2160} weighted 4:3:2:1, target spp log-uniform in
+    [1, 4096]."""
+    rng = np.random.default_rng(seed)
+    weights = np.array([w for _, w in SERVED_RESOLUTIONS], dtype=float)
+    out = []
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > window:
+            break
+        name = SERVED_SCENES[int(rng.integers(0, 3))]
+        (w, h) = SERVED_RESOLUTIONS[int(rng.choice(4, p=weights / weights.sum()))][0]
+        spp = max(1, int(round(log_uniform(rng, 1, 4096))))
+        orbit = (float(rng.uniform(0, 360)), float(rng.uniform(5, 40)))
+        cam = rt.builtin_camera(name, width=w, height=h, spp=spp, orbit=orbit)
+        out.append({"arrival": t, "scene": name, "camera": cam, "target": spp, "seed": len(out) + 1})
+    return out
+
+
+def served_measurement(rt, torch, args) -> dict:
+    """The served stream through the request server (batched steps, first frames first) against the plain form
+    (one render per request, FIFO, one at a time), on the same requests; the plain form's latencies follow from its
+    measured per-request GPU times and the arrival times (a single FIFO server)."""
+    requests = served_requests(rt, args.served_rate, args.served_window)
+    descs = {name: rt.builtin_scene(name) for name in SERVED_SCENES}
+    scenes = {name: rt.Scene(d) for name, d in descs.items()}
+    server = rt.Server(hbm_budget_bytes=120 << 30, step_seconds=args.served_step)
+    pending = list(range(len(requests)))
+    ids = {}
+    start = time.perf_counter()
+    submitted = {}
+    limit = args.served_limit
+    while True:
+        now = time.perf_counter() - start
+        while pending and requests[pending[0]]["arrival"] <= now:
+            i = pending.pop(0)
+            q = requests[i]
+            ids[i] = server.submit(scenes[q["scene"]], q["camera"], q["seed"], q["target"])
+            submitted[i] = time.perf_counter() - start
+        if len(ids) == len(requests) and all(server.poll(r)["state"] == "done" for r in ids.values()):
+            break
+        if now > limit:
+            break
+        rep = server.step()
+        if rep["active"] == 0 and rep["queued"] == 0 and pending:
+            time.sleep(max(0.0, requests[pending[0]]["arrival"] - (time.perf_counter() - start)))
+    wall = time.perf_counter() - start
+    ttff, ttt = [], []
+    for i, rid in ids.items():
+        st = server.poll(rid)
+        lag = submitted[i] - requests[i]["arrival"]
+        if st["first_frame_seconds"] >= 0:
+            ttff.append(lag + st["first_frame_seconds"])
+        if st["done_seconds"] >= 0:
+            ttt.append(lag + st["done_seconds"])
+    stats = server.stats()
+    server.close()
+
+    # The plain form: one session render per request on the resident scene, timed on the GPU, then FIFO queueing
+    service = []
+    plain_rays = 0
+    for q in requests:
+        sess = rt.Session(scenes[q["scene"]], seed=q["seed"], launch_seconds=0.05)
+        sess.set_camera(q["camera"])
+        rep = sess.render_to(q["target"])
+        sess.pixels()
+        plain_rays += sess.counters()["rays"]
+        service.append(rep["gpu_seconds"])
+        sess.close()
+    finish = 0.0
+    plain_latency = []
+    for q, s in zip(requests, service):
+        finish = max(finish, q["arrival"]) + s
+        plain_latency.append(finish - q["arrival"])
+
+    def pct(v, p):
+        return float(np.percentile(v, p)) if v else None
+
+    return {"workload": f"Poisson arrivals at {args.served_rate}/s over {args.served_window} s "
+                        f"({len(requests)} requests), scenes cover/glass/mesh-ggx, orbit cameras, 256^2..3840x2160 "
+                        f"4:3:2:1, target spp log-uniform 1-4096, HBM budget 120 GB",
+            "requests": len(requests), "completed": len(ttt), "first_frames": len(ttff), "wall_s": wall,
+            "ttff_p50_s": pct(ttff, 50), "ttff_p99_s": pct(ttff, 99),
+            "time_to_target_p50_s": pct(ttt, 50), "time_to_target_p99_s": pct(ttt, 99),
+            "served_segments_per_s": stats["rays"] / stats["gpu_seconds"] if stats["gpu_seconds"] else None,
+            "served_steps": stats["steps"], "served_launches": stats["launches"],
+            "plain_ttff_p50_s": pct(plain_latency, 50), "plain_ttff_p99_s": pct(plain_latency, 99),
+            "plain_time_to_target_p50_s": pct(plain_latency, 50),
+            "plain_time_to_target_p99_s": pct(plain_latency, 99),
+            "plain_segments_per_s": plain_rays / sum(service) if service else None,
+            "plain_note": "one render per request (a session on the resident scene), FIFO, first frame = final image"}
 
 
 def run_reference(args):
@@ -354,6 +516,11 @@ def run_b200(args):
             "shadow_rays_per_sample": cnt["shadow_rays"] / (passes * mis.width * mis.height),
             "wall_s": time.perf_counter() - t0}}
         mis.close()
+
+    if rank == 0 and not args.no_batched:
+        line["batched"] = batched_measurement(rt, torch)
+    if rank == 0 and args.served:
+        line["served"] = served_measurement(rt, torch, args)
 
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene_desc, args, os.cpu_count() or 1)

@@ -348,6 +348,100 @@ rt_status rt_session_device_sums(const rt_session* session, const double** sums,
 rt_status rt_session_set_counting(rt_session* session, int32_t on);
 rt_status rt_session_fetch_counts(const rt_session* session, uint64_t counts[4]);
 
+/* ---- batched rendering and serving (no counterpart in the reference: one session renders one view, renderer.h:
+ * 585-590; here many requests share one persistent launch per refinement step) --------------------------------- */
+
+/* One job of a batch: a scene (validated and built for the batch), the seed and passes it renders, and where its
+ * image goes (width*height*3 doubles, host memory, rows from the top). */
+typedef struct rt_batch_job
+{
+    const rt_scene_desc* scene;
+    uint64_t seed;
+    int64_t passes;             /* 0: sqrt_spp^2 */
+    double* pixels;
+} rt_batch_job;
+
+typedef struct rt_batch_options
+{
+    int64_t partial_budget_bytes; /* the partials arena a step may use; 0: 1 GiB */
+    int32_t use_graph;          /* capture the step into a CUDA graph and replay it */
+    int32_t pad0;
+} rt_batch_options;
+
+typedef struct rt_batch_report
+{
+    double seconds;             /* the whole call */
+    double setup_seconds;       /* validation, BVH builds and uploads of the jobs' scenes */
+    double gpu_seconds;         /* the steps' launches, timed on the GPU */
+    uint64_t rays;
+    uint64_t shadow_rays;
+    int32_t steps;
+    int32_t launches;
+    int32_t graph;              /* the steps ran as a captured graph */
+    int32_t pad0;
+} rt_batch_report;
+
+/* Renders every job to its passes in batched steps (config 4's 64 jobs in one persistent launch per step). */
+rt_status rt_batch_render(const rt_batch_job* jobs, int32_t count, const rt_batch_options* options,
+                          rt_batch_report* report);
+
+typedef struct rt_server rt_server;
+
+typedef struct rt_server_options
+{
+    int64_t hbm_budget_bytes;   /* what the admitted requests' sums and the step's partials may hold */
+    double step_seconds;        /* the GPU time a refinement step aims at */
+    int32_t use_graph;
+    int32_t pad0;
+} rt_server_options;
+
+enum { RT_REQUEST_QUEUED = 0, RT_REQUEST_ACTIVE = 1, RT_REQUEST_DONE = 2, RT_REQUEST_CANCELLED = 3 };
+
+typedef struct rt_request_status
+{
+    int32_t state;              /* RT_REQUEST_* */
+    int32_t pad0;
+    int64_t passes;             /* complete passes so far */
+    int64_t target;
+    double first_frame_seconds; /* from submit to the end of its first pass; < 0 until then */
+    double done_seconds;        /* from submit to its target; < 0 until then */
+} rt_request_status;
+
+typedef struct rt_server_step_report
+{
+    double gpu_seconds;
+    int32_t admitted;           /* requests admitted this step */
+    int32_t first_frames;       /* requests that got their first pass */
+    int32_t refined;            /* requests that got more passes */
+    int32_t completed;
+    int32_t active;
+    int32_t queued;
+} rt_server_step_report;
+
+typedef struct rt_server_stats
+{
+    uint64_t rays;
+    uint64_t shadow_rays;
+    double gpu_seconds;
+    int64_t steps;
+    int64_t launches;
+    int64_t completed;
+    int64_t used_bytes;
+} rt_server_stats;
+
+rt_status rt_server_create(const rt_server_options* options, rt_server** server);
+rt_status rt_server_destroy(rt_server* server);
+/* Queues a request: a view of a resident scene (the scene must outlive the request), its seed and target passes. */
+rt_status rt_server_submit(rt_server* server, rt_scene* scene, const rt_camera_desc* camera, uint64_t seed,
+                           int64_t target_passes, int64_t* request_id);
+/* One refinement step: admit what the budget allows, first frames first, then refinement; synchronous. */
+rt_status rt_server_step(rt_server* server, rt_server_step_report* report);
+rt_status rt_server_poll(const rt_server* server, int64_t request_id, rt_request_status* status);
+/* The request's image so far (sums / passes); frees a finished request's device memory. */
+rt_status rt_server_fetch(rt_server* server, int64_t request_id, double* pixels, int64_t pixel_count);
+rt_status rt_server_cancel(rt_server* server, int64_t request_id);
+rt_status rt_server_stats_get(const rt_server* server, rt_server_stats* stats);
+
 /* ---- parity hooks (no counterpart in the reference's API: its GpuTests call device functions directly) ------ */
 
 /* Closest-hit queries for given rays on the device: the first hit's primitive in SOURCE index space (spheres
@@ -391,6 +485,8 @@ typedef struct rt_owned_scene rt_owned_scene;
 rt_status rt_builtin_scene(const char* name, const rt_builtin_params* params, rt_owned_scene** scene);
 const rt_scene_desc* rt_owned_scene_desc(const rt_owned_scene* scene);
 rt_status rt_owned_scene_destroy(rt_owned_scene* scene);
+/* The camera of a built-in scene with the given overrides (an orbit, a size), its geometry built at its cheapest. */
+rt_status rt_builtin_camera(const char* name, const rt_builtin_params* params, rt_camera_desc* camera);
 /* A scene serialized once and fed to every renderer (the oracle, the reference build, this one). */
 rt_status rt_scene_save(const rt_scene_desc* scene, const char* path);
 rt_status rt_scene_load(const char* path, rt_owned_scene** scene);

@@ -20,8 +20,8 @@ from ._abi import (RT_COMBINE_BSDF_ONLY, RT_COMBINE_LIGHTS_ONLY, RT_COMBINE_POWE
                    RT_SAMPLING_MATERIAL, RT_SAMPLING_MIXTURE, RT_SAMPLING_UNIFORM)
 
 __all__ = ["RenderError", "LogicError", "NoDeviceError", "UnsupportedError", "CapacityError", "OwnedScene",
-           "builtin_scene", "load_scene", "query_device", "render", "Scene", "Session", "RenderResult",
-           "SAMPLING", "COMBINATION", "library_path"]
+           "builtin_scene", "builtin_camera", "load_scene", "query_device", "render", "Scene", "Session",
+           "RenderResult", "batch_render", "BatchResult", "Server", "SAMPLING", "COMBINATION", "library_path"]
 
 SAMPLING = {"uniform": RT_SAMPLING_UNIFORM, "material": RT_SAMPLING_MATERIAL, "lights": RT_SAMPLING_LIGHTS,
             "mixture": RT_SAMPLING_MIXTURE}
@@ -119,12 +119,10 @@ class OwnedScene:
             pass
 
 
-def builtin_scene(name: str, width: int = 0, height: int = 0, spp: int = 0, depth: int = 0,
-                  sampling: Optional[str] = None, combination: Optional[str] = None, scene_seed: int = 0,
-                  sphere_count: int = 0, mesh_level: int = 0, env_width: int = 0,
-                  orbit: Optional[tuple[float, float]] = None) -> OwnedScene:
-    """A scene the library builds by name ("weekend", "cornell", "glass", "cornell-mis", "materials", "quads",
-    "furnace", "cover-N"): the reference's scene code, flattened as its GPU translator flattens it."""
+def _builtin_params(width: int = 0, height: int = 0, spp: int = 0, depth: int = 0,
+                    sampling: Optional[str] = None, combination: Optional[str] = None, scene_seed: int = 0,
+                    sphere_count: int = 0, mesh_level: int = 0, env_width: int = 0,
+                    orbit: Optional[tuple[float, float]] = None) -> _abi.BuiltinParams:
     p = _abi.BuiltinParams()
     p.image_width = width
     p.image_height = height
@@ -139,9 +137,26 @@ def builtin_scene(name: str, width: int = 0, height: int = 0, spp: int = 0, dept
     if orbit is not None:
         p.orbit = 1
         p.orbit_azimuth, p.orbit_elevation = orbit
+    return p
+
+
+def builtin_scene(name: str, **overrides) -> OwnedScene:
+    """A scene the library builds by name ("weekend", "cornell", "glass", "cornell-mis", "materials", "quads",
+    "furnace", "env-furnace", "ggx-furnace", "mesh-ggx", "cover-N"): the reference's scene code, flattened as its GPU
+    translator flattens it. Overrides: width, height, spp, depth, sampling, combination, scene_seed, sphere_count,
+    mesh_level, env_width, orbit=(azimuth, elevation) in degrees."""
+    p = _builtin_params(**overrides)
     handle = C.c_void_p()
     _check(_lib().rt_builtin_scene(name.encode(), C.byref(p), C.byref(handle)))
     return OwnedScene(handle)
+
+
+def builtin_camera(name: str, **overrides) -> _abi.CameraDesc:
+    """The camera builtin_scene(name, **overrides) would have, without building the scene's geometry."""
+    p = _builtin_params(**overrides)
+    cam = _abi.CameraDesc()
+    _check(_lib().rt_builtin_camera(name.encode(), C.byref(p), C.byref(cam)))
+    return cam
 
 
 def load_scene(path: str) -> OwnedScene:
@@ -323,6 +338,102 @@ class Session:
         if self._handle:
             _lib().rt_session_destroy(self._handle)
             self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class BatchResult:
+    """What one batched render of many jobs returns: each job's image (height x width x 3, rows from the top)."""
+    images: list
+    seconds: float
+    setup_seconds: float
+    gpu_seconds: float
+    rays: int
+    shadow_rays: int
+    steps: int
+    launches: int
+    graph: bool
+
+
+def batch_render(jobs: list, partial_budget_bytes: int = 0, use_graph: bool = True) -> BatchResult:
+    """Renders many jobs together, one persistent launch per step over every job's work items. jobs: a list of
+    (scene, seed, passes) with scene an OwnedScene or a SceneDesc pointer and passes 0 for the camera's sqrt_spp^2."""
+    n = len(jobs)
+    table = (_abi.BatchJob * max(n, 1))()
+    images = []
+    for i, (scene, seed, passes) in enumerate(jobs):
+        desc = _desc_of(scene)
+        cam = desc.contents.camera
+        img = np.zeros((int(cam.image_height), int(cam.image_width), 3), dtype=np.float64)
+        images.append(img)
+        table[i] = _abi.BatchJob(desc, seed, passes, img.ctypes.data_as(C.POINTER(C.c_double)))
+    o = _abi.BatchOptions(partial_budget_bytes=partial_budget_bytes, use_graph=1 if use_graph else 0)
+    r = _abi.BatchReport()
+    _check(_lib().rt_batch_render(table, n, C.byref(o), C.byref(r)))
+    return BatchResult(images, r.seconds, r.setup_seconds, r.gpu_seconds, r.rays, r.shadow_rays, r.steps,
+                       r.launches, bool(r.graph))
+
+
+REQUEST_STATES = {0: "queued", 1: "active", 2: "done", 3: "cancelled"}
+
+
+class Server:
+    """A stream of render requests served in batched steps: admission under an HBM budget, a first frame (one pass)
+    for every newly admitted request before refinement, each request done at its target passes."""
+
+    def __init__(self, hbm_budget_bytes: int = 8 << 30, step_seconds: float = 0.02, use_graph: bool = True):
+        o = _abi.ServerOptions(hbm_budget_bytes=hbm_budget_bytes, step_seconds=step_seconds,
+                               use_graph=1 if use_graph else 0)
+        handle = C.c_void_p()
+        _check(_lib().rt_server_create(C.byref(o), C.byref(handle)))
+        self._handle = handle
+        self._scenes = {}  # request id -> (Scene, camera), kept alive while the request is
+
+    def submit(self, scene: Scene, camera: _abi.CameraDesc, seed: int, target_passes: int) -> int:
+        rid = C.c_int64()
+        _check(_lib().rt_server_submit(self._handle, scene._handle, C.byref(camera), seed, target_passes,
+                                       C.byref(rid)))
+        self._scenes[rid.value] = (scene, camera)
+        return rid.value
+
+    def step(self) -> dict:
+        r = _abi.ServerStepReport()
+        _check(_lib().rt_server_step(self._handle, C.byref(r)))
+        return {name: getattr(r, name) for name, _ in _abi.ServerStepReport._fields_}
+
+    def poll(self, request_id: int) -> dict:
+        s = _abi.RequestStatus()
+        _check(_lib().rt_server_poll(self._handle, request_id, C.byref(s)))
+        return {"state": REQUEST_STATES[s.state], "passes": s.passes, "target": s.target,
+                "first_frame_seconds": s.first_frame_seconds, "done_seconds": s.done_seconds}
+
+    def fetch(self, request_id: int) -> np.ndarray:
+        cam = self._scenes[request_id][1]
+        px = np.empty((int(cam.image_height), int(cam.image_width), 3), dtype=np.float64)
+        _check(_lib().rt_server_fetch(self._handle, request_id, px.ctypes.data_as(C.POINTER(C.c_double)), px.size))
+        if self.poll(request_id)["state"] == "done":
+            self._scenes.pop(request_id, None)
+        return px
+
+    def cancel(self, request_id: int) -> None:
+        _check(_lib().rt_server_cancel(self._handle, request_id))
+        self._scenes.pop(request_id, None)
+
+    def stats(self) -> dict:
+        s = _abi.ServerStats()
+        _check(_lib().rt_server_stats_get(self._handle, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in _abi.ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._handle:
+            _lib().rt_server_destroy(self._handle)
+            self._handle = None
+        self._scenes.clear()
 
     def __del__(self):
         try:

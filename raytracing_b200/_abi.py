@@ -150,6 +150,41 @@ class BuiltinParams(C.Structure):
                 ("orbit_elevation", C.c_double), ("orbit", C.c_int32), ("pad1", C.c_int32)]
 
 
+class BatchJob(C.Structure):
+    _fields_ = [("scene", C.POINTER(SceneDesc)), ("seed", C.c_uint64), ("passes", C.c_int64),
+                ("pixels", C.POINTER(C.c_double))]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("partial_budget_bytes", C.c_int64), ("use_graph", C.c_int32), ("pad0", C.c_int32)]
+
+
+class BatchReport(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("setup_seconds", C.c_double), ("gpu_seconds", C.c_double),
+                ("rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("steps", C.c_int32), ("launches", C.c_int32),
+                ("graph", C.c_int32), ("pad0", C.c_int32)]
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("step_seconds", C.c_double), ("use_graph", C.c_int32),
+                ("pad0", C.c_int32)]
+
+
+class RequestStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("pad0", C.c_int32), ("passes", C.c_int64), ("target", C.c_int64),
+                ("first_frame_seconds", C.c_double), ("done_seconds", C.c_double)]
+
+
+class ServerStepReport(C.Structure):
+    _fields_ = [("gpu_seconds", C.c_double), ("admitted", C.c_int32), ("first_frames", C.c_int32),
+                ("refined", C.c_int32), ("completed", C.c_int32), ("active", C.c_int32), ("queued", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("gpu_seconds", C.c_double),
+                ("steps", C.c_int64), ("launches", C.c_int64), ("completed", C.c_int64), ("used_bytes", C.c_int64)]
+
+
 # (name, restype, argtypes) of every entry point declared in include/rt_b200.h
 ENTRY_POINTS = [
     ("rt_last_error_message", C.c_char_p, []),
@@ -187,6 +222,17 @@ ENTRY_POINTS = [
     ("rt_owned_scene_destroy", C.c_int, [C.c_void_p]),
     ("rt_scene_save", C.c_int, [C.POINTER(SceneDesc), C.c_char_p]),
     ("rt_scene_load", C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    ("rt_builtin_camera", C.c_int, [C.c_char_p, C.POINTER(BuiltinParams), C.POINTER(CameraDesc)]),
+    ("rt_batch_render", C.c_int, [C.POINTER(BatchJob), C.c_int32, C.POINTER(BatchOptions), C.POINTER(BatchReport)]),
+    ("rt_server_create", C.c_int, [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    ("rt_server_destroy", C.c_int, [C.c_void_p]),
+    ("rt_server_submit", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(CameraDesc), C.c_uint64, C.c_int64,
+                                   C.POINTER(C.c_int64)]),
+    ("rt_server_step", C.c_int, [C.c_void_p, C.POINTER(ServerStepReport)]),
+    ("rt_server_poll", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(RequestStatus)]),
+    ("rt_server_fetch", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_double), C.c_int64]),
+    ("rt_server_cancel", C.c_int, [C.c_void_p, C.c_int64]),
+    ("rt_server_stats_get", C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
 ]
 
 _lib = None

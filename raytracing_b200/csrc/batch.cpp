@@ -1,0 +1,765 @@
+// Batched rendering and serving: the batch engine (a job table, a partials arena and a captured CUDA graph of the
+// step), rt_batch_render on top of it (config 4: many independent jobs in one persistent launch per step), and the
+// render server (config 5: a stream of requests admitted under an HBM budget, first frames before refinement).
+#include "batch.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "scene_store.h"
+
+namespace rtb
+{
+namespace
+{
+constexpr size_t default_partial_budget = size_t{1} << 30;
+} // namespace
+
+// ---- the batch engine ---------------------------------------------------------------------------------------
+
+batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
+    : use_graph_(use_graph),
+      max_partial_entries_(static_cast<int64_t>((partial_budget_bytes > 0 ? partial_budget_bytes : default_partial_budget) /
+                                                (3 * sizeof(double))))
+{
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a CUDA stream");
+    check(cudaEventCreate(&start_), "creating a CUDA event");
+    check(cudaEventCreate(&stop_), "creating a CUDA event");
+    kernel_attributes a{};
+    check(batch_attributes(a), "querying the batch kernel");
+    grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
+    work_counter_.allocate(1);
+    header_.allocate(1);
+    check(cudaMallocHost(reinterpret_cast<void**>(&header_host_), sizeof(batch_header)), "allocating pinned memory");
+}
+
+batch_engine::~batch_engine()
+{
+    release_graph();
+    if (table_host_)
+    {
+        cudaFreeHost(table_host_);
+    }
+    if (header_host_)
+    {
+        cudaFreeHost(header_host_);
+    }
+    if (start_)
+    {
+        cudaEventDestroy(start_);
+    }
+    if (stop_)
+    {
+        cudaEventDestroy(stop_);
+    }
+    if (stream_)
+    {
+        cudaStreamDestroy(stream_);
+    }
+}
+
+int64_t batch_engine::chunks_of(int64_t passes, int64_t pass_end)
+{
+    return (pass_end + pass_chunk - 1) / pass_chunk - passes / pass_chunk;
+}
+
+int64_t batch_engine::padded_of(const rt_camera_desc& camera)
+{
+    return int64_t{(camera.image_width + 7) / 8} * ((camera.image_height + 3) / 4) * 32;
+}
+
+size_t batch_engine::job_bytes(const rt_camera_desc& camera) const
+{
+    return static_cast<size_t>(camera.image_width) * static_cast<size_t>(camera.image_height) * 3 * sizeof(double) +
+           2 * sizeof(unsigned long long);
+}
+
+int batch_engine::add(std::shared_ptr<resident_scene> scene, const rt_camera_desc& camera, uint64_t seed,
+                      uint32_t job_id)
+{
+    if (camera.sampling != scene->camera().sampling)
+    {
+        fail(RT_ERR_INVALID, "a request must keep its scene's sampling strategy");
+    }
+    rt_scene_desc probe{};
+    probe.camera = camera;
+    probe.light_count = camera.sampling == RT_SAMPLING_LIGHTS || camera.sampling == RT_SAMPLING_MIXTURE ? 1 : 0;
+    rt_light_desc dummy{};
+    dummy.kind = RT_LIGHT_QUAD;
+    probe.lights = &dummy;
+    validate(probe);
+    auto j = std::make_unique<job>();
+    j->scene = std::move(scene);
+    j->camera = camera;
+    j->cam = to_camera(camera);
+    j->seed = seed;
+    j->id = job_id;
+    j->tiles_x = (camera.image_width + 7) / 8;
+    j->padded = static_cast<int>(padded_of(camera));
+    j->sums.allocate(static_cast<size_t>(camera.image_width) * camera.image_height * 3);
+    j->counters.allocate(2);
+    check(cudaMemsetAsync(j->sums.data(), 0, j->sums.bytes(), stream_), "clearing the sums");
+    check(cudaMemsetAsync(j->counters.data(), 0, j->counters.bytes(), stream_), "clearing the counters");
+    const int handle = next_handle_++;
+    jobs_[handle] = std::move(j);
+    return handle;
+}
+
+void batch_engine::remove(int handle)
+{
+    check(cudaStreamSynchronize(stream_), "finishing the batch's work");
+    jobs_.erase(handle);
+}
+
+void batch_engine::release_graph()
+{
+    if (graph_exec_)
+    {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+    }
+    if (graph_)
+    {
+        cudaGraphDestroy(graph_);
+        graph_ = nullptr;
+    }
+}
+
+void batch_engine::ensure_capacity(size_t jobs, size_t partial_doubles)
+{
+    bool moved = false;
+    if (jobs > capacity_)
+    {
+        size_t capacity = 64;
+        while (capacity < jobs)
+        {
+            capacity *= 2;
+        }
+        table_.allocate(capacity);
+        if (table_host_)
+        {
+            cudaFreeHost(table_host_);
+            table_host_ = nullptr;
+        }
+        check(cudaMallocHost(reinterpret_cast<void**>(&table_host_), capacity * sizeof(batch_job)),
+              "allocating pinned memory");
+        capacity_ = capacity;
+        moved = true;
+    }
+    if (partial_doubles > arena_.size())
+    {
+        arena_.allocate(partial_doubles + partial_doubles / 4);
+        moved = true;
+    }
+    if (moved)
+    {
+        release_graph(); // the graph's copies and kernels point at the old buffers
+    }
+}
+
+// The step as a graph: the job table and header copied from pinned memory, the work counter cleared, the persistent
+// kernel and the reduction. Replayed as is; only the pinned tables' contents change between steps.
+void batch_engine::capture()
+{
+    batch_params p{table_.data(), header_.data(), work_counter_.data()};
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capturing the batch step");
+    cudaMemcpyAsync(table_.data(), table_host_, capacity_ * sizeof(batch_job), cudaMemcpyHostToDevice, stream_);
+    cudaMemcpyAsync(header_.data(), header_host_, sizeof(batch_header), cudaMemcpyHostToDevice, stream_);
+    cudaMemsetAsync(work_counter_.data(), 0, sizeof(unsigned long long), stream_);
+    const cudaError_t launched = launch_batch(p, grid_, stream_);
+    const cudaError_t ended = cudaStreamEndCapture(stream_, &graph_);
+    check(launched, "capturing the batch kernels");
+    check(ended, "capturing the batch step");
+    check(cudaGraphInstantiate(&graph_exec_, graph_, 0), "instantiating the batch step's graph");
+}
+
+double batch_engine::step(std::vector<assignment> work)
+{
+    // A path of no rays: every sample is 0, the job needs no launch (as a session's render_to)
+    for (assignment& a : work)
+    {
+        job& j = *jobs_.at(a.handle);
+        if (j.camera.max_depth == 0 && a.pass_end > j.passes)
+        {
+            j.passes = a.pass_end;
+        }
+    }
+    // Fit the partials arena: each job its chunks, cut back while the total is over budget (at least one chunk each)
+    work.erase(std::remove_if(work.begin(), work.end(),
+                              [&](const assignment& a) { return a.pass_end <= jobs_.at(a.handle)->passes; }),
+               work.end());
+    int64_t entries = 0;
+    for (const assignment& a : work)
+    {
+        const job& j = *jobs_.at(a.handle);
+        entries += chunks_of(j.passes, a.pass_end) * j.padded;
+    }
+    while (entries > max_partial_entries_)
+    {
+        bool cut = false;
+        for (assignment& a : work)
+        {
+            const job& j = *jobs_.at(a.handle);
+            const int64_t chunks = chunks_of(j.passes, a.pass_end);
+            if (chunks > 1 && entries > max_partial_entries_)
+            {
+                const int64_t keep = std::max<int64_t>(1, chunks / 2);
+                const int64_t end = (j.passes / pass_chunk + keep) * pass_chunk;
+                entries -= (chunks - chunks_of(j.passes, end)) * j.padded;
+                a.pass_end = end;
+                cut = true;
+            }
+        }
+        if (!cut)
+        {
+            break; // one chunk per job: let it run over, the arena grows
+        }
+    }
+    if (work.empty())
+    {
+        return 0;
+    }
+    ensure_capacity(work.size(), static_cast<size_t>(entries) * 3);
+    last_samples_ = 0;
+    int64_t items = 0;
+    int64_t pixels = 0;
+    int64_t partial_offset = 0;
+    for (size_t i = 0; i < work.size(); ++i)
+    {
+        job& j = *jobs_.at(work[i].handle);
+        batch_job& b = table_host_[i];
+        b = batch_job{};
+        b.scene = j.scene->view();
+        b.cam = j.cam;
+        b.seed = j.seed;
+        b.pass_begin = j.passes;
+        b.pass_end = work[i].pass_end;
+        b.first_chunk = j.passes / pass_chunk;
+        b.chunk = pass_chunk;
+        b.chunks = static_cast<int32_t>(chunks_of(j.passes, work[i].pass_end));
+        b.tiles_x = j.tiles_x;
+        b.padded_pixels = j.padded;
+        b.round_passes = j.camera.sqrt_spp * j.camera.sqrt_spp;
+        b.quality = j.scene->quality() ? 1 : 0;
+        b.job = j.id;
+        b.item_begin = items;
+        b.pixel_begin = pixels;
+        b.partials = arena_.data() + 3 * partial_offset;
+        b.sums = j.sums.data();
+        b.counters = j.counters.data();
+        items += int64_t{b.chunks} * b.padded_pixels;
+        pixels += int64_t{j.camera.image_width} * j.camera.image_height;
+        last_samples_ += int64_t{j.camera.image_width} * j.camera.image_height * (b.pass_end - b.pass_begin);
+        partial_offset += int64_t{b.chunks} * b.padded_pixels;
+    }
+    header_host_->total_items = items;
+    header_host_->total_pixels = pixels;
+    header_host_->job_count = static_cast<int32_t>(work.size());
+    check(cudaEventRecord(start_, stream_), "recording a CUDA event");
+    if (use_graph_)
+    {
+        if (!graph_exec_)
+        {
+            capture();
+        }
+        check(cudaGraphLaunch(graph_exec_, stream_), "launching the batch step's graph");
+    }
+    else
+    {
+        check(cudaMemcpyAsync(table_.data(), table_host_, work.size() * sizeof(batch_job), cudaMemcpyHostToDevice,
+                              stream_),
+              "copying the job table");
+        check(cudaMemcpyAsync(header_.data(), header_host_, sizeof(batch_header), cudaMemcpyHostToDevice, stream_),
+              "copying the batch header");
+        check(cudaMemsetAsync(work_counter_.data(), 0, sizeof(unsigned long long), stream_), "clearing the counter");
+        check(launch_batch(batch_params{table_.data(), header_.data(), work_counter_.data()}, grid_, stream_),
+              "launching the batch kernels");
+    }
+    check(cudaEventRecord(stop_, stream_), "recording a CUDA event");
+    check(cudaEventSynchronize(stop_), "rendering the batch on the GPU");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, start_, stop_), "timing the GPU");
+    launches_ += 2;
+    for (const assignment& a : work)
+    {
+        jobs_.at(a.handle)->passes = a.pass_end;
+    }
+    return ms / 1000.0;
+}
+
+int64_t batch_engine::passes(int handle) const { return jobs_.at(handle)->passes; }
+
+void batch_engine::pixels(int handle, double* out, int64_t count)
+{
+    job& j = *jobs_.at(handle);
+    const int64_t n = int64_t{j.camera.image_width} * j.camera.image_height * 3;
+    if (count != n)
+    {
+        fail(RT_ERR_INVALID, "pixels: the buffer must hold width * height * 3 doubles");
+    }
+    if (j.passes == 0)
+    {
+        fail(RT_ERR_LOGIC, "pixels: the image has no complete pass");
+    }
+    check(cudaMemcpyAsync(out, j.sums.data(), static_cast<size_t>(n) * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+          "copying the image");
+    check(cudaStreamSynchronize(stream_), "copying the image");
+    const double scale = 1.0 / static_cast<double>(j.passes);
+    for (int64_t i = 0; i < n; ++i)
+    {
+        out[i] *= scale;
+    }
+}
+
+uint64_t batch_engine::rays(int handle) const
+{
+    unsigned long long v = 0;
+    check(cudaMemcpy(&v, jobs_.at(handle)->counters.data(), sizeof(v), cudaMemcpyDeviceToHost), "reading counts");
+    return v;
+}
+
+uint64_t batch_engine::shadow_rays(int handle) const
+{
+    unsigned long long v = 0;
+    check(cudaMemcpy(&v, jobs_.at(handle)->counters.data() + 1, sizeof(v), cudaMemcpyDeviceToHost), "reading counts");
+    return v;
+}
+
+// ---- the render server --------------------------------------------------------------------------------------
+
+render_server::render_server(const rt_server_options& options)
+    : options_(options),
+      engine_(options.hbm_budget_bytes > 0 ? std::min<size_t>(default_partial_budget,
+                                                              static_cast<size_t>(options.hbm_budget_bytes) / 4)
+                                           : default_partial_budget,
+              options.use_graph != 0)
+{
+    if (!(options_.step_seconds > 0 && options_.step_seconds <= 1))
+    {
+        fail(RT_ERR_INVALID, "step_seconds must be in (0, 1]");
+    }
+    if (options_.hbm_budget_bytes <= 0)
+    {
+        fail(RT_ERR_INVALID, "hbm_budget_bytes must be positive");
+    }
+}
+
+int64_t render_server::submit(std::shared_ptr<resident_scene> scene, const rt_camera_desc& camera, uint64_t seed,
+                              int64_t target)
+{
+    if (target < 1)
+    {
+        fail(RT_ERR_INVALID, "a request needs at least one pass");
+    }
+    request r{};
+    r.id = next_id_++;
+    r.scene = std::move(scene);
+    r.camera = camera;
+    r.seed = seed;
+    r.target = target;
+    r.submitted = clock::now();
+    r.bytes = engine_.job_bytes(camera);
+    if (static_cast<int64_t>(r.bytes) > options_.hbm_budget_bytes)
+    {
+        fail(RT_ERR_CAPACITY, "the request's image alone exceeds the HBM budget");
+    }
+    queue_.push_back(r.id);
+    requests_.emplace(r.id, std::move(r));
+    return next_id_ - 1;
+}
+
+rt_server_step_report render_server::step()
+{
+    rt_server_step_report report{};
+    // Admission, in arrival order, while the budget holds (a request waits rather than overtake an earlier one)
+    while (!queue_.empty())
+    {
+        request& r = requests_.at(queue_.front());
+        if (used_bytes_ + r.bytes > static_cast<size_t>(options_.hbm_budget_bytes))
+        {
+            break;
+        }
+        // RNG job field 0: a request's image depends on its scene, camera, seed and passes only, so it equals a
+        // session's render of the same view and seed
+        r.handle = engine_.add(r.scene, r.camera, r.seed, 0);
+        r.state = RT_REQUEST_ACTIVE;
+        used_bytes_ += r.bytes;
+        queue_.pop_front();
+        ++report.admitted;
+    }
+    // First frames: every active request without a pass gets one, whatever the step's budget
+    std::vector<batch_engine::assignment> work;
+    double planned = 0;
+    const double rate = samples_per_second_ > 0 ? samples_per_second_ : 1e9;
+    for (auto& [id, r] : requests_)
+    {
+        if (r.state == RT_REQUEST_ACTIVE && engine_.passes(r.handle) == 0)
+        {
+            work.push_back({r.handle, 1});
+            planned += double(r.camera.image_width) * r.camera.image_height / rate;
+            ++report.first_frames;
+        }
+    }
+    // Refinement: the others, least remaining work first (shortest remaining processing time, which minimises the
+    // mean time to target), while the step's time allows
+    std::vector<std::pair<double, request*>> refine;
+    for (auto& [id, r] : requests_)
+    {
+        if (r.state != RT_REQUEST_ACTIVE)
+        {
+            continue;
+        }
+        const int64_t done = engine_.passes(r.handle);
+        if (done > 0 && done < r.target)
+        {
+            refine.emplace_back(double(r.camera.image_width) * r.camera.image_height * double(r.target - done), &r);
+        }
+    }
+    std::stable_sort(refine.begin(), refine.end(),
+                     [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (auto& [remaining, rp] : refine)
+    {
+        request& r = *rp;
+        const int64_t done = engine_.passes(r.handle);
+        if (planned >= options_.step_seconds)
+        {
+            break;
+        }
+        const double per_pass = double(r.camera.image_width) * r.camera.image_height / rate;
+        const int64_t want = std::max<int64_t>(1, static_cast<int64_t>((options_.step_seconds - planned) / per_pass));
+        int64_t end = std::min(r.target, done + want);
+        // finish the chunk the request is in, or stop on a chunk boundary
+        const int64_t boundary = (done / pass_chunk + 1) * pass_chunk;
+        end = std::min(r.target, std::max(std::min(end, boundary), end / pass_chunk * pass_chunk));
+        if (end <= done)
+        {
+            end = std::min(r.target, boundary);
+        }
+        work.push_back({r.handle, end});
+        planned += per_pass * double(end - done);
+        ++report.refined;
+    }
+    if (!work.empty())
+    {
+        report.gpu_seconds = engine_.step(std::move(work));
+        if (report.gpu_seconds > 0)
+        {
+            const double measured = double(engine_.last_samples()) / report.gpu_seconds;
+            samples_per_second_ = samples_per_second_ > 0 ? 0.5 * samples_per_second_ + 0.5 * measured : measured;
+        }
+        stats_.gpu_seconds += report.gpu_seconds;
+        ++stats_.steps;
+    }
+    const auto now = clock::now();
+    for (auto& [id, r] : requests_)
+    {
+        if (r.state != RT_REQUEST_ACTIVE)
+        {
+            continue;
+        }
+        const int64_t done = engine_.passes(r.handle);
+        if (done >= 1 && r.first_frame_seconds < 0)
+        {
+            r.first_frame_seconds = std::chrono::duration<double>(now - r.submitted).count();
+        }
+        if (done >= r.target)
+        {
+            r.state = RT_REQUEST_DONE;
+            r.done_seconds = std::chrono::duration<double>(now - r.submitted).count();
+            stats_.rays += engine_.rays(r.handle);
+            stats_.shadow_rays += engine_.shadow_rays(r.handle);
+            ++stats_.completed;
+            ++report.completed;
+        }
+    }
+    for (const auto& [id, r] : requests_)
+    {
+        report.active += r.state == RT_REQUEST_ACTIVE ? 1 : 0;
+    }
+    report.queued = static_cast<int32_t>(queue_.size());
+    stats_.launches = engine_.launches();
+    stats_.used_bytes = static_cast<int64_t>(used_bytes_);
+    return report;
+}
+
+rt_request_status render_server::poll(int64_t id) const
+{
+    const auto it = requests_.find(id);
+    if (it == requests_.end())
+    {
+        fail(RT_ERR_INVALID, "no request " + std::to_string(id));
+    }
+    const request& r = it->second;
+    rt_request_status s{};
+    s.state = r.state;
+    s.passes = r.handle >= 0 ? engine_.passes(r.handle) : (r.state == RT_REQUEST_DONE ? r.target : 0);
+    s.target = r.target;
+    s.first_frame_seconds = r.first_frame_seconds;
+    s.done_seconds = r.done_seconds;
+    return s;
+}
+
+void render_server::fetch(int64_t id, double* pixels, int64_t count)
+{
+    const auto it = requests_.find(id);
+    if (it == requests_.end() || it->second.handle < 0 || it->second.state == RT_REQUEST_CANCELLED)
+    {
+        fail(RT_ERR_LOGIC, "request " + std::to_string(id) + " has no image");
+    }
+    request& r = it->second;
+    engine_.pixels(r.handle, pixels, count);
+    if (r.state == RT_REQUEST_DONE)
+    {
+        engine_.remove(r.handle);
+        r.handle = -1;
+        used_bytes_ -= r.bytes;
+        r.scene.reset();
+    }
+}
+
+void render_server::cancel(int64_t id)
+{
+    const auto it = requests_.find(id);
+    if (it == requests_.end())
+    {
+        fail(RT_ERR_INVALID, "no request " + std::to_string(id));
+    }
+    request& r = it->second;
+    if (r.state == RT_REQUEST_QUEUED)
+    {
+        queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
+    }
+    if (r.handle >= 0)
+    {
+        engine_.remove(r.handle);
+        r.handle = -1;
+        used_bytes_ -= r.bytes;
+    }
+    r.state = RT_REQUEST_CANCELLED;
+    r.scene.reset();
+}
+
+rt_server_stats render_server::stats() const { return stats_; }
+} // namespace rtb
+
+// ---- the C-ABI of batching and serving ----------------------------------------------------------------------
+
+namespace
+{
+template <class F>
+rt_status guard(F&& f)
+{
+    try
+    {
+        rtb::remember_error("");
+        f();
+        return RT_OK;
+    }
+    catch (const rtb::rt_error& e)
+    {
+        rtb::remember_error(e.what());
+        return e.status;
+    }
+    catch (const std::bad_alloc&)
+    {
+        rtb::remember_error("out of host memory");
+        return RT_ERR_RUNTIME;
+    }
+    catch (const std::exception& e)
+    {
+        rtb::remember_error(e.what());
+        return RT_ERR_RUNTIME;
+    }
+}
+
+void need(const void* p, const char* name)
+{
+    if (!p)
+    {
+        rtb::fail(RT_ERR_INVALID, std::string(name) + " is null");
+    }
+}
+} // namespace
+
+extern "C" {
+
+rt_status rt_batch_render(const rt_batch_job* jobs, int32_t count, const rt_batch_options* options,
+                          rt_batch_report* report)
+{
+    return guard([&] {
+        if (count < 0 || (count > 0 && !jobs))
+        {
+            rtb::fail(RT_ERR_INVALID, "jobs and count");
+        }
+        const auto start = std::chrono::steady_clock::now();
+        const rt_batch_options o = options ? *options : rt_batch_options{0, 1, 0};
+        rtb::batch_engine engine(o.partial_budget_bytes > 0 ? static_cast<size_t>(o.partial_budget_bytes) : 0,
+                                 o.use_graph != 0);
+        std::vector<int> handles;
+        std::vector<int64_t> targets;
+        for (int32_t i = 0; i < count; ++i)
+        {
+            need(jobs[i].scene, "jobs[i].scene");
+            need(jobs[i].pixels, "jobs[i].pixels");
+            auto scene = std::make_shared<rtb::resident_scene>(*jobs[i].scene);
+            const rt_camera_desc& c = jobs[i].scene->camera;
+            handles.push_back(engine.add(scene, c, jobs[i].seed, 0)); // images as rt_render's for the same seed
+            targets.push_back(jobs[i].passes > 0 ? jobs[i].passes : int64_t{c.sqrt_spp} * c.sqrt_spp);
+        }
+        const auto setup_end = std::chrono::steady_clock::now();
+        double gpu = 0;
+        int steps = 0;
+        while (true)
+        {
+            std::vector<rtb::batch_engine::assignment> work;
+            for (size_t i = 0; i < handles.size(); ++i)
+            {
+                if (engine.passes(handles[i]) < targets[i])
+                {
+                    work.push_back({handles[i], targets[i]});
+                }
+            }
+            if (work.empty())
+            {
+                break;
+            }
+            gpu += engine.step(std::move(work));
+            ++steps;
+        }
+        uint64_t rays = 0;
+        uint64_t shadow = 0;
+        for (int32_t i = 0; i < count; ++i)
+        {
+            const rt_camera_desc& c = jobs[i].scene->camera;
+            if (targets[static_cast<size_t>(i)] > 0)
+            {
+                engine.pixels(handles[static_cast<size_t>(i)], jobs[i].pixels, int64_t{c.image_width} * c.image_height * 3);
+            }
+            rays += engine.rays(handles[static_cast<size_t>(i)]);
+            shadow += engine.shadow_rays(handles[static_cast<size_t>(i)]);
+        }
+        if (report)
+        {
+            report->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+            report->setup_seconds = std::chrono::duration<double>(setup_end - start).count();
+            report->gpu_seconds = gpu;
+            report->rays = rays;
+            report->shadow_rays = shadow;
+            report->steps = steps;
+            report->launches = engine.launches();
+            report->graph = engine.graph_used() ? 1 : 0;
+        }
+    });
+}
+
+rt_status rt_server_create(const rt_server_options* options, rt_server** server)
+{
+    return guard([&] {
+        need(options, "options");
+        need(server, "server");
+        *server = nullptr;
+        auto s = std::make_unique<rt_server>();
+        s->server = std::make_unique<rtb::render_server>(*options);
+        *server = s.release();
+    });
+}
+
+rt_status rt_server_destroy(rt_server* server)
+{
+    return guard([&] { delete server; });
+}
+
+rt_status rt_server_submit(rt_server* server, rt_scene* scene, const rt_camera_desc* camera, uint64_t seed,
+                           int64_t target_passes, int64_t* request_id)
+{
+    return guard([&] {
+        need(server, "server");
+        need(scene, "scene");
+        need(camera, "camera");
+        need(request_id, "request_id");
+        *request_id = server->server->submit(scene->scene, *camera, seed, target_passes);
+    });
+}
+
+rt_status rt_server_step(rt_server* server, rt_server_step_report* report)
+{
+    return guard([&] {
+        need(server, "server");
+        const rt_server_step_report r = server->server->step();
+        if (report)
+        {
+            *report = r;
+        }
+    });
+}
+
+rt_status rt_server_poll(const rt_server* server, int64_t request_id, rt_request_status* status)
+{
+    return guard([&] {
+        need(server, "server");
+        need(status, "status");
+        *status = server->server->poll(request_id);
+    });
+}
+
+rt_status rt_server_fetch(rt_server* server, int64_t request_id, double* pixels, int64_t pixel_count)
+{
+    return guard([&] {
+        need(server, "server");
+        need(pixels, "pixels");
+        server->server->fetch(request_id, pixels, pixel_count);
+    });
+}
+
+rt_status rt_server_cancel(rt_server* server, int64_t request_id)
+{
+    return guard([&] {
+        need(server, "server");
+        server->server->cancel(request_id);
+    });
+}
+
+rt_status rt_server_stats_get(const rt_server* server, rt_server_stats* stats)
+{
+    return guard([&] {
+        need(server, "server");
+        need(stats, "stats");
+        *stats = server->server->stats();
+    });
+}
+
+rt_status rt_builtin_camera(const char* name, const rt_builtin_params* params, rt_camera_desc* camera)
+{
+    return guard([&] {
+        need(name, "name");
+        need(camera, "camera");
+        rt_builtin_params p{};
+        if (params)
+        {
+            p = *params;
+        }
+        else
+        {
+            p.sampling = -1;
+            p.combination = -1;
+        }
+        // The camera depends only on the scene's camera settings and the overrides, not on its geometry: build the
+        // scene at its cheapest (a level-0 mesh, a tiny map)
+        p.mesh_level = std::string(name) == "mesh-ggx" ? 1 : p.mesh_level;
+        p.env_width = 8;
+        std::unique_ptr<rtb::scene_store> s;
+        std::string error;
+        const rt_status status = rtb::build_builtin(name, p, s, error);
+        if (status != RT_OK)
+        {
+            rtb::fail(status, error);
+        }
+        *camera = s->camera;
+    });
+}
+}

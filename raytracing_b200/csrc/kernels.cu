@@ -1550,6 +1550,180 @@ __global__ void reduce_kernel(const reduce_params P)
     sum[2] = b;
 }
 
+// ---- batched launches: many jobs (requests), each its own scene, camera and passes, in one persistent kernel ------
+
+// The job whose range of the batch's item (or pixel) space holds `index`: a binary search over the jobs' starts
+template <bool PIXELS>
+__device__ __forceinline__ int find_job(const batch_job* jobs, int count, int64_t index)
+{
+    int lo = 0;
+    int hi = count - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        const int64_t begin = PIXELS ? jobs[mid].pixel_begin : jobs[mid].item_begin;
+        if (begin <= index)
+        {
+            lo = mid;
+        }
+        else
+        {
+            hi = mid - 1;
+        }
+    }
+    return lo;
+}
+
+// The same loop as render_kernel, with the job of each work item looked up in the job table: the jobs' items follow
+// each other in one item space, so the persistent threads pull work from every job at once, and a small job's tail
+// fills with another's work. Each job may use either integrator.
+__global__ void __launch_bounds__(render_block, RTB_MIN_BLOCKS_QUALITY) render_batch_kernel(const batch_params P)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lanes_below = (1u << lane) - 1u;
+    const int64_t total_items = P.header->total_items;
+    const int job_count = P.header->job_count;
+
+    uint32_t rays = 0;
+    uint32_t shadow_rays = 0;
+    bool need = true;
+    bool start = false;
+    int px = 0, py = 0;
+    int64_t pass = 0, pass_end = 0;
+    int64_t slot = 0;
+    double acc_r = 0.0, acc_g = 0.0, acc_b = 0.0;
+    const batch_job* J = nullptr;
+    sampler rng{};
+    path_state ps{};
+
+    while (true)
+    {
+        const unsigned active = __activemask();
+        const unsigned needing = __ballot_sync(active, need);
+        if (needing != 0u)
+        {
+            const int leader = __ffs(static_cast<int>(needing)) - 1;
+            unsigned long long base = 0;
+            if (static_cast<int>(lane) == leader)
+            {
+                base = atomicAdd(P.work_counter, static_cast<unsigned long long>(__popc(needing)));
+            }
+            base = __shfl_sync(active, base, leader);
+            if (need)
+            {
+                const auto item = static_cast<int64_t>(base + __popc(needing & lanes_below));
+                if (item >= total_items)
+                {
+                    break;
+                }
+                J = P.jobs + find_job<false>(P.jobs, job_count, item);
+                const int64_t local = item - J->item_begin;
+                const int64_t k = local / J->padded_pixels;
+                const int q = static_cast<int>(local - k * J->padded_pixels);
+                const int tile = q >> 5;
+                const int l = q & 31;
+                px = (tile % J->tiles_x) * 8 + (l & 7);
+                py = (tile / J->tiles_x) * 4 + (l >> 3);
+                if (px >= J->cam.width || py >= J->cam.height)
+                {
+                    continue;
+                }
+                const int64_t chunk_first = (J->first_chunk + k) * J->chunk;
+                pass = chunk_first > J->pass_begin ? chunk_first : J->pass_begin;
+                const int64_t chunk_end = chunk_first + J->chunk;
+                pass_end = chunk_end < J->pass_end ? chunk_end : J->pass_end;
+                slot = k * J->padded_pixels + q;
+                acc_r = acc_g = acc_b = 0.0;
+                rng.pixel = static_cast<uint32_t>(py) * static_cast<uint32_t>(J->cam.width) + static_cast<uint32_t>(px);
+                rng.job = J->job;
+                rays = 0;
+                shadow_rays = 0;
+                need = false;
+                start = true;
+            }
+        }
+        const camera_params& cam = J->cam;
+        if (start)
+        {
+            const int64_t round = pass / J->round_passes;
+            const int in_round = static_cast<int>(pass - round * J->round_passes);
+            const uint64_t key = J->seed + (static_cast<uint64_t>(round) << 32);
+            rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
+            rng.pass = static_cast<uint32_t>(in_round);
+            const float4 u = rng.draw(0, 0);
+            camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
+            ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
+            ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
+            ps.bsdf_pdf = 0.0f;
+            ps.specular = true;
+            ps.rays_left = cam.max_depth;
+            ps.depth = 0;
+            ps.from = -1;
+            ps.inward = false;
+            start = false;
+        }
+        hit_info h;
+        traverse<false>(J->scene, ps.o, ps.d, infinity_f, ps.from, ps.inward, -1, h);
+        ++rays;
+        ++ps.depth;
+        float3 sample;
+        const step_result r = J->quality
+                                  ? shade_quality<false>(J->scene, cam, rng, ps, h, sample, shadow_rays, nullptr)
+                                  : shade_books(J->scene, cam, rng, ps, h, sample);
+        if (r == step_result::done)
+        {
+            acc_r += without_nan(sample.x);
+            acc_g += without_nan(sample.y);
+            acc_b += without_nan(sample.z);
+            if (++pass == pass_end)
+            {
+                double* out = J->partials + 3 * slot;
+                out[0] = acc_r;
+                out[1] = acc_g;
+                out[2] = acc_b;
+                atomicAdd(J->counters, static_cast<unsigned long long>(rays));
+                if (shadow_rays)
+                {
+                    atomicAdd(J->counters + 1, static_cast<unsigned long long>(shadow_rays));
+                }
+                need = true;
+            }
+            else
+            {
+                start = true;
+            }
+        }
+    }
+}
+
+// Every job's pixels, in one grid-stride pass: each pixel's chunk partials added to its job's sums in chunk order
+__global__ void reduce_batch_kernel(const batch_params P)
+{
+    const int64_t total = P.header->total_pixels;
+    const int job_count = P.header->job_count;
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const batch_job& J = P.jobs[find_job<true>(P.jobs, job_count, i)];
+        const int64_t local = i - J.pixel_begin;
+        const int y = static_cast<int>(local / J.cam.width);
+        const int x = static_cast<int>(local - static_cast<int64_t>(y) * J.cam.width);
+        const int q = ((y >> 2) * J.tiles_x + (x >> 3)) * 32 + ((y & 3) << 3) + (x & 7);
+        double* sum = J.sums + 3 * local;
+        double r = sum[0], g = sum[1], b = sum[2];
+        for (int k = 0; k < J.chunks; ++k)
+        {
+            const double* part = J.partials + 3 * (static_cast<int64_t>(k) * J.padded_pixels + q);
+            r += part[0];
+            g += part[1];
+            b += part[2];
+        }
+        sum[0] = r;
+        sum[1] = g;
+        sum[2] = b;
+    }
+}
+
 __global__ void closest_hits_kernel(const scene_view S, const float* origins, const float* directions, int64_t count,
                                     const int32_t* prim_source, int32_t* ids, float* ts)
 {
@@ -1618,6 +1792,53 @@ cudaError_t launch_render(const launch_params& p, bool quality, bool counting, i
         }
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_batch(const batch_params& p, int grid, cudaStream_t stream)
+{
+    render_batch_kernel<<<grid, render_block, 0, stream>>>(p);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    reduce_batch_kernel<<<grid, 256, 0, stream>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_attributes(kernel_attributes& out)
+{
+    cudaFuncAttributes a{};
+    cudaError_t e = cudaFuncGetAttributes(&a, render_batch_kernel);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    int device = 0;
+    e = cudaGetDevice(&device);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    int blocks = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_batch_kernel, render_block, 0);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    cudaDeviceProp prop{};
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    out.registers = a.numRegs;
+    out.local_bytes = static_cast<int>(a.localSizeBytes);
+    out.blocks_per_sm = blocks;
+    out.threads_per_block = render_block;
+    out.max_threads_per_sm = prop.maxThreadsPerMultiProcessor;
+    out.multiprocessors = prop.multiProcessorCount;
+    return cudaSuccess;
 }
 
 cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream)

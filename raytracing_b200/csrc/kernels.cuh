@@ -44,6 +44,49 @@ struct reduce_params
     int32_t chunks;
 };
 
+// One job of a batched launch: a resident scene's view, its camera, and the passes this step renders of it. Its work
+// items are numbered from item_begin in the batch's item space, its pixels from pixel_begin in the batch's pixel
+// space (for the reduction); partials is its own slice of the batch's partials arena.
+struct alignas(16) batch_job
+{
+    scene_view scene;
+    camera_params cam;
+    uint64_t seed;
+    int64_t pass_begin;
+    int64_t pass_end;
+    int64_t first_chunk;
+    int64_t item_begin;
+    int64_t pixel_begin;
+    double* partials;
+    double* sums;                 // width * height * 3, this job's
+    unsigned long long* counters; // [0] segments, [1] shadow rays, this job's, accumulated
+    int32_t chunk;
+    int32_t chunks;
+    int32_t tiles_x;
+    int32_t padded_pixels;
+    int32_t round_passes;
+    int32_t quality;
+    uint32_t job;                 // the RNG counter's job field
+    int32_t pad0;
+};
+
+// What changes from step to step besides the jobs: read from device memory, so that a captured graph of the step
+// replays with new contents
+struct batch_header
+{
+    int64_t total_items;
+    int64_t total_pixels;
+    int32_t job_count;
+    int32_t pad0;
+};
+
+struct batch_params
+{
+    const batch_job* jobs;
+    const batch_header* header;
+    unsigned long long* work_counter;
+};
+
 // The kernels' static properties for kernel_info
 struct kernel_attributes
 {
@@ -59,6 +102,9 @@ constexpr int render_block = 128;
 
 cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream);
 cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream);
+// The batched step: the persistent kernel over every job's items, then the reduction of every job's pixels
+cudaError_t launch_batch(const batch_params& p, int grid, cudaStream_t stream);
+cudaError_t batch_attributes(kernel_attributes& out);
 cudaError_t render_attributes(bool quality, kernel_attributes& out);
 
 // Parity hooks: closest hits of given rays (source ids through prim_source), and the camera rays of one pass

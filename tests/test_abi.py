@@ -47,7 +47,10 @@ STRUCTS = {
     "rt_render_result": _abi.RenderResult, "rt_device_info": _abi.DeviceInfo,
     "rt_session_options": _abi.SessionOptions, "rt_accumulation": _abi.Accumulation,
     "rt_render_report": _abi.RenderReport, "rt_scene_stats": _abi.SceneStats,
-    "rt_builtin_params": _abi.BuiltinParams,
+    "rt_builtin_params": _abi.BuiltinParams, "rt_batch_job": _abi.BatchJob, "rt_batch_options": _abi.BatchOptions,
+    "rt_batch_report": _abi.BatchReport, "rt_server_options": _abi.ServerOptions,
+    "rt_request_status": _abi.RequestStatus, "rt_server_step_report": _abi.ServerStepReport,
+    "rt_server_stats": _abi.ServerStats,
 }
 
 
@@ -157,6 +160,19 @@ def test_no_cpu_fallback_without_gpu(rt):
     s = rt.builtin_scene("furnace", width=16)
     with pytest.raises(rt.RenderError):
         rt.render(s, seed=1)
+    with pytest.raises(rt.RenderError):
+        rt.batch_render([(s, 1, 4)])
+    with pytest.raises(rt.RenderError):
+        rt.Server()
+
+
+def test_builtin_camera_matches_the_scene(rt):
+    """The camera alone (the geometry built at its cheapest) is the full scene's camera, bit for bit."""
+    for name, kw in (("glass", dict(width=96, orbit=(30.0, 10.0))), ("mesh-ggx", dict(width=128, spp=4)),
+                     ("cover-30", dict(width=64, scene_seed=4))):
+        cam = rt.builtin_camera(name, **kw)
+        scene = rt.builtin_scene(name, **kw, **({"mesh_level": 2} if name == "mesh-ggx" else {}))
+        assert bytes(cam) == bytes(scene.camera), name
 
 
 def test_render_options_are_checked(rt):

@@ -1,0 +1,132 @@
+"""Batched rendering and serving on a B200, through the C-ABI.
+
+* A job rendered in a batch beside other jobs (other scenes, sizes, integrators) gives the image a plain render of
+  the same scene and seed gives, bit for bit: the batch's steps end on chunk boundaries, and each pixel's chunks are
+  added in chunk order whatever the step they came in.
+* The captured graph of a step gives the same images as the step launched directly.
+* A batch job's image passes ImageCompare against the oracle (the parity of the shared kernel path).
+* The server: admission under the HBM budget in arrival order, a first frame before refinement, a request done at
+  its target with an image equal (to rounding of a split first chunk) to a session's render of the same view.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed_scenes(rt):
+    return [
+        (rt.builtin_scene("glass", width=48, spp=64), 11, 64),
+        (rt.builtin_scene("cornell-mis", width=40, spp=16), 12, 20),
+        (rt.builtin_scene("cover-40", width=56, spp=16, sampling="mixture", scene_seed=3), 13, 33),
+        (rt.builtin_scene("materials", width=24, spp=4), 14, 16),
+        (rt.builtin_scene("furnace", width=16, spp=4), 15, 5),
+    ]
+
+
+def test_batch_equals_plain_renders(rt):
+    jobs = _mixed_scenes(rt)
+    b = rt.batch_render(jobs)
+    assert b.graph
+    assert b.steps >= 1 and b.launches == 2 * b.steps
+    for (scene, seed, passes), img in zip(jobs, b.images):
+        ref = rt.render(scene, seed=seed, passes=passes)
+        assert img.shape == ref.pixels.shape
+        assert np.array_equal(img, ref.pixels), (scene.width, np.abs(img - ref.pixels).max())
+    assert np.all(b.images[4] == 1.0)
+
+
+def test_batch_graph_equals_direct_launches(rt):
+    jobs = _mixed_scenes(rt)
+    a = rt.batch_render(jobs, use_graph=True)
+    b = rt.batch_render(jobs, use_graph=False)
+    assert a.graph and not b.graph
+    for x, y in zip(a.images, b.images):
+        assert np.array_equal(x, y)
+    assert a.rays == b.rays and a.shadow_rays == b.shadow_rays
+
+
+def test_batch_small_arena_takes_more_steps_same_images(rt):
+    jobs = _mixed_scenes(rt)[:3]
+    a = rt.batch_render(jobs)
+    # room for about one chunk of the largest job: the jobs are cut back to fewer chunks per step
+    b = rt.batch_render(jobs, partial_budget_bytes=48 * 48 * 24 * 2)
+    assert b.steps > a.steps
+    for x, y in zip(a.images, b.images):
+        assert np.array_equal(x, y)
+
+
+def test_batch_job_matches_oracle(rt, oracle):
+    s = rt.builtin_scene("cover-40", width=64, spp=64, sampling="mixture", scene_seed=5)
+    others = [(rt.builtin_scene("glass", width=40, spp=16), 1, 16)]
+    for gpu_seed, cpu_seed in ((101, 202), (303, 404)):
+        b = rt.batch_render([(s, gpu_seed, 64)] + others)
+        c, _ = oracle.render(s.desc, s.width, s.height, seed=cpu_seed, passes=64)
+        r = oracle.image_compare(c, b.images[0])
+        if r["verdict"] == 0:
+            return
+    raise AssertionError(f"a batch job failed ImageCompare twice: {r}")
+
+
+def _session_image(rt, scene_handle, camera, seed, passes):
+    sess = rt.Session(scene_handle, seed=seed)
+    sess.set_camera(camera)
+    sess.render_to(passes)
+    return sess.pixels()
+
+
+def test_server_serves_first_frames_then_targets(rt):
+    glass = rt.builtin_scene("glass", width=64, spp=16)
+    mis = rt.builtin_scene("cornell-mis", width=48, spp=16)
+    g = rt.Scene(glass)
+    m = rt.Scene(mis)
+    orbit = rt.builtin_camera("glass", width=80, spp=16, orbit=(40.0, 15.0))
+    server = rt.Server(hbm_budget_bytes=1 << 30, step_seconds=0.002)
+    ids = [server.submit(g, glass.camera, 5, 40), server.submit(m, mis.camera, 6, 33), server.submit(g, orbit, 7, 17)]
+    first = server.step()
+    assert first["admitted"] == 3 and first["first_frames"] == 3 and first["refined"] == 0
+    for i in ids:
+        st = server.poll(i)
+        assert st["state"] == "active" and st["passes"] == 1 and st["first_frame_seconds"] >= 0
+    steps = 1
+    while any(server.poll(i)["state"] != "done" for i in ids):
+        server.step()
+        steps += 1
+        assert steps < 500
+    views = [(g, glass.camera, 5, 40), (m, mis.camera, 6, 33), (g, orbit, 7, 17)]
+    for i, (scene, cam, seed, target) in zip(ids, views):
+        st = server.poll(i)
+        assert st["passes"] == target and st["done_seconds"] >= st["first_frame_seconds"] >= 0
+        img = server.fetch(i)
+        ref = _session_image(rt, scene, cam, seed, target)
+        np.testing.assert_allclose(img, ref, rtol=1e-12, atol=1e-12)
+    stats = server.stats()
+    assert stats["completed"] == 3 and stats["used_bytes"] == 0 and stats["rays"] > 0 and stats["shadow_rays"] > 0
+    server.close()
+
+
+def test_server_admits_under_the_budget_in_order(rt):
+    glass = rt.builtin_scene("glass", width=64, spp=16)
+    g = rt.Scene(glass)
+    one = glass.width * glass.height * 24 + 16
+    server = rt.Server(hbm_budget_bytes=one + one // 2, step_seconds=0.002)
+    ids = [server.submit(g, glass.camera, s, 16) for s in range(3)]
+    r = server.step()
+    assert r["admitted"] == 1 and r["queued"] == 2
+    assert server.poll(ids[1])["state"] == "queued"
+    with pytest.raises(rt.LogicError):
+        server.fetch(ids[1])
+    server.cancel(ids[2])
+    assert server.poll(ids[2])["state"] == "cancelled"
+    while server.poll(ids[0])["state"] != "done":
+        server.step()
+    server.fetch(ids[0])  # frees its memory: the next step admits the second
+    r = server.step()
+    assert r["admitted"] == 1 and r["queued"] == 0
+    while server.poll(ids[1])["state"] != "done":
+        server.step()
+    img = server.fetch(ids[1])
+    np.testing.assert_allclose(img, _session_image(rt, g, glass.camera, 1, 16), rtol=1e-12, atol=1e-12)
+    with pytest.raises(rt.CapacityError):
+        server.submit(g, rt.builtin_camera("glass", width=4000), 1, 1)
+    server.close()
