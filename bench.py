@@ -146,10 +146,11 @@ def cpu_baseline(scene, args, threads: int) -> dict:
 
     h = scene.height
     mid = h // 2
-    # Probe one row, then size the band to about --cpu-seconds
+    # Probe one row (one thread: rows are the unit of threading), then size the band to about --cpu-seconds on all
+    # threads
     _, probe = oracle.render(scene.desc, scene.width, h, seed=11, passes=args.spp, threads=threads,
                              row_begin=mid, row_end=mid + 1)
-    rows = int(max(1, min(h, args.cpu_seconds / max(probe["seconds"], 1e-3))))
+    rows = int(max(1, min(h, threads * args.cpu_seconds / max(probe["seconds"], 1e-3))))
     begin = max(0, mid - rows // 2)
     _, stats = oracle.render(scene.desc, scene.width, h, seed=12, passes=args.spp, threads=threads,
                              row_begin=begin, row_end=begin + rows)
@@ -329,8 +330,9 @@ def run_reference(args):
     mid = h // 2
     _, probe = oracle.render(scene.desc, scene.width, h, seed=1, passes=args.spp, threads=threads, row_begin=mid,
                              row_end=mid + 1)
-    # Each step is a band of rows of about 2 s of CPU work, so that warm-up + steps end within a few minutes
-    rows = int(max(1, min(h, 2.0 / max(probe["seconds"], 1e-3))))
+    # Each step is a band of rows of about 2 s on all threads (one row per thread at a time), so that warm-up +
+    # steps end within a few minutes
+    rows = int(max(1, min(h, threads * 2.0 / max(probe["seconds"], 1e-3))))
     begin = max(0, mid - rows // 2)
     for w in range(args.warmup):
         oracle.render(scene.desc, scene.width, h, seed=100 + w, passes=args.spp, threads=threads, row_begin=begin,

@@ -483,7 +483,6 @@ rt_server_step_report render_server::step()
     }
     report.queued = static_cast<int32_t>(queue_.size());
     stats_.launches = engine_.launches();
-    stats_.used_bytes = static_cast<int64_t>(used_bytes_);
     return report;
 }
 
@@ -544,7 +543,12 @@ void render_server::cancel(int64_t id)
     r.scene.reset();
 }
 
-rt_server_stats render_server::stats() const { return stats_; }
+rt_server_stats render_server::stats() const
+{
+    rt_server_stats s = stats_;
+    s.used_bytes = static_cast<int64_t>(used_bytes_);
+    return s;
+}
 } // namespace rtb
 
 // ---- the C-ABI of batching and serving ----------------------------------------------------------------------
