@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--extra", action="store_true", help="also measure the NEE/MIS integrator on the same scene")
     p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
+    p.add_argument("--no-reference-gpu", action="store_true",
+                   help="skip timing the reference's own CUDA renderer on the same workload")
     p.add_argument("--served", action="store_true", help="also measure the served request stream")
     p.add_argument("--served-rate", type=float, default=200.0)
     p.add_argument("--served-window", type=float, default=0.25, help="seconds of arrivals (a bounded sample)")
@@ -160,6 +162,25 @@ def cpu_baseline(scene, args, threads: int) -> dict:
                       f"({stats['rays']} segments in {stats['seconds']:.2f} s)"}
 
 
+def reference_gpu_measurement(scene_desc, passes: int, value: float) -> dict:
+    """The reference's own CUDA renderer (src/gpu, built unmodified into oracle/_ref) on the same workload and GPU:
+    gpu::render's rays over its kernel_seconds (the passes alone, timed on the GPU) — the reference's own figure."""
+    from oracle import ref_gpu
+
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so was not built (needs the reference's sources)"}
+    w, h = scene_desc.width, scene_desc.height
+    ref_gpu.render(scene_desc.desc, w, h, seed=5, passes=16)  # warm-up: module load, allocations
+    _, info = ref_gpu.render(scene_desc.desc, w, h, seed=6, passes=passes)
+    segments_per_s = info["rays"] / info["kernel_seconds"]
+    return {"segments_per_s": segments_per_s, "e2e_segments_per_s": info["rays"] / info["seconds"],
+            "kernel": info["kernel"], "registers": info["registers"],
+            "blocks_per_multiprocessor": info["blocks_per_multiprocessor"],
+            "segments_per_sample": info["rays"] / (w * h * passes),
+            "this_library_over_reference": value / segments_per_s,
+            "note": "the reference's gpu::render built from its src/gpu sources for sm_100a, same scene tables"}
+
+
 def log_uniform(rng, lo: float, hi: float) -> float:
     return float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
 
@@ -199,10 +220,26 @@ def batched_measurement(rt, torch) -> dict:
         plain_kernel += r.kernel_seconds
         plain_rays += r.rays
         identical += int(np.array_equal(r.pixels, img))
-        max_diff = max(max_diff, float(np.abs(r.pixels - img).max()))
+        max_diff = max(max_diff, abs(float(img.mean()) - float(r.pixels.mean())) / max(float(r.pixels.mean()), 1e-9))
     pixels = sum(s.width * s.height for s, _, _ in jobs)
     samples = sum(s.width * s.height * p for s, _, p in jobs)
-    return {"workload": "64 cover-scene variants (50-2000 spheres, W,H log-uniform 64-1024, spp log-uniform "
+    reference = {}
+    from oracle import ref_gpu
+
+    if ref_gpu.available():
+        ref_rays = 0
+        ref_kernel = 0.0
+        ref_wall = 0.0
+        for scene, seed, passes in jobs:
+            _, info = ref_gpu.render(scene.desc, scene.width, scene.height, seed=seed, passes=passes)
+            ref_rays += info["rays"]
+            ref_kernel += info["kernel_seconds"]
+            ref_wall += info["seconds"]
+        reference = {"reference_plain_segments_per_s": ref_rays / ref_kernel, "reference_plain_gpu_s": ref_kernel,
+                     "reference_plain_e2e_s": ref_wall,
+                     "speedup_gpu_over_reference": (b.rays / b.gpu_seconds) / (ref_rays / ref_kernel),
+                     "speedup_e2e_over_reference": ref_wall / batch_wall}
+    return {**reference, "workload": "64 cover-scene variants (50-2000 spheres, W,H log-uniform 64-1024, spp log-uniform "
                         "16-1024, seeds 0-63), mixture of sizes in one persistent launch per step",
             "pixels": pixels, "samples": samples, "segments": b.rays,
             "batched_segments_per_s": b.rays / b.gpu_seconds, "batched_gpu_s": b.gpu_seconds,
@@ -213,7 +250,8 @@ def batched_measurement(rt, torch) -> dict:
             "plain_e2e_segments_per_s": plain_rays / plain_wall, "plain_e2e_s": plain_wall,
             "speedup_gpu": (b.rays / b.gpu_seconds) / (plain_rays / plain_kernel),
             "speedup_e2e": plain_wall / batch_wall,
-            "jobs_bit_identical_to_plain": f"{identical}/{len(jobs)}", "max_abs_difference": max_diff}
+            "jobs_bit_identical_to_plain": f"{identical}/{len(jobs)}",
+            "max_relative_mean_difference_to_plain": max_diff}
 
 
 SERVED_RESOLUTIONS = [((256, 256), 4), ((512, 512), 3), ((1920, 1080), 2), ((3840, 2160), 1)]
@@ -519,6 +557,8 @@ def run_b200(args):
             "wall_s": time.perf_counter() - t0}}
         mis.close()
 
+    if rank == 0 and not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_measurement(scene_desc, passes, line["value"])
     if rank == 0 and not args.no_batched:
         line["batched"] = batched_measurement(rt, torch)
     if rank == 0 and args.served:

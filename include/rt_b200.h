@@ -301,6 +301,8 @@ typedef struct rt_scene_stats
     int64_t device_bytes;
     int32_t depth;
     int32_t max_leaf_size;
+    int32_t flat;               /* 1: a small scene of spheres and quads, searched by testing every primitive */
+    int32_t pad0;
 } rt_scene_stats;
 rt_status rt_scene_stats_get(const rt_scene* scene, rt_scene_stats* stats);
 

@@ -1,0 +1,65 @@
+"""Builds the reference's own CUDA renderer into oracle/_ref/libref_gpu.so (test infrastructure, not product).
+
+The reference's `gpu_renderer` library is eight CUDA sources under src/gpu (renderer.cu, display.cu, quality.cu,
+tonemap.cu, lamp_table.cu, environment_table.cu, CMakeLists.txt:155-165; guides.cu and denoise.cu, added to it by
+cmake/optix.cmake:203 with or without OptiX), plain nvcc translation units with no generated code and no external
+library. They are compiled here where they lie, unmodified, for sm_100a, with the
+flags its build gives them (-fmad=false for display.cu and tonemap.cu), and linked with oracle/ref_gpu_shim.cpp, a C
+entry point that converts this library's scene tables into the reference's. The output goes only to oracle/_ref/
+(git-ignored; it travels with the checkout to a GPU machine). Usage: python oracle/build_ref.py [reference root]
+"""
+from __future__ import annotations
+
+import concurrent.futures as futures
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent
+OUT = HERE / "_ref"
+LIBRARY = OUT / "libref_gpu.so"
+SOURCES = ["renderer.cu", "display.cu", "quality.cu", "tonemap.cu", "lamp_table.cu", "environment_table.cu", "guides.cu",
+           "denoise.cu"]
+NO_FMAD = {"display.cu", "tonemap.cu"}
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"{' '.join(cmd)} failed:\n{r.stdout}\n{r.stderr}")
+
+
+def build(reference: Path | None = None) -> Path | None:
+    """Returns the library's path, or None when the reference's sources are absent (e.g. on a GPU machine, which
+    uses the library built beside the checkout)."""
+    root = Path(reference) if reference else Path("/root/reference")
+    gpu = root / "src" / "gpu"
+    if not (gpu / "renderer.cu").exists():
+        return LIBRARY if LIBRARY.exists() else None
+    OUT.mkdir(exist_ok=True)
+    inputs = [gpu / s for s in SOURCES] + [HERE / "ref_gpu_shim.cpp", gpu / "renderer.h", Path(__file__)]
+    if LIBRARY.exists() and LIBRARY.stat().st_mtime > max(p.stat().st_mtime for p in inputs):
+        return LIBRARY
+
+    def compile_one(source: Path) -> Path:
+        obj = OUT / (source.stem + ".o")
+        flags = ["nvcc", "-std=c++20", "-O3", *ARCH, "-Xcompiler", "-fPIC", "-I", str(gpu), "-I",
+                 str(REPO / "include")]
+        if source.name in NO_FMAD:
+            flags.append("-fmad=false")
+        _run(flags + ["-c", str(source), "-o", str(obj)])
+        return obj
+
+    with futures.ThreadPoolExecutor(max_workers=9) as pool:
+        objects = list(pool.map(compile_one, [gpu / s for s in SOURCES] + [HERE / "ref_gpu_shim.cpp"]))
+    _run(["nvcc", "-shared", *ARCH, "-cudart", "static", "-o", str(LIBRARY), *map(str, objects)])
+    for obj in objects:
+        obj.unlink()
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    path = build(Path(sys.argv[1]) if len(sys.argv) > 1 else None)
+    print(path if path else "reference sources absent: nothing built")

@@ -139,7 +139,7 @@ class RenderReport(C.Structure):
 class SceneStats(C.Structure):
     _fields_ = [("spheres", C.c_int64), ("quads", C.c_int64), ("triangles", C.c_int64), ("nodes", C.c_int64),
                 ("leaves", C.c_int64), ("lamps", C.c_int64), ("lights", C.c_int64), ("device_bytes", C.c_int64),
-                ("depth", C.c_int32), ("max_leaf_size", C.c_int32)]
+                ("depth", C.c_int32), ("max_leaf_size", C.c_int32), ("flat", C.c_int32), ("pad0", C.c_int32)]
 
 
 class BuiltinParams(C.Structure):

@@ -14,7 +14,8 @@ namespace rtb
 {
 // The jobs of a batch, each a resident scene seen by its own camera, with its own sums, seed and passes. A step
 // renders for each chosen job the passes from where it stands to a given end, all in one persistent launch of
-// render_batch_kernel and one reduction, captured once into a CUDA graph and replayed with new job tables.
+// render_batch_kernel per search (the flat scenes' jobs, then the others) and one reduction, captured once into a
+// CUDA graph and replayed with new job tables.
 class batch_engine
 {
 public:
@@ -71,7 +72,8 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaEvent_t start_ = nullptr;
     cudaEvent_t stop_ = nullptr;
-    int grid_ = 0;
+    int grid_ = 0;      // the tree search's launch
+    int flat_grid_ = 0; // the flat search's launch
     device_array<double> arena_;
     device_array<batch_job> table_;
     device_array<batch_header> header_;

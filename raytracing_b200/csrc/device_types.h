@@ -178,6 +178,7 @@ struct scene_view
     float light_pmf;         // 1 / (lamps + the map if it is sampled)
     int32_t combination;
     int32_t has_environment; // misses see the map (the NEE/MIS integrator only), not the camera's sky
+    int32_t flat;            // a small scene of spheres and quads: closest hits test every primitive, no tree walk
     environment_view env;
 };
 } // namespace rtb

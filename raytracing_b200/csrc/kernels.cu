@@ -11,9 +11,9 @@
 // The estimators are the reference's: the books' strategies (src/gpu/camera.cuh:304-437 diffuse_bounce, trace_ray;
 // material.cuh:84-126 scatter; lights.cuh:49-227 the lights list) and the quality kernel's NEE with MIS
 // (quality_path.cuh:61-188, light_sampler.cuh:40-103, lamps.cuh:81-146, mis.cuh:30-62). What differs is the B200 form:
-// a 64-byte node holding both children's boxes, counter-based random numbers that depend only on (seed, pixel,
-// pass, depth, dimension), work items instead of one thread per pixel, and FP64 only for a large sphere's quadratic
-// and for the per-pixel sums.
+// a 64-byte node holding both children's boxes, a flat search for small scenes, counter-based random numbers that
+// depend only on (seed, pixel, pass, depth, dimension), work items instead of one thread per pixel, and FP64 only for
+// a large sphere's quadratic and for the per-pixel sums.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -100,10 +100,10 @@ struct sampler
 };
 
 // The fixed dimension blocks of a vertex: block 0 the material's own sample (direction u0 u1, lobe or mixture
-// choice u2, the lights list's pick u3), block 1 the books' lights-list point, blocks 2-3 the NEE light sample (the
-// pick, a lamp's point or the map's bin bits, coin and cell position)
+// choice u2, the lights list's pick u3; a books' vertex that aims at the lights list takes the point from u0 u1, which
+// its direction then does not use, so a books' vertex draws one block), blocks 2-3 the NEE light sample (the pick, a
+// lamp's point or the map's bin bits, coin and cell position)
 constexpr int block_material = 0;
-constexpr int block_lights = 1;
 constexpr int block_nee = 2;
 
 // ---- sampling of directions (random.cuh:95-140, material.cuh:55-64) --------------------------------------------
@@ -419,7 +419,14 @@ constexpr int traversal_done = static_cast<int>(0x80000000u);
 // first leaf it meets and keeps descending, and the warp leaves the node loop together once every lane holds a leaf;
 // then the leaf loop tests them. Node steps and leaf tests so run with the warp's lanes side by side, where a single
 // loop would run a node step for some lanes and a leaf test for the others one after the other.
-template <bool SHADOW, bool COUNT = false>
+//
+// SEARCH: search_any follows the scene's `flat`; search_flat and search_tree compile one of the two searches alone
+// (a kernel specialised for one of them keeps no code, registers or stack for the other).
+constexpr int search_any = 0;
+constexpr int search_flat = 1;
+constexpr int search_tree = 2;
+
+template <bool SHADOW, bool COUNT = false, int SEARCH = search_any>
 __device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d, float t_max, int from, bool inward,
                                          int skip, hit_info& hit, fetch_counts* counts = nullptr)
 {
@@ -431,6 +438,55 @@ __device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d
         return false;
     }
     const float inverse_a = 1.0f / length_squared(d);
+    if (SEARCH == search_flat || (SEARCH == search_any && S.flat))
+    {
+        // A small scene of spheres and quads: every primitive tested in order, no tree. The warp's lanes run the same
+        // loop over the same records (one broadcast load each), where a tree walk would split them up.
+        for (int i = 0; i < S.quad_base; ++i)
+        {
+            const bool own = i == from;
+            if ((own && !inward) || i == skip)
+            {
+                continue;
+            }
+            const float4 s = __ldg(reinterpret_cast<const float4*>(S.spheres + i));
+            float t;
+            bool entering;
+            if (hit_sphere(s, o, d, inverse_a, t_min, hit.t, own, t, entering))
+            {
+                if (SHADOW)
+                {
+                    return true;
+                }
+                hit = {i, t, entering};
+            }
+        }
+        const int quads = S.triangle_base - S.quad_base;
+        for (int i = 0; i < quads; ++i)
+        {
+            const int id = S.quad_base + i;
+            if (id == from || id == skip)
+            {
+                continue;
+            }
+            float t;
+            bool front;
+            if (hit_quad(load_quad(S.quads, i), o, d, t_min, hit.t, t, front))
+            {
+                if (SHADOW)
+                {
+                    return true;
+                }
+                hit = {id, t, front};
+            }
+        }
+        if (COUNT)
+        {
+            counts->spheres += S.quad_base;
+            counts->quads += quads;
+        }
+        return hit.id >= 0;
+    }
     const float3 inv = make_float3(safe_inverse(d.x), safe_inverse(d.y), safe_inverse(d.z));
     const float3 os = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
     int2 stack[max_bvh_depth];
@@ -833,8 +889,7 @@ __device__ __forceinline__ step_result shade_books(const scene_view& S, const ca
             }
             if (toward_lights)
             {
-                const float4 v = rng.draw(ps.depth, block_lights);
-                direction = lights_random(S, s.p, u.w, v.x, v.y);
+                direction = lights_random(S, s.p, u.w, u.x, u.y);
             }
             else
             {
@@ -1162,7 +1217,7 @@ __device__ float3 eval_lobe(int lobe, const material12& m, float3 albedo, float3
 }
 
 // One segment of an NEE/MIS path after its closest hit; the shadow ray is traced here
-template <bool COUNT>
+template <bool COUNT, int SEARCH = search_any>
 __device__ __forceinline__ step_result shade_quality(const scene_view& S, const camera_params& cam,
                                                      const sampler& rng, path_state& ps, const hit_info& h,
                                                      float3& sample, uint32_t& shadow_rays, fetch_counts* counts)
@@ -1339,7 +1394,7 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
     {
         ++shadow_rays;
         hit_info blocker;
-        const bool blocked = traverse<true, COUNT>(S, s.p, light_dir, light_distance, h.id,
+        const bool blocked = traverse<true, COUNT, SEARCH>(S, s.p, light_dir, light_distance, h.id,
                                                    dot(light_dir, s.outward) < 0.0f, skip, blocker, counts);
         if (!blocked)
         {
@@ -1375,16 +1430,24 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
 // ---- the persistent render kernel ------------------------------------------------------------------------------
 // The render kernel's resident blocks per multiprocessor, which caps its registers: the books' integrator at 64 (8
 // blocks of 128 threads measured fastest against 5 and 6 blocks, for the latency they hide), the NEE/MIS integrator,
-// whose GGX and environment code spills heavily at 64, at 80 (6 blocks)
+// whose GGX and environment code spills heavily at 64, at 80 (6 blocks); with the flat search (no tree stack) both
+// at 72 (7 blocks), measured fastest against 5, 6 and 8 on the Cornell boxes
 #ifndef RTB_MIN_BLOCKS
 #define RTB_MIN_BLOCKS 8
 #endif
 #ifndef RTB_MIN_BLOCKS_QUALITY
 #define RTB_MIN_BLOCKS_QUALITY 6
 #endif
+#ifndef RTB_MIN_BLOCKS_FLAT
+#define RTB_MIN_BLOCKS_FLAT 7
+#endif
+#ifndef RTB_MIN_BLOCKS_QUALITY_FLAT
+#define RTB_MIN_BLOCKS_QUALITY_FLAT 7
+#endif
 
-template <bool QUALITY, bool COUNT>
-__global__ void __launch_bounds__(render_block, QUALITY ? RTB_MIN_BLOCKS_QUALITY : RTB_MIN_BLOCKS)
+template <bool QUALITY, bool COUNT, bool FLAT>
+__global__ void __launch_bounds__(render_block, QUALITY ? (FLAT ? RTB_MIN_BLOCKS_QUALITY_FLAT : RTB_MIN_BLOCKS_QUALITY)
+                                                        : (FLAT ? RTB_MIN_BLOCKS_FLAT : RTB_MIN_BLOCKS))
     render_kernel(const __grid_constant__ launch_params P)
 {
     __shared__ unsigned long long block_rays;
@@ -1477,13 +1540,15 @@ __global__ void __launch_bounds__(render_block, QUALITY ? RTB_MIN_BLOCKS_QUALITY
         }
 
         // One segment: the closest hit, then the vertex's shading
+        constexpr int search = FLAT ? search_flat : search_tree;
         hit_info h;
-        traverse<false, COUNT>(P.scene, ps.o, ps.d, infinity_f, ps.from, ps.inward, -1, h, &counts);
+        traverse<false, COUNT, search>(P.scene, ps.o, ps.d, infinity_f, ps.from, ps.inward, -1, h, &counts);
         ++rays;
         ++ps.depth;
         float3 sample;
-        const step_result r = QUALITY ? shade_quality<COUNT>(P.scene, cam, rng, ps, h, sample, shadow_rays, &counts)
-                                      : shade_books(P.scene, cam, rng, ps, h, sample);
+        const step_result r =
+            QUALITY ? shade_quality<COUNT, search>(P.scene, cam, rng, ps, h, sample, shadow_rays, &counts)
+                    : shade_books(P.scene, cam, rng, ps, h, sample);
         if (r == step_result::done)
         {
             acc_r += without_nan(sample.x);
@@ -1552,12 +1617,13 @@ __global__ void reduce_kernel(const reduce_params P)
 
 // ---- batched launches: many jobs (requests), each its own scene, camera and passes, in one persistent kernel ------
 
-// The job whose range of the batch's item (or pixel) space holds `index`: a binary search over the jobs' starts
+// The job of jobs [first, end) whose range of the batch's item (or pixel) space holds `index`: a binary search over
+// the jobs' starts
 template <bool PIXELS>
-__device__ __forceinline__ int find_job(const batch_job* jobs, int count, int64_t index)
+__device__ __forceinline__ int find_job(const batch_job* jobs, int first, int end, int64_t index)
 {
-    int lo = 0;
-    int hi = count - 1;
+    int lo = first;
+    int hi = end - 1;
     while (lo < hi)
     {
         const int mid = (lo + hi + 1) >> 1;
@@ -1576,13 +1642,21 @@ __device__ __forceinline__ int find_job(const batch_job* jobs, int count, int64_
 
 // The same loop as render_kernel, with the job of each work item looked up in the job table: the jobs' items follow
 // each other in one item space, so the persistent threads pull work from every job at once, and a small job's tail
-// fills with another's work. Each job may use either integrator.
-__global__ void __launch_bounds__(render_block, RTB_MIN_BLOCKS_QUALITY) render_batch_kernel(const batch_params P)
+// fills with another's work. Each job may use either integrator. The jobs of flat scenes come first in the table and
+// the item space, and each search has its own launch (FLAT: items [0, flat_items) of jobs [0, flat_jobs); otherwise
+// the rest), compiled as render_kernel's for that search, so a job renders the same bits as its plain render.
+template <bool FLAT>
+__global__ void __launch_bounds__(render_block, FLAT ? RTB_MIN_BLOCKS_QUALITY_FLAT : RTB_MIN_BLOCKS_QUALITY)
+    render_batch_kernel(const batch_params P)
 {
+    constexpr int search = FLAT ? search_flat : search_tree;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
-    const int64_t total_items = P.header->total_items;
-    const int job_count = P.header->job_count;
+    const int64_t item_begin = FLAT ? 0 : P.header->flat_items;
+    const int64_t total_items = FLAT ? P.header->flat_items : P.header->total_items;
+    const int job_first = FLAT ? 0 : P.header->flat_jobs;
+    const int job_end = FLAT ? P.header->flat_jobs : P.header->job_count;
+    unsigned long long* const work_counter = P.work_counter + (FLAT ? 0 : 1);
 
     uint32_t rays = 0;
     uint32_t shadow_rays = 0;
@@ -1606,17 +1680,17 @@ __global__ void __launch_bounds__(render_block, RTB_MIN_BLOCKS_QUALITY) render_b
             unsigned long long base = 0;
             if (static_cast<int>(lane) == leader)
             {
-                base = atomicAdd(P.work_counter, static_cast<unsigned long long>(__popc(needing)));
+                base = atomicAdd(work_counter, static_cast<unsigned long long>(__popc(needing)));
             }
             base = __shfl_sync(active, base, leader);
             if (need)
             {
-                const auto item = static_cast<int64_t>(base + __popc(needing & lanes_below));
+                const auto item = item_begin + static_cast<int64_t>(base + __popc(needing & lanes_below));
                 if (item >= total_items)
                 {
                     break;
                 }
-                J = P.jobs + find_job<false>(P.jobs, job_count, item);
+                J = P.jobs + find_job<false>(P.jobs, job_first, job_end, item);
                 const int64_t local = item - J->item_begin;
                 const int64_t k = local / J->padded_pixels;
                 const int q = static_cast<int>(local - k * J->padded_pixels);
@@ -1663,13 +1737,13 @@ __global__ void __launch_bounds__(render_block, RTB_MIN_BLOCKS_QUALITY) render_b
             start = false;
         }
         hit_info h;
-        traverse<false>(J->scene, ps.o, ps.d, infinity_f, ps.from, ps.inward, -1, h);
+        traverse<false, false, search>(J->scene, ps.o, ps.d, infinity_f, ps.from, ps.inward, -1, h);
         ++rays;
         ++ps.depth;
         float3 sample;
-        const step_result r = J->quality
-                                  ? shade_quality<false>(J->scene, cam, rng, ps, h, sample, shadow_rays, nullptr)
-                                  : shade_books(J->scene, cam, rng, ps, h, sample);
+        const step_result r =
+            J->quality ? shade_quality<false, search>(J->scene, cam, rng, ps, h, sample, shadow_rays, nullptr)
+                       : shade_books(J->scene, cam, rng, ps, h, sample);
         if (r == step_result::done)
         {
             acc_r += without_nan(sample.x);
@@ -1704,7 +1778,7 @@ __global__ void reduce_batch_kernel(const batch_params P)
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     {
-        const batch_job& J = P.jobs[find_job<true>(P.jobs, job_count, i)];
+        const batch_job& J = P.jobs[find_job<true>(P.jobs, 0, job_count, i)];
         const int64_t local = i - J.pixel_begin;
         const int y = static_cast<int>(local / J.cam.width);
         const int x = static_cast<int>(local - static_cast<int64_t>(y) * J.cam.width);
@@ -1767,67 +1841,82 @@ __global__ void camera_rays_kernel(const camera_params cam, uint64_t seed, int64
 }
 } // namespace
 
-cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream)
+namespace
+{
+using render_function = void (*)(launch_params);
+
+// The render kernel for an integrator, the counting build or not, and a flat or a tree search
+render_function render_kernel_for(bool quality, bool counting, bool flat)
 {
     if (quality)
     {
         if (counting)
         {
-            render_kernel<true, true><<<grid, render_block, 0, stream>>>(p);
+            return flat ? render_kernel<true, true, true> : render_kernel<true, true, false>;
         }
-        else
-        {
-            render_kernel<true, false><<<grid, render_block, 0, stream>>>(p);
-        }
+        return flat ? render_kernel<true, false, true> : render_kernel<true, false, false>;
     }
-    else
+    if (counting)
     {
-        if (counting)
-        {
-            render_kernel<false, true><<<grid, render_block, 0, stream>>>(p);
-        }
-        else
-        {
-            render_kernel<false, false><<<grid, render_block, 0, stream>>>(p);
-        }
+        return flat ? render_kernel<false, true, true> : render_kernel<false, true, false>;
     }
+    return flat ? render_kernel<false, false, true> : render_kernel<false, false, false>;
+}
+} // namespace
+
+cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream)
+{
+    render_kernel_for(quality, counting, p.scene.flat != 0)<<<grid, render_block, 0, stream>>>(p);
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch(const batch_params& p, int grid, cudaStream_t stream)
+cudaError_t launch_batch(const batch_params& p, int flat_grid, int tree_grid, cudaStream_t stream)
 {
-    render_batch_kernel<<<grid, render_block, 0, stream>>>(p);
-    const cudaError_t e = cudaGetLastError();
+    render_batch_kernel<true><<<flat_grid, render_block, 0, stream>>>(p);
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
     {
         return e;
     }
-    reduce_batch_kernel<<<grid, 256, 0, stream>>>(p);
+    render_batch_kernel<false><<<tree_grid, render_block, 0, stream>>>(p);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    reduce_batch_kernel<<<tree_grid, 256, 0, stream>>>(p);
     return cudaGetLastError();
 }
 
-cudaError_t batch_attributes(kernel_attributes& out)
+namespace
+{
+// A kernel's registers, local memory and resident blocks, and the device's multiprocessors (two attribute queries:
+// cudaGetDeviceProperties would fill every field of the device's description, a cost each session paid)
+template <class Kernel>
+cudaError_t attributes_of(Kernel kernel, kernel_attributes& out)
 {
     cudaFuncAttributes a{};
-    cudaError_t e = cudaFuncGetAttributes(&a, render_batch_kernel);
-    if (e != cudaSuccess)
-    {
-        return e;
-    }
+    cudaError_t e = cudaFuncGetAttributes(&a, kernel);
     int device = 0;
-    e = cudaGetDevice(&device);
-    if (e != cudaSuccess)
+    if (e == cudaSuccess)
     {
-        return e;
+        e = cudaGetDevice(&device);
     }
     int blocks = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_batch_kernel, render_block, 0);
-    if (e != cudaSuccess)
+    if (e == cudaSuccess)
     {
-        return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, render_block, 0);
     }
-    cudaDeviceProp prop{};
-    e = cudaGetDeviceProperties(&prop, device);
+    int multiprocessors = 0;
+    int max_threads = 0;
+    if (e == cudaSuccess)
+    {
+        e = cudaDeviceGetAttribute(&multiprocessors, cudaDevAttrMultiProcessorCount, device);
+    }
+    if (e == cudaSuccess)
+    {
+        e = cudaDeviceGetAttribute(&max_threads, cudaDevAttrMaxThreadsPerMultiProcessor, device);
+    }
     if (e != cudaSuccess)
     {
         return e;
@@ -1836,9 +1925,15 @@ cudaError_t batch_attributes(kernel_attributes& out)
     out.local_bytes = static_cast<int>(a.localSizeBytes);
     out.blocks_per_sm = blocks;
     out.threads_per_block = render_block;
-    out.max_threads_per_sm = prop.maxThreadsPerMultiProcessor;
-    out.multiprocessors = prop.multiProcessorCount;
+    out.max_threads_per_sm = max_threads;
+    out.multiprocessors = multiprocessors;
     return cudaSuccess;
+}
+} // namespace
+
+cudaError_t batch_attributes(bool flat, kernel_attributes& out)
+{
+    return flat ? attributes_of(render_batch_kernel<true>, out) : attributes_of(render_batch_kernel<false>, out);
 }
 
 cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream)
@@ -1849,41 +1944,9 @@ cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-cudaError_t render_attributes(bool quality, kernel_attributes& out)
+cudaError_t render_attributes(bool quality, bool flat, kernel_attributes& out)
 {
-    cudaFuncAttributes a{};
-    cudaError_t e = quality ? cudaFuncGetAttributes(&a, render_kernel<true, false>)
-                            : cudaFuncGetAttributes(&a, render_kernel<false, false>);
-    if (e != cudaSuccess)
-    {
-        return e;
-    }
-    int device = 0;
-    e = cudaGetDevice(&device);
-    if (e != cudaSuccess)
-    {
-        return e;
-    }
-    int blocks = 0;
-    e = quality ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<true, false>, render_block, 0)
-                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, render_kernel<false, false>, render_block, 0);
-    if (e != cudaSuccess)
-    {
-        return e;
-    }
-    cudaDeviceProp prop{};
-    e = cudaGetDeviceProperties(&prop, device);
-    if (e != cudaSuccess)
-    {
-        return e;
-    }
-    out.registers = a.numRegs;
-    out.local_bytes = static_cast<int>(a.localSizeBytes);
-    out.blocks_per_sm = blocks;
-    out.threads_per_block = render_block;
-    out.max_threads_per_sm = prop.maxThreadsPerMultiProcessor;
-    out.multiprocessors = prop.multiProcessorCount;
-    return cudaSuccess;
+    return attributes_of(render_kernel_for(quality, false, flat), out);
 }
 
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,

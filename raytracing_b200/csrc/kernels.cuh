@@ -76,15 +76,16 @@ struct batch_header
 {
     int64_t total_items;
     int64_t total_pixels;
+    int64_t flat_items;     // the items of the flat scenes' jobs, which come first: [0, flat_items)
     int32_t job_count;
-    int32_t pad0;
+    int32_t flat_jobs;      // jobs [0, flat_jobs) search flat
 };
 
 struct batch_params
 {
     const batch_job* jobs;
     const batch_header* header;
-    unsigned long long* work_counter;
+    unsigned long long* work_counter; // [0] the flat launch's, [1] the tree launch's
 };
 
 // The kernels' static properties for kernel_info
@@ -102,10 +103,11 @@ constexpr int render_block = 128;
 
 cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream);
 cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream);
-// The batched step: the persistent kernel over every job's items, then the reduction of every job's pixels
-cudaError_t launch_batch(const batch_params& p, int grid, cudaStream_t stream);
-cudaError_t batch_attributes(kernel_attributes& out);
-cudaError_t render_attributes(bool quality, kernel_attributes& out);
+// The batched step: the persistent kernel over the flat scenes' items, the one over the other jobs' items, then the
+// reduction of every job's pixels
+cudaError_t launch_batch(const batch_params& p, int flat_grid, int tree_grid, cudaStream_t stream);
+cudaError_t batch_attributes(bool flat, kernel_attributes& out);
+cudaError_t render_attributes(bool quality, bool flat, kernel_attributes& out);
 
 // Parity hooks: closest hits of given rays (source ids through prim_source), and the camera rays of one pass
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,

@@ -70,6 +70,13 @@ quad12 make_quad(const rt_quad_desc& d)
 #ifndef RTB_LEAF_SIZE
 #define RTB_LEAF_SIZE 1
 #endif
+// A scene of at most RTB_FLAT_SCENE spheres and quads (no triangles) is searched without its tree: every primitive
+// tested in turn, the same loop in every lane of a warp, where a tree walk splits the lanes up. Measured on the
+// B200: the Cornell boxes (13-18 quads and spheres) and the five-sphere scene render 30-50% faster flat, while 20
+// scattered spheres are as fast either way and 40 are 25% slower flat.
+#ifndef RTB_FLAT_SCENE
+#define RTB_FLAT_SCENE 24
+#endif
 
 // A sphere whose quadratic is solved in FP64: radius large next to the spacing of floats at its center, where the
 // l-vector form's r^2 - |l|^2 is a difference of numbers near r^2 (the radius-1000 ground)
@@ -656,6 +663,7 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     view_.light_pmf = light_set == 0 ? 0.0f : static_cast<float>(1.0 / static_cast<double>(light_set));
     view_.combination = quality_ ? d.combination : RT_COMBINE_BSDF_ONLY;
     view_.has_environment = d.environment ? 1 : 0;
+    view_.flat = T == 0 && S + Q <= RTB_FLAT_SCENE ? 1 : 0;
     view_.env = env;
 
     stats_.spheres = S;
@@ -671,5 +679,6 @@ resident_scene::resident_scene(const rt_scene_desc& d)
                                                env_texels_.bytes() + env_bins_.bytes() + env_row_cos_.bytes());
     stats_.depth = tree.depth;
     stats_.max_leaf_size = options.max_leaf_size;
+    stats_.flat = view_.flat;
 }
 } // namespace rtb
