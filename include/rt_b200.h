@@ -477,8 +477,8 @@ typedef struct rt_builtin_params
     int32_t mesh_level;         /* mesh-ggx: icosphere subdivision level (8: 1,310,720 triangles) */
     int32_t env_width;          /* mesh-ggx: environment map width (height = width / 2) */
     int32_t pad0;
-    double orbit_azimuth;       /* when orbit != 0: camera orbits the look-at point (serving requests) */
-    double orbit_elevation;
+    double orbit_azimuth;       /* when orbit != 0: the camera orbits the look-at point at its distance (serving */
+    double orbit_elevation;     /* requests): azimuth about +y from +z and elevation above the horizon, in degrees */
     int32_t orbit;
     int32_t pad1;
 } rt_builtin_params;

@@ -10,6 +10,7 @@
 #pragma once
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -200,6 +201,7 @@ struct hit_record
     double t = 0;
     double u = 0, v = 0;
     bool front_face = false;
+    color color_at; // the material's color at the hit (its texture there), filled by scene::closest_event
     void set_face_normal(const ray& r, const vec3& outward)
     {
         front_face = dot(r.direction, outward) < 0;
@@ -215,6 +217,7 @@ struct sphere
     int material = -1;
     int id = -1;
     aabb bbox;
+    double uv_cos = 1, uv_sin = 0; // the turn of the rotate_y instances around it, for its texture coordinates
 
     sphere(const point3& c1, const point3& c2, double r, int mat, int ident)
         : center{c1, c2 - c1}, radius(std::fmax(0.0, r)), material(mat), id(ident)
@@ -253,8 +256,10 @@ struct sphere
         rec.set_face_normal(r, outward);
         rec.material = material;
         rec.id = id;
-        const double phi = std::atan2(-outward.z, outward.x) + std::numbers::pi;
-        const double theta = std::acos(std::clamp(-outward.y, -1.0, 1.0));
+        // get_sphere_uv of the normal in the sphere's own coordinates (turned back by its rotate_y instances)
+        const vec3 n{uv_cos * outward.x - uv_sin * outward.z, outward.y, uv_sin * outward.x + uv_cos * outward.z};
+        const double phi = std::atan2(-n.z, n.x) + std::numbers::pi;
+        const double theta = std::acos(std::clamp(-n.y, -1.0, 1.0));
         rec.u = phi / (2 * std::numbers::pi);
         rec.v = theta / std::numbers::pi;
         return rec;
@@ -585,16 +590,188 @@ private:
     }
 };
 
-// ---- materials: material.ixx, with textures reduced to the solid colors the configs use ------------------------
+// ---- materials: material.ixx -----------------------------------------------------------------------------------
 struct material
 {
     int kind = RT_LAMBERTIAN;
     color albedo;            // lambertian, diffuse_light, isotropic: the solid texture's color; metal: its albedo
+    int texture = -1;        // lambertian, diffuse_light, isotropic: its texture when it is not one solid color
     double fuzz = 0;
     double refraction_index = 1;
     int lobe = RT_MICROFACET_NONE; // the quality integrator's GGX side entry (renderer.h:249-261)
     double roughness = 0;
     double alpha = 0;              // r^2, rounded to float as the GPU's
+};
+
+// ---- texture.ixx and perlin.ixx: solid, checker, image and marble textures, in double ----------------------------
+struct perlin_table
+{
+    std::array<vec3, 256> gradients;
+    std::array<int, 256> perm_x, perm_y, perm_z;
+
+    double noise(const point3& p) const // perlin.ixx noise: Hermite-smoothed trilinear sum of gradient dot products
+    {
+        const double fx = std::floor(p.x), fy = std::floor(p.y), fz = std::floor(p.z);
+        const double u = p.x - fx, v = p.y - fy, w = p.z - fz;
+        const int i = static_cast<int>(fx), j = static_cast<int>(fy), k = static_cast<int>(fz);
+        const double uu = u * u * (3 - 2 * u), vv = v * v * (3 - 2 * v), ww = w * w * (3 - 2 * w);
+        double accum = 0;
+        for (int di = 0; di < 2; ++di)
+        {
+            for (int dj = 0; dj < 2; ++dj)
+            {
+                for (int dk = 0; dk < 2; ++dk)
+                {
+                    const vec3& g = gradients[static_cast<size_t>(perm_x[(i + di) & 255] ^ perm_y[(j + dj) & 255] ^
+                                                                  perm_z[(k + dk) & 255])];
+                    const vec3 offset{u - di, v - dj, w - dk};
+                    accum += (di * uu + (1 - di) * (1 - uu)) * (dj * vv + (1 - dj) * (1 - vv)) *
+                             (dk * ww + (1 - dk) * (1 - ww)) * dot(g, offset);
+                }
+            }
+        }
+        return accum;
+    }
+
+    double turbulence(point3 p, int depth) const // perlin.ixx turb
+    {
+        double accum = 0;
+        double weight = 1;
+        for (int layer = 0; layer < depth; ++layer)
+        {
+            accum += weight * noise(p);
+            weight *= 0.5;
+            p = 2 * p;
+        }
+        return std::fabs(accum);
+    }
+};
+
+struct image_texture_data
+{
+    int width = 0, height = 0;
+    std::vector<float> rgb; // rows from the top
+};
+
+struct texture
+{
+    int kind = RT_TEXTURE_SOLID;
+    color rgb;
+    double inv_scale = 1;
+    int even = -1, odd = -1, image = -1, perlin = -1;
+    double scale = 1;
+};
+
+struct texture_set
+{
+    std::vector<texture> textures;
+    std::vector<image_texture_data> images;
+    std::vector<perlin_table> perlins;
+
+    // texture::value at (u, v) and the point p (texture.ixx): a checker picks its texture by the parity of p's cube,
+    // an image the pixel (u, v) falls in (clamped, v flipped), a marble 0.5 (1 + sin(scale z + 10 turb(p)))
+    color value(int index, double u, double v, const point3& p) const
+    {
+        const texture& t = textures[static_cast<size_t>(index)];
+        switch (t.kind)
+        {
+        case RT_TEXTURE_CHECKER:
+        {
+            const int x = static_cast<int>(std::floor(t.inv_scale * p.x));
+            const int y = static_cast<int>(std::floor(t.inv_scale * p.y));
+            const int z = static_cast<int>(std::floor(t.inv_scale * p.z));
+            return value((x + y + z) % 2 == 0 ? t.even : t.odd, u, v, p);
+        }
+        case RT_TEXTURE_IMAGE:
+        {
+            const image_texture_data& im = images[static_cast<size_t>(t.image)];
+            const double cu = std::clamp(u, 0.0, 1.0);
+            const double cv = 1.0 - std::clamp(v, 0.0, 1.0);
+            const int i = std::min(static_cast<int>(cu * im.width), im.width - 1);
+            const int j = std::min(static_cast<int>(cv * im.height), im.height - 1);
+            const float* px = im.rgb.data() + 3 * (static_cast<size_t>(j) * im.width + i);
+            return {px[0], px[1], px[2]};
+        }
+        case RT_TEXTURE_NOISE:
+        {
+            const double gray =
+                0.5 * (1 + std::sin(t.scale * p.z + 10 * perlins[static_cast<size_t>(t.perlin)].turbulence(p, 7)));
+            return {gray, gray, gray};
+        }
+        default:
+            return t.rgb;
+        }
+    }
+};
+
+// ---- constant_medium.ixx: a volume of smoke of constant density inside a boundary --------------------------------
+struct medium
+{
+    std::unique_ptr<sphere> ball;  // the boundary: a sphere, or
+    std::vector<quad> faces;       // the quads of a convex shape
+    double neg_inv_density = 0;
+    int material = -1;
+
+    // The boundary's nearest hit in t (the quads' nearest one, as a hittable_list of them)
+    std::optional<hit_record> boundary_hit(const ray& r, interval t) const
+    {
+        if (ball)
+        {
+            return ball->hit(r, t);
+        }
+        std::optional<hit_record> closest;
+        for (const quad& q : faces)
+        {
+            if (auto rec = q.hit(r, t))
+            {
+                t.max = rec->t;
+                closest = rec;
+            }
+        }
+        return closest;
+    }
+
+    // The stretch of ray_t inside the volume (constant_medium.ixx:35-62): the boundary's first hit anywhere on the line
+    // and its next one 0.0001 beyond, clamped to ray_t
+    bool stretch(const ray& r, interval ray_t, double& t_in, double& t_out) const
+    {
+        const auto rec1 = boundary_hit(r, interval{-infinity, infinity});
+        if (!rec1)
+        {
+            return false;
+        }
+        const auto rec2 = boundary_hit(r, interval{rec1->t + 0.0001, infinity});
+        if (!rec2)
+        {
+            return false;
+        }
+        t_in = std::max(rec1->t, ray_t.min);
+        t_out = std::min(rec2->t, ray_t.max);
+        if (t_in >= t_out)
+        {
+            return false;
+        }
+        t_in = std::max(t_in, 0.0);
+        return true;
+    }
+
+    // constant_medium::hit: a particle met after an exponential free flight, or nothing
+    std::optional<double> hit(const ray& r, interval ray_t, rng& g) const
+    {
+        double t_in, t_out;
+        if (!stretch(r, ray_t, t_in, t_out))
+        {
+            return std::nullopt;
+        }
+        const double length = r.direction.length();
+        const double distance_inside = (t_out - t_in) * length;
+        const double hit_distance = neg_inv_density * std::log(g.next());
+        if (hit_distance > distance_inside)
+        {
+            return std::nullopt;
+        }
+        return t_in + hit_distance / length;
+    }
 };
 
 inline double reflectance(double cosine, double refraction_index) // material.ixx:101-107 (Schlick)
@@ -619,9 +796,54 @@ struct scene
     world geometry;
     std::vector<material> materials;
     std::vector<light_entry> lights;
+    texture_set textures;
+    std::vector<medium> media;
     rt_camera_desc camera{};
     int sampling = RT_SAMPLING_MATERIAL;
     color sky_bottom, sky_top;
+
+    // What the ray meets first: the closest surface, or a particle of smoke before it (the CPU's world.hit over a list
+    // that holds the volumes; each volume tested against the closest event so far), with the material's color there
+    // in rec.color_at. A particle's record: normal (1, 0, 0), the front, id -1.
+    std::optional<hit_record> closest_event(const ray& r, rng& g) const
+    {
+        auto rec = geometry.hit(r, interval{0.001, infinity});
+        for (const medium& m : media)
+        {
+            if (const auto t = m.hit(r, interval{0.001, rec ? rec->t : infinity}, g))
+            {
+                hit_record particle;
+                particle.t = *t;
+                particle.p = r.at(*t);
+                particle.normal = {1, 0, 0};
+                particle.front_face = true;
+                particle.material = m.material;
+                particle.id = -1;
+                rec = particle;
+            }
+        }
+        if (rec)
+        {
+            const material& mm = materials[static_cast<size_t>(rec->material)];
+            rec->color_at = mm.texture >= 0 ? textures.value(mm.texture, rec->u, rec->v, rec->p) : mm.albedo;
+        }
+        return rec;
+    }
+
+    // The chance that (0.001, t_max) of r crosses every volume without meeting a particle: exp(-sum density * length)
+    double transmittance(const ray& r, double t_max) const
+    {
+        double exponent = 0;
+        for (const medium& m : media)
+        {
+            double t_in, t_out;
+            if (m.stretch(r, interval{0.001, t_max}, t_in, t_out))
+            {
+                exponent += (t_out - t_in) * r.direction.length() / m.neg_inv_density;
+            }
+        }
+        return std::exp(exponent);
+    }
 
     double lights_pdf_value(const point3& origin, const vec3& direction) const
     {
@@ -654,10 +876,44 @@ struct scene
     }
 };
 
-// Builds the oracle's scene from the flat tables. Unsupported features (textures other than solid, media, moving
-// spheres) are reported through `error` and leave the scene empty.
+// Builds the oracle's scene from the flat tables. Tables it cannot render are reported through `error`.
 inline bool make_scene(const rt_scene_desc& d, scene& s, const char** error)
 {
+    for (int64_t i = 0; i < d.image_count; ++i)
+    {
+        const rt_image_desc& im = d.images[i];
+        image_texture_data data;
+        data.width = im.width;
+        data.height = im.height;
+        data.rgb.assign(im.rgb, im.rgb + static_cast<size_t>(im.width) * static_cast<size_t>(im.height) * 3);
+        s.textures.images.push_back(std::move(data));
+    }
+    for (int64_t i = 0; i < d.perlin_count; ++i)
+    {
+        perlin_table p;
+        for (int k = 0; k < 256; ++k)
+        {
+            p.gradients[static_cast<size_t>(k)] = from(d.perlins[i].random_vectors[k]);
+            p.perm_x[static_cast<size_t>(k)] = d.perlins[i].perm_x[k];
+            p.perm_y[static_cast<size_t>(k)] = d.perlins[i].perm_y[k];
+            p.perm_z[static_cast<size_t>(k)] = d.perlins[i].perm_z[k];
+        }
+        s.textures.perlins.push_back(p);
+    }
+    for (int64_t i = 0; i < d.texture_count; ++i)
+    {
+        const rt_texture_desc& t = d.textures[i];
+        texture tt;
+        tt.kind = t.kind;
+        tt.rgb = from(t.rgb);
+        tt.inv_scale = t.inv_scale;
+        tt.even = t.even;
+        tt.odd = t.odd;
+        tt.image = t.image;
+        tt.perlin = t.perlin;
+        tt.scale = t.scale;
+        s.textures.textures.push_back(tt);
+    }
     for (int64_t i = 0; i < d.material_count; ++i)
     {
         const rt_material_desc& m = d.materials[i];
@@ -677,12 +933,13 @@ inline bool make_scene(const rt_scene_desc& d, scene& s, const char** error)
         }
         else if (m.kind != RT_DIELECTRIC)
         {
-            if (m.texture < 0 || m.texture >= d.texture_count || d.textures[m.texture].kind != RT_TEXTURE_SOLID)
+            if (m.texture < 0 || m.texture >= d.texture_count)
             {
-                *error = "the oracle renders solid-color textures only";
+                *error = "a material refers to a texture that doesn't exist";
                 return false;
             }
             mm.albedo = from(d.textures[m.texture].rgb);
+            mm.texture = d.textures[m.texture].kind == RT_TEXTURE_SOLID ? -1 : m.texture;
         }
         s.materials.push_back(mm);
     }
@@ -692,6 +949,8 @@ inline bool make_scene(const rt_scene_desc& d, scene& s, const char** error)
         const rt_sphere_desc& sp = d.spheres[i];
         const point3 c = from(sp.center);
         s.geometry.spheres.emplace_back(c, c + from(sp.displacement), sp.radius, sp.material, id++);
+        s.geometry.spheres.back().uv_cos = sp.uv_cos;
+        s.geometry.spheres.back().uv_sin = sp.uv_sin;
     }
     for (int64_t i = 0; i < d.quad_count; ++i)
     {
@@ -710,10 +969,25 @@ inline bool make_scene(const rt_scene_desc& d, scene& s, const char** error)
                                               vertex(mesh.indices[3 * t + 2]), mesh.material, id++);
         }
     }
-    if (d.medium_count > 0)
+    for (int64_t i = 0; i < d.medium_count; ++i)
     {
-        *error = "the oracle does not render media";
-        return false;
+        const rt_medium_desc& md = d.media[i];
+        medium m;
+        m.neg_inv_density = md.neg_inv_density;
+        m.material = md.material;
+        if (md.boundary == RT_BOUNDARY_SPHERE)
+        {
+            const point3 c = from(md.sphere.center);
+            m.ball = std::make_unique<sphere>(c, c + from(md.sphere.displacement), md.sphere.radius, -1, -1);
+        }
+        else
+        {
+            for (int64_t k = 0; k < md.quad_count; ++k)
+            {
+                m.faces.emplace_back(from(md.quads[k].q), from(md.quads[k].u), from(md.quads[k].v), -1, -1);
+            }
+        }
+        s.media.push_back(std::move(m));
     }
     double cdf = 0;
     for (int64_t i = 0; i < d.light_count; ++i)
@@ -788,15 +1062,15 @@ inline color ray_color(const scene& s, const ray& r, int depth, rng& g, counters
     {
         return {0, 0, 0};
     }
-    const auto rec = s.geometry.hit(r, interval{0.001, infinity});
+    const auto rec = s.closest_event(r, g);
     ++n.rays;
     if (!rec)
     {
         return s.sky(r.direction);
     }
     const material& m = s.materials[static_cast<size_t>(rec->material)];
-    // material::emitted: a lamp glows on its front side only (material.ixx:125-128)
-    const color emitted = m.kind == RT_DIFFUSE_LIGHT && rec->front_face ? m.albedo : color{0, 0, 0};
+    // material::emitted: a lamp glows on its front side only (material.ixx:125-128), its texture's color there
+    const color emitted = m.kind == RT_DIFFUSE_LIGHT && rec->front_face ? rec->color_at : color{0, 0, 0};
     switch (m.kind)
     {
     case RT_DIFFUSE_LIGHT:
@@ -839,7 +1113,7 @@ inline color ray_color(const scene& s, const ray& r, int depth, rng& g, counters
         {
             return {0, 0, 0};
         }
-        return m.albedo * (sp / pdf_value) * ray_color(s, ray{rec->p, direction, r.time}, depth - 1, g, n);
+        return rec->color_at * (sp / pdf_value) * ray_color(s, ray{rec->p, direction, r.time}, depth - 1, g, n);
     };
     int strategy = s.sampling;
     if (strategy == RT_SAMPLING_MIXTURE && !matte)

@@ -37,7 +37,7 @@ inline std::vector<lamp> build_lamps(const scene& s)
     for (const sphere& sp : s.geometry.spheres)
     {
         const material& m = s.materials[static_cast<size_t>(sp.material)];
-        if (m.kind == RT_DIFFUSE_LIGHT && sp.center.direction.length_squared() == 0)
+        if (m.kind == RT_DIFFUSE_LIGHT && m.texture < 0 && sp.center.direction.length_squared() == 0)
         {
             lamps.push_back({RT_LIGHT_SPHERE, sp.center.origin, {}, {}, {}, sp.radius, m.albedo, sp.id});
         }
@@ -45,7 +45,7 @@ inline std::vector<lamp> build_lamps(const scene& s)
     for (const quad& q : s.geometry.quads)
     {
         const material& m = s.materials[static_cast<size_t>(q.material)];
-        if (m.kind == RT_DIFFUSE_LIGHT)
+        if (m.kind == RT_DIFFUSE_LIGHT && m.texture < 0)
         {
             lamps.push_back({RT_LIGHT_QUAD, q.q, q.u, q.v, q.normal, q.area, m.albedo, q.id});
         }
@@ -229,7 +229,7 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
     const int lights = q.light_count();
     while (true)
     {
-        const auto rec = s.geometry.hit(r, interval{0.001, infinity});
+        const auto rec = s.closest_event(r, g);
         ++n.rays;
         if (!rec)
         {
@@ -249,7 +249,9 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
             const double w = bsdf_pdf > 0 ? bsdf_weight(q.combination, bsdf_pdf, p_light) : 1.0;
             return radiance + w * (throughput * le);
         }
-        const material& m = s.materials[static_cast<size_t>(rec->material)];
+        // The material with its color at the hit (its texture there; a metal's albedo)
+        material m = s.materials[static_cast<size_t>(rec->material)];
+        m.albedo = rec->color_at;
         if (m.kind == RT_DIFFUSE_LIGHT)
         {
             double w = 1;
@@ -407,9 +409,11 @@ inline color quality_sample(const quality_scene& q, ray r, rng& g, counters& n)
         if (lit)
         {
             ++n.shadow_rays;
-            if (!occluded(s, ray{rec->p, light_dir, r.time}, light_distance, skip))
+            const ray shadow{rec->p, light_dir, r.time};
+            if (!occluded(s, shadow, light_distance, skip))
             {
-                radiance += contribution;
+                // through smoke, with the chance of crossing it (shadow.cuh:129-165)
+                radiance += s.transmittance(shadow, light_distance) * contribution;
             }
         }
         if (!scattered)

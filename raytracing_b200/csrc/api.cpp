@@ -136,46 +136,7 @@ rt_status rt_is_convex(const rt_quad_desc* quads, int64_t count, int32_t* convex
         {
             need(quads, "quads");
         }
-        // renderer.h:163-168: for every quad, all the corners of all the quads lie on one side of its plane, or on it
-        // within 1e-9 of the largest coordinate
-        double largest = 0;
-        std::vector<rt_vec3> corners;
-        for (int64_t i = 0; i < count; ++i)
-        {
-            const rt_quad_desc& q = quads[i];
-            const rt_vec3 c[4] = {q.q,
-                                  {q.q.x + q.u.x, q.q.y + q.u.y, q.q.z + q.u.z},
-                                  {q.q.x + q.v.x, q.q.y + q.v.y, q.q.z + q.v.z},
-                                  {q.q.x + q.u.x + q.v.x, q.q.y + q.u.y + q.v.y, q.q.z + q.u.z + q.v.z}};
-            for (const rt_vec3& v : c)
-            {
-                corners.push_back(v);
-                largest = std::fmax(largest, std::fmax(std::fabs(v.x), std::fmax(std::fabs(v.y), std::fabs(v.z))));
-            }
-        }
-        const double tolerance = 1e-9 * std::fmax(1.0, largest);
-        bool ok = true;
-        for (int64_t i = 0; i < count && ok; ++i)
-        {
-            const rt_quad_desc& q = quads[i];
-            const rt_vec3 n{q.u.y * q.v.z - q.u.z * q.v.y, q.u.z * q.v.x - q.u.x * q.v.z, q.u.x * q.v.y - q.u.y * q.v.x};
-            const double len = std::sqrt(n.x * n.x + n.y * n.y + n.z * n.z);
-            if (!(len > 0))
-            {
-                ok = false;
-                break;
-            }
-            bool above = false;
-            bool below = false;
-            for (const rt_vec3& c : corners)
-            {
-                const double s = ((c.x - q.q.x) * n.x + (c.y - q.q.y) * n.y + (c.z - q.q.z) * n.z) / len;
-                above = above || s > tolerance;
-                below = below || s < -tolerance;
-            }
-            ok = !(above && below);
-        }
-        *convex = ok ? 1 : 0;
+        *convex = rtb::is_convex(quads, count) ? 1 : 0;
     });
 }
 

@@ -7,6 +7,8 @@
 
 #include <cstdint>
 
+#include <vector_types.h>
+
 #ifdef __CUDACC__
 #define RTB_HD __host__ __device__
 #else
@@ -90,8 +92,13 @@ struct alignas(16) material12
     int32_t lobe;    // RT_MICROFACET_NONE, _CONDUCTOR (the material is a metal of fuzz 0), _GLOSS (a lambertian)
     float alpha;     // the GGX width r^2
     float roughness; // r: the energy table's axis
-    float pad0, pad1, pad2;
+    int32_t texture; // -1: the color is (r, g, b); otherwise its texture (a checker, an image or a noise)
+    int32_t texture_needs; // texture_needs_uv | texture_needs_point: what reading the texture needs of the hit
+    float pad2;
 };
+
+constexpr int32_t texture_needs_uv = 1;    // an image in the texture: the hit's (u, v)
+constexpr int32_t texture_needs_point = 2; // a checker: the hit point, moved exactly onto a sphere
 
 // The environment map (src/gpu/environment_data.h): texels with their sampling density, the alias table's bins, the
 // rows' cosines, and the yaw
@@ -157,6 +164,62 @@ struct camera_params
     int32_t sampling;
 };
 
+// A texture (src/gpu/texture.cuh:10-19): 32 bytes, two 16-byte loads. checker: `even`, `odd` are texture indices
+// smaller than its own and inv_scale the cubes' 1 / side; image: `table` indexes the images; noise: the noise tables
+struct alignas(16) texture8
+{
+    int32_t kind; // RT_TEXTURE_*
+    int32_t even, odd;
+    int32_t table;
+    float r, g, b;
+    float inv_scale;
+};
+
+// Where an image's texels are: texels[offset + j * width + i] is pixel (i, j), rows from the top
+struct alignas(16) image_info
+{
+    int32_t offset, width, height, pad;
+};
+
+// A marble texture (the CPU's noise_texture with its own perlin tables, perlin.ixx): 256 gradients (16 bytes each),
+// the three permutations of 0..255, and the stripes' frequency
+struct alignas(16) noise_table
+{
+    float4 gradients[256];
+    uint8_t perm_x[256];
+    uint8_t perm_y[256];
+    uint8_t perm_z[256];
+    float scale;
+    float pad[3];
+};
+
+// A sphere's texture frame (sphere.cuh:119-168): the turn of the rotate_y instances around it (u of its texture
+// coordinates is read in its own coordinates), and |c|^2 - r^2 and the bound below which a checker's point is moved
+// onto the sphere exactly (one Newton step; 0: never)
+struct alignas(16) sphere_frame
+{
+    float cos_theta, sin_theta;
+    float k, limit;
+};
+
+// At most this many volumes of smoke in a scene: a vertex draws one number per volume, from its dimension blocks 4-15
+constexpr int max_media = 48;
+
+// A volume of smoke (src/gpu/constant_medium.cuh:9-27): a box around it over the whole shutter, -1/density, its
+// isotropic material, and its boundary: a sphere (center at time 0, radius, motion) when quad_count is 0, otherwise
+// boundary quads [first_quad, first_quad + quad_count). 64 bytes.
+struct alignas(16) medium16
+{
+    float lo_x, lo_y, lo_z, neg_inv_density;
+    float hi_x, hi_y, hi_z;
+    int32_t material;
+    float cx, cy, cz, radius;
+    float dx, dy, dz;
+    int32_t first_quad;
+    int32_t quad_count;
+    int32_t pad[3];
+};
+
 // The resident scene as the kernels see it
 struct scene_view
 {
@@ -180,5 +243,18 @@ struct scene_view
     int32_t has_environment; // misses see the map (the NEE/MIS integrator only), not the camera's sky
     int32_t flat;            // a small scene of spheres and quads: closest hits test every primitive, no tree walk
     environment_view env;
+    // Textures, motion and smoke (the second book); all empty in a scene without them
+    const texture8* textures;
+    const image_info* images;
+    const float4* texels;
+    const noise_table* noises;
+    const float4* sphere_motion;      // per sphere (leaf order): the center's displacement over the shutter
+    const sphere_frame* sphere_frames; // per sphere (leaf order), for textured spheres
+    const medium16* media;
+    const quad12* boundary_quads;
+    int32_t has_motion;      // some sphere moves: rays carry a time, spheres are where they are at it
+    int32_t medium_count;
+    int32_t medium_base;     // the global id of a particle of media[0]: right after the surface primitives
+    int32_t has_textures;    // some material reads a texture (not one solid color)
 };
 } // namespace rtb

@@ -93,6 +93,9 @@ private:
 // Checks a scene's tables before anything is built (the reference's validate, renderer.cu:688-900); throws rt_error
 void validate(const rt_scene_desc& desc);
 
+// Whether the quads bound a convex shape (renderer.h:163-168 is_convex), the boundary a volume of smoke may have
+bool is_convex(const rt_quad_desc* quads, int64_t count);
+
 // The camera in the kernels' form: the pixel grid relative to the center subtracted in double (renderer.cu:512-532)
 camera_params to_camera(const rt_camera_desc& desc);
 
@@ -128,6 +131,14 @@ private:
     device_array<env_texel> env_texels_;
     device_array<alias_bin> env_bins_;
     device_array<float> env_row_cos_;
+    device_array<float4> sphere_motion_;
+    device_array<sphere_frame> sphere_frames_;
+    device_array<texture8> textures_;
+    device_array<image_info> images_;
+    device_array<float4> texels_;
+    device_array<noise_table> noises_;
+    device_array<medium16> media_;
+    device_array<quad12> boundary_quads_;
 };
 
 // The environment map's tables (environment_table.cu:81-226 build_environment): texels with their densities Y/S,

@@ -102,8 +102,11 @@ struct sampler
 // The fixed dimension blocks of a vertex: block 0 the material's own sample (direction u0 u1, lobe or mixture
 // choice u2, the lights list's pick u3; a books' vertex that aims at the lights list takes the point from u0 u1, which
 // its direction then does not use, so a books' vertex draws one block), blocks 2-3 the NEE light sample (the pick, a
-// lamp's point or the map's bin bits, coin and cell position)
+// lamp's point or the map's bin bits, coin and cell position), blocks 4-15 the free flights through the volumes of
+// smoke, one number per volume. At depth 0, block 0 is the camera ray's (stratum jitter, lens) and block 1's first
+// number the ray's time in a scene where something moves.
 constexpr int block_material = 0;
+constexpr int block_time = 1;
 constexpr int block_nee = 2;
 
 // ---- sampling of directions (random.cuh:95-140, material.cuh:55-64) --------------------------------------------
@@ -325,10 +328,29 @@ struct fetch_counts
     uint32_t triangles = 0;
 };
 
+// Sphere i (leaf order) where it is at the ray's time: its center moved by time * displacement in a scene where
+// something moves (moving_sphere::at, sphere.cuh)
+// FEATURES (here and below): the code of the second book's features (moving spheres, textures, smoke) is compiled in;
+// the render kernels of scenes without them are compiled with FEATURES = false and keep none of its registers
+template <bool FEATURES = true>
+__device__ __forceinline__ float4 sphere_at(const scene_view& S, int i, float time)
+{
+    float4 s = __ldg(reinterpret_cast<const float4*>(S.spheres + i));
+    if (FEATURES && S.has_motion)
+    {
+        const float4 m = __ldg(S.sphere_motion + i);
+        s.x = fmaf(time, m.x, s.x);
+        s.y = fmaf(time, m.y, s.y);
+        s.z = fmaf(time, m.z, s.z);
+    }
+    return s;
+}
+
 // The leaf's primitives against the ray, shrinking hit.t; true at the first hit for a shadow ray
-template <bool SHADOW, bool COUNT>
-__device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 o, float3 d, float inverse_a, int from,
-                                          bool inward, int skip, hit_info& hit, fetch_counts* counts)
+template <bool SHADOW, bool COUNT, bool FEATURES>
+__device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 o, float3 d, float time,
+                                          float inverse_a, int from, bool inward, int skip, hit_info& hit,
+                                          fetch_counts* counts)
 {
     const int kind = leaf_kind(link);
     const int count = leaf_count(link);
@@ -347,7 +369,7 @@ __device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 
             {
                 continue;
             }
-            const float4 s = __ldg(reinterpret_cast<const float4*>(S.spheres + i));
+            const float4 s = sphere_at<FEATURES>(S, i, time);
             float t;
             bool entering;
             if (hit_sphere(s, o, d, inverse_a, t_min, hit.t, own, t, entering))
@@ -426,9 +448,9 @@ constexpr int search_any = 0;
 constexpr int search_flat = 1;
 constexpr int search_tree = 2;
 
-template <bool SHADOW, bool COUNT = false, int SEARCH = search_any>
-__device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d, float t_max, int from, bool inward,
-                                         int skip, hit_info& hit, fetch_counts* counts = nullptr)
+template <bool SHADOW, bool COUNT = false, int SEARCH = search_any, bool FEATURES = true>
+__device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d, float time, float t_max, int from,
+                                         bool inward, int skip, hit_info& hit, fetch_counts* counts = nullptr)
 {
     hit.id = -1;
     hit.t = t_max;
@@ -449,7 +471,7 @@ __device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d
             {
                 continue;
             }
-            const float4 s = __ldg(reinterpret_cast<const float4*>(S.spheres + i));
+            const float4 s = sphere_at<FEATURES>(S, i, time);
             float t;
             bool entering;
             if (hit_sphere(s, o, d, inverse_a, t_min, hit.t, own, t, entering))
@@ -557,7 +579,7 @@ __device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d
         }
         while (leaf < 0)
         {
-            if (test_leaf<SHADOW, COUNT>(S, leaf, o, d, inverse_a, from, inward, skip, hit, counts))
+            if (test_leaf<SHADOW, COUNT, FEATURES>(S, leaf, o, d, time, inverse_a, from, inward, skip, hit, counts))
             {
                 return true;
             }
@@ -570,6 +592,208 @@ __device__ __forceinline__ bool traverse(const scene_view& S, float3 o, float3 d
         }
     }
     return hit.id >= 0;
+}
+
+// ---- volumes of smoke (constant_medium.cuh:29-120, camera.cuh:259-284, shadow.cuh:129-165) -------------------------
+constexpr int block_media = 4; // max_media volumes: one number each from blocks 4-15 of a vertex
+
+// Where the ray's line crosses the medium's boundary: the sphere's two roots, the sphere where it is at the ray's time,
+// kept only if the chord is longer than 0.0001; or the nearest and the farthest plane of the boundary quads the line
+// meets inside them
+__device__ bool boundary_crossings(const scene_view& S, const medium16& m, float3 o, float3 d, float time,
+                                   float inverse_a, float& t_in, float& t_out)
+{
+    if (m.quad_count == 0)
+    {
+        const float4 s = make_float4(fmaf(time, m.dx, m.cx), fmaf(time, m.dy, m.cy), fmaf(time, m.dz, m.cz), m.radius);
+        return sphere_roots(s, o, d, inverse_a, t_in, t_out) && t_out - t_in > 0.0001f;
+    }
+    t_in = infinity_f;
+    t_out = -infinity_f;
+    for (int i = m.first_quad; i < m.first_quad + m.quad_count; ++i)
+    {
+        float t;
+        bool front;
+        if (hit_quad(load_quad(S.boundary_quads, i), o, d, -infinity_f, infinity_f, t, front))
+        {
+            t_in = fminf(t_in, t);
+            t_out = fmaxf(t_out, t);
+        }
+    }
+    return t_out - t_in >= 0.0001f;
+}
+
+// The stretch [t_in, t_out] of (t_min, t_max) that lies inside the medium, or false: its box first (a ray that misses
+// the box misses the volume), then the boundary's crossings
+__device__ __forceinline__ bool medium_stretch(const scene_view& S, const medium16& m, float3 o, float3 d, float time,
+                                               float inverse_a, float3 inv, float3 os, float t_max, float& t_in,
+                                               float& t_out)
+{
+    const float a0 = fmaf(m.lo_x, inv.x, -os.x), a1 = fmaf(m.hi_x, inv.x, -os.x);
+    const float b0 = fmaf(m.lo_y, inv.y, -os.y), b1 = fmaf(m.hi_y, inv.y, -os.y);
+    const float c0 = fmaf(m.lo_z, inv.z, -os.z), c1 = fmaf(m.hi_z, inv.z, -os.z);
+    const float enter = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), t_min));
+    const float exit = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), t_max));
+    if (!(enter <= exit))
+    {
+        return false;
+    }
+    float line_in, line_out;
+    if (!boundary_crossings(S, m, o, d, time, inverse_a, line_in, line_out))
+    {
+        return false;
+    }
+    t_in = fmaxf(line_in, t_min);
+    t_out = fminf(line_out, t_max);
+    if (!(t_in < t_out))
+    {
+        return false;
+    }
+    t_in = fmaxf(t_in, 0.0f);
+    return true;
+}
+
+// What the ray meets first: the closest surface `hit`, or a particle of smoke in front of it (closest_event,
+// camera.cuh:259-284). Each volume, in the list's order, against the closest event so far: a free flight of
+// -log(u) / density from where the ray enters it (medium_collision, constant_medium.cuh:86-120), u drawn from the
+// vertex's media blocks.
+// (Not inlined, like transmittance and texture_value: their registers stay out of the render loop's, which scenes
+// without smoke or textures never call them from.)
+__device__ __noinline__ void media_event(const scene_view& S, float3 o, float3 d, float time, const sampler& rng,
+                                         int depth,
+                            hit_info& hit)
+{
+    const float inverse_a = 1.0f / length_squared(d);
+    const float3 inv = make_float3(safe_inverse(d.x), safe_inverse(d.y), safe_inverse(d.z));
+    const float3 os = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+    const float length = sqrtf(length_squared(d));
+    float4 u = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (int k = 0; k < S.medium_count; ++k)
+    {
+        if ((k & 3) == 0)
+        {
+            u = rng.draw(depth, block_media + (k >> 2));
+        }
+        const medium16 m = S.media[k];
+        float t_in, t_out;
+        if (!medium_stretch(S, m, o, d, time, inverse_a, inv, os, hit.t, t_in, t_out))
+        {
+            continue;
+        }
+        const float uk = (k & 3) == 0 ? u.x : (k & 3) == 1 ? u.y : (k & 3) == 2 ? u.z : u.w;
+        const float distance = m.neg_inv_density * logf(uk);
+        if (distance > (t_out - t_in) * length)
+        {
+            continue; // through without meeting a particle
+        }
+        hit = {S.medium_base + k, t_in + distance / length, true};
+    }
+}
+
+// The chance that (t_min, t_max) of the ray crosses every volume without meeting a particle: the expected value of
+// media_event's free-flight test over exactly the stretch it would test (transmittance, shadow.cuh:129-165)
+__device__ __noinline__ float transmittance(const scene_view& S, float3 o, float3 d, float time, float t_max)
+{
+    const float inverse_a = 1.0f / length_squared(d);
+    const float3 inv = make_float3(safe_inverse(d.x), safe_inverse(d.y), safe_inverse(d.z));
+    const float3 os = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+    const float length = sqrtf(length_squared(d));
+    float exponent = 0.0f;
+    for (int k = 0; k < S.medium_count; ++k)
+    {
+        const medium16 m = S.media[k];
+        float t_in, t_out;
+        if (medium_stretch(S, m, o, d, time, inverse_a, inv, os, t_max, t_in, t_out))
+        {
+            exponent += (t_out - t_in) * length / m.neg_inv_density;
+        }
+    }
+    return expf(exponent);
+}
+
+// ---- textures (texture.cuh, perlin.cuh: the books' solid, checker, image and marble textures) ------------------
+// Perlin noise with Hermite smoothing of the cell's coordinates and the trilinear sum of the eight corners'
+// gradient dot products (perlin.ixx noise); turbulence: 7 octaves of it, each at twice the frequency and half the
+// weight, absolute value
+__device__ float perlin_noise(const noise_table& n, float3 p)
+{
+    const float fx = floorf(p.x), fy = floorf(p.y), fz = floorf(p.z);
+    const int i = static_cast<int>(fx), j = static_cast<int>(fy), k = static_cast<int>(fz);
+    const float u = p.x - fx, v = p.y - fy, w = p.z - fz;
+    const float uu = u * u * (3.0f - 2.0f * u);
+    const float vv = v * v * (3.0f - 2.0f * v);
+    const float ww = w * w * (3.0f - 2.0f * w);
+    float accum = 0.0f;
+#pragma unroll
+    for (int di = 0; di < 2; ++di)
+    {
+        const int px = n.perm_x[(i + di) & 255];
+        const float wx = di == 0 ? 1.0f - uu : uu;
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj)
+        {
+            const int py = n.perm_y[(j + dj) & 255];
+            const float wy = dj == 0 ? 1.0f - vv : vv;
+#pragma unroll
+            for (int dk = 0; dk < 2; ++dk)
+            {
+                const int pz = n.perm_z[(k + dk) & 255];
+                const float wz = dk == 0 ? 1.0f - ww : ww;
+                const float4 g = n.gradients[px ^ py ^ pz];
+                const float dot_g = g.x * (u - static_cast<float>(di)) + g.y * (v - static_cast<float>(dj)) +
+                                    g.z * (w - static_cast<float>(dk));
+                accum += wx * wy * wz * dot_g;
+            }
+        }
+    }
+    return accum;
+}
+
+__device__ float turbulence(const noise_table& n, float3 p)
+{
+    float accum = 0.0f;
+    float weight = 1.0f;
+    for (int layer = 0; layer < 7; ++layer)
+    {
+        accum += weight * perlin_noise(n, p);
+        weight *= 0.5f;
+        p = 2.0f * p;
+    }
+    return fabsf(accum);
+}
+
+// The texture's color at the hit (texture_value, texture.cuh:60-110): a checker is walked down to the texture of the
+// point's cube (its textures come before it, so the walk ends); an image is read at (u, v) clamped to [0, 1], v
+// flipped, the pixel they fall in; a marble is 0.5 (1 + sin(scale z + 10 turbulence(p))) in every channel
+__device__ __noinline__ float3 texture_value(const scene_view& S, int index, float u, float v, float3 p)
+{
+    texture8 t = S.textures[index];
+    while (t.kind == RT_TEXTURE_CHECKER)
+    {
+        const int x = static_cast<int>(floorf(t.inv_scale * p.x));
+        const int y = static_cast<int>(floorf(t.inv_scale * p.y));
+        const int z = static_cast<int>(floorf(t.inv_scale * p.z));
+        t = S.textures[(x + y + z) % 2 == 0 ? t.even : t.odd];
+    }
+    if (t.kind == RT_TEXTURE_IMAGE)
+    {
+        const image_info im = S.images[t.table];
+        const float cu = fminf(fmaxf(u, 0.0f), 1.0f);
+        const float fv = 1.0f - fminf(fmaxf(v, 0.0f), 1.0f);
+        const int column = static_cast<int>(cu * static_cast<float>(im.width));
+        const int row = static_cast<int>(fv * static_cast<float>(im.height));
+        const int i = column < im.width - 1 ? column : im.width - 1;
+        const int j = row < im.height - 1 ? row : im.height - 1;
+        const float4 c = __ldg(S.texels + im.offset + j * im.width + i);
+        return make_float3(c.x, c.y, c.z);
+    }
+    if (t.kind == RT_TEXTURE_NOISE)
+    {
+        const noise_table& n = S.noises[t.table];
+        const float gray = 0.5f * (1.0f + sinf(n.scale * p.z + 10.0f * turbulence(n, p)));
+        return make_float3(gray, gray, gray);
+    }
+    return make_float3(t.r, t.g, t.b);
 }
 
 // ---- the books' lights list (lights.cuh:49-227) ---------------------------------------------------------------
@@ -802,6 +1026,7 @@ struct path_state
     int depth;       // rays traced so far in this sample (the next vertex's depth in the RNG counter)
     int from;
     bool inward;
+    float time;      // the moment in the shutter the sample's rays are at (0 in a scene where nothing moves)
 };
 
 // The hit as the shading needs it: point, outward normal, material, the hit's side
@@ -810,34 +1035,111 @@ struct surface
     float3 p;
     float3 outward;
     float3 normal;
+    float3 color; // the material's color here: its texture read at the hit, or its one solid color
     int material;
+    int from;     // the next ray's `from`: the hit primitive, or -1 after a particle of smoke (which has no surface)
 };
 
-__device__ __forceinline__ surface surface_at(const scene_view& S, const path_state& ps, const hit_info& h)
+// The texture coordinates of a point of a sphere (sphere.cuh:119-135): the longitude and latitude of its outward
+// normal turned back by the instances' turn, u from -x around y, v from the south pole
+__device__ __forceinline__ void sphere_uv(float3 outward, const sphere_frame& f, float& u, float& v)
+{
+    const float nx = f.cos_theta * outward.x - f.sin_theta * outward.z;
+    const float nz = f.sin_theta * outward.x + f.cos_theta * outward.z;
+    const float phi = atan2f(-nz, nx) + pi_f;
+    const float theta = acosf(fminf(fmaxf(-outward.y, -1.0f), 1.0f));
+    u = phi * (0.5f * inverse_pi_f);
+    v = theta * inverse_pi_f;
+}
+
+// The hit point moved onto the sphere by one Newton step along the outward normal, for a checker to read
+// (onto_sphere, sphere.cuh:137-168): f = |p|^2 - 2 p.c + k with k = |c|^2 - r^2 from the host, taken only while its
+// rounding bound stays below the frame's limit 2 r |c|
+__device__ __forceinline__ float3 onto_sphere(float3 p, float3 outward, float4 ball, const sphere_frame& f)
+{
+    const float3 c = make_float3(ball.x, ball.y, ball.z);
+    const float p_p = dot(p, p);
+    const float p_c = dot(p, c);
+    if (!(p_p + 2.0f * fabsf(p_c) + fabsf(f.k) < f.limit))
+    {
+        return p;
+    }
+    const float value = p_p - 2.0f * p_c + f.k;
+    return p - (value / (2.0f * fabsf(ball.w))) * outward;
+}
+
+// The hit as the shading needs it (surface_at, camera.cuh:171-253), and the material there with its color
+template <bool FEATURES = true>
+__device__ __forceinline__ surface surface_at(const scene_view& S, const path_state& ps, const hit_info& h,
+                                              material12& m)
 {
     surface s;
-    s.material = __ldg(S.prim_material + h.id);
-    if (h.id < S.quad_base)
+    s.from = h.id;
+    float u = 0.0f, v = 0.0f;
+    float4 ball = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    bool on_sphere = false;
+    if (FEATURES && h.id >= S.medium_base)
     {
-        const float4 sp = __ldg(reinterpret_cast<const float4*>(S.spheres + h.id));
+        // A particle of smoke (constant_medium::hit): any normal and side will do, the CPU's (1, 0, 0) and the front
         s.p = ps.o + h.t * ps.d;
-        s.outward = (1.0f / fabsf(sp.w)) * (s.p - make_float3(sp.x, sp.y, sp.z));
-    }
-    else if (h.id < S.triangle_base)
-    {
-        // The quad's point as the CPU computes it, t * d rounded, then the sum (camera.cuh:175-195 at_unfused)
-        const quad_v q = load_quad(S.quads, h.id - S.quad_base);
-        s.p = make_float3(__fadd_rn(ps.o.x, __fmul_rn(h.t, ps.d.x)), __fadd_rn(ps.o.y, __fmul_rn(h.t, ps.d.y)),
-                          __fadd_rn(ps.o.z, __fmul_rn(h.t, ps.d.z)));
-        s.outward = q.n;
+        s.outward = make_float3(1.0f, 0.0f, 0.0f);
+        s.normal = s.outward;
+        s.material = S.media[h.id - S.medium_base].material;
+        s.from = -1;
+        m = S.materials[s.material];
     }
     else
     {
-        const triangle_v tr = load_triangle(S.triangles, h.id - S.triangle_base);
-        s.p = ps.o + h.t * ps.d;
-        s.outward = unit_vector(cross(tr.e1, tr.e2));
+        s.material = __ldg(S.prim_material + h.id);
+        m = S.materials[s.material];
+        if (h.id < S.quad_base)
+        {
+            ball = sphere_at<FEATURES>(S, h.id, ps.time);
+            on_sphere = true;
+            s.p = ps.o + h.t * ps.d;
+            s.outward = (1.0f / fabsf(ball.w)) * (s.p - make_float3(ball.x, ball.y, ball.z));
+        }
+        else if (h.id < S.triangle_base)
+        {
+            // The quad's point as the CPU computes it, t * d rounded, then the sum (camera.cuh:175-195 at_unfused)
+            const quad_v q = load_quad(S.quads, h.id - S.quad_base);
+            s.p = make_float3(__fadd_rn(ps.o.x, __fmul_rn(h.t, ps.d.x)), __fadd_rn(ps.o.y, __fmul_rn(h.t, ps.d.y)),
+                              __fadd_rn(ps.o.z, __fmul_rn(h.t, ps.d.z)));
+            s.outward = q.n;
+            if (FEATURES && m.texture >= 0 && (m.texture_needs & texture_needs_uv) != 0)
+            {
+                // quad_uv (quad.cuh:86-94): alpha and beta of the point, from hit_quad's expressions
+                const float3 rel = h.t * ps.d - (q.q - ps.o);
+                u = dot(rel, q.a);
+                v = dot(rel, q.b);
+            }
+        }
+        else
+        {
+            const triangle_v tr = load_triangle(S.triangles, h.id - S.triangle_base);
+            s.p = ps.o + h.t * ps.d;
+            s.outward = unit_vector(cross(tr.e1, tr.e2));
+        }
+        s.normal = h.front ? s.outward : -s.outward;
     }
-    s.normal = h.front ? s.outward : -s.outward;
+    s.color = make_float3(m.r, m.g, m.b);
+    if (FEATURES && m.texture >= 0)
+    {
+        float3 point = s.p;
+        if (on_sphere && (m.texture_needs & (texture_needs_uv | texture_needs_point)) != 0)
+        {
+            const sphere_frame f = S.sphere_frames[h.id];
+            if (m.texture_needs & texture_needs_uv)
+            {
+                sphere_uv(s.outward, f, u, v);
+            }
+            if (m.texture_needs & texture_needs_point)
+            {
+                point = onto_sphere(s.p, s.outward, ball, f);
+            }
+        }
+        s.color = texture_value(S, m.texture, u, v, point);
+    }
     return s;
 }
 
@@ -849,6 +1151,7 @@ enum class step_result
 
 // One segment of a books' path (camera.cuh:364-437 trace_ray with diffuse_bounce 304-359 and scatter
 // material.cuh:84-126), after its closest hit
+template <bool FEATURES = true>
 __device__ __forceinline__ step_result shade_books(const scene_view& S, const camera_params& cam, const sampler& rng,
                                                    path_state& ps, const hit_info& h, float3& sample)
 {
@@ -857,9 +1160,9 @@ __device__ __forceinline__ step_result shade_books(const scene_view& S, const ca
         sample = ps.throughput * sky(cam, ps.d);
         return step_result::done;
     }
-    const surface s = surface_at(S, ps, h);
-    const material12 m = S.materials[s.material];
-    const float3 albedo = make_float3(m.r, m.g, m.b);
+    material12 m;
+    const surface s = surface_at<FEATURES>(S, ps, h, m);
+    const float3 albedo = s.color;
     float3 direction;
     if (m.kind == RT_DIFFUSE_LIGHT)
     {
@@ -867,13 +1170,20 @@ __device__ __forceinline__ step_result shade_books(const scene_view& S, const ca
         return step_result::done;
     }
     const float4 u = rng.draw(ps.depth, block_material);
-    if (m.kind == RT_LAMBERTIAN)
+    if (m.kind == RT_LAMBERTIAN || m.kind == RT_ISOTROPIC)
     {
+        // A diffuse bounce (diffuse_bounce, camera.cuh:300-359): a matte surface, or a particle of smoke, which keeps
+        // its own density (1/(4 pi) everywhere) except under the lights strategy (isotropic::mixes_in_lights is false)
+        const bool matte = m.kind == RT_LAMBERTIAN;
         int strategy = cam.sampling;
+        if (!matte && strategy != RT_SAMPLING_LIGHTS)
+        {
+            strategy = RT_SAMPLING_MATERIAL;
+        }
         if (strategy == RT_SAMPLING_MATERIAL)
         {
-            direction = around(s.normal, random_cosine_direction(u.x, u.y));
-            if (!(dot(s.normal, direction) > 0.0f))
+            direction = matte ? around(s.normal, random_cosine_direction(u.x, u.y)) : random_unit_vector(u.x, u.y);
+            if (matte && !(dot(s.normal, direction) > 0.0f))
             {
                 sample = make_float3(0.0f, 0.0f, 0.0f);
                 return step_result::done;
@@ -896,11 +1206,11 @@ __device__ __forceinline__ step_result shade_books(const scene_view& S, const ca
                 direction = strategy == RT_SAMPLING_UNIFORM ? random_unit_vector(u.x, u.y)
                                                             : around(s.normal, random_cosine_direction(u.x, u.y));
             }
-            const float p_scatter = cosine_density(s.normal, direction);
+            const float p_scatter = matte ? cosine_density(s.normal, direction) : uniform_sphere_density;
             float p = uniform_sphere_density;
             if (strategy != RT_SAMPLING_UNIFORM)
             {
-                const float p_lights = lights_pdf_value(S, s.p, direction, h.id);
+                const float p_lights = lights_pdf_value(S, s.p, direction, s.from);
                 p = strategy == RT_SAMPLING_LIGHTS ? p_lights : 0.5f * p_lights + 0.5f * p_scatter;
             }
             if (!(p > 0.0f) || !(p_scatter > 0.0f))
@@ -938,7 +1248,7 @@ __device__ __forceinline__ step_result shade_books(const scene_view& S, const ca
     }
     ps.o = s.p;
     ps.d = direction;
-    ps.from = h.id;
+    ps.from = s.from;
     ps.inward = dot(direction, s.outward) < 0.0f;
     return step_result::go_on;
 }
@@ -1217,7 +1527,7 @@ __device__ float3 eval_lobe(int lobe, const material12& m, float3 albedo, float3
 }
 
 // One segment of an NEE/MIS path after its closest hit; the shadow ray is traced here
-template <bool COUNT, int SEARCH = search_any>
+template <bool COUNT, int SEARCH = search_any, bool FEATURES = true>
 __device__ __forceinline__ step_result shade_quality(const scene_view& S, const camera_params& cam,
                                                      const sampler& rng, path_state& ps, const hit_info& h,
                                                      float3& sample, uint32_t& shadow_rays, fetch_counts* counts)
@@ -1243,9 +1553,9 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
         sample = ps.radiance + w * (ps.throughput * le);
         return step_result::done;
     }
-    const surface s = surface_at(S, ps, h);
-    const material12 m = S.materials[s.material];
-    const float3 albedo = make_float3(m.r, m.g, m.b);
+    material12 m;
+    const surface s = surface_at<FEATURES>(S, ps, h, m);
+    const float3 albedo = s.color;
     if (m.kind == RT_DIFFUSE_LIGHT)
     {
         float w = 1.0f;
@@ -1394,11 +1704,14 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
     {
         ++shadow_rays;
         hit_info blocker;
-        const bool blocked = traverse<true, COUNT, SEARCH>(S, s.p, light_dir, light_distance, h.id,
-                                                   dot(light_dir, s.outward) < 0.0f, skip, blocker, counts);
+        const bool blocked = traverse<true, COUNT, SEARCH, FEATURES>(
+            S, s.p, light_dir, ps.time, light_distance, s.from, dot(light_dir, s.outward) < 0.0f, skip, blocker, counts);
         if (!blocked)
         {
-            ps.radiance = ps.radiance + contribution;
+            // through smoke, the light arrives with the chance of crossing it (its expected value, not a draw)
+            const float through =
+                FEATURES && S.medium_count > 0 ? transmittance(S, s.p, light_dir, ps.time, light_distance) : 1.0f;
+            ps.radiance = ps.radiance + through * contribution;
         }
     }
     if (!scattered)
@@ -1422,7 +1735,7 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
     }
     ps.o = s.p;
     ps.d = wi;
-    ps.from = h.id;
+    ps.from = s.from;
     ps.inward = dot(wi, s.outward) < 0.0f;
     return step_result::go_on;
 }
@@ -1445,7 +1758,9 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
 #define RTB_MIN_BLOCKS_QUALITY_FLAT 7
 #endif
 
-template <bool QUALITY, bool COUNT, bool FLAT>
+// FEATURES: the scene has moving spheres, textures other than solid colors, or smoke (the counting build always
+// compiles them in)
+template <bool QUALITY, bool COUNT, bool FLAT, bool FEATURES>
 __global__ void __launch_bounds__(render_block, QUALITY ? (FLAT ? RTB_MIN_BLOCKS_QUALITY_FLAT : RTB_MIN_BLOCKS_QUALITY)
                                                         : (FLAT ? RTB_MIN_BLOCKS_FLAT : RTB_MIN_BLOCKS))
     render_kernel(const __grid_constant__ launch_params P)
@@ -1528,6 +1843,8 @@ __global__ void __launch_bounds__(render_block, QUALITY ? (FLAT ? RTB_MIN_BLOCKS
             rng.pass = static_cast<uint32_t>(in_round);
             const float4 u = rng.draw(0, 0);
             camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
+            // the moment in the shutter, in a scene where something moves (camera.ixx get_ray's ray time)
+            ps.time = FEATURES && P.scene.has_motion ? rng.draw(0, block_time).x : 0.0f;
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
             ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
             ps.bsdf_pdf = 0.0f;
@@ -1539,16 +1856,21 @@ __global__ void __launch_bounds__(render_block, QUALITY ? (FLAT ? RTB_MIN_BLOCKS
             start = false;
         }
 
-        // One segment: the closest hit, then the vertex's shading
+        // One segment: the closest event (a surface, or a particle of smoke before it), then the vertex's shading
         constexpr int search = FLAT ? search_flat : search_tree;
         hit_info h;
-        traverse<false, COUNT, search>(P.scene, ps.o, ps.d, infinity_f, ps.from, ps.inward, -1, h, &counts);
+        traverse<false, COUNT, search, FEATURES>(P.scene, ps.o, ps.d, ps.time, infinity_f, ps.from, ps.inward, -1,
+                                                 h, &counts);
         ++rays;
         ++ps.depth;
+        if (FEATURES && P.scene.medium_count > 0)
+        {
+            media_event(P.scene, ps.o, ps.d, ps.time, rng, ps.depth, h);
+        }
         float3 sample;
         const step_result r =
-            QUALITY ? shade_quality<COUNT, search>(P.scene, cam, rng, ps, h, sample, shadow_rays, &counts)
-                    : shade_books(P.scene, cam, rng, ps, h, sample);
+            QUALITY ? shade_quality<COUNT, search, FEATURES>(P.scene, cam, rng, ps, h, sample, shadow_rays, &counts)
+                    : shade_books<FEATURES>(P.scene, cam, rng, ps, h, sample);
         if (r == step_result::done)
         {
             acc_r += without_nan(sample.x);
@@ -1726,6 +2048,7 @@ __global__ void __launch_bounds__(render_block, FLAT ? RTB_MIN_BLOCKS_QUALITY_FL
             rng.pass = static_cast<uint32_t>(in_round);
             const float4 u = rng.draw(0, 0);
             camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
+            ps.time = J->scene.has_motion ? rng.draw(0, block_time).x : 0.0f;
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
             ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
             ps.bsdf_pdf = 0.0f;
@@ -1737,9 +2060,13 @@ __global__ void __launch_bounds__(render_block, FLAT ? RTB_MIN_BLOCKS_QUALITY_FL
             start = false;
         }
         hit_info h;
-        traverse<false, false, search>(J->scene, ps.o, ps.d, infinity_f, ps.from, ps.inward, -1, h);
+        traverse<false, false, search>(J->scene, ps.o, ps.d, ps.time, infinity_f, ps.from, ps.inward, -1, h);
         ++rays;
         ++ps.depth;
+        if (J->scene.medium_count > 0)
+        {
+            media_event(J->scene, ps.o, ps.d, ps.time, rng, ps.depth, h);
+        }
         float3 sample;
         const step_result r =
             J->quality ? shade_quality<false, search>(J->scene, cam, rng, ps, h, sample, shadow_rays, nullptr)
@@ -1809,7 +2136,7 @@ __global__ void closest_hits_kernel(const scene_view S, const float* origins, co
     const float3 o = make_float3(origins[3 * i], origins[3 * i + 1], origins[3 * i + 2]);
     const float3 d = make_float3(directions[3 * i], directions[3 * i + 1], directions[3 * i + 2]);
     hit_info h;
-    traverse<false>(S, o, d, infinity_f, -1, false, -1, h);
+    traverse<false>(S, o, d, 0.0f, infinity_f, -1, false, -1, h);
     ids[i] = h.id >= 0 ? prim_source[h.id] : -1;
     ts[i] = h.id >= 0 ? h.t : infinity_f;
 }
@@ -1845,28 +2172,35 @@ namespace
 {
 using render_function = void (*)(launch_params);
 
-// The render kernel for an integrator, the counting build or not, and a flat or a tree search
-render_function render_kernel_for(bool quality, bool counting, bool flat)
+template <bool QUALITY, bool FLAT>
+render_function render_kernel_of(bool counting, bool features)
+{
+    if (counting)
+    {
+        return render_kernel<QUALITY, true, FLAT, true>;
+    }
+    return features ? render_kernel<QUALITY, false, FLAT, true> : render_kernel<QUALITY, false, FLAT, false>;
+}
+
+// The render kernel for an integrator, the counting build or not, a flat or a tree search, and a scene with or
+// without the second book's features
+render_function render_kernel_for(bool quality, bool counting, bool flat, bool features)
 {
     if (quality)
     {
-        if (counting)
-        {
-            return flat ? render_kernel<true, true, true> : render_kernel<true, true, false>;
-        }
-        return flat ? render_kernel<true, false, true> : render_kernel<true, false, false>;
+        return flat ? render_kernel_of<true, true>(counting, features)
+                    : render_kernel_of<true, false>(counting, features);
     }
-    if (counting)
-    {
-        return flat ? render_kernel<false, true, true> : render_kernel<false, true, false>;
-    }
-    return flat ? render_kernel<false, false, true> : render_kernel<false, false, false>;
+    return flat ? render_kernel_of<false, true>(counting, features) : render_kernel_of<false, false>(counting, features);
 }
+
+bool has_features(const scene_view& s) { return s.has_motion != 0 || s.has_textures != 0 || s.medium_count > 0; }
 } // namespace
 
 cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream)
 {
-    render_kernel_for(quality, counting, p.scene.flat != 0)<<<grid, render_block, 0, stream>>>(p);
+    render_kernel_for(quality, counting, p.scene.flat != 0, has_features(p.scene))<<<grid, render_block, 0, stream>>>(
+        p);
     return cudaGetLastError();
 }
 
@@ -1946,7 +2280,7 @@ cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream)
 
 cudaError_t render_attributes(bool quality, bool flat, kernel_attributes& out)
 {
-    return attributes_of(render_kernel_for(quality, false, flat), out);
+    return attributes_of(render_kernel_for(quality, false, flat, false), out);
 }
 
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,

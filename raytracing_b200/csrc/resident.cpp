@@ -123,6 +123,51 @@ build_prim quad_prim(const rt_quad_desc& d, int32_t source)
 }
 } // namespace
 
+// renderer.h:163-168: for every quad, all the corners of all the quads lie on one side of its plane, or on it within
+// 1e-9 of the largest coordinate
+bool is_convex(const rt_quad_desc* quads, int64_t count)
+{
+    double largest = 0;
+    std::vector<rt_vec3> corners;
+    for (int64_t i = 0; i < count; ++i)
+    {
+        const rt_quad_desc& q = quads[i];
+        const rt_vec3 c[4] = {q.q,
+                              {q.q.x + q.u.x, q.q.y + q.u.y, q.q.z + q.u.z},
+                              {q.q.x + q.v.x, q.q.y + q.v.y, q.q.z + q.v.z},
+                              {q.q.x + q.u.x + q.v.x, q.q.y + q.u.y + q.v.y, q.q.z + q.u.z + q.v.z}};
+        for (const rt_vec3& v : c)
+        {
+            corners.push_back(v);
+            largest = std::fmax(largest, std::fmax(std::fabs(v.x), std::fmax(std::fabs(v.y), std::fabs(v.z))));
+        }
+    }
+    const double tolerance = 1e-9 * std::fmax(1.0, largest);
+    for (int64_t i = 0; i < count; ++i)
+    {
+        const rt_quad_desc& q = quads[i];
+        const rt_vec3 n = cross(q.u, q.v);
+        const double len = std::sqrt(dot(n, n));
+        if (!(len > 0))
+        {
+            return false;
+        }
+        bool above = false;
+        bool below = false;
+        for (const rt_vec3& c : corners)
+        {
+            const double s = dot(sub(c, q.q), n) / len;
+            above = above || s > tolerance;
+            below = below || s < -tolerance;
+        }
+        if (above && below)
+        {
+            return false;
+        }
+    }
+    return true;
+}
+
 void validate(const rt_scene_desc& d)
 {
     const rt_camera_desc& c = d.camera;
@@ -157,6 +202,89 @@ void validate(const rt_scene_desc& d)
     {
         fail(RT_ERR_RUNTIME, "a table has a count but no data");
     }
+    // Textures, images and Perlin tables (renderer.cu:688-760): a checker refers to textures before it, so walking a
+    // chain of checkers ends; every index in range; pixels and gradients finite
+    if ((d.image_count > 0 && !d.images) || (d.perlin_count > 0 && !d.perlins) || (d.medium_count > 0 && !d.media))
+    {
+        fail(RT_ERR_RUNTIME, "a table has a count but no data");
+    }
+    int64_t image_pixels = 0;
+    for (int64_t i = 0; i < d.image_count; ++i)
+    {
+        const rt_image_desc& im = d.images[i];
+        if (im.width < 1 || im.height < 1 || !im.rgb)
+        {
+            fail(RT_ERR_RUNTIME, "images[" + std::to_string(i) + "]: an image texture's pixels don't match its size");
+        }
+        const int64_t n = int64_t{im.width} * im.height;
+        image_pixels += n;
+        if (image_pixels >= (int64_t{1} << 31))
+        {
+            fail(RT_ERR_RUNTIME, "the images have too many pixels for the GPU renderer");
+        }
+        for (int64_t k = 0; k < 3 * n; ++k)
+        {
+            if (!std::isfinite(im.rgb[k]))
+            {
+                fail(RT_ERR_RUNTIME, "images[" + std::to_string(i) + "] has a pixel that is not a finite number");
+            }
+        }
+    }
+    for (int64_t i = 0; i < d.perlin_count; ++i)
+    {
+        const rt_perlin_desc& p = d.perlins[i];
+        for (int k = 0; k < 256; ++k)
+        {
+            const int32_t perm[3] = {p.perm_x[k], p.perm_y[k], p.perm_z[k]};
+            for (const int32_t v : perm)
+            {
+                if (v < 0 || v > 255)
+                {
+                    fail(RT_ERR_RUNTIME, "a Perlin permutation has an entry outside 0..255");
+                }
+            }
+            if (!finite(p.random_vectors[k]))
+            {
+                fail(RT_ERR_RUNTIME, "perlins[" + std::to_string(i) + "] has a gradient that is not finite");
+            }
+        }
+    }
+    for (int64_t i = 0; i < d.texture_count; ++i)
+    {
+        const rt_texture_desc& t = d.textures[i];
+        switch (t.kind)
+        {
+        case RT_TEXTURE_SOLID:
+            if (!finite(t.rgb))
+            {
+                fail(RT_ERR_RUNTIME, "textures[" + std::to_string(i) + "] is not finite");
+            }
+            break;
+        case RT_TEXTURE_CHECKER:
+            if (t.even < 0 || t.even >= i || t.odd < 0 || t.odd >= i || !std::isfinite(t.inv_scale))
+            {
+                fail(RT_ERR_RUNTIME, "textures[" + std::to_string(i) +
+                                         "]: a checker texture must refer to textures that come before it");
+            }
+            break;
+        case RT_TEXTURE_IMAGE:
+            if (t.image < 0 || t.image >= d.image_count)
+            {
+                fail(RT_ERR_RUNTIME, "textures[" + std::to_string(i) +
+                                         "]: an image texture refers to an image that doesn't exist");
+            }
+            break;
+        case RT_TEXTURE_NOISE:
+            if (t.perlin < 0 || t.perlin >= d.perlin_count || !std::isfinite(t.scale))
+            {
+                fail(RT_ERR_RUNTIME, "textures[" + std::to_string(i) +
+                                         "]: a marble texture refers to Perlin tables that don't exist");
+            }
+            break;
+        default:
+            fail(RT_ERR_RUNTIME, "textures[" + std::to_string(i) + "]: unknown texture kind");
+        }
+    }
     for (int64_t i = 0; i < d.material_count; ++i)
     {
         const rt_material_desc& m = d.materials[i];
@@ -170,19 +298,6 @@ void validate(const rt_scene_desc& d)
             {
                 fail(RT_ERR_RUNTIME, index_error("materials", i, "texture", m.texture));
             }
-            if (d.textures[m.texture].kind != RT_TEXTURE_SOLID)
-            {
-                fail(RT_ERR_UNSUPPORTED, "materials[" + std::to_string(i) +
-                                             "]: textures other than one solid color are not rendered by this build");
-            }
-            if (!finite(d.textures[m.texture].rgb))
-            {
-                fail(RT_ERR_RUNTIME, "textures[" + std::to_string(m.texture) + "] is not finite");
-            }
-        }
-        if (m.kind == RT_ISOTROPIC)
-        {
-            fail(RT_ERR_UNSUPPORTED, "isotropic materials (smoke and fog) are not rendered by this build");
         }
         if (m.kind == RT_METAL && (!finite(m.albedo) || !(m.fuzz >= 0)))
         {
@@ -200,13 +315,10 @@ void validate(const rt_scene_desc& d)
         {
             fail(RT_ERR_RUNTIME, index_error("spheres", i, "material", s.material));
         }
-        if (!finite(s.center) || !(s.radius >= 0 && std::isfinite(s.radius)))
+        if (!finite(s.center) || !(s.radius >= 0 && std::isfinite(s.radius)) || !finite(s.displacement) ||
+            !std::isfinite(s.uv_cos) || !std::isfinite(s.uv_sin))
         {
             fail(RT_ERR_RUNTIME, "spheres[" + std::to_string(i) + "] is not a finite sphere");
-        }
-        if (s.displacement.x != 0 || s.displacement.y != 0 || s.displacement.z != 0)
-        {
-            fail(RT_ERR_UNSUPPORTED, "moving spheres (motion blur) are not rendered by this build");
         }
     }
     for (int64_t i = 0; i < d.quad_count; ++i)
@@ -241,9 +353,47 @@ void validate(const rt_scene_desc& d)
             }
         }
     }
-    if (d.medium_count > 0)
+    if (d.medium_count > max_media)
     {
-        fail(RT_ERR_UNSUPPORTED, "volumes of smoke (media) are not rendered by this build");
+        fail(RT_ERR_UNSUPPORTED, "a scene may hold at most " + std::to_string(max_media) + " volumes of smoke");
+    }
+    for (int64_t i = 0; i < d.medium_count; ++i)
+    {
+        const rt_medium_desc& m = d.media[i];
+        const std::string where = "media[" + std::to_string(i) + "]";
+        if (m.material < 0 || m.material >= d.material_count || d.materials[m.material].kind != RT_ISOTROPIC)
+        {
+            fail(RT_ERR_RUNTIME, where + ": a volume of smoke must refer to an isotropic material");
+        }
+        if (!(m.neg_inv_density < 0 && std::isfinite(m.neg_inv_density)))
+        {
+            fail(RT_ERR_RUNTIME, where + ": a volume of smoke needs a finite density > 0 (neg_inv_density < 0)");
+        }
+        if (m.boundary == RT_BOUNDARY_SPHERE)
+        {
+            if (!finite(m.sphere.center) || !(m.sphere.radius > 0 && std::isfinite(m.sphere.radius)) ||
+                !finite(m.sphere.displacement))
+            {
+                fail(RT_ERR_RUNTIME, where + ": its boundary is not a finite sphere");
+            }
+        }
+        else if (m.boundary == RT_BOUNDARY_CONVEX_QUADS)
+        {
+            bool convex = m.quad_count > 0 && m.quads;
+            for (int64_t k = 0; convex && k < m.quad_count; ++k)
+            {
+                convex = finite(m.quads[k].q) && finite(m.quads[k].u) && finite(m.quads[k].v);
+            }
+            if (!convex || !is_convex(m.quads, m.quad_count))
+            {
+                fail(RT_ERR_RUNTIME, where + ": a volume of smoke must be bounded by one sphere or by quads of a convex "
+                                             "shape");
+            }
+        }
+        else
+        {
+            fail(RT_ERR_RUNTIME, where + ": a volume of smoke must be bounded by one sphere or by quads of a convex shape");
+        }
     }
     for (int64_t i = 0; i < d.light_count; ++i)
     {
@@ -364,18 +514,28 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     // The primitives' boxes for the builder
     std::vector<build_prim> prims;
     std::vector<sphere4> source_spheres;
+    std::vector<float4> source_motion;
+    std::vector<sphere_frame> source_frames;
+    bool motion = false;
     for (int64_t i = 0; i < d.sphere_count; ++i)
     {
         const rt_sphere_desc& s = d.spheres[i];
         sphere4 v{static_cast<float>(s.center.x), static_cast<float>(s.center.y), static_cast<float>(s.center.z),
                   static_cast<float>(s.radius)};
-        // sphere_box (bvh.cuh:140-152): the float sphere's extent, each bound one double step outward
+        const float4 m = make_float4(static_cast<float>(s.displacement.x), static_cast<float>(s.displacement.y),
+                                     static_cast<float>(s.displacement.z), 0.0f);
+        motion = motion || m.x != 0.0f || m.y != 0.0f || m.z != 0.0f;
+        // sphere_box (bvh.cuh:140-152): the float sphere's extent, each bound one double step outward; a moving
+        // sphere's box holds it over the whole shutter (where it is at times 0 and 1)
         build_prim p{};
         const double c[3] = {v.cx, v.cy, v.cz};
+        const double dm[3] = {m.x, m.y, m.z};
         for (int a = 0; a < 3; ++a)
         {
-            p.lo[a] = std::nextafter(c[a] - static_cast<double>(v.r), -std::numeric_limits<double>::infinity());
-            p.hi[a] = std::nextafter(c[a] + static_cast<double>(v.r), std::numeric_limits<double>::infinity());
+            const double lo = std::min(c[a], c[a] + dm[a]);
+            const double hi = std::max(c[a], c[a] + dm[a]);
+            p.lo[a] = std::nextafter(lo - static_cast<double>(v.r), -std::numeric_limits<double>::infinity());
+            p.hi[a] = std::nextafter(hi + static_cast<double>(v.r), std::numeric_limits<double>::infinity());
         }
         p.kind = kind_sphere;
         p.source = static_cast<int32_t>(i);
@@ -385,6 +545,13 @@ resident_scene::resident_scene(const rt_scene_desc& d)
             v.r = -v.r;
         }
         source_spheres.push_back(v);
+        source_motion.push_back(m);
+        // The texture frame (sphere.cuh:119-168): the instances' turn, and for onto_sphere k = |c|^2 - r^2 and the
+        // bound 2 r |c| below which its one Newton step helps
+        const double cc = dot(s.center, s.center);
+        source_frames.push_back({static_cast<float>(s.uv_cos), static_cast<float>(s.uv_sin),
+                                 static_cast<float>(cc - s.radius * s.radius),
+                                 static_cast<float>(2 * s.radius * std::sqrt(cc))});
     }
     std::vector<quad12> source_quads;
     for (int64_t i = 0; i < d.quad_count; ++i)
@@ -444,6 +611,8 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     const auto Q = static_cast<int32_t>(d.quad_count);
     const auto T = static_cast<int32_t>(source_triangles.size());
     std::vector<sphere4> spheres(tree.order[kind_sphere].size());
+    std::vector<float4> sphere_motion(motion ? spheres.size() : 0);
+    std::vector<sphere_frame> sphere_frames(spheres.size());
     std::vector<quad12> quads(tree.order[kind_quad].size());
     std::vector<triangle12> triangles(tree.order[kind_triangle].size());
     std::vector<int32_t> prim_material(static_cast<size_t>(S + Q + T));
@@ -454,6 +623,11 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     {
         const int32_t src = tree.order[kind_sphere][k];
         spheres[k] = source_spheres[static_cast<size_t>(src)];
+        sphere_frames[k] = source_frames[static_cast<size_t>(src)];
+        if (motion)
+        {
+            sphere_motion[k] = source_motion[static_cast<size_t>(src)];
+        }
         prim_material[k] = d.spheres[src].material;
         prim_source[k] = src;
         sphere_gid[static_cast<size_t>(src)] = static_cast<int32_t>(k);
@@ -474,6 +648,75 @@ resident_scene::resident_scene(const rt_scene_desc& d)
         prim_source[static_cast<size_t>(S + Q) + k] = S + Q + src;
     }
 
+    // Textures (texture.cuh): every texture as a record, an image's texels after the others', a marble's own noise
+    // tables; a material whose texture is one solid color gets the color itself and no texture to read
+    std::vector<texture8> textures;
+    std::vector<image_info> images;
+    std::vector<float4> texels;
+    std::vector<noise_table> noises;
+    for (int64_t i = 0; i < d.image_count; ++i)
+    {
+        const rt_image_desc& im = d.images[i];
+        images.push_back({static_cast<int32_t>(texels.size()), im.width, im.height, 0});
+        for (int64_t k = 0; k < int64_t{im.width} * im.height; ++k)
+        {
+            texels.push_back(make_float4(im.rgb[3 * k], im.rgb[3 * k + 1], im.rgb[3 * k + 2], 0.0f));
+        }
+    }
+    for (int64_t i = 0; i < d.texture_count; ++i)
+    {
+        const rt_texture_desc& t = d.textures[i];
+        texture8 v{};
+        v.kind = t.kind;
+        v.even = t.even;
+        v.odd = t.odd;
+        v.r = static_cast<float>(t.rgb.x);
+        v.g = static_cast<float>(t.rgb.y);
+        v.b = static_cast<float>(t.rgb.z);
+        v.inv_scale = static_cast<float>(t.inv_scale);
+        if (t.kind == RT_TEXTURE_IMAGE)
+        {
+            v.table = t.image;
+        }
+        else if (t.kind == RT_TEXTURE_NOISE)
+        {
+            v.table = static_cast<int32_t>(noises.size());
+            noise_table n{};
+            const rt_perlin_desc& p = d.perlins[t.perlin];
+            for (int k = 0; k < 256; ++k)
+            {
+                n.gradients[k] = make_float4(static_cast<float>(p.random_vectors[k].x),
+                                             static_cast<float>(p.random_vectors[k].y),
+                                             static_cast<float>(p.random_vectors[k].z), 0.0f);
+                n.perm_x[k] = static_cast<uint8_t>(p.perm_x[k]);
+                n.perm_y[k] = static_cast<uint8_t>(p.perm_y[k]);
+                n.perm_z[k] = static_cast<uint8_t>(p.perm_z[k]);
+            }
+            n.scale = static_cast<float>(t.scale);
+            noises.push_back(n);
+        }
+        textures.push_back(v);
+    }
+    // What reading a texture needs of the hit: (u, v) for an image somewhere in its checkers' tree, the point for a
+    // checker (moved onto a sphere exactly)
+    const auto needs_of = [&](int32_t root) {
+        int32_t needs = 0;
+        std::vector<int32_t> pending{root};
+        while (!pending.empty())
+        {
+            const rt_texture_desc& t = d.textures[pending.back()];
+            pending.pop_back();
+            if (t.kind == RT_TEXTURE_CHECKER)
+            {
+                needs |= texture_needs_point;
+                pending.push_back(t.even);
+                pending.push_back(t.odd);
+            }
+            needs |= t.kind == RT_TEXTURE_IMAGE ? texture_needs_uv : 0;
+        }
+        return needs;
+    };
+
     // Materials: a solid texture becomes the material's color (renderer.cu:551-600)
     std::vector<material12> materials;
     for (int64_t i = 0; i < d.material_count; ++i)
@@ -481,7 +724,14 @@ resident_scene::resident_scene(const rt_scene_desc& d)
         const rt_material_desc& m = d.materials[i];
         material12 v{};
         v.kind = m.kind;
-        const rt_vec3 color = m.kind == RT_METAL || m.kind == RT_DIELECTRIC ? m.albedo : d.textures[m.texture].rgb;
+        v.texture = -1;
+        const bool textured = m.kind == RT_LAMBERTIAN || m.kind == RT_DIFFUSE_LIGHT || m.kind == RT_ISOTROPIC;
+        if (textured && d.textures[m.texture].kind != RT_TEXTURE_SOLID)
+        {
+            v.texture = m.texture;
+            v.texture_needs = needs_of(m.texture);
+        }
+        const rt_vec3 color = textured ? d.textures[m.texture].rgb : m.albedo;
         v.r = static_cast<float>(color.x);
         v.g = static_cast<float>(color.y);
         v.b = static_cast<float>(color.z);
@@ -558,12 +808,16 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     // The NEE/MIS integrator's lamps: still spheres, then quads, glowing one solid color (lamp_table.cu)
     std::vector<emitter20> lamps;
     std::vector<int32_t> lamp_of(static_cast<size_t>(S + Q + T), -1);
-    const auto glows = [&](int32_t material) { return d.materials[material].kind == RT_DIFFUSE_LIGHT; };
+    const auto glows = [&](int32_t material) {
+        return d.materials[material].kind == RT_DIFFUSE_LIGHT &&
+               d.textures[d.materials[material].texture].kind == RT_TEXTURE_SOLID;
+    };
     const auto radiance = [&](int32_t material) { return d.textures[d.materials[material].texture].rgb; };
     for (int64_t i = 0; i < d.sphere_count; ++i)
     {
         const rt_sphere_desc& s = d.spheres[i];
-        if (glows(s.material))
+        const bool still = s.displacement.x == 0 && s.displacement.y == 0 && s.displacement.z == 0;
+        if (still && glows(s.material))
         {
             emitter20 e{};
             e.cx = static_cast<float>(s.center.x);
@@ -633,8 +887,75 @@ resident_scene::resident_scene(const rt_scene_desc& d)
         env.scale = static_cast<float>(d.environment->scale);
     }
 
+    // Volumes of smoke (constant_medium.cuh): a box over the whole shutter, rounded outward, and the boundary
+    std::vector<medium16> media;
+    std::vector<quad12> boundary_quads;
+    for (int64_t i = 0; i < d.medium_count; ++i)
+    {
+        const rt_medium_desc& m = d.media[i];
+        medium16 v{};
+        v.neg_inv_density = static_cast<float>(m.neg_inv_density);
+        v.material = m.material;
+        double lo[3] = {std::numeric_limits<double>::infinity(), std::numeric_limits<double>::infinity(),
+                        std::numeric_limits<double>::infinity()};
+        double hi[3] = {-lo[0], -lo[1], -lo[2]};
+        if (m.boundary == RT_BOUNDARY_SPHERE)
+        {
+            const rt_sphere_desc& s = m.sphere;
+            v.cx = static_cast<float>(s.center.x);
+            v.cy = static_cast<float>(s.center.y);
+            v.cz = static_cast<float>(s.center.z);
+            v.radius = static_cast<float>(s.radius);
+            v.dx = static_cast<float>(s.displacement.x);
+            v.dy = static_cast<float>(s.displacement.y);
+            v.dz = static_cast<float>(s.displacement.z);
+            motion = motion || v.dx != 0.0f || v.dy != 0.0f || v.dz != 0.0f;
+            const double c[3] = {s.center.x, s.center.y, s.center.z};
+            const double dm[3] = {s.displacement.x, s.displacement.y, s.displacement.z};
+            for (int a = 0; a < 3; ++a)
+            {
+                lo[a] = std::min(c[a], c[a] + dm[a]) - s.radius;
+                hi[a] = std::max(c[a], c[a] + dm[a]) + s.radius;
+            }
+        }
+        else
+        {
+            v.first_quad = static_cast<int32_t>(boundary_quads.size());
+            v.quad_count = static_cast<int32_t>(m.quad_count);
+            for (int64_t k = 0; k < m.quad_count; ++k)
+            {
+                boundary_quads.push_back(make_quad(m.quads[k]));
+                const build_prim b = quad_prim(m.quads[k], 0);
+                for (int a = 0; a < 3; ++a)
+                {
+                    lo[a] = std::min(lo[a], b.lo[a]);
+                    hi[a] = std::max(hi[a], b.hi[a]);
+                }
+            }
+        }
+        v.lo_x = round_down(lo[0]);
+        v.lo_y = round_down(lo[1]);
+        v.lo_z = round_down(lo[2]);
+        v.hi_x = round_up(hi[0]);
+        v.hi_y = round_up(hi[1]);
+        v.hi_z = round_up(hi[2]);
+        media.push_back(v);
+    }
+    if (motion && sphere_motion.empty())
+    {
+        sphere_motion.assign(spheres.size(), make_float4(0.0f, 0.0f, 0.0f, 0.0f)); // a moving boundary alone moves
+    }
+
     nodes_.upload(tree.nodes);
     spheres_.upload(spheres);
+    sphere_motion_.upload(sphere_motion);
+    sphere_frames_.upload(sphere_frames);
+    textures_.upload(textures);
+    images_.upload(images);
+    texels_.upload(texels);
+    noises_.upload(noises);
+    media_.upload(media);
+    boundary_quads_.upload(boundary_quads);
     quads_.upload(quads);
     triangles_.upload(triangles);
     prim_material_.upload(prim_material);
@@ -665,6 +986,21 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     view_.has_environment = d.environment ? 1 : 0;
     view_.flat = T == 0 && S + Q <= RTB_FLAT_SCENE ? 1 : 0;
     view_.env = env;
+    view_.textures = textures_.data();
+    view_.images = images_.data();
+    view_.texels = texels_.data();
+    view_.noises = noises_.data();
+    view_.sphere_motion = sphere_motion_.data();
+    view_.sphere_frames = sphere_frames_.data();
+    view_.media = media_.data();
+    view_.boundary_quads = boundary_quads_.data();
+    view_.has_motion = motion ? 1 : 0;
+    view_.has_textures = std::any_of(materials.begin(), materials.end(),
+                                     [](const material12& m) { return m.texture >= 0; })
+                             ? 1
+                             : 0;
+    view_.medium_count = static_cast<int32_t>(media.size());
+    view_.medium_base = S + Q + T;
 
     stats_.spheres = S;
     stats_.quads = Q;
@@ -676,7 +1012,10 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     stats_.device_bytes = static_cast<int64_t>(nodes_.bytes() + spheres_.bytes() + quads_.bytes() + triangles_.bytes() +
                                                prim_material_.bytes() + prim_source_.bytes() + materials_.bytes() +
                                                lights_.bytes() + lamps_.bytes() + lamp_of_.bytes() +
-                                               env_texels_.bytes() + env_bins_.bytes() + env_row_cos_.bytes());
+                                               env_texels_.bytes() + env_bins_.bytes() + env_row_cos_.bytes() +
+                                               sphere_motion_.bytes() + sphere_frames_.bytes() + textures_.bytes() +
+                                               images_.bytes() + texels_.bytes() + noises_.bytes() + media_.bytes() +
+                                               boundary_quads_.bytes());
     stats_.depth = tree.depth;
     stats_.max_leaf_size = options.max_leaf_size;
     stats_.flat = view_.flat;

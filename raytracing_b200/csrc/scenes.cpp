@@ -198,11 +198,61 @@ camera_settings cornell_camera()
     return c;
 }
 
-// scenes.ixx:79-127 random_spheres(false): the first book's cover. grid_half: the grid runs a, b in [-grid_half,
-// grid_half) (11 in the book); the small spheres keep the book's placement and material draws.
-void cover_world(scene_store& s, scene_random& rng, int grid_half)
+// texture.ixx checker_texture(scale, even, odd): the cubes of side `scale`, two solid colors
+int checker_texture(scene_store& s, double scale, rt_vec3 even, rt_vec3 odd)
 {
-    s.spheres.push_back(make_sphere(v3(0, -1000, 0), 1000, s.lambertian(v3(0.5, 0.5, 0.5))));
+    const int e = s.add_solid_texture(even);
+    const int o = s.add_solid_texture(odd);
+    rt_texture_desc t{};
+    t.kind = RT_TEXTURE_CHECKER;
+    t.even = e;
+    t.odd = o;
+    t.image = t.perlin = -1;
+    t.inv_scale = 1.0 / scale;
+    t.scale = 1;
+    s.textures.push_back(t);
+    return static_cast<int>(s.textures.size()) - 1;
+}
+
+// A material that reads a texture (lambertian, diffuse_light or isotropic)
+int textured(scene_store& s, int kind, int texture)
+{
+    rt_material_desc m{};
+    m.kind = kind;
+    m.texture = texture;
+    m.refraction_index = 1;
+    return s.add_material(m);
+}
+
+// constant_medium(boundary, density, albedo): a volume of smoke, its phase function an isotropic material
+void add_medium(scene_store& s, const rt_sphere_desc* ball, const std::vector<rt_quad_desc>* faces, double density,
+                rt_vec3 albedo)
+{
+    medium_store m;
+    m.desc.material = textured(s, RT_ISOTROPIC, s.add_solid_texture(albedo));
+    m.desc.neg_inv_density = -1.0 / density;
+    if (ball)
+    {
+        m.desc.boundary = RT_BOUNDARY_SPHERE;
+        m.desc.sphere = *ball;
+    }
+    else
+    {
+        m.desc.boundary = RT_BOUNDARY_CONVEX_QUADS;
+        m.quads = *faces;
+    }
+    s.media.push_back(std::move(m));
+}
+
+// scenes.ixx:79-127 random_spheres(bouncing): the first book's cover. grid_half: the grid runs a, b in [-grid_half,
+// grid_half) (11 in the book); the small spheres keep the book's placement and material draws. bouncing: the second
+// book's variant, a checker floor and matte spheres that jump by up to 0.5 while the shutter is open.
+void cover_world(scene_store& s, scene_random& rng, int grid_half, bool bouncing = false)
+{
+    const int ground = bouncing ? textured(s, RT_LAMBERTIAN, checker_texture(s, 0.32, v3(0.2, 0.3, 0.1),
+                                                                             v3(0.9, 0.9, 0.9)))
+                                : s.lambertian(v3(0.5, 0.5, 0.5));
+    s.spheres.push_back(make_sphere(v3(0, -1000, 0), 1000, ground));
     for (int a = -grid_half; a < grid_half; ++a)
     {
         for (int b = -grid_half; b < grid_half; ++b)
@@ -216,11 +266,16 @@ void cover_world(scene_store& s, scene_random& rng, int grid_half)
                 continue;
             }
             int material;
+            rt_vec3 jump{0, 0, 0};
             if (choose_mat < 0.8)
             {
                 const rt_vec3 c1 = rng.vec();
                 const rt_vec3 c2 = rng.vec();
                 material = s.lambertian(hadamard(c1, c2));
+                if (bouncing)
+                {
+                    jump = v3(0, rng.next(0, 0.5), 0);
+                }
             }
             else if (choose_mat < 0.95)
             {
@@ -231,7 +286,9 @@ void cover_world(scene_store& s, scene_random& rng, int grid_half)
             {
                 material = s.dielectric(1.5);
             }
-            s.spheres.push_back(make_sphere(center, 0.2, material));
+            rt_sphere_desc ball = make_sphere(center, 0.2, material);
+            ball.displacement = jump;
+            s.spheres.push_back(ball);
         }
     }
     s.spheres.push_back(make_sphere(v3(0, 1, 0), 1.0, s.dielectric(1.5)));
@@ -325,6 +382,20 @@ public:
         return std::fabs(accum);
     }
 
+    // The tables as a scene's perlin_desc (renderer.h:85-93)
+    rt_perlin_desc desc() const
+    {
+        rt_perlin_desc d{};
+        for (size_t k = 0; k < 256; ++k)
+        {
+            d.random_vectors[k] = gradients_[k];
+            d.perm_x[k] = perm_x_[k];
+            d.perm_y[k] = perm_y_[k];
+            d.perm_z[k] = perm_z_[k];
+        }
+        return d;
+    }
+
 private:
     std::array<rt_vec3, 256> gradients_;
     std::array<int, 256> perm_x_, perm_y_, perm_z_;
@@ -342,6 +413,61 @@ private:
         }
     }
 };
+
+// texture.ixx noise_texture(scale): a marble of its own Perlin tables, drawn from the scene's generator here
+int noise_texture(scene_store& s, scene_random& rng, double scale)
+{
+    const perlin_noise noise(rng);
+    s.perlins.push_back(noise.desc());
+    rt_texture_desc t{};
+    t.kind = RT_TEXTURE_NOISE;
+    t.even = t.odd = t.image = -1;
+    t.perlin = static_cast<int>(s.perlins.size()) - 1;
+    t.inv_scale = 1;
+    t.scale = scale;
+    s.textures.push_back(t);
+    return static_cast<int>(s.textures.size()) - 1;
+}
+
+// An image texture of a synthetic planet, `width` x width/2, linear colors: oceans and continents from a turbulence
+// field over the sphere, ice towards the poles. It stands in for the reference's assets/earthmap.jpg (a photograph
+// this project does not ship): the same kind of texture and the same lookups.
+int planet_texture(scene_store& s, scene_random& rng, int width)
+{
+    const int height = width / 2;
+    const perlin_noise noise(rng);
+    std::vector<float> rgb(static_cast<size_t>(width) * height * 3);
+    for (int j = 0; j < height; ++j)
+    {
+        for (int i = 0; i < width; ++i)
+        {
+            const double phi = 2 * std::numbers::pi * (i + 0.5) / width;
+            const double theta = std::numbers::pi * (j + 0.5) / height;
+            const rt_vec3 n{std::sin(theta) * std::cos(phi), std::cos(theta), std::sin(theta) * std::sin(phi)};
+            const double land = noise.turbulence(mul(3, n), 5);
+            const bool ice = std::fabs(n.y) > 0.85;
+            const rt_vec3 c = ice ? v3(0.85, 0.88, 0.9) : land > 0.35 ? v3(0.25 + 0.3 * land, 0.35, 0.12)
+                                                                      : v3(0.02, 0.08, 0.25 + 0.3 * land);
+            float* out = rgb.data() + 3 * (static_cast<size_t>(j) * width + i);
+            out[0] = static_cast<float>(c.x);
+            out[1] = static_cast<float>(c.y);
+            out[2] = static_cast<float>(c.z);
+        }
+    }
+    rt_image_desc im{};
+    im.width = width;
+    im.height = height;
+    s.images.push_back(im);
+    s.image_pixels.push_back(std::move(rgb));
+    rt_texture_desc t{};
+    t.kind = RT_TEXTURE_IMAGE;
+    t.even = t.odd = t.perlin = -1;
+    t.image = static_cast<int>(s.images.size()) - 1;
+    t.inv_scale = 1;
+    t.scale = 1;
+    s.textures.push_back(t);
+    return static_cast<int>(s.textures.size()) - 1;
+}
 
 // meshes.ixx:159-230 icosphere(level): the icosahedron, its faces turned counter-clockwise seen from outside, each
 // triangle cut into four `level` times with the edge midpoints pushed onto the unit sphere (shared between the two
@@ -464,8 +590,8 @@ void set_camera(scene_store& s, camera_settings c, const rt_builtin_params& p, b
         // A random orbit camera for served requests: the look-at point fixed, the distance kept
         const rt_vec3 to = sub(c.lookfrom, c.lookat);
         const double r = length(to);
-        const double az = p.orbit_azimuth;
-        const double el = p.orbit_elevation;
+        const double az = degrees_to_radians(p.orbit_azimuth);
+        const double el = degrees_to_radians(p.orbit_elevation);
         c.lookfrom = add(c.lookat, v3(r * std::cos(el) * std::sin(az), r * std::sin(el), r * std::cos(el) * std::cos(az)));
     }
     // camera.ixx:56-62 effective_sampling: lights and mixture need a lights list
@@ -771,6 +897,189 @@ rt_status build_builtin(const std::string& name, const rt_builtin_params& p, std
             q.sampling = RT_SAMPLING_MATERIAL;
         }
         set_camera(*s, cornell_camera(), q, true);
+    }
+    else if (name == "bouncing")
+    {
+        // scenes.ixx:176-181: the cover with a checker floor and bouncing matte spheres (motion blur)
+        cover_world(*s, rng, 11, true);
+        set_camera(*s, cover_camera(), p, false);
+    }
+    else if (name == "checker")
+    {
+        // scenes.ixx:184-196: two huge spheres with one solid checker texture
+        const int checker = textured(*s, RT_LAMBERTIAN, checker_texture(*s, 0.32, v3(0.2, 0.3, 0.1), v3(0.9, 0.9, 0.9)));
+        s->spheres.push_back(make_sphere(v3(0, -10, 0), 10, checker));
+        s->spheres.push_back(make_sphere(v3(0, 10, 0), 10, checker));
+        camera_settings c = cover_camera();
+        c.defocus_angle = 0;
+        set_camera(*s, c, p, false);
+    }
+    else if (name == "earth")
+    {
+        // scenes.ixx:199-209: an image wrapped around a sphere (a synthetic planet: see planet_texture)
+        const int surface = textured(*s, RT_LAMBERTIAN, planet_texture(*s, rng, p.env_width > 0 ? p.env_width : 512));
+        s->spheres.push_back(make_sphere(v3(0, 0, 0), 2, surface));
+        camera_settings c = cover_camera();
+        c.lookfrom = v3(0, 0, 12);
+        c.defocus_angle = 0;
+        set_camera(*s, c, p, false);
+    }
+    else if (name == "perlin" || name == "light")
+    {
+        // scenes.ixx:212-222 perlin_spheres: marble spheres (one noise texture of scale 4 for both); light
+        // (scenes.ixx:255-292): the same in the dark, lit by a glowing sphere and a glowing quad, both in the lights
+        // list (quad first)
+        const int marble = textured(*s, RT_LAMBERTIAN, noise_texture(*s, rng, 4));
+        s->spheres.push_back(make_sphere(v3(0, -1000, 0), 1000, marble));
+        s->spheres.push_back(make_sphere(v3(0, 2, 0), 2, marble));
+        camera_settings c = cover_camera();
+        c.defocus_angle = 0;
+        bool has_lights = false;
+        if (name == "light")
+        {
+            const int lamp = s->diffuse_light(v3(4, 4, 4));
+            s->spheres.push_back(make_sphere(v3(0, 7, 0), 2, lamp));
+            const rt_quad_desc quad_lamp = make_quad(v3(3, 1, -2), v3(2, 0, 0), v3(0, 2, 0), lamp);
+            s->quads.push_back(quad_lamp);
+            s->lights.push_back(quad_light(quad_lamp, 0.5));
+            s->lights.push_back(sphere_light(v3(0, 7, 0), 2, 0.5));
+            has_lights = true;
+            c = camera_settings{};
+            c.aspect_ratio = 16.0 / 9.0;
+            c.image_width = 1920;
+            c.samples_per_pixel = 1000;
+            c.max_depth = 50;
+            c.vfov = 20;
+            c.lookfrom = v3(26, 3, 6);
+            c.lookat = v3(0, 2, 0);
+        }
+        set_camera(*s, c, p, has_lights);
+    }
+    else if (name == "smoke")
+    {
+        // scenes.ixx:359-377: the Cornell box with blocks of black and white smoke (density 0.01) and a bigger,
+        // dimmer lamp
+        cornell_walls(*s);
+        const rt_quad_desc lamp = make_quad(v3(113, 554, 127), v3(330, 0, 0), v3(0, 0, 305), 0);
+        rt_quad_desc glowing = lamp;
+        glowing.material = s->diffuse_light(v3(7, 7, 7));
+        s->quads.push_back(glowing);
+        std::vector<rt_quad_desc> tall;
+        box_faces(v3(0, 0, 0), v3(165, 330, 165), tall, 0, placement{}.translated(v3(265, 0, 295)).rotated_y(15));
+        std::vector<rt_quad_desc> small;
+        box_faces(v3(0, 0, 0), v3(165, 165, 165), small, 0, placement{}.translated(v3(130, 0, 65)).rotated_y(-18));
+        add_medium(*s, nullptr, &tall, 0.01, v3(0, 0, 0));
+        add_medium(*s, nullptr, &small, 0.01, v3(1, 1, 1));
+        s->lights.push_back(quad_light(lamp, 1.0));
+        set_camera(*s, cornell_camera(), p, true);
+    }
+    else if (name == "final")
+    {
+        // scenes.ixx:380-461: the second book's final scene, its instances baked into world coordinates
+        const int ground = s->lambertian(v3(0.48, 0.83, 0.53));
+        for (int i = 0; i < 20; ++i)
+        {
+            for (int j = 0; j < 20; ++j)
+            {
+                const double w = 100.0;
+                const rt_vec3 corner0{-1000.0 + i * w, 0.0, -1000.0 + j * w};
+                const rt_vec3 corner1{corner0.x + w, rng.next(1, 101), corner0.z + w};
+                box_faces(corner0, corner1, s->quads, ground, placement{});
+            }
+        }
+        const rt_quad_desc lamp = make_quad(v3(123, 554, 147), v3(300, 0, 0), v3(0, 0, 265), 0);
+        rt_quad_desc glowing = lamp;
+        glowing.material = s->diffuse_light(v3(7, 7, 7));
+        s->quads.push_back(glowing);
+        rt_sphere_desc moving = make_sphere(v3(400, 400, 200), 50, s->lambertian(v3(0.7, 0.3, 0.1)));
+        moving.displacement = v3(30, 0, 0);
+        s->spheres.push_back(moving);
+        s->spheres.push_back(make_sphere(v3(260, 150, 45), 50, s->dielectric(1.5)));
+        s->spheres.push_back(make_sphere(v3(0, 150, 145), 50, s->metal(v3(0.8, 0.8, 0.9), 1.0)));
+        const int glass = s->dielectric(1.5);
+        const rt_sphere_desc boundary = make_sphere(v3(360, 150, 145), 70, glass);
+        s->spheres.push_back(boundary);
+        add_medium(*s, &boundary, nullptr, 0.2, v3(0.2, 0.4, 0.9));
+        const rt_sphere_desc haze = make_sphere(v3(0, 0, 0), 5000, glass);
+        add_medium(*s, &haze, nullptr, 0.0001, v3(1, 1, 1));
+        const int earth = textured(*s, RT_LAMBERTIAN, planet_texture(*s, rng, p.env_width > 0 ? p.env_width : 512));
+        s->spheres.push_back(make_sphere(v3(400, 200, 400), 100, earth));
+        const int marble = textured(*s, RT_LAMBERTIAN, noise_texture(*s, rng, 0.2));
+        s->spheres.push_back(make_sphere(v3(220, 280, 300), 80, marble));
+        // A cloud of 1000 white balls in a 165^3 cube, turned 15 degrees about y and moved: the turn is kept for the
+        // balls' texture coordinates
+        const int white = s->lambertian(v3(0.73, 0.73, 0.73));
+        const placement cloud = placement{}.translated(v3(-100, 270, 395)).rotated_y(15);
+        for (int k = 0; k < 1000; ++k)
+        {
+            rt_sphere_desc ball = make_sphere(cloud.place(rng.vec(0, 165)), 10, white);
+            ball.uv_cos = cloud.cos_theta;
+            ball.uv_sin = cloud.sin_theta;
+            s->spheres.push_back(ball);
+        }
+        s->lights.push_back(quad_light(lamp, 1.0));
+        camera_settings c;
+        c.aspect_ratio = 1.0;
+        c.image_width = 1080;
+        c.samples_per_pixel = 1000;
+        c.max_depth = 40;
+        c.vfov = 40;
+        c.lookfrom = v3(478, 278, -600);
+        c.lookat = v3(278, 278, 0);
+        set_camera(*s, c, p, true);
+    }
+    else if (name == "aluminum")
+    {
+        // scenes.ixx:464-478: the Cornell box with a tall block of polished aluminum
+        cornell_walls(*s);
+        s->quads.push_back(cornell_lamp(s->diffuse_light(v3(15, 15, 15))));
+        tall_block(*s, s->metal(v3(0.8, 0.85, 0.88), 0.0));
+        short_block(*s, s->lambertian(v3(0.73, 0.73, 0.73)));
+        s->lights.push_back(quad_light(cornell_lamp(0), 1.0));
+        set_camera(*s, cornell_camera(), p, true);
+    }
+    else if (name == "feature-furnace")
+    {
+        // The white furnace with the second book's features in it: a moving sphere with a white-on-white checker, a
+        // quad with an all-white image, a sphere and a box of white smoke. Every bounce keeps all of the light and
+        // every path ends in the white sky, so every pixel is exactly 1 under the material's own sampling, whatever
+        // the motion, the textures' lookups and the free flights do.
+        const int checker = textured(*s, RT_LAMBERTIAN, checker_texture(*s, 0.25, v3(1, 1, 1), v3(1, 1, 1)));
+        rt_sphere_desc ball = make_sphere(v3(0, 0, 0), 1.0, checker);
+        ball.displacement = v3(0.4, 0.1, 0);
+        s->spheres.push_back(ball);
+        rt_image_desc im{};
+        im.width = 4;
+        im.height = 2;
+        s->images.push_back(im);
+        s->image_pixels.emplace_back(4 * 2 * 3, 1.0f);
+        rt_texture_desc image{};
+        image.kind = RT_TEXTURE_IMAGE;
+        image.even = image.odd = image.perlin = -1;
+        image.image = 0;
+        image.inv_scale = 1;
+        image.scale = 1;
+        s->textures.push_back(image);
+        s->quads.push_back(make_quad(v3(-2, -1.5, -1), v3(4, 0, 0), v3(0, 0, 2),
+                                     textured(*s, RT_LAMBERTIAN, static_cast<int>(s->textures.size()) - 1)));
+        // (the volumes stay clear of the sphere: smoke inside an opaque surface would trap its paths)
+        const rt_sphere_desc fog = make_sphere(v3(2.1, 0.7, -0.5), 0.55, 0);
+        add_medium(*s, &fog, nullptr, 0.6, v3(1, 1, 1));
+        std::vector<rt_quad_desc> block;
+        box_faces(v3(-2.4, -0.6, -0.4), v3(-1.7, 0.6, 0.4), block, 0, placement{}.rotated_y(20));
+        add_medium(*s, nullptr, &block, 0.8, v3(1, 1, 1));
+        camera_settings c;
+        c.aspect_ratio = 16.0 / 9.0;
+        c.image_width = 480;
+        c.samples_per_pixel = 64;
+        c.max_depth = 50;
+        c.sampling = RT_SAMPLING_MATERIAL;
+        c.vfov = 30;
+        c.lookfrom = v3(0, 0, 6);
+        c.lookat = v3(0, 0, 0);
+        c.sky_bottom = v3(1, 1, 1);
+        c.sky_top = v3(1, 1, 1);
+        set_camera(*s, c, p, false);
     }
     else if (name == "furnace")
     {

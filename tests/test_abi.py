@@ -139,12 +139,54 @@ def test_inconsistent_scenes_are_refused_before_any_gpu_work(rt):
         rt.Scene(s)
 
 
-def test_unsupported_features_are_named(rt):
-    s = rt.builtin_scene("weekend", width=16)
+def test_second_book_tables_are_validated(rt):
+    """Textures, media and their references are checked before anything is built (renderer.cu:688-810)."""
+    s = rt.builtin_scene("smoke", width=16)
     d = s.desc.contents
-    d.spheres[2].displacement.y = 0.5
-    with pytest.raises(rt.UnsupportedError, match="moving"):
+    count = d.medium_count
+    d.medium_count = 49  # checked before any entry is read
+    with pytest.raises(rt.UnsupportedError, match="volumes of smoke"):
         rt.Scene(s)
+    d.medium_count = count
+    isotropic = d.media[0].material
+    d.media[0].material = d.spheres[0].material if d.sphere_count else 0
+    with pytest.raises(rt.RenderError, match="isotropic"):
+        rt.Scene(s)
+    d.media[0].material = isotropic
+    d.media[0].neg_inv_density = 1.0
+    with pytest.raises(rt.RenderError, match="density"):
+        rt.Scene(s)
+    c = rt.builtin_scene("checker", width=16)
+    cd = c.desc.contents
+    checker = next(i for i in range(cd.texture_count) if cd.textures[i].kind == 1)
+    cd.textures[checker].even = checker  # a checker must refer to textures before it
+    with pytest.raises(rt.RenderError, match="come before it"):
+        rt.Scene(c)
+    p = rt.builtin_scene("perlin", width=16)
+    p.desc.contents.perlins[0].perm_y[7] = 256
+    with pytest.raises(rt.RenderError, match="Perlin"):
+        rt.Scene(p)
+
+
+@pytest.mark.parametrize("name", ["bouncing", "checker", "earth", "perlin", "light", "smoke", "final", "aluminum"])
+def test_second_book_scenes_build_and_round_trip(rt, name, tmp_path):
+    """The reference's scene list (scenes.ixx:504-518) beyond the first book's: built, saved and loaded unchanged."""
+    s = rt.builtin_scene(name, width=32, spp=4)
+    d = s.desc.contents
+    assert d.camera.image_width == 32
+    path = tmp_path / f"{name}.rtscene"
+    s.save(str(path))
+    t = rt.load_scene(str(path))
+    e = t.desc.contents
+    for field in ("sphere_count", "quad_count", "texture_count", "image_count", "perlin_count", "medium_count",
+                  "light_count", "material_count"):
+        assert getattr(d, field) == getattr(e, field), field
+    assert bytes(d.camera) == bytes(e.camera)
+    if name == "final":
+        assert d.sphere_count == 1006 and d.quad_count == 2401 and d.medium_count == 2
+        assert d.image_count == 1 and d.perlin_count == 1
+    if name == "bouncing":
+        assert any(d.spheres[i].displacement.y != 0 for i in range(d.sphere_count))
 
 
 def test_no_cpu_fallback_without_gpu(rt):

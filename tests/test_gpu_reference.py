@@ -24,6 +24,13 @@ CASES = [
     ("cornell-mis", dict(width=96, spp=64, combination="nee"), 64),
     ("env-furnace", dict(width=64, spp=16, combination="mis"), 16),
     ("ggx-furnace", dict(width=64, spp=16), 16),
+    ("bouncing", dict(width=96, spp=16), 16),
+    ("checker", dict(width=96, spp=16), 16),
+    ("earth", dict(width=96, spp=16, env_width=128), 16),
+    ("perlin", dict(width=96, spp=16), 16),
+    ("smoke", dict(width=64, spp=64), 64),
+    ("final", dict(width=64, spp=16, env_width=128), 16),
+    ("smoke", dict(width=64, spp=64, combination="mis"), 64),
 ]
 
 
@@ -37,8 +44,10 @@ def _consistent(oracle, a_fn, b_fn, seeds):
     raise AssertionError(f"ImageCompare failed twice: {reports}")
 
 
-def test_reference_furnace_is_exactly_one(rt):
-    s = rt.builtin_scene("furnace", width=64, spp=16)
+@pytest.mark.parametrize("name", ["furnace", "feature-furnace"])
+def test_reference_furnace_is_exactly_one(rt, name):
+    """The reference renders the converted tables (textures, motion and smoke included) as they mean: exactly 1."""
+    s = rt.builtin_scene(name, width=64, spp=16)
     img, info = ref_gpu.render(s.desc, s.width, s.height, seed=3)
     assert np.all(img == 1.0)
     assert info["rays"] >= s.width * s.height * 16

