@@ -141,8 +141,9 @@ def _builtin_params(width: int = 0, height: int = 0, spp: int = 0, depth: int = 
 
 
 def builtin_scene(name: str, **overrides) -> OwnedScene:
-    """A scene the library builds by name ("weekend", "cornell", "glass", "cornell-mis", "materials", "quads",
-    "furnace", "env-furnace", "ggx-furnace", "mesh-ggx", "cover-N"): the reference's scene code, flattened as its GPU
+    """A scene the library builds by name (the reference's "materials", "weekend", "bouncing", "checker", "earth",
+    "perlin", "quads", "light", "cornell", "smoke", "final", "aluminum", "glass"; "cornell-mis", "furnace",
+    "feature-furnace", "env-furnace", "ggx-furnace", "mesh-ggx", "cover-N"): the reference's scene code, flattened as its GPU
     translator flattens it. Overrides: width, height, spp, depth, sampling, combination, scene_seed, sphere_count,
     mesh_level, env_width, orbit=(azimuth, elevation) in degrees."""
     p = _builtin_params(**overrides)
