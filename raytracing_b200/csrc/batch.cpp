@@ -31,11 +31,12 @@ batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
     check(cudaEventCreate(&start_), "creating a CUDA event");
     check(cudaEventCreate(&stop_), "creating a CUDA event");
     kernel_attributes a{};
-    check(batch_attributes(false, a), "querying the batch kernel");
-    grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
-    check(batch_attributes(true, a), "querying the batch kernel");
-    flat_grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
-    work_counter_.allocate(2);
+    for (int g = 0; g < batch_groups; ++g)
+    {
+        check(batch_attributes(g, a), "querying the batch kernel");
+        grids_[g] = a.multiprocessors * std::max(1, a.blocks_per_sm);
+    }
+    work_counter_.allocate(batch_groups);
     header_.allocate(1);
     check(cudaMallocHost(reinterpret_cast<void**>(&header_host_), sizeof(batch_header)), "allocating pinned memory");
 }
@@ -172,8 +173,8 @@ void batch_engine::capture()
     check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capturing the batch step");
     cudaMemcpyAsync(table_.data(), table_host_, capacity_ * sizeof(batch_job), cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(header_.data(), header_host_, sizeof(batch_header), cudaMemcpyHostToDevice, stream_);
-    cudaMemsetAsync(work_counter_.data(), 0, 2 * sizeof(unsigned long long), stream_);
-    const cudaError_t launched = launch_batch(p, flat_grid_, grid_, stream_);
+    cudaMemsetAsync(work_counter_.data(), 0, batch_groups * sizeof(unsigned long long), stream_);
+    const cudaError_t launched = launch_batch(p, grids_, stream_);
     const cudaError_t ended = cudaStreamEndCapture(stream_, &graph_);
     check(launched, "capturing the batch kernels");
     check(ended, "capturing the batch step");
@@ -227,11 +228,23 @@ double batch_engine::step(std::vector<assignment> work)
         return 0;
     }
     ensure_capacity(work.size(), static_cast<size_t>(entries) * 3);
-    // The flat scenes' jobs first: their items form the flat search's launch
-    const auto flat_end = std::stable_partition(
-        work.begin(), work.end(), [&](const assignment& a) { return jobs_.at(a.handle)->scene->view().flat != 0; });
-    const auto flat_jobs = static_cast<size_t>(flat_end - work.begin());
-    int64_t flat_items = 0;
+    // The jobs in their groups' order (each group's items form its own launch)
+    const auto group_of = [&](const assignment& a) {
+        const scene_view& v = jobs_.at(a.handle)->scene->view();
+        return batch_group(v.flat != 0, has_features(v));
+    };
+    std::stable_sort(work.begin(), work.end(),
+                     [&](const assignment& a, const assignment& b) { return group_of(a) < group_of(b); });
+    batch_header& header = *header_host_;
+    header = batch_header{};
+    for (size_t i = 0; i < work.size(); ++i)
+    {
+        header.group_jobs[group_of(work[i]) + 1] = static_cast<int32_t>(i + 1);
+    }
+    for (int g = 1; g <= batch_groups; ++g)
+    {
+        header.group_jobs[g] = std::max(header.group_jobs[g], header.group_jobs[g - 1]);
+    }
     last_samples_ = 0;
     int64_t items = 0;
     int64_t pixels = 0;
@@ -260,19 +273,18 @@ double batch_engine::step(std::vector<assignment> work)
         b.sums = j.sums.data();
         b.counters = j.counters.data();
         items += int64_t{b.chunks} * b.padded_pixels;
-        if (i + 1 == flat_jobs)
-        {
-            flat_items = items;
-        }
         pixels += int64_t{j.camera.image_width} * j.camera.image_height;
         last_samples_ += int64_t{j.camera.image_width} * j.camera.image_height * (b.pass_end - b.pass_begin);
         partial_offset += int64_t{b.chunks} * b.padded_pixels;
     }
-    header_host_->total_items = items;
-    header_host_->total_pixels = pixels;
-    header_host_->flat_items = flat_items;
-    header_host_->job_count = static_cast<int32_t>(work.size());
-    header_host_->flat_jobs = static_cast<int32_t>(flat_jobs);
+    // Each group's item range: from its first job's start to the next group's
+    for (int g = 0; g <= batch_groups; ++g)
+    {
+        const int32_t first = header.group_jobs[g];
+        header.group_items[g] = first < static_cast<int32_t>(work.size()) ? table_host_[first].item_begin : items;
+    }
+    header.total_pixels = pixels;
+    header.job_count = static_cast<int32_t>(work.size());
     check(cudaEventRecord(start_, stream_), "recording a CUDA event");
     if (use_graph_)
     {
@@ -289,17 +301,16 @@ double batch_engine::step(std::vector<assignment> work)
               "copying the job table");
         check(cudaMemcpyAsync(header_.data(), header_host_, sizeof(batch_header), cudaMemcpyHostToDevice, stream_),
               "copying the batch header");
-        check(cudaMemsetAsync(work_counter_.data(), 0, 2 * sizeof(unsigned long long), stream_),
+        check(cudaMemsetAsync(work_counter_.data(), 0, batch_groups * sizeof(unsigned long long), stream_),
               "clearing the counters");
-        check(launch_batch(batch_params{table_.data(), header_.data(), work_counter_.data()}, flat_grid_, grid_,
-                           stream_),
+        check(launch_batch(batch_params{table_.data(), header_.data(), work_counter_.data()}, grids_, stream_),
               "launching the batch kernels");
     }
     check(cudaEventRecord(stop_, stream_), "recording a CUDA event");
     check(cudaEventSynchronize(stop_), "rendering the batch on the GPU");
     float ms = 0;
     check(cudaEventElapsedTime(&ms, start_, stop_), "timing the GPU");
-    launches_ += 3; // the flat and the tree launches, the reduction
+    launches_ += batch_groups + 1; // each group's launch (an empty group's ends at once), the reduction
     for (const assignment& a : work)
     {
         jobs_.at(a.handle)->passes = a.pass_end;

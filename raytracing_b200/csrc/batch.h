@@ -46,7 +46,7 @@ public:
     int launches() const { return launches_; }
     int64_t last_samples() const { return last_samples_; } // pixel passes the last step rendered
     bool graph_used() const { return graph_exec_ != nullptr; }
-    int grid() const { return grid_; }
+    int grid() const { return grids_[batch_groups - 1]; }
     // The chunks of [passes, pass_end) for a job of the given camera, and its padded pixel count
     static int64_t chunks_of(int64_t passes, int64_t pass_end);
     static int64_t padded_of(const rt_camera_desc& camera);
@@ -72,8 +72,7 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaEvent_t start_ = nullptr;
     cudaEvent_t stop_ = nullptr;
-    int grid_ = 0;      // the tree search's launch
-    int flat_grid_ = 0; // the flat search's launch
+    int grids_[batch_groups] = {}; // each group's launch (batch_group: flat or tree, with or without features)
     device_array<double> arena_;
     device_array<batch_job> table_;
     device_array<batch_header> header_;

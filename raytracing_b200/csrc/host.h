@@ -202,7 +202,10 @@ private:
     int64_t plan(int64_t target, double budget_seconds) const;
 };
 
-constexpr int pass_chunk = 16; // passes per work item; chunk boundaries are absolute multiples of it
+#ifndef RTB_PASS_CHUNK
+#define RTB_PASS_CHUNK 16
+#endif
+constexpr int pass_chunk = RTB_PASS_CHUNK; // passes per work item; chunk boundaries are absolute multiples of it
 } // namespace rtb
 
 // The C-ABI's opaque handles

@@ -657,10 +657,11 @@ __device__ __forceinline__ bool medium_stretch(const scene_view& S, const medium
 // camera.cuh:259-284). Each volume, in the list's order, against the closest event so far: a free flight of
 // -log(u) / density from where the ray enters it (medium_collision, constant_medium.cuh:86-120), u drawn from the
 // vertex's media blocks.
-// (Not inlined, like transmittance and texture_value: their registers stay out of the render loop's, which scenes
-// without smoke or textures never call them from.)
-__device__ __noinline__ void media_event(const scene_view& S, float3 o, float3 d, float time, const sampler& rng,
-                                         int depth,
+// (Like transmittance and texture_value: only the kernels of scenes with these features call them, so they are
+// inlined there; measured 5-10% faster on the second book's scenes than as calls.)
+#define RTB_FEATURE_FUNCTION __device__ __forceinline__
+RTB_FEATURE_FUNCTION void media_event(const scene_view& S, float3 o, float3 d, float time, const sampler& rng,
+                                      int depth,
                             hit_info& hit)
 {
     const float inverse_a = 1.0f / length_squared(d);
@@ -692,7 +693,7 @@ __device__ __noinline__ void media_event(const scene_view& S, float3 o, float3 d
 
 // The chance that (t_min, t_max) of the ray crosses every volume without meeting a particle: the expected value of
 // media_event's free-flight test over exactly the stretch it would test (transmittance, shadow.cuh:129-165)
-__device__ __noinline__ float transmittance(const scene_view& S, float3 o, float3 d, float time, float t_max)
+RTB_FEATURE_FUNCTION float transmittance(const scene_view& S, float3 o, float3 d, float time, float t_max)
 {
     const float inverse_a = 1.0f / length_squared(d);
     const float3 inv = make_float3(safe_inverse(d.x), safe_inverse(d.y), safe_inverse(d.z));
@@ -765,7 +766,7 @@ __device__ float turbulence(const noise_table& n, float3 p)
 // The texture's color at the hit (texture_value, texture.cuh:60-110): a checker is walked down to the texture of the
 // point's cube (its textures come before it, so the walk ends); an image is read at (u, v) clamped to [0, 1], v
 // flipped, the pixel they fall in; a marble is 0.5 (1 + sin(scale z + 10 turbulence(p))) in every channel
-__device__ __noinline__ float3 texture_value(const scene_view& S, int index, float u, float v, float3 p)
+RTB_FEATURE_FUNCTION float3 texture_value(const scene_view& S, int index, float u, float v, float3 p)
 {
     texture8 t = S.textures[index];
     while (t.kind == RT_TEXTURE_CHECKER)
@@ -1757,12 +1758,27 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
 #ifndef RTB_MIN_BLOCKS_QUALITY_FLAT
 #define RTB_MIN_BLOCKS_QUALITY_FLAT 7
 #endif
+// The kernels of scenes with the second book's features (textures, motion, smoke): 96 registers (5 blocks), measured
+// fastest against 72 and 80 on the final, smoke, perlin and light scenes (their textures and free flights spill)
+#ifndef RTB_MIN_BLOCKS_FEATURES
+#define RTB_MIN_BLOCKS_FEATURES 5 // 0: as the kernel without the features
+#endif
+
+template <bool QUALITY, bool FLAT, bool FEATURES>
+constexpr int render_min_blocks()
+{
+    if (FEATURES && RTB_MIN_BLOCKS_FEATURES > 0)
+    {
+        return RTB_MIN_BLOCKS_FEATURES;
+    }
+    return QUALITY ? (FLAT ? RTB_MIN_BLOCKS_QUALITY_FLAT : RTB_MIN_BLOCKS_QUALITY)
+                   : (FLAT ? RTB_MIN_BLOCKS_FLAT : RTB_MIN_BLOCKS);
+}
 
 // FEATURES: the scene has moving spheres, textures other than solid colors, or smoke (the counting build always
 // compiles them in)
 template <bool QUALITY, bool COUNT, bool FLAT, bool FEATURES>
-__global__ void __launch_bounds__(render_block, QUALITY ? (FLAT ? RTB_MIN_BLOCKS_QUALITY_FLAT : RTB_MIN_BLOCKS_QUALITY)
-                                                        : (FLAT ? RTB_MIN_BLOCKS_FLAT : RTB_MIN_BLOCKS))
+__global__ void __launch_bounds__(render_block, render_min_blocks<QUALITY, FLAT, FEATURES>())
     render_kernel(const __grid_constant__ launch_params P)
 {
     __shared__ unsigned long long block_rays;
@@ -1967,18 +1983,19 @@ __device__ __forceinline__ int find_job(const batch_job* jobs, int first, int en
 // fills with another's work. Each job may use either integrator. The jobs of flat scenes come first in the table and
 // the item space, and each search has its own launch (FLAT: items [0, flat_items) of jobs [0, flat_jobs); otherwise
 // the rest), compiled as render_kernel's for that search, so a job renders the same bits as its plain render.
-template <bool FLAT>
-__global__ void __launch_bounds__(render_block, FLAT ? RTB_MIN_BLOCKS_QUALITY_FLAT : RTB_MIN_BLOCKS_QUALITY)
+template <bool FLAT, bool FEATURES>
+__global__ void __launch_bounds__(render_block, render_min_blocks<true, FLAT, FEATURES>())
     render_batch_kernel(const batch_params P)
 {
     constexpr int search = FLAT ? search_flat : search_tree;
+    constexpr int group = batch_group(FLAT, FEATURES);
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
-    const int64_t item_begin = FLAT ? 0 : P.header->flat_items;
-    const int64_t total_items = FLAT ? P.header->flat_items : P.header->total_items;
-    const int job_first = FLAT ? 0 : P.header->flat_jobs;
-    const int job_end = FLAT ? P.header->flat_jobs : P.header->job_count;
-    unsigned long long* const work_counter = P.work_counter + (FLAT ? 0 : 1);
+    const int64_t item_begin = P.header->group_items[group];
+    const int64_t total_items = P.header->group_items[group + 1];
+    const int job_first = P.header->group_jobs[group];
+    const int job_end = P.header->group_jobs[group + 1];
+    unsigned long long* const work_counter = P.work_counter + group;
 
     uint32_t rays = 0;
     uint32_t shadow_rays = 0;
@@ -2048,7 +2065,7 @@ __global__ void __launch_bounds__(render_block, FLAT ? RTB_MIN_BLOCKS_QUALITY_FL
             rng.pass = static_cast<uint32_t>(in_round);
             const float4 u = rng.draw(0, 0);
             camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
-            ps.time = J->scene.has_motion ? rng.draw(0, block_time).x : 0.0f;
+            ps.time = FEATURES && J->scene.has_motion ? rng.draw(0, block_time).x : 0.0f;
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
             ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
             ps.bsdf_pdf = 0.0f;
@@ -2060,17 +2077,19 @@ __global__ void __launch_bounds__(render_block, FLAT ? RTB_MIN_BLOCKS_QUALITY_FL
             start = false;
         }
         hit_info h;
-        traverse<false, false, search>(J->scene, ps.o, ps.d, ps.time, infinity_f, ps.from, ps.inward, -1, h);
+        traverse<false, false, search, FEATURES>(J->scene, ps.o, ps.d, ps.time, infinity_f, ps.from, ps.inward, -1,
+                                                 h);
         ++rays;
         ++ps.depth;
-        if (J->scene.medium_count > 0)
+        if (FEATURES && J->scene.medium_count > 0)
         {
             media_event(J->scene, ps.o, ps.d, ps.time, rng, ps.depth, h);
         }
         float3 sample;
         const step_result r =
-            J->quality ? shade_quality<false, search>(J->scene, cam, rng, ps, h, sample, shadow_rays, nullptr)
-                       : shade_books(J->scene, cam, rng, ps, h, sample);
+            J->quality
+                ? shade_quality<false, search, FEATURES>(J->scene, cam, rng, ps, h, sample, shadow_rays, nullptr)
+                : shade_books<FEATURES>(J->scene, cam, rng, ps, h, sample);
         if (r == step_result::done)
         {
             acc_r += without_nan(sample.x);
@@ -2193,8 +2212,6 @@ render_function render_kernel_for(bool quality, bool counting, bool flat, bool f
     }
     return flat ? render_kernel_of<false, true>(counting, features) : render_kernel_of<false, false>(counting, features);
 }
-
-bool has_features(const scene_view& s) { return s.has_motion != 0 || s.has_textures != 0 || s.medium_count > 0; }
 } // namespace
 
 cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream)
@@ -2204,21 +2221,38 @@ cudaError_t launch_render(const launch_params& p, bool quality, bool counting, i
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch(const batch_params& p, int flat_grid, int tree_grid, cudaStream_t stream)
+namespace
 {
-    render_batch_kernel<true><<<flat_grid, render_block, 0, stream>>>(p);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess)
+using batch_function = void (*)(batch_params);
+
+batch_function batch_kernel_of(int group)
+{
+    switch (group)
     {
-        return e;
+    case 0:
+        return render_batch_kernel<true, false>;
+    case 1:
+        return render_batch_kernel<true, true>;
+    case 2:
+        return render_batch_kernel<false, false>;
+    default:
+        return render_batch_kernel<false, true>;
     }
-    render_batch_kernel<false><<<tree_grid, render_block, 0, stream>>>(p);
-    e = cudaGetLastError();
-    if (e != cudaSuccess)
+}
+} // namespace
+
+cudaError_t launch_batch(const batch_params& p, const int* grids, cudaStream_t stream)
+{
+    for (int g = 0; g < batch_groups; ++g)
     {
-        return e;
+        batch_kernel_of(g)<<<grids[g], render_block, 0, stream>>>(p);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+        {
+            return e;
+        }
     }
-    reduce_batch_kernel<<<tree_grid, 256, 0, stream>>>(p);
+    reduce_batch_kernel<<<grids[batch_groups - 1], 256, 0, stream>>>(p);
     return cudaGetLastError();
 }
 
@@ -2265,10 +2299,7 @@ cudaError_t attributes_of(Kernel kernel, kernel_attributes& out)
 }
 } // namespace
 
-cudaError_t batch_attributes(bool flat, kernel_attributes& out)
-{
-    return flat ? attributes_of(render_batch_kernel<true>, out) : attributes_of(render_batch_kernel<false>, out);
-}
+cudaError_t batch_attributes(int group, kernel_attributes& out) { return attributes_of(batch_kernel_of(group), out); }
 
 cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream)
 {
@@ -2278,9 +2309,9 @@ cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-cudaError_t render_attributes(bool quality, bool flat, kernel_attributes& out)
+cudaError_t render_attributes(const scene_view& scene, bool quality, kernel_attributes& out)
 {
-    return attributes_of(render_kernel_for(quality, false, flat, false), out);
+    return attributes_of(render_kernel_for(quality, false, scene.flat != 0, has_features(scene)), out);
 }
 
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,

@@ -72,20 +72,29 @@ struct alignas(16) batch_job
 
 // What changes from step to step besides the jobs: read from device memory, so that a captured graph of the step
 // replays with new contents
+// Whether a scene has any of the second book's features (moving spheres, textures other than solid colors, smoke):
+// its kernels are compiled with their code, the others without
+inline bool has_features(const scene_view& s) { return s.has_motion != 0 || s.has_textures != 0 || s.medium_count > 0; }
+
+// The jobs come in four groups, each rendered by its own launch of the kernel compiled for it: flat scenes without
+// the second book's features, flat scenes with them, then the same two of tree scenes (batch_group)
+constexpr int batch_groups = 4;
+RTB_HD constexpr int batch_group(bool flat, bool features) { return (flat ? 0 : 2) + (features ? 1 : 0); }
+
 struct batch_header
 {
-    int64_t total_items;
     int64_t total_pixels;
-    int64_t flat_items;     // the items of the flat scenes' jobs, which come first: [0, flat_items)
+    int64_t group_items[batch_groups + 1]; // group g's items are [group_items[g], group_items[g + 1])
+    int32_t group_jobs[batch_groups + 1];  // and its jobs [group_jobs[g], group_jobs[g + 1])
     int32_t job_count;
-    int32_t flat_jobs;      // jobs [0, flat_jobs) search flat
+    int32_t pad0;
 };
 
 struct batch_params
 {
     const batch_job* jobs;
     const batch_header* header;
-    unsigned long long* work_counter; // [0] the flat launch's, [1] the tree launch's
+    unsigned long long* work_counter; // one per group's launch
 };
 
 // The kernels' static properties for kernel_info
@@ -103,11 +112,12 @@ constexpr int render_block = 128;
 
 cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream);
 cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream);
-// The batched step: the persistent kernel over the flat scenes' items, the one over the other jobs' items, then the
+// The batched step: the persistent kernel of each group over its jobs' items (grids[g] threads blocks), then the
 // reduction of every job's pixels
-cudaError_t launch_batch(const batch_params& p, int flat_grid, int tree_grid, cudaStream_t stream);
-cudaError_t batch_attributes(bool flat, kernel_attributes& out);
-cudaError_t render_attributes(bool quality, bool flat, kernel_attributes& out);
+cudaError_t launch_batch(const batch_params& p, const int* grids, cudaStream_t stream);
+cudaError_t batch_attributes(int group, kernel_attributes& out);
+// The attributes of the render kernel that launch_render picks for the scene and integrator
+cudaError_t render_attributes(const scene_view& scene, bool quality, kernel_attributes& out);
 
 // Parity hooks: closest hits of given rays (source ids through prim_source), and the camera rays of one pass
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,

@@ -94,7 +94,7 @@ extern "C" rt_status rt_render_passes_no_alloc(rt_scene* scene, const rt_camera_
         auto* counters = reinterpret_cast<unsigned long long*>(scratch);
         auto* partials = reinterpret_cast<double*>(scratch + counter_bytes);
         rtb::kernel_attributes a{};
-        rtb::check(rtb::render_attributes(s.quality(), s.view().flat != 0, a), "querying the render kernel");
+        rtb::check(rtb::render_attributes(s.view(), s.quality(), a), "querying the render kernel");
         const int grid = a.multiprocessors * (a.blocks_per_sm > 0 ? a.blocks_per_sm : 1);
         const int64_t max_chunks = partial_entries / padded;
         const cudaStream_t stream = nullptr;

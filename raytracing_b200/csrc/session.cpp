@@ -37,7 +37,7 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
     check(cudaEventCreate(&start_), "creating a CUDA event");
     check(cudaEventCreate(&stop_), "creating a CUDA event");
     kernel_attributes a{};
-    check(render_attributes(scene_->quality(), scene_->view().flat != 0, a), "querying the render kernel");
+    check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
     grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
     counters_.allocate(7);
     set_camera(scene_->camera());
@@ -272,7 +272,7 @@ uint64_t session::shadow_rays() const
 rt_kernel_info session::kernel() const
 {
     kernel_attributes a{};
-    check(render_attributes(scene_->quality(), scene_->view().flat != 0, a), "querying the render kernel");
+    check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
     rt_kernel_info info{};
     std::snprintf(info.name, sizeof(info.name), "%s", scene_->quality() ? "persistent nee-mis" : "persistent books");
     info.registers = a.registers;

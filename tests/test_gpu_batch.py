@@ -39,7 +39,7 @@ def test_batch_equals_plain_renders(rt):
     jobs = _mixed_scenes(rt)
     b = rt.batch_render(jobs)
     assert b.graph
-    assert b.steps >= 1 and b.launches == 3 * b.steps
+    assert b.steps >= 1 and b.launches == 5 * b.steps  # four groups' launches and the reduction
     for (scene, seed, passes), img in zip(jobs, b.images):
         ref = rt.render(scene, seed=seed, passes=passes)
         assert img.shape == ref.pixels.shape
