@@ -31,6 +31,8 @@ import numpy as np
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
+from raytracing_b200 import shard  # noqa: E402  (pure Python: the split of the work over ranks)
+
 METRIC = "path segments/s at matched ImageCompare error; served p50/p99 vs plain launch"
 UNIT = "segments/s"
 
@@ -199,10 +201,14 @@ def batched_jobs(rt, count: int = 64, seed: int = 2024):
     return jobs
 
 
-def batched_measurement(rt, torch) -> dict:
+def batched_measurement(rt, torch, rank: int = 0, world: int = 1) -> dict:
     """64 jobs in one batched render (one persistent launch per step, replayed as a CUDA graph) against the plain
-    form (one render per job), on the same jobs and seeds; every job's image compared bit for bit."""
-    jobs = batched_jobs(rt)
+    form (one render per job), on the same jobs and seeds; every job's image compared bit for bit. With N ranks the
+    jobs are split by cost (pixels x passes, longest first to the least loaded rank) and each rank renders its share
+    on its own GPU: the times are the slowest rank's, the segments everyone's (no collective on the data)."""
+    all_jobs = batched_jobs(rt)
+    costs = [s.width * s.height * p for s, _, p in all_jobs]
+    jobs = [all_jobs[i] for i in shard.my_units(costs, world, rank)]
     rt.batch_render(jobs[:4])  # warm-up (graph capture, module load)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -221,12 +227,17 @@ def batched_measurement(rt, torch) -> dict:
         plain_rays += r.rays
         identical += int(np.array_equal(r.pixels, img))
         max_diff = max(max_diff, abs(float(img.mean()) - float(r.pixels.mean())) / max(float(r.pixels.mean()), 1e-9))
-    pixels = sum(s.width * s.height for s, _, _ in jobs)
-    samples = sum(s.width * s.height * p for s, _, p in jobs)
+    pixels = sum(s.width * s.height for s, _, _ in all_jobs)
+    samples = sum(costs)
+    batch_gpu, batch_rays = shard.combine(b.gpu_seconds, b.rays)
+    batch_wall, _ = shard.combine(batch_wall, 0)
+    plain_kernel, plain_rays = shard.combine(plain_kernel, plain_rays)
+    plain_wall, _ = shard.combine(plain_wall, 0)
+    _, identical = shard.combine(0, identical)
     reference = {}
     from oracle import ref_gpu
 
-    if ref_gpu.available():
+    if ref_gpu.available() and world == 1:
         ref_rays = 0
         ref_kernel = 0.0
         ref_wall = 0.0
@@ -237,20 +248,20 @@ def batched_measurement(rt, torch) -> dict:
             ref_wall += info["seconds"]
         reference = {"reference_plain_segments_per_s": ref_rays / ref_kernel, "reference_plain_gpu_s": ref_kernel,
                      "reference_plain_e2e_s": ref_wall,
-                     "speedup_gpu_over_reference": (b.rays / b.gpu_seconds) / (ref_rays / ref_kernel),
+                     "speedup_gpu_over_reference": (batch_rays / batch_gpu) / (ref_rays / ref_kernel),
                      "speedup_e2e_over_reference": ref_wall / batch_wall}
     return {**reference, "workload": "64 cover-scene variants (50-2000 spheres, W,H log-uniform 64-1024, spp log-uniform "
                         "16-1024, seeds 0-63), mixture of sizes in one persistent launch per step",
-            "pixels": pixels, "samples": samples, "segments": b.rays,
-            "batched_segments_per_s": b.rays / b.gpu_seconds, "batched_gpu_s": b.gpu_seconds,
-            "batched_e2e_segments_per_s": b.rays / batch_wall, "batched_e2e_s": batch_wall,
+            "ranks": world, "pixels": pixels, "samples": samples, "segments": batch_rays,
+            "batched_segments_per_s": batch_rays / batch_gpu, "batched_gpu_s": batch_gpu,
+            "batched_e2e_segments_per_s": batch_rays / batch_wall, "batched_e2e_s": batch_wall,
             "batched_setup_s": b.setup_seconds, "batched_steps": b.steps, "batched_launches": b.launches,
             "graph": b.graph,
             "plain_segments_per_s": plain_rays / plain_kernel, "plain_gpu_s": plain_kernel,
             "plain_e2e_segments_per_s": plain_rays / plain_wall, "plain_e2e_s": plain_wall,
-            "speedup_gpu": (b.rays / b.gpu_seconds) / (plain_rays / plain_kernel),
+            "speedup_gpu": (batch_rays / batch_gpu) / (plain_rays / plain_kernel),
             "speedup_e2e": plain_wall / batch_wall,
-            "jobs_bit_identical_to_plain": f"{identical}/{len(jobs)}",
+            "jobs_bit_identical_to_plain": f"{int(identical)}/{len(all_jobs)}",
             "max_relative_mean_difference_to_plain": max_diff}
 
 
@@ -466,16 +477,8 @@ def run_b200(args):
         launches += report["launches"]
     clock_info = clocks.stop()
     del rays0
-    step_seconds = sum(times)
-    if dist:
-        t = torch.tensor([step_seconds], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_seconds = float(t.item())
-        r = torch.tensor([float(total_rays)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(r, op=dist.ReduceOp.SUM)
-        all_rays = float(r.item())
-    else:
-        all_rays = float(total_rays)
+    # the slowest rank's time, every rank's segments (no collective on the data path: each rank's image is its own)
+    step_seconds, all_rays = shard.combine(sum(times), total_rays)
     value = all_rays / step_seconds
 
     peaks = read_peaks()
@@ -524,13 +527,7 @@ def run_b200(args):
             e_seconds += start.elapsed_time(end) / 1000.0
             e_rays += res.rays
             del t0
-        if dist:
-            t = torch.tensor([e_seconds], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_seconds = float(t.item())
-            r = torch.tensor([float(e_rays)], dtype=torch.float64, device="cuda")
-            dist.all_reduce(r, op=dist.ReduceOp.SUM)
-            e_rays = float(r.item())
+        e_seconds, e_rays = shard.combine(e_seconds, e_rays)
         if rank == 0:
             line["e2e"] = {"value": e_rays / e_seconds, "unit": UNIT, "h2d_bytes_per_step": int(stats["device_bytes"]),
                            "d2h_bytes_per_step": int(out.nbytes),
@@ -559,8 +556,10 @@ def run_b200(args):
 
     if rank == 0 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_measurement(scene_desc, passes, line["value"])
-    if rank == 0 and not args.no_batched:
-        line["batched"] = batched_measurement(rt, torch)
+    if not args.no_batched:
+        batched = batched_measurement(rt, torch, rank, world)  # every rank: its share of the 64 jobs
+        if rank == 0:
+            line["batched"] = batched
     if rank == 0 and args.served:
         line["served"] = served_measurement(rt, torch, args)
 
