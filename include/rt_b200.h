@@ -237,11 +237,18 @@ typedef struct rt_device_info
     double memory_gib;
 } rt_device_info;
 
+/* How a session's launches run (no counterpart in the reference, whose renderer has one kernel): the persistent
+   kernel, whose lanes each carry a path from its camera ray to its end, or the wavefront, whose paths wait in device
+   memory between a shade kernel and a trace kernel that gives each lane a new ray as soon as its own is answered.
+   Both make the same image from the same seed. AUTO takes the wavefront for scenes searched through the tree and the
+   persistent kernel for the small ones searched flat (and for the counting build). */
+enum { RT_FORM_AUTO = 0, RT_FORM_PERSISTENT = 1, RT_FORM_WAVEFRONT = 2 };
+
 typedef struct rt_session_options
 {
     uint64_t seed;
     int32_t arithmetic;         /* RT_FLOAT32 */
-    int32_t pad0;
+    int32_t form;               /* RT_FORM_*; 0 (AUTO) where the caller zeroed the struct */
     double launch_seconds;
 } rt_session_options;
 

@@ -25,6 +25,7 @@ __all__ = ["RenderError", "LogicError", "NoDeviceError", "UnsupportedError", "Ca
 
 SAMPLING = {"uniform": RT_SAMPLING_UNIFORM, "material": RT_SAMPLING_MATERIAL, "lights": RT_SAMPLING_LIGHTS,
             "mixture": RT_SAMPLING_MIXTURE}
+FORMS = {"auto": _abi.RT_FORM_AUTO, "persistent": _abi.RT_FORM_PERSISTENT, "wavefront": _abi.RT_FORM_WAVEFRONT}
 COMBINATION = {"material": RT_COMBINE_BSDF_ONLY, "nee": RT_COMBINE_LIGHTS_ONLY, "mis": RT_COMBINE_POWER_HEURISTIC}
 
 
@@ -273,9 +274,11 @@ class Scene:
 class Session:
     """renderer.h:591-673 session: one view whose image gains passes on demand; its sums stay on the device."""
 
-    def __init__(self, scene: Scene, seed: int = 0, launch_seconds: float = 0.05):
+    def __init__(self, scene: Scene, seed: int = 0, launch_seconds: float = 0.05, form: str = "auto"):
+        """form: "auto", "persistent" or "wavefront" (FORMS): how the launches run; the image is the same."""
         self._scene = scene
-        o = _abi.SessionOptions(seed=seed, arithmetic=_abi.RT_FLOAT32, launch_seconds=launch_seconds)
+        o = _abi.SessionOptions(seed=seed, arithmetic=_abi.RT_FLOAT32, form=FORMS[form],
+                                launch_seconds=launch_seconds)
         handle = C.c_void_p()
         _check(_lib().rt_session_create(scene._handle, C.byref(o), C.byref(handle)))
         self._handle = handle

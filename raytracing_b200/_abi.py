@@ -16,6 +16,7 @@ RT_SAMPLING_UNIFORM, RT_SAMPLING_MATERIAL, RT_SAMPLING_LIGHTS, RT_SAMPLING_MIXTU
 RT_COMBINE_BSDF_ONLY, RT_COMBINE_LIGHTS_ONLY, RT_COMBINE_POWER_HEURISTIC = range(3)
 RT_MICROFACET_NONE, RT_MICROFACET_CONDUCTOR, RT_MICROFACET_GLOSS = range(3)
 RT_FLOAT32, RT_FLOAT64 = range(2)
+RT_FORM_AUTO, RT_FORM_PERSISTENT, RT_FORM_WAVEFRONT = range(3)
 
 
 class Vec3(C.Structure):
@@ -123,7 +124,7 @@ class DeviceInfo(C.Structure):
 
 
 class SessionOptions(C.Structure):
-    _fields_ = [("seed", C.c_uint64), ("arithmetic", C.c_int32), ("pad0", C.c_int32),
+    _fields_ = [("seed", C.c_uint64), ("arithmetic", C.c_int32), ("form", C.c_int32),
                 ("launch_seconds", C.c_double)]
 
 

@@ -197,8 +197,28 @@ private:
     int padded_pixels_ = 0;
     int64_t max_partial_entries_ = 0;
 
+    // The wavefront form (RT_FORM_WAVEFRONT, or AUTO on a tree-searched scene): its slots, queue and results, sized
+    // on the first launch that uses it; two pinned words take the queue's length back to the host
+    bool wavefront_ = false;
+    device_array<unsigned char> wave_slots_;
+    device_array<float4> query_o_;
+    device_array<float4> query_d_;
+    device_array<int4> query_meta_;
+    device_array<int4> ext_result_;
+    device_array<int32_t> shadow_result_;
+    device_array<unsigned> wave_control_;
+    device_array<float4> wave_samples_;
+    unsigned* wave_queued_ = nullptr; // pinned: the queue's length after each group of steps, two groups in flight
+    cudaEvent_t wave_done_[2] = {nullptr, nullptr};
+    int wave_max_slots_ = 0;
+    int trace_grid_ = 0;
+
     // Renders passes [passes_, end) in one launch and its reduction; returns its GPU seconds
     double launch(int64_t end);
+    // The wavefront's buffers for a launch of `samples` samples (allocated on first use, grown as needed), and its
+    // steps over them until a step queues no ray
+    wave_buffers wave_setup(int64_t samples);
+    void run_wavefront(const launch_params& p, const wave_buffers& b);
     int64_t plan(int64_t target, double budget_seconds) const;
 };
 

@@ -346,11 +346,12 @@ __device__ __forceinline__ float4 sphere_at(const scene_view& S, int i, float ti
     return s;
 }
 
-// The leaf's primitives against the ray, shrinking hit.t; true at the first hit for a shadow ray
+// The leaf's primitives against the ray, shrinking hit.t; true at the first hit for a shadow ray (SHADOW, or `any`
+// for a kernel that walks both kinds of ray)
 template <bool SHADOW, bool COUNT, bool FEATURES>
 __device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 o, float3 d, float time,
                                           float inverse_a, int from, bool inward, int skip, hit_info& hit,
-                                          fetch_counts* counts)
+                                          fetch_counts* counts, bool any = false)
 {
     const int kind = leaf_kind(link);
     const int count = leaf_count(link);
@@ -374,7 +375,7 @@ __device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 
             bool entering;
             if (hit_sphere(s, o, d, inverse_a, t_min, hit.t, own, t, entering))
             {
-                if (SHADOW)
+                if (SHADOW || any)
                 {
                     return true;
                 }
@@ -396,7 +397,7 @@ __device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 
             bool front;
             if (hit_quad(q, o, d, t_min, hit.t, t, front))
             {
-                if (SHADOW)
+                if (SHADOW || any)
                 {
                     return true;
                 }
@@ -418,7 +419,7 @@ __device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 
             bool front;
             if (hit_triangle(tr, o, d, t_min, hit.t, t, front))
             {
-                if (SHADOW)
+                if (SHADOW || any)
                 {
                     return true;
                 }
@@ -1527,11 +1528,27 @@ __device__ float3 eval_lobe(int lobe, const material12& m, float3 albedo, float3
     return make_float3(0.0f, 0.0f, 0.0f);
 }
 
-// One segment of an NEE/MIS path after its closest hit; the shadow ray is traced here
-template <bool COUNT, int SEARCH = search_any, bool FEATURES = true>
+// A shadow ray handed back to the caller instead of traced (the wavefront's trace kernel walks it): the ray, and the
+// light it brings to the path's radiance if nothing blocks it
+struct shadow_query
+{
+    float3 o, d;
+    float3 contribution;
+    float t_max;
+    int from;
+    int skip;
+    bool inward;
+    bool lit;
+};
+
+// One segment of an NEE/MIS path after its closest hit; the shadow ray is traced here, or with DEFER handed back in
+// `deferred` (lit set) with the path's radiance left without it: a `done` sample then is the radiance once the
+// caller has added the light
+template <bool COUNT, int SEARCH = search_any, bool FEATURES = true, bool DEFER = false>
 __device__ __forceinline__ step_result shade_quality(const scene_view& S, const camera_params& cam,
                                                      const sampler& rng, path_state& ps, const hit_info& h,
-                                                     float3& sample, uint32_t& shadow_rays, fetch_counts* counts)
+                                                     float3& sample, uint32_t& shadow_rays, fetch_counts* counts,
+                                                     shadow_query* deferred = nullptr)
 {
     if (h.id < 0)
     {
@@ -1701,7 +1718,17 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
                                                                        : refract(ud, s.normal, ri);
         weight = make_float3(1.0f, 1.0f, 1.0f);
     }
-    if (lit)
+    if (DEFER)
+    {
+        deferred->lit = lit;
+        if (lit)
+        {
+            ++shadow_rays;
+            *deferred = {s.p, light_dir, contribution, light_distance, s.from, skip, dot(light_dir, s.outward) < 0.0f,
+                         true};
+        }
+    }
+    else if (lit)
     {
         ++shadow_rays;
         hit_info blocker;
@@ -2185,6 +2212,532 @@ __global__ void camera_rays_kernel(const camera_params cam, uint64_t seed, int64
     directions[3 * i + 1] = d.y;
     directions[3 * i + 2] = d.z;
 }
+
+// ---- the wavefront form: resident path slots, a shade kernel and a trace kernel ----------------------------------
+// In the persistent kernel a warp walks the tree for all its lanes' rays together, and a lane whose ray left the
+// scene at the root waits for the lane whose ray goes deepest: on the mesh and the sphere grids a walk step runs with
+// 4 to 10 of 32 lanes. Here the walk is a kernel of its own whose lanes take a new ray as soon as theirs is answered
+// (Aila and Laine's persistent while-while with replacement of finished rays, HPG 2009 and its 2012 addendum), and the
+// paths between walks live in HBM as slots. A slot goes through the same steps, in the same order and with the same
+// arithmetic, as a persistent kernel's lane: the images are the persistent kernel's.
+constexpr uint32_t wave_exhausted = 1u; // no work item left for the slot
+constexpr uint32_t wave_ext = 2u;       // the path's next ray is queued (its hit comes back in ext_result)
+constexpr uint32_t wave_shadow = 4u;    // a shadow ray is queued (blocked or not comes back in shadow_result)
+constexpr uint32_t wave_finish = 8u;    // the sample ended at the shadow ray's vertex: it completes once the ray is in
+
+// A slot in HBM, structure of arrays: seven float4 rows of the path and its sample, three of its pending shadow ray,
+// each row slot_count long, so that a warp's loads and stores of a row are 512 contiguous bytes
+constexpr int wave_rows = 7;
+constexpr int wave_shadow_rows = 3;
+constexpr uint32_t wave_specular = 1u << 8;
+constexpr uint32_t wave_inward = 1u << 9;
+constexpr uint32_t wave_shadow_inward = 1u << 10;
+
+constexpr unsigned full_warp = 0xffffffffu;
+
+// The shade kernel's resident blocks per multiprocessor: 0 takes the persistent kernel's for the integrator
+#ifndef RTB_WAVE_SHADE_MIN_BLOCKS
+#define RTB_WAVE_SHADE_MIN_BLOCKS 0
+#endif
+template <bool QUALITY, bool FEATURES>
+constexpr int wave_shade_min_blocks()
+{
+    return RTB_WAVE_SHADE_MIN_BLOCKS > 0 ? RTB_WAVE_SHADE_MIN_BLOCKS : render_min_blocks<QUALITY, false, FEATURES>();
+}
+
+// A slot's step: the last walk's answers, the shading, the sample's end, a new sample, the next rays queued
+template <bool QUALITY, bool FEATURES>
+__global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, FEATURES>())
+    wave_shade_kernel(const __grid_constant__ launch_params P, const __grid_constant__ wave_buffers B)
+{
+    __shared__ unsigned long long block_rays;
+    __shared__ unsigned long long block_shadow_rays;
+    if (threadIdx.x == 0)
+    {
+        block_rays = 0;
+        block_shadow_rays = 0;
+    }
+    __syncthreads();
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    const int n = B.slot_count;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lanes_below = (1u << lane) - 1u;
+    float4* rows = static_cast<float4*>(B.slots);
+    float4* shadow_rows = rows + static_cast<int64_t>(wave_rows) * n;
+    const int4 r5 = reinterpret_cast<const int4*>(rows)[5 * n + i];
+    uint32_t flags = static_cast<uint32_t>(r5.y);
+    uint32_t rays = 0;
+    uint32_t shadow_rays = 0;
+    // a warp whose slots have all run out of work has nothing left to do in this launch
+    if (!__all_sync(full_warp, (flags & wave_exhausted) != 0u))
+    {
+        const bool live = (flags & wave_exhausted) == 0u;
+        const camera_params& cam = P.cam;
+        path_state ps;
+        sampler rng;
+        shadow_query sq;
+        int64_t sample_index = 0, pass = 0;
+        int px = r5.z, py = r5.w;
+        bool need = false;
+        bool start = false;
+        rng.job = P.job;
+        if (live)
+        {
+            const float4 r0 = rows[i];
+            const float4 r1 = rows[n + i];
+            const float4 r2 = rows[2 * n + i];
+            const float4 r3 = rows[3 * n + i];
+            const int4 r4 = reinterpret_cast<const int4*>(rows)[4 * n + i];
+            const longlong2 r6 = reinterpret_cast<const longlong2*>(rows)[6 * n + i];
+            ps.o = make_float3(r0.x, r0.y, r0.z);
+            ps.time = r0.w;
+            ps.d = make_float3(r1.x, r1.y, r1.z);
+            ps.bsdf_pdf = r1.w;
+            ps.throughput = make_float3(r2.x, r2.y, r2.z);
+            ps.radiance = make_float3(r2.w, r3.x, r3.y);
+            rng.key = make_uint2(__float_as_uint(r3.z), __float_as_uint(r3.w));
+            rng.pixel = static_cast<uint32_t>(r4.x);
+            rng.pass = static_cast<uint32_t>(r4.y);
+            ps.from = r4.z;
+            ps.rays_left = r4.w;
+            ps.depth = r5.x;
+            ps.specular = (flags & wave_specular) != 0u;
+            ps.inward = (flags & wave_inward) != 0u;
+            sample_index = r6.x;
+            pass = r6.y;
+            bool finished = false;
+            float3 sample = make_float3(0.0f, 0.0f, 0.0f);
+            if (flags & wave_shadow)
+            {
+                if (B.shadow_result[i] == 0)
+                {
+                    const float4 q0 = shadow_rows[i];
+                    const float4 q1 = shadow_rows[n + i];
+                    const int4 q2 = reinterpret_cast<const int4*>(shadow_rows)[2 * n + i];
+                    const float3 contribution = make_float3(q1.w, __int_as_float(q2.x), __int_as_float(q2.y));
+                    // through smoke, the light arrives with the chance of crossing it (its expected value)
+                    const float through =
+                        FEATURES && P.scene.medium_count > 0
+                            ? transmittance(P.scene, make_float3(q0.x, q0.y, q0.z), make_float3(q1.x, q1.y, q1.z),
+                                            ps.time, q0.w)
+                            : 1.0f;
+                    ps.radiance = ps.radiance + through * contribution;
+                }
+                flags &= ~wave_shadow;
+            }
+            if (flags & wave_finish)
+            {
+                sample = ps.radiance;
+                finished = true;
+                flags &= ~wave_finish;
+            }
+            else if (flags & wave_ext)
+            {
+                const int4 r = B.ext_result[i];
+                hit_info h;
+                h.id = r.x;
+                h.t = __int_as_float(r.y);
+                h.front = r.z != 0;
+                ++rays;
+                ++ps.depth;
+                if (FEATURES && P.scene.medium_count > 0)
+                {
+                    media_event(P.scene, ps.o, ps.d, ps.time, rng, ps.depth, h);
+                }
+                step_result res;
+                if (QUALITY)
+                {
+                    sq.lit = false; // a vertex that ends the path before its light sample queues no shadow ray
+                    res = shade_quality<false, search_tree, FEATURES, true>(P.scene, cam, rng, ps, h, sample,
+                                                                            shadow_rays, nullptr, &sq);
+                    if (sq.lit)
+                    {
+                        flags |= wave_shadow;
+                    }
+                }
+                else
+                {
+                    res = shade_books<FEATURES>(P.scene, cam, rng, ps, h, sample);
+                }
+                if (res == step_result::done)
+                {
+                    flags &= ~wave_ext;
+                    if (flags & wave_shadow)
+                    {
+                        flags |= wave_finish; // the sample's value waits for its last shadow ray
+                    }
+                    else
+                    {
+                        finished = true;
+                    }
+                }
+            }
+            else
+            {
+                need = true; // a slot without a sample
+            }
+            if (finished)
+            {
+                // the sample's value, added into its chunk's partial in pass order by the reduction
+                B.samples[sample_index] = make_float4(sample.x, sample.y, sample.z, 0.0f);
+                need = true;
+            }
+        }
+        // Samples for the slots that need one, a pass of the image after another: one atomic per warp
+        while (true)
+        {
+            const unsigned needing = __ballot_sync(full_warp, need);
+            if (needing == 0u)
+            {
+                break;
+            }
+            const int leader = __ffs(static_cast<int>(needing)) - 1;
+            unsigned long long base = 0;
+            if (static_cast<int>(lane) == leader)
+            {
+                base = atomicAdd(P.work_counter, static_cast<unsigned long long>(__popc(needing)));
+            }
+            base = __shfl_sync(full_warp, base, leader);
+            if (need)
+            {
+                const unsigned long long s = base + static_cast<unsigned long long>(__popc(needing & lanes_below));
+                if (s >= static_cast<unsigned long long>(B.sample_count))
+                {
+                    flags |= wave_exhausted;
+                    need = false;
+                }
+                else
+                {
+                    const int64_t j = static_cast<int64_t>(s / static_cast<unsigned long long>(P.padded_pixels));
+                    const int q = static_cast<int>(s % static_cast<unsigned long long>(P.padded_pixels));
+                    const int tile = q >> 5;
+                    const int l = q & 31;
+                    const int x = (tile % P.tiles_x) * 8 + (l & 7);
+                    const int y = (tile / P.tiles_x) * 4 + (l >> 3);
+                    if (x < cam.width && y < cam.height) // a lane of a tile over the image's edge claims again
+                    {
+                        px = x;
+                        py = y;
+                        sample_index = static_cast<int64_t>(s);
+                        pass = P.pass_begin + j;
+                        rng.pixel = static_cast<uint32_t>(y) * static_cast<uint32_t>(cam.width) + static_cast<uint32_t>(x);
+                        need = false;
+                        start = true;
+                    }
+                }
+            }
+        }
+        if (start)
+        {
+            // A new sample, as the persistent kernel starts one
+            const int64_t round = pass / P.round_passes;
+            const int in_round = static_cast<int>(pass - round * P.round_passes);
+            const uint64_t key = P.seed + (static_cast<uint64_t>(round) << 32);
+            rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
+            rng.pass = static_cast<uint32_t>(in_round);
+            const float4 u = rng.draw(0, 0);
+            camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
+            ps.time = FEATURES && P.scene.has_motion ? rng.draw(0, block_time).x : 0.0f;
+            ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
+            ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
+            ps.bsdf_pdf = 0.0f;
+            ps.specular = true;
+            ps.rays_left = cam.max_depth;
+            ps.depth = 0;
+            ps.from = -1;
+            ps.inward = false;
+            flags |= wave_ext;
+        }
+        // The slot's queries: one atomic per warp for its next rays and its shadow rays
+        const bool ext = (flags & wave_ext) != 0u;
+        const bool shadow = QUALITY && (flags & wave_shadow) != 0u;
+        const unsigned ext_lanes = __ballot_sync(full_warp, ext);
+        const unsigned shadow_lanes = __ballot_sync(full_warp, shadow);
+        const int queued = __popc(ext_lanes) + __popc(shadow_lanes);
+        if (queued > 0)
+        {
+            unsigned base = 0;
+            if (lane == 0u)
+            {
+                base = atomicAdd(B.control, static_cast<unsigned>(queued));
+            }
+            base = __shfl_sync(full_warp, base, 0);
+            if (ext)
+            {
+                const unsigned q = base + static_cast<unsigned>(__popc(ext_lanes & lanes_below));
+                B.query_o[q] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time);
+                B.query_d[q] = make_float4(ps.d.x, ps.d.y, ps.d.z, infinity_f);
+                B.query_meta[q] = make_int4(ps.from, ps.inward ? 1 : 0, -1, i);
+            }
+            if (shadow)
+            {
+                const unsigned q = base + static_cast<unsigned>(__popc(ext_lanes)) +
+                                   static_cast<unsigned>(__popc(shadow_lanes & lanes_below));
+                B.query_o[q] = make_float4(sq.o.x, sq.o.y, sq.o.z, ps.time);
+                B.query_d[q] = make_float4(sq.d.x, sq.d.y, sq.d.z, sq.t_max);
+                B.query_meta[q] = make_int4(sq.from, (sq.inward ? 1 : 0) | 2, sq.skip, i);
+                // what the next step needs of it: the light it brings and, through smoke, its segment
+                shadow_rows[i] = make_float4(sq.o.x, sq.o.y, sq.o.z, sq.t_max);
+                shadow_rows[n + i] = make_float4(sq.d.x, sq.d.y, sq.d.z, sq.contribution.x);
+                reinterpret_cast<int4*>(shadow_rows)[2 * n + i] =
+                    make_int4(__float_as_int(sq.contribution.y), __float_as_int(sq.contribution.z), 0, 0);
+            }
+        }
+        if (live)
+        {
+            flags = (flags & ~(wave_specular | wave_inward)) | (ps.specular ? wave_specular : 0u) |
+                    (ps.inward ? wave_inward : 0u);
+            if (flags & wave_exhausted)
+            {
+                reinterpret_cast<int4*>(rows)[5 * n + i] = make_int4(0, static_cast<int>(flags), px, py);
+            }
+            else
+            {
+                rows[i] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time);
+                rows[n + i] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf);
+                rows[2 * n + i] = make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x);
+                rows[3 * n + i] =
+                    make_float4(ps.radiance.y, ps.radiance.z, __uint_as_float(rng.key.x), __uint_as_float(rng.key.y));
+                reinterpret_cast<int4*>(rows)[4 * n + i] = make_int4(static_cast<int>(rng.pixel),
+                                                                     static_cast<int>(rng.pass), ps.from, ps.rays_left);
+                reinterpret_cast<int4*>(rows)[5 * n + i] = make_int4(ps.depth, static_cast<int>(flags), px, py);
+                reinterpret_cast<longlong2*>(rows)[6 * n + i] = make_longlong2(sample_index, pass);
+            }
+        }
+    }
+    if (rays)
+    {
+        atomicAdd(&block_rays, static_cast<unsigned long long>(rays));
+    }
+    if (QUALITY && shadow_rays)
+    {
+        atomicAdd(&block_shadow_rays, static_cast<unsigned long long>(shadow_rays));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        if (block_rays)
+        {
+            atomicAdd(P.counters, block_rays);
+        }
+        if (QUALITY && block_shadow_rays)
+        {
+            atomicAdd(P.counters + 1, block_shadow_rays);
+        }
+    }
+}
+
+// The trace kernel's resident blocks per multiprocessor (64 registers at 8) and the number of lanes still walking
+// under which a warp stops to give its idle lanes new queries (the addendum's 20 of 32)
+#ifndef RTB_TRACE_MIN_BLOCKS
+#define RTB_TRACE_MIN_BLOCKS 8
+#endif
+#ifndef RTB_REFILL_LANES
+#define RTB_REFILL_LANES 20
+#endif
+
+// The queued queries' walks through the tree: closest hits for the paths' next rays, any hit for shadow rays (the
+// persistent kernel's traverse, the same node order, leaf tests and self-intersection rules)
+template <bool FEATURES>
+__global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
+    wave_trace_kernel(const __grid_constant__ scene_view S, const __grid_constant__ wave_buffers B)
+{
+    const unsigned count = B.control[0];
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned lanes_below = (1u << lane) - 1u;
+    int2 stack[max_bvh_depth];
+    int sp = 0;
+    int link = traversal_done;
+    int leaf = 0;
+    bool has_query = false;
+    bool drained = false; // the warp found the queue empty: no idle lane can take a query any more
+    float3 o = make_float3(0.0f, 0.0f, 0.0f);
+    float3 d = o, inv = o, os = o;
+    float time = 0.0f;
+    float inverse_a = 0.0f;
+    int from = -1, skip = -1, slot = 0;
+    bool inward = false, shadow = false;
+    hit_info hit{-1, 0.0f, false};
+    const auto pop = [&]() -> int {
+        while (sp > 0)
+        {
+            const int2 e = stack[--sp];
+            if (shadow || __int_as_float(e.y) < hit.t)
+            {
+                return e.x;
+            }
+        }
+        return traversal_done;
+    };
+    while (true)
+    {
+        const bool idle = link == traversal_done && leaf == 0;
+        if (idle && has_query)
+        {
+            if (shadow)
+            {
+                B.shadow_result[slot] = hit.id >= 0 ? 1 : 0;
+            }
+            else
+            {
+                B.ext_result[slot] = make_int4(hit.id, __float_as_int(hit.t), hit.front ? 1 : 0, 0);
+            }
+            has_query = false;
+        }
+        // New queries for the idle lanes: one atomic per warp
+        const unsigned active = __activemask();
+        const unsigned want = __ballot_sync(active, idle);
+        if (want != 0u)
+        {
+            const int leader = __ffs(static_cast<int>(want)) - 1;
+            unsigned base = 0;
+            if (static_cast<int>(lane) == leader)
+            {
+                base = atomicAdd(B.control + 1, static_cast<unsigned>(__popc(want)));
+            }
+            base = __shfl_sync(active, base, leader);
+            drained = base + static_cast<unsigned>(__popc(want)) >= count;
+            if (idle)
+            {
+                const unsigned q = base + static_cast<unsigned>(__popc(want & lanes_below));
+                if (q >= count)
+                {
+                    break; // the queue is empty: this lane is done
+                }
+                const float4 qo = B.query_o[q];
+                const float4 qd = B.query_d[q];
+                const int4 qm = B.query_meta[q];
+                o = make_float3(qo.x, qo.y, qo.z);
+                time = qo.w;
+                d = make_float3(qd.x, qd.y, qd.z);
+                hit.id = -1;
+                hit.t = qd.w;
+                hit.front = false;
+                from = qm.x;
+                inward = (qm.y & 1) != 0;
+                shadow = (qm.y & 2) != 0;
+                skip = qm.z;
+                slot = qm.w;
+                inverse_a = 1.0f / length_squared(d);
+                inv = make_float3(safe_inverse(d.x), safe_inverse(d.y), safe_inverse(d.z));
+                os = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
+                sp = 0;
+                leaf = 0;
+                link = S.node_count == 0 ? traversal_done : 0;
+                has_query = true;
+            }
+        }
+        // The walk, until this lane's query is answered or too few lanes are still walking
+        while (true)
+        {
+            while (link >= 0)
+            {
+                const float4* np = reinterpret_cast<const float4*>(S.nodes + link);
+                const float4 nx = __ldg(np);
+                const float4 ny = __ldg(np + 1);
+                const float4 nz = __ldg(np + 2);
+                const int2 nl = __ldg(reinterpret_cast<const int2*>(np + 3));
+                const float a0 = fmaf(nx.x, inv.x, -os.x), a1 = fmaf(nx.y, inv.x, -os.x);
+                const float b0 = fmaf(ny.x, inv.y, -os.y), b1 = fmaf(ny.y, inv.y, -os.y);
+                const float c0 = fmaf(nz.x, inv.z, -os.z), c1 = fmaf(nz.y, inv.z, -os.z);
+                const float enter0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), t_min));
+                const float exit0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
+                const float a2 = fmaf(nx.z, inv.x, -os.x), a3 = fmaf(nx.w, inv.x, -os.x);
+                const float b2 = fmaf(ny.z, inv.y, -os.y), b3 = fmaf(ny.w, inv.y, -os.y);
+                const float c2 = fmaf(nz.z, inv.z, -os.z), c3 = fmaf(nz.w, inv.z, -os.z);
+                const float enter1 = fmaxf(fmaxf(fminf(a2, a3), fminf(b2, b3)), fmaxf(fminf(c2, c3), t_min));
+                const float exit1 = fminf(fminf(fmaxf(a2, a3), fmaxf(b2, b3)), fminf(fmaxf(c2, c3), hit.t));
+                const bool h0 = enter0 <= exit0;
+                const bool h1 = enter1 <= exit1;
+                if (h0 && h1)
+                {
+                    const bool second_first = enter1 < enter0;
+                    link = second_first ? nl.y : nl.x;
+                    stack[sp++] =
+                        make_int2(second_first ? nl.x : nl.y, __float_as_int(second_first ? enter0 : enter1));
+                }
+                else if (h0 || h1)
+                {
+                    link = h0 ? nl.x : nl.y;
+                }
+                else
+                {
+                    link = pop();
+                }
+                if (link < 0 && link != traversal_done && leaf == 0)
+                {
+                    leaf = link;
+                    link = pop();
+                }
+                if (!__any_sync(__activemask(), leaf == 0))
+                {
+                    break;
+                }
+            }
+            while (leaf < 0)
+            {
+                if (test_leaf<false, false, FEATURES>(S, leaf, o, d, time, inverse_a, from, inward, skip, hit, nullptr,
+                                                      shadow))
+                {
+                    hit.id = 1; // a shadow ray's blocker: answered
+                    leaf = 0;
+                    link = traversal_done;
+                    break;
+                }
+                leaf = 0;
+                if (link < 0 && link != traversal_done)
+                {
+                    leaf = link;
+                    link = pop();
+                }
+            }
+            if (link == traversal_done && leaf == 0)
+            {
+                break;
+            }
+            if (!drained && __popc(__activemask()) < RTB_REFILL_LANES)
+            {
+                break;
+            }
+        }
+    }
+}
+
+// The wavefront's samples into the image's sums: each chunk's samples added in pass order into its partial, the
+// partials in chunk order into the sums, as the persistent kernel's lanes and reduce_kernel add them
+__global__ void wave_reduce_kernel(const reduce_params R, const float4* samples, int64_t pass_begin, int64_t pass_end,
+                                   int32_t chunk)
+{
+    const int x = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = static_cast<int>(blockIdx.y);
+    if (x >= R.width || y >= R.height)
+    {
+        return;
+    }
+    const int q = ((y >> 2) * R.tiles_x + (x >> 3)) * 32 + ((y & 3) << 3) + (x & 7);
+    double* sum = R.sums + 3 * (static_cast<int64_t>(y) * R.width + x);
+    double r = sum[0], g = sum[1], b = sum[2];
+    int64_t pass = pass_begin;
+    while (pass < pass_end)
+    {
+        const int64_t chunk_end = (pass / chunk + 1) * chunk;
+        const int64_t end = chunk_end < pass_end ? chunk_end : pass_end;
+        double pr = 0.0, pg = 0.0, pb = 0.0;
+        for (; pass < end; ++pass)
+        {
+            const float4 s = samples[(pass - pass_begin) * R.padded_pixels + q];
+            pr += without_nan(s.x);
+            pg += without_nan(s.y);
+            pb += without_nan(s.z);
+        }
+        r += pr;
+        g += pg;
+        b += pb;
+    }
+    sum[0] = r;
+    sum[1] = g;
+    sum[2] = b;
+}
 } // namespace
 
 namespace
@@ -2325,6 +2878,64 @@ cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const
     const auto grid = static_cast<unsigned>((count + block - 1) / block);
     closest_hits_kernel<<<grid, block, 0, stream>>>(s, origins, directions, count, prim_source, ids, ts);
     return cudaGetLastError();
+}
+
+size_t wave_slot_bytes() { return (wave_rows + wave_shadow_rows) * sizeof(float4); }
+
+namespace
+{
+using wave_shade_function = void (*)(launch_params, wave_buffers);
+using wave_trace_function = void (*)(scene_view, wave_buffers);
+
+wave_shade_function wave_shade_of(bool quality, bool features)
+{
+    if (quality)
+    {
+        return features ? wave_shade_kernel<true, true> : wave_shade_kernel<true, false>;
+    }
+    return features ? wave_shade_kernel<false, true> : wave_shade_kernel<false, false>;
+}
+
+wave_trace_function wave_trace_of(bool features) { return features ? wave_trace_kernel<true> : wave_trace_kernel<false>; }
+} // namespace
+
+cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
+                             cudaStream_t stream)
+{
+    cudaError_t e = cudaMemsetAsync(b.control, 0, 2 * sizeof(unsigned), stream);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    const bool features = has_features(p.scene);
+    wave_shade_of(quality, features)<<<b.slot_count / render_block, render_block, 0, stream>>>(p, b);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    wave_trace_of(features)<<<trace_grid, render_block, 0, stream>>>(p.scene, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
+                               int32_t chunk, cudaStream_t stream)
+{
+    const dim3 block(128, 1);
+    const dim3 grid(static_cast<unsigned>((r.width + 127) / 128), static_cast<unsigned>(r.height));
+    wave_reduce_kernel<<<grid, block, 0, stream>>>(r, b.samples, pass_begin, pass_end, chunk);
+    return cudaGetLastError();
+}
+
+cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace)
+{
+    const bool features = has_features(scene);
+    const cudaError_t e = attributes_of(wave_shade_of(quality, features), shade);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    return attributes_of(wave_trace_of(features), trace);
 }
 
 cudaError_t launch_camera_rays(const camera_params& cam, uint64_t seed, int64_t pass, int32_t round_passes,

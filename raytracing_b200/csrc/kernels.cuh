@@ -119,6 +119,35 @@ cudaError_t batch_attributes(int group, kernel_attributes& out);
 // The attributes of the render kernel that launch_render picks for the scene and integrator
 cudaError_t render_attributes(const scene_view& scene, bool quality, kernel_attributes& out);
 
+// The wavefront form of a launch, for scenes searched through the tree: `slot_count` resident paths, each the state a
+// lane of the persistent kernel keeps in registers (its sample, path and pending shadow ray), advanced by steps of two
+// kernels. The shade kernel (one thread per slot) takes the last step's hits, shades, stores finished samples, claims
+// new ones and queues each slot's next ray and shadow ray; the trace kernel (persistent) walks the queued rays, each
+// lane taking the next query as soon as its own is answered. A step that queues nothing ends the launch, and the
+// reduction adds the samples into the sums chunk by chunk, in pass order.
+struct wave_buffers
+{
+    void* slots;            // slot_count slots of wave_slot_bytes() each, zeroed before a launch
+    int32_t slot_count;     // a multiple of render_block
+    float4* samples;        // sample_count: (pass - pass_begin) * padded_pixels + tile slot -> the sample's value
+    int64_t sample_count;   // (pass_end - pass_begin) * padded_pixels
+    float4* query_o;        // 2 * slot_count queries: origin, time
+    float4* query_d;        // direction, t_max
+    int4* query_meta;       // from, flags (1 inward, 2 shadow), skip, slot
+    int4* ext_result;       // per slot: the next ray's hit (id, t's bits, front)
+    int32_t* shadow_result; // per slot: 1 if the shadow ray was blocked
+    unsigned* control;      // [0] queries the last shade step queued, [1] queries the trace kernel took
+};
+size_t wave_slot_bytes();
+// One step: clears the queue, the shade kernel over the slots, the trace kernel (trace_grid blocks) over the queue
+cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
+                             cudaStream_t stream);
+// The samples of passes [pass_begin, pass_end) into the sums (chunk partials in pass order, added in chunk order)
+cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
+                               int32_t chunk, cudaStream_t stream);
+// The shade kernel's and the trace kernel's attributes for the scene and integrator
+cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace);
+
 // Parity hooks: closest hits of given rays (source ids through prim_source), and the camera rays of one pass
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,
                                 const int32_t* prim_source, int32_t* ids, float* ts, cudaStream_t stream);

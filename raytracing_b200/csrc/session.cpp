@@ -19,6 +19,18 @@ namespace
 {
 constexpr double max_launch_seconds = 0.5;              // renderer.h:413
 constexpr size_t partial_budget_bytes = size_t{1} << 30; // a launch's chunk partials: at most 1 GiB
+// The wavefront's slots (paths in flight: 2^20 take 160 MB, and their queries 96 MB; the trace kernel's throughput
+// grew with them up to here on the mesh, where a step's walks must outlast its slowest one), and its steps per group
+// between two looks at the queue's length
+#ifndef RTB_WAVE_SLOTS
+#define RTB_WAVE_SLOTS (1 << 20)
+#endif
+#ifndef RTB_WAVE_GROUP
+#define RTB_WAVE_GROUP 8
+#endif
+constexpr int wave_slots = RTB_WAVE_SLOTS / render_block * render_block;
+constexpr size_t wave_sample_budget_bytes = size_t{2} << 30; // a wavefront launch's samples (16 bytes each): 2 GiB
+constexpr int wave_group = RTB_WAVE_GROUP;
 } // namespace
 
 session::session(std::shared_ptr<resident_scene> scene, const rt_session_options& options)
@@ -36,15 +48,46 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
     check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a CUDA stream");
     check(cudaEventCreate(&start_), "creating a CUDA event");
     check(cudaEventCreate(&stop_), "creating a CUDA event");
+    if (options_.form < RT_FORM_AUTO || options_.form > RT_FORM_WAVEFRONT)
+    {
+        fail(RT_ERR_INVALID, "form must be RT_FORM_AUTO, RT_FORM_PERSISTENT or RT_FORM_WAVEFRONT");
+    }
     kernel_attributes a{};
     check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
     grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
+    const scene_view& view = scene_->view();
+    wavefront_ = options_.form == RT_FORM_WAVEFRONT ||
+                 (options_.form == RT_FORM_AUTO && view.flat == 0 && view.node_count > 0);
+    if (wavefront_)
+    {
+        kernel_attributes shade{}, trace{};
+        check(wave_attributes(view, scene_->quality(), shade, trace), "querying the wavefront kernels");
+        trace_grid_ = trace.multiprocessors * std::max(1, trace.blocks_per_sm);
+        wave_max_slots_ = wave_slots;
+        check(cudaHostAlloc(reinterpret_cast<void**>(&wave_queued_), 2 * sizeof(unsigned), cudaHostAllocDefault),
+              "allocating pinned memory");
+        for (auto& e : wave_done_)
+        {
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating a CUDA event");
+        }
+    }
     counters_.allocate(7);
     set_camera(scene_->camera());
 }
 
 session::~session()
 {
+    for (auto& e : wave_done_)
+    {
+        if (e)
+        {
+            cudaEventDestroy(e);
+        }
+    }
+    if (wave_queued_)
+    {
+        cudaFreeHost(wave_queued_);
+    }
     partials_.release();
     sums_.release();
     counters_.release();
@@ -108,8 +151,12 @@ int64_t session::plan(int64_t target, double budget_seconds) const
         end = passes_ + static_cast<int64_t>(std::min(passes, 1e12));
         end = std::max(next_chunk, end / pass_chunk * pass_chunk);
     }
-    // At most what the partials buffer holds
-    const int64_t max_chunks = std::max<int64_t>(1, max_partial_entries_ / padded_pixels_);
+    // At most what the partials buffer holds (the wavefront: its samples buffer)
+    const int64_t max_chunks =
+        wavefront_ && !counting_
+            ? std::max<int64_t>(1, static_cast<int64_t>(wave_sample_budget_bytes / sizeof(float4)) /
+                                       (static_cast<int64_t>(padded_pixels_) * pass_chunk))
+            : std::max<int64_t>(1, max_partial_entries_ / padded_pixels_);
     end = std::min(end, (passes_ / pass_chunk + max_chunks) * pass_chunk);
     return std::min(end, target);
 }
@@ -118,8 +165,9 @@ double session::launch(int64_t end)
 {
     const int64_t first_chunk = passes_ / pass_chunk;
     const int64_t chunks = (end + pass_chunk - 1) / pass_chunk - first_chunk;
+    const bool wave = wavefront_ && !counting_;
     const size_t needed = static_cast<size_t>(chunks) * static_cast<size_t>(padded_pixels_) * 3;
-    if (partials_.size() < needed)
+    if (!wave && partials_.size() < needed)
     {
         partials_.allocate(needed);
     }
@@ -151,9 +199,22 @@ double session::launch(int64_t end)
     r.chunks = p.chunks;
 
     check(cudaMemsetAsync(counters_.data(), 0, sizeof(unsigned long long), stream_), "resetting the work counter");
+    wave_buffers b{};
+    if (wave)
+    {
+        b = wave_setup(static_cast<int64_t>(padded_pixels_) * (end - passes_)); // allocated before the timing starts
+    }
     check(cudaEventRecord(start_, stream_), "recording a CUDA event");
-    check(launch_render(p, scene_->quality(), counting_, grid_, stream_), "launching the render kernel");
-    check(launch_reduce(r, stream_), "launching the reduction");
+    if (wave)
+    {
+        run_wavefront(p, b);
+        check(launch_wave_reduce(r, b, p.pass_begin, p.pass_end, p.chunk, stream_), "launching the reduction");
+    }
+    else
+    {
+        check(launch_render(p, scene_->quality(), counting_, grid_, stream_), "launching the render kernel");
+        check(launch_reduce(r, stream_), "launching the reduction");
+    }
     check(cudaEventRecord(stop_, stream_), "recording a CUDA event");
     check(cudaEventSynchronize(stop_), "rendering on the GPU");
     float ms = 0;
@@ -164,6 +225,76 @@ double session::launch(int64_t end)
     passes_ = end;
     kernel_seconds_ += seconds;
     return seconds;
+}
+
+wave_buffers session::wave_setup(int64_t samples)
+{
+    if (wave_slots_.size() == 0)
+    {
+        const auto n = static_cast<size_t>(wave_max_slots_);
+        wave_slots_.allocate(n * wave_slot_bytes());
+        query_o_.allocate(2 * n);
+        query_d_.allocate(2 * n);
+        query_meta_.allocate(2 * n);
+        ext_result_.allocate(n);
+        shadow_result_.allocate(n);
+        wave_control_.allocate(2);
+    }
+    if (wave_samples_.size() < static_cast<size_t>(samples))
+    {
+        wave_samples_.allocate(static_cast<size_t>(samples));
+    }
+    const int64_t wanted = (samples + render_block - 1) / render_block * render_block;
+    wave_buffers b{};
+    b.slots = wave_slots_.data();
+    b.slot_count = static_cast<int32_t>(std::min<int64_t>(wave_max_slots_, wanted));
+    b.samples = wave_samples_.data();
+    b.sample_count = samples;
+    b.query_o = query_o_.data();
+    b.query_d = query_d_.data();
+    b.query_meta = query_meta_.data();
+    b.ext_result = ext_result_.data();
+    b.shadow_result = shadow_result_.data();
+    b.control = wave_control_.data();
+    return b;
+}
+
+void session::run_wavefront(const launch_params& p, const wave_buffers& b)
+{
+    const int64_t samples = b.sample_count;
+    check(cudaMemsetAsync(b.slots, 0, static_cast<size_t>(b.slot_count) * wave_slot_bytes(), stream_),
+          "clearing the path slots");
+    // A sample takes at most max_depth + 1 steps (its segments, then the one that adds its last shadow ray) and a slot
+    // renders at most its share of the samples one after another: twice that bounds a launch that works
+    const int64_t samples_per_slot = (samples + b.slot_count - 1) / b.slot_count;
+    const int64_t step_limit = 2 * (samples_per_slot * (camera_.max_depth + 2) + 4 * wave_group);
+    // Groups of steps, two in flight: the host reads one group's queue length while the next group runs; a group
+    // after the end finds every slot out of work and costs a few microseconds a step
+    int64_t steps = 0;
+    for (int group = 0;; ++group)
+    {
+        for (int s = 0; s < wave_group; ++s)
+        {
+            check(launch_wave_step(p, scene_->quality(), b, trace_grid_, stream_), "launching a wavefront step");
+        }
+        steps += wave_group;
+        const int k = group & 1;
+        check(cudaMemcpyAsync(wave_queued_ + k, b.control, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_),
+              "reading the queue's length");
+        check(cudaEventRecord(wave_done_[k], stream_), "recording a CUDA event");
+        if (group > 0)
+        {
+            check(cudaEventSynchronize(wave_done_[k ^ 1]), "rendering on the GPU");
+            if (wave_queued_[k ^ 1] == 0)
+            {
+                break;
+            }
+        }
+        if (steps > step_limit)
+        {
+            fail(RT_ERR_RUNTIME, "the wavefront's paths did not finish within their steps");
+        }
+    }
 }
 
 rt_render_report session::render_to(int64_t target)
@@ -272,9 +403,18 @@ uint64_t session::shadow_rays() const
 rt_kernel_info session::kernel() const
 {
     kernel_attributes a{};
-    check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
+    if (wavefront_ && !counting_)
+    {
+        kernel_attributes shade{};
+        check(wave_attributes(scene_->view(), scene_->quality(), shade, a), "querying the wavefront kernels");
+    }
+    else
+    {
+        check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
+    }
     rt_kernel_info info{};
-    std::snprintf(info.name, sizeof(info.name), "%s", scene_->quality() ? "persistent nee-mis" : "persistent books");
+    const char* form = wavefront_ && !counting_ ? "wavefront" : "persistent";
+    std::snprintf(info.name, sizeof(info.name), "%s %s", form, scene_->quality() ? "nee-mis" : "books");
     info.registers = a.registers;
     info.local_bytes = a.local_bytes;
     info.blocks_per_multiprocessor = a.blocks_per_sm;
