@@ -2235,6 +2235,30 @@ constexpr uint32_t wave_shadow_inward = 1u << 10;
 
 constexpr unsigned full_warp = 0xffffffffu;
 
+// The slots, queries, answers and samples pass through L2 once per step: loaded and stored evict-first (.cs), so that
+// they do not push the tree and the primitives, which every walk reads, out of L2
+#ifndef RTB_WAVE_STREAMING
+#define RTB_WAVE_STREAMING 1
+#endif
+template <class T>
+__device__ __forceinline__ T stream_load(const T* p)
+{
+#if RTB_WAVE_STREAMING
+    return __ldcs(p);
+#else
+    return *p;
+#endif
+}
+template <class T>
+__device__ __forceinline__ void stream_store(T* p, T v)
+{
+#if RTB_WAVE_STREAMING
+    __stcs(p, v);
+#else
+    *p = v;
+#endif
+}
+
 // The shade kernel's resident blocks per multiprocessor: 0 takes the persistent kernel's for the integrator
 #ifndef RTB_WAVE_SHADE_MIN_BLOCKS
 #define RTB_WAVE_SHADE_MIN_BLOCKS 0
@@ -2250,24 +2274,15 @@ template <bool QUALITY, bool FEATURES>
 __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, FEATURES>())
     wave_shade_kernel(const __grid_constant__ launch_params P, const __grid_constant__ wave_buffers B)
 {
-    __shared__ unsigned long long block_rays;
-    __shared__ unsigned long long block_shadow_rays;
-    if (threadIdx.x == 0)
-    {
-        block_rays = 0;
-        block_shadow_rays = 0;
-    }
-    __syncthreads();
     const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     const int n = B.slot_count;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
     float4* rows = static_cast<float4*>(B.slots);
     float4* shadow_rows = rows + static_cast<int64_t>(wave_rows) * n;
-    const int4 r5 = reinterpret_cast<const int4*>(rows)[5 * n + i];
+    const int4 r5 = stream_load(reinterpret_cast<const int4*>(rows) + 5 * n + i);
     uint32_t flags = static_cast<uint32_t>(r5.y);
-    uint32_t rays = 0;
-    uint32_t shadow_rays = 0;
+    uint32_t shadow_rays = 0; // counted by the trace kernel, which walks them
     // a warp whose slots have all run out of work has nothing left to do in this launch
     if (!__all_sync(full_warp, (flags & wave_exhausted) != 0u))
     {
@@ -2283,12 +2298,12 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
         rng.job = P.job;
         if (live)
         {
-            const float4 r0 = rows[i];
-            const float4 r1 = rows[n + i];
-            const float4 r2 = rows[2 * n + i];
-            const float4 r3 = rows[3 * n + i];
-            const int4 r4 = reinterpret_cast<const int4*>(rows)[4 * n + i];
-            const longlong2 r6 = reinterpret_cast<const longlong2*>(rows)[6 * n + i];
+            const float4 r0 = stream_load(rows + i);
+            const float4 r1 = stream_load(rows + n + i);
+            const float4 r2 = stream_load(rows + 2 * n + i);
+            const float4 r3 = stream_load(rows + 3 * n + i);
+            const int4 r4 = stream_load(reinterpret_cast<const int4*>(rows) + 4 * n + i);
+            const longlong2 r6 = stream_load(reinterpret_cast<const longlong2*>(rows) + 6 * n + i);
             ps.o = make_float3(r0.x, r0.y, r0.z);
             ps.time = r0.w;
             ps.d = make_float3(r1.x, r1.y, r1.z);
@@ -2309,11 +2324,11 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
             float3 sample = make_float3(0.0f, 0.0f, 0.0f);
             if (flags & wave_shadow)
             {
-                if (B.shadow_result[i] == 0)
+                if (stream_load(B.shadow_result + i) == 0)
                 {
-                    const float4 q0 = shadow_rows[i];
-                    const float4 q1 = shadow_rows[n + i];
-                    const int4 q2 = reinterpret_cast<const int4*>(shadow_rows)[2 * n + i];
+                    const float4 q0 = stream_load(shadow_rows + i);
+                    const float4 q1 = stream_load(shadow_rows + n + i);
+                    const int4 q2 = stream_load(reinterpret_cast<const int4*>(shadow_rows) + 2 * n + i);
                     const float3 contribution = make_float3(q1.w, __int_as_float(q2.x), __int_as_float(q2.y));
                     // through smoke, the light arrives with the chance of crossing it (its expected value)
                     const float through =
@@ -2333,12 +2348,11 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
             }
             else if (flags & wave_ext)
             {
-                const int4 r = B.ext_result[i];
+                const int4 r = stream_load(B.ext_result + i);
                 hit_info h;
                 h.id = r.x;
                 h.t = __int_as_float(r.y);
                 h.front = r.z != 0;
-                ++rays;
                 ++ps.depth;
                 if (FEATURES && P.scene.medium_count > 0)
                 {
@@ -2379,7 +2393,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
             if (finished)
             {
                 // the sample's value, added into its chunk's partial in pass order by the reduction
-                B.samples[sample_index] = make_float4(sample.x, sample.y, sample.z, 0.0f);
+                stream_store(B.samples + sample_index, make_float4(sample.x, sample.y, sample.z, 0.0f));
                 need = true;
             }
         }
@@ -2465,22 +2479,22 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
             if (ext)
             {
                 const unsigned q = base + static_cast<unsigned>(__popc(ext_lanes & lanes_below));
-                B.query_o[q] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time);
-                B.query_d[q] = make_float4(ps.d.x, ps.d.y, ps.d.z, infinity_f);
-                B.query_meta[q] = make_int4(ps.from, ps.inward ? 1 : 0, -1, i);
+                stream_store(B.query_o + q, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time));
+                stream_store(B.query_d + q, make_float4(ps.d.x, ps.d.y, ps.d.z, infinity_f));
+                stream_store(B.query_meta + q, make_int4(ps.from, ps.inward ? 1 : 0, -1, i));
             }
             if (shadow)
             {
                 const unsigned q = base + static_cast<unsigned>(__popc(ext_lanes)) +
                                    static_cast<unsigned>(__popc(shadow_lanes & lanes_below));
-                B.query_o[q] = make_float4(sq.o.x, sq.o.y, sq.o.z, ps.time);
-                B.query_d[q] = make_float4(sq.d.x, sq.d.y, sq.d.z, sq.t_max);
-                B.query_meta[q] = make_int4(sq.from, (sq.inward ? 1 : 0) | 2, sq.skip, i);
+                stream_store(B.query_o + q, make_float4(sq.o.x, sq.o.y, sq.o.z, ps.time));
+                stream_store(B.query_d + q, make_float4(sq.d.x, sq.d.y, sq.d.z, sq.t_max));
+                stream_store(B.query_meta + q, make_int4(sq.from, (sq.inward ? 1 : 0) | 2, sq.skip, i));
                 // what the next step needs of it: the light it brings and, through smoke, its segment
-                shadow_rows[i] = make_float4(sq.o.x, sq.o.y, sq.o.z, sq.t_max);
-                shadow_rows[n + i] = make_float4(sq.d.x, sq.d.y, sq.d.z, sq.contribution.x);
-                reinterpret_cast<int4*>(shadow_rows)[2 * n + i] =
-                    make_int4(__float_as_int(sq.contribution.y), __float_as_int(sq.contribution.z), 0, 0);
+                stream_store(shadow_rows + i, make_float4(sq.o.x, sq.o.y, sq.o.z, sq.t_max));
+                stream_store(shadow_rows + n + i, make_float4(sq.d.x, sq.d.y, sq.d.z, sq.contribution.x));
+                stream_store(reinterpret_cast<int4*>(shadow_rows) + 2 * n + i,
+                             make_int4(__float_as_int(sq.contribution.y), __float_as_int(sq.contribution.z), 0, 0));
             }
         }
         if (live)
@@ -2489,40 +2503,22 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                     (ps.inward ? wave_inward : 0u);
             if (flags & wave_exhausted)
             {
-                reinterpret_cast<int4*>(rows)[5 * n + i] = make_int4(0, static_cast<int>(flags), px, py);
+                stream_store(reinterpret_cast<int4*>(rows) + 5 * n + i, make_int4(0, static_cast<int>(flags), px, py));
             }
             else
             {
-                rows[i] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time);
-                rows[n + i] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf);
-                rows[2 * n + i] = make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x);
-                rows[3 * n + i] =
-                    make_float4(ps.radiance.y, ps.radiance.z, __uint_as_float(rng.key.x), __uint_as_float(rng.key.y));
-                reinterpret_cast<int4*>(rows)[4 * n + i] = make_int4(static_cast<int>(rng.pixel),
-                                                                     static_cast<int>(rng.pass), ps.from, ps.rays_left);
-                reinterpret_cast<int4*>(rows)[5 * n + i] = make_int4(ps.depth, static_cast<int>(flags), px, py);
-                reinterpret_cast<longlong2*>(rows)[6 * n + i] = make_longlong2(sample_index, pass);
+                stream_store(rows + i, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time));
+                stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf));
+                stream_store(rows + 2 * n + i,
+                             make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x));
+                stream_store(rows + 3 * n + i, make_float4(ps.radiance.y, ps.radiance.z, __uint_as_float(rng.key.x),
+                                                           __uint_as_float(rng.key.y)));
+                stream_store(reinterpret_cast<int4*>(rows) + 4 * n + i,
+                             make_int4(static_cast<int>(rng.pixel), static_cast<int>(rng.pass), ps.from, ps.rays_left));
+                stream_store(reinterpret_cast<int4*>(rows) + 5 * n + i,
+                             make_int4(ps.depth, static_cast<int>(flags), px, py));
+                stream_store(reinterpret_cast<longlong2*>(rows) + 6 * n + i, make_longlong2(sample_index, pass));
             }
-        }
-    }
-    if (rays)
-    {
-        atomicAdd(&block_rays, static_cast<unsigned long long>(rays));
-    }
-    if (QUALITY && shadow_rays)
-    {
-        atomicAdd(&block_shadow_rays, static_cast<unsigned long long>(shadow_rays));
-    }
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        if (block_rays)
-        {
-            atomicAdd(P.counters, block_rays);
-        }
-        if (QUALITY && block_shadow_rays)
-        {
-            atomicAdd(P.counters + 1, block_shadow_rays);
         }
     }
 }
@@ -2540,9 +2536,17 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
 // persistent kernel's traverse, the same node order, leaf tests and self-intersection rules)
 template <bool FEATURES>
 __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
-    wave_trace_kernel(const __grid_constant__ scene_view S, const __grid_constant__ wave_buffers B)
+    wave_trace_kernel(const __grid_constant__ scene_view S, const __grid_constant__ wave_buffers B,
+                      unsigned long long* counters)
 {
+    __shared__ unsigned block_walks[2]; // the block's closest-hit and shadow queries: the path segments and shadow rays
+    if (threadIdx.x < 2)
+    {
+        block_walks[threadIdx.x] = 0;
+    }
+    __syncthreads();
     const unsigned count = B.control[0];
+    unsigned walks[2] = {0, 0};
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
     int2 stack[max_bvh_depth];
@@ -2569,44 +2573,41 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
         }
         return traversal_done;
     };
+    // Warp-synchronous: every lane runs every loop, with nothing to do once its query is answered and the queue is
+    // empty, so that each ballot sees the whole warp and the refill rule holds as written
     while (true)
     {
-        const bool idle = link == traversal_done && leaf == 0;
-        if (idle && has_query)
+        const bool answered = has_query && link == traversal_done && leaf == 0;
+        if (answered)
         {
             if (shadow)
             {
-                B.shadow_result[slot] = hit.id >= 0 ? 1 : 0;
+                stream_store(B.shadow_result + slot, hit.id >= 0 ? 1 : 0);
             }
             else
             {
-                B.ext_result[slot] = make_int4(hit.id, __float_as_int(hit.t), hit.front ? 1 : 0, 0);
+                stream_store(B.ext_result + slot, make_int4(hit.id, __float_as_int(hit.t), hit.front ? 1 : 0, 0));
             }
             has_query = false;
         }
         // New queries for the idle lanes: one atomic per warp
-        const unsigned active = __activemask();
-        const unsigned want = __ballot_sync(active, idle);
-        if (want != 0u)
+        const unsigned idle = __ballot_sync(full_warp, !has_query);
+        if (idle != 0u && !drained)
         {
-            const int leader = __ffs(static_cast<int>(want)) - 1;
+            const int leader = __ffs(static_cast<int>(idle)) - 1;
             unsigned base = 0;
             if (static_cast<int>(lane) == leader)
             {
-                base = atomicAdd(B.control + 1, static_cast<unsigned>(__popc(want)));
+                base = atomicAdd(B.control + 1, static_cast<unsigned>(__popc(idle)));
             }
-            base = __shfl_sync(active, base, leader);
-            drained = base + static_cast<unsigned>(__popc(want)) >= count;
-            if (idle)
+            base = __shfl_sync(full_warp, base, leader);
+            drained = base + static_cast<unsigned>(__popc(idle)) >= count;
+            const unsigned q = base + static_cast<unsigned>(__popc(idle & lanes_below));
+            if (!has_query && q < count)
             {
-                const unsigned q = base + static_cast<unsigned>(__popc(want & lanes_below));
-                if (q >= count)
-                {
-                    break; // the queue is empty: this lane is done
-                }
-                const float4 qo = B.query_o[q];
-                const float4 qd = B.query_d[q];
-                const int4 qm = B.query_meta[q];
+                const float4 qo = stream_load(B.query_o + q);
+                const float4 qd = stream_load(B.query_d + q);
+                const int4 qm = stream_load(B.query_meta + q);
                 o = make_float3(qo.x, qo.y, qo.z);
                 time = qo.w;
                 d = make_float3(qd.x, qd.y, qd.z);
@@ -2618,6 +2619,7 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
                 shadow = (qm.y & 2) != 0;
                 skip = qm.z;
                 slot = qm.w;
+                ++walks[shadow ? 1 : 0];
                 inverse_a = 1.0f / length_squared(d);
                 inv = make_float3(safe_inverse(d.x), safe_inverse(d.y), safe_inverse(d.z));
                 os = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
@@ -2627,79 +2629,107 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
                 has_query = true;
             }
         }
-        // The walk, until this lane's query is answered or too few lanes are still walking
+        if (__ballot_sync(full_warp, has_query) == 0u)
+        {
+            break; // the queue is empty and every lane's query answered
+        }
+        // The walks, until fewer than RTB_REFILL_LANES lanes are still walking (or none, once the queue is empty)
         while (true)
         {
-            while (link >= 0)
+            // inner nodes: a lane descends, setting aside the first leaf it meets, until every descending lane holds one
+            while (true)
             {
-                const float4* np = reinterpret_cast<const float4*>(S.nodes + link);
-                const float4 nx = __ldg(np);
-                const float4 ny = __ldg(np + 1);
-                const float4 nz = __ldg(np + 2);
-                const int2 nl = __ldg(reinterpret_cast<const int2*>(np + 3));
-                const float a0 = fmaf(nx.x, inv.x, -os.x), a1 = fmaf(nx.y, inv.x, -os.x);
-                const float b0 = fmaf(ny.x, inv.y, -os.y), b1 = fmaf(ny.y, inv.y, -os.y);
-                const float c0 = fmaf(nz.x, inv.z, -os.z), c1 = fmaf(nz.y, inv.z, -os.z);
-                const float enter0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), t_min));
-                const float exit0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
-                const float a2 = fmaf(nx.z, inv.x, -os.x), a3 = fmaf(nx.w, inv.x, -os.x);
-                const float b2 = fmaf(ny.z, inv.y, -os.y), b3 = fmaf(ny.w, inv.y, -os.y);
-                const float c2 = fmaf(nz.z, inv.z, -os.z), c3 = fmaf(nz.w, inv.z, -os.z);
-                const float enter1 = fmaxf(fmaxf(fminf(a2, a3), fminf(b2, b3)), fmaxf(fminf(c2, c3), t_min));
-                const float exit1 = fminf(fminf(fmaxf(a2, a3), fmaxf(b2, b3)), fminf(fmaxf(c2, c3), hit.t));
-                const bool h0 = enter0 <= exit0;
-                const bool h1 = enter1 <= exit1;
-                if (h0 && h1)
-                {
-                    const bool second_first = enter1 < enter0;
-                    link = second_first ? nl.y : nl.x;
-                    stack[sp++] =
-                        make_int2(second_first ? nl.x : nl.y, __float_as_int(second_first ? enter0 : enter1));
-                }
-                else if (h0 || h1)
-                {
-                    link = h0 ? nl.x : nl.y;
-                }
-                else
-                {
-                    link = pop();
-                }
-                if (link < 0 && link != traversal_done && leaf == 0)
-                {
-                    leaf = link;
-                    link = pop();
-                }
-                if (!__any_sync(__activemask(), leaf == 0))
+                const bool descending = has_query && link >= 0;
+                if (!__any_sync(full_warp, descending))
                 {
                     break;
                 }
-            }
-            while (leaf < 0)
-            {
-                if (test_leaf<false, false, FEATURES>(S, leaf, o, d, time, inverse_a, from, inward, skip, hit, nullptr,
-                                                      shadow))
+                if (descending)
                 {
-                    hit.id = 1; // a shadow ray's blocker: answered
-                    leaf = 0;
-                    link = traversal_done;
+                    const float4* np = reinterpret_cast<const float4*>(S.nodes + link);
+                    const float4 nx = __ldg(np);
+                    const float4 ny = __ldg(np + 1);
+                    const float4 nz = __ldg(np + 2);
+                    const int2 nl = __ldg(reinterpret_cast<const int2*>(np + 3));
+                    const float a0 = fmaf(nx.x, inv.x, -os.x), a1 = fmaf(nx.y, inv.x, -os.x);
+                    const float b0 = fmaf(ny.x, inv.y, -os.y), b1 = fmaf(ny.y, inv.y, -os.y);
+                    const float c0 = fmaf(nz.x, inv.z, -os.z), c1 = fmaf(nz.y, inv.z, -os.z);
+                    const float enter0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), t_min));
+                    const float exit0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
+                    const float a2 = fmaf(nx.z, inv.x, -os.x), a3 = fmaf(nx.w, inv.x, -os.x);
+                    const float b2 = fmaf(ny.z, inv.y, -os.y), b3 = fmaf(ny.w, inv.y, -os.y);
+                    const float c2 = fmaf(nz.z, inv.z, -os.z), c3 = fmaf(nz.w, inv.z, -os.z);
+                    const float enter1 = fmaxf(fmaxf(fminf(a2, a3), fminf(b2, b3)), fmaxf(fminf(c2, c3), t_min));
+                    const float exit1 = fminf(fminf(fmaxf(a2, a3), fmaxf(b2, b3)), fminf(fmaxf(c2, c3), hit.t));
+                    const bool h0 = enter0 <= exit0;
+                    const bool h1 = enter1 <= exit1;
+                    if (h0 && h1)
+                    {
+                        const bool second_first = enter1 < enter0;
+                        link = second_first ? nl.y : nl.x;
+                        stack[sp++] =
+                            make_int2(second_first ? nl.x : nl.y, __float_as_int(second_first ? enter0 : enter1));
+                    }
+                    else if (h0 || h1)
+                    {
+                        link = h0 ? nl.x : nl.y;
+                    }
+                    else
+                    {
+                        link = pop();
+                    }
+                    if (link < 0 && link != traversal_done && leaf == 0)
+                    {
+                        leaf = link;
+                        link = pop();
+                    }
+                }
+                if (!__any_sync(full_warp, has_query && link >= 0 && leaf == 0))
+                {
+                    break; // every lane still descending holds a leaf: test them together
+                }
+            }
+            // leaves
+            while (true)
+            {
+                const bool testing = has_query && leaf < 0;
+                if (!__any_sync(full_warp, testing))
+                {
                     break;
                 }
-                leaf = 0;
-                if (link < 0 && link != traversal_done)
+                if (testing)
                 {
-                    leaf = link;
-                    link = pop();
+                    if (test_leaf<false, false, FEATURES>(S, leaf, o, d, time, inverse_a, from, inward, skip, hit,
+                                                          nullptr, shadow))
+                    {
+                        hit.id = 1; // a shadow ray's blocker: answered
+                        leaf = 0;
+                        link = traversal_done;
+                    }
+                    else
+                    {
+                        leaf = 0;
+                        if (link < 0 && link != traversal_done)
+                        {
+                            leaf = link;
+                            link = pop();
+                        }
+                    }
                 }
             }
-            if (link == traversal_done && leaf == 0)
-            {
-                break;
-            }
-            if (!drained && __popc(__activemask()) < RTB_REFILL_LANES)
+            const unsigned walking = __ballot_sync(full_warp, has_query && !(link == traversal_done && leaf == 0));
+            if (walking == 0u || (!drained && __popc(walking) < RTB_REFILL_LANES))
             {
                 break;
             }
         }
+    }
+    atomicAdd(&block_walks[0], walks[0]);
+    atomicAdd(&block_walks[1], walks[1]);
+    __syncthreads();
+    if (threadIdx.x < 2 && block_walks[threadIdx.x] != 0u)
+    {
+        atomicAdd(counters + threadIdx.x, static_cast<unsigned long long>(block_walks[threadIdx.x]));
     }
 }
 
@@ -2885,7 +2915,7 @@ size_t wave_slot_bytes() { return (wave_rows + wave_shadow_rows) * sizeof(float4
 namespace
 {
 using wave_shade_function = void (*)(launch_params, wave_buffers);
-using wave_trace_function = void (*)(scene_view, wave_buffers);
+using wave_trace_function = void (*)(scene_view, wave_buffers, unsigned long long*);
 
 wave_shade_function wave_shade_of(bool quality, bool features)
 {
@@ -2914,7 +2944,7 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     {
         return e;
     }
-    wave_trace_of(features)<<<trace_grid, render_block, 0, stream>>>(p.scene, b);
+    wave_trace_of(features)<<<trace_grid, render_block, 0, stream>>>(p.scene, b, p.counters);
     return cudaGetLastError();
 }
 
