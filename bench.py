@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
     p.add_argument("--no-reference-gpu", action="store_true",
                    help="skip timing the reference's own CUDA renderer on the same workload")
+    p.add_argument("--no-mesh", action="store_true", help="skip the triangle-mesh (GGX, environment) measurement")
     p.add_argument("--served", action="store_true", help="also measure the served request stream")
     p.add_argument("--served-rate", type=float, default=200.0)
     p.add_argument("--served-window", type=float, default=0.25, help="seconds of arrivals (a bounded sample)")
@@ -181,6 +182,33 @@ def reference_gpu_measurement(scene_desc, passes: int, value: float) -> dict:
             "segments_per_sample": info["rays"] / (w * h * passes),
             "this_library_over_reference": value / segments_per_s,
             "note": "the reference's gpu::render built from its src/gpu sources for sm_100a, same scene tables"}
+
+
+def mesh_measurement(rt, torch) -> dict:
+    """The triangle-mesh workload (an icosphere of 1.31M triangles displaced by Perlin noise, GGX metal on a glossy
+    plane, a 1024x512 environment map with a sun, importance-sampled; 1920x1080, 256 spp, depth 16, NEE with MIS)
+    in both forms of a session: the wavefront (its default on a tree-searched scene) and the persistent kernel.
+    Timed on the GPU by the session's own events; the scene is far larger than L2."""
+    desc = rt.builtin_scene("mesh-ggx")
+    scene = rt.Scene(desc)
+    passes = desc.round_passes  # sqrt_spp^2: 256
+    out = {"workload": f"mesh-ggx {desc.width}x{desc.height}, {passes} spp, depth {desc.camera.max_depth}, "
+                       f"{scene.stats()['triangles']} triangles, NEE/MIS with the environment map",
+           "scene_stats": scene.stats()}
+    for form in ("wavefront", "persistent"):
+        sess = rt.Session(scene, seed=3, form=form, launch_seconds=0.5)
+        sess.render_to(16)  # warm-up: module load, buffers
+        sess.set_camera(desc.camera)
+        torch.cuda.synchronize()
+        rep = sess.render_to(passes)
+        cnt = sess.counters()
+        out[form] = {"segments_per_s": cnt["rays"] / rep["gpu_seconds"],
+                     "queries_per_s": (cnt["rays"] + cnt["shadow_rays"]) / rep["gpu_seconds"],
+                     "gpu_s": rep["gpu_seconds"], "launches": rep["launches"], "segments": cnt["rays"],
+                     "shadow_rays": cnt["shadow_rays"], "kernel": sess.kernel()}
+        sess.close()
+    out["wavefront_over_persistent"] = out["wavefront"]["segments_per_s"] / out["persistent"]["segments_per_s"]
+    return out
 
 
 def log_uniform(rng, lo: float, hi: float) -> float:
@@ -320,11 +348,14 @@ def served_measurement(rt, torch, args) -> dict:
             time.sleep(max(0.0, requests[pending[0]]["arrival"] - (time.perf_counter() - start)))
     wall = time.perf_counter() - start
     ttff, ttt = [], []
+    by_size = {}
     for i, rid in ids.items():
         st = server.poll(rid)
         lag = submitted[i] - requests[i]["arrival"]
         if st["first_frame_seconds"] >= 0:
             ttff.append(lag + st["first_frame_seconds"])
+            cam = requests[i]["camera"]
+            by_size.setdefault(f"{cam.image_width}x{cam.image_height}", []).append(lag + st["first_frame_seconds"])
         if st["done_seconds"] >= 0:
             ttt.append(lag + st["done_seconds"])
     stats = server.stats()
@@ -355,6 +386,9 @@ def served_measurement(rt, torch, args) -> dict:
                         f"4:3:2:1, target spp log-uniform 1-4096, HBM budget 120 GB",
             "requests": len(requests), "completed": len(ttt), "first_frames": len(ttff), "wall_s": wall,
             "ttff_p50_s": pct(ttff, 50), "ttff_p99_s": pct(ttff, 99),
+            "ttff_by_resolution": {k: {"requests": len(v), "p50_s": pct(v, 50), "p99_s": pct(v, 99)}
+                                   for k, v in sorted(by_size.items())},
+            "step_seconds": args.served_step,
             "time_to_target_p50_s": pct(ttt, 50), "time_to_target_p99_s": pct(ttt, 99),
             "served_segments_per_s": stats["rays"] / stats["gpu_seconds"] if stats["gpu_seconds"] else None,
             "served_steps": stats["steps"], "served_launches": stats["launches"],
@@ -556,6 +590,8 @@ def run_b200(args):
 
     if rank == 0 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_measurement(scene_desc, passes, line["value"])
+    if rank == 0 and not args.no_mesh:
+        line["mesh"] = mesh_measurement(rt, torch)
     if not args.no_batched:
         batched = batched_measurement(rt, torch, rank, world)  # every rank: its share of the 64 jobs
         if rank == 0:

@@ -18,6 +18,13 @@ namespace rtb
 namespace
 {
 constexpr size_t default_partial_budget = size_t{1} << 30;
+// A tree-searched scene of at least this many nodes renders in the wavefront form: on the mesh (768k nodes) its walks
+// are long and diverge, and the wavefront renders it 2.5 times as fast; on the cover scenes (50 to 2000 spheres) the
+// persistent kernel is as fast and needs no queues
+#ifndef RTB_WAVE_MIN_NODES
+#define RTB_WAVE_MIN_NODES 16384
+#endif
+constexpr int wave_min_nodes = RTB_WAVE_MIN_NODES;
 } // namespace
 
 // ---- the batch engine ---------------------------------------------------------------------------------------
@@ -31,11 +38,15 @@ batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
     check(cudaEventCreate(&start_), "creating a CUDA event");
     check(cudaEventCreate(&stop_), "creating a CUDA event");
     kernel_attributes a{};
-    for (int g = 0; g < batch_groups; ++g)
+    for (int g = 0; g < persistent_groups; ++g)
     {
         check(batch_attributes(g, a), "querying the batch kernel");
         grids_[g] = a.multiprocessors * std::max(1, a.blocks_per_sm);
     }
+    kernel_attributes shade{}, trace{};
+    check(wave_attributes(scene_view{}, false, shade, trace), "querying the wavefront kernels");
+    trace_grid_ = trace.multiprocessors * std::max(1, trace.blocks_per_sm);
+    wave_ = std::make_unique<wave_runner>(wave_slots, wave_group);
     work_counter_.allocate(batch_groups);
     header_.allocate(1);
     check(cudaMallocHost(reinterpret_cast<void**>(&header_host_), sizeof(batch_header)), "allocating pinned memory");
@@ -174,7 +185,7 @@ void batch_engine::capture()
     cudaMemcpyAsync(table_.data(), table_host_, capacity_ * sizeof(batch_job), cudaMemcpyHostToDevice, stream_);
     cudaMemcpyAsync(header_.data(), header_host_, sizeof(batch_header), cudaMemcpyHostToDevice, stream_);
     cudaMemsetAsync(work_counter_.data(), 0, batch_groups * sizeof(unsigned long long), stream_);
-    const cudaError_t launched = launch_batch(p, grids_, stream_);
+    const cudaError_t launched = launch_batch(p, grids_, 0, persistent_groups, stream_);
     const cudaError_t ended = cudaStreamEndCapture(stream_, &graph_);
     check(launched, "capturing the batch kernels");
     check(ended, "capturing the batch step");
@@ -231,7 +242,8 @@ double batch_engine::step(std::vector<assignment> work)
     // The jobs in their groups' order (each group's items form its own launch)
     const auto group_of = [&](const assignment& a) {
         const scene_view& v = jobs_.at(a.handle)->scene->view();
-        return batch_group(v.flat != 0, has_features(v));
+        return v.flat == 0 && v.node_count >= wave_min_nodes ? wave_batch_group(has_features(v))
+                                                             : batch_group(v.flat != 0, has_features(v));
     };
     std::stable_sort(work.begin(), work.end(),
                      [&](const assignment& a, const assignment& b) { return group_of(a) < group_of(b); });
@@ -285,6 +297,21 @@ double batch_engine::step(std::vector<assignment> work)
     }
     header.total_pixels = pixels;
     header.job_count = static_cast<int32_t>(work.size());
+    // The tree groups' samples, numbered job after job within each group, and the wavefront's buffers for the largest
+    // (allocated before the timing starts)
+    int64_t group_samples[batch_groups] = {};
+    int group_depth[batch_groups] = {};
+    for (int g = persistent_groups; g < batch_groups; ++g)
+    {
+        for (int32_t i = header.group_jobs[g]; i < header.group_jobs[g + 1]; ++i)
+        {
+            batch_job& b = table_host_[i];
+            b.sample_begin = group_samples[g];
+            group_samples[g] += (b.pass_end - b.pass_begin) * int64_t{b.padded_pixels};
+            group_depth[g] = std::max(group_depth[g], b.cam.max_depth);
+        }
+    }
+    wave_->setup(std::max(group_samples[wave_batch_group(false)], group_samples[wave_batch_group(true)]));
     check(cudaEventRecord(start_, stream_), "recording a CUDA event");
     if (use_graph_)
     {
@@ -303,14 +330,35 @@ double batch_engine::step(std::vector<assignment> work)
               "copying the batch header");
         check(cudaMemsetAsync(work_counter_.data(), 0, batch_groups * sizeof(unsigned long long), stream_),
               "clearing the counters");
-        check(launch_batch(batch_params{table_.data(), header_.data(), work_counter_.data()}, grids_, stream_),
+        check(launch_batch(batch_params{table_.data(), header_.data(), work_counter_.data()}, grids_, 0,
+                           persistent_groups, stream_),
               "launching the batch kernels");
     }
+    launches_ += persistent_groups; // each persistent group's launch (an empty group's ends at once)
+    for (int g = persistent_groups; g < batch_groups; ++g)
+    {
+        if (group_samples[g] == 0)
+        {
+            continue;
+        }
+        // the group's samples claimed through its own work counter, zeroed with the others at the step's start
+        const wave_batch w{table_.data(),          header.group_jobs[g],      header.group_jobs[g + 1],
+                           header.group_items[g], header.group_items[g + 1], work_counter_.data() + g};
+        const bool features = g == wave_batch_group(true);
+        const wave_buffers b = wave_->setup(group_samples[g]);
+        const int64_t steps = wave_->run(b, group_depth[g], stream_, [&] {
+            return launch_wave_batch_step(w, features, b, trace_grid_, stream_);
+        });
+        check(launch_wave_batch_partials(w, b, stream_), "launching the wavefront's partials");
+        launches_ += static_cast<int>(2 * steps + 1);
+    }
+    check(launch_batch_reduce(batch_params{table_.data(), header_.data(), work_counter_.data()}, grids_[0], stream_),
+          "launching the batch reduction");
+    launches_ += 1;
     check(cudaEventRecord(stop_, stream_), "recording a CUDA event");
     check(cudaEventSynchronize(stop_), "rendering the batch on the GPU");
     float ms = 0;
     check(cudaEventElapsedTime(&ms, start_, stop_), "timing the GPU");
-    launches_ += batch_groups + 1; // each group's launch (an empty group's ends at once), the reduction
     for (const assignment& a : work)
     {
         jobs_.at(a.handle)->passes = a.pass_end;

@@ -13,9 +13,10 @@
 namespace rtb
 {
 // The jobs of a batch, each a resident scene seen by its own camera, with its own sums, seed and passes. A step
-// renders for each chosen job the passes from where it stands to a given end, all in one persistent launch of
-// render_batch_kernel per search (the flat scenes' jobs, then the others) and one reduction, captured once into a
-// CUDA graph and replayed with new job tables.
+// renders for each chosen job the passes from where it stands to a given end: the jobs of flat-searched scenes in one
+// persistent launch of render_batch_kernel per group (captured once into a CUDA graph with the table's copies and
+// replayed with new tables), the jobs of tree-searched scenes in the wavefront form, all of a group's jobs in one
+// pool of slots, then one reduction of every job's chunk partials into its sums.
 class batch_engine
 {
 public:
@@ -46,7 +47,7 @@ public:
     int launches() const { return launches_; }
     int64_t last_samples() const { return last_samples_; } // pixel passes the last step rendered
     bool graph_used() const { return graph_exec_ != nullptr; }
-    int grid() const { return grids_[batch_groups - 1]; }
+    int grid() const { return grids_[persistent_groups - 1]; }
     // The chunks of [passes, pass_end) for a job of the given camera, and its padded pixel count
     static int64_t chunks_of(int64_t passes, int64_t pass_end);
     static int64_t padded_of(const rt_camera_desc& camera);
@@ -72,7 +73,9 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaEvent_t start_ = nullptr;
     cudaEvent_t stop_ = nullptr;
-    int grids_[batch_groups] = {}; // each group's launch (batch_group: flat or tree, with or without features)
+    int grids_[persistent_groups] = {}; // each persistent group's launch (batch_group)
+    std::unique_ptr<wave_runner> wave_;  // the large trees' groups (wave_batch_group)
+    int trace_grid_ = 0;
     device_array<double> arena_;
     device_array<batch_job> table_;
     device_array<batch_header> header_;

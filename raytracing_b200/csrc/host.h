@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -153,6 +154,48 @@ struct environment_tables
 };
 environment_tables build_environment(const rt_environment_desc& env);
 
+// The wavefront's host side: its buffers, sized to a launch's samples (slots: at most max_slots) and kept for the next,
+// and the loop of steps, in groups of `group` with two groups in flight, until a step queues no ray
+class wave_runner
+{
+public:
+    explicit wave_runner(int max_slots_, int group_) : max_slots(max_slots_), group(group_) {}
+    ~wave_runner();
+    wave_runner(const wave_runner&) = delete;
+    wave_runner& operator=(const wave_runner&) = delete;
+
+    wave_buffers setup(int64_t samples);
+    // step() enqueues one step on `stream`; returns the steps run
+    int64_t run(const wave_buffers& b, int max_depth, cudaStream_t stream, const std::function<cudaError_t()>& step);
+
+    const int max_slots;
+    const int group;
+
+private:
+    device_array<unsigned char> slots_;
+    device_array<float4> query_o_;
+    device_array<float4> query_d_;
+    device_array<int4> query_meta_;
+    device_array<int4> ext_result_;
+    device_array<int32_t> shadow_result_;
+    device_array<unsigned> control_;
+    device_array<float4> samples_;
+    unsigned* queued_ = nullptr; // pinned: the queue's length after each group of steps
+    cudaEvent_t done_[2] = {nullptr, nullptr};
+};
+
+// The wavefront's slots (paths in flight: 2^20 take 160 MB, and their queries 96 MB; the trace kernel's throughput
+// grew with them up to here on the mesh, where a step's walks must outlast its slowest one) and its steps per group
+// between two looks at the queue's length
+#ifndef RTB_WAVE_SLOTS
+#define RTB_WAVE_SLOTS (1 << 20)
+#endif
+#ifndef RTB_WAVE_GROUP
+#define RTB_WAVE_GROUP 8
+#endif
+constexpr int wave_slots = RTB_WAVE_SLOTS / render_block * render_block;
+constexpr int wave_group = RTB_WAVE_GROUP;
+
 // One view of a resident scene whose image gains passes on demand (renderer.h:591-673)
 class session
 {
@@ -197,28 +240,14 @@ private:
     int padded_pixels_ = 0;
     int64_t max_partial_entries_ = 0;
 
-    // The wavefront form (RT_FORM_WAVEFRONT, or AUTO on a tree-searched scene): its slots, queue and results, sized
-    // on the first launch that uses it; two pinned words take the queue's length back to the host
+    // The wavefront form (RT_FORM_WAVEFRONT, or AUTO on a tree-searched scene)
     bool wavefront_ = false;
-    device_array<unsigned char> wave_slots_;
-    device_array<float4> query_o_;
-    device_array<float4> query_d_;
-    device_array<int4> query_meta_;
-    device_array<int4> ext_result_;
-    device_array<int32_t> shadow_result_;
-    device_array<unsigned> wave_control_;
-    device_array<float4> wave_samples_;
-    unsigned* wave_queued_ = nullptr; // pinned: the queue's length after each group of steps, two groups in flight
-    cudaEvent_t wave_done_[2] = {nullptr, nullptr};
-    int wave_max_slots_ = 0;
+    std::unique_ptr<wave_runner> wave_;
     int trace_grid_ = 0;
 
     // Renders passes [passes_, end) in one launch and its reduction; returns its GPU seconds
     double launch(int64_t end);
-    // The wavefront's buffers for a launch of `samples` samples (allocated on first use, grown as needed), and its
-    // steps over them until a step queues no ray
-    wave_buffers wave_setup(int64_t samples);
-    void run_wavefront(const launch_params& p, const wave_buffers& b);
+
     int64_t plan(int64_t target, double budget_seconds) const;
 };
 

@@ -1984,7 +1984,11 @@ __global__ void reduce_kernel(const reduce_params P)
 
 // The job of jobs [first, end) whose range of the batch's item (or pixel) space holds `index`: a binary search over
 // the jobs' starts
-template <bool PIXELS>
+constexpr int job_items = 0;   // find_job by item_begin
+constexpr int job_pixels = 1;  // by pixel_begin
+constexpr int job_samples = 2; // by sample_begin (a wavefront group's sample space)
+
+template <int SPACE>
 __device__ __forceinline__ int find_job(const batch_job* jobs, int first, int end, int64_t index)
 {
     int lo = first;
@@ -1992,7 +1996,9 @@ __device__ __forceinline__ int find_job(const batch_job* jobs, int first, int en
     while (lo < hi)
     {
         const int mid = (lo + hi + 1) >> 1;
-        const int64_t begin = PIXELS ? jobs[mid].pixel_begin : jobs[mid].item_begin;
+        const int64_t begin = SPACE == job_pixels    ? jobs[mid].pixel_begin
+                              : SPACE == job_samples ? jobs[mid].sample_begin
+                                                     : jobs[mid].item_begin;
         if (begin <= index)
         {
             lo = mid;
@@ -2056,7 +2062,7 @@ __global__ void __launch_bounds__(render_block, render_min_blocks<true, FLAT, FE
                 {
                     break;
                 }
-                J = P.jobs + find_job<false>(P.jobs, job_first, job_end, item);
+                J = P.jobs + find_job<job_items>(P.jobs, job_first, job_end, item);
                 const int64_t local = item - J->item_begin;
                 const int64_t k = local / J->padded_pixels;
                 const int q = static_cast<int>(local - k * J->padded_pixels);
@@ -2151,7 +2157,7 @@ __global__ void reduce_batch_kernel(const batch_params P)
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     {
-        const batch_job& J = P.jobs[find_job<true>(P.jobs, 0, job_count, i)];
+        const batch_job& J = P.jobs[find_job<job_pixels>(P.jobs, 0, job_count, i)];
         const int64_t local = i - J.pixel_begin;
         const int y = static_cast<int>(local / J.cam.width);
         const int x = static_cast<int>(local - static_cast<int64_t>(y) * J.cam.width);
@@ -2231,7 +2237,6 @@ constexpr int wave_rows = 7;
 constexpr int wave_shadow_rows = 3;
 constexpr uint32_t wave_specular = 1u << 8;
 constexpr uint32_t wave_inward = 1u << 9;
-constexpr uint32_t wave_shadow_inward = 1u << 10;
 
 constexpr unsigned full_warp = 0xffffffffu;
 
@@ -2269,10 +2274,13 @@ constexpr int wave_shade_min_blocks()
     return RTB_WAVE_SHADE_MIN_BLOCKS > 0 ? RTB_WAVE_SHADE_MIN_BLOCKS : render_min_blocks<QUALITY, false, FEATURES>();
 }
 
-// A slot's step: the last walk's answers, the shading, the sample's end, a new sample, the next rays queued
-template <bool QUALITY, bool FEATURES>
-__global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, FEATURES>())
-    wave_shade_kernel(const __grid_constant__ launch_params P, const __grid_constant__ wave_buffers B)
+// A slot's step: the last walk's answers, the shading, the sample's end, a new sample, the next rays queued.
+// BATCH: the slots render the samples of a group of batch jobs (W), each slot its job's scene, camera and integrator
+// (QUALITY is then the job's own); otherwise the launch's one view (P).
+template <bool QUALITY, bool FEATURES, bool BATCH>
+__global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY || BATCH, FEATURES>())
+    wave_shade_kernel(const __grid_constant__ launch_params P, const __grid_constant__ wave_buffers B,
+                      const __grid_constant__ wave_batch W)
 {
     const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     const int n = B.slot_count;
@@ -2282,20 +2290,52 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
     float4* shadow_rows = rows + static_cast<int64_t>(wave_rows) * n;
     const int4 r5 = stream_load(reinterpret_cast<const int4*>(rows) + 5 * n + i);
     uint32_t flags = static_cast<uint32_t>(r5.y);
-    uint32_t shadow_rays = 0; // counted by the trace kernel, which walks them
+    uint32_t shadow_rays = 0; // counted where the walks are (the trace kernel), or as queued (BATCH)
     // a warp whose slots have all run out of work has nothing left to do in this launch
     if (!__all_sync(full_warp, (flags & wave_exhausted) != 0u))
     {
         const bool live = (flags & wave_exhausted) == 0u;
-        const camera_params& cam = P.cam;
+        // the slot's job: its scene, camera and numbers (a session's launch: the launch's own)
+        int job = BATCH ? r5.w : 0;
+        const batch_job* J = BATCH ? W.jobs + job : nullptr;
+        const auto scene = [&]() -> const scene_view& {
+            if constexpr (BATCH)
+            {
+                return J->scene;
+            }
+            else
+            {
+                return P.scene;
+            }
+        };
+        const auto camera = [&]() -> const camera_params& {
+            if constexpr (BATCH)
+            {
+                return J->cam;
+            }
+            else
+            {
+                return P.cam;
+            }
+        };
+        const auto quality = [&]() -> bool {
+            if constexpr (BATCH)
+            {
+                return J->quality != 0;
+            }
+            else
+            {
+                return QUALITY;
+            }
+        };
         path_state ps;
         sampler rng;
         shadow_query sq;
         int64_t sample_index = 0, pass = 0;
-        int px = r5.z, py = r5.w;
+        int px = r5.z & 0xffff, py = r5.z >> 16;
         bool need = false;
         bool start = false;
-        rng.job = P.job;
+        rng.job = BATCH ? J->job : P.job;
         if (live)
         {
             const float4 r0 = stream_load(rows + i);
@@ -2332,8 +2372,8 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                     const float3 contribution = make_float3(q1.w, __int_as_float(q2.x), __int_as_float(q2.y));
                     // through smoke, the light arrives with the chance of crossing it (its expected value)
                     const float through =
-                        FEATURES && P.scene.medium_count > 0
-                            ? transmittance(P.scene, make_float3(q0.x, q0.y, q0.z), make_float3(q1.x, q1.y, q1.z),
+                        FEATURES && scene().medium_count > 0
+                            ? transmittance(scene(), make_float3(q0.x, q0.y, q0.z), make_float3(q1.x, q1.y, q1.z),
                                             ps.time, q0.w)
                             : 1.0f;
                     ps.radiance = ps.radiance + through * contribution;
@@ -2354,15 +2394,15 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                 h.t = __int_as_float(r.y);
                 h.front = r.z != 0;
                 ++ps.depth;
-                if (FEATURES && P.scene.medium_count > 0)
+                if (FEATURES && scene().medium_count > 0)
                 {
-                    media_event(P.scene, ps.o, ps.d, ps.time, rng, ps.depth, h);
+                    media_event(scene(), ps.o, ps.d, ps.time, rng, ps.depth, h);
                 }
                 step_result res;
-                if (QUALITY)
+                if (quality())
                 {
                     sq.lit = false; // a vertex that ends the path before its light sample queues no shadow ray
-                    res = shade_quality<false, search_tree, FEATURES, true>(P.scene, cam, rng, ps, h, sample,
+                    res = shade_quality<false, search_tree, FEATURES, true>(scene(), camera(), rng, ps, h, sample,
                                                                             shadow_rays, nullptr, &sq);
                     if (sq.lit)
                     {
@@ -2371,7 +2411,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                 }
                 else
                 {
-                    res = shade_books<FEATURES>(P.scene, cam, rng, ps, h, sample);
+                    res = shade_books<FEATURES>(scene(), camera(), rng, ps, h, sample);
                 }
                 if (res == step_result::done)
                 {
@@ -2397,7 +2437,8 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                 need = true;
             }
         }
-        // Samples for the slots that need one, a pass of the image after another: one atomic per warp
+        // Samples for the slots that need one, a pass of the image after another (of each job after another): one
+        // atomic per warp
         while (true)
         {
             const unsigned needing = __ballot_sync(full_warp, need);
@@ -2409,7 +2450,8 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
             unsigned long long base = 0;
             if (static_cast<int>(lane) == leader)
             {
-                base = atomicAdd(P.work_counter, static_cast<unsigned long long>(__popc(needing)));
+                base = atomicAdd(BATCH ? W.work_counter : P.work_counter,
+                                 static_cast<unsigned long long>(__popc(needing)));
             }
             base = __shfl_sync(full_warp, base, leader);
             if (need)
@@ -2422,19 +2464,30 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                 }
                 else
                 {
-                    const int64_t j = static_cast<int64_t>(s / static_cast<unsigned long long>(P.padded_pixels));
-                    const int q = static_cast<int>(s % static_cast<unsigned long long>(P.padded_pixels));
+                    const int k = BATCH ? find_job<job_samples>(W.jobs, W.job_first, W.job_end,
+                                                                 static_cast<int64_t>(s))
+                                        : 0;
+                    const batch_job* K = BATCH ? W.jobs + k : nullptr;
+                    const int padded = BATCH ? K->padded_pixels : P.padded_pixels;
+                    const int tiles_x = BATCH ? K->tiles_x : P.tiles_x;
+                    const camera_params& c = BATCH ? K->cam : P.cam;
+                    const int64_t local = static_cast<int64_t>(s) - (BATCH ? K->sample_begin : 0);
+                    const int64_t j = local / padded;
+                    const int q = static_cast<int>(local - j * padded);
                     const int tile = q >> 5;
                     const int l = q & 31;
-                    const int x = (tile % P.tiles_x) * 8 + (l & 7);
-                    const int y = (tile / P.tiles_x) * 4 + (l >> 3);
-                    if (x < cam.width && y < cam.height) // a lane of a tile over the image's edge claims again
+                    const int x = (tile % tiles_x) * 8 + (l & 7);
+                    const int y = (tile / tiles_x) * 4 + (l >> 3);
+                    if (x < c.width && y < c.height) // a lane of a tile over the image's edge claims again
                     {
                         px = x;
                         py = y;
+                        job = k;
+                        J = K;
                         sample_index = static_cast<int64_t>(s);
-                        pass = P.pass_begin + j;
-                        rng.pixel = static_cast<uint32_t>(y) * static_cast<uint32_t>(cam.width) + static_cast<uint32_t>(x);
+                        pass = (BATCH ? K->pass_begin : P.pass_begin) + j;
+                        rng.job = BATCH ? K->job : P.job;
+                        rng.pixel = static_cast<uint32_t>(y) * static_cast<uint32_t>(c.width) + static_cast<uint32_t>(x);
                         need = false;
                         start = true;
                     }
@@ -2444,14 +2497,16 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
         if (start)
         {
             // A new sample, as the persistent kernel starts one
-            const int64_t round = pass / P.round_passes;
-            const int in_round = static_cast<int>(pass - round * P.round_passes);
-            const uint64_t key = P.seed + (static_cast<uint64_t>(round) << 32);
+            const int round_passes = BATCH ? J->round_passes : P.round_passes;
+            const int64_t round = pass / round_passes;
+            const int in_round = static_cast<int>(pass - round * round_passes);
+            const uint64_t key = (BATCH ? J->seed : P.seed) + (static_cast<uint64_t>(round) << 32);
             rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
             rng.pass = static_cast<uint32_t>(in_round);
             const float4 u = rng.draw(0, 0);
+            const camera_params& cam = camera();
             camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
-            ps.time = FEATURES && P.scene.has_motion ? rng.draw(0, block_time).x : 0.0f;
+            ps.time = FEATURES && scene().has_motion ? rng.draw(0, block_time).x : 0.0f;
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
             ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
             ps.bsdf_pdf = 0.0f;
@@ -2464,10 +2519,27 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
         }
         // The slot's queries: one atomic per warp for its next rays and its shadow rays
         const bool ext = (flags & wave_ext) != 0u;
-        const bool shadow = QUALITY && (flags & wave_shadow) != 0u;
+        const bool shadow = (QUALITY || BATCH) && (flags & wave_shadow) != 0u;
         const unsigned ext_lanes = __ballot_sync(full_warp, ext);
         const unsigned shadow_lanes = __ballot_sync(full_warp, shadow);
         const int queued = __popc(ext_lanes) + __popc(shadow_lanes);
+        if constexpr (BATCH)
+        {
+            // each job's segments and shadow rays, counted as queued: one atomic per job of the warp
+            const unsigned peers = __match_any_sync(full_warp, ext || shadow ? job : -1);
+            if ((ext || shadow) && static_cast<int>(lane) == __ffs(static_cast<int>(peers)) - 1)
+            {
+                const unsigned e = __popc(peers & ext_lanes), sh = __popc(peers & shadow_lanes);
+                if (e)
+                {
+                    atomicAdd(J->counters, static_cast<unsigned long long>(e));
+                }
+                if (sh)
+                {
+                    atomicAdd(J->counters + 1, static_cast<unsigned long long>(sh));
+                }
+            }
+        }
         if (queued > 0)
         {
             unsigned base = 0;
@@ -2481,7 +2553,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                 const unsigned q = base + static_cast<unsigned>(__popc(ext_lanes & lanes_below));
                 stream_store(B.query_o + q, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time));
                 stream_store(B.query_d + q, make_float4(ps.d.x, ps.d.y, ps.d.z, infinity_f));
-                stream_store(B.query_meta + q, make_int4(ps.from, ps.inward ? 1 : 0, -1, i));
+                stream_store(B.query_meta + q, make_int4(ps.from, (ps.inward ? 1 : 0) | (job << 2), -1, i));
             }
             if (shadow)
             {
@@ -2489,7 +2561,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                                    static_cast<unsigned>(__popc(shadow_lanes & lanes_below));
                 stream_store(B.query_o + q, make_float4(sq.o.x, sq.o.y, sq.o.z, ps.time));
                 stream_store(B.query_d + q, make_float4(sq.d.x, sq.d.y, sq.d.z, sq.t_max));
-                stream_store(B.query_meta + q, make_int4(sq.from, (sq.inward ? 1 : 0) | 2, sq.skip, i));
+                stream_store(B.query_meta + q, make_int4(sq.from, (sq.inward ? 1 : 0) | 2 | (job << 2), sq.skip, i));
                 // what the next step needs of it: the light it brings and, through smoke, its segment
                 stream_store(shadow_rows + i, make_float4(sq.o.x, sq.o.y, sq.o.z, sq.t_max));
                 stream_store(shadow_rows + n + i, make_float4(sq.d.x, sq.d.y, sq.d.z, sq.contribution.x));
@@ -2503,7 +2575,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                     (ps.inward ? wave_inward : 0u);
             if (flags & wave_exhausted)
             {
-                stream_store(reinterpret_cast<int4*>(rows) + 5 * n + i, make_int4(0, static_cast<int>(flags), px, py));
+                stream_store(reinterpret_cast<int4*>(rows) + 5 * n + i, make_int4(0, static_cast<int>(flags), 0, 0));
             }
             else
             {
@@ -2516,7 +2588,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
                 stream_store(reinterpret_cast<int4*>(rows) + 4 * n + i,
                              make_int4(static_cast<int>(rng.pixel), static_cast<int>(rng.pass), ps.from, ps.rays_left));
                 stream_store(reinterpret_cast<int4*>(rows) + 5 * n + i,
-                             make_int4(ps.depth, static_cast<int>(flags), px, py));
+                             make_int4(ps.depth, static_cast<int>(flags), px | (py << 16), job));
                 stream_store(reinterpret_cast<longlong2*>(rows) + 6 * n + i, make_longlong2(sample_index, pass));
             }
         }
@@ -2533,11 +2605,13 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY, F
 #endif
 
 // The queued queries' walks through the tree: closest hits for the paths' next rays, any hit for shadow rays (the
-// persistent kernel's traverse, the same node order, leaf tests and self-intersection rules)
-template <bool FEATURES>
+// persistent kernel's traverse, the same node order, leaf tests and self-intersection rules). BATCH: each query
+// walks its own job's scene (the job in its flags); otherwise the launch's scene S. The walks are counted into
+// `counters` when it is given.
+template <bool FEATURES, bool BATCH>
 __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
-    wave_trace_kernel(const __grid_constant__ scene_view S, const __grid_constant__ wave_buffers B,
-                      unsigned long long* counters)
+    wave_trace_kernel(const __grid_constant__ scene_view S0, const __grid_constant__ wave_buffers B,
+                      const __grid_constant__ wave_batch W, unsigned long long* counters)
 {
     __shared__ unsigned block_walks[2]; // the block's closest-hit and shadow queries: the path segments and shadow rays
     if (threadIdx.x < 2)
@@ -2562,6 +2636,9 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
     int from = -1, skip = -1, slot = 0;
     bool inward = false, shadow = false;
     hit_info hit{-1, 0.0f, false};
+    // the scene the lane's query walks: its job's, or the launch's (a __grid_constant__ parameter, read in place)
+    const scene_view* job_scene = BATCH ? &W.jobs[W.job_first].scene : &S0;
+    const auto scene = [&]() -> const scene_view& { return *job_scene; };
     const auto pop = [&]() -> int {
         while (sp > 0)
         {
@@ -2619,13 +2696,17 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
                 shadow = (qm.y & 2) != 0;
                 skip = qm.z;
                 slot = qm.w;
+                if constexpr (BATCH)
+                {
+                    job_scene = &W.jobs[qm.y >> 2].scene;
+                }
                 ++walks[shadow ? 1 : 0];
                 inverse_a = 1.0f / length_squared(d);
                 inv = make_float3(safe_inverse(d.x), safe_inverse(d.y), safe_inverse(d.z));
                 os = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
                 sp = 0;
                 leaf = 0;
-                link = S.node_count == 0 ? traversal_done : 0;
+                link = scene().node_count == 0 ? traversal_done : 0;
                 has_query = true;
             }
         }
@@ -2646,7 +2727,7 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
                 }
                 if (descending)
                 {
-                    const float4* np = reinterpret_cast<const float4*>(S.nodes + link);
+                    const float4* np = reinterpret_cast<const float4*>(scene().nodes + link);
                     const float4 nx = __ldg(np);
                     const float4 ny = __ldg(np + 1);
                     const float4 nz = __ldg(np + 2);
@@ -2699,8 +2780,8 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
                 }
                 if (testing)
                 {
-                    if (test_leaf<false, false, FEATURES>(S, leaf, o, d, time, inverse_a, from, inward, skip, hit,
-                                                          nullptr, shadow))
+                    if (test_leaf<false, false, FEATURES>(scene(), leaf, o, d, time, inverse_a, from, inward, skip,
+                                                          hit, nullptr, shadow))
                     {
                         hit.id = 1; // a shadow ray's blocker: answered
                         leaf = 0;
@@ -2727,7 +2808,7 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
     atomicAdd(&block_walks[0], walks[0]);
     atomicAdd(&block_walks[1], walks[1]);
     __syncthreads();
-    if (threadIdx.x < 2 && block_walks[threadIdx.x] != 0u)
+    if (counters != nullptr && threadIdx.x < 2 && block_walks[threadIdx.x] != 0u)
     {
         atomicAdd(counters + threadIdx.x, static_cast<unsigned long long>(block_walks[threadIdx.x]));
     }
@@ -2767,6 +2848,41 @@ __global__ void wave_reduce_kernel(const reduce_params R, const float4* samples,
     sum[0] = r;
     sum[1] = g;
     sum[2] = b;
+}
+
+// A wavefront group's samples into its jobs' chunk partials, laid out as the persistent batch kernel writes them: each
+// work item (chunk, pixel) the sum of its passes' samples in pass order; items of pixels over the image's edge skipped
+__global__ void wave_batch_partials_kernel(const wave_batch W, const float4* samples)
+{
+    for (int64_t i = W.item_first + static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < W.item_end;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        const batch_job& J = W.jobs[find_job<job_items>(W.jobs, W.job_first, W.job_end, i)];
+        const int64_t local = i - J.item_begin;
+        const int64_t k = local / J.padded_pixels;
+        const int q = static_cast<int>(local - k * J.padded_pixels);
+        const int tile = q >> 5;
+        const int l = q & 31;
+        if ((tile % J.tiles_x) * 8 + (l & 7) >= J.cam.width || (tile / J.tiles_x) * 4 + (l >> 3) >= J.cam.height)
+        {
+            continue;
+        }
+        const int64_t chunk_first = (J.first_chunk + k) * J.chunk;
+        const int64_t begin = chunk_first > J.pass_begin ? chunk_first : J.pass_begin;
+        const int64_t end = chunk_first + J.chunk < J.pass_end ? chunk_first + J.chunk : J.pass_end;
+        double r = 0.0, g = 0.0, b = 0.0;
+        for (int64_t pass = begin; pass < end; ++pass)
+        {
+            const float4 s = samples[J.sample_begin + (pass - J.pass_begin) * J.padded_pixels + q];
+            r += without_nan(s.x);
+            g += without_nan(s.y);
+            b += without_nan(s.z);
+        }
+        double* out = J.partials + 3 * local;
+        out[0] = r;
+        out[1] = g;
+        out[2] = b;
+    }
 }
 } // namespace
 
@@ -2824,9 +2940,9 @@ batch_function batch_kernel_of(int group)
 }
 } // namespace
 
-cudaError_t launch_batch(const batch_params& p, const int* grids, cudaStream_t stream)
+cudaError_t launch_batch(const batch_params& p, const int* grids, int first_group, int end_group, cudaStream_t stream)
 {
-    for (int g = 0; g < batch_groups; ++g)
+    for (int g = first_group; g < end_group; ++g)
     {
         batch_kernel_of(g)<<<grids[g], render_block, 0, stream>>>(p);
         const cudaError_t e = cudaGetLastError();
@@ -2835,7 +2951,12 @@ cudaError_t launch_batch(const batch_params& p, const int* grids, cudaStream_t s
             return e;
         }
     }
-    reduce_batch_kernel<<<grids[batch_groups - 1], 256, 0, stream>>>(p);
+    return cudaSuccess;
+}
+
+cudaError_t launch_batch_reduce(const batch_params& p, int grid, cudaStream_t stream)
+{
+    reduce_batch_kernel<<<grid, 256, 0, stream>>>(p);
     return cudaGetLastError();
 }
 
@@ -2914,19 +3035,22 @@ size_t wave_slot_bytes() { return (wave_rows + wave_shadow_rows) * sizeof(float4
 
 namespace
 {
-using wave_shade_function = void (*)(launch_params, wave_buffers);
-using wave_trace_function = void (*)(scene_view, wave_buffers, unsigned long long*);
+using wave_shade_function = void (*)(launch_params, wave_buffers, wave_batch);
+using wave_trace_function = void (*)(scene_view, wave_buffers, wave_batch, unsigned long long*);
 
 wave_shade_function wave_shade_of(bool quality, bool features)
 {
     if (quality)
     {
-        return features ? wave_shade_kernel<true, true> : wave_shade_kernel<true, false>;
+        return features ? wave_shade_kernel<true, true, false> : wave_shade_kernel<true, false, false>;
     }
-    return features ? wave_shade_kernel<false, true> : wave_shade_kernel<false, false>;
+    return features ? wave_shade_kernel<false, true, false> : wave_shade_kernel<false, false, false>;
 }
 
-wave_trace_function wave_trace_of(bool features) { return features ? wave_trace_kernel<true> : wave_trace_kernel<false>; }
+wave_trace_function wave_trace_of(bool features)
+{
+    return features ? wave_trace_kernel<true, false> : wave_trace_kernel<false, false>;
+}
 } // namespace
 
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
@@ -2938,13 +3062,45 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
         return e;
     }
     const bool features = has_features(p.scene);
-    wave_shade_of(quality, features)<<<b.slot_count / render_block, render_block, 0, stream>>>(p, b);
+    wave_shade_of(quality, features)<<<b.slot_count / render_block, render_block, 0, stream>>>(p, b, wave_batch{});
     e = cudaGetLastError();
     if (e != cudaSuccess)
     {
         return e;
     }
-    wave_trace_of(features)<<<trace_grid, render_block, 0, stream>>>(p.scene, b, p.counters);
+    wave_trace_of(features)<<<trace_grid, render_block, 0, stream>>>(p.scene, b, wave_batch{}, p.counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, const wave_buffers& b, int trace_grid,
+                                   cudaStream_t stream)
+{
+    cudaError_t e = cudaMemsetAsync(b.control, 0, 2 * sizeof(unsigned), stream);
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    const launch_params none{};
+    const auto shade = features ? wave_shade_kernel<false, true, true> : wave_shade_kernel<false, false, true>;
+    shade<<<b.slot_count / render_block, render_block, 0, stream>>>(none, b, w);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+    {
+        return e;
+    }
+    const auto trace = features ? wave_trace_kernel<true, true> : wave_trace_kernel<false, true>;
+    trace<<<trace_grid, render_block, 0, stream>>>(scene_view{}, b, w, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream)
+{
+    if (w.item_end <= w.item_first)
+    {
+        return cudaSuccess;
+    }
+    const int64_t blocks = std::min<int64_t>((w.item_end - w.item_first + 255) / 256, 148 * 16);
+    wave_batch_partials_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(w, b.samples);
     return cudaGetLastError();
 }
 

@@ -46,7 +46,8 @@ struct reduce_params
 
 // One job of a batched launch: a resident scene's view, its camera, and the passes this step renders of it. Its work
 // items are numbered from item_begin in the batch's item space, its pixels from pixel_begin in the batch's pixel
-// space (for the reduction); partials is its own slice of the batch's partials arena.
+// space (for the reduction); partials is its own slice of the batch's partials arena. A job of a group the wavefront
+// renders numbers its samples from sample_begin in its group's sample space.
 struct alignas(16) batch_job
 {
     scene_view scene;
@@ -57,6 +58,7 @@ struct alignas(16) batch_job
     int64_t first_chunk;
     int64_t item_begin;
     int64_t pixel_begin;
+    int64_t sample_begin;
     double* partials;
     double* sums;                 // width * height * 3, this job's
     unsigned long long* counters; // [0] segments, [1] shadow rays, this job's, accumulated
@@ -76,10 +78,14 @@ struct alignas(16) batch_job
 // its kernels are compiled with their code, the others without
 inline bool has_features(const scene_view& s) { return s.has_motion != 0 || s.has_textures != 0 || s.medium_count > 0; }
 
-// The jobs come in four groups, each rendered by its own launch of the kernel compiled for it: flat scenes without
-// the second book's features, flat scenes with them, then the same two of tree scenes (batch_group)
-constexpr int batch_groups = 4;
+// The jobs come in six groups. Four are rendered each by its own launch of the persistent kernel compiled for it:
+// flat scenes without the second book's features, flat scenes with them, then the same two of tree scenes
+// (batch_group). The last two, the scenes of large trees without and with the features (wave_batch_group), are
+// rendered in the wavefront form, whose walks pay for their queues only where the walks are long.
+constexpr int persistent_groups = 4;
+constexpr int batch_groups = 6;
 RTB_HD constexpr int batch_group(bool flat, bool features) { return (flat ? 0 : 2) + (features ? 1 : 0); }
+RTB_HD constexpr int wave_batch_group(bool features) { return persistent_groups + (features ? 1 : 0); }
 
 struct batch_header
 {
@@ -97,6 +103,18 @@ struct batch_params
     unsigned long long* work_counter; // one per group's launch
 };
 
+// The batch engine's groups of tree-searched jobs in the wavefront form: the jobs [job_first, job_end) of the table,
+// their samples numbered from 0 (job j's from jobs[j].sample_begin) up to the wave_buffers' sample_count
+struct wave_batch
+{
+    const batch_job* jobs;
+    int32_t job_first;
+    int32_t job_end;
+    int64_t item_first; // the group's work items [item_first, item_end) in the batch's item space
+    int64_t item_end;
+    unsigned long long* work_counter; // the group's samples taken so far (zero at the start)
+};
+
 // The kernels' static properties for kernel_info
 struct kernel_attributes
 {
@@ -112,9 +130,10 @@ constexpr int render_block = 128;
 
 cudaError_t launch_render(const launch_params& p, bool quality, bool counting, int grid, cudaStream_t stream);
 cudaError_t launch_reduce(const reduce_params& p, cudaStream_t stream);
-// The batched step: the persistent kernel of each group over its jobs' items (grids[g] threads blocks), then the
-// reduction of every job's pixels
-cudaError_t launch_batch(const batch_params& p, const int* grids, cudaStream_t stream);
+// The batched step: the persistent kernel of groups [first_group, end_group) over their jobs' items (grids[g]
+// blocks each), and the reduction of every job's pixels
+cudaError_t launch_batch(const batch_params& p, const int* grids, int first_group, int end_group, cudaStream_t stream);
+cudaError_t launch_batch_reduce(const batch_params& p, int grid, cudaStream_t stream);
 cudaError_t batch_attributes(int group, kernel_attributes& out);
 // The attributes of the render kernel that launch_render picks for the scene and integrator
 cudaError_t render_attributes(const scene_view& scene, bool quality, kernel_attributes& out);
@@ -145,6 +164,11 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
 // The samples of passes [pass_begin, pass_end) into the sums (chunk partials in pass order, added in chunk order)
 cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
                                int32_t chunk, cudaStream_t stream);
+// The same for a group of batch jobs (features: the group's kernels compile the second book's features), and the
+// group's samples into its jobs' chunk partials (then the batch's reduction adds them into the sums)
+cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, const wave_buffers& b, int trace_grid,
+                                   cudaStream_t stream);
+cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream);
 // The shade kernel's and the trace kernel's attributes for the scene and integrator
 cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace);
 

@@ -19,18 +19,7 @@ namespace
 {
 constexpr double max_launch_seconds = 0.5;              // renderer.h:413
 constexpr size_t partial_budget_bytes = size_t{1} << 30; // a launch's chunk partials: at most 1 GiB
-// The wavefront's slots (paths in flight: 2^20 take 160 MB, and their queries 96 MB; the trace kernel's throughput
-// grew with them up to here on the mesh, where a step's walks must outlast its slowest one), and its steps per group
-// between two looks at the queue's length
-#ifndef RTB_WAVE_SLOTS
-#define RTB_WAVE_SLOTS (1 << 20)
-#endif
-#ifndef RTB_WAVE_GROUP
-#define RTB_WAVE_GROUP 8
-#endif
-constexpr int wave_slots = RTB_WAVE_SLOTS / render_block * render_block;
 constexpr size_t wave_sample_budget_bytes = size_t{2} << 30; // a wavefront launch's samples (16 bytes each): 2 GiB
-constexpr int wave_group = RTB_WAVE_GROUP;
 } // namespace
 
 session::session(std::shared_ptr<resident_scene> scene, const rt_session_options& options)
@@ -63,13 +52,7 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
         kernel_attributes shade{}, trace{};
         check(wave_attributes(view, scene_->quality(), shade, trace), "querying the wavefront kernels");
         trace_grid_ = trace.multiprocessors * std::max(1, trace.blocks_per_sm);
-        wave_max_slots_ = wave_slots;
-        check(cudaHostAlloc(reinterpret_cast<void**>(&wave_queued_), 2 * sizeof(unsigned), cudaHostAllocDefault),
-              "allocating pinned memory");
-        for (auto& e : wave_done_)
-        {
-            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating a CUDA event");
-        }
+        wave_ = std::make_unique<wave_runner>(wave_slots, wave_group);
     }
     counters_.allocate(7);
     set_camera(scene_->camera());
@@ -77,17 +60,6 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
 
 session::~session()
 {
-    for (auto& e : wave_done_)
-    {
-        if (e)
-        {
-            cudaEventDestroy(e);
-        }
-    }
-    if (wave_queued_)
-    {
-        cudaFreeHost(wave_queued_);
-    }
     partials_.release();
     sums_.release();
     counters_.release();
@@ -202,12 +174,13 @@ double session::launch(int64_t end)
     wave_buffers b{};
     if (wave)
     {
-        b = wave_setup(static_cast<int64_t>(padded_pixels_) * (end - passes_)); // allocated before the timing starts
+        b = wave_->setup(static_cast<int64_t>(padded_pixels_) * (end - passes_)); // allocated before the timing starts
     }
     check(cudaEventRecord(start_, stream_), "recording a CUDA event");
     if (wave)
     {
-        run_wavefront(p, b);
+        const bool quality = scene_->quality();
+        wave_->run(b, camera_.max_depth, stream_, [&] { return launch_wave_step(p, quality, b, trace_grid_, stream_); });
         check(launch_wave_reduce(r, b, p.pass_begin, p.pass_end, p.chunk, stream_), "launching the reduction");
     }
     else
@@ -225,76 +198,6 @@ double session::launch(int64_t end)
     passes_ = end;
     kernel_seconds_ += seconds;
     return seconds;
-}
-
-wave_buffers session::wave_setup(int64_t samples)
-{
-    if (wave_slots_.size() == 0)
-    {
-        const auto n = static_cast<size_t>(wave_max_slots_);
-        wave_slots_.allocate(n * wave_slot_bytes());
-        query_o_.allocate(2 * n);
-        query_d_.allocate(2 * n);
-        query_meta_.allocate(2 * n);
-        ext_result_.allocate(n);
-        shadow_result_.allocate(n);
-        wave_control_.allocate(2);
-    }
-    if (wave_samples_.size() < static_cast<size_t>(samples))
-    {
-        wave_samples_.allocate(static_cast<size_t>(samples));
-    }
-    const int64_t wanted = (samples + render_block - 1) / render_block * render_block;
-    wave_buffers b{};
-    b.slots = wave_slots_.data();
-    b.slot_count = static_cast<int32_t>(std::min<int64_t>(wave_max_slots_, wanted));
-    b.samples = wave_samples_.data();
-    b.sample_count = samples;
-    b.query_o = query_o_.data();
-    b.query_d = query_d_.data();
-    b.query_meta = query_meta_.data();
-    b.ext_result = ext_result_.data();
-    b.shadow_result = shadow_result_.data();
-    b.control = wave_control_.data();
-    return b;
-}
-
-void session::run_wavefront(const launch_params& p, const wave_buffers& b)
-{
-    const int64_t samples = b.sample_count;
-    check(cudaMemsetAsync(b.slots, 0, static_cast<size_t>(b.slot_count) * wave_slot_bytes(), stream_),
-          "clearing the path slots");
-    // A sample takes at most max_depth + 1 steps (its segments, then the one that adds its last shadow ray) and a slot
-    // renders at most its share of the samples one after another: twice that bounds a launch that works
-    const int64_t samples_per_slot = (samples + b.slot_count - 1) / b.slot_count;
-    const int64_t step_limit = 2 * (samples_per_slot * (camera_.max_depth + 2) + 4 * wave_group);
-    // Groups of steps, two in flight: the host reads one group's queue length while the next group runs; a group
-    // after the end finds every slot out of work and costs a few microseconds a step
-    int64_t steps = 0;
-    for (int group = 0;; ++group)
-    {
-        for (int s = 0; s < wave_group; ++s)
-        {
-            check(launch_wave_step(p, scene_->quality(), b, trace_grid_, stream_), "launching a wavefront step");
-        }
-        steps += wave_group;
-        const int k = group & 1;
-        check(cudaMemcpyAsync(wave_queued_ + k, b.control, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_),
-              "reading the queue's length");
-        check(cudaEventRecord(wave_done_[k], stream_), "recording a CUDA event");
-        if (group > 0)
-        {
-            check(cudaEventSynchronize(wave_done_[k ^ 1]), "rendering on the GPU");
-            if (wave_queued_[k ^ 1] == 0)
-            {
-                break;
-            }
-        }
-        if (steps > step_limit)
-        {
-            fail(RT_ERR_RUNTIME, "the wavefront's paths did not finish within their steps");
-        }
-    }
 }
 
 rt_render_report session::render_to(int64_t target)

@@ -1,0 +1,104 @@
+// The wavefront's host side, shared by sessions and the batch engine: its buffers (grown to the launch, never shrunk)
+// and the loop of steps that ends when a step queues no ray.
+#include <algorithm>
+#include <functional>
+
+#include "host.h"
+
+namespace rtb
+{
+wave_runner::~wave_runner()
+{
+    for (auto& e : done_)
+    {
+        if (e)
+        {
+            cudaEventDestroy(e);
+        }
+    }
+    if (queued_)
+    {
+        cudaFreeHost(queued_);
+    }
+}
+
+wave_buffers wave_runner::setup(int64_t samples)
+{
+    if (!queued_)
+    {
+        check(cudaHostAlloc(reinterpret_cast<void**>(&queued_), 2 * sizeof(unsigned), cudaHostAllocDefault),
+              "allocating pinned memory");
+        for (auto& e : done_)
+        {
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating a CUDA event");
+        }
+        control_.allocate(2);
+    }
+    const int64_t wanted = (samples + render_block - 1) / render_block * render_block;
+    const auto n = static_cast<size_t>(std::min<int64_t>(max_slots, std::max<int64_t>(wanted, render_block)));
+    if (ext_result_.size() < n)
+    {
+        slots_.allocate(n * wave_slot_bytes());
+        query_o_.allocate(2 * n);
+        query_d_.allocate(2 * n);
+        query_meta_.allocate(2 * n);
+        ext_result_.allocate(n);
+        shadow_result_.allocate(n);
+    }
+    if (samples_.size() < static_cast<size_t>(samples))
+    {
+        samples_.allocate(static_cast<size_t>(samples));
+    }
+    wave_buffers b{};
+    b.slots = slots_.data();
+    b.slot_count = static_cast<int32_t>(n);
+    b.samples = samples_.data();
+    b.sample_count = samples;
+    b.query_o = query_o_.data();
+    b.query_d = query_d_.data();
+    b.query_meta = query_meta_.data();
+    b.ext_result = ext_result_.data();
+    b.shadow_result = shadow_result_.data();
+    b.control = control_.data();
+    return b;
+}
+
+int64_t wave_runner::run(const wave_buffers& b, int max_depth, cudaStream_t stream,
+                         const std::function<cudaError_t()>& step)
+{
+    check(cudaMemsetAsync(b.slots, 0, static_cast<size_t>(b.slot_count) * wave_slot_bytes(), stream),
+          "clearing the path slots");
+    // A sample takes at most max_depth + 1 steps (its segments, then the one that adds its last shadow ray) and a slot
+    // renders at most its share of the samples one after another: twice that bounds a launch that works
+    const int64_t samples_per_slot = (b.sample_count + b.slot_count - 1) / b.slot_count;
+    const int64_t step_limit = 2 * (samples_per_slot * (max_depth + 2) + 4 * group);
+    // Groups of steps, two in flight: the host reads one group's queue length while the next group runs; a group
+    // after the end finds every slot out of work and costs a few microseconds a step
+    int64_t steps = 0;
+    for (int g = 0;; ++g)
+    {
+        for (int s = 0; s < group; ++s)
+        {
+            check(step(), "launching a wavefront step");
+        }
+        steps += group;
+        const int k = g & 1;
+        check(cudaMemcpyAsync(queued_ + k, b.control, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
+              "reading the queue's length");
+        check(cudaEventRecord(done_[k], stream), "recording a CUDA event");
+        if (g > 0)
+        {
+            check(cudaEventSynchronize(done_[k ^ 1]), "rendering on the GPU");
+            if (queued_[k ^ 1] == 0)
+            {
+                break;
+            }
+        }
+        if (steps > step_limit)
+        {
+            fail(RT_ERR_RUNTIME, "the wavefront's paths did not finish within their steps");
+        }
+    }
+    return steps;
+}
+} // namespace rtb

@@ -39,7 +39,9 @@ def test_batch_equals_plain_renders(rt):
     jobs = _mixed_scenes(rt)
     b = rt.batch_render(jobs)
     assert b.graph
-    assert b.steps >= 1 and b.launches == 5 * b.steps  # four groups' launches and the reduction
+    # per step: the two flat groups' persistent launches and the reduction, and for the tree-searched jobs (the cover
+    # scene) the wavefront's shade and trace launches of each step and its partials
+    assert b.steps >= 1 and b.launches > 3 * b.steps
     for (scene, seed, passes), img in zip(jobs, b.images):
         ref = rt.render(scene, seed=seed, passes=passes)
         assert img.shape == ref.pixels.shape
@@ -141,3 +143,19 @@ def test_server_admits_under_the_budget_in_order(rt):
     with pytest.raises(rt.CapacityError):
         server.submit(g, rt.builtin_camera("glass", width=4000), 1, 1)
     server.close()
+
+
+def test_large_tree_jobs_take_the_wavefront(rt):
+    """A job of a large tree (the mesh at 82k triangles) renders in the batch's wavefront groups beside jobs of the
+    persistent groups; its image is a session's render of the same view and seed (the session's wavefront: the same
+    samples, to the rounding of separately compiled kernels)."""
+    jobs = [(rt.builtin_scene("mesh-ggx", width=64, spp=16, mesh_level=6, env_width=64), 21, 16),
+            (rt.builtin_scene("cover-40", width=40, spp=16, scene_seed=5), 22, 16),
+            (rt.builtin_scene("glass", width=32, spp=16), 23, 16)]
+    b = rt.batch_render(jobs)
+    assert b.launches > 5 * b.steps  # the wavefront's steps beside the persistent groups' launches and the reduction
+    for (scene, seed, passes), img in zip(jobs, b.images):
+        ref = rt.render(scene, seed=seed, passes=passes).pixels
+        close = np.isclose(img, ref, rtol=1e-4, atol=1e-5 * max(abs(ref.mean()), 1e-3))
+        assert close.mean() >= 0.99, close.mean()
+        assert abs(img.mean() - ref.mean()) <= 2e-4 * max(abs(ref.mean()), 1e-3), (img.mean(), ref.mean())
