@@ -332,6 +332,7 @@ def served_measurement(rt, torch, args) -> dict:
     start = time.perf_counter()
     submitted = {}
     limit = args.served_limit
+    step_log = []  # (wall s, GPU s, first frames, refined, admitted) of each step
     while True:
         now = time.perf_counter() - start
         while pending and requests[pending[0]]["arrival"] <= now:
@@ -344,6 +345,8 @@ def served_measurement(rt, torch, args) -> dict:
         if now > limit:
             break
         rep = server.step()
+        step_log.append((round(time.perf_counter() - start, 4), round(rep["gpu_seconds"], 5), rep["first_frames"],
+                         rep["refined"], rep["admitted"]))
         if rep["active"] == 0 and rep["queued"] == 0 and pending:
             time.sleep(max(0.0, requests[pending[0]]["arrival"] - (time.perf_counter() - start)))
     wall = time.perf_counter() - start
@@ -389,6 +392,9 @@ def served_measurement(rt, torch, args) -> dict:
             "ttff_by_resolution": {k: {"requests": len(v), "p50_s": pct(v, 50), "p99_s": pct(v, 99)}
                                    for k, v in sorted(by_size.items())},
             "step_seconds": args.served_step,
+            "step_gpu_seconds_max": max((s[1] for s in step_log), default=None),
+            "steps_over_twice_the_budget": sum(1 for s in step_log if s[1] > 2 * args.served_step),
+            "first_steps": step_log[:12],
             "time_to_target_p50_s": pct(ttt, 50), "time_to_target_p99_s": pct(ttt, 99),
             "served_segments_per_s": stats["rays"] / stats["gpu_seconds"] if stats["gpu_seconds"] else None,
             "served_steps": stats["steps"], "served_launches": stats["launches"],

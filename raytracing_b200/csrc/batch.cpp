@@ -49,11 +49,19 @@ batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
     wave_ = std::make_unique<wave_runner>(wave_slots, wave_group);
     work_counter_.allocate(batch_groups);
     header_.allocate(1);
+    // The device's pool keeps what the jobs free for the next jobs (a process-wide setting of this process's pool)
+    int device = 0;
+    check(cudaGetDevice(&device), "querying the device");
+    cudaMemPool_t pool = nullptr;
+    check(cudaDeviceGetDefaultMemPool(&pool, device), "querying the memory pool");
+    uint64_t keep = UINT64_MAX;
+    check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "setting the memory pool");
     check(cudaMallocHost(reinterpret_cast<void**>(&header_host_), sizeof(batch_header)), "allocating pinned memory");
 }
 
 batch_engine::~batch_engine()
 {
+    jobs_.clear(); // their arrays are freed on the stream, before it goes
     release_graph();
     if (table_host_)
     {
@@ -115,8 +123,8 @@ int batch_engine::add(std::shared_ptr<resident_scene> scene, const rt_camera_des
     j->id = job_id;
     j->tiles_x = (camera.image_width + 7) / 8;
     j->padded = static_cast<int>(padded_of(camera));
-    j->sums.allocate(static_cast<size_t>(camera.image_width) * camera.image_height * 3);
-    j->counters.allocate(2);
+    j->sums.allocate_async(static_cast<size_t>(camera.image_width) * camera.image_height * 3, stream_);
+    j->counters.allocate_async(2, stream_);
     check(cudaMemsetAsync(j->sums.data(), 0, j->sums.bytes(), stream_), "clearing the sums");
     check(cudaMemsetAsync(j->counters.data(), 0, j->counters.bytes(), stream_), "clearing the counters");
     const int handle = next_handle_++;
@@ -466,24 +474,36 @@ rt_server_step_report render_server::step()
         queue_.pop_front();
         ++report.admitted;
     }
-    // First frames: every active request without a pass gets one, whatever the step's budget
+    // First frames, in arrival order, while the step's time allows (at least one): a burst of large first frames
+    // spreads over steps rather than holding up the ones behind it for a long step
     std::vector<batch_engine::assignment> work;
+    std::vector<std::pair<const resident_scene*, double>> step_samples; // each job's scene and pixel passes
     double planned = 0;
-    const double rate = samples_per_second_ > 0 ? samples_per_second_ : 1e9;
     for (auto& [id, r] : requests_)
     {
         if (r.state == RT_REQUEST_ACTIVE && engine_.passes(r.handle) == 0)
         {
+            const double pixels = double(r.camera.image_width) * r.camera.image_height;
+            if (report.first_frames > 0 && planned + pixels * cost_of(r.scene.get()) > options_.step_seconds)
+            {
+                break;
+            }
             work.push_back({r.handle, 1});
-            planned += double(r.camera.image_width) * r.camera.image_height / rate;
+            step_samples.emplace_back(r.scene.get(), pixels);
+            planned += pixels * cost_of(r.scene.get());
             ++report.first_frames;
         }
     }
     // Refinement: the others, least remaining work first (shortest remaining processing time, which minimises the
-    // mean time to target), while the step's time allows
+    // mean time to target), while the step's time allows. A step with first frames carries nothing else: a first
+    // frame waits for no refinement, and the next step refines.
     std::vector<std::pair<double, request*>> refine;
     for (auto& [id, r] : requests_)
     {
+        if (report.first_frames > 0)
+        {
+            break;
+        }
         if (r.state != RT_REQUEST_ACTIVE)
         {
             continue;
@@ -504,7 +524,7 @@ rt_server_step_report render_server::step()
         {
             break;
         }
-        const double per_pass = double(r.camera.image_width) * r.camera.image_height / rate;
+        const double per_pass = double(r.camera.image_width) * r.camera.image_height * cost_of(r.scene.get());
         const int64_t want = std::max<int64_t>(1, static_cast<int64_t>((options_.step_seconds - planned) / per_pass));
         int64_t end = std::min(r.target, done + want);
         // finish the chunk the request is in, or stop on a chunk boundary
@@ -515,6 +535,8 @@ rt_server_step_report render_server::step()
             end = std::min(r.target, boundary);
         }
         work.push_back({r.handle, end});
+        step_samples.emplace_back(r.scene.get(), double(r.camera.image_width) * r.camera.image_height *
+                                                     double(end - done));
         planned += per_pass * double(end - done);
         ++report.refined;
     }
@@ -523,8 +545,7 @@ rt_server_step_report render_server::step()
         report.gpu_seconds = engine_.step(std::move(work));
         if (report.gpu_seconds > 0)
         {
-            const double measured = double(engine_.last_samples()) / report.gpu_seconds;
-            samples_per_second_ = samples_per_second_ > 0 ? 0.5 * samples_per_second_ + 0.5 * measured : measured;
+            learn_costs(step_samples, report.gpu_seconds);
         }
         stats_.gpu_seconds += report.gpu_seconds;
         ++stats_.steps;
@@ -558,6 +579,40 @@ rt_server_step_report render_server::step()
     report.queued = static_cast<int32_t>(queue_.size());
     stats_.launches = engine_.launches();
     return report;
+}
+
+double render_server::cost_of(const resident_scene* scene) const
+{
+    const auto it = cost_.find(scene);
+    return it != cost_.end() ? it->second : (default_cost_ > 0 ? default_cost_ : 1e-9);
+}
+
+// The seconds a pixel pass costs, per scene (the mesh costs several times the Cornell box's): a step's measured time
+// against its prediction corrects each of its scenes in proportion to that scene's predicted share of the step
+void render_server::learn_costs(const std::vector<std::pair<const resident_scene*, double>>& samples, double seconds)
+{
+    double predicted = 0, total = 0;
+    std::map<const resident_scene*, double> share;
+    for (const auto& [scene, n] : samples)
+    {
+        const double c = cost_of(scene) * n;
+        share[scene] += c;
+        predicted += c;
+        total += n;
+    }
+    if (!(predicted > 0) || !(total > 0))
+    {
+        return;
+    }
+    const double measured = seconds / total;
+    default_cost_ = default_cost_ > 0 ? 0.5 * default_cost_ + 0.5 * measured : measured;
+    const double factor = seconds / predicted;
+    for (const auto& [scene, c] : share)
+    {
+        const bool fresh = cost_.find(scene) == cost_.end();
+        const double corrected = cost_of(scene) * std::pow(factor, c / predicted);
+        cost_[scene] = fresh ? corrected : 0.5 * cost_of(scene) + 0.5 * corrected;
+    }
 }
 
 rt_request_status render_server::poll(int64_t id) const

@@ -130,8 +130,12 @@ private:
     std::deque<int64_t> queue_;
     int64_t next_id_ = 1;
     size_t used_bytes_ = 0;
-    double samples_per_second_ = 0;
+    std::map<const resident_scene*, double> cost_; // seconds per pixel pass, learned per scene
+    double default_cost_ = 0;                      // the same over every scene, for a scene not seen yet
     rt_server_stats stats_{};
+
+    double cost_of(const resident_scene* scene) const;
+    void learn_costs(const std::vector<std::pair<const resident_scene*, double>>& samples, double seconds);
 };
 } // namespace rtb
 

@@ -38,7 +38,7 @@ public:
     ~device_array() { release(); }
     device_array(const device_array&) = delete;
     device_array& operator=(const device_array&) = delete;
-    device_array(device_array&& o) noexcept : data_(o.data_), count_(o.count_)
+    device_array(device_array&& o) noexcept : data_(o.data_), count_(o.count_), stream_(o.stream_)
     {
         o.data_ = nullptr;
         o.count_ = 0;
@@ -50,6 +50,7 @@ public:
             release();
             data_ = o.data_;
             count_ = o.count_;
+            stream_ = o.stream_;
             o.data_ = nullptr;
             o.count_ = 0;
         }
@@ -73,14 +74,36 @@ public:
             check(cudaMemcpy(data_, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "copying to the device");
         }
     }
+    // Stream-ordered, from the device's memory pool (no device-wide synchronisation; the pool keeps freed memory for
+    // the next request): for arrays that come and go while kernels run, as a server's requests do. `stream` must
+    // outlive the array.
+    void allocate_async(size_t count, cudaStream_t stream)
+    {
+        release();
+        if (count > 0)
+        {
+            check(cudaMallocAsync(reinterpret_cast<void**>(&data_), count * sizeof(T), stream),
+                  "allocating device memory");
+            stream_ = stream;
+        }
+        count_ = count;
+    }
     void release()
     {
         if (data_)
         {
-            cudaFree(data_);
+            if (stream_)
+            {
+                cudaFreeAsync(data_, stream_);
+            }
+            else
+            {
+                cudaFree(data_);
+            }
         }
         data_ = nullptr;
         count_ = 0;
+        stream_ = nullptr;
     }
     T* data() const { return data_; }
     size_t size() const { return count_; }
@@ -89,6 +112,7 @@ public:
 private:
     T* data_ = nullptr;
     size_t count_ = 0;
+    cudaStream_t stream_ = nullptr; // set when allocated stream-ordered
 };
 
 // Checks a scene's tables before anything is built (the reference's validate, renderer.cu:688-900); throws rt_error

@@ -36,18 +36,20 @@ wave_buffers wave_runner::setup(int64_t samples)
     }
     const int64_t wanted = (samples + render_block - 1) / render_block * render_block;
     const auto n = static_cast<size_t>(std::min<int64_t>(max_slots, std::max<int64_t>(wanted, render_block)));
+    // grown by doubling, never shrunk: a stream of launches of growing size reallocates a few times, not every time
     if (ext_result_.size() < n)
     {
-        slots_.allocate(n * wave_slot_bytes());
-        query_o_.allocate(2 * n);
-        query_d_.allocate(2 * n);
-        query_meta_.allocate(2 * n);
-        ext_result_.allocate(n);
-        shadow_result_.allocate(n);
+        const size_t c = std::min<size_t>(static_cast<size_t>(max_slots), std::max(n, 2 * ext_result_.size()));
+        slots_.allocate(c * wave_slot_bytes());
+        query_o_.allocate(2 * c);
+        query_d_.allocate(2 * c);
+        query_meta_.allocate(2 * c);
+        ext_result_.allocate(c);
+        shadow_result_.allocate(c);
     }
     if (samples_.size() < static_cast<size_t>(samples))
     {
-        samples_.allocate(static_cast<size_t>(samples));
+        samples_.allocate(std::max(static_cast<size_t>(samples), 2 * samples_.size()));
     }
     wave_buffers b{};
     b.slots = slots_.data();
