@@ -353,9 +353,14 @@ double batch_engine::step(std::vector<assignment> work)
         const wave_batch w{table_.data(),          header.group_jobs[g],      header.group_jobs[g + 1],
                            header.group_items[g], header.group_items[g + 1], work_counter_.data() + g};
         const bool features = g == wave_batch_group(true);
+        bool wide = true;
+        for (int32_t i = header.group_jobs[g]; i < header.group_jobs[g + 1]; ++i)
+        {
+            wide = wide && table_host_[i].scene.wide_nodes != nullptr;
+        }
         const wave_buffers b = wave_->setup(group_samples[g]);
         const int64_t steps = wave_->run(b, group_depth[g], stream_, [&] {
-            return launch_wave_batch_step(w, features, b, trace_grid_, stream_);
+            return launch_wave_batch_step(w, features, wide, b, trace_grid_, stream_);
         });
         check(launch_wave_batch_partials(w, b, stream_), "launching the wavefront's partials");
         launches_ += static_cast<int>(2 * steps + 1);

@@ -282,4 +282,84 @@ bvh_result build_bvh(std::vector<build_prim> prims, const bvh_options& options)
     b.run();
     return out;
 }
+namespace
+{
+// A child of a binary node: its box and link
+struct wide_child
+{
+    float lo[3], hi[3];
+    int32_t link;
+};
+
+wide_child child_of(const bvh_node& n, int c)
+{
+    return {{n.x[2 * c], n.y[2 * c], n.z[2 * c]}, {n.x[2 * c + 1], n.y[2 * c + 1], n.z[2 * c + 1]}, n.link[c]};
+}
+
+double area(const wide_child& c)
+{
+    const double dx = c.hi[0] - c.lo[0], dy = c.hi[1] - c.lo[1], dz = c.hi[2] - c.lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+int32_t collapse(const std::vector<bvh_node>& nodes, int32_t index, std::vector<bvh4_node>& out, int32_t level,
+                 int32_t& depth)
+{
+    depth = std::max(depth, level);
+    std::vector<wide_child> kids = {child_of(nodes[static_cast<size_t>(index)], 0),
+                                    child_of(nodes[static_cast<size_t>(index)], 1)};
+    while (kids.size() < 4)
+    {
+        int best = -1;
+        for (int k = 0; k < static_cast<int>(kids.size()); ++k)
+        {
+            if (kids[static_cast<size_t>(k)].link >= 0 && (best < 0 || area(kids[static_cast<size_t>(k)]) >
+                                                                           area(kids[static_cast<size_t>(best)])))
+            {
+                best = k;
+            }
+        }
+        if (best < 0)
+        {
+            break; // only leaves left
+        }
+        const bvh_node& n = nodes[static_cast<size_t>(kids[static_cast<size_t>(best)].link)];
+        kids[static_cast<size_t>(best)] = child_of(n, 0);
+        kids.insert(kids.begin() + best + 1, child_of(n, 1));
+    }
+    const auto self = static_cast<int32_t>(out.size());
+    out.emplace_back();
+    int32_t links[4] = {traversal_done_link, traversal_done_link, traversal_done_link, traversal_done_link};
+    for (size_t k = 0; k < kids.size(); ++k)
+    {
+        links[k] = kids[k].link >= 0 ? collapse(nodes, kids[k].link, out, level + 1, depth) : kids[k].link;
+    }
+    bvh4_node& w = out[static_cast<size_t>(self)];
+    for (int k = 0; k < 4; ++k)
+    {
+        const bool used = k < static_cast<int>(kids.size());
+        const wide_child c = used ? kids[static_cast<size_t>(k)] : wide_child{{0, 0, 0}, {0, 0, 0}, 0};
+        w.lo_x[k] = c.lo[0];
+        w.hi_x[k] = c.hi[0];
+        w.lo_y[k] = c.lo[1];
+        w.hi_y[k] = c.hi[1];
+        w.lo_z[k] = c.lo[2];
+        w.hi_z[k] = c.hi[2];
+        w.link[k] = links[k];
+        w.pad[k] = 0;
+    }
+    return self;
+}
+} // namespace
+
+int32_t collapse_bvh4(const std::vector<bvh_node>& nodes, std::vector<bvh4_node>& out)
+{
+    out.clear();
+    int32_t depth = 0;
+    if (!nodes.empty())
+    {
+        collapse(nodes, 0, out, 1, depth);
+    }
+    return depth;
+}
 } // namespace rtb

@@ -38,6 +38,11 @@ struct bvh_result
 // Throws std::runtime_error when the tree would be deeper than the traversal stack (max_bvh_depth)
 bvh_result build_bvh(std::vector<build_prim> prims, const bvh_options& options);
 
+// The binary tree collapsed four wide (each node takes its children's children, the largest first, while it has
+// fewer than four); returns the wide tree's depth. The children's boxes are the binary nodes' own, so both walks
+// test the same boxes.
+int32_t collapse_bvh4(const std::vector<bvh_node>& nodes, std::vector<bvh4_node>& out);
+
 // A double bound rounded to float toward -inf / +inf
 float round_down(double x);
 float round_up(double x);

@@ -35,6 +35,26 @@ struct alignas(64) bvh_node
 };
 static_assert(sizeof(bvh_node) == 64, "a node is four 16-byte loads");
 
+// The same tree collapsed four wide, for the wavefront's walk: the boxes of up to four children per axis and bound
+// (lo_x = the four children's x minima, ...), then their links (a leaf as in bvh_node, traversal_done for an unused
+// slot). A walk step reads 128 bytes and decides four children, and a walk takes about half the dependent steps.
+struct alignas(64) bvh4_node
+{
+    float lo_x[4];
+    float hi_x[4];
+    float lo_y[4];
+    float hi_y[4];
+    float lo_z[4];
+    float hi_z[4];
+    int32_t link[4];
+    int32_t pad[4];
+};
+static_assert(sizeof(bvh4_node) == 128, "a wide node is eight 16-byte loads");
+// No more nodes to visit, and a wide node's unused slot (a leaf link never takes this value: its kind field would be 3)
+constexpr int32_t traversal_done_link = static_cast<int32_t>(0x80000000u);
+constexpr int wide_stack = 96;   // the wide walk's stack: up to three entries a level, 32 levels
+constexpr int max_wide_depth = wide_stack / 3;
+
 // Primitive kinds; a leaf holds primitives of one kind, contiguous in that kind's array
 enum prim_kind : int32_t
 {
@@ -224,6 +244,7 @@ struct alignas(16) medium16
 struct scene_view
 {
     const bvh_node* nodes;
+    const bvh4_node* wide_nodes; // the tree four wide (null when it would be deeper than max_wide_depth)
     const sphere4* spheres;     // global ids [0, quad_base)
     const quad12* quads;        // [quad_base, triangle_base)
     const triangle12* triangles;// [triangle_base, ...)

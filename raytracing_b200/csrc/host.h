@@ -144,6 +144,7 @@ private:
     scene_view view_{};
     rt_scene_stats stats_{};
     device_array<bvh_node> nodes_;
+    device_array<bvh4_node> wide_nodes_;
     device_array<sphere4> spheres_;
     device_array<quad12> quads_;
     device_array<triangle12> triangles_;

@@ -431,7 +431,7 @@ __device__ __forceinline__ bool test_leaf(const scene_view& S, int link, float3 
 }
 
 // No more nodes to visit (a leaf link never takes this value: its kind field would be 3)
-constexpr int traversal_done = static_cast<int>(0x80000000u);
+constexpr int traversal_done = traversal_done_link;
 
 // The closest hit in (t_min, t_max) (SHADOW = false; the CPU's world.hit, bvh.cuh:576-706), or whether anything lies
 // there (SHADOW = true; shadow.cuh:26-109 occluded, `skip` not tested). The self-intersection rules of the primitive
@@ -2605,10 +2605,11 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
 #endif
 
 // The queued queries' walks through the tree: closest hits for the paths' next rays, any hit for shadow rays (the
-// persistent kernel's traverse, the same node order, leaf tests and self-intersection rules). BATCH: each query
-// walks its own job's scene (the job in its flags); otherwise the launch's scene S. The walks are counted into
-// `counters` when it is given.
-template <bool FEATURES, bool BATCH>
+// persistent kernel's traverse, the same leaf tests and self-intersection rules). WIDE: the tree four wide, a node's
+// hit children visited nearest first (a four-key sorting network); otherwise the binary tree in the persistent
+// kernel's node order. BATCH: each query walks its own job's scene (the job in its flags); otherwise the launch's
+// scene S0. The walks are counted into `counters` when it is given.
+template <bool FEATURES, bool BATCH, bool WIDE>
 __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
     wave_trace_kernel(const __grid_constant__ scene_view S0, const __grid_constant__ wave_buffers B,
                       const __grid_constant__ wave_batch W, unsigned long long* counters)
@@ -2623,7 +2624,7 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
     unsigned walks[2] = {0, 0};
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
-    int2 stack[max_bvh_depth];
+    int2 stack[WIDE ? wide_stack : max_bvh_depth];
     int sp = 0;
     int link = traversal_done;
     int leaf = 0;
@@ -2725,7 +2726,72 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
                 {
                     break;
                 }
-                if (descending)
+                if (WIDE && descending)
+                {
+                    const float4* np = reinterpret_cast<const float4*>(scene().wide_nodes + link);
+                    const float4 lx = __ldg(np), hx = __ldg(np + 1);
+                    const float4 ly = __ldg(np + 2), hy = __ldg(np + 3);
+                    const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+                    const int4 nl = __ldg(reinterpret_cast<const int4*>(np + 6));
+                    // each child's entry distance, or infinity where the ray misses it (or the slot is unused)
+                    const auto entry = [&](float lox, float hix, float loy, float hiy, float loz, float hiz,
+                                           int child) -> float {
+                        const float a0 = fmaf(lox, inv.x, -os.x), a1 = fmaf(hix, inv.x, -os.x);
+                        const float b0 = fmaf(loy, inv.y, -os.y), b1 = fmaf(hiy, inv.y, -os.y);
+                        const float c0 = fmaf(loz, inv.z, -os.z), c1 = fmaf(hiz, inv.z, -os.z);
+                        const float enter = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), t_min));
+                        const float exit = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), hit.t));
+                        return enter <= exit && child != traversal_done ? enter : infinity_f;
+                    };
+                    float k0 = entry(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, nl.x);
+                    float k1 = entry(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, nl.y);
+                    float k2 = entry(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, nl.z);
+                    float k3 = entry(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, nl.w);
+                    int l0 = nl.x, l1 = nl.y, l2 = nl.z, l3 = nl.w;
+                    const auto order = [](float& ka, int& la, float& kb, int& lb) {
+                        if (kb < ka)
+                        {
+                            const float k = ka;
+                            ka = kb;
+                            kb = k;
+                            const int l = la;
+                            la = lb;
+                            lb = l;
+                        }
+                    };
+                    order(k0, l0, k1, l1);
+                    order(k2, l2, k3, l3);
+                    order(k0, l0, k2, l2);
+                    order(k1, l1, k3, l3);
+                    order(k1, l1, k2, l2);
+                    if (k0 == infinity_f)
+                    {
+                        link = pop();
+                    }
+                    else
+                    {
+                        // the far ones wait on the stack, farthest deepest; the nearest is next
+                        if (k3 != infinity_f)
+                        {
+                            stack[sp++] = make_int2(l3, __float_as_int(k3));
+                        }
+                        if (k2 != infinity_f)
+                        {
+                            stack[sp++] = make_int2(l2, __float_as_int(k2));
+                        }
+                        if (k1 != infinity_f)
+                        {
+                            stack[sp++] = make_int2(l1, __float_as_int(k1));
+                        }
+                        link = l0;
+                    }
+                    if (link < 0 && link != traversal_done && leaf == 0)
+                    {
+                        leaf = link;
+                        link = pop();
+                    }
+                }
+                else if (descending)
                 {
                     const float4* np = reinterpret_cast<const float4*>(scene().nodes + link);
                     const float4 nx = __ldg(np);
@@ -3038,6 +3104,16 @@ namespace
 using wave_shade_function = void (*)(launch_params, wave_buffers, wave_batch);
 using wave_trace_function = void (*)(scene_view, wave_buffers, wave_batch, unsigned long long*);
 
+template <bool BATCH>
+wave_trace_function wave_trace_variant(bool features, bool wide)
+{
+    if (wide)
+    {
+        return features ? wave_trace_kernel<true, BATCH, true> : wave_trace_kernel<false, BATCH, true>;
+    }
+    return features ? wave_trace_kernel<true, BATCH, false> : wave_trace_kernel<false, BATCH, false>;
+}
+
 wave_shade_function wave_shade_of(bool quality, bool features)
 {
     if (quality)
@@ -3047,10 +3123,7 @@ wave_shade_function wave_shade_of(bool quality, bool features)
     return features ? wave_shade_kernel<false, true, false> : wave_shade_kernel<false, false, false>;
 }
 
-wave_trace_function wave_trace_of(bool features)
-{
-    return features ? wave_trace_kernel<true, false> : wave_trace_kernel<false, false>;
-}
+wave_trace_function wave_trace_of(bool features, bool wide) { return wave_trace_variant<false>(features, wide); }
 } // namespace
 
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
@@ -3068,12 +3141,13 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     {
         return e;
     }
-    wave_trace_of(features)<<<trace_grid, render_block, 0, stream>>>(p.scene, b, wave_batch{}, p.counters);
+    wave_trace_of(features, p.scene.wide_nodes != nullptr)<<<trace_grid, render_block, 0, stream>>>(
+        p.scene, b, wave_batch{}, p.counters);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, const wave_buffers& b, int trace_grid,
-                                   cudaStream_t stream)
+cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, bool wide, const wave_buffers& b,
+                                   int trace_grid, cudaStream_t stream)
 {
     cudaError_t e = cudaMemsetAsync(b.control, 0, 2 * sizeof(unsigned), stream);
     if (e != cudaSuccess)
@@ -3088,8 +3162,7 @@ cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, const wav
     {
         return e;
     }
-    const auto trace = features ? wave_trace_kernel<true, true> : wave_trace_kernel<false, true>;
-    trace<<<trace_grid, render_block, 0, stream>>>(scene_view{}, b, w, nullptr);
+    wave_trace_variant<true>(features, wide)<<<trace_grid, render_block, 0, stream>>>(scene_view{}, b, w, nullptr);
     return cudaGetLastError();
 }
 
@@ -3121,7 +3194,7 @@ cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attrib
     {
         return e;
     }
-    return attributes_of(wave_trace_of(features), trace);
+    return attributes_of(wave_trace_of(features, scene.wide_nodes != nullptr), trace);
 }
 
 cudaError_t launch_camera_rays(const camera_params& cam, uint64_t seed, int64_t pass, int32_t round_passes,

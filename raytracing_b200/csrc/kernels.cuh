@@ -164,10 +164,11 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
 // The samples of passes [pass_begin, pass_end) into the sums (chunk partials in pass order, added in chunk order)
 cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
                                int32_t chunk, cudaStream_t stream);
-// The same for a group of batch jobs (features: the group's kernels compile the second book's features), and the
-// group's samples into its jobs' chunk partials (then the batch's reduction adds them into the sums)
-cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, const wave_buffers& b, int trace_grid,
-                                   cudaStream_t stream);
+// The same for a group of batch jobs (features: the group's kernels compile the second book's features; wide: every
+// job's scene has its tree four wide), and the group's samples into its jobs' chunk partials (then the batch's
+// reduction adds them into the sums)
+cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, bool wide, const wave_buffers& b,
+                                   int trace_grid, cudaStream_t stream);
 cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream);
 // The shade kernel's and the trace kernel's attributes for the scene and integrator
 cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace);

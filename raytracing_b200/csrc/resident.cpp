@@ -947,6 +947,15 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     }
 
     nodes_.upload(tree.nodes);
+    // The tree four wide for the wavefront's walk, unless its depth would overflow that walk's stack
+    if (!tree.nodes.empty())
+    {
+        std::vector<bvh4_node> wide;
+        if (collapse_bvh4(tree.nodes, wide) <= max_wide_depth)
+        {
+            wide_nodes_.upload(wide);
+        }
+    }
     spheres_.upload(spheres);
     sphere_motion_.upload(sphere_motion);
     sphere_frames_.upload(sphere_frames);
@@ -966,6 +975,7 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     lamp_of_.upload(lamp_of);
 
     view_.nodes = nodes_.data();
+    view_.wide_nodes = wide_nodes_.data();
     view_.spheres = spheres_.data();
     view_.quads = quads_.data();
     view_.triangles = triangles_.data();
