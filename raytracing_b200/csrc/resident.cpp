@@ -70,6 +70,10 @@ quad12 make_quad(const rt_quad_desc& d)
 #ifndef RTB_LEAF_SIZE
 #define RTB_LEAF_SIZE 1
 #endif
+// and a scene with triangles leaves of at most RTB_TRIANGLE_LEAF (a triangle's test is cheap next to a node step)
+#ifndef RTB_TRIANGLE_LEAF
+#define RTB_TRIANGLE_LEAF 4
+#endif
 // A scene of at most RTB_FLAT_SCENE spheres and quads (no triangles) is searched without its tree: every primitive
 // tested in turn, the same loop in every lane of a warp, where a tree walk splits the lanes up. Measured on the
 // B200: the Cornell boxes (13-18 quads and spheres) and the five-sphere scene render 30-50% faster flat, while 20
@@ -603,7 +607,7 @@ resident_scene::resident_scene(const rt_scene_desc& d)
 
     bvh_options options;
     options.max_leaf_size = prims.size() <= RTB_SMALL_SCENE ? max_leaf_size
-                                                            : (source_triangles.empty() ? RTB_LEAF_SIZE : 4);
+                                                            : (source_triangles.empty() ? RTB_LEAF_SIZE : RTB_TRIANGLE_LEAF);
     const bvh_result tree = build_bvh(std::move(prims), options);
 
     // Each kind's array in leaf order; global ids: spheres, then quads, then triangles
