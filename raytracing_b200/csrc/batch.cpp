@@ -379,6 +379,21 @@ double batch_engine::step(std::vector<assignment> work)
     return ms / 1000.0;
 }
 
+void batch_engine::reserve_pool(size_t bytes)
+{
+    // an allocation and its release: the pool keeps the memory (its release threshold is the maximum)
+    void* p = nullptr;
+    check(cudaMallocAsync(&p, bytes, stream_), "growing the memory pool");
+    check(cudaFreeAsync(p, stream_), "growing the memory pool");
+    check(cudaStreamSynchronize(stream_), "growing the memory pool");
+}
+
+void batch_engine::reserve_wavefront(int64_t samples)
+{
+    wave_->setup(samples);
+    check(preload_wave_batch(), "loading the wavefront's kernels");
+}
+
 int64_t batch_engine::passes(int handle) const { return jobs_.at(handle)->passes; }
 
 void batch_engine::pixels(int handle, double* out, int64_t count)
@@ -434,6 +449,10 @@ render_server::render_server(const rt_server_options& options)
     {
         fail(RT_ERR_INVALID, "hbm_budget_bytes must be positive");
     }
+    // What the first requests would otherwise wait for: the wavefront's buffers (its slots and the samples of a step
+    // of 64M samples, about 1.3 GB) and its kernels' modules, and the memory pool grown to hold requests' sums
+    engine_.reserve_wavefront(int64_t{1} << 26);
+    engine_.reserve_pool(std::min<size_t>(static_cast<size_t>(options_.hbm_budget_bytes), size_t{8} << 30));
 }
 
 int64_t render_server::submit(std::shared_ptr<resident_scene> scene, const rt_camera_desc& camera, uint64_t seed,

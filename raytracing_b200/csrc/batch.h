@@ -38,6 +38,11 @@ public:
     // chunks (at least one each), so every assignment makes progress.
     double step(std::vector<assignment> work);
 
+    // The wavefront's buffers for steps of up to `samples` samples and its kernels loaded now, not on first use
+    void reserve_wavefront(int64_t samples);
+    // The device's memory pool grown to `bytes` now (the jobs' sums come from it), so that admitting requests
+    // maps no new memory
+    void reserve_pool(size_t bytes);
     int64_t passes(int handle) const;
     void pixels(int handle, double* out, int64_t count);
     uint64_t rays(int handle) const;

@@ -3166,6 +3166,27 @@ cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, bool wide
     return cudaGetLastError();
 }
 
+cudaError_t preload_wave_batch()
+{
+    cudaFuncAttributes a{};
+    const void* kernels[] = {reinterpret_cast<const void*>(wave_shade_kernel<false, false, true>),
+                             reinterpret_cast<const void*>(wave_shade_kernel<false, true, true>),
+                             reinterpret_cast<const void*>(wave_trace_variant<true>(false, false)),
+                             reinterpret_cast<const void*>(wave_trace_variant<true>(false, true)),
+                             reinterpret_cast<const void*>(wave_trace_variant<true>(true, false)),
+                             reinterpret_cast<const void*>(wave_trace_variant<true>(true, true)),
+                             reinterpret_cast<const void*>(wave_batch_partials_kernel)};
+    for (const void* k : kernels)
+    {
+        const cudaError_t e = cudaFuncGetAttributes(&a, k);
+        if (e != cudaSuccess)
+        {
+            return e;
+        }
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream)
 {
     if (w.item_end <= w.item_first)

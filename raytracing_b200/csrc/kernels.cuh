@@ -170,6 +170,8 @@ cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, in
 cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, bool wide, const wave_buffers& b,
                                    int trace_grid, cudaStream_t stream);
 cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream);
+// Loads the batch wavefront's kernels (every variant) now, so that no step pays for loading them
+cudaError_t preload_wave_batch();
 // The shade kernel's and the trace kernel's attributes for the scene and integrator
 cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace);
 
