@@ -55,10 +55,10 @@ def parse():
     p.add_argument("--no-reference-gpu", action="store_true",
                    help="skip timing the reference's own CUDA renderer on the same workload")
     p.add_argument("--no-mesh", action="store_true", help="skip the triangle-mesh (GGX, environment) measurement")
-    p.add_argument("--served", action="store_true", help="also measure the served request stream")
+    p.add_argument("--no-served", action="store_true", help="skip the served request stream's measurement")
     p.add_argument("--served-rate", type=float, default=200.0)
     p.add_argument("--served-window", type=float, default=0.25, help="seconds of arrivals (a bounded sample)")
-    p.add_argument("--served-step", type=float, default=0.02, help="GPU seconds a server step aims at")
+    p.add_argument("--served-step", type=float, default=0.01, help="GPU seconds a server step aims at")
     p.add_argument("--served-limit", type=float, default=300.0, help="wall seconds after which serving stops")
     return p.parse_args()
 
@@ -602,7 +602,7 @@ def run_b200(args):
         batched = batched_measurement(rt, torch, rank, world)  # every rank: its share of the 64 jobs
         if rank == 0:
             line["batched"] = batched
-    if rank == 0 and args.served:
+    if rank == 0 and not args.no_served:
         line["served"] = served_measurement(rt, torch, args)
 
     if rank == 0 and not args.no_cpu_baseline:
