@@ -496,6 +496,7 @@ def run_b200(args):
     times = []
     rays0 = session.counters()
     launches = 0
+    kernel_launches = 0
     kernel_seconds = 0.0
     total_rays = 0
     total_shadow = 0
@@ -515,6 +516,7 @@ def run_b200(args):
         total_shadow += cnt["shadow_rays"]
         kernel_seconds += report["gpu_seconds"]
         launches += report["launches"]
+        kernel_launches += report["kernel_launches"]
     clock_info = clocks.stop()
     del rays0
     # the slowest rank's time, every rank's segments (no collective on the data path: each rank's image is its own)
@@ -540,7 +542,7 @@ def run_b200(args):
                 "warmup": args.warmup, "ms_per_step": 1000 * step_seconds / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": workload_config(args, scene_desc), "roofline": roofline, "clocks": clock_info,
-                "gpu_launches": 2 * launches,
+                "gpu_launches": kernel_launches,
                 "segments_per_sample": total_rays / (args.steps * passes * scene.width * scene.height),
                 "shadow_rays_per_sample": total_shadow / (args.steps * passes * scene.width * scene.height),
                 "kernel": session.kernel(), "scene_stats": stats}

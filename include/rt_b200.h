@@ -223,7 +223,7 @@ typedef struct rt_render_result
     uint64_t shadow_rays;       /* NEE shadow queries, counted apart */
     int64_t passes;
     int32_t launches;
-    int32_t pad0;
+    int32_t kernel_launches;    /* as rt_render_report's */
     rt_kernel_info kernel;
 } rt_render_result;
 
@@ -265,7 +265,8 @@ typedef struct rt_render_report
 {
     rt_accumulation state;
     int32_t launches;
-    int32_t pad0;
+    int32_t kernel_launches;    /* GPU kernels the call launched: a persistent launch's render and reduction, a
+                                   wavefront launch's shade and trace per step and its reduction (no counterpart) */
     double gpu_seconds;
     double longest_launch_seconds;
 } rt_render_report;

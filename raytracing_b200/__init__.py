@@ -298,14 +298,14 @@ class Session:
     def render_to(self, passes: int) -> dict:
         r = _abi.RenderReport()
         _check(_lib().rt_session_render_to(self._handle, passes, C.byref(r)))
-        return {"passes": r.state.passes, "launches": r.launches, "gpu_seconds": r.gpu_seconds,
-                "longest_launch_seconds": r.longest_launch_seconds}
+        return {"passes": r.state.passes, "launches": r.launches, "kernel_launches": r.kernel_launches,
+                "gpu_seconds": r.gpu_seconds, "longest_launch_seconds": r.longest_launch_seconds}
 
     def render_for(self, seconds: float, pass_limit: int) -> dict:
         r = _abi.RenderReport()
         _check(_lib().rt_session_render_for(self._handle, seconds, pass_limit, C.byref(r)))
-        return {"passes": r.state.passes, "launches": r.launches, "gpu_seconds": r.gpu_seconds,
-                "longest_launch_seconds": r.longest_launch_seconds}
+        return {"passes": r.state.passes, "launches": r.launches, "kernel_launches": r.kernel_launches,
+                "gpu_seconds": r.gpu_seconds, "longest_launch_seconds": r.longest_launch_seconds}
 
     def pixels(self, out: Optional[np.ndarray] = None) -> np.ndarray:
         px = out if out is not None else np.empty((self.height, self.width, 3), dtype=np.float64)

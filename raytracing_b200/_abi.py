@@ -112,8 +112,8 @@ class KernelInfo(C.Structure):
 
 class RenderResult(C.Structure):
     _fields_ = [("seconds", C.c_double), ("kernel_seconds", C.c_double), ("rays", C.c_uint64),
-                ("shadow_rays", C.c_uint64), ("passes", C.c_int64), ("launches", C.c_int32), ("pad0", C.c_int32),
-                ("kernel", KernelInfo)]
+                ("shadow_rays", C.c_uint64), ("passes", C.c_int64), ("launches", C.c_int32),
+                ("kernel_launches", C.c_int32), ("kernel", KernelInfo)]
 
 
 class DeviceInfo(C.Structure):
@@ -133,7 +133,7 @@ class Accumulation(C.Structure):
 
 
 class RenderReport(C.Structure):
-    _fields_ = [("state", Accumulation), ("launches", C.c_int32), ("pad0", C.c_int32),
+    _fields_ = [("state", Accumulation), ("launches", C.c_int32), ("kernel_launches", C.c_int32),
                 ("gpu_seconds", C.c_double), ("longest_launch_seconds", C.c_double)]
 
 

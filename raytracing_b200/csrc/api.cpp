@@ -319,6 +319,7 @@ rt_status rt_render(const rt_scene_desc* scene, const rt_render_options* options
             result->shadow_rays = s.shadow_rays();
             result->passes = passes;
             result->launches = report.launches;
+            result->kernel_launches = report.kernel_launches;
             result->kernel = s.kernel();
             result->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
         }

@@ -61,7 +61,8 @@ batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
 
 batch_engine::~batch_engine()
 {
-    jobs_.clear(); // their arrays are freed on the stream, before it goes
+    jobs_.clear(); // their arrays (and the wavefront's) are freed on the stream, before it goes
+    wave_.reset();
     release_graph();
     if (table_host_)
     {
@@ -319,7 +320,7 @@ double batch_engine::step(std::vector<assignment> work)
             group_depth[g] = std::max(group_depth[g], b.cam.max_depth);
         }
     }
-    wave_->setup(std::max(group_samples[wave_batch_group(false)], group_samples[wave_batch_group(true)]));
+    wave_->setup(std::max(group_samples[wave_batch_group(false)], group_samples[wave_batch_group(true)]), stream_);
     check(cudaEventRecord(start_, stream_), "recording a CUDA event");
     if (use_graph_)
     {
@@ -358,7 +359,7 @@ double batch_engine::step(std::vector<assignment> work)
         {
             wide = wide && table_host_[i].scene.wide_nodes != nullptr;
         }
-        const wave_buffers b = wave_->setup(group_samples[g]);
+        const wave_buffers b = wave_->setup(group_samples[g], stream_);
         const int64_t steps = wave_->run(b, group_depth[g], stream_, [&] {
             return launch_wave_batch_step(w, features, wide, b, trace_grid_, stream_);
         });
@@ -390,7 +391,7 @@ void batch_engine::reserve_pool(size_t bytes)
 
 void batch_engine::reserve_wavefront(int64_t samples)
 {
-    wave_->setup(samples);
+    wave_->setup(samples, stream_);
     check(preload_wave_batch(), "loading the wavefront's kernels");
 }
 

@@ -184,12 +184,14 @@ environment_tables build_environment(const rt_environment_desc& env);
 class wave_runner
 {
 public:
-    explicit wave_runner(int max_slots_, int group_) : max_slots(max_slots_), group(group_) {}
+    wave_runner(int max_slots_, int group_);
     ~wave_runner();
     wave_runner(const wave_runner&) = delete;
     wave_runner& operator=(const wave_runner&) = delete;
 
-    wave_buffers setup(int64_t samples);
+    // Buffers from the device's memory pool, stream-ordered on `stream` (which must outlive the runner): a one-shot
+    // render that needs them takes them from what earlier renders left in the pool
+    wave_buffers setup(int64_t samples, cudaStream_t stream);
     // step() enqueues one step on `stream`; returns the steps run
     int64_t run(const wave_buffers& b, int max_depth, cudaStream_t stream, const std::function<cudaError_t()>& step);
 
@@ -268,6 +270,7 @@ private:
     // The wavefront form (RT_FORM_WAVEFRONT, or AUTO on a tree-searched scene)
     bool wavefront_ = false;
     std::unique_ptr<wave_runner> wave_;
+    int32_t last_kernel_launches_ = 0; // the last launch's kernels
     int trace_grid_ = 0;
 
     // Renders passes [passes_, end) in one launch and its reduction; returns its GPU seconds

@@ -2880,6 +2880,96 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
     }
 }
 
+// A flat-searched scene's query in the wavefront: every sphere, then every quad, in order (the persistent kernel's
+// flat search, the same tests and self-intersection rules); `any` (a shadow ray) stops at the first hit
+template <bool FEATURES>
+__device__ __forceinline__ void flat_search(const scene_view& S, float3 o, float3 d, float time, int from, bool inward,
+                                            int skip, bool any, hit_info& hit)
+{
+    const float inverse_a = 1.0f / length_squared(d);
+    for (int i = 0; i < S.quad_base; ++i)
+    {
+        const bool own = i == from;
+        if ((own && !inward) || i == skip)
+        {
+            continue;
+        }
+        const float4 s = sphere_at<FEATURES>(S, i, time);
+        float t;
+        bool entering;
+        if (hit_sphere(s, o, d, inverse_a, t_min, hit.t, own, t, entering))
+        {
+            hit = {i, t, entering};
+            if (any)
+            {
+                return;
+            }
+        }
+    }
+    const int quads = S.triangle_base - S.quad_base;
+    for (int i = 0; i < quads; ++i)
+    {
+        const int id = S.quad_base + i;
+        if (id == from || id == skip)
+        {
+            continue;
+        }
+        float t;
+        bool front;
+        if (hit_quad(load_quad(S.quads, i), o, d, t_min, hit.t, t, front))
+        {
+            hit = {id, t, front};
+            if (any)
+            {
+                return;
+            }
+        }
+    }
+}
+
+// The queued queries of a flat-searched scene: one query per thread at a time (grid-stride), every lane the same
+// loop over the same records, no tree, no stack, no refill
+template <bool FEATURES>
+__global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
+    wave_flat_trace_kernel(const __grid_constant__ scene_view S, const __grid_constant__ wave_buffers B,
+                           unsigned long long* counters)
+{
+    __shared__ unsigned block_walks[2];
+    if (threadIdx.x < 2)
+    {
+        block_walks[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    const unsigned count = B.control[0];
+    unsigned walks[2] = {0, 0};
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += gridDim.x * blockDim.x)
+    {
+        const float4 qo = stream_load(B.query_o + q);
+        const float4 qd = stream_load(B.query_d + q);
+        const int4 qm = stream_load(B.query_meta + q);
+        const bool shadow = (qm.y & 2) != 0;
+        hit_info hit{-1, qd.w, false};
+        flat_search<FEATURES>(S, make_float3(qo.x, qo.y, qo.z), make_float3(qd.x, qd.y, qd.z), qo.w, qm.x,
+                              (qm.y & 1) != 0, qm.z, shadow, hit);
+        if (shadow)
+        {
+            stream_store(B.shadow_result + qm.w, hit.id >= 0 ? 1 : 0);
+        }
+        else
+        {
+            stream_store(B.ext_result + qm.w, make_int4(hit.id, __float_as_int(hit.t), hit.front ? 1 : 0, 0));
+        }
+        ++walks[shadow ? 1 : 0];
+    }
+    atomicAdd(&block_walks[0], walks[0]);
+    atomicAdd(&block_walks[1], walks[1]);
+    __syncthreads();
+    if (counters != nullptr && threadIdx.x < 2 && block_walks[threadIdx.x] != 0u)
+    {
+        atomicAdd(counters + threadIdx.x, static_cast<unsigned long long>(block_walks[threadIdx.x]));
+    }
+}
+
 // The wavefront's samples into the image's sums: each chunk's samples added in pass order into its partial, the
 // partials in chunk order into the sums, as the persistent kernel's lanes and reduce_kernel add them
 __global__ void wave_reduce_kernel(const reduce_params R, const float4* samples, int64_t pass_begin, int64_t pass_end,
@@ -3141,8 +3231,16 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     {
         return e;
     }
-    wave_trace_of(features, p.scene.wide_nodes != nullptr)<<<trace_grid, render_block, 0, stream>>>(
-        p.scene, b, wave_batch{}, p.counters);
+    if (p.scene.flat != 0)
+    {
+        const auto flat = features ? wave_flat_trace_kernel<true> : wave_flat_trace_kernel<false>;
+        flat<<<trace_grid, render_block, 0, stream>>>(p.scene, b, p.counters);
+    }
+    else
+    {
+        wave_trace_of(features, p.scene.wide_nodes != nullptr)<<<trace_grid, render_block, 0, stream>>>(
+            p.scene, b, wave_batch{}, p.counters);
+    }
     return cudaGetLastError();
 }
 

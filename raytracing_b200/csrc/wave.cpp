@@ -7,6 +7,17 @@
 
 namespace rtb
 {
+wave_runner::wave_runner(int max_slots_, int group_) : max_slots(max_slots_), group(group_)
+{
+    // the device's pool keeps what is freed for the next allocation (a setting of this process's pool)
+    int device = 0;
+    check(cudaGetDevice(&device), "querying the device");
+    cudaMemPool_t pool = nullptr;
+    check(cudaDeviceGetDefaultMemPool(&pool, device), "querying the memory pool");
+    uint64_t keep = UINT64_MAX;
+    check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "setting the memory pool");
+}
+
 wave_runner::~wave_runner()
 {
     for (auto& e : done_)
@@ -22,7 +33,7 @@ wave_runner::~wave_runner()
     }
 }
 
-wave_buffers wave_runner::setup(int64_t samples)
+wave_buffers wave_runner::setup(int64_t samples, cudaStream_t stream)
 {
     if (!queued_)
     {
@@ -32,7 +43,7 @@ wave_buffers wave_runner::setup(int64_t samples)
         {
             check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating a CUDA event");
         }
-        control_.allocate(2);
+        control_.allocate_async(2, stream);
     }
     const int64_t wanted = (samples + render_block - 1) / render_block * render_block;
     const auto n = static_cast<size_t>(std::min<int64_t>(max_slots, std::max<int64_t>(wanted, render_block)));
@@ -40,16 +51,16 @@ wave_buffers wave_runner::setup(int64_t samples)
     if (ext_result_.size() < n)
     {
         const size_t c = std::min<size_t>(static_cast<size_t>(max_slots), std::max(n, 2 * ext_result_.size()));
-        slots_.allocate(c * wave_slot_bytes());
-        query_o_.allocate(2 * c);
-        query_d_.allocate(2 * c);
-        query_meta_.allocate(2 * c);
-        ext_result_.allocate(c);
-        shadow_result_.allocate(c);
+        slots_.allocate_async(c * wave_slot_bytes(), stream);
+        query_o_.allocate_async(2 * c, stream);
+        query_d_.allocate_async(2 * c, stream);
+        query_meta_.allocate_async(2 * c, stream);
+        ext_result_.allocate_async(c, stream);
+        shadow_result_.allocate_async(c, stream);
     }
     if (samples_.size() < static_cast<size_t>(samples))
     {
-        samples_.allocate(std::max(static_cast<size_t>(samples), 2 * samples_.size()));
+        samples_.allocate_async(std::max(static_cast<size_t>(samples), 2 * samples_.size()), stream);
     }
     wave_buffers b{};
     b.slots = slots_.data();

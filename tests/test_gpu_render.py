@@ -158,7 +158,7 @@ def test_env_furnace_is_exactly_one(rt):
     s = rt.builtin_scene("env-furnace", width=480, spp=64)
     r = rt.render(s, seed=5)
     assert np.all(r.pixels == 1.0), (r.pixels.min(), r.pixels.max())
-    assert r.kernel["name"] == "persistent nee-mis"
+    assert r.kernel["name"].endswith("nee-mis")
 
 
 def test_ggx_furnace_keeps_the_light(rt):

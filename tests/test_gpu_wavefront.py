@@ -2,14 +2,15 @@
 
 A session in the wavefront form renders the samples the persistent kernel renders: the same work items, the same
 random numbers, each sample's segments shaded by the same code in the same order, its shadow rays' light added before
-its next vertex, its passes added into the item's partial in pass order. The trace kernel's walk is the persistent
-kernel's traverse (node order, leaf tests, self-intersection rules), so the hits are the same. The two forms are
-compiled as different kernels, so the compiler's fused multiply-adds may round a few values differently.
+its next vertex, its passes added into the item's partial in pass order. The trace kernel's search is the persistent
+kernel's (the tree's leaf tests and self-intersection rules, four wide; or every primitive in turn for a flat scene),
+so the hits are the same. The two forms are compiled as different kernels, so the compiler's fused multiply-adds may
+round a few values differently.
 
 Covered: spheres in a tree (books and NEE/MIS), the triangle mesh with GGX and the environment map's shadow rays,
-the Cornell box's lamp shadow rays (its tree walked though the persistent kernel searches it flat), and the second
-book's textures, smoke (free flights, transmittance on shadow rays) and motion blur; more work items than slots (a slot
-renders several items in turn); many short launches; paths of one and two segments.
+the flat-searched Cornell boxes (books with the lights list, NEE/MIS with lamp shadow rays), and the second book's
+textures, smoke (free flights, transmittance on shadow rays) and motion blur; more samples than slots (a slot renders
+several samples in turn); many short launches; paths of one and two segments.
 """
 import numpy as np
 import pytest
@@ -34,6 +35,7 @@ CASES = [
     ("weekend", dict(width=48, spp=16, combination="mis"), 16),
     ("mesh-ggx", dict(width=64, spp=16, mesh_level=4, env_width=64), 16),
     ("cornell-mis", dict(width=48, spp=16), 16),
+    ("glass", dict(width=48, spp=16), 16),
     ("final", dict(width=64, spp=16), 16),
     ("smoke", dict(width=48, spp=16, combination="mis"), 16),
     ("bouncing", dict(width=48, spp=16), 16),
@@ -62,15 +64,21 @@ def test_wavefront_equals_persistent(rt, name, kw, passes):
     assert abs(ca["shadow_rays"] - cb["shadow_rays"]) <= 1e-3 * max(ca["shadow_rays"], 100), (ca, cb)
 
 
-def test_auto_form_follows_the_search(rt):
+def test_auto_form_follows_the_scene(rt):
+    # the wavefront for a tree (weekend) and for a flat scene with lights (the glass Cornell box); the persistent
+    # kernel for a bare flat scene (five quads under the sky)
     tree = rt.Session(rt.Scene(rt.builtin_scene("weekend", width=32, spp=1)), seed=1)
-    flat = rt.Session(rt.Scene(rt.builtin_scene("glass", width=32, spp=1)), seed=1)
+    lit = rt.Session(rt.Scene(rt.builtin_scene("glass", width=32, spp=1)), seed=1)
+    bare = rt.Session(rt.Scene(rt.builtin_scene("quads", width=32, spp=1)), seed=1)
     assert tree.kernel()["name"].startswith("wavefront")
-    assert flat.kernel()["name"].startswith("persistent")
+    assert lit.kernel()["name"].startswith("wavefront")
+    assert bare.kernel()["name"].startswith("persistent")
+    rep = lit.render_to(1)
+    assert rep["kernel_launches"] >= 3 and rep["kernel_launches"] % 2 == 1  # shade and trace per step, the reduction
 
 
 def test_more_items_than_slots(rt):
-    # 1024 x 576 pixels in one chunk: more work items than the ~450k slots, so slots take items in turn
+    # 1024 x 576 pixels, 16 passes: 9.4M samples for 2^20 slots, so slots take samples in turn
     a, b = _pair(rt, "weekend", dict(width=1024, spp=16), 16)
     _same_render(b.pixels(), a.pixels())
 

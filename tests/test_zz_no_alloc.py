@@ -33,8 +33,9 @@ def test_no_alloc_matches_session_on_two_calls_in_a_row(rt):
     camera = desc.camera
     seed = 77
 
-    # The existing entry point: a session rendered to 48, then 96 passes
-    session = rt.Session(scene, seed=seed)
+    # The existing entry point: a session rendered to 48, then 96 passes, in the persistent form (the no-allocation
+    # render runs the same persistent kernel; a session would take the wavefront for this scene by default)
+    session = rt.Session(scene, seed=seed, form="persistent")
     session.render_to(48)
     expected_48 = session.pixels().copy()
     session.render_to(96)
