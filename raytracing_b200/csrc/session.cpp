@@ -103,7 +103,10 @@ void session::set_camera(const rt_camera_desc& camera)
     padded_pixels_ = tiles_x_ * tiles_y * 32;
     max_partial_entries_ = static_cast<int64_t>(partial_budget_bytes / (3 * sizeof(double)));
     const size_t pixels = static_cast<size_t>(camera.image_width) * static_cast<size_t>(camera.image_height);
-    sums_.allocate(pixels * 3);
+    if (sums_.size() != pixels * 3)
+    {
+        sums_.allocate(pixels * 3); // a view of the same size keeps its sums' memory (cleared below)
+    }
     check(cudaMemsetAsync(sums_.data(), 0, sums_.bytes(), stream_), "clearing the sums");
     check(cudaMemsetAsync(counters_.data(), 0, counters_.bytes(), stream_), "clearing the counters");
     check(cudaStreamSynchronize(stream_), "clearing the sums");
