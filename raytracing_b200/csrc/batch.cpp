@@ -49,20 +49,16 @@ batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
     wave_ = std::make_unique<wave_runner>(wave_slots, wave_group);
     work_counter_.allocate(batch_groups);
     header_.allocate(1);
-    // The device's pool keeps what the jobs free for the next jobs (a process-wide setting of this process's pool)
-    int device = 0;
-    check(cudaGetDevice(&device), "querying the device");
-    cudaMemPool_t pool = nullptr;
-    check(cudaDeviceGetDefaultMemPool(&pool, device), "querying the memory pool");
-    uint64_t keep = UINT64_MAX;
-    check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "setting the memory pool");
+    retain_pool_memory(); // what the jobs free stays in the pool for the next jobs
     check(cudaMallocHost(reinterpret_cast<void**>(&header_host_), sizeof(batch_header)), "allocating pinned memory");
 }
 
 batch_engine::~batch_engine()
 {
-    jobs_.clear(); // their arrays (and the wavefront's) are freed on the stream, before it goes
+    jobs_.clear(); // their arrays (and the wavefront's, the arena and the table) are freed on the stream, before it goes
     wave_.reset();
+    arena_.release();
+    table_.release();
     release_graph();
     if (table_host_)
     {
@@ -163,7 +159,7 @@ void batch_engine::ensure_capacity(size_t jobs, size_t partial_doubles)
         {
             capacity *= 2;
         }
-        table_.allocate(capacity);
+        table_.allocate_async(capacity, stream_);
         if (table_host_)
         {
             cudaFreeHost(table_host_);
@@ -176,7 +172,7 @@ void batch_engine::ensure_capacity(size_t jobs, size_t partial_doubles)
     }
     if (partial_doubles > arena_.size())
     {
-        arena_.allocate(partial_doubles + partial_doubles / 4);
+        arena_.allocate_async(partial_doubles + partial_doubles / 4, stream_);
         moved = true;
     }
     if (moved)

@@ -179,6 +179,10 @@ struct environment_tables
 };
 environment_tables build_environment(const rt_environment_desc& env);
 
+// The device's memory pool keeps what is freed for the next stream-ordered allocation (a setting of this process's
+// pool): the scratch that comes and goes with renders, views and requests is mapped once, not on every allocation
+void retain_pool_memory();
+
 // The wavefront's host side: its buffers, sized to a launch's samples (slots: at most max_slots) and kept for the next,
 // and the loop of steps, in groups of `group` with two groups in flight, until a step queues no ray
 class wave_runner

@@ -35,6 +35,7 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
     }
     check(cudaSetDevice(scene_->device()), "selecting the scene's device");
     check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a CUDA stream");
+    retain_pool_memory(); // the sums and the launches' scratch come from the pool, stream-ordered
     check(cudaEventCreate(&start_), "creating a CUDA event");
     check(cudaEventCreate(&stop_), "creating a CUDA event");
     if (options_.form < RT_FORM_AUTO || options_.form > RT_FORM_WAVEFRONT)
@@ -105,7 +106,7 @@ void session::set_camera(const rt_camera_desc& camera)
     const size_t pixels = static_cast<size_t>(camera.image_width) * static_cast<size_t>(camera.image_height);
     if (sums_.size() != pixels * 3)
     {
-        sums_.allocate(pixels * 3); // a view of the same size keeps its sums' memory (cleared below)
+        sums_.allocate_async(pixels * 3, stream_); // a view of the same size keeps its sums' memory (cleared below)
     }
     check(cudaMemsetAsync(sums_.data(), 0, sums_.bytes(), stream_), "clearing the sums");
     check(cudaMemsetAsync(counters_.data(), 0, counters_.bytes(), stream_), "clearing the counters");
@@ -150,7 +151,7 @@ double session::launch(int64_t end)
     const size_t needed = static_cast<size_t>(chunks) * static_cast<size_t>(padded_pixels_) * 3;
     if (!wave && partials_.size() < needed)
     {
-        partials_.allocate(needed);
+        partials_.allocate_async(needed, stream_);
     }
     launch_params p{};
     p.scene = scene_->view();

@@ -7,9 +7,8 @@
 
 namespace rtb
 {
-wave_runner::wave_runner(int max_slots_, int group_) : max_slots(max_slots_), group(group_)
+void retain_pool_memory()
 {
-    // the device's pool keeps what is freed for the next allocation (a setting of this process's pool)
     int device = 0;
     check(cudaGetDevice(&device), "querying the device");
     cudaMemPool_t pool = nullptr;
@@ -17,6 +16,8 @@ wave_runner::wave_runner(int max_slots_, int group_) : max_slots(max_slots_), gr
     uint64_t keep = UINT64_MAX;
     check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "setting the memory pool");
 }
+
+wave_runner::wave_runner(int max_slots_, int group_) : max_slots(max_slots_), group(group_) { retain_pool_memory(); }
 
 wave_runner::~wave_runner()
 {
