@@ -135,8 +135,9 @@ def read_peaks() -> dict:
 
 
 def read_traffic() -> float | None:
-    """DRAM bytes per path segment of the render kernel, from the committed ncu summary (profiles/)."""
-    path = REPO / "profiles" / "render_kernel_glass.md"
+    """DRAM bytes per path segment of the workload's kernels (the wavefront's shade and trace kernels), from the
+    committed ncu summary (profiles/)."""
+    path = REPO / "profiles" / "wavefront_glass.md"
     if not path.exists():
         return None
     for line in path.read_text().splitlines():
@@ -533,8 +534,9 @@ def run_b200(args):
                 "peak_source": peaks["source"],
                 "algorithmic_bytes_per_segment": bytes_per_segment,
                 "note": "BVH node (64 B) and primitive (16/48 B) fetches per closest-hit or shadow query, counted on "
-                        "this workload's rays; they are served from L1/L2, not HBM, so the kernel is bound by "
-                        "traversal latency and FP32 issue, far below this ceiling"}
+                        "this workload's rays; they are served from L1/L2, not HBM. The DRAM traffic (`traffic`, "
+                        "per launch) is the wavefront's slot state and queues, about 237 B per segment; the kernels "
+                        "are bound by latency and divergent issue"}
 
     line = None
     if rank == 0:
