@@ -391,7 +391,8 @@ typedef struct rt_batch_report
     int32_t pad0;
 } rt_batch_report;
 
-/* Renders every job to its passes in batched steps (config 4's 64 jobs in one persistent launch per step). */
+/* Renders every job to its passes in batched steps (many jobs of any size and scene per step, one persistent launch
+   per group of them). */
 rt_status rt_batch_render(const rt_batch_job* jobs, int32_t count, const rt_batch_options* options,
                           rt_batch_report* report);
 
@@ -467,10 +468,10 @@ rt_status rt_scene_camera_rays(rt_scene* scene, uint64_t seed, int64_t pass, flo
 
 /* ---- built-in scenes (scenes.ixx:79-518, gpu_scenes*.ixx) ---------------------------------------------------- */
 
-/* A scene the library builds from its name, owning its tables. Names: "weekend" (cover, config 1), "cornell",
- * "glass" (config 2 geometry), "cornell-mis" (glass under NEE+MIS), "materials", "quads", "furnace" (every pixel
- * exactly 1: a closed white sky), "mesh-ggx" (config 3), "cover-N" (cover variant of about N random spheres, config
- * 4, with its own seed). width, spp, depth override the scene's camera when > 0; scene_seed picks the scene's random
+/* A scene the library builds from its name, owning its tables. Names: "weekend" (the first book's cover), "cornell",
+ * "glass" (the Cornell box with a glass ball), "cornell-mis" (glass under NEE+MIS), "materials", "quads", "furnace"
+ * (every pixel exactly 1: a closed white sky), "mesh-ggx" (the displaced 1.3M-triangle icosphere in GGX metal under an
+ * HDR sky), "cover-N" (a cover variant of about N random spheres, with its own seed). width, spp, depth override the scene's camera when > 0; scene_seed picks the scene's random
  * content (the CPU's scene generator, mt19937_64 seeded as scenes.ixx's main thread). */
 typedef struct rt_builtin_params
 {

@@ -379,7 +379,7 @@ struct quad
     }
 };
 
-// A triangle (the meshes of the configs; the reference traces them only through OptiX). Möller–Trumbore in double,
+// A triangle (the displaced icosphere's; the reference traces meshes only through OptiX). Möller–Trumbore in double,
 // closed barycentric bounds, outward normal e1 x e2 (counter-clockwise seen from the front).
 struct triangle
 {

@@ -1,6 +1,6 @@
 // Batched rendering and serving: the batch engine (a job table, a partials arena and a captured CUDA graph of the
-// step), rt_batch_render on top of it (config 4: many independent jobs in one persistent launch per step), and the
-// render server (config 5: a stream of requests admitted under an HBM budget, first frames before refinement).
+// step), rt_batch_render on top of it (many independent jobs in one persistent launch per group and step), and the
+// render server (a stream of requests admitted under an HBM budget, first frames before refinement).
 #include "batch.h"
 
 #include <algorithm>

@@ -98,7 +98,7 @@ private:
     void release_graph();
 };
 
-// The server of a stream of render requests (config 5 of the bench): requests are admitted under an HBM budget, every
+// The server of a stream of render requests: requests are admitted under an HBM budget, every
 // step gives the newly admitted their first frame (one pass) before it refines the others, and a request is done when
 // it reaches its target passes. Driven by the caller: submit between steps, step, poll, fetch.
 class render_server

@@ -186,8 +186,8 @@ def test_mesh_first_hits_match_oracle(rt, oracle):
 
 
 def test_mesh_ggx_image_matches_oracle(rt, oracle):
-    """Config 3 reduced: the displaced icosphere (level 4), GGX metal, glossy-coat plane, the sun-lit sky sampled
-    by its alias table, NEE with power-heuristic MIS."""
+    """The mesh workload reduced: the displaced icosphere (level 4), GGX metal, glossy-coat plane, the sun-lit sky
+    sampled by its alias table, NEE with power-heuristic MIS."""
     r, g, cstats = _compare_with_rerun(rt, oracle, "mesh-ggx", 64, [(11, 12), (13, 14)], width=128, spp=64,
                                        mesh_level=4, env_width=256)
     assert g.shadow_rays > 0

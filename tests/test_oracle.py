@@ -168,7 +168,7 @@ def test_ggx_energy_table_matches_reference(oracle):
     diff = np.abs(table - ref)
     assert diff.max() < 1e-3, diff.max()  # the reference's own quadrature vs its independent table: 9.2e-4
     assert diff.mean() < 3e-5, diff.mean()
-    # where config 3's rough metal (r = 0.3) reads it, tighter still
+    # where the mesh's rough metal (r = 0.3) reads it, tighter still
     assert np.abs(table[9:11, 4:] - ref[9:11, 4:]).max() < 1e-4
 
 
