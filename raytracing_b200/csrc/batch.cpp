@@ -46,7 +46,7 @@ batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
     kernel_attributes shade{}, trace{};
     check(wave_attributes(scene_view{}, false, shade, trace), "querying the wavefront kernels");
     trace_grid_ = trace.multiprocessors * std::max(1, trace.blocks_per_sm);
-    wave_ = std::make_unique<wave_runner>(wave_slots, wave_group);
+    wave_ = std::make_unique<wave_runner>(wave_slots_large, wave_group); // its groups are the large trees'
     work_counter_.allocate(batch_groups);
     header_.allocate(1);
     retain_pool_memory(); // what the jobs free stays in the pool for the next jobs

@@ -215,17 +215,29 @@ private:
     cudaEvent_t done_[2] = {nullptr, nullptr};
 };
 
-// The wavefront's slots (paths in flight: 2^20 take 160 MB, and their queries 96 MB; the trace kernel's throughput
-// grew with them up to here on the mesh, where a step's walks must outlast its slowest one) and its steps per group
-// between two looks at the queue's length
+// The wavefront's slots (paths in flight: 2^20 take 160 MB, and their queries 96 MB) and its steps per group between
+// two looks at the queue's length. Measured on the B200 from 2^18 to 2^21 slots: the mesh gains up to 1.5 x 2^20
+// (+11% over 2^20: a step's queries must outlast its slowest, longest walk) and so do the bare flat scenes (+3% on the
+// glass Cornell box), while the sphere trees and the textured scenes lose 5-7% past 2^20 (wave_slots_for)
 #ifndef RTB_WAVE_SLOTS
 #define RTB_WAVE_SLOTS (1 << 20)
+#endif
+#ifndef RTB_WAVE_SLOTS_LARGE
+#define RTB_WAVE_SLOTS_LARGE (3 << 19)
 #endif
 #ifndef RTB_WAVE_GROUP
 #define RTB_WAVE_GROUP 8
 #endif
 constexpr int wave_slots = RTB_WAVE_SLOTS / render_block * render_block;
+constexpr int wave_slots_large = RTB_WAVE_SLOTS_LARGE / render_block * render_block;
 constexpr int wave_group = RTB_WAVE_GROUP;
+// The pool for a scene: the larger one for a scene with triangles, or a flat-searched one without textures, motion
+// or smoke
+inline int wave_slots_for(const scene_view& v)
+{
+    const bool triangles = v.prim_count > v.triangle_base;
+    return triangles || (v.flat != 0 && !has_features(v)) ? wave_slots_large : wave_slots;
+}
 
 // One view of a resident scene whose image gains passes on demand (renderer.h:591-673)
 class session

@@ -58,7 +58,7 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
         kernel_attributes shade{}, trace{};
         check(wave_attributes(view, scene_->quality(), shade, trace), "querying the wavefront kernels");
         trace_grid_ = trace.multiprocessors * std::max(1, trace.blocks_per_sm);
-        wave_ = std::make_unique<wave_runner>(wave_slots, wave_group);
+        wave_ = std::make_unique<wave_runner>(wave_slots_for(view), wave_group);
     }
     counters_.allocate(7);
     set_camera(scene_->camera());
