@@ -2332,7 +2332,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         sampler rng;
         shadow_query sq;
         int64_t sample_index = 0, pass = 0;
-        int px = r5.z & 0xffff, py = r5.z >> 16;
+        int px = 0, py = 0; // the pixel of a sample claimed in this step (a slot's camera ray needs no more)
         bool need = false;
         bool start = false;
         rng.job = BATCH ? J->job : P.job;
@@ -2588,7 +2588,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                 stream_store(reinterpret_cast<int4*>(rows) + 4 * n + i,
                              make_int4(static_cast<int>(rng.pixel), static_cast<int>(rng.pass), ps.from, ps.rays_left));
                 stream_store(reinterpret_cast<int4*>(rows) + 5 * n + i,
-                             make_int4(ps.depth, static_cast<int>(flags), px | (py << 16), job));
+                             make_int4(ps.depth, static_cast<int>(flags), 0, job));
                 stream_store(reinterpret_cast<longlong2*>(rows) + 6 * n + i, make_longlong2(sample_index, pass));
             }
         }
