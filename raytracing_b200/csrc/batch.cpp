@@ -18,13 +18,8 @@ namespace rtb
 namespace
 {
 constexpr size_t default_partial_budget = size_t{1} << 30;
-// A tree-searched scene of at least this many nodes renders in the wavefront form: on the mesh (768k nodes) its walks
-// are long and diverge, and the wavefront renders it 2.5 times as fast; on the cover scenes (50 to 2000 spheres) the
-// persistent kernel is as fast and needs no queues
-#ifndef RTB_WAVE_MIN_NODES
-#define RTB_WAVE_MIN_NODES 16384
-#endif
-constexpr int wave_min_nodes = RTB_WAVE_MIN_NODES;
+// A step of at most this many samples in the wavefront form (a server's step: about 10 ms) is a short step
+constexpr int64_t short_step_samples = int64_t{12} << 20;
 } // namespace
 
 // ---- the batch engine ---------------------------------------------------------------------------------------
@@ -46,7 +41,7 @@ batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
     kernel_attributes shade{}, trace{};
     check(wave_attributes(scene_view{}, false, shade, trace), "querying the wavefront kernels");
     trace_grid_ = trace.multiprocessors * std::max(1, trace.blocks_per_sm);
-    wave_ = std::make_unique<wave_runner>(wave_slots_large, wave_group); // its groups are the large trees'
+    wave_ = std::make_unique<wave_runner>(wave_slots_mesh, wave_group); // the wavefront groups' slots, in turn
     work_counter_.allocate(batch_groups);
     header_.allocate(1);
     retain_pool_memory(); // what the jobs free stays in the pool for the next jobs
@@ -244,11 +239,32 @@ double batch_engine::step(std::vector<assignment> work)
         return 0;
     }
     ensure_capacity(work.size(), static_cast<size_t>(entries) * 3);
+    // A short step (a server's) keeps its wavefront runs to one: every run ends with a drain (its last paths finishing
+    // while most slots idle, a path's length of steps), so the tree-searched jobs share one group (the kernels with
+    // the second book's features render the scenes without them) and the flat-searched ones take the persistent
+    // kernel, whose tail overlaps nothing either but is shorter. Measured on the 10 ms steps of the served stream: 2%
+    // above the flat scenes in a wavefront group of their own, whose second drain costs more than its walks save.
+    int64_t wave_samples = 0;
+    bool tree_features = false;
+    for (const assignment& a : work)
+    {
+        const job& j = *jobs_.at(a.handle);
+        const scene_view& v = j.scene->view();
+        if (wavefront_suits(v))
+        {
+            wave_samples += (a.pass_end - j.passes) * int64_t{j.padded};
+            tree_features = tree_features || (v.flat == 0 && has_features(v));
+        }
+    }
+    const bool short_step = wave_samples <= short_step_samples;
     // The jobs in their groups' order (each group's items form its own launch)
     const auto group_of = [&](const assignment& a) {
         const scene_view& v = jobs_.at(a.handle)->scene->view();
-        return v.flat == 0 && v.node_count >= wave_min_nodes ? wave_batch_group(has_features(v))
-                                                             : batch_group(v.flat != 0, has_features(v));
+        if (!wavefront_suits(v) || (short_step && v.flat != 0))
+        {
+            return batch_group(v.flat != 0, has_features(v));
+        }
+        return short_step ? wave_batch_group(false, tree_features) : wave_batch_group(v.flat != 0, has_features(v));
     };
     std::stable_sort(work.begin(), work.end(),
                      [&](const assignment& a, const assignment& b) { return group_of(a) < group_of(b); });
@@ -302,8 +318,8 @@ double batch_engine::step(std::vector<assignment> work)
     }
     header.total_pixels = pixels;
     header.job_count = static_cast<int32_t>(work.size());
-    // The tree groups' samples, numbered job after job within each group, and the wavefront's buffers for the largest
-    // (allocated before the timing starts)
+    // The wavefront groups' samples, numbered job after job within each group, and the wavefront's buffers for the
+    // largest (allocated before the timing starts)
     int64_t group_samples[batch_groups] = {};
     int group_depth[batch_groups] = {};
     for (int g = persistent_groups; g < batch_groups; ++g)
@@ -316,7 +332,7 @@ double batch_engine::step(std::vector<assignment> work)
             group_depth[g] = std::max(group_depth[g], b.cam.max_depth);
         }
     }
-    wave_->setup(std::max(group_samples[wave_batch_group(false)], group_samples[wave_batch_group(true)]), stream_);
+    wave_->setup(*std::max_element(group_samples, group_samples + batch_groups), stream_);
     check(cudaEventRecord(start_, stream_), "recording a CUDA event");
     if (use_graph_)
     {
@@ -349,7 +365,8 @@ double batch_engine::step(std::vector<assignment> work)
         // the group's samples claimed through its own work counter, zeroed with the others at the step's start
         const wave_batch w{table_.data(),          header.group_jobs[g],      header.group_jobs[g + 1],
                            header.group_items[g], header.group_items[g + 1], work_counter_.data() + g};
-        const bool features = g == wave_batch_group(true);
+        const bool flat = g == wave_batch_group(true, false) || g == wave_batch_group(true, true);
+        const bool features = g == wave_batch_group(flat, true);
         bool wide = true;
         for (int32_t i = header.group_jobs[g]; i < header.group_jobs[g + 1]; ++i)
         {
@@ -357,7 +374,7 @@ double batch_engine::step(std::vector<assignment> work)
         }
         const wave_buffers b = wave_->setup(group_samples[g], stream_);
         const int64_t steps = wave_->run(b, group_depth[g], stream_, [&] {
-            return launch_wave_batch_step(w, features, wide, b, trace_grid_, stream_);
+            return launch_wave_batch_step(w, flat, features, wide, b, trace_grid_, stream_);
         });
         check(launch_wave_batch_partials(w, b, stream_), "launching the wavefront's partials");
         launches_ += static_cast<int>(2 * steps + 1);

@@ -79,7 +79,7 @@ private:
     cudaEvent_t start_ = nullptr;
     cudaEvent_t stop_ = nullptr;
     int grids_[persistent_groups] = {}; // each persistent group's launch (batch_group)
-    std::unique_ptr<wave_runner> wave_;  // the large trees' groups (wave_batch_group)
+    std::unique_ptr<wave_runner> wave_;  // the wavefront's groups (wave_batch_group), one after another
     int trace_grid_ = 0;
     device_array<double> arena_;
     device_array<batch_job> table_;

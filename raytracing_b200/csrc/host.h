@@ -216,27 +216,37 @@ private:
 };
 
 // The wavefront's slots (paths in flight: 2^20 take 160 MB, and their queries 96 MB) and its steps per group between
-// two looks at the queue's length. Measured on the B200 from 2^18 to 2^21 slots: the mesh gains up to 1.5 x 2^20
-// (+11% over 2^20: a step's queries must outlast its slowest, longest walk) and so do the bare flat scenes (+3% on the
-// glass Cornell box), while the sphere trees and the textured scenes lose 5-7% past 2^20 (wave_slots_for)
+// two looks at the queue's length. Measured on the B200 from 2^18 to 3 x 2^20 slots: the mesh gains up to 3 x 2^20
+// (+11% from 2^20 to 1.5 x 2^20, +7.5% more to 3 x 2^20: a step's queries must outlast its slowest, longest walk), the
+// bare flat scenes up to 1.5 x 2^20 (+3% on the glass Cornell box; the lamp-lit one loses 6% at 3 x 2^20), while the
+// sphere trees and the textured scenes lose 5-7% past 2^20 (wave_slots_for). The batch engine's pool is the mesh's
+// (its 64-job batch of sphere trees: +3.5% from 1.5 x 2^20 to 3 x 2^20).
 #ifndef RTB_WAVE_SLOTS
 #define RTB_WAVE_SLOTS (1 << 20)
 #endif
 #ifndef RTB_WAVE_SLOTS_LARGE
 #define RTB_WAVE_SLOTS_LARGE (3 << 19)
 #endif
+#ifndef RTB_WAVE_SLOTS_MESH
+#define RTB_WAVE_SLOTS_MESH (3 << 20)
+#endif
 #ifndef RTB_WAVE_GROUP
 #define RTB_WAVE_GROUP 8
 #endif
 constexpr int wave_slots = RTB_WAVE_SLOTS / render_block * render_block;
 constexpr int wave_slots_large = RTB_WAVE_SLOTS_LARGE / render_block * render_block;
+constexpr int wave_slots_mesh = RTB_WAVE_SLOTS_MESH / render_block * render_block;
 constexpr int wave_group = RTB_WAVE_GROUP;
-// The pool for a scene: the larger one for a scene with triangles, or a flat-searched one without textures, motion
-// or smoke
+// The pool for a scene: the largest for a scene with triangles, the larger one for a flat-searched one without
+// textures, motion or smoke
 inline int wave_slots_for(const scene_view& v)
 {
     const bool triangles = v.prim_count > v.triangle_base;
-    return triangles || (v.flat != 0 && !has_features(v)) ? wave_slots_large : wave_slots;
+    if (triangles)
+    {
+        return wave_slots_mesh;
+    }
+    return v.flat != 0 && !has_features(v) ? wave_slots_large : wave_slots;
 }
 
 // One view of a resident scene whose image gains passes on demand (renderer.h:591-673)

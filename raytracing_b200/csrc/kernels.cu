@@ -2235,6 +2235,7 @@ constexpr uint32_t wave_finish = 8u;    // the sample ended at the shadow ray's 
 // each row slot_count long, so that a warp's loads and stores of a row are 512 contiguous bytes
 constexpr int wave_rows = 7;
 constexpr int wave_shadow_rows = 3;
+constexpr int wave_flags_row = 5; // depth, flags, unused, job: a slot whose row is zero has no sample
 constexpr uint32_t wave_specular = 1u << 8;
 constexpr uint32_t wave_inward = 1u << 9;
 
@@ -2288,7 +2289,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     const unsigned lanes_below = (1u << lane) - 1u;
     float4* rows = static_cast<float4*>(B.slots);
     float4* shadow_rows = rows + static_cast<int64_t>(wave_rows) * n;
-    const int4 r5 = stream_load(reinterpret_cast<const int4*>(rows) + 5 * n + i);
+    const int4 r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + i);
     uint32_t flags = static_cast<uint32_t>(r5.y);
     uint32_t shadow_rays = 0; // counted where the walks are (the trace kernel), or as queued (BATCH)
     // a warp whose slots have all run out of work has nothing left to do in this launch
@@ -2575,7 +2576,8 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                     (ps.inward ? wave_inward : 0u);
             if (flags & wave_exhausted)
             {
-                stream_store(reinterpret_cast<int4*>(rows) + 5 * n + i, make_int4(0, static_cast<int>(flags), 0, 0));
+                stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
+                             make_int4(0, static_cast<int>(flags), 0, 0));
             }
             else
             {
@@ -2587,7 +2589,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                                                            __uint_as_float(rng.key.y)));
                 stream_store(reinterpret_cast<int4*>(rows) + 4 * n + i,
                              make_int4(static_cast<int>(rng.pixel), static_cast<int>(rng.pass), ps.from, ps.rays_left));
-                stream_store(reinterpret_cast<int4*>(rows) + 5 * n + i,
+                stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
                              make_int4(ps.depth, static_cast<int>(flags), 0, job));
                 stream_store(reinterpret_cast<longlong2*>(rows) + 6 * n + i, make_longlong2(sample_index, pass));
             }
@@ -2928,11 +2930,12 @@ __device__ __forceinline__ void flat_search(const scene_view& S, float3 o, float
 }
 
 // The queued queries of a flat-searched scene: one query per thread at a time (grid-stride), every lane the same
-// loop over the same records, no tree, no stack, no refill
-template <bool FEATURES>
+// loop over the same records, no tree, no stack, no refill. BATCH: each query searches its job's scene (W's table; a
+// warp's lanes may loop over different scenes), its walks counted where the shade kernel queued it.
+template <bool FEATURES, bool BATCH>
 __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
     wave_flat_trace_kernel(const __grid_constant__ scene_view S, const __grid_constant__ wave_buffers B,
-                           unsigned long long* counters)
+                           const __grid_constant__ wave_batch W, unsigned long long* counters)
 {
     __shared__ unsigned block_walks[2];
     if (threadIdx.x < 2)
@@ -2949,7 +2952,12 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
         const int4 qm = stream_load(B.query_meta + q);
         const bool shadow = (qm.y & 2) != 0;
         hit_info hit{-1, qd.w, false};
-        flat_search<FEATURES>(S, make_float3(qo.x, qo.y, qo.z), make_float3(qd.x, qd.y, qd.z), qo.w, qm.x,
+        const scene_view* scene = &S;
+        if constexpr (BATCH)
+        {
+            scene = &W.jobs[qm.y >> 2].scene;
+        }
+        flat_search<FEATURES>(*scene, make_float3(qo.x, qo.y, qo.z), make_float3(qd.x, qd.y, qd.z), qo.w, qm.x,
                               (qm.y & 1) != 0, qm.z, shadow, hit);
         if (shadow)
         {
@@ -3189,6 +3197,13 @@ cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const
 
 size_t wave_slot_bytes() { return (wave_rows + wave_shadow_rows) * sizeof(float4); }
 
+cudaError_t clear_wave_slots(const wave_buffers& b, cudaStream_t stream)
+{
+    // the other rows are written when a slot's first sample starts
+    return cudaMemsetAsync(static_cast<float4*>(b.slots) + int64_t{wave_flags_row} * b.slot_count, 0,
+                           static_cast<size_t>(b.slot_count) * sizeof(float4), stream);
+}
+
 namespace
 {
 using wave_shade_function = void (*)(launch_params, wave_buffers, wave_batch);
@@ -3214,6 +3229,12 @@ wave_shade_function wave_shade_of(bool quality, bool features)
 }
 
 wave_trace_function wave_trace_of(bool features, bool wide) { return wave_trace_variant<false>(features, wide); }
+
+template <bool BATCH>
+wave_trace_function wave_flat_trace_of(bool features)
+{
+    return features ? wave_flat_trace_kernel<true, BATCH> : wave_flat_trace_kernel<false, BATCH>;
+}
 } // namespace
 
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
@@ -3233,8 +3254,8 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     }
     if (p.scene.flat != 0)
     {
-        const auto flat = features ? wave_flat_trace_kernel<true> : wave_flat_trace_kernel<false>;
-        flat<<<trace_grid, render_block, 0, stream>>>(p.scene, b, p.counters);
+        wave_flat_trace_of<false>(features)<<<trace_grid, render_block, 0, stream>>>(p.scene, b, wave_batch{},
+                                                                                     p.counters);
     }
     else
     {
@@ -3244,7 +3265,7 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     return cudaGetLastError();
 }
 
-cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, bool wide, const wave_buffers& b,
+cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, const wave_buffers& b,
                                    int trace_grid, cudaStream_t stream)
 {
     cudaError_t e = cudaMemsetAsync(b.control, 0, 2 * sizeof(unsigned), stream);
@@ -3260,7 +3281,8 @@ cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, bool wide
     {
         return e;
     }
-    wave_trace_variant<true>(features, wide)<<<trace_grid, render_block, 0, stream>>>(scene_view{}, b, w, nullptr);
+    const wave_trace_function trace = flat ? wave_flat_trace_of<true>(features) : wave_trace_variant<true>(features, wide);
+    trace<<<trace_grid, render_block, 0, stream>>>(scene_view{}, b, w, nullptr);
     return cudaGetLastError();
 }
 
@@ -3273,6 +3295,8 @@ cudaError_t preload_wave_batch()
                              reinterpret_cast<const void*>(wave_trace_variant<true>(false, true)),
                              reinterpret_cast<const void*>(wave_trace_variant<true>(true, false)),
                              reinterpret_cast<const void*>(wave_trace_variant<true>(true, true)),
+                             reinterpret_cast<const void*>(wave_flat_trace_of<true>(false)),
+                             reinterpret_cast<const void*>(wave_flat_trace_of<true>(true)),
                              reinterpret_cast<const void*>(wave_batch_partials_kernel)};
     for (const void* k : kernels)
     {
@@ -3313,6 +3337,7 @@ cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attrib
     {
         return e;
     }
+    // the walk's kernel sizes the trace grid of either search (the flat one is launched with the same grid)
     return attributes_of(wave_trace_of(features, scene.wide_nodes != nullptr), trace);
 }
 

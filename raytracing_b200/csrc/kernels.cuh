@@ -78,14 +78,26 @@ struct alignas(16) batch_job
 // its kernels are compiled with their code, the others without
 inline bool has_features(const scene_view& s) { return s.has_motion != 0 || s.has_textures != 0 || s.medium_count > 0; }
 
-// The jobs come in six groups. Four are rendered each by its own launch of the persistent kernel compiled for it:
-// flat scenes without the second book's features, flat scenes with them, then the same two of tree scenes
-// (batch_group). The last two, the scenes of large trees without and with the features (wave_batch_group), are
-// rendered in the wavefront form, whose walks pay for their queues only where the walks are long.
+// Whether a scene renders in the wavefront form unless a form is asked for: every tree-searched scene (its walks
+// diverge: the mesh 3.2 times and the sphere scenes 1.2-2 times as fast as in the persistent kernel) and a
+// flat-searched scene whose shading is heavy (lights or lamps, the second book's features, an environment: the glass
+// Cornell box 10-16% faster, the marble spheres 55%); the bare small flat scenes (five spheres or five quads under
+// the sky), whose paths are one or two cheap segments that cannot pay for the slots' traffic, stay in the persistent
+// kernel (40% slower in the wavefront).
+inline bool wavefront_suits(const scene_view& v)
+{
+    const bool heavy = v.light_count > 0 || v.lamp_count > 0 || has_features(v) || v.has_environment;
+    return v.node_count > 0 && (v.flat == 0 || heavy);
+}
+
+// The jobs come in eight groups: the scenes of each search (flat, tree) without and with the second book's features,
+// in each form. The first four are rendered each by its own launch of the persistent kernel compiled for it
+// (batch_group), the other four each by its own run of the wavefront's steps (wave_batch_group); a scene takes the
+// form wavefront_suits gives it, as a session's render of it does.
 constexpr int persistent_groups = 4;
-constexpr int batch_groups = 6;
+constexpr int batch_groups = 8;
 RTB_HD constexpr int batch_group(bool flat, bool features) { return (flat ? 0 : 2) + (features ? 1 : 0); }
-RTB_HD constexpr int wave_batch_group(bool features) { return persistent_groups + (features ? 1 : 0); }
+RTB_HD constexpr int wave_batch_group(bool flat, bool features) { return persistent_groups + batch_group(flat, features); }
 
 struct batch_header
 {
@@ -146,7 +158,7 @@ cudaError_t render_attributes(const scene_view& scene, bool quality, kernel_attr
 // reduction adds the samples into the sums chunk by chunk, in pass order.
 struct wave_buffers
 {
-    void* slots;            // slot_count slots of wave_slot_bytes() each, zeroed before a launch
+    void* slots;            // slot_count slots of wave_slot_bytes() each, cleared before a launch
     int32_t slot_count;     // a multiple of render_block
     float4* samples;        // sample_count: (pass - pass_begin) * padded_pixels + tile slot -> the sample's value
     int64_t sample_count;   // (pass_end - pass_begin) * padded_pixels
@@ -158,16 +170,18 @@ struct wave_buffers
     unsigned* control;      // [0] queries the last shade step queued, [1] queries the trace kernel took
 };
 size_t wave_slot_bytes();
+// Every slot without a sample (its flags row zeroed), before a launch's first step
+cudaError_t clear_wave_slots(const wave_buffers& b, cudaStream_t stream);
 // One step: clears the queue, the shade kernel over the slots, the trace kernel (trace_grid blocks) over the queue
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
                              cudaStream_t stream);
 // The samples of passes [pass_begin, pass_end) into the sums (chunk partials in pass order, added in chunk order)
 cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
                                int32_t chunk, cudaStream_t stream);
-// The same for a group of batch jobs (features: the group's kernels compile the second book's features; wide: every
-// job's scene has its tree four wide), and the group's samples into its jobs' chunk partials (then the batch's
-// reduction adds them into the sums)
-cudaError_t launch_wave_batch_step(const wave_batch& w, bool features, bool wide, const wave_buffers& b,
+// The same for a group of batch jobs (flat: the group's scenes are searched flat; features: its kernels compile the
+// second book's features; wide: every job's tree is four wide), and the group's samples into its jobs' chunk
+// partials (then the batch's reduction adds them into the sums)
+cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, const wave_buffers& b,
                                    int trace_grid, cudaStream_t stream);
 cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream);
 // Loads the batch wavefront's kernels (every variant) now, so that no step pays for loading them

@@ -46,13 +46,7 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
     check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
     grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
     const scene_view& view = scene_->view();
-    // AUTO: the wavefront for a tree-searched scene (its walks diverge), and for a flat-searched one whose paths are
-    // long or whose shading is heavy (lights, textures, smoke: glass Cornell box 10% faster, marble spheres 60%);
-    // the persistent kernel for the bare small scenes, whose short paths cannot pay for the wavefront's queues
-    // (five spheres or five quads under the sky: 40% slower in the wavefront)
-    const bool heavy = view.light_count > 0 || view.lamp_count > 0 || has_features(view) || view.has_environment;
-    wavefront_ = options_.form == RT_FORM_WAVEFRONT ||
-                 (options_.form == RT_FORM_AUTO && view.node_count > 0 && (view.flat == 0 || heavy));
+    wavefront_ = options_.form == RT_FORM_WAVEFRONT || (options_.form == RT_FORM_AUTO && wavefront_suits(view));
     if (wavefront_)
     {
         kernel_attributes shade{}, trace{};

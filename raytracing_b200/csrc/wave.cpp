@@ -80,8 +80,7 @@ wave_buffers wave_runner::setup(int64_t samples, cudaStream_t stream)
 int64_t wave_runner::run(const wave_buffers& b, int max_depth, cudaStream_t stream,
                          const std::function<cudaError_t()>& step)
 {
-    check(cudaMemsetAsync(b.slots, 0, static_cast<size_t>(b.slot_count) * wave_slot_bytes(), stream),
-          "clearing the path slots");
+    check(clear_wave_slots(b, stream), "clearing the path slots");
     // A sample takes at most max_depth + 1 steps (its segments, then the one that adds its last shadow ray) and a slot
     // renders at most its share of the samples one after another: twice that bounds a launch that works
     const int64_t samples_per_slot = (b.sample_count + b.slot_count - 1) / b.slot_count;

@@ -39,9 +39,9 @@ def test_batch_equals_plain_renders(rt):
     jobs = _mixed_scenes(rt)
     b = rt.batch_render(jobs)
     assert b.graph
-    # per step: the two flat groups' persistent launches and the reduction, and for the tree-searched jobs (the cover
-    # scene) the wavefront's shade and trace launches of each step and its partials
-    assert b.steps >= 1 and b.launches > 3 * b.steps
+    # per step: the four persistent groups' launches and the reduction, and for the jobs in the wavefront form (the
+    # lit Cornell boxes, the cover scene) each group's shade and trace launches of each wavefront step and its partials
+    assert b.steps >= 1 and b.launches > 5 * b.steps
     for (scene, seed, passes), img in zip(jobs, b.images):
         ref = rt.render(scene, seed=seed, passes=passes)
         assert img.shape == ref.pixels.shape
@@ -57,6 +57,31 @@ def test_batch_graph_equals_direct_launches(rt):
     for x, y in zip(a.images, b.images):
         assert np.array_equal(x, y)
     assert a.rays == b.rays and a.shadow_rays == b.shadow_rays
+
+
+def test_batch_jobs_take_their_forms(rt):
+    # a bare flat scene in the persistent groups; a tree in the wavefront's groups; a lit flat scene in the persistent
+    # kernel in a short step (one wavefront run a step at most) and in the wavefront's flat-searched group in a long one
+    bare = rt.batch_render([(rt.builtin_scene("quads", width=32, spp=4), 1, 4)])
+    assert bare.launches == 5 * bare.steps  # the four persistent groups' launches and the reduction
+    short = rt.batch_render([(rt.builtin_scene("glass", width=32, spp=4), 1, 4)])
+    assert short.launches == 5 * short.steps
+    tree = rt.batch_render([(rt.builtin_scene("cover-40", width=32, spp=4), 1, 4)])
+    assert tree.launches >= 8 * tree.steps  # and a wavefront run's steps (two launches each) and its partials
+
+
+def test_long_step_flat_jobs_take_the_wavefront(rt):
+    """A step of more than 12M samples renders a lit flat scene (the glass Cornell box, 13M samples) in the wavefront's
+    flat-searched group; its image is a session's (the session's wavefront and flat search, to the rounding of
+    separately compiled kernels)."""
+    scene = rt.builtin_scene("glass", width=320, spp=128)
+    b = rt.batch_render([(scene, 31, 128)])
+    assert b.launches >= 8 * b.steps
+    ref = rt.render(scene, seed=31, passes=128).pixels
+    img = b.images[0]
+    close = np.isclose(img, ref, rtol=1e-4, atol=1e-5 * max(abs(ref.mean()), 1e-3))
+    assert close.mean() >= 0.99, close.mean()
+    assert abs(img.mean() - ref.mean()) <= 2e-4 * max(abs(ref.mean()), 1e-3), (img.mean(), ref.mean())
 
 
 def test_batch_small_arena_takes_more_steps_same_images(rt):
@@ -146,14 +171,14 @@ def test_server_admits_under_the_budget_in_order(rt):
 
 
 def test_large_tree_jobs_take_the_wavefront(rt):
-    """A job of a large tree (the mesh at 82k triangles) renders in the batch's wavefront groups beside jobs of the
-    persistent groups; its image is a session's render of the same view and seed (the session's wavefront: the same
-    samples, to the rounding of separately compiled kernels)."""
+    """A job of a large tree (the mesh at 82k triangles) renders in the batch's wavefront groups beside jobs of other
+    groups; its image is a session's render of the same view and seed (the session's wavefront: the same samples, to
+    the rounding of separately compiled kernels)."""
     jobs = [(rt.builtin_scene("mesh-ggx", width=64, spp=16, mesh_level=6, env_width=64), 21, 16),
             (rt.builtin_scene("cover-40", width=40, spp=16, scene_seed=5), 22, 16),
             (rt.builtin_scene("glass", width=32, spp=16), 23, 16)]
     b = rt.batch_render(jobs)
-    assert b.launches > 5 * b.steps  # the wavefront's steps beside the persistent groups' launches and the reduction
+    assert b.launches > 8 * b.steps  # the wavefront groups' steps beside the persistent groups' launches and the reduction
     for (scene, seed, passes), img in zip(jobs, b.images):
         ref = rt.render(scene, seed=seed, passes=passes).pixels
         close = np.isclose(img, ref, rtol=1e-4, atol=1e-5 * max(abs(ref.mean()), 1e-3))
