@@ -231,7 +231,7 @@ def batched_jobs(rt, count: int = 64, seed: int = 2024):
 
 
 def batched_measurement(rt, torch, rank: int = 0, world: int = 1) -> dict:
-    """64 jobs in one batched render (one persistent launch per step, replayed as a CUDA graph) against the plain
+    """64 jobs in one batched render (the jobs' wavefront runs sharing one slot pool, per step) against the plain
     form (one render per job), on the same jobs and seeds; every job's image compared bit for bit. With N ranks the
     jobs are split by cost (pixels x passes, longest first to the least loaded rank) and each rank renders its share
     on its own GPU: the times are the slowest rank's, the segments everyone's (no collective on the data)."""
@@ -280,7 +280,7 @@ def batched_measurement(rt, torch, rank: int = 0, world: int = 1) -> dict:
                      "speedup_gpu_over_reference": (batch_rays / batch_gpu) / (ref_rays / ref_kernel),
                      "speedup_e2e_over_reference": ref_wall / batch_wall}
     return {**reference, "workload": "64 cover-scene variants (50-2000 spheres, W,H log-uniform 64-1024, spp log-uniform "
-                        "16-1024, seeds 0-63), mixture of sizes in one persistent launch per step",
+                        "16-1024, seeds 0-63), mixture of sizes sharing one wavefront run per step",
             "ranks": world, "pixels": pixels, "samples": samples, "segments": batch_rays,
             "batched_segments_per_s": batch_rays / batch_gpu, "batched_gpu_s": batch_gpu,
             "batched_e2e_segments_per_s": batch_rays / batch_wall, "batched_e2e_s": batch_wall,

@@ -359,7 +359,7 @@ rt_status rt_session_set_counting(rt_session* session, int32_t on);
 rt_status rt_session_fetch_counts(const rt_session* session, uint64_t counts[4]);
 
 /* ---- batched rendering and serving (no counterpart in the reference: one session renders one view, renderer.h:
- * 585-590; here many requests share one persistent launch per refinement step) --------------------------------- */
+ * 585-590; here many requests share each refinement step's launches) ------------------------------------------- */
 
 /* One job of a batch: a scene (validated and built for the batch), the seed and passes it renders, and where its
  * image goes (width*height*3 doubles, host memory, rows from the top). */
@@ -391,8 +391,8 @@ typedef struct rt_batch_report
     int32_t pad0;
 } rt_batch_report;
 
-/* Renders every job to its passes in batched steps (many jobs of any size and scene per step, one persistent launch
-   per group of them). */
+/* Renders every job to its passes in batched steps (many jobs of any size and scene per step; each group of them,
+   by search and form, one persistent launch or one wavefront run per step). */
 rt_status rt_batch_render(const rt_batch_job* jobs, int32_t count, const rt_batch_options* options,
                           rt_batch_report* report);
 

@@ -365,7 +365,8 @@ class BatchResult:
 
 
 def batch_render(jobs: list, partial_budget_bytes: int = 0, use_graph: bool = True) -> BatchResult:
-    """Renders many jobs together, one persistent launch per step over every job's work items. jobs: a list of
+    """Renders many jobs together: per step, one launch (persistent kernel) or one run (wavefront) per group of jobs
+    over all their work items. jobs: a list of
     (scene, seed, passes) with scene an OwnedScene or a SceneDesc pointer and passes 0 for the camera's sqrt_spp^2."""
     n = len(jobs)
     table = (_abi.BatchJob * max(n, 1))()
