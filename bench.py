@@ -558,6 +558,7 @@ def run_b200(args):
         rt.render(scene_desc, seed=seed, passes=passes, launch_seconds=0.5, out=out)  # warm-up
         e_seconds = 0.0
         e_rays = 0
+        e_each = []
         for k in range(e2e_steps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -568,7 +569,8 @@ def run_b200(args):
             torch.cuda.synchronize()
             end.record()
             end.synchronize()
-            e_seconds += start.elapsed_time(end) / 1000.0
+            e_each.append(start.elapsed_time(end))
+            e_seconds += e_each[-1] / 1000.0
             e_rays += res.rays
             del t0
         e_seconds, e_rays = shard.combine(e_seconds, e_rays)
@@ -576,6 +578,9 @@ def run_b200(args):
             line["e2e"] = {"value": e_rays / e_seconds, "unit": UNIT, "h2d_bytes_per_step": int(stats["device_bytes"]),
                            "d2h_bytes_per_step": int(out.nbytes),
                            "ms_per_step": 1000 * e_seconds / e2e_steps,
+                           # each call's time: the host's share (scene build, teardown: about 7 ms) is the difference
+                           # to the kernels' time; a call far above it met host interference
+                           "ms_each": [round(x, 1) for x in e_each], "kernel_ms_last": round(1000 * res.kernel_seconds, 1),
                            "path": "raytracing_b200.render -> rt_render (validate, BVH build, upload, launches, "
                                    "download of width*height*3 doubles)"}
 
