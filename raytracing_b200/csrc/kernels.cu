@@ -2236,6 +2236,9 @@ constexpr uint32_t wave_finish = 8u;    // the sample ended at the shadow ray's 
 constexpr int wave_rows = 7;
 constexpr int wave_shadow_rows = 3;
 constexpr int wave_flags_row = 5; // depth, flags, unused, job: a slot whose row is zero has no sample
+// A query's flags (its meta's second word): 1 the ray starts inside the surface it leaves, 2 a shadow ray, 4 a new
+// sample's camera ray still to be made (a primary query); the job above them (<< 3)
+constexpr int wave_query_primary = 4;
 constexpr uint32_t wave_specular = 1u << 8;
 constexpr uint32_t wave_inward = 1u << 9;
 
@@ -2336,6 +2339,8 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         int px = 0, py = 0; // the pixel of a sample claimed in this step (a slot's camera ray needs no more)
         bool need = false;
         bool start = false;
+        bool primary = false; // a new sample whose camera ray the trace kernel makes (wave_camera_query)
+        int round_pass = 0;   // its pass within its round of strata
         rng.job = BATCH ? J->job : P.job;
         if (live)
         {
@@ -2500,14 +2505,22 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             // A new sample, as the persistent kernel starts one
             const int round_passes = BATCH ? J->round_passes : P.round_passes;
             const int64_t round = pass / round_passes;
-            const int in_round = static_cast<int>(pass - round * round_passes);
+            round_pass = static_cast<int>(pass - round * round_passes);
             const uint64_t key = (BATCH ? J->seed : P.seed) + (static_cast<uint64_t>(round) << 32);
             rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
-            rng.pass = static_cast<uint32_t>(in_round);
-            const float4 u = rng.draw(0, 0);
+            rng.pass = static_cast<uint32_t>(round_pass);
             const camera_params& cam = camera();
-            camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
-            ps.time = FEATURES && scene().has_motion ? rng.draw(0, block_time).x : 0.0f;
+            // Under a tree walk and the heavier shading (NEE/MIS, the second book's features) the trace kernel makes
+            // the camera ray, a warp's 32 at once, instead of this warp for its few new samples: the mesh +3.6%, the
+            // second book's final scene +3.7%. The books' plain sphere scenes (-2%) and the flat searches (-3% to
+            // -7%: their trace kernel's tail grows by it) make their own here.
+            primary = (quality() || FEATURES) && scene().flat == 0;
+            if (!primary)
+            {
+                const float4 u = rng.draw(0, 0);
+                camera_ray(cam, px, py, round_pass % cam.sqrt_spp, round_pass / cam.sqrt_spp, u, ps.o, ps.d);
+                ps.time = FEATURES && scene().has_motion ? rng.draw(0, block_time).x : 0.0f;
+            }
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
             ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
             ps.bsdf_pdf = 0.0f;
@@ -2518,19 +2531,22 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             ps.inward = false;
             flags |= wave_ext;
         }
-        // The slot's queries: one atomic per warp for its next rays and its shadow rays
-        const bool ext = (flags & wave_ext) != 0u;
+        // The slot's queries: one atomic per warp for its next rays and its shadow rays from the bottom of the queue,
+        // one for its new samples' camera rays (primary queries) from the top down
+        const bool ext = (flags & wave_ext) != 0u && !primary;
         const bool shadow = (QUALITY || BATCH) && (flags & wave_shadow) != 0u;
         const unsigned ext_lanes = __ballot_sync(full_warp, ext);
         const unsigned shadow_lanes = __ballot_sync(full_warp, shadow);
+        const unsigned primary_lanes = __ballot_sync(full_warp, primary);
         const int queued = __popc(ext_lanes) + __popc(shadow_lanes);
         if constexpr (BATCH)
         {
             // each job's segments and shadow rays, counted as queued: one atomic per job of the warp
-            const unsigned peers = __match_any_sync(full_warp, ext || shadow ? job : -1);
-            if ((ext || shadow) && static_cast<int>(lane) == __ffs(static_cast<int>(peers)) - 1)
+            const bool any = ext || shadow || primary;
+            const unsigned peers = __match_any_sync(full_warp, any ? job : -1);
+            if (any && static_cast<int>(lane) == __ffs(static_cast<int>(peers)) - 1)
             {
-                const unsigned e = __popc(peers & ext_lanes), sh = __popc(peers & shadow_lanes);
+                const unsigned e = __popc(peers & (ext_lanes | primary_lanes)), sh = __popc(peers & shadow_lanes);
                 if (e)
                 {
                     atomicAdd(J->counters, static_cast<unsigned long long>(e));
@@ -2554,7 +2570,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                 const unsigned q = base + static_cast<unsigned>(__popc(ext_lanes & lanes_below));
                 stream_store(B.query_o + q, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time));
                 stream_store(B.query_d + q, make_float4(ps.d.x, ps.d.y, ps.d.z, infinity_f));
-                stream_store(B.query_meta + q, make_int4(ps.from, (ps.inward ? 1 : 0) | (job << 2), -1, i));
+                stream_store(B.query_meta + q, make_int4(ps.from, (ps.inward ? 1 : 0) | (job << 3), -1, i));
             }
             if (shadow)
             {
@@ -2562,12 +2578,33 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                                    static_cast<unsigned>(__popc(shadow_lanes & lanes_below));
                 stream_store(B.query_o + q, make_float4(sq.o.x, sq.o.y, sq.o.z, ps.time));
                 stream_store(B.query_d + q, make_float4(sq.d.x, sq.d.y, sq.d.z, sq.t_max));
-                stream_store(B.query_meta + q, make_int4(sq.from, (sq.inward ? 1 : 0) | 2 | (job << 2), sq.skip, i));
+                stream_store(B.query_meta + q, make_int4(sq.from, (sq.inward ? 1 : 0) | 2 | (job << 3), sq.skip, i));
                 // what the next step needs of it: the light it brings and, through smoke, its segment
                 stream_store(shadow_rows + i, make_float4(sq.o.x, sq.o.y, sq.o.z, sq.t_max));
                 stream_store(shadow_rows + n + i, make_float4(sq.d.x, sq.d.y, sq.d.z, sq.contribution.x));
                 stream_store(reinterpret_cast<int4*>(shadow_rows) + 2 * n + i,
                              make_int4(__float_as_int(sq.contribution.y), __float_as_int(sq.contribution.z), 0, 0));
+            }
+        }
+        if (primary_lanes != 0u)
+        {
+            const int leader = __ffs(static_cast<int>(primary_lanes)) - 1;
+            unsigned base = 0;
+            if (static_cast<int>(lane) == leader)
+            {
+                base = atomicAdd(B.control + 2, static_cast<unsigned>(__popc(primary_lanes)));
+            }
+            base = __shfl_sync(full_warp, base, leader);
+            if (primary)
+            {
+                // the pixel, the pass in its round and the RNG's key: what the camera ray is made of
+                const unsigned q = 2u * static_cast<unsigned>(n) - 1u -
+                                   (base + static_cast<unsigned>(__popc(primary_lanes & lanes_below)));
+                stream_store(B.query_o + q, make_float4(__int_as_float(px), __int_as_float(py),
+                                                        __int_as_float(round_pass), 0.0f));
+                stream_store(B.query_d + q, make_float4(__uint_as_float(rng.key.x), __uint_as_float(rng.key.y), 0.0f,
+                                                        infinity_f));
+                stream_store(B.query_meta + q, make_int4(-1, wave_query_primary | (job << 3), -1, i));
             }
         }
         if (live)
@@ -2597,6 +2634,41 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     }
 }
 
+// The query at position q of the queue: the shade step's next rays and shadow rays fill it from the bottom (`lower`
+// of them), its new samples' camera rays from the top down. A primary query (pixel, pass in its round, the RNG's key) is
+// made into its camera ray here, the persistent kernel's start of a sample with the same random numbers, and the ray
+// goes into its slot's first two rows, which the shade step that meets its hit reads.
+template <bool FEATURES, bool BATCH>
+__device__ __forceinline__ void wave_camera_query(const wave_buffers& B, const wave_batch& W, const scene_view& S0,
+                                                  unsigned q, unsigned lower, float4& qo, float4& qd, int4& qm)
+{
+    const unsigned k = q < lower ? q : 2u * static_cast<unsigned>(B.slot_count) - 1u - (q - lower);
+    qo = stream_load(B.query_o + k);
+    qd = stream_load(B.query_d + k);
+    qm = stream_load(B.query_meta + k);
+    if (qm.y & wave_query_primary)
+    {
+        const batch_job* J = BATCH ? W.jobs + (qm.y >> 3) : nullptr;
+        const camera_params& cam = BATCH ? J->cam : B.cam;
+        const scene_view& S = BATCH ? J->scene : S0;
+        const int px = __float_as_int(qo.x), py = __float_as_int(qo.y), round_pass = __float_as_int(qo.z);
+        sampler rng;
+        rng.key = make_uint2(__float_as_uint(qd.x), __float_as_uint(qd.y));
+        rng.pixel = static_cast<uint32_t>(py) * static_cast<uint32_t>(cam.width) + static_cast<uint32_t>(px);
+        rng.pass = static_cast<uint32_t>(round_pass);
+        rng.job = BATCH ? J->job : B.job;
+        float3 o, d;
+        camera_ray(cam, px, py, round_pass % cam.sqrt_spp, round_pass / cam.sqrt_spp, rng.draw(0, 0), o, d);
+        const float time = FEATURES && S.has_motion ? rng.draw(0, block_time).x : 0.0f;
+        float4* rows = static_cast<float4*>(B.slots);
+        stream_store(rows + qm.w, make_float4(o.x, o.y, o.z, time));
+        stream_store(rows + B.slot_count + qm.w, make_float4(d.x, d.y, d.z, 0.0f)); // bsdf_pdf 0 at the camera
+        qo = make_float4(o.x, o.y, o.z, time);
+        qd = make_float4(d.x, d.y, d.z, infinity_f);
+        qm.y &= ~wave_query_primary;
+    }
+}
+
 // The trace kernel's resident blocks per multiprocessor (64 registers at 8) and the number of lanes still walking
 // under which a warp stops to give its idle lanes new queries (the addendum's 20 of 32)
 #ifndef RTB_TRACE_MIN_BLOCKS
@@ -2622,7 +2694,8 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
         block_walks[threadIdx.x] = 0;
     }
     __syncthreads();
-    const unsigned count = B.control[0];
+    const unsigned lower = B.control[0];
+    const unsigned count = lower + B.control[2];
     unsigned walks[2] = {0, 0};
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
@@ -2685,9 +2758,9 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
             const unsigned q = base + static_cast<unsigned>(__popc(idle & lanes_below));
             if (!has_query && q < count)
             {
-                const float4 qo = stream_load(B.query_o + q);
-                const float4 qd = stream_load(B.query_d + q);
-                const int4 qm = stream_load(B.query_meta + q);
+                float4 qo, qd;
+                int4 qm;
+                wave_camera_query<FEATURES, BATCH>(B, W, S0, q, lower, qo, qd, qm);
                 o = make_float3(qo.x, qo.y, qo.z);
                 time = qo.w;
                 d = make_float3(qd.x, qd.y, qd.z);
@@ -2701,7 +2774,7 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
                 slot = qm.w;
                 if constexpr (BATCH)
                 {
-                    job_scene = &W.jobs[qm.y >> 2].scene;
+                    job_scene = &W.jobs[qm.y >> 3].scene;
                 }
                 ++walks[shadow ? 1 : 0];
                 inverse_a = 1.0f / length_squared(d);
@@ -2955,7 +3028,7 @@ __global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
         const scene_view* scene = &S;
         if constexpr (BATCH)
         {
-            scene = &W.jobs[qm.y >> 2].scene;
+            scene = &W.jobs[qm.y >> 3].scene;
         }
         flat_search<FEATURES>(*scene, make_float3(qo.x, qo.y, qo.z), make_float3(qd.x, qd.y, qd.z), qo.w, qm.x,
                               (qm.y & 1) != 0, qm.z, shadow, hit);
@@ -3237,10 +3310,13 @@ wave_trace_function wave_flat_trace_of(bool features)
 }
 } // namespace
 
-cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
+cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& slots, int trace_grid,
                              cudaStream_t stream)
 {
-    cudaError_t e = cudaMemsetAsync(b.control, 0, 2 * sizeof(unsigned), stream);
+    wave_buffers b = slots; // with the launch's camera and RNG job, for the camera rays the trace kernel makes
+    b.cam = p.cam;
+    b.job = p.job;
+    cudaError_t e = cudaMemsetAsync(b.control, 0, 3 * sizeof(unsigned), stream);
     if (e != cudaSuccess)
     {
         return e;
@@ -3268,7 +3344,7 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
 cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, const wave_buffers& b,
                                    int trace_grid, cudaStream_t stream)
 {
-    cudaError_t e = cudaMemsetAsync(b.control, 0, 2 * sizeof(unsigned), stream);
+    cudaError_t e = cudaMemsetAsync(b.control, 0, 3 * sizeof(unsigned), stream);
     if (e != cudaSuccess)
     {
         return e;

@@ -164,10 +164,14 @@ struct wave_buffers
     int64_t sample_count;   // (pass_end - pass_begin) * padded_pixels
     float4* query_o;        // 2 * slot_count queries: origin, time
     float4* query_d;        // direction, t_max
-    int4* query_meta;       // from, flags (1 inward, 2 shadow), skip, slot
+    int4* query_meta;       // from, flags (1 inward, 2 shadow, 4 a camera ray to make; the job << 3), skip, slot
     int4* ext_result;       // per slot: the next ray's hit (id, t's bits, front)
     int32_t* shadow_result; // per slot: 1 if the shadow ray was blocked
-    unsigned* control;      // [0] queries the last shade step queued, [1] queries the trace kernel took
+    // [0] next rays and shadow rays the last shade step queued (from the bottom), [1] queries the trace kernel took,
+    // [2] camera rays it queued (from the top down; tree-searched scenes only); [3] unused
+    unsigned* control;
+    camera_params cam;      // a session's launch: its camera and RNG job field (a batch: each job's, in its table)
+    uint32_t job;
 };
 size_t wave_slot_bytes();
 // Every slot without a sample (its flags row zeroed), before a launch's first step

@@ -38,13 +38,13 @@ wave_buffers wave_runner::setup(int64_t samples, cudaStream_t stream)
 {
     if (!queued_)
     {
-        check(cudaHostAlloc(reinterpret_cast<void**>(&queued_), 2 * sizeof(unsigned), cudaHostAllocDefault),
+        check(cudaHostAlloc(reinterpret_cast<void**>(&queued_), 8 * sizeof(unsigned), cudaHostAllocDefault),
               "allocating pinned memory");
         for (auto& e : done_)
         {
             check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating a CUDA event");
         }
-        control_.allocate_async(2, stream);
+        control_.allocate_async(4, stream);
     }
     const int64_t wanted = (samples + render_block - 1) / render_block * render_block;
     const auto n = static_cast<size_t>(std::min<int64_t>(max_slots, std::max<int64_t>(wanted, render_block)));
@@ -96,13 +96,14 @@ int64_t wave_runner::run(const wave_buffers& b, int max_depth, cudaStream_t stre
         }
         steps += group;
         const int k = g & 1;
-        check(cudaMemcpyAsync(queued_ + k, b.control, sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
+        check(cudaMemcpyAsync(queued_ + 4 * k, b.control, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
               "reading the queue's length");
         check(cudaEventRecord(done_[k], stream), "recording a CUDA event");
         if (g > 0)
         {
             check(cudaEventSynchronize(done_[k ^ 1]), "rendering on the GPU");
-            if (queued_[k ^ 1] == 0)
+            const unsigned* q = queued_ + 4 * (k ^ 1);
+            if (q[0] + q[2] == 0) // no next ray, shadow ray or camera ray queued
             {
                 break;
             }
