@@ -348,6 +348,52 @@ rt_status rt_session_kernel(const rt_session* session, rt_kernel_info* info);
 rt_status rt_render_passes_no_alloc(rt_scene* scene, const rt_camera_desc* camera, uint64_t seed, int64_t pass_begin,
                                     int64_t pass_end, double* device_sums, uint64_t* rays, uint64_t* shadow_rays);
 
+/* ---- the display transform and the image files (renderer.h:278-303, 623-635; image.ixx:93-203) ------------ */
+
+/* renderer.h:286-292 tone_map: how linear light becomes a screen's bytes. BOOKS: the books' bytes (gamma 2 as a
+ * square root, clamped to 0.999, times 256 truncated; image::save_png's to_byte). NONE: the light times 2^exposure,
+ * clipped to [0, 1], sRGB-encoded. AGX: Troy Sobotka's AgX (16.5 stops on a log2 curve). NEUTRAL: Khronos PBR Neutral,
+ * then sRGB. The last three are dithered by interleaved gradient noise of the pixel's position. */
+enum { RT_TONE_BOOKS = 0, RT_TONE_NONE = 1, RT_TONE_AGX = 2, RT_TONE_NEUTRAL = 3 };
+
+/* renderer.h:294-303 display_options: a tone map and an exposure in stops, a finite number within +-24
+ * (max_exposure); BOOKS takes no exposure (RT_ERR_INVALID otherwise, as check_display, renderer.cu:1204-1220). */
+typedef struct rt_display_options
+{
+    int32_t tone_map;           /* RT_TONE_* */
+    int32_t pad0;
+    double exposure;
+} rt_display_options;
+
+/* session::display(options) (renderer.h:623-635): the image of the complete passes as 4 bytes per pixel (red, green,
+ * blue, 255), rows from the top, computed on the GPU from the FP64 sums (the reference's display.cu and tonemap.cu
+ * kernels, bit for bit). byte_count must be width*height*4. RT_ERR_LOGIC before the image has a complete pass. */
+rt_status rt_session_display(rt_session* session, const rt_display_options* options, uint8_t* rgba,
+                             int64_t byte_count);
+
+/* The same transform on an image kept in device memory by the caller (a served frame, the no-allocation entry
+ * point's sums): device_sums holds width*height*3 doubles, the sums of `passes` passes; device_rgba receives
+ * width*height*4 bytes (4-byte aligned). Queued on `stream` (a cudaStream_t; NULL: the default stream) and not waited
+ * for. No counterpart in the reference's API (its session keeps its sums private). */
+rt_status rt_display_device(const double* device_sums, int32_t width, int32_t height, int64_t passes,
+                            const rt_display_options* options, uint8_t* device_rgba, void* stream);
+
+/* image::save (image.ixx:170-184): writes `pixels` (width*height*3 linear doubles, rows from the top) to `path` in
+ * the format its extension names, .pfm or .png in any letter case (RT_ERR_INVALID for another). PFM (save_pfm,
+ * image.ixx:157-168): "PF", the size, -1.0, rows from the bottom as little-endian float32, the linear values. PNG
+ * (save_png, image.ixx:116-145): 8-bit RGB of the display transform's bytes under `options` (NULL: BOOKS; a tone map
+ * other than BOOKS is computed on the GPU, as the reference computes its tone maps' bytes). */
+rt_status rt_image_save(const char* path, const double* pixels, int32_t width, int32_t height,
+                        const rt_display_options* options);
+
+/* image::mean_radiance (image.ixx:93-103): the average over all pixels of (r + g + b) / 3, summed in pixel order as
+ * the reference's average() folds them. */
+rt_status rt_image_mean_radiance(const double* pixels, int32_t width, int32_t height, double* mean);
+
+/* The session's image of complete passes saved as rt_image_save saves pixels(), and its mean radiance. */
+rt_status rt_session_save(rt_session* session, const char* path, const rt_display_options* options);
+rt_status rt_session_mean_radiance(const rt_session* session, double* mean);
+
 /* Device-resident variant for callers that keep the image on the GPU (a served frame, a display transform):
  * the device address of the per-pixel sums (3 doubles per pixel, rows from the top) and of the pass count. */
 rt_status rt_session_device_sums(const rt_session* session, const double** sums, int64_t* passes);
@@ -450,6 +496,10 @@ rt_status rt_server_step(rt_server* server, rt_server_step_report* report);
 rt_status rt_server_poll(const rt_server* server, int64_t request_id, rt_request_status* status);
 /* The request's image so far (sums / passes); frees a finished request's device memory. */
 rt_status rt_server_fetch(rt_server* server, int64_t request_id, double* pixels, int64_t pixel_count);
+/* The request's image so far through the display transform (rt_session_display's bytes for its view): the frame a
+ * served client is shown. Keeps the request's memory (a later rt_server_fetch frees a finished one). */
+rt_status rt_server_display(rt_server* server, int64_t request_id, const rt_display_options* options, uint8_t* rgba,
+                            int64_t byte_count);
 rt_status rt_server_cancel(rt_server* server, int64_t request_id);
 rt_status rt_server_stats_get(const rt_server* server, rt_server_stats* stats);
 

@@ -56,6 +56,9 @@ def load() -> C.CDLL:
         lib.oracle_closest_hits.restype = C.c_int
         lib.oracle_closest_hits.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64,
                                             C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        lib.oracle_hit_distances.restype = C.c_int
+        lib.oracle_hit_distances.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64,
+                                             C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         lib.oracle_image_compare.restype = C.c_int
         lib.oracle_image_compare.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, C.c_int32,
                                              C.c_int32, C.POINTER(CompareResult)]
@@ -101,6 +104,53 @@ def closest_hits(desc, origins: np.ndarray, directions: np.ndarray, brute_force:
     if status != 0:
         raise RuntimeError(lib.oracle_last_error().decode())
     return ids, ts
+
+
+def hit_distances(desc, origins: np.ndarray, directions: np.ndarray, ids: np.ndarray) -> np.ndarray:
+    """Where, in double, each ray meets primitive ids[i] (source index space) over (0.001, inf); inf where it does
+    not or ids[i] < 0."""
+    lib = load()
+    o = np.ascontiguousarray(origins, dtype=np.float64).reshape(-1, 3)
+    d = np.ascontiguousarray(directions, dtype=np.float64).reshape(-1, 3)
+    k = np.ascontiguousarray(ids, dtype=np.int32).reshape(-1)
+    ts = np.empty(k.size, dtype=np.float64)
+    status = lib.oracle_hit_distances(_desc_pointer(desc), o.ctypes.data_as(C.POINTER(C.c_double)),
+                                      d.ctypes.data_as(C.POINTER(C.c_double)), k.size,
+                                      k.ctypes.data_as(C.POINTER(C.c_int32)), ts.ctypes.data_as(C.POINTER(C.c_double)))
+    if status != 0:
+        raise RuntimeError(lib.oracle_last_error().decode())
+    return ts
+
+
+def first_hit_mismatches(desc, origins, directions, ids, ref_ids, ts=None, ref_ts=None, tie_rel: float = 1e-6) -> dict:
+    """First-hit parity of `ids` against `ref_ids` on the same rays (both source index space, -1 a miss). Of the rays
+    whose ids differ, a tie is one where both searches hit a surface at the same distance within `tie_rel` relative
+    (the reference's tracer-check class `ties`, tests/tracer_check_layout.h: another primitive at the same t): either
+    the double search meets both primitives within `tie_rel` of each other, or the two searches' own distances
+    (`ts`, `ref_ts`, where given) agree within `tie_rel`. Every other difference is a mismatch."""
+    ids = np.asarray(ids).reshape(-1)
+    ref_ids = np.asarray(ref_ids).reshape(-1)
+    bad = np.flatnonzero(ids != ref_ids)
+    ties = 0
+    if bad.size:
+        o = np.asarray(origins, dtype=np.float64).reshape(-1, 3)[bad]
+        d = np.asarray(directions, dtype=np.float64).reshape(-1, 3)[bad]
+        ta = hit_distances(desc, o, d, ids[bad])
+        tb = hit_distances(desc, o, d, ref_ids[bad])
+
+        def close(a, b):
+            both = np.isfinite(a) & np.isfinite(b) & (ids[bad] >= 0) & (ref_ids[bad] >= 0)
+            a0 = np.where(both, a, 1.0)
+            b0 = np.where(both, b, 1.0)
+            return both & (np.abs(a0 - b0) <= tie_rel * np.minimum(np.abs(a0), np.abs(b0)))
+
+        tie = close(ta, tb)
+        if ts is not None and ref_ts is not None:
+            tie |= close(np.asarray(ts, dtype=np.float64).reshape(-1)[bad],
+                         np.asarray(ref_ts, dtype=np.float64).reshape(-1)[bad])
+        ties = int(np.count_nonzero(tie))
+    return {"rays": int(ids.size), "mismatches": int(bad.size), "ties": ties,
+            "non_tie_mismatches": int(bad.size) - ties, "tie_rel": tie_rel}
 
 
 def image_compare(a: np.ndarray, b: np.ndarray, tile: int = 32) -> dict:

@@ -4,13 +4,18 @@ The reference's `gpu_renderer` library is eight CUDA sources under src/gpu (rend
 tonemap.cu, lamp_table.cu, environment_table.cu, CMakeLists.txt:155-165; guides.cu and denoise.cu, added to it by
 cmake/optix.cmake:203 with or without OptiX), plain nvcc translation units with no generated code and no external
 library. They are compiled here where they lie, unmodified, for sm_100a, with the
-flags its build gives them (-fmad=false for display.cu and tonemap.cu), and linked with oracle/ref_gpu_shim.cpp, a C
-entry point that converts this library's scene tables into the reference's. The output goes only to oracle/_ref/
-(git-ignored; it travels with the checkout to a GPU machine). Usage: python oracle/build_ref.py [reference root]
+flags its build gives them (-fmad=false for display.cu and tonemap.cu), and linked with oracle/ref_gpu_shim.cpp (C
+entry points that convert this library's scene tables into the reference's and call its render and display
+transforms) and oracle/ref_closest_hit.cu (the reference's device closest_hit on given rays). The output goes only to
+oracle/_ref/ (git-ignored; it travels with the checkout to a GPU machine).
+
+Usage: python oracle/build_ref.py [reference root]. The root is the argument, else the environment variable
+RT_REFERENCE_ROOT, else a folder named `reference` beside this repository's checkout.
 """
 from __future__ import annotations
 
 import concurrent.futures as futures
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -31,29 +36,41 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError(f"{' '.join(cmd)} failed:\n{r.stdout}\n{r.stderr}")
 
 
+SHIMS = ["ref_gpu_shim.cpp", "ref_closest_hit.cu"]
+
+
+def reference_root(reference: Path | str | None = None) -> Path:
+    """Where the reference's checkout is: the argument, else $RT_REFERENCE_ROOT, else `reference` beside the repo."""
+    if reference:
+        return Path(reference)
+    if os.environ.get("RT_REFERENCE_ROOT"):
+        return Path(os.environ["RT_REFERENCE_ROOT"])
+    return REPO.parent / "reference"
+
+
 def build(reference: Path | None = None) -> Path | None:
     """Returns the library's path, or None when the reference's sources are absent (e.g. on a GPU machine, which
     uses the library built beside the checkout)."""
-    root = Path(reference) if reference else Path("/root/reference")
-    gpu = root / "src" / "gpu"
+    gpu = reference_root(reference) / "src" / "gpu"
     if not (gpu / "renderer.cu").exists():
         return LIBRARY if LIBRARY.exists() else None
     OUT.mkdir(exist_ok=True)
-    inputs = [gpu / s for s in SOURCES] + [HERE / "ref_gpu_shim.cpp", gpu / "renderer.h", Path(__file__)]
+    inputs = ([gpu / s for s in SOURCES] + [HERE / s for s in SHIMS] +
+              [HERE / "ref_scene_convert.h", gpu / "renderer.h", Path(__file__)])
     if LIBRARY.exists() and LIBRARY.stat().st_mtime > max(p.stat().st_mtime for p in inputs):
         return LIBRARY
 
     def compile_one(source: Path) -> Path:
-        obj = OUT / (source.stem + ".o")
+        obj = OUT / (source.name + ".o")
         flags = ["nvcc", "-std=c++20", "-O3", *ARCH, "-Xcompiler", "-fPIC", "-I", str(gpu), "-I",
-                 str(REPO / "include")]
+                 str(REPO / "include"), "-I", str(HERE)]
         if source.name in NO_FMAD:
             flags.append("-fmad=false")
         _run(flags + ["-c", str(source), "-o", str(obj)])
         return obj
 
     with futures.ThreadPoolExecutor(max_workers=9) as pool:
-        objects = list(pool.map(compile_one, [gpu / s for s in SOURCES] + [HERE / "ref_gpu_shim.cpp"]))
+        objects = list(pool.map(compile_one, [gpu / s for s in SOURCES] + [HERE / s for s in SHIMS]))
     _run(["nvcc", "-shared", *ARCH, "-cudart", "static", "-o", str(LIBRARY), *map(str, objects)])
     for obj in objects:
         obj.unlink()

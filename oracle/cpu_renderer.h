@@ -502,6 +502,28 @@ public:
         return hit_node(root_, r, t, skip);
     }
 
+    // Primitive `id` alone (source index space: spheres, then quads, then triangles), for the first-hit test's tie
+    // rule: where it is hit along the ray in double, if at all
+    std::optional<hit_record> hit_id(int id, const ray& r, interval t) const
+    {
+        const auto n_spheres = static_cast<int>(spheres.size());
+        const auto n_quads = static_cast<int>(quads.size());
+        if (id < 0)
+        {
+            return std::nullopt;
+        }
+        if (id < n_spheres)
+        {
+            return spheres[static_cast<size_t>(id)].hit(r, t);
+        }
+        if (id < n_spheres + n_quads)
+        {
+            return quads[static_cast<size_t>(id - n_spheres)].hit(r, t);
+        }
+        const auto k = static_cast<size_t>(id - n_spheres - n_quads);
+        return k < triangles.size() ? triangles[k].hit(r, t) : std::nullopt;
+    }
+
     // The closest hit by testing every primitive in turn (hittable_list::hit, hittable.ixx:170-183): the brute-force
     // check the first-hit parity test compares against
     std::optional<hit_record> hit_brute_force(const ray& r, interval t) const

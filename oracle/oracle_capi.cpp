@@ -173,6 +173,31 @@ int oracle_closest_hits(const rt_scene_desc* desc, const double* origins, const 
     return 0;
 }
 
+// For the first-hit test's tie rule: where, in double, each ray meets the primitive ids[i] (source index space) over
+// (0.001, inf), or inf where it does not (or ids[i] < 0). A mismatch between two searches is a tie when both
+// primitives are met at the same distance within the stated relative tolerance (coplanar or touching faces: the
+// reference's tracer-check class `ties`, tests/tracer_check_layout.h).
+int oracle_hit_distances(const rt_scene_desc* desc, const double* origins, const double* directions, int64_t count,
+                         const int32_t* ids, double* ts)
+{
+    oracle::scene s;
+    const char* error = nullptr;
+    if (!desc || !oracle::make_scene(*desc, s, &error))
+    {
+        set_error(error ? error : "null argument");
+        return 1;
+    }
+    for (int64_t i = 0; i < count; ++i)
+    {
+        const oracle::ray r{{origins[3 * i], origins[3 * i + 1], origins[3 * i + 2]},
+                            {directions[3 * i], directions[3 * i + 1], directions[3 * i + 2]},
+                            0};
+        const auto rec = s.geometry.hit_id(ids[i], r, oracle::interval{0.001, oracle::infinity});
+        ts[i] = rec ? rec->t : oracle::infinity;
+    }
+    return 0;
+}
+
 int oracle_image_compare(const float* a, const float* b, int32_t width, int32_t height, int32_t tile_size,
                          oracle::compare_result* result)
 {

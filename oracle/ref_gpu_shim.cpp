@@ -1,170 +1,29 @@
-// Test infrastructure, not product: a C entry point into the reference's own CUDA renderer (its src/gpu sources,
+// Test infrastructure, not product: C entry points into the reference's own CUDA renderer (its src/gpu sources,
 // compiled unmodified into oracle/_ref by oracle/build_ref.py), so that tests and the bench can render a scene given
 // as this library's C tables with the reference itself. It converts rt_scene_desc into the reference's gpu::scene_desc
 // (src/gpu/renderer.h:381-395, member types 43-377), calls gpu::render (renderer.h:526) and copies the result out.
-// Triangle meshes are refused: the reference renders them only through OptiX, which is absent here.
+// Triangle meshes are refused: the reference renders them only through OptiX, which is absent here. A second entry
+// point runs the reference's display transforms (display.cu, tonemap.cu) on given sums.
 #include "renderer.h" // the reference's header, from its source tree
 
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <exception>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
+#include <cuda_runtime.h>
+
+#include "display.cuh" // the reference's display transforms, from its source tree
+#include "ref_scene_convert.h"
+#include "tonemap.cuh"
 #include "rt_b200.h"
 
 namespace
 {
-gpu::vec3d to_ref(const rt_vec3& v) { return {v.x, v.y, v.z}; }
-
-gpu::quad_desc to_ref(const rt_quad_desc& q)
-{
-    gpu::quad_desc r;
-    r.q = to_ref(q.q);
-    r.u = to_ref(q.u);
-    r.v = to_ref(q.v);
-    r.material = q.material;
-    return r;
-}
-
-gpu::sphere_desc to_ref(const rt_sphere_desc& s)
-{
-    gpu::sphere_desc r;
-    r.center = to_ref(s.center);
-    r.radius = s.radius;
-    r.material = s.material;
-    r.displacement = to_ref(s.displacement);
-    r.uv_cos = s.uv_cos;
-    r.uv_sin = s.uv_sin;
-    return r;
-}
-
-gpu::image_desc to_ref(const rt_image_desc& im)
-{
-    gpu::image_desc r;
-    r.width = im.width;
-    r.height = im.height;
-    const size_t n = static_cast<size_t>(im.width) * static_cast<size_t>(im.height) * 3;
-    r.rgb.assign(im.rgb, im.rgb + n);
-    return r;
-}
-
-gpu::camera_desc to_ref(const rt_camera_desc& c)
-{
-    gpu::camera_desc r;
-    r.image_width = c.image_width;
-    r.image_height = c.image_height;
-    r.sqrt_spp = c.sqrt_spp;
-    r.max_depth = c.max_depth;
-    r.center = to_ref(c.center);
-    r.pixel00_loc = to_ref(c.pixel00_loc);
-    r.pixel_delta_u = to_ref(c.pixel_delta_u);
-    r.pixel_delta_v = to_ref(c.pixel_delta_v);
-    r.defocus = c.defocus != 0;
-    r.defocus_disk_u = to_ref(c.defocus_disk_u);
-    r.defocus_disk_v = to_ref(c.defocus_disk_v);
-    r.sky_bottom = to_ref(c.sky_bottom);
-    r.sky_top = to_ref(c.sky_top);
-    r.sampling = static_cast<gpu::sampling_strategy>(c.sampling);
-    return r;
-}
-
-gpu::scene_desc to_ref(const rt_scene_desc& d)
-{
-    gpu::scene_desc s;
-    for (int64_t i = 0; i < d.sphere_count; ++i)
-    {
-        s.spheres.push_back(to_ref(d.spheres[i]));
-    }
-    for (int64_t i = 0; i < d.material_count; ++i)
-    {
-        const rt_material_desc& m = d.materials[i];
-        gpu::material_desc r;
-        r.kind = static_cast<gpu::material_kind>(m.kind);
-        r.albedo = to_ref(m.albedo);
-        r.fuzz = m.fuzz;
-        r.refraction_index = m.refraction_index;
-        r.texture = m.texture;
-        s.materials.push_back(r);
-    }
-    s.camera = to_ref(d.camera);
-    for (int64_t i = 0; i < d.texture_count; ++i)
-    {
-        const rt_texture_desc& t = d.textures[i];
-        gpu::texture_desc r;
-        r.kind = static_cast<gpu::texture_kind>(t.kind);
-        r.rgb = to_ref(t.rgb);
-        r.inv_scale = t.inv_scale;
-        r.even = t.even;
-        r.odd = t.odd;
-        r.image = t.image;
-        r.scale = t.scale;
-        r.perlin = t.perlin;
-        s.textures.push_back(r);
-    }
-    for (int64_t i = 0; i < d.image_count; ++i)
-    {
-        s.images.push_back(to_ref(d.images[i]));
-    }
-    for (int64_t i = 0; i < d.perlin_count; ++i)
-    {
-        gpu::perlin_desc p;
-        for (int k = 0; k < gpu::perlin_point_count; ++k)
-        {
-            p.random_vectors[k] = to_ref(d.perlins[i].random_vectors[k]);
-            p.perm_x[k] = d.perlins[i].perm_x[k];
-            p.perm_y[k] = d.perlins[i].perm_y[k];
-            p.perm_z[k] = d.perlins[i].perm_z[k];
-        }
-        s.perlins.push_back(p);
-    }
-    for (int64_t i = 0; i < d.quad_count; ++i)
-    {
-        s.quads.push_back(to_ref(d.quads[i]));
-    }
-    for (int64_t i = 0; i < d.medium_count; ++i)
-    {
-        const rt_medium_desc& m = d.media[i];
-        gpu::medium_desc r;
-        r.boundary = static_cast<gpu::boundary_shape>(m.boundary);
-        r.sphere = to_ref(m.sphere);
-        for (int64_t k = 0; k < m.quad_count; ++k)
-        {
-            r.quads.push_back(to_ref(m.quads[k]));
-        }
-        r.neg_inv_density = m.neg_inv_density;
-        r.material = m.material;
-        s.media.push_back(r);
-    }
-    for (int64_t i = 0; i < d.light_count; ++i)
-    {
-        const rt_light_desc& l = d.lights[i];
-        gpu::light_desc r;
-        r.kind = static_cast<gpu::light_shape>(l.kind);
-        r.quad = to_ref(l.quad);
-        r.center = to_ref(l.center);
-        r.radius = l.radius;
-        r.weight = l.weight;
-        s.lights.push_back(r);
-    }
-    s.quality.combination = static_cast<gpu::light_combination>(d.combination);
-    for (int64_t i = 0; i < d.microfacet_count; ++i)
-    {
-        gpu::microfacet_desc r;
-        r.kind = static_cast<gpu::microfacet_kind>(d.microfacets[i].kind);
-        r.roughness = d.microfacets[i].roughness;
-        s.quality.microfacets.push_back(r);
-    }
-    if (d.environment)
-    {
-        gpu::environment_desc e;
-        e.image = to_ref(d.environment->image);
-        e.yaw_degrees = d.environment->yaw_degrees;
-        e.scale = d.environment->scale;
-        s.quality.environment = e;
-    }
-    return s;
-}
+using ref_convert::to_ref;
 
 void copy_error(const char* what, char* error, int error_size)
 {
@@ -233,6 +92,58 @@ int ref_gpu_render(const rt_scene_desc* scene, uint64_t seed, int64_t passes, in
     }
     catch (const std::exception& e)
     {
+        copy_error(e.what(), error, error_size);
+        return 1;
+    }
+}
+}
+
+extern "C" {
+
+// The reference's display transform (src/gpu/display.cu:26 rgba8_kernel for books, tonemap.cu:25 tone_map_kernel for
+// the tone maps; both compiled -fmad=false) on given sums: width * height * 3 doubles in host memory, each channel's
+// sum times `scale` (1 / passes) as session::display computes it for an image of complete passes
+// (renderer.cu:1388-1470). op: 0 books, 1 none, 2 agx, 3 neutral (renderer.h:286-292); exposure in stops, turned
+// into float(2^EV) as session::display does. Writes width * height * 4 bytes. Returns 0, or 1 with the message.
+int ref_gpu_display_bytes(const double* sums, int32_t width, int32_t height, double scale, int32_t op, double exposure,
+                          uint8_t* rgba, char* error, int32_t error_size)
+{
+    double* d_sums = nullptr;
+    uint8_t* d_rgba = nullptr;
+    try
+    {
+        const size_t pixels = static_cast<size_t>(width) * static_cast<size_t>(height);
+        if (cudaMalloc(&d_sums, pixels * 3 * sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&d_rgba, pixels * 4) != cudaSuccess)
+        {
+            throw std::runtime_error("allocating device memory");
+        }
+        if (cudaMemcpy(d_sums, sums, pixels * 3 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        {
+            throw std::runtime_error("copying the sums");
+        }
+        const auto tone = static_cast<gpu::tone_map>(op);
+        if (tone == gpu::tone_map::books)
+        {
+            gpu::detail::to_rgba8(d_sums, width, 0, height, scale, d_rgba);
+        }
+        else
+        {
+            const auto exposure_scale = static_cast<float>(std::exp2(exposure));
+            gpu::detail::to_rgba8_toned(d_sums, width, 0, height, scale, tone, exposure_scale, d_rgba);
+        }
+        if (cudaMemcpy(rgba, d_rgba, pixels * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        {
+            throw std::runtime_error("copying the bytes");
+        }
+        cudaFree(d_sums);
+        cudaFree(d_rgba);
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        cudaFree(d_sums);
+        cudaFree(d_rgba);
         copy_error(e.what(), error, error_size);
         return 1;
     }

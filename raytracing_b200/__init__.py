@@ -271,6 +271,40 @@ class Scene:
             pass
 
 
+TONE_MAPS = {"books": _abi.RT_TONE_BOOKS, "none": _abi.RT_TONE_NONE, "agx": _abi.RT_TONE_AGX,
+             "neutral": _abi.RT_TONE_NEUTRAL}
+
+
+def _display_options(tone: str = "books", exposure: float = 0.0) -> _abi.DisplayOptions:
+    """renderer.h:294-303 display_options: a tone map (TONE_MAPS) and an exposure in stops."""
+    return _abi.DisplayOptions(tone_map=TONE_MAPS[tone], exposure=exposure)
+
+
+def save_image(path: str, pixels: np.ndarray, tone: str = "books", exposure: float = 0.0) -> None:
+    """image::save (image.ixx:170-184): .pfm keeps the linear values, .png the display transform's bytes."""
+    px = np.ascontiguousarray(pixels, dtype=np.float64)
+    h, w, _ = px.shape
+    o = _display_options(tone, exposure)
+    _check(_lib().rt_image_save(str(path).encode(), px.ctypes.data_as(C.POINTER(C.c_double)), w, h, C.byref(o)))
+
+
+def mean_radiance(pixels: np.ndarray) -> float:
+    """image::mean_radiance (image.ixx:93-103): the average of (r + g + b) / 3 over the pixels."""
+    px = np.ascontiguousarray(pixels, dtype=np.float64)
+    h, w, _ = px.shape
+    out = C.c_double()
+    _check(_lib().rt_image_mean_radiance(px.ctypes.data_as(C.POINTER(C.c_double)), w, h, C.byref(out)))
+    return out.value
+
+
+def display_device(sums_ptr: int, width: int, height: int, passes: int, rgba_ptr: int, tone: str = "books",
+                   exposure: float = 0.0, stream: int = 0) -> None:
+    """The display transform of device sums into device bytes (rt_display_device), queued on `stream`."""
+    o = _display_options(tone, exposure)
+    _check(_lib().rt_display_device(C.c_void_p(sums_ptr), width, height, passes, C.byref(o), C.c_void_p(rgba_ptr),
+                                    C.c_void_p(stream or None)))
+
+
 class Session:
     """renderer.h:591-673 session: one view whose image gains passes on demand; its sums stay on the device."""
 
@@ -311,6 +345,23 @@ class Session:
         px = out if out is not None else np.empty((self.height, self.width, 3), dtype=np.float64)
         _check(_lib().rt_session_pixels(self._handle, px.ctypes.data_as(C.POINTER(C.c_double)), px.size))
         return px
+
+    def display(self, tone: str = "books", exposure: float = 0.0) -> np.ndarray:
+        """session::display(options) (renderer.h:623-635): height x width x 4 bytes (RGB and 255)."""
+        out = np.empty((self.height, self.width, 4), dtype=np.uint8)
+        o = _display_options(tone, exposure)
+        _check(_lib().rt_session_display(self._handle, C.byref(o), out.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                         out.size))
+        return out
+
+    def save(self, path: str, tone: str = "books", exposure: float = 0.0) -> None:
+        o = _display_options(tone, exposure)
+        _check(_lib().rt_session_save(self._handle, str(path).encode(), C.byref(o)))
+
+    def mean_radiance(self) -> float:
+        out = C.c_double()
+        _check(_lib().rt_session_mean_radiance(self._handle, C.byref(out)))
+        return out.value
 
     def counters(self) -> dict:
         rays = C.c_uint64()
@@ -424,6 +475,15 @@ class Server:
         if self.poll(request_id)["state"] == "done":
             self._scenes.pop(request_id, None)
         return px
+
+    def display(self, request_id: int, tone: str = "books", exposure: float = 0.0) -> np.ndarray:
+        """The request's frame so far through the display transform: height x width x 4 bytes."""
+        cam = self._scenes[request_id][1]
+        out = np.empty((int(cam.image_height), int(cam.image_width), 4), dtype=np.uint8)
+        o = _display_options(tone, exposure)
+        _check(_lib().rt_server_display(self._handle, request_id, C.byref(o),
+                                        out.ctypes.data_as(C.POINTER(C.c_uint8)), out.size))
+        return out
 
     def cancel(self, request_id: int) -> None:
         _check(_lib().rt_server_cancel(self._handle, request_id))

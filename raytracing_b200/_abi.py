@@ -17,6 +17,7 @@ RT_COMBINE_BSDF_ONLY, RT_COMBINE_LIGHTS_ONLY, RT_COMBINE_POWER_HEURISTIC = range
 RT_MICROFACET_NONE, RT_MICROFACET_CONDUCTOR, RT_MICROFACET_GLOSS = range(3)
 RT_FLOAT32, RT_FLOAT64 = range(2)
 RT_FORM_AUTO, RT_FORM_PERSISTENT, RT_FORM_WAVEFRONT = range(3)
+RT_TONE_BOOKS, RT_TONE_NONE, RT_TONE_AGX, RT_TONE_NEUTRAL = range(4)
 
 
 class Vec3(C.Structure):
@@ -75,6 +76,10 @@ class MicrofacetDesc(C.Structure):
 
 class EnvironmentDesc(C.Structure):
     _fields_ = [("image", ImageDesc), ("yaw_degrees", C.c_double), ("scale", C.c_double)]
+
+
+class DisplayOptions(C.Structure):
+    _fields_ = [("tone_map", C.c_int32), ("pad0", C.c_int32), ("exposure", C.c_double)]
 
 
 class MeshDesc(C.Structure):
@@ -212,6 +217,14 @@ ENTRY_POINTS = [
     ("rt_session_device_sums", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
     ("rt_render_passes_no_alloc", C.c_int, [C.c_void_p, C.POINTER(CameraDesc), C.c_uint64, C.c_int64, C.c_int64,
                                             C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("rt_session_display", C.c_int, [C.c_void_p, C.POINTER(DisplayOptions), C.POINTER(C.c_uint8), C.c_int64]),
+    ("rt_display_device", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int64, C.POINTER(DisplayOptions),
+                                    C.c_void_p, C.c_void_p]),
+    ("rt_image_save", C.c_int, [C.c_char_p, C.POINTER(C.c_double), C.c_int32, C.c_int32,
+                                C.POINTER(DisplayOptions)]),
+    ("rt_image_mean_radiance", C.c_int, [C.POINTER(C.c_double), C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    ("rt_session_save", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(DisplayOptions)]),
+    ("rt_session_mean_radiance", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("rt_session_set_counting", C.c_int, [C.c_void_p, C.c_int32]),
     ("rt_session_fetch_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64 * 4)]),
     ("rt_scene_closest_hits", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64,
@@ -232,6 +245,8 @@ ENTRY_POINTS = [
     ("rt_server_step", C.c_int, [C.c_void_p, C.POINTER(ServerStepReport)]),
     ("rt_server_poll", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(RequestStatus)]),
     ("rt_server_fetch", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_double), C.c_int64]),
+    ("rt_server_display", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(DisplayOptions), C.POINTER(C.c_uint8),
+                                    C.c_int64]),
     ("rt_server_cancel", C.c_int, [C.c_void_p, C.c_int64]),
     ("rt_server_stats_get", C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
 ]

@@ -21,6 +21,9 @@ OUT = PACKAGE / "_lib"
 BUILD = PACKAGE / "_build"
 LIBRARY = OUT / "librt_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Compiled with -fmad=false: the display transform's bytes follow the order its products and sums are written in,
+# as the reference compiles its display units (its CMakeLists.txt:159-165)
+NO_FMAD = {"display.cu"}
 
 
 def nvcc() -> str:
@@ -42,6 +45,8 @@ def _compile(source: Path) -> Path:
     cmd = [nvcc()] + _common_flags()
     if source.suffix == ".cu":
         cmd += ARCH + ["-lineinfo", "-Xptxas", "-warn-spills"]
+        if source.name in NO_FMAD:
+            cmd.append("-fmad=false")
     else:
         cmd += ["-x", "c++"]
     cmd += ["-c", str(source), "-o", str(obj)]

@@ -1,5 +1,6 @@
 // The C-ABI (include/rt_b200.h): every entry point catches what the C++ runtime throws and returns its status, with
 // the message kept per thread for rt_last_error_message().
+#include <cctype>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -7,6 +8,7 @@
 #include <exception>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "host.h"
 #include "scene_store.h"
@@ -272,6 +274,104 @@ rt_status rt_session_device_sums(const rt_session* session, const double** sums,
         need(passes, "passes");
         *sums = session->session->device_sums();
         *passes = session->session->state().passes;
+    });
+}
+
+rt_status rt_session_display(rt_session* session, const rt_display_options* options, uint8_t* rgba,
+                             int64_t byte_count)
+{
+    return guarded([&] {
+        need(session, "session");
+        need(options, "options");
+        need(rgba, "rgba");
+        session->session->display(*options, rgba, byte_count);
+    });
+}
+
+rt_status rt_display_device(const double* device_sums, int32_t width, int32_t height, int64_t passes,
+                            const rt_display_options* options, uint8_t* device_rgba, void* stream)
+{
+    return guarded([&] {
+        need(device_sums, "device_sums");
+        need(options, "options");
+        need(device_rgba, "device_rgba");
+        if (width < 1 || height < 1)
+        {
+            rtb::fail(RT_ERR_INVALID, "an image is at least 1 x 1");
+        }
+        if (passes <= 0)
+        {
+            rtb::fail(RT_ERR_LOGIC, "the image has no complete pass to show");
+        }
+        rtb::launch_display(device_sums, width, height, 1.0 / static_cast<double>(passes), *options, device_rgba,
+                            static_cast<cudaStream_t>(stream));
+    });
+}
+
+rt_status rt_image_save(const char* path, const double* pixels, int32_t width, int32_t height,
+                        const rt_display_options* options)
+{
+    return guarded([&] {
+        need(path, "path");
+        need(pixels, "pixels");
+        const rt_display_options books{};
+        rtb::save_image(path, pixels, width, height, options ? *options : books);
+    });
+}
+
+rt_status rt_image_mean_radiance(const double* pixels, int32_t width, int32_t height, double* mean)
+{
+    return guarded([&] {
+        need(pixels, "pixels");
+        need(mean, "mean");
+        if (width < 1 || height < 1)
+        {
+            rtb::fail(RT_ERR_INVALID, "an image is at least 1 x 1");
+        }
+        *mean = rtb::mean_radiance(pixels, static_cast<int64_t>(width) * height);
+    });
+}
+
+rt_status rt_session_save(rt_session* session, const char* path, const rt_display_options* options)
+{
+    return guarded([&] {
+        need(session, "session");
+        need(path, "path");
+        const rt_display_options books{};
+        const rt_display_options& o = options ? *options : books;
+        rtb::check_display(o);
+        const rt_camera_desc& c = session->session->camera();
+        const size_t n = static_cast<size_t>(c.image_width) * static_cast<size_t>(c.image_height);
+        std::string name(path);
+        std::string ext = name.size() >= 4 ? name.substr(name.size() - 4) : "";
+        for (char& ch : ext)
+        {
+            ch = static_cast<char>(std::tolower(static_cast<unsigned char>(ch)));
+        }
+        if (ext == ".png")
+        {
+            // the bytes the session's display shows (the GPU's, for every tone map)
+            std::vector<uint8_t> rgba(n * 4);
+            session->session->display(o, rgba.data(), static_cast<int64_t>(rgba.size()));
+            rtb::save_png_rgba(path, rgba.data(), c.image_width, c.image_height);
+            return;
+        }
+        std::vector<double> pixels(n * 3);
+        session->session->pixels(pixels.data(), static_cast<int64_t>(pixels.size()));
+        rtb::save_image(path, pixels.data(), c.image_width, c.image_height, o);
+    });
+}
+
+rt_status rt_session_mean_radiance(const rt_session* session, double* mean)
+{
+    return guarded([&] {
+        need(session, "session");
+        need(mean, "mean");
+        const rt_camera_desc& c = session->session->camera();
+        const size_t n = static_cast<size_t>(c.image_width) * static_cast<size_t>(c.image_height);
+        std::vector<double> pixels(n * 3);
+        session->session->pixels(pixels.data(), static_cast<int64_t>(pixels.size()));
+        *mean = rtb::mean_radiance(pixels.data(), static_cast<int64_t>(n));
     });
 }
 

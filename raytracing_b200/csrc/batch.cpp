@@ -54,6 +54,7 @@ batch_engine::~batch_engine()
     wave_.reset();
     arena_.release();
     table_.release();
+    rgba_.release();
     release_graph();
     if (table_host_)
     {
@@ -432,6 +433,30 @@ void batch_engine::pixels(int handle, double* out, int64_t count)
     }
 }
 
+void batch_engine::display(int handle, const rt_display_options& options, uint8_t* out, int64_t count)
+{
+    check_display(options);
+    job& j = *jobs_.at(handle);
+    const int64_t n = int64_t{j.camera.image_width} * j.camera.image_height * 4;
+    if (count != n)
+    {
+        fail(RT_ERR_INVALID, "display: the buffer must hold width * height * 4 bytes");
+    }
+    if (j.passes == 0)
+    {
+        fail(RT_ERR_LOGIC, "the image has no complete pass to show");
+    }
+    if (rgba_.size() < static_cast<size_t>(n))
+    {
+        rgba_.allocate_async(static_cast<size_t>(n), stream_);
+    }
+    launch_display(j.sums.data(), j.camera.image_width, j.camera.image_height, 1.0 / static_cast<double>(j.passes),
+                   options, rgba_.data(), stream_);
+    check(cudaMemcpyAsync(out, rgba_.data(), static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream_),
+          "copying the display's bytes");
+    check(cudaStreamSynchronize(stream_), "converting the image for the display");
+}
+
 uint64_t batch_engine::rays(int handle) const
 {
     unsigned long long v = 0;
@@ -688,6 +713,16 @@ void render_server::fetch(int64_t id, double* pixels, int64_t count)
     }
 }
 
+void render_server::display(int64_t id, const rt_display_options& options, uint8_t* rgba, int64_t count)
+{
+    const auto it = requests_.find(id);
+    if (it == requests_.end() || it->second.handle < 0 || it->second.state == RT_REQUEST_CANCELLED)
+    {
+        fail(RT_ERR_LOGIC, "request " + std::to_string(id) + " has no image");
+    }
+    engine_.display(it->second.handle, options, rgba, count);
+}
+
 void render_server::cancel(int64_t id)
 {
     const auto it = requests_.find(id);
@@ -884,6 +919,17 @@ rt_status rt_server_fetch(rt_server* server, int64_t request_id, double* pixels,
         need(server, "server");
         need(pixels, "pixels");
         server->server->fetch(request_id, pixels, pixel_count);
+    });
+}
+
+rt_status rt_server_display(rt_server* server, int64_t request_id, const rt_display_options* options, uint8_t* rgba,
+                            int64_t byte_count)
+{
+    return guard([&] {
+        need(server, "server");
+        need(options, "options");
+        need(rgba, "rgba");
+        server->server->display(request_id, *options, rgba, byte_count);
     });
 }
 

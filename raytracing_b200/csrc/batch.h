@@ -45,6 +45,8 @@ public:
     void reserve_pool(size_t bytes);
     int64_t passes(int handle) const;
     void pixels(int handle, double* out, int64_t count);
+    // The job's image through the display transform, 4 bytes per pixel into host memory
+    void display(int handle, const rt_display_options& options, uint8_t* out, int64_t count);
     uint64_t rays(int handle) const;
     uint64_t shadow_rays(int handle) const;
     size_t job_bytes(const rt_camera_desc& camera) const;
@@ -85,6 +87,7 @@ private:
     device_array<batch_job> table_;
     device_array<batch_header> header_;
     device_array<unsigned long long> work_counter_;
+    device_array<uint8_t> rgba_; // a job's display bytes, grown on demand
     batch_job* table_host_ = nullptr;   // pinned
     batch_header* header_host_ = nullptr;
     size_t capacity_ = 0;               // jobs the table (and the captured graph) hold
@@ -110,6 +113,7 @@ public:
     rt_server_step_report step();
     rt_request_status poll(int64_t id) const;
     void fetch(int64_t id, double* pixels, int64_t count);
+    void display(int64_t id, const rt_display_options& options, uint8_t* rgba, int64_t count);
     void cancel(int64_t id);
     rt_server_stats stats() const;
 

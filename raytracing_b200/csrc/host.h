@@ -115,6 +115,18 @@ private:
     cudaStream_t stream_ = nullptr; // set when allocated stream-ordered
 };
 
+// The display transform (display.cu): the options' check (renderer.cu:1204-1220) and the kernel over an image's sums
+// times `scale`, queued on `stream`
+constexpr double max_exposure_stops = 24; // renderer.h:303
+void check_display(const rt_display_options& options);
+void launch_display(const double* sums, int width, int height, double scale, const rt_display_options& options,
+                    uint8_t* rgba, cudaStream_t stream);
+// The image files (image_io.cpp): PFM and PNG writers, the mean radiance
+void save_image(const char* path, const double* pixels, int width, int height, const rt_display_options& options);
+double mean_radiance(const double* pixels, int64_t pixel_count);
+// A PNG's bytes already computed (8-bit RGBA, rows from the top) written as an RGB PNG
+void save_png_rgba(const char* path, const uint8_t* rgba, int width, int height);
+
 // Checks a scene's tables before anything is built (the reference's validate, renderer.cu:688-900); throws rt_error
 void validate(const rt_scene_desc& desc);
 
@@ -268,6 +280,9 @@ public:
     double kernel_seconds() const { return kernel_seconds_; }
     rt_kernel_info kernel() const;
     const double* device_sums() const { return sums_.data(); }
+    // session::display(options): the complete passes' bytes, 4 per pixel, into host memory
+    void display(const rt_display_options& options, uint8_t* rgba, int64_t byte_count);
+    int64_t passes() const { return passes_; }
     // The counting build: launches that also count node fetches and primitive tests (slower; for the roofline)
     void set_counting(bool on) { counting_ = on; }
     void fetch_counts(uint64_t out[4]) const;
@@ -284,6 +299,7 @@ private:
     device_array<double> sums_;
     device_array<double> partials_;
     device_array<unsigned long long> counters_; // [0] work, [1] rays, [2] shadow rays, [3..6] the counting build's
+    device_array<uint8_t> rgba_;                 // the display's bytes, grown on demand
     bool counting_ = false;
     int64_t passes_ = 0;
     double kernel_seconds_ = 0;

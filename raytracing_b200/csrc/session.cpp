@@ -61,6 +61,7 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
 session::~session()
 {
     wave_.reset(); // its arrays are freed on the stream, before it goes
+    rgba_.release();
     partials_.release();
     sums_.release();
     counters_.release();
@@ -287,6 +288,30 @@ void session::pixels(double* out, int64_t count) const
     {
         out[i] *= scale;
     }
+}
+
+void session::display(const rt_display_options& options, uint8_t* rgba, int64_t byte_count)
+{
+    check_display(options);
+    const int64_t n = static_cast<int64_t>(camera_.image_width) * camera_.image_height * 4;
+    if (byte_count != n)
+    {
+        fail(RT_ERR_INVALID, "display: the buffer must hold width * height * 4 bytes");
+    }
+    if (passes_ == 0)
+    {
+        fail(RT_ERR_LOGIC, "the image has no complete pass to show");
+    }
+    if (rgba_.size() < static_cast<size_t>(n))
+    {
+        rgba_.allocate_async(static_cast<size_t>(n), stream_);
+    }
+    // 1 / passes, as pixels() scales: a books byte equals the CPU writer's byte of the same pixel
+    launch_display(sums_.data(), camera_.image_width, camera_.image_height, 1.0 / static_cast<double>(passes_), options,
+                   rgba_.data(), stream_);
+    check(cudaMemcpyAsync(rgba, rgba_.data(), static_cast<size_t>(n), cudaMemcpyDeviceToHost, stream_),
+          "copying the display's bytes");
+    check(cudaStreamSynchronize(stream_), "converting the image for the display");
 }
 
 uint64_t session::rays() const

@@ -50,7 +50,7 @@ STRUCTS = {
     "rt_builtin_params": _abi.BuiltinParams, "rt_batch_job": _abi.BatchJob, "rt_batch_options": _abi.BatchOptions,
     "rt_batch_report": _abi.BatchReport, "rt_server_options": _abi.ServerOptions,
     "rt_request_status": _abi.RequestStatus, "rt_server_step_report": _abi.ServerStepReport,
-    "rt_server_stats": _abi.ServerStats,
+    "rt_server_stats": _abi.ServerStats, "rt_display_options": _abi.DisplayOptions,
 }
 
 
