@@ -14,6 +14,12 @@ Arms:
 
 One process per GPU under torchrun: every rank renders its own independent image (its own seed) of the same
 workload, so per-GPU work is fixed as N grows (weak scaling); the step times are max-reduced over ranks.
+
+After the timed region (rank 0, untimed): the last timed image is checked at its full size against the reference's
+own renderer (ImageCompare, `parity`) and both images' error against the FP64 65,536-spp oracle render is reported;
+the same workload under NEE with power-heuristic MIS is measured and checked the same way (`nee_mis`); one more render
+with CUDA events around every kernel gives the dominant kernel's roofline; then the triangle mesh, the 64 batched jobs
+(each job ImageCompared with a plain render) and the served stream.
 """
 from __future__ import annotations
 
@@ -50,7 +56,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU-baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--extra", action="store_true", help="also measure the NEE/MIS integrator on the same scene")
+    p.add_argument("--no-mis", action="store_true", help="skip the NEE/MIS integrator on the same workload")
     p.add_argument("--no-batched", action="store_true", help="skip the 64-job batched measurement")
     p.add_argument("--no-reference-gpu", action="store_true",
                    help="skip timing the reference's own CUDA renderer on the same workload")
@@ -134,16 +140,137 @@ def read_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def read_traffic() -> float | None:
-    """DRAM bytes per path segment of the workload's kernels (the wavefront's shade and trace kernels), from the
-    committed ncu summary (profiles/)."""
-    path = REPO / "profiles" / "wavefront_glass.md"
+# The wavefront's state per unit of work, by the layout of its slots and queues (raytracing_b200/csrc/kernels.cu): what
+# the shade kernel must move through HBM for each segment (the slot's seven 16-byte rows in and out, the walk's answer,
+# the next query of 48 bytes), for each shadow ray (its answer, its three rows out and back in, its query) and for each
+# sample (its value). These are the bytes that bind the shade kernel: the scene itself (a few KB) is read from L1.
+SHADE_BYTES_PER_SEGMENT = 2 * 7 * 16 + 16 + 48
+SHADE_BYTES_PER_SHADOW_RAY = 4 + 2 * 3 * 16 + 48
+SHADE_BYTES_PER_SAMPLE = 16
+# FP32 operations per primitive test and per node visit (slab test: 6 FMA + 6 min/max), the trace kernels' arithmetic
+FLOPS_PER_NODE, FLOPS_PER_SPHERE, FLOPS_PER_QUAD, FLOPS_PER_TRIANGLE = 12, 20, 25, 30
+
+
+def roofline_of(times: dict, counts: dict, samples: int, fetched: dict, counted: int, scene_bytes_per_query: float,
+                peaks: dict, fp32_peak: float, render_seconds: float) -> dict:
+    """The roofline of the render's dominant kernel, from per-kernel CUDA-event times of one render of the workload.
+    The wavefront's shade kernel is bound by HBM on the slot state it streams; the trace kernel (and the persistent
+    kernel) by FP32 arithmetic on the scene's primitives, which sit in L1."""
+    active = {k: v for k, v in times.items() if v[1] > 0 and v[0] > 0}
+    total = sum(v[0] for v in active.values())
+    dominant = max(active, key=lambda k: active[k][0])
+    rays, shadow = counts["rays"], counts["shadow_rays"]
+    queries = rays + shadow
+    flops_per_query = (FLOPS_PER_NODE * fetched["nodes"] + FLOPS_PER_SPHERE * fetched["spheres"] +
+                       FLOPS_PER_QUAD * fetched["quads"] + FLOPS_PER_TRIANGLE * fetched["triangles"]) / max(counted, 1)
+    kernels = {k: {"seconds": v[0], "launches": v[1], "avg_launch_us": 1e6 * v[0] / v[1], "share": v[0] / total}
+               for k, v in active.items()}
+
+    def fp32_roof(kind: str) -> dict:
+        sec = active[kind][0]
+        achieved = flops_per_query * queries / sec / 1e12
+        return {"bound": "fp32", "kernel": kind, "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "flops_per_query": flops_per_query,
+                "peak_source": "measured here: FP32 GEMM through cuBLAS, TF32 off"}
+
+    if dominant == "shade":
+        state = rays * SHADE_BYTES_PER_SEGMENT + shadow * SHADE_BYTES_PER_SHADOW_RAY + samples * SHADE_BYTES_PER_SAMPLE
+        sec = active["shade"][0]
+        achieved = state / sec / 1e9
+        out = {"bound": "hbm", "kernel": "wave_shade_kernel", "achieved": achieved, "peak": peaks["hbm_gbs"],
+               "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+               "peak_source": peaks["source"], "algorithmic_bytes_per_segment": state / rays,
+               "algorithmic_bytes_per_launch": state / active["shade"][1],
+               "note": "the slot state the shade kernel streams per segment (rows in and out, answer, next query), "
+                       "per shadow ray and per sample, over its CUDA-event time; the scene's own bytes "
+                       f"({scene_bytes_per_query:.0f} per query) are served from L1. DRAM traffic per launch is in "
+                       "the committed ncu summary under profiles/"}
+        if "trace" in active:
+            out["trace_kernel"] = fp32_roof("trace")
+    else:
+        out = fp32_roof(dominant)
+        out["traffic"] = None
+    out["kernels"] = kernels
+    out["events_total_over_render"] = total / render_seconds
+    return out
+
+
+GOLDEN = REPO / "tests" / "golden"
+
+
+def trimmed_rms(a: np.ndarray, b: np.ndarray, trim: float = 0.01) -> tuple[float, float]:
+    """PfmStats' RMS of the channel average's difference (tests/pfm_stats.cpp:344-367): (trimmed, full), the trimmed
+    one leaving out the largest share `trim` of the squared differences (fireflies, lamp edges)."""
+    d = a.mean(axis=2) - b.mean(axis=2)
+    d2 = np.sort((d * d).ravel())
+    drop = int(np.floor(d2.size * trim))
+    return float(np.sqrt(d2[: d2.size - drop].mean())), float(np.sqrt(d2.mean()))
+
+
+def error_vs_fp64(name: str, images: dict) -> dict:
+    """Each image's error against the FP64 high-spp oracle render of the same scene and view (tests/golden/fp64_*.npz,
+    made by tests/golden/make_fp64_oracle.py): PfmStats' trimmed RMS, and the ratio of this library's error to the
+    reference renderer's at the same spp and strategy ("matched" within 5%)."""
+    path = GOLDEN / f"fp64_{name}.npz"
     if not path.exists():
-        return None
-    for line in path.read_text().splitlines():
-        if line.startswith("dram_bytes_per_segment:"):
-            return float(line.split(":", 1)[1].split()[0])
-    return None
+        return {"unavailable": f"{path.name} is missing (tests/golden/make_fp64_oracle.py makes it)"}
+    z = np.load(path)
+    oracle_img = z["image"].astype(np.float64)
+    out = {"oracle": f"{z['renderer']}, {int(z['width'])}x{int(z['height'])}, {int(z['passes'])} passes",
+           "metric": "RMS of the channel average's difference, trimmed by 1% (PfmStats)"}
+    for key, img in images.items():
+        if img is None or img.shape != oracle_img.shape:
+            continue
+        t, full = trimmed_rms(img, oracle_img)
+        out[key] = {"trimmed_rms": t, "rms": full}
+    if "this_library" in out and "reference_gpu" in out:
+        ratio = out["this_library"]["trimmed_rms"] / out["reference_gpu"]["trimmed_rms"]
+        out["ratio"] = ratio
+        out["matched"] = bool(abs(ratio - 1.0) <= 0.05)
+    return out
+
+
+def image_parity(reference_fn, ours: np.ndarray, seeds=(6, 7)) -> dict:
+    """ImageCompare (src/image_compare.cpp, restated in the oracle) between this library's image and an independent
+    render of the same scene, spp and strategy by the reference's renderer; a failure is re-run once with a fresh seed
+    (the reference's re-run rule)."""
+    from oracle import binding as oracle
+
+    attempts = []
+    for seed in seeds:
+        r = oracle.image_compare(reference_fn(seed), ours)
+        attempts.append({"verdict": "consistent" if r["verdict"] == 0 else "different",
+                         "whole_image_z": r["whole_image_z"], "all_tiles_z": r["all_tiles_z"],
+                         "largest_tile_z": r["largest_tile_z"], "tiles_over_3": r["tiles_over_3"],
+                         "tested_tiles": r["tested_tiles"],
+                         "thresholds": [r["threshold_whole_image"], r["threshold_all_tiles"],
+                                        r["threshold_largest_tile"], r["threshold_tiles_over_3"]]})
+        if r["verdict"] == 0:
+            break
+    return {"verdict": attempts[-1]["verdict"], "attempts": attempts}
+
+
+def fp32_peak_tflops(torch) -> float:
+    """The FP32 (non-tensor) arithmetic peak measured on this GPU: a plain FP32 GEMM through cuBLAS with TF32 off,
+    8192^3, the best of five after warm-up."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, device="cuda", dtype=torch.float32)
+    b = torch.randn(8192, 8192, device="cuda", dtype=torch.float32)
+    for _ in range(2):
+        torch.mm(a, b)
+    best = 0.0
+    for _ in range(5):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.mm(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * 8192 ** 3 / (s.elapsed_time(e) / 1000.0) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    return best
 
 
 def cpu_baseline(scene, args, threads: int) -> dict:
@@ -156,7 +283,7 @@ def cpu_baseline(scene, args, threads: int) -> dict:
     # threads
     _, probe = oracle.render(scene.desc, scene.width, h, seed=11, passes=args.spp, threads=threads,
                              row_begin=mid, row_end=mid + 1)
-    rows = int(max(1, min(h, threads * args.cpu_seconds / max(probe["seconds"], 1e-3))))
+    rows = int(min(h, threads * max(1, int(args.cpu_seconds / max(probe["seconds"], 1e-3)))))
     begin = max(0, mid - rows // 2)
     _, stats = oracle.render(scene.desc, scene.width, h, seed=12, passes=args.spp, threads=threads,
                              row_begin=begin, row_end=begin + rows)
@@ -175,9 +302,9 @@ def reference_gpu_measurement(scene_desc, passes: int, value: float) -> dict:
         return {"unavailable": "oracle/_ref/libref_gpu.so was not built (needs the reference's sources)"}
     w, h = scene_desc.width, scene_desc.height
     ref_gpu.render(scene_desc.desc, w, h, seed=5, passes=16)  # warm-up: module load, allocations
-    _, info = ref_gpu.render(scene_desc.desc, w, h, seed=6, passes=passes)
+    image, info = ref_gpu.render(scene_desc.desc, w, h, seed=6, passes=passes)
     segments_per_s = info["rays"] / info["kernel_seconds"]
-    return {"segments_per_s": segments_per_s, "e2e_segments_per_s": info["rays"] / info["seconds"],
+    return {"image": image, "segments_per_s": segments_per_s, "e2e_segments_per_s": info["rays"] / info["seconds"],
             "kernel": info["kernel"], "registers": info["registers"],
             "blocks_per_multiprocessor": info["blocks_per_multiprocessor"],
             "segments_per_sample": info["rays"] / (w * h * passes),
@@ -210,6 +337,37 @@ def mesh_measurement(rt, torch) -> dict:
         sess.close()
     out["wavefront_over_persistent"] = out["wavefront"]["segments_per_s"] / out["persistent"]["segments_per_s"]
     return out
+
+
+def mis_measurement(rt, torch, args, steps: int, seed: int) -> tuple[dict, np.ndarray]:
+    """The same workload under NEE with power-heuristic MIS (the quality integrator; the reference's quality kernel,
+    src/gpu/quality.cu): the glass Cornell box at the same size, spp and depth, its lamp the light NEE samples.
+    Device-timed renders from zero with the scene resident; returns the measurement and the last image."""
+    desc = rt.builtin_scene("cornell-mis", width=args.width, spp=args.spp, depth=args.depth)
+    passes = desc.round_passes if args.spp <= 0 else args.spp
+    sess = rt.Session(rt.Scene(desc), seed=seed, launch_seconds=0.5)
+    sess.render_to(min(passes, 64))  # warm-up: buffers, module load
+    seconds = 0.0
+    rays = shadow = launches = 0
+    for _ in range(steps):
+        sess.set_camera(desc.camera)
+        torch.cuda.synchronize()
+        rep = sess.render_to(passes)
+        c = sess.counters()
+        seconds += rep["gpu_seconds"]
+        rays += c["rays"]
+        shadow += c["shadow_rays"]
+        launches += rep["kernel_launches"]
+    image = sess.pixels()
+    samples = steps * passes * desc.width * desc.height
+    out = {"workload": f"cornell-mis (the glass box, NEE + power-heuristic MIS), {desc.width}x{desc.height}, "
+                       f"{passes} spp, depth {desc.camera.max_depth}",
+           "segments_per_s": rays / seconds, "shadow_rays_per_s": shadow / seconds,
+           "queries_per_s": (rays + shadow) / seconds, "ms_per_render": 1000 * seconds / steps, "renders": steps,
+           "segments_per_sample": rays / samples, "shadow_rays_per_sample": shadow / samples,
+           "kernel": sess.kernel(), "gpu_launches_per_render": launches // steps}
+    sess.close()
+    return out, image, desc, passes
 
 
 def log_uniform(rng, lo: float, hi: float) -> float:
@@ -248,6 +406,11 @@ def batched_measurement(rt, torch, rank: int = 0, world: int = 1) -> dict:
     plain_rays = 0
     identical = 0
     max_diff = 0.0
+    consistent = 0
+    reruns = 0
+    worst_z = 0.0
+    from oracle import binding as oracle
+
     for (scene, seed, passes), img in zip(jobs, b.images):
         t0 = time.perf_counter()
         r = rt.render(scene, seed=seed, passes=passes)
@@ -256,6 +419,15 @@ def batched_measurement(rt, torch, rank: int = 0, world: int = 1) -> dict:
         plain_rays += r.rays
         identical += int(np.array_equal(r.pixels, img))
         max_diff = max(max_diff, abs(float(img.mean()) - float(r.pixels.mean())) / max(float(r.pixels.mean()), 1e-9))
+        # Per-job ImageCompare against a plain render with an independent seed (untimed); one re-run on an alarm
+        for attempt in range(2):
+            other = rt.render(scene, seed=seed + 100_000 * (attempt + 1), passes=passes).pixels
+            cmp = oracle.image_compare(other, img)
+            if cmp["verdict"] == 0:
+                consistent += 1
+                worst_z = max(worst_z, abs(cmp["whole_image_z"]))
+                break
+            reruns += 1
     pixels = sum(s.width * s.height for s, _, _ in all_jobs)
     samples = sum(costs)
     batch_gpu, batch_rays = shard.combine(b.gpu_seconds, b.rays)
@@ -263,6 +435,7 @@ def batched_measurement(rt, torch, rank: int = 0, world: int = 1) -> dict:
     plain_kernel, plain_rays = shard.combine(plain_kernel, plain_rays)
     plain_wall, _ = shard.combine(plain_wall, 0)
     _, identical = shard.combine(0, identical)
+    _, consistent = shard.combine(0, consistent)
     reference = {}
     from oracle import ref_gpu
 
@@ -291,6 +464,10 @@ def batched_measurement(rt, torch, rank: int = 0, world: int = 1) -> dict:
             "speedup_gpu": (batch_rays / batch_gpu) / (plain_rays / plain_kernel),
             "speedup_e2e": plain_wall / batch_wall,
             "jobs_bit_identical_to_plain": f"{int(identical)}/{len(all_jobs)}",
+            "jobs_image_compare_consistent_with_plain": f"{int(consistent)}/{len(all_jobs)}",
+            "image_compare_reruns": reruns, "largest_whole_image_z": worst_z,
+            "image_compare_note": "each job against a plain render of the same scene and passes with an independent "
+                                  "seed, one re-run on an alarm (the reference's rule)",
             "max_relative_mean_difference_to_plain": max_diff}
 
 
@@ -422,7 +599,9 @@ def run_reference(args):
                              row_end=mid + 1)
     # Each step is a band of rows of about 2 s on all threads (one row per thread at a time), so that warm-up +
     # steps end within a few minutes
-    rows = int(max(1, min(h, threads * 2.0 / max(probe["seconds"], 1e-3))))
+    # A whole number of rows per thread (rows are the unit of threading), so no thread idles in the last round
+    per_thread = max(1, int(2.0 / max(probe["seconds"], 1e-3)))
+    rows = int(min(h, threads * per_thread))
     begin = max(0, mid - rows // 2)
     for w in range(args.warmup):
         oracle.render(scene.desc, scene.width, h, seed=100 + w, passes=args.spp, threads=threads, row_begin=begin,
@@ -520,23 +699,23 @@ def run_b200(args):
         kernel_launches += report["kernel_launches"]
     clock_info = clocks.stop()
     del rays0
+    timed_image = session.pixels()  # the last timed render (every step renders the same seed), for the parity check
+
+    # Per-kernel times of the same workload (untimed: CUDA events around every kernel), for the roofline
+    session.set_timing(True)
+    session.set_camera(camera)
+    profiled = session.render_to(passes)
+    kernel_times = session.kernel_times()
+    prof_counts = session.counters()
+    session.set_timing(False)
     # the slowest rank's time, every rank's segments (no collective on the data path: each rank's image is its own)
     step_seconds, all_rays = shard.combine(sum(times), total_rays)
     value = all_rays / step_seconds
 
     peaks = read_peaks()
-    achieved_gbs = bytes_per_segment * (total_rays + total_shadow) / kernel_seconds / 1e9
-    traffic_per_segment = read_traffic()
-    launches_avg_segments = (total_rays + total_shadow) / max(launches, 1)
-    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved_gbs / peaks["hbm_gbs"],
-                "traffic": traffic_per_segment * launches_avg_segments if traffic_per_segment else None,
-                "peak_source": peaks["source"],
-                "algorithmic_bytes_per_segment": bytes_per_segment,
-                "note": "BVH node (64 B) and primitive (16/48 B) fetches per closest-hit or shadow query, counted on "
-                        "this workload's rays; they are served from L1/L2, not HBM. The DRAM traffic (`traffic`, "
-                        "per launch) is the wavefront's slot state and queues, about 237 B per segment; the kernels "
-                        "are bound by latency and divergent issue"}
+    fp32_peak = fp32_peak_tflops(torch)
+    roofline = roofline_of(kernel_times, prof_counts, passes * scene.width * scene.height, fetched,
+                           segments_counted, bytes_per_segment, peaks, fp32_peak, profiled["gpu_seconds"])
 
     line = None
     if rank == 0:
@@ -584,27 +763,37 @@ def run_b200(args):
                            "path": "raytracing_b200.render -> rt_render (validate, BVH build, upload, launches, "
                                    "download of width*height*3 doubles)"}
 
-    if rank == 0 and args.extra:
-        mis_desc = rt.builtin_scene("cornell-mis", width=args.width, spp=args.spp, depth=args.depth)
-        mis = rt.Session(rt.Scene(mis_desc), seed=seed, launch_seconds=0.5)
-        mis.render_to(min(passes, 64))
-        mis.set_camera(mis_desc.camera)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        rep = mis.render_to(passes)
-        torch.cuda.synchronize()
-        cnt = mis.counters()
-        line["extra"] = {"cornell_glass_nee_mis": {
-            "segments_per_s": cnt["rays"] / rep["gpu_seconds"],
-            "shadow_rays_per_s": cnt["shadow_rays"] / rep["gpu_seconds"],
-            "queries_per_s": (cnt["rays"] + cnt["shadow_rays"]) / rep["gpu_seconds"],
-            "segments_per_sample": cnt["rays"] / (passes * mis.width * mis.height),
-            "shadow_rays_per_sample": cnt["shadow_rays"] / (passes * mis.width * mis.height),
-            "wall_s": time.perf_counter() - t0}}
-        mis.close()
+    mis = mis_image = mis_desc = None
+    if rank == 0 and not args.no_mis:
+        mis, mis_image, mis_desc, mis_passes = mis_measurement(rt, torch, args, max(1, min(args.steps, 3)), seed)
+        line["nee_mis"] = mis
 
     if rank == 0 and not args.no_reference_gpu:
-        line["reference_gpu"] = reference_gpu_measurement(scene_desc, passes, line["value"])
+        ref = reference_gpu_measurement(scene_desc, passes, line["value"])
+        ref_image = ref.pop("image", None)
+        line["reference_gpu"] = ref
+        # Parity of the timed image at its full size: ImageCompare against the reference's own renderer (the same
+        # scene tables, spp and strategy, another seed), and both images' error against the FP64 oracle render
+        if ref_image is not None:
+            from oracle import ref_gpu
+
+            w, h = scene.width, scene.height
+            line["parity"] = {
+                "workload": line["config"]["workload"],
+                "image_compare_vs_reference": image_parity(
+                    lambda sd: ref_image if sd == 6 else ref_gpu.render(scene_desc.desc, w, h, seed=sd,
+                                                                         passes=passes)[0], timed_image),
+                "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": timed_image,
+                                                            "reference_gpu": ref_image})}
+            if mis is not None:
+                mis_ref_fn = lambda sd: ref_gpu.render(mis_desc.desc, mis_desc.width, mis_desc.height,  # noqa: E731
+                                                       seed=sd, passes=mis_passes)[0]
+                mis_ref = mis_ref_fn(8)
+                mis["parity"] = {
+                    "image_compare_vs_reference": image_parity(lambda sd: mis_ref if sd == 8 else mis_ref_fn(sd),
+                                                               mis_image, seeds=(8, 9)),
+                    "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": mis_image,
+                                                                "reference_gpu": mis_ref})}
     if rank == 0 and not args.no_mesh:
         line["mesh"] = mesh_measurement(rt, torch)
     if not args.no_batched:

@@ -341,10 +341,14 @@ rt_status rt_session_kernel(const rt_session* session, rt_kernel_info* info);
  * per-chunk partial sums) comes from a fixed 64 MiB array in the library's device image instead: an image may have
  * at most 2,796,192 pixels once padded to 8x4 tiles (about 1920x1440), larger ones return RT_ERR_CAPACITY. Every GPU
  * that loads the library holds that array until the process exits. The first call on a device looks up the array's
- * address (cudaGetSymbolAddress) with that device current, so make that first call before any stream capture. Every
- * call shares the array and leaves its contents behind; calls are synchronous, and two calls that overlap on the GPU
- * (from two host threads) race. Passes are rendered in the same chunks as a session's, so the sums equal a
- * session's render of the same seed and passes bit for bit. rays / shadow_rays (may be NULL): this call's counts. */
+ * address (cudaGetSymbolAddress) with that device current and creates the device's stream for these calls (a
+ * non-blocking stream: a call neither waits for nor delays the caller's streams), so make that first call before any
+ * stream capture. Every call shares the array and leaves its contents behind; calls are synchronous (each waits for
+ * its own stream), and two calls that overlap on the GPU (from two host threads) race. Passes are rendered in
+ * launches of whole 16-pass chunks, aligned to multiples of 16 as a session aligns its launches: when pass_begin and
+ * pass_end fall on multiples of 16 (or on the boundaries a session's launches used), the sums equal that session's
+ * render of the same seed and passes bit for bit; a range that starts or ends inside a chunk sums that chunk in two
+ * parts, equal to the session's to rounding. rays / shadow_rays (may be NULL): this call's counts. */
 rt_status rt_render_passes_no_alloc(rt_scene* scene, const rt_camera_desc* camera, uint64_t seed, int64_t pass_begin,
                                     int64_t pass_end, double* device_sums, uint64_t* rays, uint64_t* shadow_rays);
 
@@ -397,6 +401,19 @@ rt_status rt_session_mean_radiance(const rt_session* session, double* mean);
 /* Device-resident variant for callers that keep the image on the GPU (a served frame, a display transform):
  * the device address of the per-pixel sums (3 doubles per pixel, rows from the top) and of the pass count. */
 rt_status rt_session_device_sums(const rt_session* session, const double** sums, int64_t* passes);
+
+/* Per-kernel timing (no counterpart in the reference, whose render_result gives the launches' total only): while on,
+ * every kernel a launch runs is bracketed by CUDA events on the session's stream and its time added to its kind's
+ * total: [0] the persistent render kernel, [1] the wavefront's shade kernel, [2] its trace kernel, [3] the
+ * reductions. Off by default (the events cost a few microseconds a kernel); totals since the view was set. */
+enum { RT_KERNEL_RENDER = 0, RT_KERNEL_SHADE = 1, RT_KERNEL_TRACE = 2, RT_KERNEL_REDUCE = 3 };
+typedef struct rt_kernel_times
+{
+    double seconds[4];
+    int64_t launches[4];
+} rt_kernel_times;
+rt_status rt_session_set_timing(rt_session* session, int32_t on);
+rt_status rt_session_kernel_times(const rt_session* session, rt_kernel_times* times);
 
 /* The counting build (no counterpart in the reference): while on, launches also count BVH node fetches and sphere,
  * quad and triangle tests (closest-hit and shadow traversals together), the measured work behind the roofline's

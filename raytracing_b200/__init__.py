@@ -375,6 +375,18 @@ class Session:
         _check(_lib().rt_session_kernel(self._handle, C.byref(k)))
         return _kernel_dict(k)
 
+    def set_timing(self, on: bool) -> None:
+        """Per-kernel timing: CUDA events around every kernel of every launch (slows launches a little)."""
+        _check(_lib().rt_session_set_timing(self._handle, 1 if on else 0))
+
+    def kernel_times(self) -> dict:
+        """{kind: (seconds, launches)} for the persistent render, shade, trace and reduction kernels since the view
+        was set (with timing on)."""
+        t = _abi.KernelTimes()
+        _check(_lib().rt_session_kernel_times(self._handle, C.byref(t)))
+        return {name: (t.seconds[k], int(t.launches[k])) for k, name in enumerate(("render", "shade", "trace",
+                                                                                      "reduce"))}
+
     def set_counting(self, on: bool) -> None:
         _check(_lib().rt_session_set_counting(self._handle, 1 if on else 0))
 

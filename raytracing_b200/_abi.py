@@ -82,6 +82,10 @@ class DisplayOptions(C.Structure):
     _fields_ = [("tone_map", C.c_int32), ("pad0", C.c_int32), ("exposure", C.c_double)]
 
 
+class KernelTimes(C.Structure):
+    _fields_ = [("seconds", C.c_double * 4), ("launches", C.c_int64 * 4)]
+
+
 class MeshDesc(C.Structure):
     _fields_ = [("positions", C.POINTER(C.c_float)), ("vertex_count", C.c_int64),
                 ("indices", C.POINTER(C.c_uint32)), ("triangle_count", C.c_int64), ("material", C.c_int32),
@@ -225,6 +229,8 @@ ENTRY_POINTS = [
     ("rt_image_mean_radiance", C.c_int, [C.POINTER(C.c_double), C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
     ("rt_session_save", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(DisplayOptions)]),
     ("rt_session_mean_radiance", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    ("rt_session_set_timing", C.c_int, [C.c_void_p, C.c_int32]),
+    ("rt_session_kernel_times", C.c_int, [C.c_void_p, C.POINTER(KernelTimes)]),
     ("rt_session_set_counting", C.c_int, [C.c_void_p, C.c_int32]),
     ("rt_session_fetch_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64 * 4)]),
     ("rt_scene_closest_hits", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64,

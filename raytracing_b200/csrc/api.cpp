@@ -375,6 +375,23 @@ rt_status rt_session_mean_radiance(const rt_session* session, double* mean)
     });
 }
 
+rt_status rt_session_set_timing(rt_session* session, int32_t on)
+{
+    return guarded([&] {
+        need(session, "session");
+        session->session->set_timing(on != 0);
+    });
+}
+
+rt_status rt_session_kernel_times(const rt_session* session, rt_kernel_times* times)
+{
+    return guarded([&] {
+        need(session, "session");
+        need(times, "times");
+        *times = session->session->kernel_times();
+    });
+}
+
 rt_status rt_session_set_counting(rt_session* session, int32_t on)
 {
     return guarded([&] {

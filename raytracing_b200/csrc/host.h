@@ -280,6 +280,9 @@ public:
     double kernel_seconds() const { return kernel_seconds_; }
     rt_kernel_info kernel() const;
     const double* device_sums() const { return sums_.data(); }
+    // Per-kernel timing (events around every kernel of every launch; slows launches a little): rt_kernel_times
+    void set_timing(bool on) { timing_ = on; }
+    rt_kernel_times kernel_times() const { return times_; }
     // session::display(options): the complete passes' bytes, 4 per pixel, into host memory
     void display(const rt_display_options& options, uint8_t* rgba, int64_t byte_count);
     int64_t passes() const { return passes_; }
@@ -314,6 +317,12 @@ private:
     std::unique_ptr<wave_runner> wave_;
     int32_t last_kernel_launches_ = 0; // the last launch's kernels
     int trace_grid_ = 0;
+
+    // Per-kernel timing: a pool of events, grown as launches need them
+    bool timing_ = false;
+    rt_kernel_times times_{};
+    std::vector<cudaEvent_t> marks_;
+    cudaEvent_t* marks(size_t count);
 
     // Renders passes [passes_, end) in one launch and its reduction; returns its GPU seconds
     double launch(int64_t end);

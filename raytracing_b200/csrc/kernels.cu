@@ -3310,8 +3310,10 @@ wave_trace_function wave_flat_trace_of(bool features)
 }
 } // namespace
 
+// marks (when given): three events recorded before the shade kernel, between the two kernels and after the trace
+// kernel, for per-kernel timing
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& slots, int trace_grid,
-                             cudaStream_t stream)
+                             cudaStream_t stream, const cudaEvent_t* marks)
 {
     wave_buffers b = slots; // with the launch's camera and RNG job, for the camera rays the trace kernel makes
     b.cam = p.cam;
@@ -3322,11 +3324,19 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
         return e;
     }
     const bool features = has_features(p.scene);
+    if (marks)
+    {
+        cudaEventRecord(marks[0], stream);
+    }
     wave_shade_of(quality, features)<<<b.slot_count / render_block, render_block, 0, stream>>>(p, b, wave_batch{});
     e = cudaGetLastError();
     if (e != cudaSuccess)
     {
         return e;
+    }
+    if (marks)
+    {
+        cudaEventRecord(marks[1], stream);
     }
     if (p.scene.flat != 0)
     {
@@ -3338,7 +3348,12 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
         wave_trace_of(features, p.scene.wide_nodes != nullptr)<<<trace_grid, render_block, 0, stream>>>(
             p.scene, b, wave_batch{}, p.counters);
     }
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (marks && e == cudaSuccess)
+    {
+        cudaEventRecord(marks[2], stream);
+    }
+    return e;
 }
 
 cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, const wave_buffers& b,

@@ -178,7 +178,8 @@ size_t wave_slot_bytes();
 cudaError_t clear_wave_slots(const wave_buffers& b, cudaStream_t stream);
 // One step: clears the queue, the shade kernel over the slots, the trace kernel (trace_grid blocks) over the queue
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
-                             cudaStream_t stream);
+                             cudaStream_t stream,
+                             const cudaEvent_t* marks = nullptr);
 // The samples of passes [pass_begin, pass_end) into the sums (chunk partials in pass order, added in chunk order)
 cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
                                int32_t chunk, cudaStream_t stream);

@@ -11,8 +11,10 @@
 // The scratch lives in a file-scope __device__ array. Every GPU that loads the library holds it until the process
 // exits, and every call shares it: its contents are the last call's. Host code cannot use the array's name as a
 // device address, so the first call on each device looks the address up with cudaGetSymbolAddress, with that device
-// current, and passes it to the kernels. Calls are synchronous; two calls that overlap on the GPU (from two host
-// threads) would race on the shared scratch.
+// current, and passes it to the kernels. That first call also creates the device's stream for these calls (a
+// non-blocking stream, so a call neither waits for nor holds up the caller's other streams; creating it allocates no
+// device memory). Calls are synchronous: each waits for its own work on that stream before it returns. Two calls
+// that overlap on the GPU (from two host threads) would race on the shared scratch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,9 +38,10 @@ static __device__ __align__(256) unsigned char no_alloc_scratch[scratch_bytes];
 constexpr int max_devices = 64;
 std::mutex setup_mutex;
 unsigned char* scratch_address[max_devices] = {};
+cudaStream_t scratch_stream[max_devices] = {};
 
-// The scratch's device address on `device` (current): looked up once per device
-unsigned char* scratch_on(int device)
+// The scratch's device address on `device` (current) and the device's stream for these calls: set up once per device
+unsigned char* scratch_on(int device, cudaStream_t& stream)
 {
     if (device < 0 || device >= max_devices)
     {
@@ -49,8 +52,12 @@ unsigned char* scratch_on(int device)
     {
         void* p = nullptr;
         rtb::check(cudaGetSymbolAddress(&p, no_alloc_scratch), "looking up the no-allocation scratch");
+        cudaStream_t s = nullptr;
+        rtb::check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "creating the no-allocation stream");
+        scratch_stream[device] = s;
         scratch_address[device] = static_cast<unsigned char*>(p);
     }
+    stream = scratch_stream[device];
     return scratch_address[device];
 }
 } // namespace
@@ -90,14 +97,14 @@ extern "C" rt_status rt_render_passes_no_alloc(rt_scene* scene, const rt_camera_
                                            std::to_string(partial_entries) + " (64 MiB)");
         }
         rtb::check(cudaSetDevice(s.device()), "selecting the scene's device");
-        unsigned char* scratch = scratch_on(s.device());
+        cudaStream_t stream = nullptr;
+        unsigned char* scratch = scratch_on(s.device(), stream);
         auto* counters = reinterpret_cast<unsigned long long*>(scratch);
         auto* partials = reinterpret_cast<double*>(scratch + counter_bytes);
         rtb::kernel_attributes a{};
         rtb::check(rtb::render_attributes(s.view(), s.quality(), a), "querying the render kernel");
         const int grid = a.multiprocessors * (a.blocks_per_sm > 0 ? a.blocks_per_sm : 1);
         const int64_t max_chunks = partial_entries / padded;
-        const cudaStream_t stream = nullptr;
         // The ray counters start at zero for this call; the work counter before every launch
         rtb::check(cudaMemsetAsync(counters, 0, counter_bytes, stream), "clearing the scratch counters");
         int64_t pass = pass_begin;

@@ -58,8 +58,23 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
     set_camera(scene_->camera());
 }
 
+cudaEvent_t* session::marks(size_t count)
+{
+    while (marks_.size() < count)
+    {
+        cudaEvent_t e = nullptr;
+        check(cudaEventCreate(&e), "creating a CUDA event");
+        marks_.push_back(e);
+    }
+    return marks_.data();
+}
+
 session::~session()
 {
+    for (cudaEvent_t e : marks_)
+    {
+        cudaEventDestroy(e);
+    }
     wave_.reset(); // its arrays are freed on the stream, before it goes
     rgba_.release();
     partials_.release();
@@ -109,6 +124,7 @@ void session::set_camera(const rt_camera_desc& camera)
     passes_ = 0;
     kernel_seconds_ = 0;
     samples_per_second_ = 0;
+    times_ = rt_kernel_times{};
 }
 
 int64_t session::plan(int64_t target, double budget_seconds) const
@@ -183,22 +199,74 @@ double session::launch(int64_t end)
         b = wave_->setup(static_cast<int64_t>(padded_pixels_) * (end - passes_), stream_);
     }
     check(cudaEventRecord(start_, stream_), "recording a CUDA event");
+    int64_t steps = 0;
+    cudaEvent_t* reduce_marks = timing_ ? marks(2) : nullptr;
     if (wave)
     {
         const bool quality = scene_->quality();
-        const int64_t steps =
-            wave_->run(b, camera_.max_depth, stream_, [&] { return launch_wave_step(p, quality, b, trace_grid_, stream_); });
+        steps = wave_->run(b, camera_.max_depth, stream_, [&] {
+            const cudaEvent_t* m = nullptr;
+            if (timing_)
+            {
+                m = marks(static_cast<size_t>(2 + 3 * (steps + 1))) + 2 + 3 * steps;
+            }
+            ++steps;
+            return launch_wave_step(p, quality, b, trace_grid_, stream_, m);
+        });
         last_kernel_launches_ = static_cast<int32_t>(2 * steps + 1);
+        if (timing_)
+        {
+            reduce_marks = marks_.data();
+            check(cudaEventRecord(reduce_marks[0], stream_), "recording a CUDA event");
+        }
         check(launch_wave_reduce(r, b, p.pass_begin, p.pass_end, p.chunk, stream_), "launching the reduction");
     }
     else
     {
+        cudaEvent_t* m = timing_ ? marks(3) : nullptr;
         check(launch_render(p, scene_->quality(), counting_, grid_, stream_), "launching the render kernel");
+        if (m)
+        {
+            check(cudaEventRecord(m[2], stream_), "recording a CUDA event");
+            reduce_marks = m + 2;
+        }
         check(launch_reduce(r, stream_), "launching the reduction");
         last_kernel_launches_ = 2;
     }
+    if (timing_)
+    {
+        check(cudaEventRecord(wave ? reduce_marks[1] : marks_[1], stream_), "recording a CUDA event");
+    }
     check(cudaEventRecord(stop_, stream_), "recording a CUDA event");
     check(cudaEventSynchronize(stop_), "rendering on the GPU");
+    if (timing_)
+    {
+        const auto elapsed = [](cudaEvent_t a, cudaEvent_t b) {
+            float ms = 0;
+            check(cudaEventElapsedTime(&ms, a, b), "timing a kernel");
+            return ms / 1000.0;
+        };
+        if (wave)
+        {
+            for (int64_t k = 0; k < steps; ++k)
+            {
+                const cudaEvent_t* m = marks_.data() + 2 + 3 * k;
+                times_.seconds[RT_KERNEL_SHADE] += elapsed(m[0], m[1]);
+                times_.seconds[RT_KERNEL_TRACE] += elapsed(m[1], m[2]);
+            }
+            times_.launches[RT_KERNEL_SHADE] += steps;
+            times_.launches[RT_KERNEL_TRACE] += steps;
+            times_.seconds[RT_KERNEL_REDUCE] += elapsed(marks_[0], marks_[1]);
+        }
+        else
+        {
+            // marks: [0] unused, [1] after the reduction, [2] after the render kernel; the render starts at start_
+            times_.seconds[RT_KERNEL_RENDER] += elapsed(start_, marks_[2]);
+            ++times_.launches[RT_KERNEL_RENDER];
+            times_.seconds[RT_KERNEL_REDUCE] += elapsed(marks_[2], marks_[1]);
+        }
+        ++times_.launches[RT_KERNEL_REDUCE];
+    }
     float ms = 0;
     check(cudaEventElapsedTime(&ms, start_, stop_), "timing the GPU");
     const double seconds = std::max(1e-6, ms / 1000.0);

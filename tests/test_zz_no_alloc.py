@@ -56,6 +56,35 @@ def test_no_alloc_matches_session_on_two_calls_in_a_row(rt):
         np.testing.assert_allclose(got, expected, rtol=1e-12, atol=1e-15)
 
 
+def test_no_alloc_splits_a_call_into_launches_that_fit_its_scratch(rt):
+    """An image whose padded pixels nearly fill the scratch (1920 x 1400: 2,688,000 of 2,796,192 entries) takes one
+    16-pass chunk a launch, so passes 0-48 are three render+reduce launches in one call; the sums and the ray counts
+    equal a persistent-form session's of the same seed and passes."""
+    import torch
+
+    from raytracing_b200 import _abi
+
+    lib = _abi.load()
+    rt.set_device(0)
+    desc = rt.builtin_scene("cornell", width=1920, height=1400, spp=1)
+    scene = rt.Scene(desc)
+    w, h = scene.width, scene.height
+    assert (w, h) == (1920, 1400)
+    session = rt.Session(scene, seed=5, form="persistent")
+    session.render_to(48)
+    expected = session.pixels()
+    expected_rays = session.counters()["rays"]
+    sums = _device_buffer(h * w * 3)
+    rays = C.c_uint64()
+    status = lib.rt_render_passes_no_alloc(scene._handle, C.byref(desc.camera), 5, 0, 48, C.c_void_p(sums.data_ptr()),
+                                           C.byref(rays), None)
+    assert status == 0, lib.rt_last_error_message()
+    torch.cuda.synchronize()
+    got = sums.cpu().numpy().reshape(h, w, 3) / 48
+    np.testing.assert_allclose(got, expected, rtol=1e-12, atol=1e-15)
+    assert rays.value == expected_rays
+
+
 def test_no_alloc_refuses_images_beyond_its_scratch(rt):
     from raytracing_b200 import _abi
 
