@@ -325,6 +325,8 @@ def mesh_measurement(rt, torch) -> dict:
            "scene_stats": scene.stats()}
     for form in ("wavefront", "persistent"):
         sess = rt.Session(scene, seed=3, form=form, launch_seconds=0.5)
+        if form == "wavefront":
+            out["autotune"] = sess.autotune(trial_passes=8)
         sess.render_to(16)  # warm-up: module load, buffers
         sess.set_camera(desc.camera)
         torch.cuda.synchronize()
@@ -660,6 +662,8 @@ def run_b200(args):
 
     session = rt.Session(scene, seed=seed, launch_seconds=0.5)
     camera = scene_desc.camera
+    # The wavefront's launch shape chosen by the library's autotuner on this view (untimed, before the warm-up)
+    tuning = session.autotune(trial_passes=16)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step():
@@ -726,7 +730,7 @@ def run_b200(args):
                 "gpu_launches": kernel_launches,
                 "segments_per_sample": total_rays / (args.steps * passes * scene.width * scene.height),
                 "shadow_rays_per_sample": total_shadow / (args.steps * passes * scene.width * scene.height),
-                "kernel": session.kernel(), "scene_stats": stats}
+                "kernel": session.kernel(), "scene_stats": stats, "autotune": tuning}
     session.close()
     del flush
 

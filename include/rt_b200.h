@@ -415,6 +415,36 @@ typedef struct rt_kernel_times
 rt_status rt_session_set_timing(rt_session* session, int32_t on);
 rt_status rt_session_kernel_times(const rt_session* session, rt_kernel_times* times);
 
+/* The wavefront's autotuner (no counterpart in the reference, whose launch planner sizes launches but never the
+ * kernels' shapes, renderer.cu:201-308): short renders of the session's view under candidate launch shapes, one knob
+ * after another from the built-in defaults: the trace kernel's register cap (as the minimum blocks per multiprocessor
+ * its launch bounds give: 8, or 6 with more registers a thread) and its grid (blocks per multiprocessor); the slot
+ * pool, which is the query queue's capacity (two queries a slot); the shade kernel's block size. The best shape stays
+ * with the session and is remembered, per device and scene class (flat or tree, integrator, features, triangles,
+ * size), for the sessions made after it. The image does not depend on the shape. The view must have no passes yet
+ * (RT_ERR_LOGIC otherwise) and starts over afterwards; a persistent-form session has nothing to tune (slots 0). */
+typedef struct rt_tuning
+{
+    int32_t slots;
+    int32_t trace_blocks_per_sm;
+    int32_t shade_block;
+    int32_t trace_min_blocks;
+    int32_t trace_registers;    /* the chosen trace kernel's registers a thread */
+    int32_t trials;             /* renders measured (0: the shape came from an earlier session's tuning, or defaults) */
+    int32_t from_cache;         /* 1: taken from an earlier tuning of the same scene class */
+    int32_t pad0;
+    double samples_per_second;  /* the chosen shape's measured speed (pixel passes a second) */
+    double default_samples_per_second; /* the built-in defaults' */
+} rt_tuning;
+rt_status rt_session_autotune(rt_session* session, int64_t trial_passes, rt_tuning* result);
+rt_status rt_session_tuning(const rt_session* session, rt_tuning* current);
+/* The autotuner's search on a caller-given measure (its selection logic without a GPU, for tests): the candidates
+ * of a GPU whose trace kernels fit max_trace_blocks (default cap) and max_trace_blocks_roomy (roomy cap) blocks a
+ * multiprocessor, each measured by measure(shape, user) in samples per second. */
+typedef double (*rt_tune_measure_fn)(const rt_tuning* shape, void* user);
+rt_status rt_autotune_simulate(int32_t max_trace_blocks, int32_t max_trace_blocks_roomy, rt_tune_measure_fn measure,
+                               void* user, rt_tuning* result);
+
 /* The counting build (no counterpart in the reference): while on, launches also count BVH node fetches and sphere,
  * quad and triangle tests (closest-hit and shadow traversals together), the measured work behind the roofline's
  * algorithmic bytes. Slower; off by default. counts: nodes, spheres, quads, triangles since the view was set. */

@@ -305,6 +305,21 @@ def display_device(sums_ptr: int, width: int, height: int, passes: int, rgba_ptr
                                     C.c_void_p(stream or None)))
 
 
+def _tuning_dict(t: _abi.Tuning) -> dict:
+    return {name: getattr(t, name) for name, _ in _abi.Tuning._fields_ if name != "pad0"}
+
+
+def autotune_simulate(measure, max_trace_blocks: int = 8, max_trace_blocks_roomy: int = 6) -> dict:
+    """The autotuner's search (the library's own code) on a Python measure(shape dict) -> samples per second."""
+    def call(shape, _user):
+        return float(measure(_tuning_dict(shape.contents)))
+
+    cb = _abi.TUNE_MEASURE(call)
+    t = _abi.Tuning()
+    _check(_lib().rt_autotune_simulate(max_trace_blocks, max_trace_blocks_roomy, cb, None, C.byref(t)))
+    return _tuning_dict(t)
+
+
 class Session:
     """renderer.h:591-673 session: one view whose image gains passes on demand; its sums stay on the device."""
 
@@ -374,6 +389,18 @@ class Session:
         k = _abi.KernelInfo()
         _check(_lib().rt_session_kernel(self._handle, C.byref(k)))
         return _kernel_dict(k)
+
+    def autotune(self, trial_passes: int = 16) -> dict:
+        """The wavefront's autotuner on this view (which must have no passes yet; it starts over afterwards): the
+        chosen launch shape and its measured speed against the built-in defaults'."""
+        t = _abi.Tuning()
+        _check(_lib().rt_session_autotune(self._handle, trial_passes, C.byref(t)))
+        return _tuning_dict(t)
+
+    def tuning(self) -> dict:
+        t = _abi.Tuning()
+        _check(_lib().rt_session_tuning(self._handle, C.byref(t)))
+        return _tuning_dict(t)
 
     def set_timing(self, on: bool) -> None:
         """Per-kernel timing: CUDA events around every kernel of every launch (slows launches a little)."""

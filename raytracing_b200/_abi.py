@@ -86,6 +86,16 @@ class KernelTimes(C.Structure):
     _fields_ = [("seconds", C.c_double * 4), ("launches", C.c_int64 * 4)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("trace_blocks_per_sm", C.c_int32), ("shade_block", C.c_int32),
+                ("trace_min_blocks", C.c_int32), ("trace_registers", C.c_int32), ("trials", C.c_int32),
+                ("from_cache", C.c_int32), ("pad0", C.c_int32), ("samples_per_second", C.c_double),
+                ("default_samples_per_second", C.c_double)]
+
+
+TUNE_MEASURE = C.CFUNCTYPE(C.c_double, C.POINTER(Tuning), C.c_void_p)
+
+
 class MeshDesc(C.Structure):
     _fields_ = [("positions", C.POINTER(C.c_float)), ("vertex_count", C.c_int64),
                 ("indices", C.POINTER(C.c_uint32)), ("triangle_count", C.c_int64), ("material", C.c_int32),
@@ -231,6 +241,9 @@ ENTRY_POINTS = [
     ("rt_session_mean_radiance", C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     ("rt_session_set_timing", C.c_int, [C.c_void_p, C.c_int32]),
     ("rt_session_kernel_times", C.c_int, [C.c_void_p, C.POINTER(KernelTimes)]),
+    ("rt_session_autotune", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(Tuning)]),
+    ("rt_session_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    ("rt_autotune_simulate", C.c_int, [C.c_int32, C.c_int32, TUNE_MEASURE, C.c_void_p, C.POINTER(Tuning)]),
     ("rt_session_set_counting", C.c_int, [C.c_void_p, C.c_int32]),
     ("rt_session_fetch_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64 * 4)]),
     ("rt_scene_closest_hits", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64,

@@ -392,6 +392,27 @@ rt_status rt_session_kernel_times(const rt_session* session, rt_kernel_times* ti
     });
 }
 
+rt_status rt_session_autotune(rt_session* session, int64_t trial_passes, rt_tuning* result)
+{
+    return guarded([&] {
+        need(session, "session");
+        const rt_tuning t = session->session->autotune(trial_passes);
+        if (result)
+        {
+            *result = t;
+        }
+    });
+}
+
+rt_status rt_session_tuning(const rt_session* session, rt_tuning* current)
+{
+    return guarded([&] {
+        need(session, "session");
+        need(current, "current");
+        *current = session->session->tuning();
+    });
+}
+
 rt_status rt_session_set_counting(rt_session* session, int32_t on)
 {
     return guarded([&] {

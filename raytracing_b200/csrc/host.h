@@ -6,6 +6,8 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <tuple>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -261,6 +263,37 @@ inline int wave_slots_for(const scene_view& v)
     return v.flat != 0 && !has_features(v) ? wave_slots_large : wave_slots;
 }
 
+// The wavefront's autotuner (tuner.cpp): a launch shape, the knobs' candidate values, and the search
+struct tune_candidate
+{
+    int slots;
+    int trace_blocks_per_sm;
+    int shade_block;
+    int trace_min_blocks;
+};
+struct tune_space
+{
+    std::vector<std::pair<int, int>> trace; // (register cap as min blocks, blocks per multiprocessor)
+    std::vector<int> slots;
+    std::vector<int> shade_blocks;
+};
+struct tune_outcome
+{
+    tune_candidate best;
+    double best_speed;
+    double default_speed;
+    int trials;
+};
+tune_space default_tune_space(int max_trace_blocks, int max_trace_blocks_roomy);
+tune_candidate default_candidate(int slots, int max_trace_blocks);
+rt_tuning to_tuning(const tune_candidate& c);
+tune_outcome coordinate_descent(const tune_candidate& start, const tune_space& space,
+                                const std::function<double(const tune_candidate&)>& measure);
+std::tuple<int, int, int, int, int, int, int> tune_key(int device, const scene_view& v, bool quality);
+bool cached_tuning(const std::tuple<int, int, int, int, int, int, int>& key, tune_candidate& out);
+void remember_tuning(const std::tuple<int, int, int, int, int, int, int>& key, const tune_candidate& c);
+void forget_tunings();
+
 // One view of a resident scene whose image gains passes on demand (renderer.h:591-673)
 class session
 {
@@ -280,6 +313,10 @@ public:
     double kernel_seconds() const { return kernel_seconds_; }
     rt_kernel_info kernel() const;
     const double* device_sums() const { return sums_.data(); }
+    // The autotuner: short renders of this view under candidate launch shapes (the view must have no passes yet; it
+    // starts over afterwards), the best shape kept for this session and remembered for its scene class
+    rt_tuning autotune(int64_t trial_passes);
+    rt_tuning tuning() const { return tuning_; }
     // Per-kernel timing (events around every kernel of every launch; slows launches a little): rt_kernel_times
     void set_timing(bool on) { timing_ = on; }
     rt_kernel_times kernel_times() const { return times_; }
@@ -316,7 +353,11 @@ private:
     bool wavefront_ = false;
     std::unique_ptr<wave_runner> wave_;
     int32_t last_kernel_launches_ = 0; // the last launch's kernels
-    int trace_grid_ = 0;
+    wave_shape shape_{};                // how a step is launched (the autotuner's choice or the defaults)
+    tune_candidate tuned_{};
+    rt_tuning tuning_{};
+    int multiprocessors_ = 0;
+    void apply(const tune_candidate& c);
 
     // Per-kernel timing: a pool of events, grown as launches need them
     bool timing_ = false;

@@ -2672,7 +2672,7 @@ __device__ __forceinline__ void wave_camera_query(const wave_buffers& B, const w
 // The trace kernel's resident blocks per multiprocessor (64 registers at 8) and the number of lanes still walking
 // under which a warp stops to give its idle lanes new queries (the addendum's 20 of 32)
 #ifndef RTB_TRACE_MIN_BLOCKS
-#define RTB_TRACE_MIN_BLOCKS 8
+#define RTB_TRACE_MIN_BLOCKS RTB_TRACE_MIN_BLOCKS_DEFAULT
 #endif
 #ifndef RTB_REFILL_LANES
 #define RTB_REFILL_LANES 20
@@ -2683,8 +2683,8 @@ __device__ __forceinline__ void wave_camera_query(const wave_buffers& B, const w
 // hit children visited nearest first (a four-key sorting network); otherwise the binary tree in the persistent
 // kernel's node order. BATCH: each query walks its own job's scene (the job in its flags); otherwise the launch's
 // scene S0. The walks are counted into `counters` when it is given.
-template <bool FEATURES, bool BATCH, bool WIDE>
-__global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
+template <bool FEATURES, bool BATCH, bool WIDE, int MINB = RTB_TRACE_MIN_BLOCKS>
+__global__ void __launch_bounds__(render_block, MINB)
     wave_trace_kernel(const __grid_constant__ scene_view S0, const __grid_constant__ wave_buffers B,
                       const __grid_constant__ wave_batch W, unsigned long long* counters)
 {
@@ -3005,8 +3005,8 @@ __device__ __forceinline__ void flat_search(const scene_view& S, float3 o, float
 // The queued queries of a flat-searched scene: one query per thread at a time (grid-stride), every lane the same
 // loop over the same records, no tree, no stack, no refill. BATCH: each query searches its job's scene (W's table; a
 // warp's lanes may loop over different scenes), its walks counted where the shade kernel queued it.
-template <bool FEATURES, bool BATCH>
-__global__ void __launch_bounds__(render_block, RTB_TRACE_MIN_BLOCKS)
+template <bool FEATURES, bool BATCH, int MINB = RTB_TRACE_MIN_BLOCKS>
+__global__ void __launch_bounds__(render_block, MINB)
     wave_flat_trace_kernel(const __grid_constant__ scene_view S, const __grid_constant__ wave_buffers B,
                            const __grid_constant__ wave_batch W, unsigned long long* counters)
 {
@@ -3301,20 +3301,42 @@ wave_shade_function wave_shade_of(bool quality, bool features)
     return features ? wave_shade_kernel<false, true, false> : wave_shade_kernel<false, false, false>;
 }
 
-wave_trace_function wave_trace_of(bool features, bool wide) { return wave_trace_variant<false>(features, wide); }
+// A session's walk at one of the register caps the autotuner chooses between: the default blocks per multiprocessor
+// (64 registers a thread at 8 blocks of 128) or fewer blocks with more registers (80 at 6)
+wave_trace_function wave_trace_of(bool features, bool wide, int min_blocks = RTB_TRACE_MIN_BLOCKS)
+{
+    if (min_blocks == wave_trace_roomy_blocks)
+    {
+        if (wide)
+        {
+            return features ? wave_trace_kernel<true, false, true, wave_trace_roomy_blocks>
+                            : wave_trace_kernel<false, false, true, wave_trace_roomy_blocks>;
+        }
+        return features ? wave_trace_kernel<true, false, false, wave_trace_roomy_blocks>
+                        : wave_trace_kernel<false, false, false, wave_trace_roomy_blocks>;
+    }
+    return wave_trace_variant<false>(features, wide);
+}
 
 template <bool BATCH>
-wave_trace_function wave_flat_trace_of(bool features)
+wave_trace_function wave_flat_trace_of(bool features, int min_blocks = RTB_TRACE_MIN_BLOCKS)
 {
+    if (!BATCH && min_blocks == wave_trace_roomy_blocks)
+    {
+        return features ? wave_flat_trace_kernel<true, false, wave_trace_roomy_blocks>
+                        : wave_flat_trace_kernel<false, false, wave_trace_roomy_blocks>;
+    }
     return features ? wave_flat_trace_kernel<true, BATCH> : wave_flat_trace_kernel<false, BATCH>;
 }
 } // namespace
 
 // marks (when given): three events recorded before the shade kernel, between the two kernels and after the trace
 // kernel, for per-kernel timing
-cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& slots, int trace_grid,
+cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& slots, const wave_shape& shape,
                              cudaStream_t stream, const cudaEvent_t* marks)
 {
+    const int trace_grid = shape.trace_grid;
+    const int shade_block = shape.shade_block > 0 ? shape.shade_block : render_block;
     wave_buffers b = slots; // with the launch's camera and RNG job, for the camera rays the trace kernel makes
     b.cam = p.cam;
     b.job = p.job;
@@ -3328,7 +3350,7 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     {
         cudaEventRecord(marks[0], stream);
     }
-    wave_shade_of(quality, features)<<<b.slot_count / render_block, render_block, 0, stream>>>(p, b, wave_batch{});
+    wave_shade_of(quality, features)<<<b.slot_count / shade_block, shade_block, 0, stream>>>(p, b, wave_batch{});
     e = cudaGetLastError();
     if (e != cudaSuccess)
     {
@@ -3340,12 +3362,13 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     }
     if (p.scene.flat != 0)
     {
-        wave_flat_trace_of<false>(features)<<<trace_grid, render_block, 0, stream>>>(p.scene, b, wave_batch{},
-                                                                                     p.counters);
+        wave_flat_trace_of<false>(features, shape.trace_min_blocks)<<<trace_grid, render_block, 0, stream>>>(
+            p.scene, b, wave_batch{}, p.counters);
     }
     else
     {
-        wave_trace_of(features, p.scene.wide_nodes != nullptr)<<<trace_grid, render_block, 0, stream>>>(
+        wave_trace_of(features, p.scene.wide_nodes != nullptr, shape.trace_min_blocks)<<<trace_grid, render_block, 0,
+                                                                                          stream>>>(
             p.scene, b, wave_batch{}, p.counters);
     }
     e = cudaGetLastError();
@@ -3420,7 +3443,8 @@ cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, in
     return cudaGetLastError();
 }
 
-cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace)
+cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace,
+                            int trace_min_blocks)
 {
     const bool features = has_features(scene);
     const cudaError_t e = attributes_of(wave_shade_of(quality, features), shade);
@@ -3428,8 +3452,12 @@ cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attrib
     {
         return e;
     }
-    // the walk's kernel sizes the trace grid of either search (the flat one is launched with the same grid)
-    return attributes_of(wave_trace_of(features, scene.wide_nodes != nullptr), trace);
+    // the session's trace kernel of the scene's search at the given register cap
+    if (scene.flat != 0)
+    {
+        return attributes_of(wave_flat_trace_of<false>(features, trace_min_blocks), trace);
+    }
+    return attributes_of(wave_trace_of(features, scene.wide_nodes != nullptr, trace_min_blocks), trace);
 }
 
 cudaError_t launch_camera_rays(const camera_params& cam, uint64_t seed, int64_t pass, int32_t round_passes,

@@ -177,9 +177,21 @@ size_t wave_slot_bytes();
 // Every slot without a sample (its flags row zeroed), before a launch's first step
 cudaError_t clear_wave_slots(const wave_buffers& b, cudaStream_t stream);
 // One step: clears the queue, the shade kernel over the slots, the trace kernel (trace_grid blocks) over the queue
-cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, int trace_grid,
-                             cudaStream_t stream,
-                             const cudaEvent_t* marks = nullptr);
+// How a session's wavefront step is launched (the autotuner's choice): the trace kernel's grid and register cap (its
+// minimum resident blocks per multiprocessor: RTB_TRACE_MIN_BLOCKS or wave_trace_roomy_blocks), the shade kernel's
+// block size (64 or 128 threads)
+constexpr int wave_trace_roomy_blocks = 6;
+#ifndef RTB_TRACE_MIN_BLOCKS_DEFAULT
+#define RTB_TRACE_MIN_BLOCKS_DEFAULT 8
+#endif
+struct wave_shape
+{
+    int trace_grid;
+    int shade_block;
+    int trace_min_blocks;
+};
+cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, const wave_shape& shape,
+                             cudaStream_t stream, const cudaEvent_t* marks = nullptr);
 // The samples of passes [pass_begin, pass_end) into the sums (chunk partials in pass order, added in chunk order)
 cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
                                int32_t chunk, cudaStream_t stream);
@@ -192,7 +204,10 @@ cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& 
 // Loads the batch wavefront's kernels (every variant) now, so that no step pays for loading them
 cudaError_t preload_wave_batch();
 // The shade kernel's and the trace kernel's attributes for the scene and integrator
-cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace);
+// The shade kernel's and the session's trace kernel's attributes (the trace kernel of the scene's search, at the given
+// register cap)
+cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace,
+                            int trace_min_blocks = RTB_TRACE_MIN_BLOCKS_DEFAULT);
 
 // Parity hooks: closest hits of given rays (source ids through prim_source), and the camera rays of one pass
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,

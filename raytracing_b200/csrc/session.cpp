@@ -47,15 +47,101 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
     grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
     const scene_view& view = scene_->view();
     wavefront_ = options_.form == RT_FORM_WAVEFRONT || (options_.form == RT_FORM_AUTO && wavefront_suits(view));
+    multiprocessors_ = a.multiprocessors;
     if (wavefront_)
     {
         kernel_attributes shade{}, trace{};
         check(wave_attributes(view, scene_->quality(), shade, trace), "querying the wavefront kernels");
-        trace_grid_ = trace.multiprocessors * std::max(1, trace.blocks_per_sm);
-        wave_ = std::make_unique<wave_runner>(wave_slots_for(view), wave_group);
+        // The built-in shape, or the one an earlier session's autotuning chose for this scene class
+        tune_candidate c = default_candidate(wave_slots_for(view), trace.blocks_per_sm);
+        tune_candidate cached{};
+        if (cached_tuning(tune_key(scene_->device(), view, scene_->quality()), cached))
+        {
+            c = cached;
+            tuning_.from_cache = 1;
+        }
+        apply(c);
     }
     counters_.allocate(7);
     set_camera(scene_->camera());
+}
+
+void session::apply(const tune_candidate& c)
+{
+    if (!wave_ || wave_->max_slots != c.slots)
+    {
+        wave_.reset();
+        wave_ = std::make_unique<wave_runner>(c.slots, wave_group);
+    }
+    tuned_ = c;
+    shape_.trace_grid = multiprocessors_ * c.trace_blocks_per_sm;
+    shape_.shade_block = c.shade_block;
+    shape_.trace_min_blocks = c.trace_min_blocks;
+    const int from_cache = tuning_.from_cache;
+    const int trials = tuning_.trials;
+    const double speed = tuning_.samples_per_second;
+    const double base = tuning_.default_samples_per_second;
+    tuning_ = to_tuning(c);
+    tuning_.from_cache = from_cache;
+    tuning_.trials = trials;
+    tuning_.samples_per_second = speed;
+    tuning_.default_samples_per_second = base;
+    kernel_attributes shade{}, trace{};
+    check(wave_attributes(scene_->view(), scene_->quality(), shade, trace, c.trace_min_blocks),
+          "querying the wavefront kernels");
+    tuning_.trace_registers = trace.registers;
+}
+
+rt_tuning session::autotune(int64_t trial_passes)
+{
+    if (!wavefront_)
+    {
+        return rt_tuning{}; // the persistent kernel's launches have no shape to choose
+    }
+    if (passes_ != 0)
+    {
+        fail(RT_ERR_LOGIC, "autotune needs a view with no passes yet (it renders trials of its own)");
+    }
+    if (trial_passes < 1 || trial_passes > 1 << 20)
+    {
+        fail(RT_ERR_INVALID, "trial_passes must be in [1, 2^20]");
+    }
+    const scene_view& view = scene_->view();
+    kernel_attributes shade{}, trace{}, roomy{};
+    check(wave_attributes(view, scene_->quality(), shade, trace), "querying the wavefront kernels");
+    check(wave_attributes(view, scene_->quality(), shade, roomy, wave_trace_roomy_blocks),
+          "querying the wavefront kernels");
+    const tune_space space = default_tune_space(trace.blocks_per_sm, roomy.blocks_per_sm);
+    const double samples = static_cast<double>(camera_.image_width) * camera_.image_height *
+                           static_cast<double>(trial_passes);
+    const bool counting = counting_;
+    counting_ = false;
+    // Each candidate: the best of two renders of the trial passes from a fresh image
+    const auto measure = [&](const tune_candidate& c) {
+        apply(c);
+        double best = 0;
+        for (int k = 0; k < 2; ++k)
+        {
+            set_camera(camera_);
+            double seconds = 0;
+            while (passes_ < trial_passes)
+            {
+                seconds += launch(plan(trial_passes, options_.launch_seconds));
+            }
+            best = std::max(best, samples / std::max(seconds, 1e-9));
+        }
+        return best;
+    };
+    const tune_outcome o = coordinate_descent(tuned_, space, measure);
+    counting_ = counting;
+    tuning_.from_cache = 0;
+    tuning_.trials = o.trials;
+    tuning_.samples_per_second = o.best_speed;
+    tuning_.default_samples_per_second = o.default_speed;
+    apply(o.best);
+    remember_tuning(tune_key(scene_->device(), view, scene_->quality()), o.best);
+    set_camera(camera_);
+    return tuning_;
 }
 
 cudaEvent_t* session::marks(size_t count)
@@ -211,7 +297,7 @@ double session::launch(int64_t end)
                 m = marks(static_cast<size_t>(2 + 3 * (steps + 1))) + 2 + 3 * steps;
             }
             ++steps;
-            return launch_wave_step(p, quality, b, trace_grid_, stream_, m);
+            return launch_wave_step(p, quality, b, shape_, stream_, m);
         });
         last_kernel_launches_ = static_cast<int32_t>(2 * steps + 1);
         if (timing_)
@@ -412,7 +498,9 @@ rt_kernel_info session::kernel() const
     if (wavefront_ && !counting_)
     {
         kernel_attributes shade{};
-        check(wave_attributes(scene_->view(), scene_->quality(), shade, a), "querying the wavefront kernels");
+        check(wave_attributes(scene_->view(), scene_->quality(), shade, a, shape_.trace_min_blocks),
+              "querying the wavefront kernels");
+        a.blocks_per_sm = tuned_.trace_blocks_per_sm; // the trace kernel's launch, as the shape has it
     }
     else
     {

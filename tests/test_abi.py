@@ -51,7 +51,7 @@ STRUCTS = {
     "rt_batch_report": _abi.BatchReport, "rt_server_options": _abi.ServerOptions,
     "rt_request_status": _abi.RequestStatus, "rt_server_step_report": _abi.ServerStepReport,
     "rt_server_stats": _abi.ServerStats, "rt_display_options": _abi.DisplayOptions,
-    "rt_kernel_times": _abi.KernelTimes,
+    "rt_kernel_times": _abi.KernelTimes, "rt_tuning": _abi.Tuning,
 }
 
 
