@@ -2278,21 +2278,115 @@ constexpr int wave_shade_min_blocks()
     return RTB_WAVE_SHADE_MIN_BLOCKS > 0 ? RTB_WAVE_SHADE_MIN_BLOCKS : render_min_blocks<QUALITY, false, FEATURES>();
 }
 
+// What a slot's hit needs of the shading, for the block-level sort: its material's kind and lobe, or the miss, the
+// sample's end, a slot without a sample, a slot out of work (last). Only the grouping depends on it.
+constexpr int shade_keys = 12;
+__device__ __forceinline__ int shade_key(const scene_view& S, uint32_t flags, const int4& answer)
+{
+    if (flags & wave_exhausted)
+    {
+        return shade_keys - 1;
+    }
+    if ((flags & wave_finish) || !(flags & wave_ext))
+    {
+        return shade_keys - 2; // a sample that ends here or a slot that needs one: a camera ray is next
+    }
+    const int id = answer.x;
+    if (id < 0 || id >= S.prim_count)
+    {
+        return shade_keys - 3; // the sky or the environment (or a particle of smoke)
+    }
+    const material12* m = S.materials + __ldg(S.prim_material + id);
+    const int kind = __ldg(&m->kind);
+    const int lobe = __ldg(&m->lobe);
+    return min(kind, 4) * 2 + (lobe != RT_MICROFACET_NONE ? 1 : 0);
+}
+
 // A slot's step: the last walk's answers, the shading, the sample's end, a new sample, the next rays queued.
 // BATCH: the slots render the samples of a group of batch jobs (W), each slot its job's scene, camera and integrator
 // (QUALITY is then the job's own); otherwise the launch's one view (P).
-template <bool QUALITY, bool FEATURES, bool BATCH>
+// Every load of the slot's rows and answer is issued at the start, before any of them is needed, so the step waits
+// for one round trip to memory, not one for the flags and another for what they say to read.
+// SORT (a session's launch): the block's slots are first staged in shared memory (coalesced loads), sorted by what
+// their hits need of the shading (shade_key: a counting sort of the block's 64 or 128 keys), shaded by the threads in
+// that order, so that a warp's lanes take the same branches, and written back from shared memory in slot order.
+template <bool QUALITY, bool FEATURES, bool BATCH, bool SORT = false>
 __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY || BATCH, FEATURES>())
     wave_shade_kernel(const __grid_constant__ launch_params P, const __grid_constant__ wave_buffers B,
                       const __grid_constant__ wave_batch W)
 {
-    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    static_assert(!(SORT && BATCH), "the sorted step is a session's");
     const int n = B.slot_count;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
     float4* rows = static_cast<float4*>(B.slots);
     float4* shadow_rows = rows + static_cast<int64_t>(wave_rows) * n;
-    const int4 r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + i);
+    const int own = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    // the slot's rows and its answer, all loads issued together
+    float4 r0 = stream_load(rows + own);
+    float4 r1 = stream_load(rows + n + own);
+    float4 r2 = stream_load(rows + 2 * n + own);
+    float4 r3 = stream_load(rows + 3 * n + own);
+    int4 r4 = stream_load(reinterpret_cast<const int4*>(rows) + 4 * n + own);
+    int4 r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + own);
+    longlong2 r6 = stream_load(reinterpret_cast<const longlong2*>(rows) + 6 * n + own);
+    int4 answer = stream_load(B.ext_result + own);
+    int i = own; // the slot this thread shades
+    // SORT: the staging of the block's slots, their order, and what each slot's write-back needs
+    __shared__ float4 stage[SORT ? wave_rows + 1 : 1][SORT ? render_block : 1];
+    __shared__ int order[SORT ? render_block : 1];
+    __shared__ int bins[SORT ? shade_keys : 1];
+    __shared__ uint8_t store_mode[SORT ? render_block : 1]; // 0 nothing, 1 the flags row, 2 every row
+    if constexpr (SORT)
+    {
+        const int t = static_cast<int>(threadIdx.x);
+        stage[0][t] = r0;
+        stage[1][t] = r1;
+        stage[2][t] = r2;
+        stage[3][t] = r3;
+        stage[4][t] = make_float4(__int_as_float(r4.x), __int_as_float(r4.y), __int_as_float(r4.z),
+                                  __int_as_float(r4.w));
+        stage[5][t] = make_float4(__int_as_float(r5.x), __int_as_float(r5.y), __int_as_float(r5.z),
+                                  __int_as_float(r5.w));
+        reinterpret_cast<longlong2*>(&stage[6][0])[t] = r6;
+        stage[7][t] = make_float4(__int_as_float(answer.x), __int_as_float(answer.y), __int_as_float(answer.z),
+                                  __int_as_float(answer.w));
+        store_mode[t] = 0;
+        if (t < shade_keys)
+        {
+            bins[t] = 0;
+        }
+        __syncthreads();
+        const int key = shade_key(P.scene, static_cast<uint32_t>(r5.y), answer);
+        const int rank = atomicAdd(&bins[key], 1);
+        __syncthreads();
+        if (t == 0)
+        {
+            int sum = 0;
+            for (int k = 0; k < shade_keys; ++k)
+            {
+                const int c = bins[k];
+                bins[k] = sum;
+                sum += c;
+            }
+        }
+        __syncthreads();
+        order[bins[key] + rank] = t;
+        __syncthreads();
+        const int j = order[t];
+        i = static_cast<int>(blockIdx.x * blockDim.x) + j;
+        r0 = stage[0][j];
+        r1 = stage[1][j];
+        r2 = stage[2][j];
+        r3 = stage[3][j];
+        const float4 s4 = stage[4][j];
+        r4 = make_int4(__float_as_int(s4.x), __float_as_int(s4.y), __float_as_int(s4.z), __float_as_int(s4.w));
+        const float4 s5 = stage[5][j];
+        r5 = make_int4(__float_as_int(s5.x), __float_as_int(s5.y), __float_as_int(s5.z), __float_as_int(s5.w));
+        r6 = reinterpret_cast<const longlong2*>(&stage[6][0])[j];
+        const float4 s7 = stage[7][j];
+        answer = make_int4(__float_as_int(s7.x), __float_as_int(s7.y), __float_as_int(s7.z), __float_as_int(s7.w));
+    }
     uint32_t flags = static_cast<uint32_t>(r5.y);
     uint32_t shadow_rays = 0; // counted where the walks are (the trace kernel), or as queued (BATCH)
     // a warp whose slots have all run out of work has nothing left to do in this launch
@@ -2344,12 +2438,6 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         rng.job = BATCH ? J->job : P.job;
         if (live)
         {
-            const float4 r0 = stream_load(rows + i);
-            const float4 r1 = stream_load(rows + n + i);
-            const float4 r2 = stream_load(rows + 2 * n + i);
-            const float4 r3 = stream_load(rows + 3 * n + i);
-            const int4 r4 = stream_load(reinterpret_cast<const int4*>(rows) + 4 * n + i);
-            const longlong2 r6 = stream_load(reinterpret_cast<const longlong2*>(rows) + 6 * n + i);
             ps.o = make_float3(r0.x, r0.y, r0.z);
             ps.time = r0.w;
             ps.d = make_float3(r1.x, r1.y, r1.z);
@@ -2394,7 +2482,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             }
             else if (flags & wave_ext)
             {
-                const int4 r = stream_load(B.ext_result + i);
+                const int4 r = answer;
                 hit_info h;
                 h.id = r.x;
                 h.t = __int_as_float(r.y);
@@ -2611,7 +2699,32 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         {
             flags = (flags & ~(wave_specular | wave_inward)) | (ps.specular ? wave_specular : 0u) |
                     (ps.inward ? wave_inward : 0u);
-            if (flags & wave_exhausted)
+            if constexpr (SORT)
+            {
+                // into the staging, written back in slot order below
+                const int j = i - static_cast<int>(blockIdx.x * blockDim.x);
+                if (flags & wave_exhausted)
+                {
+                    stage[5][j] = make_float4(0.0f, __int_as_float(static_cast<int>(flags)), 0.0f, 0.0f);
+                    store_mode[j] = 1;
+                }
+                else
+                {
+                    stage[0][j] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time);
+                    stage[1][j] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf);
+                    stage[2][j] = make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x);
+                    stage[3][j] = make_float4(ps.radiance.y, ps.radiance.z, __uint_as_float(rng.key.x),
+                                              __uint_as_float(rng.key.y));
+                    stage[4][j] = make_float4(__int_as_float(static_cast<int>(rng.pixel)),
+                                              __int_as_float(static_cast<int>(rng.pass)), __int_as_float(ps.from),
+                                              __int_as_float(ps.rays_left));
+                    stage[5][j] = make_float4(__int_as_float(ps.depth), __int_as_float(static_cast<int>(flags)), 0.0f,
+                                              __int_as_float(job));
+                    reinterpret_cast<longlong2*>(&stage[6][0])[j] = make_longlong2(sample_index, pass);
+                    store_mode[j] = 2;
+                }
+            }
+            else if (flags & wave_exhausted)
             {
                 stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
                              make_int4(0, static_cast<int>(flags), 0, 0));
@@ -2630,6 +2743,36 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                              make_int4(ps.depth, static_cast<int>(flags), 0, job));
                 stream_store(reinterpret_cast<longlong2*>(rows) + 6 * n + i, make_longlong2(sample_index, pass));
             }
+        }
+    }
+    if constexpr (SORT)
+    {
+        // the block's slots written back in slot order: each row's stores coalesced
+        __syncthreads();
+        const int t = static_cast<int>(threadIdx.x);
+        const int mode = store_mode[t];
+        if (mode == 1)
+        {
+            const float4 s5 = stage[5][t];
+            stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + own,
+                         make_int4(0, __float_as_int(s5.y), 0, 0));
+        }
+        else if (mode == 2)
+        {
+            stream_store(rows + own, stage[0][t]);
+            stream_store(rows + n + own, stage[1][t]);
+            stream_store(rows + 2 * n + own, stage[2][t]);
+            stream_store(rows + 3 * n + own, stage[3][t]);
+            const float4 s4 = stage[4][t];
+            stream_store(reinterpret_cast<int4*>(rows) + 4 * n + own,
+                         make_int4(__float_as_int(s4.x), __float_as_int(s4.y), __float_as_int(s4.z),
+                                   __float_as_int(s4.w)));
+            const float4 s5 = stage[5][t];
+            stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + own,
+                         make_int4(__float_as_int(s5.x), __float_as_int(s5.y), __float_as_int(s5.z),
+                                   __float_as_int(s5.w)));
+            stream_store(reinterpret_cast<longlong2*>(rows) + 6 * n + own,
+                         reinterpret_cast<const longlong2*>(&stage[6][0])[t]);
         }
     }
 }
@@ -3292,8 +3435,16 @@ wave_trace_function wave_trace_variant(bool features, bool wide)
     return features ? wave_trace_kernel<true, BATCH, false> : wave_trace_kernel<false, BATCH, false>;
 }
 
-wave_shade_function wave_shade_of(bool quality, bool features)
+wave_shade_function wave_shade_of(bool quality, bool features, bool sort = false)
 {
+    if (sort)
+    {
+        if (quality)
+        {
+            return features ? wave_shade_kernel<true, true, false, true> : wave_shade_kernel<true, false, false, true>;
+        }
+        return features ? wave_shade_kernel<false, true, false, true> : wave_shade_kernel<false, false, false, true>;
+    }
     if (quality)
     {
         return features ? wave_shade_kernel<true, true, false> : wave_shade_kernel<true, false, false>;
@@ -3350,7 +3501,8 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     {
         cudaEventRecord(marks[0], stream);
     }
-    wave_shade_of(quality, features)<<<b.slot_count / shade_block, shade_block, 0, stream>>>(p, b, wave_batch{});
+    wave_shade_of(quality, features, shape.shade_sort != 0)<<<b.slot_count / shade_block, shade_block, 0, stream>>>(
+        p, b, wave_batch{});
     e = cudaGetLastError();
     if (e != cudaSuccess)
     {
@@ -3444,10 +3596,10 @@ cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, in
 }
 
 cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace,
-                            int trace_min_blocks)
+                            int trace_min_blocks, bool shade_sort)
 {
     const bool features = has_features(scene);
-    const cudaError_t e = attributes_of(wave_shade_of(quality, features), shade);
+    const cudaError_t e = attributes_of(wave_shade_of(quality, features, shade_sort), shade);
     if (e != cudaSuccess)
     {
         return e;

@@ -77,6 +77,7 @@ void session::apply(const tune_candidate& c)
     shape_.trace_grid = multiprocessors_ * c.trace_blocks_per_sm;
     shape_.shade_block = c.shade_block;
     shape_.trace_min_blocks = c.trace_min_blocks;
+    shape_.shade_sort = c.shade_sort;
     const int from_cache = tuning_.from_cache;
     const int trials = tuning_.trials;
     const double speed = tuning_.samples_per_second;

@@ -20,7 +20,7 @@ def test_autotune_keeps_the_image_and_is_remembered(rt, name, kw):
     t = tuned.autotune(trial_passes=16)
     assert t["trials"] >= 8
     assert t["slots"] in (1 << 19, 1 << 20, 3 << 19, 1 << 21, 3 << 20)
-    assert t["shade_block"] in (64, 128) and t["trace_min_blocks"] in (6, 8)
+    assert t["shade_block"] in (64, 128) and t["trace_min_blocks"] in (6, 8) and t["shade_sort"] in (0, 1)
     assert 1 <= t["trace_blocks_per_sm"] <= 16 and t["trace_registers"] > 0
     assert t["samples_per_second"] >= t["default_samples_per_second"] > 0
     assert tuned.state() == 0  # the view starts over after the trials
@@ -31,8 +31,8 @@ def test_autotune_keeps_the_image_and_is_remembered(rt, name, kw):
     later = rt.Session(scene, seed=21, form="wavefront")
     c = later.tuning()
     assert c["from_cache"] == 1
-    assert {k: c[k] for k in ("slots", "trace_blocks_per_sm", "shade_block", "trace_min_blocks")} == \
-        {k: t[k] for k in ("slots", "trace_blocks_per_sm", "shade_block", "trace_min_blocks")}
+    assert {k: c[k] for k in ("slots", "trace_blocks_per_sm", "shade_block", "trace_min_blocks", "shade_sort")} == \
+        {k: t[k] for k in ("slots", "trace_blocks_per_sm", "shade_block", "trace_min_blocks", "shade_sort")}
     with pytest.raises(rt.LogicError):
         later.render_to(16)
         later.autotune(16)  # a view with passes cannot be tuned
