@@ -77,6 +77,38 @@ def build(reference: Path | None = None) -> Path | None:
     return LIBRARY
 
 
+SHIM = OUT / "librenderer_b200.so"
+
+
+def build_shim(reference: Path | None = None) -> Path | None:
+    """The reference's gpu:: API served by this library: the shim INTEGRATION.md documents (its first C++ block,
+    extracted as written) compiled against the reference's renderer.h, with oracle/shim_driver.cpp, linked to the
+    product library. Returns its path, or None without the reference's sources or the product library."""
+    import re
+
+    gpu = reference_root(reference) / "src" / "gpu"
+    product = REPO / "raytracing_b200" / "_lib" / "librt_b200.so"
+    doc = REPO / "INTEGRATION.md"
+    if not (gpu / "renderer.h").exists() or not product.exists():
+        return SHIM if SHIM.exists() else None
+    OUT.mkdir(exist_ok=True)
+    inputs = [doc, HERE / "shim_driver.cpp", HERE / "ref_scene_convert.h", gpu / "renderer.h", product, Path(__file__)]
+    if SHIM.exists() and SHIM.stat().st_mtime > max(p.stat().st_mtime for p in inputs):
+        return SHIM
+    blocks = re.findall(r"```cpp\n(.*?)```", doc.read_text(), re.S)
+    if not blocks:
+        raise RuntimeError("INTEGRATION.md has no C++ block: the shim is missing")
+    source = OUT / "renderer_b200.cpp"
+    source.write_text(blocks[0])
+    _run(["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", "-Werror", "-I", str(gpu), "-I",
+          str(REPO / "include"), "-I", str(HERE), str(source), str(HERE / "shim_driver.cpp"), "-o", str(SHIM),
+          "-L", str(product.parent), "-lrt_b200", "-Wl,--no-undefined",
+          "-Wl,-rpath,$ORIGIN/../../raytracing_b200/_lib"])
+    return SHIM
+
+
 if __name__ == "__main__":
     path = build(Path(sys.argv[1]) if len(sys.argv) > 1 else None)
     print(path if path else "reference sources absent: nothing built")
+    shim = build_shim(Path(sys.argv[1]) if len(sys.argv) > 1 else None)
+    print(shim if shim else "no shim built (the reference's header or the product library is absent)")

@@ -222,3 +222,20 @@ def test_render_options_are_checked(rt):
     s = rt.builtin_scene("furnace", width=16)
     with pytest.raises((ValueError, rt.RenderError)):
         rt.render(s, passes=-1)
+
+
+def test_integration_shim_compiles_against_the_reference_header(tmp_path):
+    """INTEGRATION.md's C++ shim (the reference's gpu:: API on this C-ABI) compiles as written against the
+    reference's own src/gpu/renderer.h, warnings as errors (where the reference's sources are present)."""
+    from oracle import build_ref
+
+    header = build_ref.reference_root() / "src" / "gpu" / "renderer.h"
+    if not header.exists() or shutil.which("g++") is None:
+        pytest.skip("the reference's sources (or g++) are not here")
+    blocks = re.findall(r"```cpp\n(.*?)```", (REPO / "INTEGRATION.md").read_text(), re.S)
+    assert blocks, "INTEGRATION.md has no C++ block"
+    source = tmp_path / "renderer_b200.cpp"
+    source.write_text(blocks[0])
+    r = subprocess.run(["g++", "-std=c++20", "-fsyntax-only", "-Wall", "-Wextra", "-Werror", "-I", str(header.parent),
+                        "-I", str(REPO / "include"), str(source)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
