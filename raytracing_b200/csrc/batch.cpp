@@ -374,9 +374,12 @@ double batch_engine::step(std::vector<assignment> work)
             wide = wide && table_host_[i].scene.wide_nodes != nullptr;
         }
         const wave_buffers b = wave_->setup(group_samples[g], stream_);
-        const int64_t steps = wave_->run(b, group_depth[g], stream_, [&] {
-            return launch_wave_batch_step(w, flat, features, wide, b, trace_grid_, stream_);
-        });
+        const int64_t steps = wave_->run(
+            b, group_depth[g], stream_,
+            [&](bool draining) {
+                return launch_wave_batch_step(w, flat, features, wide, b, trace_grid_, stream_, draining);
+            },
+            work_counter_.data() + g);
         check(launch_wave_batch_partials(w, b, stream_), "launching the wavefront's partials");
         launches_ += static_cast<int>(2 * steps + 1);
     }

@@ -211,7 +211,12 @@ public:
     // render that needs them takes them from what earlier renders left in the pool
     wave_buffers setup(int64_t samples, cudaStream_t stream);
     // step() enqueues one step on `stream`; returns the steps run
-    int64_t run(const wave_buffers& b, int max_depth, cudaStream_t stream, const std::function<cudaError_t()>& step);
+    // The steps of one launch until a step queues nothing. step(draining) launches one; draining is true once the
+    // host has seen every sample of the launch claimed (work_counter, when given, at sample_count or beyond): the
+    // shade kernel then reads a slot's rows only if the slot still has work.
+    int64_t run(const wave_buffers& b, int max_depth, cudaStream_t stream,
+                const std::function<cudaError_t(bool draining)>& step,
+                const unsigned long long* work_counter = nullptr);
 
     const int max_slots;
     const int group;
@@ -226,6 +231,7 @@ private:
     device_array<unsigned> control_;
     device_array<float4> samples_;
     unsigned* queued_ = nullptr; // pinned: the queue's length after each group of steps
+    unsigned long long* claimed_ = nullptr; // pinned: the launch's work counter after each group
     cudaEvent_t done_[2] = {nullptr, nullptr};
 };
 

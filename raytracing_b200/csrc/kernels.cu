@@ -2322,15 +2322,39 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     float4* rows = static_cast<float4*>(B.slots);
     float4* shadow_rows = rows + static_cast<int64_t>(wave_rows) * n;
     const int own = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
-    // the slot's rows and its answer, all loads issued together
-    float4 r0 = stream_load(rows + own);
-    float4 r1 = stream_load(rows + n + own);
-    float4 r2 = stream_load(rows + 2 * n + own);
-    float4 r3 = stream_load(rows + 3 * n + own);
-    int4 r4 = stream_load(reinterpret_cast<const int4*>(rows) + 4 * n + own);
-    int4 r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + own);
-    longlong2 r6 = stream_load(reinterpret_cast<const longlong2*>(rows) + 6 * n + own);
-    int4 answer = stream_load(B.ext_result + own);
+    // The slot's rows and its answer: all loads issued together while samples are left to claim (nearly every slot
+    // has work); once every sample is claimed (the drain) the flags first, and the rest only for a slot with work
+    float4 r0, r1, r2, r3;
+    int4 r4, r5, answer;
+    longlong2 r6;
+    const auto load_rest = [&] {
+        r0 = stream_load(rows + own);
+        r1 = stream_load(rows + n + own);
+        r2 = stream_load(rows + 2 * n + own);
+        r3 = stream_load(rows + 3 * n + own);
+        r4 = stream_load(reinterpret_cast<const int4*>(rows) + 4 * n + own);
+        r6 = stream_load(reinterpret_cast<const longlong2*>(rows) + 6 * n + own);
+        answer = stream_load(B.ext_result + own);
+    };
+    if (!B.draining)
+    {
+        load_rest();
+        r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + own);
+    }
+    else
+    {
+        r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + own);
+        if ((static_cast<uint32_t>(r5.y) & wave_exhausted) == 0u)
+        {
+            load_rest();
+        }
+        else
+        {
+            r0 = r1 = r2 = r3 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            r4 = answer = make_int4(0, 0, 0, 0);
+            r6 = make_longlong2(0, 0);
+        }
+    }
     int i = own; // the slot this thread shades
     // SORT: the staging of the block's slots, their order, and what each slot's write-back needs
     __shared__ float4 stage[SORT ? wave_rows + 1 : 1][SORT ? render_block : 1];
@@ -3484,13 +3508,14 @@ wave_trace_function wave_flat_trace_of(bool features, int min_blocks = RTB_TRACE
 // marks (when given): three events recorded before the shade kernel, between the two kernels and after the trace
 // kernel, for per-kernel timing
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& slots, const wave_shape& shape,
-                             cudaStream_t stream, const cudaEvent_t* marks)
+                             cudaStream_t stream, const cudaEvent_t* marks, bool draining)
 {
     const int trace_grid = shape.trace_grid;
     const int shade_block = shape.shade_block > 0 ? shape.shade_block : render_block;
     wave_buffers b = slots; // with the launch's camera and RNG job, for the camera rays the trace kernel makes
     b.cam = p.cam;
     b.job = p.job;
+    b.draining = draining ? 1 : 0;
     cudaError_t e = cudaMemsetAsync(b.control, 0, 3 * sizeof(unsigned), stream);
     if (e != cudaSuccess)
     {
@@ -3532,7 +3557,7 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
 }
 
 cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, const wave_buffers& b,
-                                   int trace_grid, cudaStream_t stream)
+                                   int trace_grid, cudaStream_t stream, bool draining)
 {
     cudaError_t e = cudaMemsetAsync(b.control, 0, 3 * sizeof(unsigned), stream);
     if (e != cudaSuccess)
@@ -3541,14 +3566,16 @@ cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features
     }
     const launch_params none{};
     const auto shade = features ? wave_shade_kernel<false, true, true> : wave_shade_kernel<false, false, true>;
-    shade<<<b.slot_count / render_block, render_block, 0, stream>>>(none, b, w);
+    wave_buffers bd = b;
+    bd.draining = draining ? 1 : 0;
+    shade<<<b.slot_count / render_block, render_block, 0, stream>>>(none, bd, w);
     e = cudaGetLastError();
     if (e != cudaSuccess)
     {
         return e;
     }
     const wave_trace_function trace = flat ? wave_flat_trace_of<true>(features) : wave_trace_variant<true>(features, wide);
-    trace<<<trace_grid, render_block, 0, stream>>>(scene_view{}, b, w, nullptr);
+    trace<<<trace_grid, render_block, 0, stream>>>(scene_view{}, bd, w, nullptr);
     return cudaGetLastError();
 }
 

@@ -172,6 +172,7 @@ struct wave_buffers
     unsigned* control;
     camera_params cam;      // a session's launch: its camera and RNG job field (a batch: each job's, in its table)
     uint32_t job;
+    int32_t draining;       // every sample is claimed: the shade kernel reads a slot's rows only if it has work
 };
 size_t wave_slot_bytes();
 // Every slot without a sample (its flags row zeroed), before a launch's first step
@@ -192,7 +193,7 @@ struct wave_shape
 };
 // One step: clears the queue, the shade kernel over the slots, the trace kernel (shape.trace_grid blocks) over the queue
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, const wave_shape& shape,
-                             cudaStream_t stream, const cudaEvent_t* marks = nullptr);
+                             cudaStream_t stream, const cudaEvent_t* marks = nullptr, bool draining = false);
 // The samples of passes [pass_begin, pass_end) into the sums (chunk partials in pass order, added in chunk order)
 cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
                                int32_t chunk, cudaStream_t stream);
@@ -200,7 +201,8 @@ cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, in
 // second book's features; wide: every job's tree is four wide), and the group's samples into its jobs' chunk
 // partials (then the batch's reduction adds them into the sums)
 cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, const wave_buffers& b,
-                                   int trace_grid, cudaStream_t stream);
+                                   int trace_grid, cudaStream_t stream,
+                                   bool draining = false);
 cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream);
 // Loads the batch wavefront's kernels (every variant) now, so that no step pays for loading them
 cudaError_t preload_wave_batch();

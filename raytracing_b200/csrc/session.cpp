@@ -291,15 +291,18 @@ double session::launch(int64_t end)
     if (wave)
     {
         const bool quality = scene_->quality();
-        steps = wave_->run(b, camera_.max_depth, stream_, [&] {
-            const cudaEvent_t* m = nullptr;
-            if (timing_)
-            {
-                m = marks(static_cast<size_t>(2 + 3 * (steps + 1))) + 2 + 3 * steps;
-            }
-            ++steps;
-            return launch_wave_step(p, quality, b, shape_, stream_, m);
-        });
+        steps = wave_->run(
+            b, camera_.max_depth, stream_,
+            [&](bool draining) {
+                const cudaEvent_t* m = nullptr;
+                if (timing_)
+                {
+                    m = marks(static_cast<size_t>(2 + 3 * (steps + 1))) + 2 + 3 * steps;
+                }
+                ++steps;
+                return launch_wave_step(p, quality, b, shape_, stream_, m, draining);
+            },
+            counters_.data());
         last_kernel_launches_ = static_cast<int32_t>(2 * steps + 1);
         if (timing_)
         {

@@ -32,6 +32,10 @@ wave_runner::~wave_runner()
     {
         cudaFreeHost(queued_);
     }
+    if (claimed_)
+    {
+        cudaFreeHost(claimed_);
+    }
 }
 
 wave_buffers wave_runner::setup(int64_t samples, cudaStream_t stream)
@@ -39,6 +43,8 @@ wave_buffers wave_runner::setup(int64_t samples, cudaStream_t stream)
     if (!queued_)
     {
         check(cudaHostAlloc(reinterpret_cast<void**>(&queued_), 8 * sizeof(unsigned), cudaHostAllocDefault),
+              "allocating pinned memory");
+        check(cudaHostAlloc(reinterpret_cast<void**>(&claimed_), 2 * sizeof(unsigned long long), cudaHostAllocDefault),
               "allocating pinned memory");
         for (auto& e : done_)
         {
@@ -78,7 +84,7 @@ wave_buffers wave_runner::setup(int64_t samples, cudaStream_t stream)
 }
 
 int64_t wave_runner::run(const wave_buffers& b, int max_depth, cudaStream_t stream,
-                         const std::function<cudaError_t()>& step)
+                         const std::function<cudaError_t(bool draining)>& step, const unsigned long long* work_counter)
 {
     check(clear_wave_slots(b, stream), "clearing the path slots");
     // A sample takes at most max_depth + 1 steps (its segments, then the one that adds its last shadow ray) and a slot
@@ -88,16 +94,23 @@ int64_t wave_runner::run(const wave_buffers& b, int max_depth, cudaStream_t stre
     // Groups of steps, two in flight: the host reads one group's queue length while the next group runs; a group
     // after the end finds every slot out of work and costs a few microseconds a step
     int64_t steps = 0;
+    bool draining = false;
     for (int g = 0;; ++g)
     {
         for (int s = 0; s < group; ++s)
         {
-            check(step(), "launching a wavefront step");
+            check(step(draining), "launching a wavefront step");
         }
         steps += group;
         const int k = g & 1;
         check(cudaMemcpyAsync(queued_ + 4 * k, b.control, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream),
               "reading the queue's length");
+        if (work_counter)
+        {
+            check(cudaMemcpyAsync(claimed_ + k, work_counter, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                  stream),
+                  "reading the work counter");
+        }
         check(cudaEventRecord(done_[k], stream), "recording a CUDA event");
         if (g > 0)
         {
@@ -107,6 +120,7 @@ int64_t wave_runner::run(const wave_buffers& b, int max_depth, cudaStream_t stre
             {
                 break;
             }
+            draining = draining || (work_counter && claimed_[k ^ 1] >= static_cast<unsigned long long>(b.sample_count));
         }
         if (steps > step_limit)
         {
