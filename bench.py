@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--served-window", type=float, default=0.25, help="seconds of arrivals (a bounded sample)")
     p.add_argument("--served-step", type=float, default=0.01, help="GPU seconds a server step aims at")
     p.add_argument("--served-limit", type=float, default=300.0, help="wall seconds after which serving stops")
+    p.add_argument("--served-long-window", type=float, default=5.0,
+                   help="seconds of arrivals of the long stream (first frames of about 1,000 requests)")
     return p.parse_args()
 
 
@@ -585,6 +587,61 @@ def served_measurement(rt, torch, args) -> dict:
             "plain_note": "one render per request (a session on the resident scene), FIFO, first frame = final image"}
 
 
+def served_first_frames(rt, args) -> dict:
+    """The served stream over a long window (default 5 s of Poisson arrivals at 200/s, about 1,000 requests of the
+    same distributions), served until every request has its first frame: time-to-first-frame percentiles over all of
+    them (by resolution too), with the server refining the earlier requests meanwhile. Time to target is reported for
+    the requests that reached it in that time (the rest are cancelled: the full stream holds about 100x what one GPU
+    renders in real time)."""
+    requests = served_requests(rt, args.served_rate, args.served_long_window, seed=11)
+    scenes = {name: rt.Scene(rt.builtin_scene(name)) for name in SERVED_SCENES}
+    server = rt.Server(hbm_budget_bytes=120 << 30, step_seconds=args.served_step)
+    pending = list(range(len(requests)))
+    ids, submitted = {}, {}
+    start = time.perf_counter()
+    steps = 0
+    while True:
+        now = time.perf_counter() - start
+        while pending and requests[pending[0]]["arrival"] <= now:
+            i = pending.pop(0)
+            q = requests[i]
+            ids[i] = server.submit(scenes[q["scene"]], q["camera"], q["seed"], q["target"])
+            submitted[i] = time.perf_counter() - start
+        if not pending and all(server.poll(r)["first_frame_seconds"] >= 0 for r in ids.values()):
+            break
+        if now > args.served_long_window + 60:
+            break
+        rep = server.step()
+        steps += 1
+        if rep["active"] == 0 and rep["queued"] == 0 and pending:
+            time.sleep(max(0.0, requests[pending[0]]["arrival"] - (time.perf_counter() - start)))
+    wall = time.perf_counter() - start
+    ttff, ttt, by_size = [], [], {}
+    for i, rid in ids.items():
+        st = server.poll(rid)
+        lag = submitted[i] - requests[i]["arrival"]
+        if st["first_frame_seconds"] >= 0:
+            ttff.append(lag + st["first_frame_seconds"])
+            cam = requests[i]["camera"]
+            by_size.setdefault(f"{cam.image_width}x{cam.image_height}", []).append(lag + st["first_frame_seconds"])
+        if st["done_seconds"] >= 0:
+            ttt.append(lag + st["done_seconds"])
+    stats = server.stats()
+    server.close()
+
+    def pct(v, p):
+        return float(np.percentile(v, p)) if v else None
+
+    return {"workload": f"Poisson arrivals at {args.served_rate}/s over {args.served_long_window} s "
+                        f"({len(requests)} requests), the served stream's distributions, served until every request "
+                        f"has its first frame",
+            "requests": len(requests), "first_frames": len(ttff), "wall_s": wall, "steps": steps,
+            "ttff_p50_s": pct(ttff, 50), "ttff_p99_s": pct(ttff, 99), "ttff_max_s": max(ttff) if ttff else None,
+            "ttff_by_resolution": {k: {"requests": len(v), "p50_s": pct(v, 50), "p99_s": pct(v, 99)}
+                                   for k, v in sorted(by_size.items())},
+            "reached_target": len(ttt), "time_to_target_p50_s": pct(ttt, 50), "gpu_s": stats["gpu_seconds"]}
+
+
 def run_reference(args):
     world, rank, _ = rank_info()
     if rank != 0:
@@ -806,6 +863,8 @@ def run_b200(args):
             line["batched"] = batched
     if rank == 0 and not args.no_served:
         line["served"] = served_measurement(rt, torch, args)
+        if args.served_long_window > 0:
+            line["served"]["long_stream"] = served_first_frames(rt, args)
 
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene_desc, args, os.cpu_count() or 1)
