@@ -314,7 +314,7 @@ def reference_gpu_measurement(scene_desc, passes: int, value: float) -> dict:
             "note": "the reference's gpu::render built from its src/gpu sources for sm_100a, same scene tables"}
 
 
-def mesh_measurement(rt, torch) -> dict:
+def mesh_measurement(rt, torch, peaks: dict) -> dict:
     """The triangle-mesh workload (an icosphere of 1.31M triangles displaced by Perlin noise, GGX metal on a glossy
     plane, a 1024x512 environment map with a sun, importance-sampled; 1920x1080, 256 spp, depth 16, NEE with MIS)
     in both forms of a session: the wavefront (its default on a tree-searched scene) and the persistent kernel.
@@ -325,6 +325,17 @@ def mesh_measurement(rt, torch) -> dict:
     out = {"workload": f"mesh-ggx {desc.width}x{desc.height}, {passes} spp, depth {desc.camera.max_depth}, "
                        f"{scene.stats()['triangles']} triangles, NEE/MIS with the environment map",
            "scene_stats": scene.stats()}
+    # The tree's algorithmic bytes per query: node visits (64 B) and triangle tests (48 B) counted on the workload's
+    # own rays by the counting build (the binary walk; the four-wide walk reads 128-B nodes about half as often)
+    counting = rt.Session(scene, seed=4, launch_seconds=0.5)
+    counting.set_counting(True)
+    counting.render_to(2)
+    fetched = counting.fetch_counts()
+    cc = counting.counters()
+    counting.close()
+    queries = max(cc["rays"] + cc["shadow_rays"], 1)
+    bytes_per_query = (64 * fetched["nodes"] + 16 * fetched["spheres"] + 48 * fetched["quads"] +
+                       48 * fetched["triangles"]) / queries
     for form in ("wavefront", "persistent"):
         sess = rt.Session(scene, seed=3, form=form, launch_seconds=0.5)
         if form == "wavefront":
@@ -338,6 +349,26 @@ def mesh_measurement(rt, torch) -> dict:
                      "queries_per_s": (cnt["rays"] + cnt["shadow_rays"]) / rep["gpu_seconds"],
                      "gpu_s": rep["gpu_seconds"], "launches": rep["launches"], "segments": cnt["rays"],
                      "shadow_rays": cnt["shadow_rays"], "kernel": sess.kernel()}
+        if form == "wavefront":
+            # the walks' bytes over the trace kernel's own CUDA-event time, against the HBM roofline
+            sess.set_timing(True)
+            sess.set_camera(desc.camera)
+            sess.render_to(min(passes, 64))
+            kt = sess.kernel_times()
+            tc = sess.counters()
+            sess.set_timing(False)
+            walks = tc["rays"] + tc["shadow_rays"]
+            achieved = bytes_per_query * walks / kt["trace"][0] / 1e9
+            out["bvh_fetch_roofline"] = {
+                "bound": "hbm", "kernel": "wave_trace_kernel (four-wide walk)", "achieved": achieved,
+                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "peak_source": peaks["source"], "algorithmic_bytes_per_query": bytes_per_query,
+                "node_visits_per_query": fetched["nodes"] / queries,
+                "triangle_tests_per_query": fetched["triangles"] / queries,
+                "trace_share": kt["trace"][0] / (kt["trace"][0] + kt["shade"][0] + kt["reduce"][0]),
+                "note": "BVH node and triangle bytes a walk reads (counting build, binary walk) over the trace "
+                        "kernel's event time; the tree (49 MB of nodes, 63 MB of triangles) is about L2's size, so "
+                        "part of these bytes come from L2"}
         sess.close()
     out["wavefront_over_persistent"] = out["wavefront"]["segments_per_s"] / out["persistent"]["segments_per_s"]
     return out
@@ -856,7 +887,7 @@ def run_b200(args):
                     "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": mis_image,
                                                                 "reference_gpu": mis_ref})}
     if rank == 0 and not args.no_mesh:
-        line["mesh"] = mesh_measurement(rt, torch)
+        line["mesh"] = mesh_measurement(rt, torch, peaks)
     if not args.no_batched:
         batched = batched_measurement(rt, torch, rank, world)  # every rank: its share of the 64 jobs
         if rank == 0:
