@@ -275,6 +275,30 @@ def fp32_peak_tflops(torch) -> float:
     return best
 
 
+def config_errors(rt, seed: int) -> dict:
+    """The other workloads' error against their FP64 oracle renders (tests/golden/fp64_*.npz), beside an independent
+    render of the same spp and strategy: the first book's cover scene at 400x225, 32 passes (against the reference's
+    float renderer), and the mesh scene (level 8, GGX, environment) reduced to 240x135 at 256 spp (against the CPU
+    oracle, as the reference traces triangles only through OptiX)."""
+    from oracle import binding as oracle
+    from oracle import ref_gpu
+
+    out = {}
+    w = rt.builtin_scene("weekend", width=400, spp=16, depth=50)
+    ours = rt.render(w, seed=seed, passes=32).pixels
+    ref = ref_gpu.render(w.desc, w.width, w.height, seed=seed + 1, passes=32)[0] if ref_gpu.available() else None
+    out["cover_400x225_32spp"] = error_vs_fp64("weekend", {"this_library": ours, "reference_gpu": ref})
+    m = rt.builtin_scene("mesh-ggx", width=240, spp=16)
+    ours = rt.render(m, seed=seed, passes=256).pixels
+    cpu, _ = oracle.render(m.desc, m.width, m.height, seed=seed + 2, passes=256)
+    e = error_vs_fp64("mesh-ggx", {"this_library": ours, "cpu_oracle": cpu})
+    if "this_library" in e and "cpu_oracle" in e:
+        e["ratio"] = e["this_library"]["trimmed_rms"] / e["cpu_oracle"]["trimmed_rms"]
+        e["matched"] = bool(abs(e["ratio"] - 1.0) <= 0.05)
+    out["mesh_240x135_256spp"] = e
+    return out
+
+
 def cpu_baseline(scene, args, threads: int) -> dict:
     """The reference's CPU renderer (restated as the oracle) on a bounded band of rows of the same workload."""
     from oracle import binding as oracle
@@ -339,7 +363,7 @@ def mesh_measurement(rt, torch, peaks: dict) -> dict:
     for form in ("wavefront", "persistent"):
         sess = rt.Session(scene, seed=3, form=form, launch_seconds=0.5)
         if form == "wavefront":
-            out["autotune"] = sess.autotune(trial_passes=8)
+            out["autotune"] = sess.autotune()
         sess.render_to(16)  # warm-up: module load, buffers
         sess.set_camera(desc.camera)
         torch.cuda.synchronize()
@@ -751,7 +775,7 @@ def run_b200(args):
     session = rt.Session(scene, seed=seed, launch_seconds=0.5)
     camera = scene_desc.camera
     # The wavefront's launch shape chosen by the library's autotuner on this view (untimed, before the warm-up)
-    tuning = session.autotune(trial_passes=16)
+    tuning = session.autotune()
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def step():
@@ -886,6 +910,8 @@ def run_b200(args):
                                                                mis_image, seeds=(8, 9)),
                     "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": mis_image,
                                                                 "reference_gpu": mis_ref})}
+    if rank == 0 and not args.no_reference_gpu:
+        line["error_vs_fp64_by_config"] = config_errors(rt, seed)
     if rank == 0 and not args.no_mesh:
         line["mesh"] = mesh_measurement(rt, torch, peaks)
     if not args.no_batched:

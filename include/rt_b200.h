@@ -437,8 +437,14 @@ typedef struct rt_tuning
     double samples_per_second;  /* the chosen shape's measured speed (pixel passes a second) */
     double default_samples_per_second; /* the built-in defaults' */
 } rt_tuning;
+/* trial_passes: the passes of each measured launch (after a one-chunk launch, as the session's planner probes);
+ * 0: enough for about 32 million samples, so that every candidate pool reaches its steady state. */
 rt_status rt_session_autotune(rt_session* session, int64_t trial_passes, rt_tuning* result);
 rt_status rt_session_tuning(const rt_session* session, rt_tuning* current);
+/* Applies a shape an earlier autotune reported (slots, trace_blocks_per_sm, shade_block, trace_min_blocks, shade_sort;
+ * the other fields are ignored), so a service can keep its tunings across processes. RT_ERR_INVALID for a value the
+ * kernels do not take, RT_ERR_LOGIC for a persistent-form session. */
+rt_status rt_session_set_tuning(rt_session* session, const rt_tuning* shape);
 /* The autotuner's search on a caller-given measure (its selection logic without a GPU, for tests): the candidates
  * of a GPU whose trace kernels fit max_trace_blocks (default cap) and max_trace_blocks_roomy (roomy cap) blocks a
  * multiprocessor, each measured by measure(shape, user) in samples per second. */

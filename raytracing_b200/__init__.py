@@ -390,7 +390,13 @@ class Session:
         _check(_lib().rt_session_kernel(self._handle, C.byref(k)))
         return _kernel_dict(k)
 
-    def autotune(self, trial_passes: int = 16) -> dict:
+    def set_tuning(self, shape: dict) -> None:
+        """Applies a launch shape (a dict as autotune() and tuning() return)."""
+        t = _abi.Tuning(**{k: int(shape[k]) for k in ("slots", "trace_blocks_per_sm", "shade_block",
+                                                        "trace_min_blocks", "shade_sort")})
+        _check(_lib().rt_session_set_tuning(self._handle, C.byref(t)))
+
+    def autotune(self, trial_passes: int = 0) -> dict:
         """The wavefront's autotuner on this view (which must have no passes yet; it starts over afterwards): the
         chosen launch shape and its measured speed against the built-in defaults'."""
         t = _abi.Tuning()

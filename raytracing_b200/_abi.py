@@ -243,6 +243,7 @@ ENTRY_POINTS = [
     ("rt_session_kernel_times", C.c_int, [C.c_void_p, C.POINTER(KernelTimes)]),
     ("rt_session_autotune", C.c_int, [C.c_void_p, C.c_int64, C.POINTER(Tuning)]),
     ("rt_session_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    ("rt_session_set_tuning", C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     ("rt_autotune_simulate", C.c_int, [C.c_int32, C.c_int32, TUNE_MEASURE, C.c_void_p, C.POINTER(Tuning)]),
     ("rt_session_set_counting", C.c_int, [C.c_void_p, C.c_int32]),
     ("rt_session_fetch_counts", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64 * 4)]),

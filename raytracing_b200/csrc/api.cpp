@@ -404,6 +404,15 @@ rt_status rt_session_autotune(rt_session* session, int64_t trial_passes, rt_tuni
     });
 }
 
+rt_status rt_session_set_tuning(rt_session* session, const rt_tuning* shape)
+{
+    return guarded([&] {
+        need(session, "session");
+        need(shape, "shape");
+        session->session->set_tuning(*shape);
+    });
+}
+
 rt_status rt_session_tuning(const rt_session* session, rt_tuning* current)
 {
     return guarded([&] {

@@ -93,12 +93,13 @@ struct alignas(16) quad12
     float az, bx, by, bz;
 };
 
-// A triangle: a vertex and two edges, 48 bytes (the last float is unused), three 16-byte loads
+// A triangle: its three vertices as the mesh gives them (a vertex shared by two triangles is the same floats in both,
+// which the watertight test needs), 48 bytes (the last three floats unused), three 16-byte loads
 struct alignas(16) triangle12
 {
-    float ax, ay, az, e1x;
-    float e1y, e1z, e2x, e2y;
-    float e2z, pad0, pad1, pad2;
+    float ax, ay, az, bx;
+    float by, bz, cx, cy;
+    float cz, pad0, pad1, pad2;
 };
 
 // A material as the shading reads it (src/gpu/material.cuh:18-26), with the NEE/MIS integrator's GGX side entry

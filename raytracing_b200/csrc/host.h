@@ -325,6 +325,8 @@ public:
     // starts over afterwards), the best shape kept for this session and remembered for its scene class
     rt_tuning autotune(int64_t trial_passes);
     rt_tuning tuning() const { return tuning_; }
+    // A launch shape given by the caller (one an earlier autotune reported, kept across processes)
+    void set_tuning(const rt_tuning& t);
     // Per-kernel timing (events around every kernel of every launch; slows launches a little): rt_kernel_times
     void set_timing(bool on) { timing_ = on; }
     rt_kernel_times kernel_times() const { return times_; }

@@ -577,12 +577,12 @@ resident_scene::resident_scene(const rt_scene_desc& d)
             tr.ax = a[0];
             tr.ay = a[1];
             tr.az = a[2];
-            tr.e1x = b[0] - a[0];
-            tr.e1y = b[1] - a[1];
-            tr.e1z = b[2] - a[2];
-            tr.e2x = c[0] - a[0];
-            tr.e2y = c[1] - a[1];
-            tr.e2z = c[2] - a[2];
+            tr.bx = b[0];
+            tr.by = b[1];
+            tr.bz = b[2];
+            tr.cx = c[0];
+            tr.cy = c[1];
+            tr.cz = c[2];
             build_prim p{};
             double largest = 0;
             for (int axis = 0; axis < 3; ++axis)

@@ -20,6 +20,7 @@ namespace
 constexpr double max_launch_seconds = 0.5;              // renderer.h:413
 constexpr size_t partial_budget_bytes = size_t{1} << 30; // a launch's chunk partials: at most 1 GiB
 constexpr size_t wave_sample_budget_bytes = size_t{2} << 30; // a wavefront launch's samples (16 bytes each): 2 GiB
+constexpr double trial_samples = 32e6; // the autotuner's measured launch, by default
 } // namespace
 
 session::session(std::shared_ptr<resident_scene> scene, const rt_session_options& options)
@@ -93,6 +94,40 @@ void session::apply(const tune_candidate& c)
     tuning_.trace_registers = trace.registers;
 }
 
+void session::set_tuning(const rt_tuning& t)
+{
+    if (!wavefront_)
+    {
+        fail(RT_ERR_LOGIC, "a persistent-form session has no launch shape to set");
+    }
+    kernel_attributes shade{}, trace{};
+    const scene_view& view = scene_->view();
+    if (t.trace_min_blocks != RTB_TRACE_MIN_BLOCKS_DEFAULT && t.trace_min_blocks != wave_trace_roomy_blocks)
+    {
+        fail(RT_ERR_INVALID, "trace_min_blocks must be 8 or 6");
+    }
+    check(wave_attributes(view, scene_->quality(), shade, trace, t.trace_min_blocks), "querying the wavefront kernels");
+    if (t.trace_blocks_per_sm < 1 || t.trace_blocks_per_sm > trace.blocks_per_sm)
+    {
+        fail(RT_ERR_INVALID, "trace_blocks_per_sm must be from 1 to the trace kernel's occupancy");
+    }
+    if (t.slots < render_block || t.slots > (1 << 24) || t.slots % render_block != 0)
+    {
+        fail(RT_ERR_INVALID, "slots must be a multiple of 128 up to 2^24");
+    }
+    if (t.shade_block != render_block && t.shade_block != render_block / 2)
+    {
+        fail(RT_ERR_INVALID, "shade_block must be 64 or 128");
+    }
+    if (t.shade_sort != 0 && t.shade_sort != 1)
+    {
+        fail(RT_ERR_INVALID, "shade_sort must be 0 or 1");
+    }
+    apply({t.slots, t.trace_blocks_per_sm, t.shade_block, t.trace_min_blocks, t.shade_sort});
+    tuning_.from_cache = 0;
+    tuning_.trials = 0;
+}
+
 rt_tuning session::autotune(int64_t trial_passes)
 {
     if (!wavefront_)
@@ -103,9 +138,9 @@ rt_tuning session::autotune(int64_t trial_passes)
     {
         fail(RT_ERR_LOGIC, "autotune needs a view with no passes yet (it renders trials of its own)");
     }
-    if (trial_passes < 1 || trial_passes > 1 << 20)
+    if (trial_passes < 0 || trial_passes > 1 << 20)
     {
-        fail(RT_ERR_INVALID, "trial_passes must be in [1, 2^20]");
+        fail(RT_ERR_INVALID, "trial_passes must be in [0, 2^20]");
     }
     const scene_view& view = scene_->view();
     kernel_attributes shade{}, trace{}, roomy{};
@@ -113,22 +148,33 @@ rt_tuning session::autotune(int64_t trial_passes)
     check(wave_attributes(view, scene_->quality(), shade, roomy, wave_trace_roomy_blocks),
           "querying the wavefront kernels");
     const tune_space space = default_tune_space(trace.blocks_per_sm, roomy.blocks_per_sm);
-    const double samples = static_cast<double>(camera_.image_width) * camera_.image_height *
-                           static_cast<double>(trial_passes);
+    const double pixels = static_cast<double>(camera_.image_width) * camera_.image_height;
+    // The measured launch: whole chunks, by default about 32M samples, enough for the pool's largest candidate to
+    // reach its steady state (a launch of a few slot generations would favour small pools, which ramp up and drain
+    // sooner, over the pools a long render runs best with)
+    int64_t measured = trial_passes;
+    if (measured == 0)
+    {
+        measured = static_cast<int64_t>(std::ceil(trial_samples / pixels));
+    }
+    measured = std::max<int64_t>(pass_chunk, (measured + pass_chunk - 1) / pass_chunk * pass_chunk);
+    const int64_t max_passes =
+        std::max<int64_t>(pass_chunk, static_cast<int64_t>(wave_sample_budget_bytes / sizeof(float4)) /
+                                          (static_cast<int64_t>(padded_pixels_) * pass_chunk) * pass_chunk - pass_chunk);
+    measured = std::min(measured, max_passes);
+    const double samples = pixels * static_cast<double>(measured);
     const bool counting = counting_;
     counting_ = false;
-    // Each candidate: the best of two renders of the trial passes from a fresh image
+    // Each candidate: the best of two measured launches, each after a one-chunk launch (the planner's probe) from a
+    // fresh image
     const auto measure = [&](const tune_candidate& c) {
         apply(c);
         double best = 0;
         for (int k = 0; k < 2; ++k)
         {
             set_camera(camera_);
-            double seconds = 0;
-            while (passes_ < trial_passes)
-            {
-                seconds += launch(plan(trial_passes, options_.launch_seconds));
-            }
+            launch(pass_chunk);
+            const double seconds = launch(pass_chunk + measured);
             best = std::max(best, samples / std::max(seconds, 1e-9));
         }
         return best;

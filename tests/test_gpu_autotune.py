@@ -28,6 +28,15 @@ def test_autotune_keeps_the_image_and_is_remembered(rt, name, kw):
     assert np.array_equal(tuned.pixels(), reference)
     assert before["trials"] == 0
 
+    # a shape set by hand gives the same image too
+    manual = rt.Session(scene, seed=21, form="wavefront")
+    manual.set_tuning(dict(slots=1 << 19, trace_blocks_per_sm=4, shade_block=64, trace_min_blocks=6, shade_sort=1))
+    assert manual.tuning()["slots"] == 1 << 19 and manual.tuning()["shade_sort"] == 1
+    manual.render_to(32)
+    assert np.array_equal(manual.pixels(), reference)
+    with pytest.raises(ValueError):
+        manual.set_tuning(dict(slots=1000, trace_blocks_per_sm=4, shade_block=64, trace_min_blocks=6, shade_sort=1))
+
     later = rt.Session(scene, seed=21, form="wavefront")
     c = later.tuning()
     assert c["from_cache"] == 1

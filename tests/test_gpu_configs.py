@@ -124,3 +124,24 @@ def test_first_hits_three_ways(rt, oracle, name, width):
         _assert_first_hits(oracle, s.desc, o, d, ids, ref_ids, ts, ref_ts)
         _assert_first_hits(oracle, s.desc, o, d, ids, cpu_ids, ts, cpu_ts)
         _assert_first_hits(oracle, s.desc, o, d, ref_ids, cpu_ids, ref_ts, cpu_ts)
+
+
+@needs_reference
+def test_error_against_the_fp64_oracle_matches_the_references(rt):
+    """The glass box at its full size, 1024 spp: this library's image and the reference renderer's (same spp and
+    strategy) have the same error against the FP64 65,536-spp oracle render (tests/golden/fp64_glass.npz, made by the
+    reference's own renderer in double): PfmStats' trimmed RMS (tests/pfm_stats.cpp:344-367) within 5%."""
+    from pathlib import Path
+
+    z = np.load(Path(__file__).resolve().parent / "golden" / "fp64_glass.npz")
+    truth = z["image"].astype(np.float64)
+    s = rt.builtin_scene("glass", width=600, spp=1024, depth=50)
+
+    def trimmed(img):
+        d = img.mean(axis=2) - truth.mean(axis=2)
+        d2 = np.sort((d * d).ravel())
+        return float(np.sqrt(d2[: d2.size - int(d2.size * 0.01)].mean()))
+
+    ours = trimmed(rt.render(s, seed=31, launch_seconds=0.5).pixels)
+    ref = trimmed(ref_gpu.render(s.desc, s.width, s.height, seed=32)[0])
+    assert abs(ours / ref - 1.0) <= 0.05, (ours, ref)
