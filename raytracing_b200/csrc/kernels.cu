@@ -2277,11 +2277,14 @@ constexpr uint32_t wave_ext = 2u;       // the path's next ray is queued (its hi
 constexpr uint32_t wave_shadow = 4u;    // a shadow ray is queued (blocked or not comes back in shadow_result)
 constexpr uint32_t wave_finish = 8u;    // the sample ended at the shadow ray's vertex: it completes once the ray is in
 
-// A slot in HBM, structure of arrays: seven float4 rows of the path and its sample, three of its pending shadow ray,
-// each row slot_count long, so that a warp's loads and stores of a row are 512 contiguous bytes
-constexpr int wave_rows = 7;
+// A slot in HBM, structure of arrays: five float4 rows of the path and its sample, three of its pending shadow ray,
+// each row slot_count long, so that a warp's loads and stores of a row are 512 contiguous bytes. Rows: the ray's
+// origin and time; its direction and the last BSDF density; the throughput and the radiance's red; the radiance's
+// green and blue, the primitive the ray leaves and the rays left; the depth, the flags, the sample's number and the
+// job. The sample's pass, pixel and random-number key are not stored: they follow from its number (sample_rng).
+constexpr int wave_rows = 5;
 constexpr int wave_shadow_rows = 3;
-constexpr int wave_flags_row = 5; // depth, flags, unused, job: a slot whose row is zero has no sample
+constexpr int wave_flags_row = 4; // depth, flags, sample, job: a slot whose row is zero has no sample
 // A query's flags (its meta's second word): 1 the ray starts inside the surface it leaves, 2 a shadow ray, 4 a new
 // sample's camera ray still to be made (a primary query); the job above them (<< 3)
 constexpr int wave_query_primary = 4;
@@ -2322,6 +2325,37 @@ template <bool QUALITY, bool FEATURES>
 constexpr int wave_shade_min_blocks()
 {
     return RTB_WAVE_SHADE_MIN_BLOCKS > 0 ? RTB_WAVE_SHADE_MIN_BLOCKS : render_min_blocks<QUALITY, false, FEATURES>();
+}
+
+// Where sample number `local` of a launch (or of a batch job) lies: pass-major, then the pixels in 8x4 tiles (a
+// warp's worth); x may fall past the image's right edge or y past its bottom in the last tiles
+struct sample_place
+{
+    int64_t pass;
+    int x, y;
+};
+
+__device__ __forceinline__ sample_place place_of(int64_t local, int padded, int tiles_x, int64_t pass_begin)
+{
+    const int64_t j = local / padded;
+    const int q = static_cast<int>(local - j * padded);
+    const int tile = q >> 5;
+    const int l = q & 31;
+    return {pass_begin + j, (tile % tiles_x) * 8 + (l & 7), (tile / tiles_x) * 4 + (l >> 3)};
+}
+
+// A sample's random-number stream: its pixel, its pass within its round of strata, and the round's key
+// (seed + round * 2^32), as the persistent kernel sets them when it starts the sample
+__device__ __forceinline__ int sample_rng(const sample_place& at, int width, int round_passes, uint64_t seed,
+                                          sampler& rng)
+{
+    const int64_t round = at.pass / round_passes;
+    const int round_pass = static_cast<int>(at.pass - round * round_passes);
+    const uint64_t key = seed + (static_cast<uint64_t>(round) << 32);
+    rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
+    rng.pass = static_cast<uint32_t>(round_pass);
+    rng.pixel = static_cast<uint32_t>(at.y) * static_cast<uint32_t>(width) + static_cast<uint32_t>(at.x);
+    return round_pass;
 }
 
 // What a slot's hit needs of the shading, for the block-level sort: its material's kind and lobe, or the miss, the
@@ -2371,15 +2405,12 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     // The slot's rows and its answer: all loads issued together while samples are left to claim (nearly every slot
     // has work); once every sample is claimed (the drain) the flags first, and the rest only for a slot with work
     float4 r0, r1, r2, r3;
-    int4 r4, r5, answer;
-    longlong2 r6;
+    int4 r5, answer; // r5: the flags row
     const auto load_rest = [&] {
         r0 = stream_load(rows + own);
         r1 = stream_load(rows + n + own);
         r2 = stream_load(rows + 2 * n + own);
         r3 = stream_load(rows + 3 * n + own);
-        r4 = stream_load(reinterpret_cast<const int4*>(rows) + 4 * n + own);
-        r6 = stream_load(reinterpret_cast<const longlong2*>(rows) + 6 * n + own);
         answer = stream_load(B.ext_result + own);
     };
     if (!B.draining)
@@ -2397,8 +2428,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         else
         {
             r0 = r1 = r2 = r3 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            r4 = answer = make_int4(0, 0, 0, 0);
-            r6 = make_longlong2(0, 0);
+            answer = make_int4(0, 0, 0, 0);
         }
     }
     int i = own; // the slot this thread shades
@@ -2414,13 +2444,10 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         stage[1][t] = r1;
         stage[2][t] = r2;
         stage[3][t] = r3;
-        stage[4][t] = make_float4(__int_as_float(r4.x), __int_as_float(r4.y), __int_as_float(r4.z),
-                                  __int_as_float(r4.w));
-        stage[5][t] = make_float4(__int_as_float(r5.x), __int_as_float(r5.y), __int_as_float(r5.z),
-                                  __int_as_float(r5.w));
-        reinterpret_cast<longlong2*>(&stage[6][0])[t] = r6;
-        stage[7][t] = make_float4(__int_as_float(answer.x), __int_as_float(answer.y), __int_as_float(answer.z),
-                                  __int_as_float(answer.w));
+        stage[wave_flags_row][t] = make_float4(__int_as_float(r5.x), __int_as_float(r5.y), __int_as_float(r5.z),
+                                               __int_as_float(r5.w));
+        stage[wave_rows][t] = make_float4(__int_as_float(answer.x), __int_as_float(answer.y),
+                                          __int_as_float(answer.z), __int_as_float(answer.w));
         store_mode[t] = 0;
         if (t < shade_keys)
         {
@@ -2449,13 +2476,10 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         r1 = stage[1][j];
         r2 = stage[2][j];
         r3 = stage[3][j];
-        const float4 s4 = stage[4][j];
-        r4 = make_int4(__float_as_int(s4.x), __float_as_int(s4.y), __float_as_int(s4.z), __float_as_int(s4.w));
-        const float4 s5 = stage[5][j];
+        const float4 s5 = stage[wave_flags_row][j];
         r5 = make_int4(__float_as_int(s5.x), __float_as_int(s5.y), __float_as_int(s5.z), __float_as_int(s5.w));
-        r6 = reinterpret_cast<const longlong2*>(&stage[6][0])[j];
-        const float4 s7 = stage[7][j];
-        answer = make_int4(__float_as_int(s7.x), __float_as_int(s7.y), __float_as_int(s7.z), __float_as_int(s7.w));
+        const float4 sa = stage[wave_rows][j];
+        answer = make_int4(__float_as_int(sa.x), __float_as_int(sa.y), __float_as_int(sa.z), __float_as_int(sa.w));
     }
     uint32_t flags = static_cast<uint32_t>(r5.y);
     uint32_t shadow_rays = 0; // counted where the walks are (the trace kernel), or as queued (BATCH)
@@ -2514,16 +2538,21 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             ps.bsdf_pdf = r1.w;
             ps.throughput = make_float3(r2.x, r2.y, r2.z);
             ps.radiance = make_float3(r2.w, r3.x, r3.y);
-            rng.key = make_uint2(__float_as_uint(r3.z), __float_as_uint(r3.w));
-            rng.pixel = static_cast<uint32_t>(r4.x);
-            rng.pass = static_cast<uint32_t>(r4.y);
-            ps.from = r4.z;
-            ps.rays_left = r4.w;
+            ps.from = __float_as_int(r3.z);
+            ps.rays_left = __float_as_int(r3.w);
             ps.depth = r5.x;
             ps.specular = (flags & wave_specular) != 0u;
             ps.inward = (flags & wave_inward) != 0u;
-            sample_index = r6.x;
-            pass = r6.y;
+            sample_index = static_cast<int64_t>(static_cast<uint32_t>(r5.z));
+            if (flags & (wave_ext | wave_shadow | wave_finish))
+            {
+                // the sample's stream, from its number
+                const int64_t local = sample_index - (BATCH ? J->sample_begin : 0);
+                const sample_place at = place_of(local, BATCH ? J->padded_pixels : P.padded_pixels,
+                                                 BATCH ? J->tiles_x : P.tiles_x, BATCH ? J->pass_begin : P.pass_begin);
+                sample_rng(at, camera().width, BATCH ? J->round_passes : P.round_passes, BATCH ? J->seed : P.seed,
+                           rng);
+            }
             bool finished = false;
             float3 sample = make_float3(0.0f, 0.0f, 0.0f);
             if (flags & wave_shadow)
@@ -2632,26 +2661,20 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                                                                  static_cast<int64_t>(s))
                                         : 0;
                     const batch_job* K = BATCH ? W.jobs + k : nullptr;
-                    const int padded = BATCH ? K->padded_pixels : P.padded_pixels;
-                    const int tiles_x = BATCH ? K->tiles_x : P.tiles_x;
                     const camera_params& c = BATCH ? K->cam : P.cam;
                     const int64_t local = static_cast<int64_t>(s) - (BATCH ? K->sample_begin : 0);
-                    const int64_t j = local / padded;
-                    const int q = static_cast<int>(local - j * padded);
-                    const int tile = q >> 5;
-                    const int l = q & 31;
-                    const int x = (tile % tiles_x) * 8 + (l & 7);
-                    const int y = (tile / tiles_x) * 4 + (l >> 3);
-                    if (x < c.width && y < c.height) // a lane of a tile over the image's edge claims again
+                    const sample_place at = place_of(local, BATCH ? K->padded_pixels : P.padded_pixels,
+                                                     BATCH ? K->tiles_x : P.tiles_x,
+                                                     BATCH ? K->pass_begin : P.pass_begin);
+                    if (at.x < c.width && at.y < c.height) // a lane of a tile over the image's edge claims again
                     {
-                        px = x;
-                        py = y;
+                        px = at.x;
+                        py = at.y;
                         job = k;
                         J = K;
                         sample_index = static_cast<int64_t>(s);
-                        pass = (BATCH ? K->pass_begin : P.pass_begin) + j;
+                        pass = at.pass;
                         rng.job = BATCH ? K->job : P.job;
-                        rng.pixel = static_cast<uint32_t>(y) * static_cast<uint32_t>(c.width) + static_cast<uint32_t>(x);
                         need = false;
                         start = true;
                     }
@@ -2661,13 +2684,9 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         if (start)
         {
             // A new sample, as the persistent kernel starts one
-            const int round_passes = BATCH ? J->round_passes : P.round_passes;
-            const int64_t round = pass / round_passes;
-            round_pass = static_cast<int>(pass - round * round_passes);
-            const uint64_t key = (BATCH ? J->seed : P.seed) + (static_cast<uint64_t>(round) << 32);
-            rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
-            rng.pass = static_cast<uint32_t>(round_pass);
             const camera_params& cam = camera();
+            round_pass = sample_rng({pass, px, py}, cam.width, BATCH ? J->round_passes : P.round_passes,
+                                    BATCH ? J->seed : P.seed, rng);
             // Under a tree walk and the heavier shading (NEE/MIS, the second book's features) the trace kernel makes
             // the camera ray, a warp's 32 at once, instead of this warp for its few new samples: the mesh +3.6%, the
             // second book's final scene +3.7%. The books' plain sphere scenes (-2%) and the flat searches (-3% to
@@ -2775,7 +2794,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                 const int j = i - static_cast<int>(blockIdx.x * blockDim.x);
                 if (flags & wave_exhausted)
                 {
-                    stage[5][j] = make_float4(0.0f, __int_as_float(static_cast<int>(flags)), 0.0f, 0.0f);
+                    stage[wave_flags_row][j] = make_float4(0.0f, __int_as_float(static_cast<int>(flags)), 0.0f, 0.0f);
                     store_mode[j] = 1;
                 }
                 else
@@ -2783,14 +2802,11 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                     stage[0][j] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time);
                     stage[1][j] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf);
                     stage[2][j] = make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x);
-                    stage[3][j] = make_float4(ps.radiance.y, ps.radiance.z, __uint_as_float(rng.key.x),
-                                              __uint_as_float(rng.key.y));
-                    stage[4][j] = make_float4(__int_as_float(static_cast<int>(rng.pixel)),
-                                              __int_as_float(static_cast<int>(rng.pass)), __int_as_float(ps.from),
+                    stage[3][j] = make_float4(ps.radiance.y, ps.radiance.z, __int_as_float(ps.from),
                                               __int_as_float(ps.rays_left));
-                    stage[5][j] = make_float4(__int_as_float(ps.depth), __int_as_float(static_cast<int>(flags)), 0.0f,
-                                              __int_as_float(job));
-                    reinterpret_cast<longlong2*>(&stage[6][0])[j] = make_longlong2(sample_index, pass);
+                    stage[wave_flags_row][j] =
+                        make_float4(__int_as_float(ps.depth), __int_as_float(static_cast<int>(flags)),
+                                    __uint_as_float(static_cast<uint32_t>(sample_index)), __int_as_float(job));
                     store_mode[j] = 2;
                 }
             }
@@ -2805,13 +2821,12 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                 stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf));
                 stream_store(rows + 2 * n + i,
                              make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x));
-                stream_store(rows + 3 * n + i, make_float4(ps.radiance.y, ps.radiance.z, __uint_as_float(rng.key.x),
-                                                           __uint_as_float(rng.key.y)));
-                stream_store(reinterpret_cast<int4*>(rows) + 4 * n + i,
-                             make_int4(static_cast<int>(rng.pixel), static_cast<int>(rng.pass), ps.from, ps.rays_left));
+                stream_store(rows + 3 * n + i, make_float4(ps.radiance.y, ps.radiance.z, __int_as_float(ps.from),
+                                                           __int_as_float(ps.rays_left)));
                 stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
-                             make_int4(ps.depth, static_cast<int>(flags), 0, job));
-                stream_store(reinterpret_cast<longlong2*>(rows) + 6 * n + i, make_longlong2(sample_index, pass));
+                             make_int4(ps.depth, static_cast<int>(flags), static_cast<int>(static_cast<uint32_t>(
+                                                                              sample_index)),
+                                       job));
             }
         }
     }
@@ -2823,7 +2838,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         const int mode = store_mode[t];
         if (mode == 1)
         {
-            const float4 s5 = stage[5][t];
+            const float4 s5 = stage[wave_flags_row][t];
             stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + own,
                          make_int4(0, __float_as_int(s5.y), 0, 0));
         }
@@ -2833,16 +2848,10 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             stream_store(rows + n + own, stage[1][t]);
             stream_store(rows + 2 * n + own, stage[2][t]);
             stream_store(rows + 3 * n + own, stage[3][t]);
-            const float4 s4 = stage[4][t];
-            stream_store(reinterpret_cast<int4*>(rows) + 4 * n + own,
-                         make_int4(__float_as_int(s4.x), __float_as_int(s4.y), __float_as_int(s4.z),
-                                   __float_as_int(s4.w)));
-            const float4 s5 = stage[5][t];
+            const float4 s5 = stage[wave_flags_row][t];
             stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + own,
                          make_int4(__float_as_int(s5.x), __float_as_int(s5.y), __float_as_int(s5.z),
                                    __float_as_int(s5.w)));
-            stream_store(reinterpret_cast<longlong2*>(rows) + 6 * n + own,
-                         reinterpret_cast<const longlong2*>(&stage[6][0])[t]);
         }
     }
 }

@@ -52,6 +52,10 @@ wave_buffers wave_runner::setup(int64_t samples, cudaStream_t stream)
         }
         control_.allocate_async(4, stream);
     }
+    if (samples >= (int64_t{1} << 32))
+    {
+        fail(RT_ERR_CAPACITY, "a wavefront run holds fewer than 2^32 samples (a slot keeps its sample's number in 32 bits)");
+    }
     const int64_t wanted = (samples + render_block - 1) / render_block * render_block;
     const auto n = static_cast<size_t>(std::min<int64_t>(max_slots, std::max<int64_t>(wanted, render_block)));
     // grown by doubling, never shrunk: a stream of launches of growing size reallocates a few times, not every time
