@@ -419,8 +419,7 @@ rt_status rt_session_kernel_times(const rt_session* session, rt_kernel_times* ti
  * kernels' shapes, renderer.cu:201-308): short renders of the session's view under candidate launch shapes, one knob
  * after another from the built-in defaults: the trace kernel's register cap (as the minimum blocks per multiprocessor
  * its launch bounds give: 8, or 6 with more registers a thread) and its grid (blocks per multiprocessor); the slot
- * pool, which is the query queue's capacity (two queries a slot); whether the shade kernel first sorts its block's
- * slots by what their hits need (material, miss, a new sample), and its block size. The best shape stays
+ * pool, which is the query queue's capacity (two queries a slot); the shade kernel's block size. The best shape stays
  * with the session and is remembered, per device and scene class (flat or tree, integrator, features, triangles,
  * size), for the sessions made after it. The image does not depend on the shape. The view must have no passes yet
  * (RT_ERR_LOGIC otherwise) and starts over afterwards; a persistent-form session has nothing to tune (slots 0). */
@@ -433,7 +432,7 @@ typedef struct rt_tuning
     int32_t trace_registers;    /* the chosen trace kernel's registers a thread */
     int32_t trials;             /* renders measured (0: the shape came from an earlier session's tuning, or defaults) */
     int32_t from_cache;         /* 1: taken from an earlier tuning of the same scene class */
-    int32_t shade_sort;         /* 1: the shade kernel sorts its block's slots by what their hits need first */
+    int32_t pad0;
     double samples_per_second;  /* the chosen shape's measured speed (pixel passes a second) */
     double default_samples_per_second; /* the built-in defaults' */
 } rt_tuning;
@@ -441,7 +440,7 @@ typedef struct rt_tuning
  * 0: enough for about 32 million samples, so that every candidate pool reaches its steady state. */
 rt_status rt_session_autotune(rt_session* session, int64_t trial_passes, rt_tuning* result);
 rt_status rt_session_tuning(const rt_session* session, rt_tuning* current);
-/* Applies a shape an earlier autotune reported (slots, trace_blocks_per_sm, shade_block, trace_min_blocks, shade_sort;
+/* Applies a shape an earlier autotune reported (slots, trace_blocks_per_sm, shade_block, trace_min_blocks;
  * the other fields are ignored), so a service can keep its tunings across processes. RT_ERR_INVALID for a value the
  * kernels do not take, RT_ERR_LOGIC for a persistent-form session. */
 rt_status rt_session_set_tuning(rt_session* session, const rt_tuning* shape);

@@ -58,7 +58,7 @@ def load() -> C.CDLL:
                                             C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         lib.oracle_hit_distances.restype = C.c_int
         lib.oracle_hit_distances.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int64,
-                                             C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+                                             C.POINTER(C.c_int32), C.c_double, C.POINTER(C.c_double)]
         lib.oracle_image_compare.restype = C.c_int
         lib.oracle_image_compare.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, C.c_int32,
                                              C.c_int32, C.POINTER(CompareResult)]
@@ -106,9 +106,9 @@ def closest_hits(desc, origins: np.ndarray, directions: np.ndarray, brute_force:
     return ids, ts
 
 
-def hit_distances(desc, origins: np.ndarray, directions: np.ndarray, ids: np.ndarray) -> np.ndarray:
+def hit_distances(desc, origins: np.ndarray, directions: np.ndarray, ids: np.ndarray, slack: float = 0.0) -> np.ndarray:
     """Where, in double, each ray meets primitive ids[i] (source index space) over (0.001, inf); inf where it does
-    not or ids[i] < 0."""
+    not or ids[i] < 0. slack: a quad's or triangle's barycentrics accepted that far outside their bounds."""
     lib = load()
     o = np.ascontiguousarray(origins, dtype=np.float64).reshape(-1, 3)
     d = np.ascontiguousarray(directions, dtype=np.float64).reshape(-1, 3)
@@ -116,18 +116,24 @@ def hit_distances(desc, origins: np.ndarray, directions: np.ndarray, ids: np.nda
     ts = np.empty(k.size, dtype=np.float64)
     status = lib.oracle_hit_distances(_desc_pointer(desc), o.ctypes.data_as(C.POINTER(C.c_double)),
                                       d.ctypes.data_as(C.POINTER(C.c_double)), k.size,
-                                      k.ctypes.data_as(C.POINTER(C.c_int32)), ts.ctypes.data_as(C.POINTER(C.c_double)))
+                                      k.ctypes.data_as(C.POINTER(C.c_int32)), slack,
+                                      ts.ctypes.data_as(C.POINTER(C.c_double)))
     if status != 0:
         raise RuntimeError(lib.oracle_last_error().decode())
     return ts
+
+
+EDGE_SLACK = 1e-4  # barycentric slack of a float search's hit on an edge two primitives share
 
 
 def first_hit_mismatches(desc, origins, directions, ids, ref_ids, ts=None, ref_ts=None, tie_rel: float = 1e-6) -> dict:
     """First-hit parity of `ids` against `ref_ids` on the same rays (both source index space, -1 a miss). Of the rays
     whose ids differ, a tie is one where both searches hit a surface at the same distance within `tie_rel` relative
     (the reference's tracer-check class `ties`, tests/tracer_check_layout.h: another primitive at the same t): either
-    the double search meets both primitives within `tie_rel` of each other, or the two searches' own distances
-    (`ts`, `ref_ts`, where given) agree within `tie_rel`. Every other difference is a mismatch."""
+    the double search meets both primitives within `tie_rel` of each other (each quad or triangle taken with its
+    edges widened by EDGE_SLACK of its size, the float rounding of a hit on the edge it shares with its neighbour), or
+    the two searches' own distances (`ts`, `ref_ts`, where given) agree within `tie_rel`. Every other difference is a
+    mismatch; `examples` lists a few (ray, ids, distances)."""
     ids = np.asarray(ids).reshape(-1)
     ref_ids = np.asarray(ref_ids).reshape(-1)
     bad = np.flatnonzero(ids != ref_ids)
@@ -135,8 +141,8 @@ def first_hit_mismatches(desc, origins, directions, ids, ref_ids, ts=None, ref_t
     if bad.size:
         o = np.asarray(origins, dtype=np.float64).reshape(-1, 3)[bad]
         d = np.asarray(directions, dtype=np.float64).reshape(-1, 3)[bad]
-        ta = hit_distances(desc, o, d, ids[bad])
-        tb = hit_distances(desc, o, d, ref_ids[bad])
+        ta = hit_distances(desc, o, d, ids[bad], EDGE_SLACK)
+        tb = hit_distances(desc, o, d, ref_ids[bad], EDGE_SLACK)
 
         def close(a, b):
             both = np.isfinite(a) & np.isfinite(b) & (ids[bad] >= 0) & (ref_ids[bad] >= 0)
@@ -149,8 +155,16 @@ def first_hit_mismatches(desc, origins, directions, ids, ref_ids, ts=None, ref_t
             tie |= close(np.asarray(ts, dtype=np.float64).reshape(-1)[bad],
                          np.asarray(ref_ts, dtype=np.float64).reshape(-1)[bad])
         ties = int(np.count_nonzero(tie))
+        others = np.flatnonzero(~tie)[:5]
+        examples = [{"ray": int(bad[k]), "ids": [int(ids[bad[k]]), int(ref_ids[bad[k]])],
+                     "double_t": [float(ta[k]), float(tb[k])],
+                     "own_t": [float(np.asarray(ts).reshape(-1)[bad[k]]) if ts is not None else None,
+                               float(np.asarray(ref_ts).reshape(-1)[bad[k]]) if ref_ts is not None else None]}
+                    for k in others]
+    else:
+        examples = []
     return {"rays": int(ids.size), "mismatches": int(bad.size), "ties": ties,
-            "non_tie_mismatches": int(bad.size) - ties, "tie_rel": tie_rel}
+            "non_tie_mismatches": int(bad.size) - ties, "tie_rel": tie_rel, "examples": examples}
 
 
 def image_compare(a: np.ndarray, b: np.ndarray, tile: int = 32) -> dict:

@@ -327,7 +327,8 @@ struct quad
         bbox = enclose(aabb::from_corners(q, q + u + v), aabb::from_corners(q + u, q + v));
     }
 
-    std::optional<hit_record> hit(const ray& r, interval ray_t) const // quad.ixx:68-106
+    // slack (the first-hit test's tie rule only): alpha and beta accepted that far outside [0, 1]
+    std::optional<hit_record> hit(const ray& r, interval ray_t, double slack = 0) const // quad.ixx:68-106
     {
         const double denom = dot(normal, r.direction);
         if (std::fabs(denom) < 1e-8)
@@ -343,7 +344,7 @@ struct quad
         const vec3 p = intersection - q;
         const double alpha = dot(w, cross(p, v));
         const double beta = dot(w, cross(u, p));
-        const interval unit{0, 1};
+        const interval unit{-slack, 1 + slack};
         if (!unit.contains(alpha) || !unit.contains(beta))
         {
             return std::nullopt;
@@ -394,7 +395,8 @@ struct triangle
         const point3 hi{std::max({a.x, b.x, c.x}), std::max({a.y, b.y, c.y}), std::max({a.z, b.z, c.z})};
         bbox = aabb::from_corners(lo, hi);
     }
-    std::optional<hit_record> hit(const ray& r, interval ray_t) const
+    // slack (the first-hit test's tie rule only): barycentrics accepted that far outside the triangle
+    std::optional<hit_record> hit(const ray& r, interval ray_t, double slack = 0) const
     {
         const vec3 e1 = b - a;
         const vec3 e2 = c - a;
@@ -407,13 +409,13 @@ struct triangle
         const double inv = 1 / det;
         const vec3 tv = r.origin - a;
         const double beta = dot(tv, pv) * inv;
-        if (beta < 0 || beta > 1)
+        if (beta < -slack || beta > 1 + slack)
         {
             return std::nullopt;
         }
         const vec3 qv = cross(tv, e1);
         const double gamma = dot(r.direction, qv) * inv;
-        if (gamma < 0 || beta + gamma > 1)
+        if (gamma < -slack || beta + gamma > 1 + slack)
         {
             return std::nullopt;
         }
@@ -504,7 +506,7 @@ public:
 
     // Primitive `id` alone (source index space: spheres, then quads, then triangles), for the first-hit test's tie
     // rule: where it is hit along the ray in double, if at all
-    std::optional<hit_record> hit_id(int id, const ray& r, interval t) const
+    std::optional<hit_record> hit_id(int id, const ray& r, interval t, double slack = 0) const
     {
         const auto n_spheres = static_cast<int>(spheres.size());
         const auto n_quads = static_cast<int>(quads.size());
@@ -518,10 +520,10 @@ public:
         }
         if (id < n_spheres + n_quads)
         {
-            return quads[static_cast<size_t>(id - n_spheres)].hit(r, t);
+            return quads[static_cast<size_t>(id - n_spheres)].hit(r, t, slack);
         }
         const auto k = static_cast<size_t>(id - n_spheres - n_quads);
-        return k < triangles.size() ? triangles[k].hit(r, t) : std::nullopt;
+        return k < triangles.size() ? triangles[k].hit(r, t, slack) : std::nullopt;
     }
 
     // The closest hit by testing every primitive in turn (hittable_list::hit, hittable.ixx:170-183): the brute-force

@@ -174,11 +174,12 @@ int oracle_closest_hits(const rt_scene_desc* desc, const double* origins, const 
 }
 
 // For the first-hit test's tie rule: where, in double, each ray meets the primitive ids[i] (source index space) over
-// (0.001, inf), or inf where it does not (or ids[i] < 0). A mismatch between two searches is a tie when both
+// (0.001, inf), or inf where it does not (or ids[i] < 0); a quad's or a triangle's barycentrics may lie `slack` outside
+// their bounds (a float search's hit on the edge a neighbour shares). A mismatch between two searches is a tie when both
 // primitives are met at the same distance within the stated relative tolerance (coplanar or touching faces: the
 // reference's tracer-check class `ties`, tests/tracer_check_layout.h).
 int oracle_hit_distances(const rt_scene_desc* desc, const double* origins, const double* directions, int64_t count,
-                         const int32_t* ids, double* ts)
+                         const int32_t* ids, double slack, double* ts)
 {
     oracle::scene s;
     const char* error = nullptr;
@@ -192,7 +193,7 @@ int oracle_hit_distances(const rt_scene_desc* desc, const double* origins, const
         const oracle::ray r{{origins[3 * i], origins[3 * i + 1], origins[3 * i + 2]},
                             {directions[3 * i], directions[3 * i + 1], directions[3 * i + 2]},
                             0};
-        const auto rec = s.geometry.hit_id(ids[i], r, oracle::interval{0.001, oracle::infinity});
+        const auto rec = s.geometry.hit_id(ids[i], r, oracle::interval{0.001, oracle::infinity}, slack);
         ts[i] = rec ? rec->t : oracle::infinity;
     }
     return 0;

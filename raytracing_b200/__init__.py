@@ -393,7 +393,7 @@ class Session:
     def set_tuning(self, shape: dict) -> None:
         """Applies a launch shape (a dict as autotune() and tuning() return)."""
         t = _abi.Tuning(**{k: int(shape[k]) for k in ("slots", "trace_blocks_per_sm", "shade_block",
-                                                        "trace_min_blocks", "shade_sort")})
+                                                        "trace_min_blocks")})
         _check(_lib().rt_session_set_tuning(self._handle, C.byref(t)))
 
     def autotune(self, trial_passes: int = 0) -> dict:

@@ -89,7 +89,7 @@ class KernelTimes(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("slots", C.c_int32), ("trace_blocks_per_sm", C.c_int32), ("shade_block", C.c_int32),
                 ("trace_min_blocks", C.c_int32), ("trace_registers", C.c_int32), ("trials", C.c_int32),
-                ("from_cache", C.c_int32), ("shade_sort", C.c_int32), ("samples_per_second", C.c_double),
+                ("from_cache", C.c_int32), ("pad0", C.c_int32), ("samples_per_second", C.c_double),
                 ("default_samples_per_second", C.c_double)]
 
 

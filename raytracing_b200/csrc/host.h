@@ -276,14 +276,12 @@ struct tune_candidate
     int trace_blocks_per_sm;
     int shade_block;
     int trace_min_blocks;
-    int shade_sort;
 };
 struct tune_space
 {
     std::vector<std::pair<int, int>> trace; // (register cap as min blocks, blocks per multiprocessor)
     std::vector<int> slots;
     std::vector<int> shade_blocks;
-    std::vector<int> shade_sorts;
 };
 struct tune_outcome
 {

@@ -2358,44 +2358,16 @@ __device__ __forceinline__ int sample_rng(const sample_place& at, int width, int
     return round_pass;
 }
 
-// What a slot's hit needs of the shading, for the block-level sort: its material's kind and lobe, or the miss, the
-// sample's end, a slot without a sample, a slot out of work (last). Only the grouping depends on it.
-constexpr int shade_keys = 12;
-__device__ __forceinline__ int shade_key(const scene_view& S, uint32_t flags, const int4& answer)
-{
-    if (flags & wave_exhausted)
-    {
-        return shade_keys - 1;
-    }
-    if ((flags & wave_finish) || !(flags & wave_ext))
-    {
-        return shade_keys - 2; // a sample that ends here or a slot that needs one: a camera ray is next
-    }
-    const int id = answer.x;
-    if (id < 0 || id >= S.prim_count)
-    {
-        return shade_keys - 3; // the sky or the environment (or a particle of smoke)
-    }
-    const material12* m = S.materials + __ldg(S.prim_material + id);
-    const int kind = __ldg(&m->kind);
-    const int lobe = __ldg(&m->lobe);
-    return min(kind, 4) * 2 + (lobe != RT_MICROFACET_NONE ? 1 : 0);
-}
-
 // A slot's step: the last walk's answers, the shading, the sample's end, a new sample, the next rays queued.
 // BATCH: the slots render the samples of a group of batch jobs (W), each slot its job's scene, camera and integrator
 // (QUALITY is then the job's own); otherwise the launch's one view (P).
 // Every load of the slot's rows and answer is issued at the start, before any of them is needed, so the step waits
 // for one round trip to memory, not one for the flags and another for what they say to read.
-// SORT (a session's launch): the block's slots are first staged in shared memory (coalesced loads), sorted by what
-// their hits need of the shading (shade_key: a counting sort of the block's 64 or 128 keys), shaded by the threads in
-// that order, so that a warp's lanes take the same branches, and written back from shared memory in slot order.
-template <bool QUALITY, bool FEATURES, bool BATCH, bool SORT = false>
+template <bool QUALITY, bool FEATURES, bool BATCH>
 __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY || BATCH, FEATURES>())
     wave_shade_kernel(const __grid_constant__ launch_params P, const __grid_constant__ wave_buffers B,
                       const __grid_constant__ wave_batch W)
 {
-    static_assert(!(SORT && BATCH), "the sorted step is a session's");
     const int n = B.slot_count;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned lanes_below = (1u << lane) - 1u;
@@ -2431,56 +2403,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             answer = make_int4(0, 0, 0, 0);
         }
     }
-    int i = own; // the slot this thread shades
-    // SORT: the staging of the block's slots, their order, and what each slot's write-back needs
-    __shared__ float4 stage[SORT ? wave_rows + 1 : 1][SORT ? render_block : 1];
-    __shared__ int order[SORT ? render_block : 1];
-    __shared__ int bins[SORT ? shade_keys : 1];
-    __shared__ uint8_t store_mode[SORT ? render_block : 1]; // 0 nothing, 1 the flags row, 2 every row
-    if constexpr (SORT)
-    {
-        const int t = static_cast<int>(threadIdx.x);
-        stage[0][t] = r0;
-        stage[1][t] = r1;
-        stage[2][t] = r2;
-        stage[3][t] = r3;
-        stage[wave_flags_row][t] = make_float4(__int_as_float(r5.x), __int_as_float(r5.y), __int_as_float(r5.z),
-                                               __int_as_float(r5.w));
-        stage[wave_rows][t] = make_float4(__int_as_float(answer.x), __int_as_float(answer.y),
-                                          __int_as_float(answer.z), __int_as_float(answer.w));
-        store_mode[t] = 0;
-        if (t < shade_keys)
-        {
-            bins[t] = 0;
-        }
-        __syncthreads();
-        const int key = shade_key(P.scene, static_cast<uint32_t>(r5.y), answer);
-        const int rank = atomicAdd(&bins[key], 1);
-        __syncthreads();
-        if (t == 0)
-        {
-            int sum = 0;
-            for (int k = 0; k < shade_keys; ++k)
-            {
-                const int c = bins[k];
-                bins[k] = sum;
-                sum += c;
-            }
-        }
-        __syncthreads();
-        order[bins[key] + rank] = t;
-        __syncthreads();
-        const int j = order[t];
-        i = static_cast<int>(blockIdx.x * blockDim.x) + j;
-        r0 = stage[0][j];
-        r1 = stage[1][j];
-        r2 = stage[2][j];
-        r3 = stage[3][j];
-        const float4 s5 = stage[wave_flags_row][j];
-        r5 = make_int4(__float_as_int(s5.x), __float_as_int(s5.y), __float_as_int(s5.z), __float_as_int(s5.w));
-        const float4 sa = stage[wave_rows][j];
-        answer = make_int4(__float_as_int(sa.x), __float_as_int(sa.y), __float_as_int(sa.z), __float_as_int(sa.w));
-    }
+    const int i = own; // the slot this thread shades
     uint32_t flags = static_cast<uint32_t>(r5.y);
     uint32_t shadow_rays = 0; // counted where the walks are (the trace kernel), or as queued (BATCH)
     // a warp whose slots have all run out of work has nothing left to do in this launch
@@ -2788,29 +2711,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         {
             flags = (flags & ~(wave_specular | wave_inward)) | (ps.specular ? wave_specular : 0u) |
                     (ps.inward ? wave_inward : 0u);
-            if constexpr (SORT)
-            {
-                // into the staging, written back in slot order below
-                const int j = i - static_cast<int>(blockIdx.x * blockDim.x);
-                if (flags & wave_exhausted)
-                {
-                    stage[wave_flags_row][j] = make_float4(0.0f, __int_as_float(static_cast<int>(flags)), 0.0f, 0.0f);
-                    store_mode[j] = 1;
-                }
-                else
-                {
-                    stage[0][j] = make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time);
-                    stage[1][j] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf);
-                    stage[2][j] = make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x);
-                    stage[3][j] = make_float4(ps.radiance.y, ps.radiance.z, __int_as_float(ps.from),
-                                              __int_as_float(ps.rays_left));
-                    stage[wave_flags_row][j] =
-                        make_float4(__int_as_float(ps.depth), __int_as_float(static_cast<int>(flags)),
-                                    __uint_as_float(static_cast<uint32_t>(sample_index)), __int_as_float(job));
-                    store_mode[j] = 2;
-                }
-            }
-            else if (flags & wave_exhausted)
+            if (flags & wave_exhausted)
             {
                 stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
                              make_int4(0, static_cast<int>(flags), 0, 0));
@@ -2828,30 +2729,6 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                                                                               sample_index)),
                                        job));
             }
-        }
-    }
-    if constexpr (SORT)
-    {
-        // the block's slots written back in slot order: each row's stores coalesced
-        __syncthreads();
-        const int t = static_cast<int>(threadIdx.x);
-        const int mode = store_mode[t];
-        if (mode == 1)
-        {
-            const float4 s5 = stage[wave_flags_row][t];
-            stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + own,
-                         make_int4(0, __float_as_int(s5.y), 0, 0));
-        }
-        else if (mode == 2)
-        {
-            stream_store(rows + own, stage[0][t]);
-            stream_store(rows + n + own, stage[1][t]);
-            stream_store(rows + 2 * n + own, stage[2][t]);
-            stream_store(rows + 3 * n + own, stage[3][t]);
-            const float4 s5 = stage[wave_flags_row][t];
-            stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + own,
-                         make_int4(__float_as_int(s5.x), __float_as_int(s5.y), __float_as_int(s5.z),
-                                   __float_as_int(s5.w)));
         }
     }
 }
@@ -3514,16 +3391,8 @@ wave_trace_function wave_trace_variant(bool features, bool wide)
     return features ? wave_trace_kernel<true, BATCH, false> : wave_trace_kernel<false, BATCH, false>;
 }
 
-wave_shade_function wave_shade_of(bool quality, bool features, bool sort = false)
+wave_shade_function wave_shade_of(bool quality, bool features)
 {
-    if (sort)
-    {
-        if (quality)
-        {
-            return features ? wave_shade_kernel<true, true, false, true> : wave_shade_kernel<true, false, false, true>;
-        }
-        return features ? wave_shade_kernel<false, true, false, true> : wave_shade_kernel<false, false, false, true>;
-    }
     if (quality)
     {
         return features ? wave_shade_kernel<true, true, false> : wave_shade_kernel<true, false, false>;
@@ -3581,8 +3450,7 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     {
         cudaEventRecord(marks[0], stream);
     }
-    wave_shade_of(quality, features, shape.shade_sort != 0)<<<b.slot_count / shade_block, shade_block, 0, stream>>>(
-        p, b, wave_batch{});
+    wave_shade_of(quality, features)<<<b.slot_count / shade_block, shade_block, 0, stream>>>(p, b, wave_batch{});
     e = cudaGetLastError();
     if (e != cudaSuccess)
     {
@@ -3678,10 +3546,10 @@ cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, in
 }
 
 cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace,
-                            int trace_min_blocks, bool shade_sort)
+                            int trace_min_blocks)
 {
     const bool features = has_features(scene);
-    const cudaError_t e = attributes_of(wave_shade_of(quality, features, shade_sort), shade);
+    const cudaError_t e = attributes_of(wave_shade_of(quality, features), shade);
     if (e != cudaSuccess)
     {
         return e;

@@ -179,7 +179,7 @@ size_t wave_slot_bytes();
 cudaError_t clear_wave_slots(const wave_buffers& b, cudaStream_t stream);
 // How a session's wavefront step is launched (the autotuner's choice): the trace kernel's grid and register cap (its
 // minimum resident blocks per multiprocessor: RTB_TRACE_MIN_BLOCKS or wave_trace_roomy_blocks), the shade kernel's
-// block size (64 or 128 threads) and whether it sorts its block's slots before shading them
+// block size (64 or 128 threads)
 constexpr int wave_trace_roomy_blocks = 6;
 #ifndef RTB_TRACE_MIN_BLOCKS_DEFAULT
 #define RTB_TRACE_MIN_BLOCKS_DEFAULT 8
@@ -189,7 +189,6 @@ struct wave_shape
     int trace_grid;
     int shade_block;
     int trace_min_blocks;
-    int shade_sort; // 1: the shade kernel sorts its block's slots by what their hits need (SORT)
 };
 // One step: clears the queue, the shade kernel over the slots, the trace kernel (shape.trace_grid blocks) over the queue
 cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_buffers& b, const wave_shape& shape,
@@ -210,7 +209,7 @@ cudaError_t preload_wave_batch();
 // The shade kernel's and the session's trace kernel's attributes (the trace kernel of the scene's search, at the given
 // register cap)
 cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace,
-                            int trace_min_blocks = RTB_TRACE_MIN_BLOCKS_DEFAULT, bool shade_sort = false);
+                            int trace_min_blocks = RTB_TRACE_MIN_BLOCKS_DEFAULT);
 
 // Parity hooks: closest hits of given rays (source ids through prim_source), and the camera rays of one pass
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,

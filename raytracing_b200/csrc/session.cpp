@@ -78,7 +78,6 @@ void session::apply(const tune_candidate& c)
     shape_.trace_grid = multiprocessors_ * c.trace_blocks_per_sm;
     shape_.shade_block = c.shade_block;
     shape_.trace_min_blocks = c.trace_min_blocks;
-    shape_.shade_sort = c.shade_sort;
     const int from_cache = tuning_.from_cache;
     const int trials = tuning_.trials;
     const double speed = tuning_.samples_per_second;
@@ -119,11 +118,7 @@ void session::set_tuning(const rt_tuning& t)
     {
         fail(RT_ERR_INVALID, "shade_block must be 64 or 128");
     }
-    if (t.shade_sort != 0 && t.shade_sort != 1)
-    {
-        fail(RT_ERR_INVALID, "shade_sort must be 0 or 1");
-    }
-    apply({t.slots, t.trace_blocks_per_sm, t.shade_block, t.trace_min_blocks, t.shade_sort});
+    apply({t.slots, t.trace_blocks_per_sm, t.shade_block, t.trace_min_blocks});
     tuning_.from_cache = 0;
     tuning_.trials = 0;
 }

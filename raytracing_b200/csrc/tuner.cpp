@@ -46,14 +46,13 @@ tune_space default_tune_space(int max_trace_blocks, int max_trace_blocks_roomy)
     }
     s.slots = {1 << 19, 1 << 20, 3 << 19, 1 << 21, 3 << 20};
     s.shade_blocks = {render_block, render_block / 2};
-    s.shade_sorts = {0, 1};
     return s;
 }
 
 tune_candidate default_candidate(int slots, int max_trace_blocks)
 {
     return {slots, std::min(RTB_TRACE_MIN_BLOCKS_DEFAULT, std::max(1, max_trace_blocks)), render_block,
-            RTB_TRACE_MIN_BLOCKS_DEFAULT, 0};
+            RTB_TRACE_MIN_BLOCKS_DEFAULT};
 }
 
 rt_tuning to_tuning(const tune_candidate& c)
@@ -63,7 +62,6 @@ rt_tuning to_tuning(const tune_candidate& c)
     t.trace_blocks_per_sm = c.trace_blocks_per_sm;
     t.shade_block = c.shade_block;
     t.trace_min_blocks = c.trace_min_blocks;
-    t.shade_sort = c.shade_sort;
     return t;
 }
 
@@ -77,8 +75,7 @@ tune_outcome coordinate_descent(const tune_candidate& start, const tune_space& s
     out.trials = 1;
     const auto consider = [&](const tune_candidate& c) {
         if (c.slots == out.best.slots && c.trace_blocks_per_sm == out.best.trace_blocks_per_sm &&
-            c.shade_block == out.best.shade_block && c.trace_min_blocks == out.best.trace_min_blocks &&
-            c.shade_sort == out.best.shade_sort)
+            c.shade_block == out.best.shade_block && c.trace_min_blocks == out.best.trace_min_blocks)
         {
             return;
         }
@@ -106,18 +103,11 @@ tune_outcome coordinate_descent(const tune_candidate& start, const tune_space& s
         c.slots = slots;
         consider(c);
     }
-    // 3. the shade kernel: whether it sorts its block's slots, then its block size
+    // 3. the shade kernel's block size
     const tune_candidate after_slots = out.best;
-    for (const int sort : space.shade_sorts)
-    {
-        tune_candidate c = after_slots;
-        c.shade_sort = sort;
-        consider(c);
-    }
-    const tune_candidate after_sort = out.best;
     for (const int block : space.shade_blocks)
     {
-        tune_candidate c = after_sort;
+        tune_candidate c = after_slots;
         c.shade_block = block;
         consider(c);
     }

@@ -8,7 +8,7 @@ synthetic speed model instead of GPU renders.
 """
 import raytracing_b200 as rt
 
-DEFAULT = {"slots": 1 << 20, "trace_blocks_per_sm": 8, "shade_block": 128, "trace_min_blocks": 8, "shade_sort": 0}
+DEFAULT = {"slots": 1 << 20, "trace_blocks_per_sm": 8, "shade_block": 128, "trace_min_blocks": 8}
 
 
 def _shape(s):
@@ -19,23 +19,22 @@ def test_finds_the_best_of_every_knob():
     trace_gain = {(8, 10): 1.00, (8, 8): 1.05, (8, 6): 0.97, (8, 4): 0.9, (6, 6): 1.12, (6, 4): 1.0}
     slot_gain = {1 << 19: 0.8, 1 << 20: 1.0, 3 << 19: 1.04, 1 << 21: 1.09, 3 << 20: 1.07}
     block_gain = {128: 1.0, 64: 1.03}
-    sort_gain = {0: 1.0, 1: 1.2}
     seen = []
 
     def measure(s):
         seen.append(dict(s))
         assert s["trace_blocks_per_sm"] <= (10 if s["trace_min_blocks"] == 8 else 6)
         return 1e9 * trace_gain[(s["trace_min_blocks"], s["trace_blocks_per_sm"])] * slot_gain[s["slots"]] * \
-            block_gain[s["shade_block"]] * sort_gain[s["shade_sort"]]
+            block_gain[s["shade_block"]]
 
     t = rt.autotune_simulate(measure, max_trace_blocks=10, max_trace_blocks_roomy=6)
     assert (t["trace_min_blocks"], t["trace_blocks_per_sm"]) == (6, 6)
-    assert t["slots"] == 1 << 21 and t["shade_block"] == 64 and t["shade_sort"] == 1
+    assert t["slots"] == 1 << 21 and t["shade_block"] == 64
     assert t["samples_per_second"] == measure(t)
     assert t["default_samples_per_second"] == 1e9 * 1.05
     assert _shape(seen[0]) == DEFAULT  # the built-in defaults are measured first
-    # 1 default + 5 other trace shapes + 4 other slot pools + the sort + 1 other block size
-    assert t["trials"] == 12 == len(seen) - 1
+    # 1 default + 5 other trace shapes + 4 other slot pools + 1 other block size
+    assert t["trials"] == 11 == len(seen) - 1
 
 
 def test_keeps_the_defaults_within_noise():
