@@ -143,10 +143,10 @@ def read_peaks() -> dict:
 
 
 # The wavefront's state per unit of work, by the layout of its slots and queues (raytracing_b200/csrc/kernels.cu): what
-# the shade kernel must move through HBM for each segment (the slot's seven 16-byte rows in and out, the walk's answer,
+# the shade kernel must move through HBM for each segment (the slot's five 16-byte rows in and out, the walk's answer,
 # the next query of 48 bytes), for each shadow ray (its answer, its three rows out and back in, its query) and for each
 # sample (its value). These are the bytes that bind the shade kernel: the scene itself (a few KB) is read from L1.
-SHADE_BYTES_PER_SEGMENT = 2 * 7 * 16 + 16 + 48
+SHADE_BYTES_PER_SEGMENT = 2 * 5 * 16 + 16 + 48
 SHADE_BYTES_PER_SHADOW_RAY = 4 + 2 * 3 * 16 + 48
 SHADE_BYTES_PER_SAMPLE = 16
 # FP32 operations per primitive test and per node visit (slab test: 6 FMA + 6 min/max), the trace kernels' arithmetic
@@ -655,6 +655,7 @@ def served_first_frames(rt, args) -> dict:
     ids, submitted = {}, {}
     start = time.perf_counter()
     steps = 0
+    log = []  # (wall s at the step's start, wall s it took, GPU s, first frames, refined, admitted, queued)
     while True:
         now = time.perf_counter() - start
         while pending and requests[pending[0]]["arrival"] <= now:
@@ -666,7 +667,10 @@ def served_first_frames(rt, args) -> dict:
             break
         if now > args.served_long_window + 60:
             break
+        t0 = time.perf_counter()
         rep = server.step()
+        log.append((round(t0 - start, 4), round(time.perf_counter() - t0, 4), round(rep["gpu_seconds"], 5),
+                    rep["first_frames"], rep["refined"], rep["admitted"], rep["queued"]))
         steps += 1
         if rep["active"] == 0 and rep["queued"] == 0 and pending:
             time.sleep(max(0.0, requests[pending[0]]["arrival"] - (time.perf_counter() - start)))
@@ -694,7 +698,9 @@ def served_first_frames(rt, args) -> dict:
             "ttff_p50_s": pct(ttff, 50), "ttff_p99_s": pct(ttff, 99), "ttff_max_s": max(ttff) if ttff else None,
             "ttff_by_resolution": {k: {"requests": len(v), "p50_s": pct(v, 50), "p99_s": pct(v, 99)}
                                    for k, v in sorted(by_size.items())},
-            "reached_target": len(ttt), "time_to_target_p50_s": pct(ttt, 50), "gpu_s": stats["gpu_seconds"]}
+            "reached_target": len(ttt), "time_to_target_p50_s": pct(ttt, 50), "gpu_s": stats["gpu_seconds"],
+            "longest_steps": sorted(log, key=lambda e: -e[1])[:8],
+            "step_log_fields": "wall start s, wall s, GPU s, first frames, refined, admitted, queued"}
 
 
 def run_reference(args):

@@ -319,11 +319,55 @@ __device__ __forceinline__ float edge_function(float px, float py, float qx, flo
     return static_cast<float>(static_cast<double>(px) * qy - static_cast<double>(py) * qx);
 }
 
+// The same test in double, for a ray whose float edge functions are too close to 0 to be sure of their signs: one
+// grazing the triangle (its projection a sliver) or passing within rounding of an edge
+__device__ __noinline__ bool hit_triangle_double(const triangle_v& tr, const ray_shear& r, float3 o, float3 d,
+                                                 float t_min, float t_max, float& t, bool& front)
+{
+    const double ox = o.x, oy = o.y, oz = o.z;
+    const double rel[3][3] = {{tr.a.x - ox, tr.a.y - oy, tr.a.z - oz},
+                              {tr.b.x - ox, tr.b.y - oy, tr.b.z - oz},
+                              {tr.c.x - ox, tr.c.y - oy, tr.c.z - oz}};
+    const double dir[3] = {d.x, d.y, d.z};
+    const double sz = 1.0 / dir[r.kz];
+    const double sx = dir[r.kx] * sz, sy = dir[r.ky] * sz;
+    double px[3], py[3], pz[3];
+    for (int k = 0; k < 3; ++k)
+    {
+        pz[k] = rel[k][r.kz];
+        px[k] = rel[k][r.kx] - sx * pz[k];
+        py[k] = rel[k][r.ky] - sy * pz[k];
+    }
+    const double u = px[2] * py[1] - py[2] * px[1];
+    const double v = px[0] * py[2] - py[0] * px[2];
+    const double w = px[1] * py[0] - py[1] * px[0];
+    if ((u < 0.0 || v < 0.0 || w < 0.0) && (u > 0.0 || v > 0.0 || w > 0.0))
+    {
+        return false;
+    }
+    const double det = u + v + w;
+    if (det == 0.0)
+    {
+        return false;
+    }
+    const double tt = (u * pz[0] + v * pz[1] + w * pz[2]) * sz / det;
+    t = static_cast<float>(tt);
+    if (!(t_min < t && t < t_max))
+    {
+        return false;
+    }
+    front = dot(d, cross(tr.b - tr.a, tr.c - tr.a)) < 0.0f;
+    return true;
+}
+
+__device__ __forceinline__ float max_abs(float3 v) { return fmaxf(fabsf(v.x), fmaxf(fabsf(v.y), fabsf(v.z))); }
+
 // Woop, Benthin and Wald, "Watertight Ray/Triangle Intersection" (JCGT 2013): the triangle's vertices sheared into
 // the ray's frame, the three edge functions of the origin's projection, all of one sign; so a ray through an edge or a
 // vertex shared by triangles hits at least one of them, with no crack between (Möller-Trumbore in float lets such a
-// ray through both, about 4 rays in a million on the 1.3M-triangle mesh). Barycentrics closed, t open. The front is
-// the side (b - a) x (c - a) points to.
+// ray through both, about 4 rays in a million on the 1.3M-triangle mesh). An edge function within its float rounding
+// of 0 (a grazing ray, or one within rounding of an edge) sends the test to double. Barycentrics closed, t open. The
+// front is the side (b - a) x (c - a) points to.
 __device__ __forceinline__ bool hit_triangle(const triangle_v& tr, const ray_shear& r, float3 o, float3 d,
                                              float t_min, float t_max, float& t, bool& front)
 {
@@ -335,6 +379,16 @@ __device__ __forceinline__ bool hit_triangle(const triangle_v& tr, const ray_she
     const float u = edge_function(cx, cy, bx, by);
     const float v = edge_function(ax, ay, cx, cy);
     const float w = edge_function(bx, by, ax, ay);
+    // The edge functions' rounding: the shear's (a few units of the vertices' largest coordinate's last place) times
+    // the projected coordinates' size, with a margin
+    const float coords = fmaxf(max_abs(pa), fmaxf(max_abs(pb), max_abs(pc)));
+    const float sheared = fmaxf(fmaxf(fmaxf(fabsf(ax), fabsf(ay)), fmaxf(fabsf(bx), fabsf(by))),
+                                fmaxf(fabsf(cx), fabsf(cy)));
+    const float rounding = 5e-7f * coords * sheared;
+    if (fabsf(u) <= rounding || fabsf(v) <= rounding || fabsf(w) <= rounding)
+    {
+        return hit_triangle_double(tr, r, o, d, t_min, t_max, t, front);
+    }
     if ((u < 0.0f || v < 0.0f || w < 0.0f) && (u > 0.0f || v > 0.0f || w > 0.0f))
     {
         return false;
