@@ -64,7 +64,9 @@ def parse():
     p.add_argument("--no-served", action="store_true", help="skip the served request stream's measurement")
     p.add_argument("--served-rate", type=float, default=200.0)
     p.add_argument("--served-window", type=float, default=0.25, help="seconds of arrivals (a bounded sample)")
-    p.add_argument("--served-step", type=float, default=0.01, help="GPU seconds a server step aims at")
+    p.add_argument("--served-step", type=float, default=0.01, help="GPU seconds a batched server step aims at")
+    p.add_argument("--served-continuous-step", type=float, default=0.002,
+                   help="GPU seconds a step of the continuous server runs before it returns to take arrivals")
     p.add_argument("--served-limit", type=float, default=300.0, help="wall seconds after which serving stops")
     p.add_argument("--served-long-window", type=float, default=5.0,
                    help="seconds of arrivals of the long stream (first frames of about 1,000 requests)")
@@ -556,19 +558,15 @@ def served_requests(rt, rate: float, window: float, seed: int = 7):
     return out
 
 
-def served_measurement(rt, torch, args) -> dict:
-    """The served stream through the request server (batched steps, first frames first) against the plain form
-    (one render per request, FIFO, one at a time), on the same requests; the plain form's latencies follow from its
-    measured per-request GPU times and the arrival times (a single FIFO server)."""
-    requests = served_requests(rt, args.served_rate, args.served_window)
-    descs = {name: rt.builtin_scene(name) for name in SERVED_SCENES}
-    scenes = {name: rt.Scene(d) for name, d in descs.items()}
-    server = rt.Server(hbm_budget_bytes=120 << 30, step_seconds=args.served_step)
+def serve_stream(rt, scenes, requests, continuous: bool, step_seconds: float, limit: float) -> dict:
+    """The requests submitted at their arrival times to a server (the continuous wavefront, or batched steps) and
+    served until every one is done or `limit` wall seconds have passed: time-to-first-frame and time-to-target
+    percentiles, and the server's segments per GPU second and per wall second."""
+    server = rt.Server(hbm_budget_bytes=120 << 30, step_seconds=step_seconds, continuous=continuous)
     pending = list(range(len(requests)))
     ids = {}
     start = time.perf_counter()
     submitted = {}
-    limit = args.served_limit
     step_log = []  # (wall s, GPU s, first frames, refined, admitted) of each step
     while True:
         now = time.perf_counter() - start
@@ -600,6 +598,39 @@ def served_measurement(rt, torch, args) -> dict:
             ttt.append(lag + st["done_seconds"])
     stats = server.stats()
     server.close()
+    return {"server": "continuous wavefront" if continuous else "batched steps",
+            "requests": len(requests), "completed": len(ttt), "first_frames": len(ttff), "wall_s": wall,
+            "ttff_p50_s": pct(ttff, 50), "ttff_p99_s": pct(ttff, 99),
+            "ttff_by_resolution": {k: {"requests": len(v), "p50_s": pct(v, 50), "p99_s": pct(v, 99)}
+                                   for k, v in sorted(by_size.items())},
+            "step_seconds": step_seconds,
+            "step_gpu_seconds_max": max((s[1] for s in step_log), default=None),
+            "steps_over_twice_the_budget": sum(1 for s in step_log if s[1] > 2 * step_seconds),
+            "first_steps": step_log[:12],
+            "time_to_target_p50_s": pct(ttt, 50), "time_to_target_p99_s": pct(ttt, 99),
+            "served_segments_per_s": stats["rays"] / stats["gpu_seconds"] if stats["gpu_seconds"] else None,
+            "served_segments_per_wall_s": stats["rays"] / wall if wall > 0 else None,
+            "served_gpu_s": stats["gpu_seconds"], "served_steps": stats["steps"],
+            "served_launches": stats["launches"], "groups_of_steps": stats["groups"],
+            "busy_slots": stats["busy_slots"]}
+
+
+def pct(v, p):
+    return float(np.percentile(v, p)) if v else None
+
+
+def served_measurement(rt, torch, args) -> dict:
+    """The served stream through the request server against the plain form (one render per request, FIFO, one at a
+    time), on the same requests: the continuous wavefront (the headline), the batched steps beside it, and the plain
+    form's latencies from its measured per-request GPU times and the arrival times (a single FIFO server)."""
+    requests = served_requests(rt, args.served_rate, args.served_window)
+    scenes = {name: rt.Scene(rt.builtin_scene(name)) for name in SERVED_SCENES}
+    out = serve_stream(rt, scenes, requests, True, args.served_continuous_step, args.served_limit)
+    batched = serve_stream(rt, scenes, requests, False, args.served_step, args.served_limit)
+    out["batched_server"] = {k: batched[k] for k in ("step_seconds", "ttff_p50_s", "ttff_p99_s", "wall_s",
+                                                     "time_to_target_p50_s", "time_to_target_p99_s",
+                                                     "served_segments_per_s", "served_segments_per_wall_s",
+                                                     "served_steps", "served_launches", "completed")}
 
     # The plain form: one session render per request on the resident scene, timed on the GPU, then FIFO queueing
     service = []
@@ -617,32 +648,19 @@ def served_measurement(rt, torch, args) -> dict:
     for q, s in zip(requests, service):
         finish = max(finish, q["arrival"]) + s
         plain_latency.append(finish - q["arrival"])
-
-    def pct(v, p):
-        return float(np.percentile(v, p)) if v else None
-
-    return {"workload": f"Poisson arrivals at {args.served_rate}/s over {args.served_window} s "
-                        f"({len(requests)} requests), scenes cover/glass/mesh-ggx, orbit cameras, 256^2..3840x2160 "
-                        f"4:3:2:1, target spp log-uniform 1-4096, HBM budget 120 GB",
-            "requests": len(requests), "completed": len(ttt), "first_frames": len(ttff), "wall_s": wall,
-            "ttff_p50_s": pct(ttff, 50), "ttff_p99_s": pct(ttff, 99),
-            "ttff_by_resolution": {k: {"requests": len(v), "p50_s": pct(v, 50), "p99_s": pct(v, 99)}
-                                   for k, v in sorted(by_size.items())},
-            "step_seconds": args.served_step,
-            "step_gpu_seconds_max": max((s[1] for s in step_log), default=None),
-            "steps_over_twice_the_budget": sum(1 for s in step_log if s[1] > 2 * args.served_step),
-            "first_steps": step_log[:12],
-            "time_to_target_p50_s": pct(ttt, 50), "time_to_target_p99_s": pct(ttt, 99),
-            "served_segments_per_s": stats["rays"] / stats["gpu_seconds"] if stats["gpu_seconds"] else None,
-            "served_steps": stats["steps"], "served_launches": stats["launches"],
-            "plain_ttff_p50_s": pct(plain_latency, 50), "plain_ttff_p99_s": pct(plain_latency, 99),
-            "plain_time_to_target_p50_s": pct(plain_latency, 50),
-            "plain_time_to_target_p99_s": pct(plain_latency, 99),
-            "plain_segments_per_s": plain_rays / sum(service) if service else None,
-            "plain_note": "one render per request (a session on the resident scene), FIFO, first frame = final image"}
+    out.update({
+        "workload": f"Poisson arrivals at {args.served_rate}/s over {args.served_window} s "
+                    f"({len(requests)} requests), scenes cover/glass/mesh-ggx, orbit cameras, 256^2..3840x2160 "
+                    f"4:3:2:1, target spp log-uniform 1-4096, HBM budget 120 GB",
+        "plain_ttff_p50_s": pct(plain_latency, 50), "plain_ttff_p99_s": pct(plain_latency, 99),
+        "plain_time_to_target_p50_s": pct(plain_latency, 50),
+        "plain_time_to_target_p99_s": pct(plain_latency, 99),
+        "plain_segments_per_s": plain_rays / sum(service) if service else None,
+        "plain_note": "one render per request (a session on the resident scene), FIFO, first frame = final image"})
+    return out
 
 
-def served_first_frames(rt, args) -> dict:
+def served_first_frames(rt, args, continuous: bool = True) -> dict:
     """The served stream over a long window (default 5 s of Poisson arrivals at 200/s, about 1,000 requests of the
     same distributions), served until every request has its first frame: time-to-first-frame percentiles over all of
     them (by resolution too), with the server refining the earlier requests meanwhile. Time to target is reported for
@@ -650,7 +668,9 @@ def served_first_frames(rt, args) -> dict:
     renders in real time)."""
     requests = served_requests(rt, args.served_rate, args.served_long_window, seed=11)
     scenes = {name: rt.Scene(rt.builtin_scene(name)) for name in SERVED_SCENES}
-    server = rt.Server(hbm_budget_bytes=120 << 30, step_seconds=args.served_step)
+    server = rt.Server(hbm_budget_bytes=120 << 30,
+                       step_seconds=args.served_continuous_step if continuous else args.served_step,
+                       continuous=continuous)
     pending = list(range(len(requests)))
     ids, submitted = {}, {}
     start = time.perf_counter()
@@ -691,7 +711,8 @@ def served_first_frames(rt, args) -> dict:
     def pct(v, p):
         return float(np.percentile(v, p)) if v else None
 
-    return {"workload": f"Poisson arrivals at {args.served_rate}/s over {args.served_long_window} s "
+    return {"server": "continuous wavefront" if continuous else "batched steps",
+            "workload": f"Poisson arrivals at {args.served_rate}/s over {args.served_long_window} s "
                         f"({len(requests)} requests), the served stream's distributions, served until every request "
                         f"has its first frame",
             "requests": len(requests), "first_frames": len(ttff), "wall_s": wall, "steps": steps,
@@ -699,6 +720,7 @@ def served_first_frames(rt, args) -> dict:
             "ttff_by_resolution": {k: {"requests": len(v), "p50_s": pct(v, 50), "p99_s": pct(v, 99)}
                                    for k, v in sorted(by_size.items())},
             "reached_target": len(ttt), "time_to_target_p50_s": pct(ttt, 50), "gpu_s": stats["gpu_seconds"],
+            "busy_slots": stats["busy_slots"],
             "longest_steps": sorted(log, key=lambda e: -e[1])[:8],
             "step_log_fields": "wall start s, wall s, GPU s, first frames, refined, admitted, queued"}
 
@@ -928,6 +950,11 @@ def run_b200(args):
         line["served"] = served_measurement(rt, torch, args)
         if args.served_long_window > 0:
             line["served"]["long_stream"] = served_first_frames(rt, args)
+            batched_long = served_first_frames(rt, args, continuous=False)
+            line["served"]["long_stream"]["batched_server"] = {
+                k: batched_long[k] for k in ("ttff_p50_s", "ttff_p99_s", "ttff_max_s", "ttff_by_resolution",
+                                             "reached_target", "time_to_target_p50_s", "gpu_s", "wall_s", "steps",
+                                             "longest_steps")}
 
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene_desc, args, os.cpu_count() or 1)

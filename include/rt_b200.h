@@ -502,7 +502,19 @@ typedef struct rt_server_options
     int64_t hbm_budget_bytes;   /* what the admitted requests' sums and the step's partials may hold */
     double step_seconds;        /* the GPU time a refinement step aims at */
     int32_t use_graph;
-    int32_t pad0;
+    /* 1: the continuous wavefront. One pool of path slots lives as long as the server; a request's first pass is
+     * published into it when the request is admitted and its refinement while the unclaimed backlog is short, so that
+     * no step drains the pool. A step then runs the pool for about step_seconds of GPU time and returns with work
+     * still running. Images equal a session's rendered to one pass, then to the target. 0: batched steps (each step
+     * a batch of passes, drained before it returns). */
+    int32_t continuous;
+    /* The continuous wavefront (ignored otherwise): its slot pool (a multiple of 128; 0: 1.5 x 2^20), its steps
+     * between two readings of the counts (1-16; 0: 2; a sample published now is claimable from the next group but
+     * one), and the unclaimed backlog it keeps published ahead of the slots, in seconds of GPU time at the measured
+     * rate, three groups' time if more (0: 0.002). */
+    int32_t slots;
+    int32_t group_steps;
+    double lookahead_seconds;
 } rt_server_options;
 
 enum { RT_REQUEST_QUEUED = 0, RT_REQUEST_ACTIVE = 1, RT_REQUEST_DONE = 2, RT_REQUEST_CANCELLED = 3 };
@@ -537,6 +549,10 @@ typedef struct rt_server_stats
     int64_t launches;
     int64_t completed;
     int64_t used_bytes;
+    /* The continuous wavefront: groups of steps run, and the mean over groups of the pool's slots that queued a ray
+     * in the group's last step (1: no slot idle). 0 for batched steps. */
+    int64_t groups;
+    double busy_slots;
 } rt_server_stats;
 
 rt_status rt_server_create(const rt_server_options* options, rt_server** server);

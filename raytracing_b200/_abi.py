@@ -187,7 +187,8 @@ class BatchReport(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("step_seconds", C.c_double), ("use_graph", C.c_int32),
-                ("pad0", C.c_int32)]
+                ("continuous", C.c_int32), ("slots", C.c_int32), ("group_steps", C.c_int32),
+                ("lookahead_seconds", C.c_double)]
 
 
 class RequestStatus(C.Structure):
@@ -202,7 +203,8 @@ class ServerStepReport(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [("rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("gpu_seconds", C.c_double),
-                ("steps", C.c_int64), ("launches", C.c_int64), ("completed", C.c_int64), ("used_bytes", C.c_int64)]
+                ("steps", C.c_int64), ("launches", C.c_int64), ("completed", C.c_int64), ("used_bytes", C.c_int64),
+                ("groups", C.c_int64), ("busy_slots", C.c_double)]
 
 
 # (name, restype, argtypes) of every entry point declared in include/rt_b200.h

@@ -476,12 +476,7 @@ uint64_t batch_engine::shadow_rays(int handle) const
 
 // ---- the render server --------------------------------------------------------------------------------------
 
-render_server::render_server(const rt_server_options& options)
-    : options_(options),
-      engine_(options.hbm_budget_bytes > 0 ? std::min<size_t>(default_partial_budget,
-                                                              static_cast<size_t>(options.hbm_budget_bytes) / 4)
-                                           : default_partial_budget,
-              options.use_graph != 0)
+render_server::render_server(const rt_server_options& options) : options_(options)
 {
     if (!(options_.step_seconds > 0 && options_.step_seconds <= 1))
     {
@@ -491,10 +486,132 @@ render_server::render_server(const rt_server_options& options)
     {
         fail(RT_ERR_INVALID, "hbm_budget_bytes must be positive");
     }
+    if (options_.continuous != 0 && options_.continuous != 1)
+    {
+        fail(RT_ERR_INVALID, "continuous must be 0 or 1");
+    }
+    if (options_.continuous)
+    {
+        // The pool of the flat-searched scenes (a compromise between the mesh, which gains up to 3 x 2^20 slots, and
+        // the sphere trees, which lose past 2^20) and a ring of 2^26 sample values (1 GB: a 4K first frame and the
+        // refinement backlog many times over)
+        if (options_.slots < 0 || options_.slots % render_block != 0 || options_.group_steps < 0 ||
+            options_.group_steps > 16 || !(options_.lookahead_seconds >= 0 && options_.lookahead_seconds <= 1))
+        {
+            fail(RT_ERR_INVALID, "slots must be a non-negative multiple of 128, group_steps in 0..16 and "
+                                 "lookahead_seconds in [0, 1]");
+        }
+        stream_ = std::make_unique<stream_engine>(options_.slots > 0 ? options_.slots : wave_slots_large,
+                                                  int64_t{1} << 26, options_.group_steps > 0 ? options_.group_steps : 2,
+                                                  options_.lookahead_seconds > 0 ? options_.lookahead_seconds : 0.002);
+        // The requests' memory (48 bytes a pixel) mapped now: a pool grown while requests wait stalls the step that
+        // admits them (tens of GB at once when large requests arrive together)
+        stream_->reserve_pool(std::min<size_t>(static_cast<size_t>(options_.hbm_budget_bytes), size_t{64} << 30));
+        return;
+    }
+    engine_ = std::make_unique<batch_engine>(std::min<size_t>(default_partial_budget,
+                                                              static_cast<size_t>(options.hbm_budget_bytes) / 4),
+                                             options.use_graph != 0);
     // What the first requests would otherwise wait for: the wavefront's buffers (its slots and the samples of a step
-    // of 64M samples, about 1.3 GB) and its kernels' modules, and the memory pool grown to hold requests' sums
-    engine_.reserve_wavefront(int64_t{1} << 26);
-    engine_.reserve_pool(std::min<size_t>(static_cast<size_t>(options_.hbm_budget_bytes), size_t{8} << 30));
+    // of 64M samples, about 1.3 GB) and its kernels' modules, and the memory pool grown to hold requests' sums (a
+    // pool grown while requests wait stalls the step that admits them: tens of GB when large requests arrive together)
+    engine_->reserve_wavefront(int64_t{1} << 26);
+    engine_->reserve_pool(std::min<size_t>(static_cast<size_t>(options_.hbm_budget_bytes), size_t{64} << 30));
+}
+
+int64_t render_server::passes_of(const request& r) const
+{
+    if (r.handle < 0)
+    {
+        return r.state == RT_REQUEST_DONE ? r.target : 0;
+    }
+    return stream_ ? stream_->passes(r.handle) : engine_->passes(r.handle);
+}
+
+// A request's device memory back to the budget
+void render_server::release(request& r)
+{
+    if (r.handle >= 0)
+    {
+        if (stream_)
+        {
+            stream_->remove(r.handle);
+        }
+        else
+        {
+            engine_->remove(r.handle);
+        }
+        r.handle = -1;
+        used_bytes_ -= r.bytes;
+    }
+    r.scene.reset();
+}
+
+// A step of the continuous wavefront: admission as in a batched step, then the pool runs for about step_seconds of
+// GPU time (first frames are published at once, refinement while the backlog is short); a request's state follows
+// the passes its sums hold
+rt_server_step_report render_server::step_continuous()
+{
+    rt_server_step_report report{};
+    while (!queue_.empty())
+    {
+        request& r = requests_.at(queue_.front());
+        if (used_bytes_ + r.bytes > static_cast<size_t>(options_.hbm_budget_bytes))
+        {
+            break;
+        }
+        // RNG job field 0, as in a batched step: the image equals a session's of the same view and seed
+        r.handle = stream_->add(r.scene, r.camera, r.seed, 0, r.target);
+        r.state = RT_REQUEST_ACTIVE;
+        used_bytes_ += r.bytes;
+        queue_.pop_front();
+        ++report.admitted;
+    }
+    std::map<int64_t, int64_t> before;
+    for (const auto& [id, r] : requests_)
+    {
+        if (r.state == RT_REQUEST_ACTIVE)
+        {
+            before[id] = stream_->passes(r.handle);
+        }
+    }
+    report.gpu_seconds = stream_->advance(options_.step_seconds);
+    stats_.gpu_seconds += report.gpu_seconds;
+    ++stats_.steps;
+    const auto now = clock::now();
+    for (auto& [id, r] : requests_)
+    {
+        if (r.state != RT_REQUEST_ACTIVE)
+        {
+            continue;
+        }
+        const int64_t done = stream_->passes(r.handle);
+        const int64_t was = before[id];
+        report.first_frames += was == 0 && done >= 1 ? 1 : 0;
+        report.refined += was >= 1 && done > was ? 1 : 0;
+        if (done >= 1 && r.first_frame_seconds < 0)
+        {
+            r.first_frame_seconds = std::chrono::duration<double>(now - r.submitted).count();
+        }
+        if (done >= r.target)
+        {
+            r.state = RT_REQUEST_DONE;
+            r.done_seconds = std::chrono::duration<double>(now - r.submitted).count();
+            stats_.rays += stream_->rays(r.handle);
+            stats_.shadow_rays += stream_->shadow_rays(r.handle);
+            ++stats_.completed;
+            ++report.completed;
+        }
+    }
+    for (const auto& [id, r] : requests_)
+    {
+        report.active += r.state == RT_REQUEST_ACTIVE ? 1 : 0;
+    }
+    report.queued = static_cast<int32_t>(queue_.size());
+    stats_.launches = stream_->launches();
+    stats_.groups = stream_->groups();
+    stats_.busy_slots = stream_->busy_slots();
+    return report;
 }
 
 int64_t render_server::submit(std::shared_ptr<resident_scene> scene, const rt_camera_desc& camera, uint64_t seed,
@@ -511,7 +628,7 @@ int64_t render_server::submit(std::shared_ptr<resident_scene> scene, const rt_ca
     r.seed = seed;
     r.target = target;
     r.submitted = clock::now();
-    r.bytes = engine_.job_bytes(camera);
+    r.bytes = stream_ ? stream_engine::job_bytes(camera) : engine_->job_bytes(camera);
     if (static_cast<int64_t>(r.bytes) > options_.hbm_budget_bytes)
     {
         fail(RT_ERR_CAPACITY, "the request's image alone exceeds the HBM budget");
@@ -523,6 +640,10 @@ int64_t render_server::submit(std::shared_ptr<resident_scene> scene, const rt_ca
 
 rt_server_step_report render_server::step()
 {
+    if (stream_)
+    {
+        return step_continuous();
+    }
     rt_server_step_report report{};
     // Admission, in arrival order, while the budget holds (a request waits rather than overtake an earlier one)
     while (!queue_.empty())
@@ -534,7 +655,7 @@ rt_server_step_report render_server::step()
         }
         // RNG job field 0: a request's image depends on its scene, camera, seed and passes only, so it equals a
         // session's render of the same view and seed
-        r.handle = engine_.add(r.scene, r.camera, r.seed, 0);
+        r.handle = engine_->add(r.scene, r.camera, r.seed, 0);
         r.state = RT_REQUEST_ACTIVE;
         used_bytes_ += r.bytes;
         queue_.pop_front();
@@ -547,7 +668,7 @@ rt_server_step_report render_server::step()
     double planned = 0;
     for (auto& [id, r] : requests_)
     {
-        if (r.state == RT_REQUEST_ACTIVE && engine_.passes(r.handle) == 0)
+        if (r.state == RT_REQUEST_ACTIVE && engine_->passes(r.handle) == 0)
         {
             const double pixels = double(r.camera.image_width) * r.camera.image_height;
             if (report.first_frames > 0 && planned + pixels * cost_of(r.scene.get()) > options_.step_seconds)
@@ -574,7 +695,7 @@ rt_server_step_report render_server::step()
         {
             continue;
         }
-        const int64_t done = engine_.passes(r.handle);
+        const int64_t done = engine_->passes(r.handle);
         if (done > 0 && done < r.target)
         {
             refine.emplace_back(double(r.camera.image_width) * r.camera.image_height * double(r.target - done), &r);
@@ -585,7 +706,7 @@ rt_server_step_report render_server::step()
     for (auto& [remaining, rp] : refine)
     {
         request& r = *rp;
-        const int64_t done = engine_.passes(r.handle);
+        const int64_t done = engine_->passes(r.handle);
         if (planned >= options_.step_seconds)
         {
             break;
@@ -608,7 +729,7 @@ rt_server_step_report render_server::step()
     }
     if (!work.empty())
     {
-        report.gpu_seconds = engine_.step(std::move(work));
+        report.gpu_seconds = engine_->step(std::move(work));
         if (report.gpu_seconds > 0)
         {
             learn_costs(step_samples, report.gpu_seconds);
@@ -623,7 +744,7 @@ rt_server_step_report render_server::step()
         {
             continue;
         }
-        const int64_t done = engine_.passes(r.handle);
+        const int64_t done = engine_->passes(r.handle);
         if (done >= 1 && r.first_frame_seconds < 0)
         {
             r.first_frame_seconds = std::chrono::duration<double>(now - r.submitted).count();
@@ -632,8 +753,8 @@ rt_server_step_report render_server::step()
         {
             r.state = RT_REQUEST_DONE;
             r.done_seconds = std::chrono::duration<double>(now - r.submitted).count();
-            stats_.rays += engine_.rays(r.handle);
-            stats_.shadow_rays += engine_.shadow_rays(r.handle);
+            stats_.rays += engine_->rays(r.handle);
+            stats_.shadow_rays += engine_->shadow_rays(r.handle);
             ++stats_.completed;
             ++report.completed;
         }
@@ -643,7 +764,7 @@ rt_server_step_report render_server::step()
         report.active += r.state == RT_REQUEST_ACTIVE ? 1 : 0;
     }
     report.queued = static_cast<int32_t>(queue_.size());
-    stats_.launches = engine_.launches();
+    stats_.launches = engine_->launches();
     return report;
 }
 
@@ -691,7 +812,7 @@ rt_request_status render_server::poll(int64_t id) const
     const request& r = it->second;
     rt_request_status s{};
     s.state = r.state;
-    s.passes = r.handle >= 0 ? engine_.passes(r.handle) : (r.state == RT_REQUEST_DONE ? r.target : 0);
+    s.passes = passes_of(r);
     s.target = r.target;
     s.first_frame_seconds = r.first_frame_seconds;
     s.done_seconds = r.done_seconds;
@@ -706,13 +827,17 @@ void render_server::fetch(int64_t id, double* pixels, int64_t count)
         fail(RT_ERR_LOGIC, "request " + std::to_string(id) + " has no image");
     }
     request& r = it->second;
-    engine_.pixels(r.handle, pixels, count);
+    if (stream_)
+    {
+        stream_->pixels(r.handle, pixels, count);
+    }
+    else
+    {
+        engine_->pixels(r.handle, pixels, count);
+    }
     if (r.state == RT_REQUEST_DONE)
     {
-        engine_.remove(r.handle);
-        r.handle = -1;
-        used_bytes_ -= r.bytes;
-        r.scene.reset();
+        release(r);
     }
 }
 
@@ -723,7 +848,14 @@ void render_server::display(int64_t id, const rt_display_options& options, uint8
     {
         fail(RT_ERR_LOGIC, "request " + std::to_string(id) + " has no image");
     }
-    engine_.display(it->second.handle, options, rgba, count);
+    if (stream_)
+    {
+        stream_->display(it->second.handle, options, rgba, count);
+    }
+    else
+    {
+        engine_->display(it->second.handle, options, rgba, count);
+    }
 }
 
 void render_server::cancel(int64_t id)
@@ -738,14 +870,8 @@ void render_server::cancel(int64_t id)
     {
         queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
     }
-    if (r.handle >= 0)
-    {
-        engine_.remove(r.handle);
-        r.handle = -1;
-        used_bytes_ -= r.bytes;
-    }
+    release(r);
     r.state = RT_REQUEST_CANCELLED;
-    r.scene.reset();
 }
 
 rt_server_stats render_server::stats() const

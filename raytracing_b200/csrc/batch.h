@@ -101,9 +101,146 @@ private:
     void release_graph();
 };
 
+// The server's continuous wavefront: one pool of path slots for the server's life, into which requests' samples
+// are published in segments as they are scheduled (first frames at once, refinement while the unclaimed backlog is
+// short), steps launched in groups two at a time, each finished segment reduced into its request's image (stream.cpp)
+class stream_engine
+{
+public:
+    stream_engine(int slots, int64_t value_capacity, int group_steps, double lookahead_seconds);
+    ~stream_engine();
+    stream_engine(const stream_engine&) = delete;
+    stream_engine& operator=(const stream_engine&) = delete;
+
+    // A request: its view of a resident scene, RNG seed and job field, and target passes; its first pass is published
+    // at the next advance. Its sums and accumulator (48 bytes a pixel) stay resident until remove.
+    int add(std::shared_ptr<resident_scene> scene, const rt_camera_desc& camera, uint64_t seed, uint32_t job_id,
+            int64_t target);
+    // Stops publishing the request's samples, waits for those in flight and frees its memory
+    void remove(int handle);
+    // Runs groups of steps until at least `seconds` of GPU time have been read back (one group at least when there is
+    // work); returns the GPU seconds read. A group may still be running on return.
+    double advance(double seconds);
+    bool has_work() const;
+    // The device's memory pool grown to `bytes` now (the requests' sums come from it)
+    void reserve_pool(size_t bytes);
+    int64_t passes(int handle) const; // complete passes in the request's sums
+    void pixels(int handle, double* out, int64_t count);
+    void display(int handle, const rt_display_options& options, uint8_t* out, int64_t count);
+    uint64_t rays(int handle) const;
+    uint64_t shadow_rays(int handle) const;
+    int64_t launches() const { return launches_; }
+    double gpu_seconds() const { return gpu_seconds_; }
+    int64_t groups() const { return groups_; }
+    // the mean over groups of the slots that queued a ray in the group's last step, as a fraction of the pool
+    double busy_slots() const { return groups_ > 0 ? busy_sum_ / static_cast<double>(groups_) : 0.0; }
+    static size_t job_bytes(const rt_camera_desc& camera);
+
+private:
+    struct request
+    {
+        std::shared_ptr<resident_scene> scene;
+        rt_camera_desc camera{};
+        camera_params cam{};
+        uint64_t seed = 0;
+        uint32_t id = 0;
+        int64_t target = 0;
+        int tiles_x = 0;
+        int64_t padded = 0;
+        device_array<double> sums;
+        device_array<double> acc; // the chunk accumulator: the passes since the sums' last addition
+        device_array<unsigned long long> counters;
+        int64_t published = 0; // its samples published, reduced (pass-major numbering)
+        int64_t reduced = 0;
+        int64_t passes = 0;
+        bool cancelled = false;
+        std::deque<int64_t> segments; // its segments in flight, oldest first
+    };
+    struct segment
+    {
+        int handle = -1; // the request; -1 once reduced
+        bool finished = false;
+        int64_t local_begin = 0;
+        int64_t local_end = 0;
+        int64_t global_begin = 0;
+        int64_t value_offset = 0;
+    };
+
+    // What a group reads from the host when it starts: the published limit and the window of segments
+    struct group_control
+    {
+        int64_t published;
+        int32_t window_first;
+        int32_t window_end;
+    };
+
+    int64_t value_room(int64_t count) const;
+    cudaGraphExec_t group_graph(int k);
+    int64_t publish(int handle, request& r, int64_t count);
+    void schedule();
+    void launch_group();
+    double finish_group();
+    bool reduce_finished(int group);
+    static size_t readback_bytes();
+
+    const int slot_count_;
+    const int64_t value_capacity_;
+    const int group_steps_;          // wavefront steps between two readings of the counts
+    const double lookahead_seconds_; // the unclaimed backlog refinement keeps, in GPU time
+    cudaStream_t stream_ = nullptr;
+    cudaStream_t reduce_stream_ = nullptr;
+    cudaEvent_t group_start_[2] = {};
+    cudaEvent_t group_done_[2] = {};
+    cudaEvent_t reduced_ = nullptr;
+    device_array<unsigned char> slots_;
+    device_array<float4> query_o_;
+    device_array<float4> query_d_;
+    device_array<int4> query_meta_;
+    device_array<int4> ext_result_;
+    device_array<int32_t> shadow_result_;
+    device_array<unsigned> control_;
+    device_array<unsigned long long> counters_;
+    device_array<batch_job> table_;
+    device_array<unsigned long long> done_;
+    device_array<float4> values_;
+    device_array<stream_reduce_item> reduce_items_;
+    device_array<uint8_t> rgba_;
+    unsigned char* readback_ = nullptr; // pinned, one per group in flight
+    group_control* staging_ = nullptr;  // pinned, one per group in flight
+    cudaGraphExec_t graphs_[8] = {};    // (features, wide, group slot)
+    std::vector<batch_job> table_host_;
+    std::vector<segment> segments_;
+    wave_buffers buffers_{};
+    int trace_grid_ = 0;
+    std::map<int, std::unique_ptr<request>> requests_;
+    std::vector<int> fresh_; // requests whose first pass is not yet published
+    int next_handle_ = 0;
+    int64_t next_segment_ = 0;   // logical segment numbers: [oldest_segment_, next_segment_) hold table entries
+    int64_t oldest_segment_ = 0;
+    int live_segments_ = 0;      // published and not yet reduced
+    int64_t published_ = 0;      // samples published
+    int64_t taken_ = 0;          // samples surely taken by a slot
+    int64_t value_head_ = 0;
+    int64_t group_limit_[2] = {};    // each group in flight: the published limit it runs with
+    int64_t group_segments_[2] = {}; // and the segments published before it
+    int group_index_ = 0;
+    int in_flight_ = 0;
+    double claim_rate_ = 0;      // samples taken per GPU second, smoothed
+    double group_seconds_ = 0;   // a group's GPU time, smoothed
+    bool features_ = false;      // the kernels' variant: any scene with the second book's features
+    bool wide_ = true;           // every scene's tree four wide
+    unsigned long long last_progress_ = 0; // the claims and finished samples last read
+    int stalled_groups_ = 0;               // groups read since they last changed
+    int64_t launches_ = 0;
+    double gpu_seconds_ = 0;
+    int64_t groups_ = 0;
+    double busy_sum_ = 0;
+};
+
 // The server of a stream of render requests: requests are admitted under an HBM budget, every
 // step gives the newly admitted their first frame (one pass) before it refines the others, and a request is done when
-// it reaches its target passes. Driven by the caller: submit between steps, step, poll, fetch.
+// it reaches its target passes. Driven by the caller: submit between steps, step, poll, fetch. Its steps are batches
+// of passes (batch_engine) or runs of the continuous wavefront (stream_engine).
 class render_server
 {
 public:
@@ -134,7 +271,8 @@ private:
         size_t bytes = 0;
     };
     rt_server_options options_;
-    batch_engine engine_;
+    std::unique_ptr<batch_engine> engine_;  // batched steps
+    std::unique_ptr<stream_engine> stream_; // or the continuous wavefront
     std::map<int64_t, request> requests_;
     std::deque<int64_t> queue_;
     int64_t next_id_ = 1;
@@ -143,6 +281,9 @@ private:
     double default_cost_ = 0;                      // the same over every scene, for a scene not seen yet
     rt_server_stats stats_{};
 
+    int64_t passes_of(const request& r) const;
+    rt_server_step_report step_continuous();
+    void release(request& r);
     double cost_of(const resident_scene* scene) const;
     void learn_costs(const std::vector<std::pair<const resident_scene*, double>>& samples, double seconds);
 };

@@ -2089,16 +2089,17 @@ constexpr int job_pixels = 1;  // by pixel_begin
 constexpr int job_samples = 2; // by sample_begin (a wavefront group's sample space)
 
 template <int SPACE>
-__device__ __forceinline__ int find_job(const batch_job* jobs, int first, int end, int64_t index)
+__device__ __forceinline__ int find_job(const batch_job* jobs, int first, int end, int64_t index, int mask = 0)
 {
     int lo = first;
     int hi = end - 1;
     while (lo < hi)
     {
         const int mid = (lo + hi + 1) >> 1;
-        const int64_t begin = SPACE == job_pixels    ? jobs[mid].pixel_begin
-                              : SPACE == job_samples ? jobs[mid].sample_begin
-                                                     : jobs[mid].item_begin;
+        const batch_job& j = jobs[mask != 0 ? (mid & mask) : mid]; // a stream run's ring: [first, end) unwrapped
+        const int64_t begin = SPACE == job_pixels    ? j.pixel_begin
+                              : SPACE == job_samples ? j.sample_begin
+                                                     : j.item_begin;
         if (begin <= index)
         {
             lo = mid;
@@ -2344,6 +2345,8 @@ constexpr int wave_flags_row = 4; // depth, flags, sample, job: a slot whose row
 constexpr int wave_query_primary = 4;
 constexpr uint32_t wave_specular = 1u << 8;
 constexpr uint32_t wave_inward = 1u << 9;
+constexpr uint32_t wave_reserved = 1u << 10; // a stream run's slot holds a claim beyond what is published (its number
+                                             // in the flags row's last two words) and waits for it
 
 constexpr unsigned full_warp = 0xffffffffu;
 
@@ -2460,12 +2463,18 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     const int i = own; // the slot this thread shades
     uint32_t flags = static_cast<uint32_t>(r5.y);
     uint32_t shadow_rays = 0; // counted where the walks are (the trace kernel), or as queued (BATCH)
+    // Samples may be claimed below `limit`: the launch's count, or what a stream run's host has published
+    const bool stream_run = BATCH && W.published != nullptr;
+    const unsigned long long limit =
+        stream_run ? __ldcg(W.published) : static_cast<unsigned long long>(B.sample_count);
+    const int2 window =
+        stream_run ? __ldcg(reinterpret_cast<const int2*>(W.window)) : make_int2(W.job_first, W.job_end);
     // a warp whose slots have all run out of work has nothing left to do in this launch
     if (!__all_sync(full_warp, (flags & wave_exhausted) != 0u))
     {
         const bool live = (flags & wave_exhausted) == 0u;
         // the slot's job: its scene, camera and numbers (a session's launch: the launch's own)
-        int job = BATCH ? r5.w : 0;
+        int job = BATCH && (flags & wave_reserved) == 0u ? r5.w : 0;
         const batch_job* J = BATCH ? W.jobs + job : nullptr;
         const auto scene = [&]() -> const scene_view& {
             if constexpr (BATCH)
@@ -2504,6 +2513,9 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         int px = 0, py = 0; // the pixel of a sample claimed in this step (a slot's camera ray needs no more)
         bool need = false;
         bool start = false;
+        bool ready = false;             // a stream run's reservation the host has since published
+        unsigned long long reserved = 0;
+        int finished_job = -1;          // a stream run's segment whose sample this slot finished
         bool primary = false; // a new sample whose camera ray the trace kernel makes (wave_camera_query)
         int round_pass = 0;   // its pass within its round of strata
         rng.job = BATCH ? J->job : P.job;
@@ -2524,7 +2536,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             if (flags & (wave_ext | wave_shadow | wave_finish))
             {
                 // the sample's stream, from its number
-                const int64_t local = sample_index - (BATCH ? J->sample_begin : 0);
+                const int64_t local = sample_index + (BATCH ? J->local_begin : 0);
                 const sample_place at = place_of(local, BATCH ? J->padded_pixels : P.padded_pixels,
                                                  BATCH ? J->tiles_x : P.tiles_x, BATCH ? J->pass_begin : P.pass_begin);
                 sample_rng(at, camera().width, BATCH ? J->round_passes : P.round_passes, BATCH ? J->seed : P.seed,
@@ -2596,6 +2608,23 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                     }
                 }
             }
+            else if (BATCH && (flags & wave_reserved))
+            {
+                // a stream run's claim made before the host published it: taken below once it has
+                const unsigned long long held =
+                    static_cast<unsigned long long>(static_cast<uint32_t>(r5.z)) |
+                    (static_cast<unsigned long long>(static_cast<uint32_t>(r5.w)) << 32);
+                if (held < limit)
+                {
+                    reserved = held;
+                    ready = true;
+                }
+                else
+                {
+                    sample_index = static_cast<uint32_t>(held);
+                    job = static_cast<int>(held >> 32);
+                }
+            }
             else
             {
                 need = true; // a slot without a sample
@@ -2603,12 +2632,74 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             if (finished)
             {
                 // the sample's value, added into its chunk's partial in pass order by the reduction
-                stream_store(B.samples + sample_index, make_float4(sample.x, sample.y, sample.z, 0.0f));
+                const float4 value = make_float4(sample.x, sample.y, sample.z, 0.0f);
+                if (stream_run)
+                {
+                    stream_store(J->values + sample_index, value);
+                    finished_job = job; // counted below, one atomic per segment per warp
+                }
+                else
+                {
+                    stream_store(B.samples + (BATCH ? J->sample_begin : 0) + sample_index, value);
+                }
                 need = true;
             }
         }
+        if (stream_run)
+        {
+            // the warp's finished samples counted per segment: the host reduces a segment once all are in
+            const unsigned peers = __match_any_sync(full_warp, finished_job);
+            if (finished_job >= 0 && (peers & lanes_below) == 0u)
+            {
+                atomicAdd(W.jobs[finished_job].done, static_cast<unsigned long long>(__popc(peers)));
+            }
+        }
+        // Sample s taken by this slot: its job, its pixel and pass (false for a lane of a tile over the image's edge,
+        // which claims again; in a stream run it counts as done, having no value to wait for)
+        const auto take = [&](unsigned long long s) -> bool {
+            int k = 0;
+            if constexpr (BATCH)
+            {
+                k = find_job<job_samples>(W.jobs, window.x, window.y, static_cast<int64_t>(s), W.job_mask);
+                k = W.job_mask != 0 ? (k & W.job_mask) : k;
+            }
+            const batch_job* K = BATCH ? W.jobs + k : nullptr;
+            const camera_params& c = BATCH ? K->cam : P.cam;
+            const int64_t index = static_cast<int64_t>(s) - (BATCH ? K->sample_begin : 0);
+            if (stream_run && index < 0)
+            {
+                // below the window the host gave: a sample no entry holds; reported, never written
+                atomicOr(B.control + 3, 1u);
+                return false;
+            }
+            const sample_place at = place_of(index + (BATCH ? K->local_begin : 0),
+                                             BATCH ? K->padded_pixels : P.padded_pixels, BATCH ? K->tiles_x : P.tiles_x,
+                                             BATCH ? K->pass_begin : P.pass_begin);
+            if (!(at.x < c.width && at.y < c.height))
+            {
+                if (stream_run)
+                {
+                    atomicAdd(K->done, 1ull);
+                }
+                return false;
+            }
+            px = at.x;
+            py = at.y;
+            job = k;
+            J = K;
+            sample_index = index;
+            pass = at.pass;
+            rng.job = BATCH ? K->job : P.job;
+            start = true;
+            return true;
+        };
+        if (ready)
+        {
+            flags &= ~wave_reserved;
+            need = !take(reserved);
+        }
         // Samples for the slots that need one, a pass of the image after another (of each job after another): one
-        // atomic per warp
+        // atomic per warp. In a stream run a claim beyond what is published waits in the slot (wave_reserved).
         while (true)
         {
             const unsigned needing = __ballot_sync(full_warp, need);
@@ -2627,34 +2718,23 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             if (need)
             {
                 const unsigned long long s = base + static_cast<unsigned long long>(__popc(needing & lanes_below));
-                if (s >= static_cast<unsigned long long>(B.sample_count))
+                if (s >= limit)
                 {
-                    flags |= wave_exhausted;
+                    if (stream_run)
+                    {
+                        flags |= wave_reserved;
+                        sample_index = static_cast<uint32_t>(s);
+                        job = static_cast<int>(s >> 32);
+                    }
+                    else
+                    {
+                        flags |= wave_exhausted;
+                    }
                     need = false;
                 }
                 else
                 {
-                    const int k = BATCH ? find_job<job_samples>(W.jobs, W.job_first, W.job_end,
-                                                                 static_cast<int64_t>(s))
-                                        : 0;
-                    const batch_job* K = BATCH ? W.jobs + k : nullptr;
-                    const camera_params& c = BATCH ? K->cam : P.cam;
-                    const int64_t local = static_cast<int64_t>(s) - (BATCH ? K->sample_begin : 0);
-                    const sample_place at = place_of(local, BATCH ? K->padded_pixels : P.padded_pixels,
-                                                     BATCH ? K->tiles_x : P.tiles_x,
-                                                     BATCH ? K->pass_begin : P.pass_begin);
-                    if (at.x < c.width && at.y < c.height) // a lane of a tile over the image's edge claims again
-                    {
-                        px = at.x;
-                        py = at.y;
-                        job = k;
-                        J = K;
-                        sample_index = static_cast<int64_t>(s);
-                        pass = at.pass;
-                        rng.job = BATCH ? K->job : P.job;
-                        need = false;
-                        start = true;
-                    }
+                    need = !take(s);
                 }
             }
         }
@@ -3240,6 +3320,63 @@ __global__ void wave_reduce_kernel(const reduce_params R, const float4* samples,
     sum[2] = b;
 }
 
+// A stream run's finished segments into their requests' images (stream_reduce_item): one thread per pixel of an
+// item; the segment's samples of that pixel, pass after pass, into the request's chunk accumulator, which goes into
+// the sums after a chunk's last pass, after the first pass (the first frame) and at the target. A pixel's passes
+// arrive in order (the host reduces a request's segments one after another), so a pixel's sums are the session's
+// chunk partials added in chunk order, up to the first frame's split of the first chunk.
+__global__ void stream_reduce_kernel(const stream_reduce_item* items, int32_t count, int64_t total_pixels)
+{
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total_pixels;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    {
+        int lo = 0, hi = count - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (items[mid].pixel_begin <= i)
+            {
+                lo = mid;
+            }
+            else
+            {
+                hi = mid - 1;
+            }
+        }
+        const stream_reduce_item& it = items[lo];
+        const int64_t pixel = i - it.pixel_begin;
+        const int y = static_cast<int>(pixel / it.width);
+        const int x = static_cast<int>(pixel - static_cast<int64_t>(y) * it.width);
+        const int q = ((y >> 2) * it.tiles_x + (x >> 3)) * 32 + ((y & 3) << 3) + (x & 7);
+        // the passes whose sample of this pixel lies in [local_begin, local_end)
+        const int64_t padded = it.padded_pixels;
+        int64_t pass = (it.local_begin - q + padded - 1) / padded;
+        pass = pass < 0 ? 0 : pass;
+        double* acc = it.acc + 3 * pixel;
+        double* sum = it.sums + 3 * pixel;
+        double ar = acc[0], ag = acc[1], ab = acc[2];
+        for (int64_t local = pass * padded + q; local < it.local_end; local += padded, ++pass)
+        {
+            const float4 v = it.values[local - it.local_begin];
+            ar += without_nan(v.x);
+            ag += without_nan(v.y);
+            ab += without_nan(v.z);
+            const int64_t done = pass + 1;
+            if (done % it.chunk == 0 || done == 1 || done == it.target)
+            {
+                sum[0] += ar;
+                sum[1] += ag;
+                sum[2] += ab;
+                ar = ag = ab = 0.0;
+            }
+        }
+        acc[0] = ar;
+        acc[1] = ag;
+        acc[2] = ab;
+    }
+}
+
+
 // A wavefront group's samples into its jobs' chunk partials, laid out as the persistent batch kernel writes them: each
 // work item (chunk, pixel) the sum of its passes' samples in pass order; items of pixels over the image's edge skipped
 __global__ void wave_batch_partials_kernel(const wave_batch W, const float4* samples)
@@ -3577,6 +3714,19 @@ cudaError_t preload_wave_batch()
         }
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_stream_reduce(const stream_reduce_item* items, int32_t count, int64_t total_pixels,
+                                 cudaStream_t stream)
+{
+    if (count <= 0 || total_pixels <= 0)
+    {
+        return cudaSuccess;
+    }
+    const int64_t wanted = (total_pixels + 255) / 256;
+    const int64_t blocks = wanted < 148 * 16 ? wanted : 148 * 16;
+    stream_reduce_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(items, count, total_pixels);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream)

@@ -70,10 +70,14 @@ struct alignas(16) batch_job
     int32_t quality;
     uint32_t job;                 // the RNG counter's job field
     int32_t pad0;
+    // A stream run's segment (the server's continuous wavefront): its samples are [sample_begin, sample_begin +
+    // pass-major count) of the run's sample space, numbered within the request from local_begin; their values go to
+    // values[local - local_begin] and each finished one is counted in *done
+    float4* values;
+    unsigned long long* done;
+    int64_t local_begin;
 };
 
-// What changes from step to step besides the jobs: read from device memory, so that a captured graph of the step
-// replays with new contents
 // Whether a scene has any of the second book's features (moving spheres, textures other than solid colors, smoke):
 // its kernels are compiled with their code, the others without
 inline bool has_features(const scene_view& s) { return s.has_motion != 0 || s.has_textures != 0 || s.medium_count > 0; }
@@ -125,7 +129,37 @@ struct wave_batch
     int64_t item_first; // the group's work items [item_first, item_end) in the batch's item space
     int64_t item_end;
     unsigned long long* work_counter; // the group's samples taken so far (zero at the start)
+    // A stream run (the server's continuous wavefront; null in a batch's run): samples are claimed up to *published,
+    // a claim beyond it waits in its slot until the host publishes that far; the jobs are segments in a ring of
+    // job_mask + 1 entries, the window window[0] .. window[1] counted without wrapping (in device memory with the
+    // limit, so that one captured graph of steps serves every group)
+    const unsigned long long* published;
+    int32_t job_mask;
+    int32_t pad0;
+    const int32_t* window;
 };
+
+// The stream run's reduction: each item a segment's samples added, pixel by pixel in pass order, into its request's
+// chunk accumulator, which goes into the request's sums at every chunk's end, after the first pass (the first frame)
+// and at the target, as a session adds its chunk partials
+struct stream_reduce_item
+{
+    const float4* values;
+    double* sums;
+    double* acc;
+    int64_t local_begin; // the segment's samples [local_begin, local_end) of the request's pass-major numbering
+    int64_t local_end;
+    int64_t pixel_begin; // the item's pixels in the launch's pixel space
+    int64_t target;
+    int32_t padded_pixels;
+    int32_t tiles_x;
+    int32_t width;
+    int32_t height;
+    int32_t chunk;       // passes a chunk (16)
+    int32_t pad0;
+};
+cudaError_t launch_stream_reduce(const stream_reduce_item* items, int32_t count, int64_t total_pixels,
+                                 cudaStream_t stream);
 
 // The kernels' static properties for kernel_info
 struct kernel_attributes
@@ -168,7 +202,8 @@ struct wave_buffers
     int4* ext_result;       // per slot: the next ray's hit (id, t's bits, front)
     int32_t* shadow_result; // per slot: 1 if the shadow ray was blocked
     // [0] next rays and shadow rays the last shade step queued (from the bottom), [1] queries the trace kernel took,
-    // [2] camera rays it queued (from the top down; tree-searched scenes only); [3] unused
+    // [2] camera rays it queued (from the top down; tree-searched scenes only); [3] a stream run's error flag (a claim
+    // outside the window of segments it was given), never cleared by a step
     unsigned* control;
     camera_params cam;      // a session's launch: its camera and RNG job field (a batch: each job's, in its table)
     uint32_t job;
