@@ -502,11 +502,12 @@ typedef struct rt_server_options
     int64_t hbm_budget_bytes;   /* what the admitted requests' sums and the step's partials may hold */
     double step_seconds;        /* the GPU time a refinement step aims at */
     int32_t use_graph;
-    /* 1: the continuous wavefront. One pool of path slots lives as long as the server; a request's first pass is
-     * published into it when the request is admitted and its refinement while the unclaimed backlog is short, so that
-     * no step drains the pool. A step then runs the pool for about step_seconds of GPU time and returns with work
-     * still running. Images equal a session's rendered to one pass, then to the target. 0: batched steps (each step
-     * a batch of passes, drained before it returns). */
+    /* 1: the continuous wavefront. One pool of path slots lives as long as the server, and a request's refinement
+     * is published into it while the unclaimed backlog is short, so that no step drains the pool; its first pass is
+     * rendered in a batched step of first frames (whose last paths advance through steps of a few slots, not of the
+     * whole pool) and handed over. A step runs the pool for about step_seconds of GPU time and returns with work still
+     * running. Images equal a session's rendered to one pass, then to the target. 2: the same with the first passes
+     * published into the pool too. 0: batched steps (each step a batch of passes, drained before it returns). */
     int32_t continuous;
     /* The continuous wavefront (ignored otherwise): its slot pool (a multiple of 128; 0: 1.5 x 2^20), its steps
      * between two readings of the counts (1-16; 0: 2; a sample published now is claimable from the next group but

@@ -485,13 +485,14 @@ REQUEST_STATES = {0: "queued", 1: "active", 2: "done", 3: "cancelled"}
 
 class Server:
     """A stream of render requests served in batched steps: admission under an HBM budget, a first frame (one pass)
-    for every newly admitted request before refinement, each request done at its target passes. `continuous`: the
-    requests' samples go into one pool of path slots kept running across steps (rt_server_options.continuous)."""
+    for every newly admitted request before refinement, each request done at its target passes. `continuous` 1: the
+    refinement runs in one pool of path slots kept running across steps, first frames in batched steps of their own;
+    2: first frames in the pool too (rt_server_options.continuous)."""
 
     def __init__(self, hbm_budget_bytes: int = 8 << 30, step_seconds: float = 0.02, use_graph: bool = True,
-                 continuous: bool = False, slots: int = 0, group_steps: int = 0, lookahead_seconds: float = 0.0):
+                 continuous: int = 0, slots: int = 0, group_steps: int = 0, lookahead_seconds: float = 0.0):
         o = _abi.ServerOptions(hbm_budget_bytes=hbm_budget_bytes, step_seconds=step_seconds,
-                               use_graph=1 if use_graph else 0, continuous=1 if continuous else 0, slots=slots,
+                               use_graph=1 if use_graph else 0, continuous=int(continuous), slots=slots,
                                group_steps=group_steps, lookahead_seconds=lookahead_seconds)
         handle = C.c_void_p()
         _check(_lib().rt_server_create(C.byref(o), C.byref(handle)))

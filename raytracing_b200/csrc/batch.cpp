@@ -24,12 +24,15 @@ constexpr int64_t short_step_samples = int64_t{12} << 20;
 
 // ---- the batch engine ---------------------------------------------------------------------------------------
 
-batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph)
+batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph, bool high_priority)
     : use_graph_(use_graph),
       max_partial_entries_(static_cast<int64_t>((partial_budget_bytes > 0 ? partial_budget_bytes : default_partial_budget) /
                                                 (3 * sizeof(double))))
 {
-    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a CUDA stream");
+    int least = 0, greatest = 0;
+    check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "querying stream priorities");
+    check(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, high_priority ? greatest : least),
+          "creating a CUDA stream");
     check(cudaEventCreate(&start_), "creating a CUDA event");
     check(cudaEventCreate(&stop_), "creating a CUDA event");
     kernel_attributes a{};
@@ -414,6 +417,14 @@ void batch_engine::reserve_wavefront(int64_t samples)
 
 int64_t batch_engine::passes(int handle) const { return jobs_.at(handle)->passes; }
 
+void batch_engine::copy_sums(int handle, double* device_out)
+{
+    const job& j = *jobs_.at(handle);
+    check(cudaMemcpyAsync(device_out, j.sums.data(), j.sums.bytes(), cudaMemcpyDeviceToDevice, stream_),
+          "copying a job's sums");
+    check(cudaStreamSynchronize(stream_), "copying a job's sums");
+}
+
 void batch_engine::pixels(int handle, double* out, int64_t count)
 {
     job& j = *jobs_.at(handle);
@@ -486,9 +497,9 @@ render_server::render_server(const rt_server_options& options) : options_(option
     {
         fail(RT_ERR_INVALID, "hbm_budget_bytes must be positive");
     }
-    if (options_.continuous != 0 && options_.continuous != 1)
+    if (options_.continuous < 0 || options_.continuous > 2)
     {
-        fail(RT_ERR_INVALID, "continuous must be 0 or 1");
+        fail(RT_ERR_INVALID, "continuous must be 0, 1 or 2");
     }
     if (options_.continuous)
     {
@@ -504,6 +515,10 @@ render_server::render_server(const rt_server_options& options) : options_(option
         stream_ = std::make_unique<stream_engine>(options_.slots > 0 ? options_.slots : wave_slots_large,
                                                   int64_t{1} << 26, options_.group_steps > 0 ? options_.group_steps : 2,
                                                   options_.lookahead_seconds > 0 ? options_.lookahead_seconds : 0.002);
+        // First frames are rendered in batched steps of their own (a first frame's last paths then advance through
+        // steps of a few slots, not of the whole pool), on a stream whose kernels go first, and handed over
+        engine_ = std::make_unique<batch_engine>(size_t{256} << 20, options.use_graph != 0, true);
+        engine_->reserve_wavefront(int64_t{1} << 24);
         // The requests' memory (48 bytes a pixel) mapped now: a pool grown while requests wait stalls the step that
         // admits them (tens of GB at once when large requests arrive together)
         stream_->reserve_pool(std::min<size_t>(static_cast<size_t>(options_.hbm_budget_bytes), size_t{64} << 30));
@@ -531,6 +546,11 @@ int64_t render_server::passes_of(const request& r) const
 // A request's device memory back to the budget
 void render_server::release(request& r)
 {
+    if (r.first_handle >= 0)
+    {
+        engine_->remove(r.first_handle);
+        r.first_handle = -1;
+    }
     if (r.handle >= 0)
     {
         if (stream_)
@@ -547,9 +567,10 @@ void render_server::release(request& r)
     r.scene.reset();
 }
 
-// A step of the continuous wavefront: admission as in a batched step, then the pool runs for about step_seconds of
-// GPU time (first frames are published at once, refinement while the backlog is short); a request's state follows
-// the passes its sums hold
+// A step of the continuous wavefront: admission as in a batched step; the first frames of the admitted requests in
+// a batched step of their own (arrival order, about max(first_frame_seconds, step_seconds) of them, at least one),
+// handed over to the pool; then, if no first frame is left waiting, the pool runs for about step_seconds of GPU time
+// and returns with work still running. A request's state follows the passes its sums hold.
 rt_server_step_report render_server::step_continuous()
 {
     rt_server_step_report report{};
@@ -561,7 +582,13 @@ rt_server_step_report render_server::step_continuous()
             break;
         }
         // RNG job field 0, as in a batched step: the image equals a session's of the same view and seed
-        r.handle = stream_->add(r.scene, r.camera, r.seed, 0, r.target);
+        const bool batched_first = options_.continuous == 1;
+        r.handle = stream_->add(r.scene, r.camera, r.seed, 0, r.target, batched_first);
+        if (batched_first)
+        {
+            r.first_handle = engine_->add(r.scene, r.camera, r.seed, 0);
+            first_queue_.push_back(r.id);
+        }
         r.state = RT_REQUEST_ACTIVE;
         used_bytes_ += r.bytes;
         queue_.pop_front();
@@ -575,7 +602,58 @@ rt_server_step_report render_server::step_continuous()
             before[id] = stream_->passes(r.handle);
         }
     }
-    report.gpu_seconds = stream_->advance(options_.step_seconds);
+    // First frames: no group is launched meanwhile, and the groups in flight give way to the batch engine's stream
+    std::vector<batch_engine::assignment> work;
+    std::vector<std::pair<const resident_scene*, double>> step_samples;
+    std::vector<int64_t> firsts;
+    double planned = 0;
+    while (!first_queue_.empty())
+    {
+        const int64_t id = first_queue_.front();
+        const auto it = requests_.find(id);
+        if (it == requests_.end() || it->second.first_handle < 0)
+        {
+            first_queue_.pop_front();
+            continue;
+        }
+        request& r = it->second;
+        const double pixels = double(r.camera.image_width) * r.camera.image_height;
+        if (!work.empty() && planned + pixels * cost_of(r.scene.get()) > std::max(first_frame_seconds,
+                                                                                     options_.step_seconds))
+        {
+            break;
+        }
+        work.push_back({r.first_handle, 1});
+        step_samples.emplace_back(r.scene.get(), pixels);
+        planned += pixels * cost_of(r.scene.get());
+        firsts.push_back(id);
+        first_queue_.pop_front();
+    }
+    if (!work.empty())
+    {
+        const double seconds = engine_->step(std::move(work));
+        if (seconds > 0)
+        {
+            learn_costs(step_samples, seconds);
+        }
+        report.gpu_seconds += seconds;
+        for (const int64_t id : firsts)
+        {
+            request& r = requests_.at(id);
+            engine_->copy_sums(r.first_handle, stream_->sums(r.handle));
+            first_rays_ += engine_->rays(r.first_handle);
+            first_shadow_rays_ += engine_->shadow_rays(r.first_handle);
+            engine_->remove(r.first_handle);
+            r.first_handle = -1;
+            stream_->first_pass_done(r.handle);
+        }
+    }
+    // Refinement, unless first frames are still waiting: they take the next step too (as in batched steps, a first
+    // frame waits for no refinement; the pool's paths wait in their slots meanwhile, without draining)
+    if (first_queue_.empty())
+    {
+        report.gpu_seconds += stream_->advance(options_.step_seconds);
+    }
     stats_.gpu_seconds += report.gpu_seconds;
     ++stats_.steps;
     const auto now = clock::now();
@@ -608,7 +686,7 @@ rt_server_step_report render_server::step_continuous()
         report.active += r.state == RT_REQUEST_ACTIVE ? 1 : 0;
     }
     report.queued = static_cast<int32_t>(queue_.size());
-    stats_.launches = stream_->launches();
+    stats_.launches = stream_->launches() + engine_->launches();
     stats_.groups = stream_->groups();
     stats_.busy_slots = stream_->busy_slots();
     return report;
@@ -870,6 +948,7 @@ void render_server::cancel(int64_t id)
     {
         queue_.erase(std::remove(queue_.begin(), queue_.end(), id), queue_.end());
     }
+    first_queue_.erase(std::remove(first_queue_.begin(), first_queue_.end(), id), first_queue_.end());
     release(r);
     r.state = RT_REQUEST_CANCELLED;
 }
@@ -878,6 +957,9 @@ rt_server_stats render_server::stats() const
 {
     rt_server_stats s = stats_;
     s.used_bytes = static_cast<int64_t>(used_bytes_);
+    // the continuous server's first frames, counted when handed over
+    s.rays += first_rays_;
+    s.shadow_rays += first_shadow_rays_;
     return s;
 }
 } // namespace rtb

@@ -20,7 +20,9 @@ namespace rtb
 class batch_engine
 {
 public:
-    batch_engine(size_t partial_budget_bytes, bool use_graph);
+    // high_priority: its stream's kernels go ahead of other streams' (a server's first frames beside its continuous
+    // wavefront)
+    batch_engine(size_t partial_budget_bytes, bool use_graph, bool high_priority = false);
     ~batch_engine();
     batch_engine(const batch_engine&) = delete;
     batch_engine& operator=(const batch_engine&) = delete;
@@ -45,6 +47,8 @@ public:
     void reserve_pool(size_t bytes);
     int64_t passes(int handle) const;
     void pixels(int handle, double* out, int64_t count);
+    // The job's sums (width * height * 3 doubles) into device memory, complete on return
+    void copy_sums(int handle, double* device_out);
     // The job's image through the display transform, 4 bytes per pixel into host memory
     void display(int handle, const rt_display_options& options, uint8_t* out, int64_t count);
     uint64_t rays(int handle) const;
@@ -112,10 +116,14 @@ public:
     stream_engine(const stream_engine&) = delete;
     stream_engine& operator=(const stream_engine&) = delete;
 
-    // A request: its view of a resident scene, RNG seed and job field, and target passes; its first pass is published
-    // at the next advance. Its sums and accumulator (48 bytes a pixel) stay resident until remove.
+    // A request: its view of a resident scene, RNG seed and job field, and target passes. Its first pass is published
+    // at the next advance, or, with first_pass_elsewhere, rendered by the caller into sums(handle) and handed over by
+    // first_pass_done. Its sums and accumulator (48 bytes a pixel) stay resident until remove.
     int add(std::shared_ptr<resident_scene> scene, const rt_camera_desc& camera, uint64_t seed, uint32_t job_id,
-            int64_t target);
+            int64_t target, bool first_pass_elsewhere = false);
+    double* sums(int handle) { return requests_.at(handle)->sums.data(); }
+    // The request's first pass is in its sums (written and complete before the call): refinement may start
+    void first_pass_done(int handle);
     // Stops publishing the request's samples, waits for those in flight and frees its memory
     void remove(int handle);
     // Runs groups of steps until at least `seconds` of GPU time have been read back (one group at least when there is
@@ -140,6 +148,7 @@ private:
     struct request
     {
         std::shared_ptr<resident_scene> scene;
+        bool awaiting_first = false; // its first pass is rendered elsewhere and not yet handed over
         rt_camera_desc camera{};
         camera_params cam{};
         uint64_t seed = 0;
@@ -202,6 +211,7 @@ private:
     device_array<unsigned long long> counters_;
     device_array<batch_job> table_;
     device_array<unsigned long long> done_;
+    device_array<int64_t> starts_; // each ring entry's first sample
     device_array<float4> values_;
     device_array<stream_reduce_item> reduce_items_;
     device_array<uint8_t> rgba_;
@@ -264,6 +274,7 @@ private:
         uint64_t seed;
         int64_t target;
         int handle = -1;
+        int first_handle = -1; // the continuous server: its first frame's job in the batch engine, until handed over
         int32_t state = RT_REQUEST_QUEUED;
         clock::time_point submitted;
         double first_frame_seconds = -1;
@@ -271,10 +282,15 @@ private:
         size_t bytes = 0;
     };
     rt_server_options options_;
-    std::unique_ptr<batch_engine> engine_;  // batched steps
-    std::unique_ptr<stream_engine> stream_; // or the continuous wavefront
+    std::unique_ptr<batch_engine> engine_;  // batched steps (the continuous server: its first frames)
+    std::unique_ptr<stream_engine> stream_; // the continuous wavefront (refinement)
     std::map<int64_t, request> requests_;
     std::deque<int64_t> queue_;
+    std::deque<int64_t> first_queue_; // the continuous server: admitted requests whose first frame is still to render
+    uint64_t first_rays_ = 0;          // and the rays of the first frames it has handed over
+    uint64_t first_shadow_rays_ = 0;
+    // the estimated GPU time of a step of first frames (at least one frame a step)
+    static constexpr double first_frame_seconds = 0.004;
     int64_t next_id_ = 1;
     size_t used_bytes_ = 0;
     std::map<const resident_scene*, double> cost_; // seconds per pixel pass, learned per scene

@@ -2654,14 +2654,38 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                 atomicAdd(W.jobs[finished_job].done, static_cast<unsigned long long>(__popc(peers)));
             }
         }
+        // A stream run's segment (logical number) holding sample s: `hint` first (a warp's claims are consecutive
+        // numbers, nearly always in its leader's segment), else a binary search over the ring of segment starts
+        const auto find_segment = [&](int64_t s, int hint) -> int {
+            const int mask = W.job_mask;
+            if (hint >= window.x && hint < window.y && W.starts[hint & mask] <= s &&
+                (hint + 1 >= window.y || s < W.starts[(hint + 1) & mask]))
+            {
+                return hint;
+            }
+            int lo = window.x, hi = window.y - 1;
+            while (lo < hi)
+            {
+                const int mid = (lo + hi + 1) >> 1;
+                if (W.starts[mid & mask] <= s)
+                {
+                    lo = mid;
+                }
+                else
+                {
+                    hi = mid - 1;
+                }
+            }
+            return lo;
+        };
         // Sample s taken by this slot: its job, its pixel and pass (false for a lane of a tile over the image's edge,
         // which claims again; in a stream run it counts as done, having no value to wait for)
-        const auto take = [&](unsigned long long s) -> bool {
+        const auto take = [&](unsigned long long s, int hint) -> bool {
             int k = 0;
             if constexpr (BATCH)
             {
-                k = find_job<job_samples>(W.jobs, window.x, window.y, static_cast<int64_t>(s), W.job_mask);
-                k = W.job_mask != 0 ? (k & W.job_mask) : k;
+                k = stream_run ? (find_segment(static_cast<int64_t>(s), hint) & W.job_mask)
+                               : find_job<job_samples>(W.jobs, window.x, window.y, static_cast<int64_t>(s));
             }
             const batch_job* K = BATCH ? W.jobs + k : nullptr;
             const camera_params& c = BATCH ? K->cam : P.cam;
@@ -2696,7 +2720,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         if (ready)
         {
             flags &= ~wave_reserved;
-            need = !take(reserved);
+            need = !take(reserved, -1);
         }
         // Samples for the slots that need one, a pass of the image after another (of each job after another): one
         // atomic per warp. In a stream run a claim beyond what is published waits in the slot (wave_reserved).
@@ -2715,6 +2739,15 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                                  static_cast<unsigned long long>(__popc(needing)));
             }
             base = __shfl_sync(full_warp, base, leader);
+            int hint = -1;
+            if (stream_run)
+            {
+                if (static_cast<int>(lane) == leader && base < limit)
+                {
+                    hint = find_segment(static_cast<int64_t>(base), -1);
+                }
+                hint = __shfl_sync(full_warp, hint, leader);
+            }
             if (need)
             {
                 const unsigned long long s = base + static_cast<unsigned long long>(__popc(needing & lanes_below));
@@ -2734,7 +2767,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                 }
                 else
                 {
-                    need = !take(s);
+                    need = !take(s, hint);
                 }
             }
         }
@@ -2902,6 +2935,15 @@ __device__ __forceinline__ void wave_camera_query(const wave_buffers& B, const w
     }
 }
 
+template <bool FEATURES>
+__device__ __forceinline__ void flat_search(const scene_view& S, float3 o, float3 d, float time, int from, bool inward,
+                                            int skip, bool any, hit_info& hit);
+// The same, called rather than inlined: a walk compiled with the flat search inlined beside its own leaf tests rounds
+// differently (the shared tests are contracted differently), and the walk must give a session's hits bit for bit
+template <bool FEATURES>
+__device__ __noinline__ void flat_search_call(const scene_view& S, float3 o, float3 d, float time, int from,
+                                              bool inward, int skip, bool any, hit_info& hit);
+
 // The trace kernel's resident blocks per multiprocessor (64 registers at 8) and the number of lanes still walking
 // under which a warp stops to give its idle lanes new queries (the addendum's 20 of 32)
 #ifndef RTB_TRACE_MIN_BLOCKS
@@ -2948,6 +2990,10 @@ __global__ void __launch_bounds__(render_block, MINB)
     // the scene the lane's query walks: its job's, or the launch's (a __grid_constant__ parameter, read in place)
     const scene_view* job_scene = BATCH ? &W.jobs[W.job_first].scene : &S0;
     const auto scene = [&]() -> const scene_view& { return *job_scene; };
+    // the lane's tree, read from its scene once a query (a batch's scene is in global memory, where every read of it
+    // in the walk would wait on L1 behind the stack's stores)
+    const bvh_node* tree_nodes = scene().nodes;
+    const bvh4_node* tree_wide = scene().wide_nodes;
     const auto pop = [&]() -> int {
         while (sp > 0)
         {
@@ -3008,6 +3054,8 @@ __global__ void __launch_bounds__(render_block, MINB)
                 if constexpr (BATCH)
                 {
                     job_scene = &W.jobs[qm.y >> 3].scene;
+                    tree_nodes = scene().nodes;
+                    tree_wide = scene().wide_nodes;
                 }
                 ++walks[shadow ? 1 : 0];
                 inverse_a = 1.0f / length_squared(d);
@@ -3017,6 +3065,13 @@ __global__ void __launch_bounds__(render_block, MINB)
                 leaf = 0;
                 link = scene().node_count == 0 ? traversal_done : 0;
                 has_query = true;
+                if (BATCH && scene().flat != 0)
+                {
+                    // a flat-searched scene beside tree-searched ones (a stream run): its query answered here by the
+                    // flat search, the same hits its session's flat trace kernel finds
+                    flat_search_call<FEATURES>(scene(), o, d, time, from, inward, skip, shadow, hit);
+                    link = traversal_done;
+                }
             }
         }
         if (__ballot_sync(full_warp, has_query) == 0u)
@@ -3036,7 +3091,7 @@ __global__ void __launch_bounds__(render_block, MINB)
                 }
                 if (WIDE && descending)
                 {
-                    const float4* np = reinterpret_cast<const float4*>(scene().wide_nodes + link);
+                    const float4* np = reinterpret_cast<const float4*>(tree_wide + link);
                     const float4 lx = __ldg(np), hx = __ldg(np + 1);
                     const float4 ly = __ldg(np + 2), hy = __ldg(np + 3);
                     const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
@@ -3101,7 +3156,7 @@ __global__ void __launch_bounds__(render_block, MINB)
                 }
                 else if (descending)
                 {
-                    const float4* np = reinterpret_cast<const float4*>(scene().nodes + link);
+                    const float4* np = reinterpret_cast<const float4*>(tree_nodes + link);
                     const float4 nx = __ldg(np);
                     const float4 ny = __ldg(np + 1);
                     const float4 nz = __ldg(np + 2);
@@ -3233,6 +3288,13 @@ __device__ __forceinline__ void flat_search(const scene_view& S, float3 o, float
             }
         }
     }
+}
+
+template <bool FEATURES>
+__device__ __noinline__ void flat_search_call(const scene_view& S, float3 o, float3 d, float time, int from,
+                                              bool inward, int skip, bool any, hit_info& hit)
+{
+    flat_search<FEATURES>(S, o, d, time, from, inward, skip, any, hit);
 }
 
 // The queued queries of a flat-searched scene: one query per thread at a time (grid-stride), every lane the same

@@ -137,6 +137,7 @@ struct wave_batch
     int32_t job_mask;
     int32_t pad0;
     const int32_t* window;
+    const int64_t* starts; // each ring entry's first sample (its sample_begin), compact for the claims' search
 };
 
 // The stream run's reduction: each item a segment's samples added, pixel by pixel in pass order, into its request's

@@ -61,11 +61,13 @@ stream_engine::stream_engine(int slots, int64_t value_capacity, int group_steps,
     counters_.allocate_async(3, stream_); // [0] samples claimed, [1] samples published, [2] the segments' window
     table_.allocate_async(segment_ring, stream_);
     done_.allocate_async(segment_ring, stream_);
+    starts_.allocate_async(segment_ring, stream_);
     values_.allocate_async(static_cast<size_t>(value_capacity_), stream_);
     check(cudaMemsetAsync(counters_.data(), 0, counters_.bytes(), stream_), "clearing the stream's counters");
     check(cudaMemsetAsync(done_.data(), 0, done_.bytes(), stream_), "clearing the segments' counts");
     check(cudaMemsetAsync(control_.data(), 0, control_.bytes(), stream_), "clearing the queue");
     check(cudaMemsetAsync(table_.data(), 0, table_.bytes(), stream_), "clearing the segment table");
+    check(cudaMemsetAsync(starts_.data(), 0, starts_.bytes(), stream_), "clearing the segment starts");
     check(cudaHostAlloc(reinterpret_cast<void**>(&readback_), 2 * readback_bytes(), cudaHostAllocDefault),
           "allocating pinned memory");
     check(cudaHostAlloc(reinterpret_cast<void**>(&staging_), 2 * sizeof(group_control), cudaHostAllocDefault),
@@ -118,6 +120,7 @@ stream_engine::~stream_engine()
     counters_.release();
     table_.release();
     done_.release();
+    starts_.release();
     values_.release();
     reduce_items_.release();
     rgba_.release();
@@ -167,7 +170,7 @@ size_t stream_engine::job_bytes(const rt_camera_desc& camera)
 }
 
 int stream_engine::add(std::shared_ptr<resident_scene> scene, const rt_camera_desc& camera, uint64_t seed,
-                       uint32_t job_id, int64_t target)
+                       uint32_t job_id, int64_t target, bool first_pass_elsewhere)
 {
     if (target < 1)
     {
@@ -202,15 +205,35 @@ int stream_engine::add(std::shared_ptr<resident_scene> scene, const rt_camera_de
     check(cudaMemsetAsync(r->sums.data(), 0, r->sums.bytes(), stream_), "clearing the sums");
     check(cudaMemsetAsync(r->acc.data(), 0, r->acc.bytes(), stream_), "clearing the accumulator");
     check(cudaMemsetAsync(r->counters.data(), 0, r->counters.bytes(), stream_), "clearing the counters");
+    const int handle = next_handle_++;
     if (camera.max_depth == 0)
     {
         r->published = r->reduced = r->padded * target; // a path of no rays: every sample is 0
         r->passes = target;
     }
-    const int handle = next_handle_++;
-    fresh_.push_back(handle);
+    else if (first_pass_elsewhere)
+    {
+        r->awaiting_first = true;
+    }
+    else
+    {
+        fresh_.push_back(handle);
+    }
     requests_[handle] = std::move(r);
     return handle;
+}
+
+void stream_engine::first_pass_done(int handle)
+{
+    request& r = *requests_.at(handle);
+    if (!r.awaiting_first)
+    {
+        return; // a request of no rays: its passes were complete at admission
+    }
+    // the sums hold pass 0, the accumulator is clear: the next flush is at the first chunk's end
+    r.awaiting_first = false;
+    r.published = r.reduced = r.padded;
+    r.passes = 1;
 }
 
 void stream_engine::remove(int handle)
@@ -296,6 +319,8 @@ int64_t stream_engine::publish(int handle, request& r, int64_t count)
     // the host's entry may change as soon as the call returns)
     check(cudaMemsetAsync(done_.data() + slot, 0, sizeof(unsigned long long), stream_), "clearing a count");
     check(cudaMemcpyAsync(table_.data() + slot, &b, sizeof(batch_job), cudaMemcpyHostToDevice, stream_),
+          "publishing a segment");
+    check(cudaMemcpyAsync(starts_.data() + slot, &b.sample_begin, sizeof(int64_t), cudaMemcpyHostToDevice, stream_),
           "publishing a segment");
     published_ += count;
     value_head_ = at + count;
@@ -392,6 +417,7 @@ cudaGraphExec_t stream_engine::group_graph(int k)
     w.published = counters_.data() + 1;
     w.job_mask = segment_ring - 1;
     w.window = reinterpret_cast<const int32_t*>(counters_.data() + 2);
+    w.starts = starts_.data();
     unsigned char* rb = readback_ + static_cast<size_t>(k) * readback_bytes();
     cudaGraph_t graph = nullptr;
     check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capturing a group of steps");
