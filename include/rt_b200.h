@@ -193,13 +193,18 @@ typedef struct rt_scene_desc
 
 /* ---- options and results: renderer.h:404-492, 530-562 -------------------------------------------------------- */
 
+/* renderer.h:402-409 precision: the number type the GPU computes with. RT_FLOAT32 is the hot path. RT_FLOAT64 renders
+ * the books' scenes (spheres, moving spheres, quads, smoke, textures; the four books' strategies) with every number of a
+ * path in double and 53-bit random numbers, in the persistent form: a mode to compare with, as the reference's. As
+ * there, the NEE/MIS integrator (rt_scene_desc.quality) and triangle meshes compute in float only (RT_ERR_INVALID), and
+ * a float64 session displays the books' bytes only. */
 enum { RT_FLOAT32 = 0, RT_FLOAT64 = 1 };
 
 typedef struct rt_render_options
 {
     uint64_t seed;              /* round r draws with seed + r * 2^32 (renderer.h:564-566) */
     int64_t passes;             /* 0: sqrt_spp^2; > 0: exactly that many */
-    int32_t arithmetic;         /* RT_FLOAT32 (the hot path); RT_FLOAT64 is refused: FP64 is used only where needed */
+    int32_t arithmetic;         /* RT_FLOAT32 (the hot path) or RT_FLOAT64 (the books' integrator in double) */
     int32_t pad0;
     double launch_seconds;      /* how long one launch is planned to take, (0, 0.5] */
 } rt_render_options;
@@ -247,7 +252,7 @@ enum { RT_FORM_AUTO = 0, RT_FORM_PERSISTENT = 1, RT_FORM_WAVEFRONT = 2 };
 typedef struct rt_session_options
 {
     uint64_t seed;
-    int32_t arithmetic;         /* RT_FLOAT32 */
+    int32_t arithmetic;         /* RT_FLOAT32 or RT_FLOAT64 (a persistent-form session; RT_FORM_WAVEFRONT is refused) */
     int32_t form;               /* RT_FORM_*; 0 (AUTO) where the caller zeroed the struct */
     double launch_seconds;
 } rt_session_options;

@@ -57,6 +57,31 @@ int shim_render(const rt_scene_desc* scene, uint64_t seed, int64_t passes, int32
     }
 }
 
+// gpu::render(scene, options) with options.arithmetic = precision::float64 (fp64 != 0) or float32: its pixels and
+// ray count. Returns 0, or 1 with the exception's message.
+int shim_render_precision(const rt_scene_desc* scene, uint64_t seed, int64_t passes, int32_t fp64, double* pixels,
+                          uint64_t* rays, char* error, int32_t error_size)
+{
+    try
+    {
+        const gpu::scene_desc s = ref_convert::to_ref(*scene);
+        gpu::render_options o;
+        o.seed = seed;
+        o.passes = passes;
+        o.quality_kernel = scene->quality != 0;
+        o.arithmetic = fp64 != 0 ? gpu::precision::float64 : gpu::precision::float32;
+        const gpu::render_result r = gpu::render(s, o);
+        std::memcpy(pixels, r.pixels.data(), r.pixels.size() * sizeof(double));
+        *rays = r.rays;
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        copy_error(e.what(), error, error_size);
+        return 1;
+    }
+}
+
 // A gpu::session of the scene: render_to(passes), then pixels() and display(options) as the viewer calls them
 int shim_session(const rt_scene_desc* scene, uint64_t seed, int64_t passes, int32_t tone, double exposure,
                  double* pixels, uint8_t* rgba, char* error, int32_t error_size)

@@ -205,16 +205,20 @@ def _desc_of(scene) -> "C._Pointer[_abi.SceneDesc]":
     return scene.desc if isinstance(scene, OwnedScene) else scene
 
 
+ARITHMETIC = {"float32": _abi.RT_FLOAT32, "float64": _abi.RT_FLOAT64}
+
+
 def render(scene, seed: int = 0, passes: int = 0, launch_seconds: float = 0.05,
-           out: Optional[np.ndarray] = None) -> RenderResult:
-    """renderer.h:526 render(): the whole job through the C-ABI, host tables in, host pixels out."""
+           out: Optional[np.ndarray] = None, arithmetic: str = "float32") -> RenderResult:
+    """renderer.h:526 render(): the whole job through the C-ABI, host tables in, host pixels out. arithmetic:
+    "float32" (the hot path) or "float64" (the books' integrator in double, renderer.h:402-409)."""
     desc = _desc_of(scene)
     cam = desc.contents.camera
     h, w = int(cam.image_height), int(cam.image_width)
     pixels = out if out is not None else np.empty((h, w, 3), dtype=np.float64)
     if pixels.shape != (h, w, 3) or pixels.dtype != np.float64 or not pixels.flags.c_contiguous:
         raise ValueError("out must be a C-contiguous float64 array of shape (height, width, 3)")
-    o = _abi.RenderOptions(seed=seed, passes=passes, arithmetic=_abi.RT_FLOAT32, launch_seconds=launch_seconds)
+    o = _abi.RenderOptions(seed=seed, passes=passes, arithmetic=ARITHMETIC[arithmetic], launch_seconds=launch_seconds)
     r = _abi.RenderResult()
     _check(_lib().rt_render(desc, C.byref(o), pixels.ctypes.data_as(C.POINTER(C.c_double)), pixels.size,
                             C.byref(r)))
@@ -323,10 +327,12 @@ def autotune_simulate(measure, max_trace_blocks: int = 8, max_trace_blocks_roomy
 class Session:
     """renderer.h:591-673 session: one view whose image gains passes on demand; its sums stay on the device."""
 
-    def __init__(self, scene: Scene, seed: int = 0, launch_seconds: float = 0.05, form: str = "auto"):
-        """form: "auto", "persistent" or "wavefront" (FORMS): how the launches run; the image is the same."""
+    def __init__(self, scene: Scene, seed: int = 0, launch_seconds: float = 0.05, form: str = "auto",
+                 arithmetic: str = "float32"):
+        """form: "auto", "persistent" or "wavefront" (FORMS): how the launches run; the image is the same.
+        arithmetic: "float32" or "float64" (ARITHMETIC; float64 renders the books' scenes in the persistent form)."""
         self._scene = scene
-        o = _abi.SessionOptions(seed=seed, arithmetic=_abi.RT_FLOAT32, form=FORMS[form],
+        o = _abi.SessionOptions(seed=seed, arithmetic=ARITHMETIC[arithmetic], form=FORMS[form],
                                 launch_seconds=launch_seconds)
         handle = C.c_void_p()
         _check(_lib().rt_session_create(scene._handle, C.byref(o), C.byref(handle)))

@@ -279,4 +279,109 @@ struct scene_view
     int32_t medium_base;     // the global id of a particle of media[0]: right after the surface primitives
     int32_t has_textures;    // some material reads a texture (not one solid color)
 };
+
+// ---- the same tables in double, for the books' integrator in FP64 (precision::float64, renderer.h:402-409) --------
+// They follow the float tables' leaf order and global ids (one tree serves both: its float boxes, widened by
+// box_margin, hold every double primitive), so prim_material, the lights' twins and the tree are shared.
+struct alignas(16) d4
+{
+    double x, y, z, w;
+};
+
+// A sphere (center, radius), its motion over the shutter (w unused), and its texture frame as sphere_frame
+using sphere_d = d4;
+using motion_d = d4;
+using frame_d = d4; // cos_theta, sin_theta, k, limit
+
+// A quad: corner, unit normal, the dual basis alpha and beta axes (make_quad's numbers, not rounded to float)
+struct alignas(16) quad_d
+{
+    double q[3], n[3], a[3], b[3];
+};
+
+struct alignas(16) material_d
+{
+    double r, g, b;
+    double fuzz, ior;
+    int32_t kind;
+    int32_t texture;
+    int32_t texture_needs;
+    int32_t pad;
+};
+
+struct alignas(16) light_d
+{
+    quad_d quad;
+    double u[3], v[3], c[3];
+    double area, cdf, radius, weight;
+    int32_t kind;
+    int32_t twin;
+};
+
+struct alignas(16) texture_d
+{
+    int32_t kind, even, odd, table;
+    double r, g, b, inv_scale;
+};
+
+struct alignas(16) noise_d
+{
+    d4 gradients[256];
+    uint8_t perm_x[256];
+    uint8_t perm_y[256];
+    uint8_t perm_z[256];
+    double scale;
+};
+
+struct alignas(16) medium_d
+{
+    double lo[3], hi[3];
+    double neg_inv_density;
+    double c[3];
+    double radius;
+    double dm[3];
+    int32_t material;
+    int32_t first_quad;
+    int32_t quad_count;
+    int32_t pad;
+};
+
+// The camera in double: the pixel grid relative to the center, the lens, the sky
+struct camera_d
+{
+    int32_t width, height, sqrt_spp, max_depth;
+    double recip_sqrt_spp;
+    double center[3], to_pixel00[3], delta_u[3], delta_v[3], disk_u[3], disk_v[3], sky_bottom[3], sky_top[3];
+    int32_t defocus;
+    int32_t sampling;
+};
+
+struct scene_view_f64
+{
+    const bvh_node* nodes;      // the float tree (boxes rounded outward), shared with the float tables
+    const sphere_d* spheres;    // leaf order, as scene_view's
+    const quad_d* quads;
+    const int32_t* prim_material;
+    const material_d* materials;
+    const light_d* lights;
+    const texture_d* textures;
+    const image_info* images;
+    const float4* texels;       // an image's texels are given as floats
+    const noise_d* noises;
+    const motion_d* sphere_motion;
+    const frame_d* sphere_frames;
+    const medium_d* media;
+    const quad_d* boundary_quads;
+    double box_margin;          // how far a double primitive may reach past its float box: node bounds are widened by it
+    int32_t node_count;
+    int32_t flat;
+    int32_t quad_base;
+    int32_t prim_count;
+    int32_t light_count;
+    int32_t has_motion;
+    int32_t medium_count;
+    int32_t medium_base;
+    int32_t has_textures;
+    int32_t pad;
+};
 } // namespace rtb

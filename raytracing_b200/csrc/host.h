@@ -137,6 +137,7 @@ bool is_convex(const rt_quad_desc* quads, int64_t count);
 
 // The camera in the kernels' form: the pixel grid relative to the center subtracted in double (renderer.cu:512-532)
 camera_params to_camera(const rt_camera_desc& desc);
+camera_d to_camera_d(const rt_camera_desc& desc);
 
 // A scene on the device: its BVH, primitives, materials, lights and lamps, uploaded once
 class resident_scene
@@ -150,12 +151,27 @@ public:
     const int32_t* prim_source() const { return prim_source_.data(); }
     const rt_scene_stats& stats() const { return stats_; }
     int device() const { return device_; }
+    // The double tables for the books' integrator in FP64, made for the scenes it can render (no NEE/MIS, no
+    // triangles); null otherwise
+    const scene_view_f64* view_f64() const { return has_f64_ ? &view_f64_ : nullptr; }
 
 private:
     int device_ = 0;
     rt_camera_desc camera_{};
     bool quality_ = false;
     scene_view view_{};
+    bool has_f64_ = false;
+    scene_view_f64 view_f64_{};
+    device_array<sphere_d> spheres_d_;
+    device_array<motion_d> sphere_motion_d_;
+    device_array<frame_d> sphere_frames_d_;
+    device_array<quad_d> quads_d_;
+    device_array<material_d> materials_d_;
+    device_array<light_d> lights_d_;
+    device_array<texture_d> textures_d_;
+    device_array<noise_d> noises_d_;
+    device_array<medium_d> media_d_;
+    device_array<quad_d> boundary_quads_d_;
     rt_scene_stats stats_{};
     device_array<bvh_node> nodes_;
     device_array<bvh4_node> wide_nodes_;
@@ -332,7 +348,14 @@ public:
     void display(const rt_display_options& options, uint8_t* rgba, int64_t byte_count);
     int64_t passes() const { return passes_; }
     // The counting build: launches that also count node fetches and primitive tests (slower; for the roofline)
-    void set_counting(bool on) { counting_ = on; }
+    void set_counting(bool on)
+    {
+        if (on && f64_)
+        {
+            fail(RT_ERR_LOGIC, "the counting build computes in float32");
+        }
+        counting_ = on;
+    }
     void fetch_counts(uint64_t out[4]) const;
     const rt_camera_desc& camera() const { return camera_; }
 
@@ -341,6 +364,8 @@ private:
     rt_session_options options_;
     rt_camera_desc camera_{};
     camera_params cam_{};
+    camera_d cam_d_{};  // the same view in double, for an FP64 session
+    bool f64_ = false;  // RT_FLOAT64: the books' integrator in double, persistent form
     cudaStream_t stream_ = nullptr;
     cudaEvent_t start_ = nullptr;
     cudaEvent_t stop_ = nullptr;

@@ -20,6 +20,7 @@
 
 #include "ggx_energy_table.h"
 #include "kernels.cuh"
+#include "philox.cuh"
 #include "rt_b200.h"
 
 namespace rtb
@@ -54,27 +55,7 @@ constexpr float inverse_pi_f = 0.318309886183790671538f;
 constexpr float uniform_sphere_density = 0.0795774715459476678844f; // 1 / (4 pi)
 constexpr float infinity_f = __builtin_huge_valf();
 
-// ---- counter-based random numbers ------------------------------------------------------------------------------
-// Philox4x32-10 (Salmon, Moraes, Dror and Shaw, "Parallel Random Numbers: As Easy as 1, 2, 3", SC 2011): ten rounds of
-// two 32x32->64 multiplies and a Feistel-like mix, keyed by the seed. The counter is (pixel, pass in the round,
-// depth << 4 | block, job): every number a sample draws is a pure function of the seed and where it is used, so a
-// seed fixes every image, whatever thread, launch or batch renders it.
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
-{
-#pragma unroll
-    for (int round = 0; round < 10; ++round)
-    {
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
-        const uint32_t lo0 = 0xD2511F53u * c.x;
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
-        const uint32_t lo1 = 0xCD9E8D57u * c.z;
-        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-        k.x += 0x9E3779B9u;
-        k.y += 0xBB67AE85u;
-    }
-    return c;
-}
-
+// ---- counter-based random numbers (philox.cuh) -------------------------------------------------------------------
 // 24 random bits as a float in [0, 1 - 2^-24]: every value k / 2^24 exactly, as random_real<float> (random.cuh:79-93)
 __device__ __forceinline__ float to_unit(uint32_t x) { return static_cast<float>(x >> 8) * 0x1p-24f; }
 

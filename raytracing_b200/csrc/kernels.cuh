@@ -247,6 +247,31 @@ cudaError_t preload_wave_batch();
 cudaError_t wave_attributes(const scene_view& scene, bool quality, kernel_attributes& shade, kernel_attributes& trace,
                             int trace_min_blocks = RTB_TRACE_MIN_BLOCKS_DEFAULT);
 
+// The books' integrator in double (precision::float64; renderer.h:402-409, all_books_kernel<double>,
+// renderer.cu:445-451): a persistent launch over the same (pixel, chunk) work items as launch_params' and into the
+// same chunk partials, so launch_reduce adds them into the sums. Its own random numbers: 53-bit uniforms.
+struct launch_params_f64
+{
+    scene_view_f64 scene;
+    camera_d cam;
+    uint64_t seed;
+    int64_t pass_begin;
+    int64_t pass_end;
+    int64_t first_chunk;
+    int32_t chunk;
+    int32_t chunks;
+    int32_t tiles_x;
+    int32_t padded_pixels;
+    int64_t total_items;
+    int32_t round_passes;
+    int32_t pad0;
+    unsigned long long* work_counter;
+    double* partials;
+    unsigned long long* counters; // [0] path segments
+};
+cudaError_t launch_render_f64(const launch_params_f64& p, int grid, cudaStream_t stream);
+cudaError_t render_f64_attributes(const scene_view_f64& scene, kernel_attributes& out);
+
 // Parity hooks: closest hits of given rays (source ids through prim_source), and the camera rays of one pass
 cudaError_t launch_closest_hits(const scene_view& s, const float* origins, const float* directions, int64_t count,
                                 const int32_t* prim_source, int32_t* ids, float* ts, cudaStream_t stream);

@@ -61,6 +61,17 @@ quad12 make_quad(const rt_quad_desc& d)
     return q;
 }
 
+// The same quad in double, for the FP64 integrator
+quad_d make_quad_d(const rt_quad_desc& d)
+{
+    const rt_vec3 n = cross(d.u, d.v);
+    const rt_vec3 normal = scale(1 / std::sqrt(dot(n, n)), n);
+    const rt_vec3 w = scale(1 / dot(n, n), n);
+    const rt_vec3 a = cross(d.v, w);
+    const rt_vec3 b = cross(w, d.u);
+    return quad_d{{d.q.x, d.q.y, d.q.z}, {normal.x, normal.y, normal.z}, {a.x, a.y, a.z}, {b.x, b.y, b.z}};
+}
+
 // A scene of at most RTB_SMALL_SCENE primitives gets one leaf per primitive kind (a test of all of them beats a
 // tree walk there, as the reference found for up to 8 shapes, renderer.cu:75-82); a larger scene of spheres and quads
 // gets leaves of at most RTB_LEAF_SIZE
@@ -504,6 +515,32 @@ camera_params to_camera(const rt_camera_desc& d)
     c.disk_v = to_f3(d.defocus_disk_v);
     c.sky_bottom = to_f3(d.sky_bottom);
     c.sky_top = to_f3(d.sky_top);
+    c.sampling = d.sampling;
+    return c;
+}
+
+camera_d to_camera_d(const rt_camera_desc& d)
+{
+    const auto put = [](double* out, rt_vec3 v) {
+        out[0] = v.x;
+        out[1] = v.y;
+        out[2] = v.z;
+    };
+    camera_d c{};
+    c.width = d.image_width;
+    c.height = d.image_height;
+    c.sqrt_spp = d.sqrt_spp;
+    c.max_depth = d.max_depth;
+    c.recip_sqrt_spp = 1.0 / d.sqrt_spp;
+    put(c.center, d.center);
+    put(c.to_pixel00, sub(d.pixel00_loc, d.center));
+    put(c.delta_u, d.pixel_delta_u);
+    put(c.delta_v, d.pixel_delta_v);
+    put(c.disk_u, d.defocus_disk_u);
+    put(c.disk_v, d.defocus_disk_v);
+    put(c.sky_bottom, d.sky_bottom);
+    put(c.sky_top, d.sky_top);
+    c.defocus = d.defocus;
     c.sampling = d.sampling;
     return c;
 }
@@ -1016,6 +1053,209 @@ resident_scene::resident_scene(const rt_scene_desc& d)
     view_.medium_count = static_cast<int32_t>(media.size());
     view_.medium_base = S + Q + T;
 
+    // The double tables of the books' integrator in FP64 (precision::float64 renders the books' scenes only: the
+    // NEE/MIS integrator and triangle meshes compute in float, renderer.cu:2064-2078), in the float tables' leaf order
+    has_f64_ = !quality_ && T == 0;
+    if (has_f64_)
+    {
+        std::vector<sphere_d> spheres_d(spheres.size());
+        std::vector<motion_d> motion_d_rows(sphere_motion.empty() ? 0 : spheres.size());
+        std::vector<frame_d> frames_d(spheres.size());
+        // How far a double sphere can stand out of the box the builder made around its float copy (center, motion and
+        // radius each rounded to float): the walk widens every node bound by twice that, and by a hair more for the
+        // slab test's own rounding
+        double stand_out = 0;
+        double largest = 1;
+        for (size_t k = 0; k < spheres.size(); ++k)
+        {
+            const int32_t src = tree.order[kind_sphere][k];
+            const rt_sphere_desc& s = d.spheres[src];
+            spheres_d[k] = {s.center.x, s.center.y, s.center.z, s.radius};
+            if (!motion_d_rows.empty())
+            {
+                motion_d_rows[k] = {s.displacement.x, s.displacement.y, s.displacement.z, 0.0};
+            }
+            const double cc = dot(s.center, s.center);
+            frames_d[k] = {s.uv_cos, s.uv_sin, cc - s.radius * s.radius, 2 * s.radius * std::sqrt(cc)};
+            const sphere4& f = source_spheres[static_cast<size_t>(src)];
+            const float4& fm = source_motion[static_cast<size_t>(src)];
+            const double center_gap = std::max({std::fabs(f.cx - s.center.x), std::fabs(f.cy - s.center.y),
+                                                std::fabs(f.cz - s.center.z)});
+            const double motion_gap = std::max({std::fabs(fm.x - s.displacement.x), std::fabs(fm.y - s.displacement.y),
+                                                std::fabs(fm.z - s.displacement.z)});
+            stand_out = std::max(stand_out, center_gap + motion_gap + std::fabs(std::fabs(f.r) - s.radius));
+            largest = std::max({largest, std::sqrt(cc) + s.radius + std::sqrt(dot(s.displacement, s.displacement))});
+        }
+        std::vector<quad_d> quads_d(quads.size());
+        for (size_t k = 0; k < quads.size(); ++k)
+        {
+            const rt_quad_desc& q = d.quads[tree.order[kind_quad][k]];
+            quads_d[k] = make_quad_d(q);
+            largest = std::max({largest, std::fabs(q.q.x) + std::fabs(q.u.x) + std::fabs(q.v.x),
+                                std::fabs(q.q.y) + std::fabs(q.u.y) + std::fabs(q.v.y),
+                                std::fabs(q.q.z) + std::fabs(q.u.z) + std::fabs(q.v.z)});
+        }
+        std::vector<material_d> materials_d(materials.size());
+        for (size_t i = 0; i < materials.size(); ++i)
+        {
+            const rt_material_desc& m = d.materials[i];
+            const bool textured = m.kind == RT_LAMBERTIAN || m.kind == RT_DIFFUSE_LIGHT || m.kind == RT_ISOTROPIC;
+            const rt_vec3 color = textured ? d.textures[m.texture].rgb : m.albedo;
+            material_d& v = materials_d[i];
+            v.r = color.x;
+            v.g = color.y;
+            v.b = color.z;
+            v.fuzz = std::min(m.fuzz, 1.0);
+            v.ior = m.refraction_index;
+            v.kind = m.kind;
+            v.texture = materials[i].texture;
+            v.texture_needs = materials[i].texture_needs;
+        }
+        std::vector<texture_d> textures_d;
+        std::vector<noise_d> noises_d;
+        for (int64_t i = 0; i < d.texture_count; ++i)
+        {
+            const rt_texture_desc& t = d.textures[i];
+            texture_d v{};
+            v.kind = t.kind;
+            v.even = t.even;
+            v.odd = t.odd;
+            v.table = textures[static_cast<size_t>(i)].table;
+            v.r = t.rgb.x;
+            v.g = t.rgb.y;
+            v.b = t.rgb.z;
+            v.inv_scale = t.inv_scale;
+            if (t.kind == RT_TEXTURE_NOISE)
+            {
+                noise_d n{};
+                const rt_perlin_desc& p = d.perlins[t.perlin];
+                for (int k = 0; k < 256; ++k)
+                {
+                    n.gradients[k] = {p.random_vectors[k].x, p.random_vectors[k].y, p.random_vectors[k].z, 0.0};
+                    n.perm_x[k] = static_cast<uint8_t>(p.perm_x[k]);
+                    n.perm_y[k] = static_cast<uint8_t>(p.perm_y[k]);
+                    n.perm_z[k] = static_cast<uint8_t>(p.perm_z[k]);
+                }
+                n.scale = t.scale;
+                noises_d.push_back(n);
+            }
+            textures_d.push_back(v);
+        }
+        std::vector<light_d> lights_d(lights.size());
+        double cdf = 0;
+        for (size_t i = 0; i < lights.size(); ++i)
+        {
+            const rt_light_desc& l = d.lights[i];
+            light_d& v = lights_d[i];
+            cdf += l.weight;
+            v.kind = l.kind;
+            v.twin = lights[i].twin;
+            v.weight = l.weight;
+            v.cdf = cdf;
+            if (l.kind == RT_LIGHT_QUAD)
+            {
+                v.quad = make_quad_d(l.quad);
+                const rt_vec3 n = cross(l.quad.u, l.quad.v);
+                v.area = std::sqrt(dot(n, n));
+                v.u[0] = l.quad.u.x;
+                v.u[1] = l.quad.u.y;
+                v.u[2] = l.quad.u.z;
+                v.v[0] = l.quad.v.x;
+                v.v[1] = l.quad.v.y;
+                v.v[2] = l.quad.v.z;
+            }
+            else
+            {
+                v.c[0] = l.center.x;
+                v.c[1] = l.center.y;
+                v.c[2] = l.center.z;
+                v.radius = l.radius;
+            }
+        }
+        std::vector<medium_d> media_d(media.size());
+        std::vector<quad_d> boundary_d;
+        for (size_t i = 0; i < media.size(); ++i)
+        {
+            const rt_medium_desc& m = d.media[i];
+            medium_d& v = media_d[i];
+            v.neg_inv_density = m.neg_inv_density;
+            v.material = m.material;
+            v.first_quad = static_cast<int32_t>(boundary_d.size());
+            v.quad_count = media[i].quad_count;
+            for (int a = 0; a < 3; ++a)
+            {
+                v.lo[a] = std::numeric_limits<double>::infinity();
+                v.hi[a] = -std::numeric_limits<double>::infinity();
+            }
+            if (m.boundary == RT_BOUNDARY_SPHERE)
+            {
+                const rt_sphere_desc& s = m.sphere;
+                const double c[3] = {s.center.x, s.center.y, s.center.z};
+                const double dm[3] = {s.displacement.x, s.displacement.y, s.displacement.z};
+                for (int a = 0; a < 3; ++a)
+                {
+                    v.c[a] = c[a];
+                    v.dm[a] = dm[a];
+                    v.lo[a] = std::min(c[a], c[a] + dm[a]) - s.radius;
+                    v.hi[a] = std::max(c[a], c[a] + dm[a]) + s.radius;
+                }
+                v.radius = s.radius;
+            }
+            else
+            {
+                for (int64_t k = 0; k < m.quad_count; ++k)
+                {
+                    boundary_d.push_back(make_quad_d(m.quads[k]));
+                    const build_prim b = quad_prim(m.quads[k], 0);
+                    for (int a = 0; a < 3; ++a)
+                    {
+                        v.lo[a] = std::min(v.lo[a], b.lo[a]);
+                        v.hi[a] = std::max(v.hi[a], b.hi[a]);
+                    }
+                }
+            }
+        }
+        if (motion && motion_d_rows.empty())
+        {
+            motion_d_rows.assign(spheres.size(), d4{0.0, 0.0, 0.0, 0.0}); // a moving boundary alone moves
+        }
+        spheres_d_.upload(spheres_d);
+        sphere_motion_d_.upload(motion_d_rows);
+        sphere_frames_d_.upload(frames_d);
+        quads_d_.upload(quads_d);
+        materials_d_.upload(materials_d);
+        lights_d_.upload(lights_d);
+        textures_d_.upload(textures_d);
+        noises_d_.upload(noises_d);
+        media_d_.upload(media_d);
+        boundary_quads_d_.upload(boundary_d);
+
+        view_f64_.nodes = nodes_.data();
+        view_f64_.spheres = spheres_d_.data();
+        view_f64_.quads = quads_d_.data();
+        view_f64_.prim_material = prim_material_.data();
+        view_f64_.materials = materials_d_.data();
+        view_f64_.lights = lights_d_.data();
+        view_f64_.textures = textures_d_.data();
+        view_f64_.images = images_.data();
+        view_f64_.texels = texels_.data();
+        view_f64_.noises = noises_d_.data();
+        view_f64_.sphere_motion = sphere_motion_d_.data();
+        view_f64_.sphere_frames = sphere_frames_d_.data();
+        view_f64_.media = media_d_.data();
+        view_f64_.boundary_quads = boundary_quads_d_.data();
+        view_f64_.box_margin = 2 * stand_out + 1e-12 * largest;
+        view_f64_.node_count = view_.node_count;
+        view_f64_.flat = view_.flat;
+        view_f64_.quad_base = S;
+        view_f64_.prim_count = S + Q;
+        view_f64_.light_count = static_cast<int32_t>(lights.size());
+        view_f64_.has_motion = view_.has_motion;
+        view_f64_.medium_count = view_.medium_count;
+        view_f64_.medium_base = S + Q;
+        view_f64_.has_textures = view_.has_textures;
+    }
+
     stats_.spheres = S;
     stats_.quads = Q;
     stats_.triangles = T;
@@ -1029,7 +1269,10 @@ resident_scene::resident_scene(const rt_scene_desc& d)
                                                env_texels_.bytes() + env_bins_.bytes() + env_row_cos_.bytes() +
                                                sphere_motion_.bytes() + sphere_frames_.bytes() + textures_.bytes() +
                                                images_.bytes() + texels_.bytes() + noises_.bytes() + media_.bytes() +
-                                               boundary_quads_.bytes());
+                                               boundary_quads_.bytes() + spheres_d_.bytes() +
+                                               sphere_motion_d_.bytes() + sphere_frames_d_.bytes() + quads_d_.bytes() +
+                                               materials_d_.bytes() + lights_d_.bytes() + textures_d_.bytes() +
+                                               noises_d_.bytes() + media_d_.bytes() + boundary_quads_d_.bytes());
     stats_.depth = tree.depth;
     stats_.max_leaf_size = options.max_leaf_size;
     stats_.flat = view_.flat;

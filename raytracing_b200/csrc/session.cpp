@@ -26,9 +26,26 @@ constexpr double trial_samples = 32e6; // the autotuner's measured launch, by de
 session::session(std::shared_ptr<resident_scene> scene, const rt_session_options& options)
     : scene_(std::move(scene)), options_(options)
 {
-    if (options_.arithmetic != RT_FLOAT32)
+    if (options_.arithmetic != RT_FLOAT32 && options_.arithmetic != RT_FLOAT64)
     {
-        fail(RT_ERR_INVALID, "this integrator computes in float32, with FP64 only for large spheres and the sums");
+        fail(RT_ERR_INVALID, "arithmetic must be RT_FLOAT32 or RT_FLOAT64");
+    }
+    f64_ = options_.arithmetic == RT_FLOAT64;
+    if (f64_)
+    {
+        // What computes in float only, in the reference's order and sense (renderer.cu:2047-2078)
+        if (scene_->quality())
+        {
+            fail(RT_ERR_INVALID, "the quality kernel computes in float only");
+        }
+        if (scene_->view_f64() == nullptr)
+        {
+            fail(RT_ERR_INVALID, "a scene with triangle meshes renders in float only");
+        }
+        if (options_.form == RT_FORM_WAVEFRONT)
+        {
+            fail(RT_ERR_INVALID, "the wavefront form computes in float only");
+        }
     }
     if (!(options_.launch_seconds > 0 && options_.launch_seconds <= max_launch_seconds))
     {
@@ -44,10 +61,18 @@ session::session(std::shared_ptr<resident_scene> scene, const rt_session_options
         fail(RT_ERR_INVALID, "form must be RT_FORM_AUTO, RT_FORM_PERSISTENT or RT_FORM_WAVEFRONT");
     }
     kernel_attributes a{};
-    check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
+    if (f64_)
+    {
+        check(render_f64_attributes(*scene_->view_f64(), a), "querying the FP64 render kernel");
+    }
+    else
+    {
+        check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
+    }
     grid_ = a.multiprocessors * std::max(1, a.blocks_per_sm);
     const scene_view& view = scene_->view();
-    wavefront_ = options_.form == RT_FORM_WAVEFRONT || (options_.form == RT_FORM_AUTO && wavefront_suits(view));
+    wavefront_ = !f64_ &&
+                 (options_.form == RT_FORM_WAVEFRONT || (options_.form == RT_FORM_AUTO && wavefront_suits(view)));
     multiprocessors_ = a.multiprocessors;
     if (wavefront_)
     {
@@ -237,6 +262,7 @@ void session::set_camera(const rt_camera_desc& camera)
     validate(probe);
     camera_ = camera;
     cam_ = to_camera(camera);
+    cam_d_ = to_camera_d(camera);
     tiles_x_ = (camera.image_width + 7) / 8;
     const int tiles_y = (camera.image_height + 3) / 4;
     padded_pixels_ = tiles_x_ * tiles_y * 32;
@@ -355,7 +381,30 @@ double session::launch(int64_t end)
     else
     {
         cudaEvent_t* m = timing_ ? marks(3) : nullptr;
-        check(launch_render(p, scene_->quality(), counting_, grid_, stream_), "launching the render kernel");
+        if (f64_)
+        {
+            launch_params_f64 p64{};
+            p64.scene = *scene_->view_f64();
+            p64.cam = cam_d_;
+            p64.seed = p.seed;
+            p64.pass_begin = p.pass_begin;
+            p64.pass_end = p.pass_end;
+            p64.first_chunk = p.first_chunk;
+            p64.chunk = p.chunk;
+            p64.chunks = p.chunks;
+            p64.tiles_x = p.tiles_x;
+            p64.padded_pixels = p.padded_pixels;
+            p64.total_items = p.total_items;
+            p64.round_passes = p.round_passes;
+            p64.work_counter = p.work_counter;
+            p64.partials = p.partials;
+            p64.counters = p.counters;
+            check(launch_render_f64(p64, grid_, stream_), "launching the FP64 render kernel");
+        }
+        else
+        {
+            check(launch_render(p, scene_->quality(), counting_, grid_, stream_), "launching the render kernel");
+        }
         if (m)
         {
             check(cudaEventRecord(m[2], stream_), "recording a CUDA event");
@@ -492,6 +541,10 @@ void session::pixels(double* out, int64_t count) const
 void session::display(const rt_display_options& options, uint8_t* rgba, int64_t byte_count)
 {
     check_display(options);
+    if (f64_ && options.tone_map != RT_TONE_BOOKS)
+    {
+        fail(RT_ERR_INVALID, "a tone map other than books is a new display transform, which works in float only");
+    }
     const int64_t n = static_cast<int64_t>(camera_.image_width) * camera_.image_height * 4;
     if (byte_count != n)
     {
@@ -547,13 +600,18 @@ rt_kernel_info session::kernel() const
               "querying the wavefront kernels");
         a.blocks_per_sm = tuned_.trace_blocks_per_sm; // the trace kernel's launch, as the shape has it
     }
+    else if (f64_)
+    {
+        check(render_f64_attributes(*scene_->view_f64(), a), "querying the FP64 render kernel");
+    }
     else
     {
         check(render_attributes(scene_->view(), scene_->quality(), a), "querying the render kernel");
     }
     rt_kernel_info info{};
     const char* form = wavefront_ && !counting_ ? "wavefront" : "persistent";
-    std::snprintf(info.name, sizeof(info.name), "%s %s", form, scene_->quality() ? "nee-mis" : "books");
+    std::snprintf(info.name, sizeof(info.name), "%s %s", form,
+                  f64_ ? "books fp64" : (scene_->quality() ? "nee-mis" : "books"));
     info.registers = a.registers;
     info.local_bytes = a.local_bytes;
     info.blocks_per_multiprocessor = a.blocks_per_sm;

@@ -60,3 +60,28 @@ def test_reference_session_and_tone_map_through_the_shim(rt):
                             b2.ctypes.data_as(C.POINTER(C.c_uint8)), err, 512) == 0, err.value
     assert np.array_equal(p2, pixels)
     assert np.array_equal(b2, session.display())
+
+
+def test_reference_float64_render_through_the_shim_equals_the_c_abi(rt):
+    """precision::float64 through the reference's gpu::render reaches this library's FP64 integrator; a quality scene
+    in float64 is refused there with the reference's error class (std::invalid_argument)."""
+    s = rt.builtin_scene("bouncing", width=64, spp=4)
+    lib = _lib()
+    lib.shim_render_precision.restype = C.c_int
+    lib.shim_render_precision.argtypes = [C.c_void_p, C.c_uint64, C.c_int64, C.c_int32, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_uint64), C.c_char_p, C.c_int32]
+    pixels = np.zeros((s.height, s.width, 3))
+    rays = C.c_uint64()
+    err = C.create_string_buffer(512)
+    assert lib.shim_render_precision(C.cast(s.desc, C.c_void_p), 11, 32, 1, pixels.ctypes.data_as(
+        C.POINTER(C.c_double)), C.byref(rays), err, 512) == 0, err.value
+    ours = rt.render(s, seed=11, passes=32, arithmetic="float64")
+    assert ours.kernel["name"] == "persistent books fp64"
+    assert np.array_equal(pixels, ours.pixels)
+    assert rays.value == ours.rays
+
+    q = rt.builtin_scene("cornell-mis", width=32, spp=4)
+    p2 = np.zeros((q.height, q.width, 3))
+    assert lib.shim_render_precision(C.cast(q.desc, C.c_void_p), 1, 4, 1, p2.ctypes.data_as(C.POINTER(C.c_double)),
+                                     C.byref(rays), err, 512) == 1
+    assert b"float only" in err.value
