@@ -171,6 +171,24 @@ struct alignas(16) emitter20
     float er, eg, eb, pad1;
 };
 
+// A divisor d (1 <= d < 2^32) with its multiplier, for division by multiplication (Granlund and Montgomery, "Division by
+// Invariant Integers using Multiplication", PLDI 1994): for every n < 2^32, n / d is the high 64 bits of the 128-bit
+// product n * magic with magic = floor((2^64 - 1) / d) + 1. The product overshoots n / d by n (magic - 2^64 / d) / 2^64
+// < 2^-32, less than the 1/d that n / d's fraction stays below the next integer, so the quotient is exact; d = 1 keeps
+// n (magic 0). The kernels turn sample and work-item numbers into passes and pixels this way, where a division would
+// be a long software sequence.
+struct fast_divisor
+{
+    uint64_t magic;
+    uint32_t d;
+    uint32_t pad;
+};
+
+inline fast_divisor make_fast_divisor(uint32_t d)
+{
+    return {d > 1 ? ~uint64_t{0} / d + 1 : 0, d, 0};
+}
+
 // The camera (src/gpu/camera.cuh:33-50), pixel grid relative to the center computed in double on the host
 struct camera_params
 {
@@ -183,6 +201,12 @@ struct camera_params
     f3 disk_u, disk_v;
     f3 sky_bottom, sky_top;
     int32_t sampling;
+    // The view's divisors: a round's strata a side (sqrt_spp), a round's passes (sqrt_spp^2), the 8x4 tiles a row
+    // ((width + 7) / 8) and the padded pixels (tiles * 32) a pass of samples or work items spans
+    fast_divisor div_sqrt_spp;
+    fast_divisor div_round_passes;
+    fast_divisor div_tiles_x;
+    fast_divisor div_padded;
 };
 
 // A texture (src/gpu/texture.cuh:10-19): 32 bytes, two 16-byte loads. checker: `even`, `odd` are texture indices

@@ -56,6 +56,19 @@ constexpr float uniform_sphere_density = 0.0795774715459476678844f; // 1 / (4 pi
 constexpr float infinity_f = __builtin_huge_valf();
 
 // ---- counter-based random numbers (philox.cuh) -------------------------------------------------------------------
+// n / d by the divisor's multiplier (fast_divisor), for n < 2^32
+__device__ __forceinline__ uint32_t quotient(uint32_t n, const fast_divisor& v)
+{
+    return v.magic != 0 ? static_cast<uint32_t>(__umul64hi(static_cast<unsigned long long>(n), v.magic)) : n;
+}
+
+// A pass's stratum within its round: column s_i = round_pass % sqrt_spp, row s_j = round_pass / sqrt_spp
+__device__ __forceinline__ void stratum_of(const camera_params& cam, int round_pass, int& s_i, int& s_j)
+{
+    s_j = static_cast<int>(quotient(static_cast<uint32_t>(round_pass), cam.div_sqrt_spp));
+    s_i = round_pass - s_j * cam.sqrt_spp;
+}
+
 // 24 random bits as a float in [0, 1 - 2^-24]: every value k / 2^24 exactly, as random_real<float> (random.cuh:79-93)
 __device__ __forceinline__ float to_unit(uint32_t x) { return static_cast<float>(x >> 8) * 0x1p-24f; }
 
@@ -1872,6 +1885,61 @@ __device__ __forceinline__ step_result shade_quality(const scene_view& S, const 
 #define RTB_MIN_BLOCKS_FEATURES 5 // 0: as the kernel without the features
 #endif
 
+// Where sample number `local` of a launch (or of a batch job) lies: pass-major, then the pixels in 8x4 tiles (a
+// warp's worth); x may fall past the image's right edge or y past its bottom in the last tiles
+struct sample_place
+{
+    int64_t pass;
+    int x, y;
+};
+
+// (uses the camera's divisors: cam.div_padded and cam.div_tiles_x; a number of 2^32 or more, which only a served
+// request's numbering reaches, takes the 64-bit division)
+__device__ __forceinline__ sample_place place_of(int64_t local, const camera_params& cam, int64_t pass_begin)
+{
+    const uint32_t padded = cam.div_padded.d;
+    int64_t j;
+    int q;
+    if (local < (int64_t{1} << 32))
+    {
+        const auto n = static_cast<uint32_t>(local);
+        const uint32_t jj = quotient(n, cam.div_padded);
+        j = jj;
+        q = static_cast<int>(n - jj * padded);
+    }
+    else
+    {
+        j = local / padded;
+        q = static_cast<int>(local - j * padded);
+    }
+    const int tile = q >> 5;
+    const int l = q & 31;
+    const auto ty = static_cast<int>(quotient(static_cast<uint32_t>(tile), cam.div_tiles_x));
+    const int tx = tile - ty * static_cast<int>(cam.div_tiles_x.d);
+    return {pass_begin + j, tx * 8 + (l & 7), ty * 4 + (l >> 3)};
+}
+
+// A pass's round of strata and its pass within the round (cam.div_round_passes)
+__device__ __forceinline__ int64_t round_of(int64_t pass, const camera_params& cam)
+{
+    return pass < (int64_t{1} << 32) ? static_cast<int64_t>(quotient(static_cast<uint32_t>(pass), cam.div_round_passes))
+                                     : pass / static_cast<int64_t>(cam.div_round_passes.d);
+}
+
+// A sample's random-number stream: its pixel, its pass within its round of strata, and the round's key
+// (seed + round * 2^32), as the persistent kernel sets them when it starts the sample
+__device__ __forceinline__ int sample_rng(const sample_place& at, const camera_params& cam, uint64_t seed, sampler& rng)
+{
+    const int width = cam.width;
+    const int64_t round = round_of(at.pass, cam);
+    const int round_pass = static_cast<int>(at.pass - round * static_cast<int64_t>(cam.div_round_passes.d));
+    const uint64_t key = seed + (static_cast<uint64_t>(round) << 32);
+    rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
+    rng.pass = static_cast<uint32_t>(round_pass);
+    rng.pixel = static_cast<uint32_t>(at.y) * static_cast<uint32_t>(width) + static_cast<uint32_t>(at.x);
+    return round_pass;
+}
+
 template <bool QUALITY, bool FLAT, bool FEATURES>
 constexpr int render_min_blocks()
 {
@@ -1936,12 +2004,11 @@ __global__ void __launch_bounds__(render_block, render_min_blocks<QUALITY, FLAT,
                 {
                     break; // no work left for this lane
                 }
-                const int64_t k = static_cast<int64_t>(item / static_cast<unsigned long long>(P.padded_pixels));
-                const int q = static_cast<int>(item % static_cast<unsigned long long>(P.padded_pixels));
-                const int tile = q >> 5;
-                const int l = q & 31;
-                px = (tile % P.tiles_x) * 8 + (l & 7);
-                py = (tile / P.tiles_x) * 4 + (l >> 3);
+                const sample_place at = place_of(static_cast<int64_t>(item), cam, 0);
+                const int64_t k = at.pass; // the item's chunk within the launch
+                const int q = static_cast<int>(static_cast<int64_t>(item) - k * P.padded_pixels);
+                px = at.x;
+                py = at.y;
                 if (px >= cam.width || py >= cam.height)
                 {
                     continue; // a lane of a tile that hangs over the image's edge: nothing to render
@@ -1960,13 +2027,15 @@ __global__ void __launch_bounds__(render_block, render_min_blocks<QUALITY, FLAT,
         if (start)
         {
             // A new sample: pass n is pass n % k^2 of round n / k^2, whose numbers come from seed + round * 2^32
-            const int64_t round = pass / P.round_passes;
+            const int64_t round = round_of(pass, cam);
             const int in_round = static_cast<int>(pass - round * P.round_passes);
             const uint64_t key = P.seed + (static_cast<uint64_t>(round) << 32);
             rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
             rng.pass = static_cast<uint32_t>(in_round);
             const float4 u = rng.draw(0, 0);
-            camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
+            int s_i, s_j;
+            stratum_of(cam, in_round, s_i, s_j);
+            camera_ray(cam, px, py, s_i, s_j, u, ps.o, ps.d);
             // the moment in the shutter, in a scene where something moves (camera.ixx get_ray's ray time)
             ps.time = FEATURES && P.scene.has_motion ? rng.draw(0, block_time).x : 0.0f;
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
@@ -2146,12 +2215,11 @@ __global__ void __launch_bounds__(render_block, render_min_blocks<true, FLAT, FE
                 }
                 J = P.jobs + find_job<job_items>(P.jobs, job_first, job_end, item);
                 const int64_t local = item - J->item_begin;
-                const int64_t k = local / J->padded_pixels;
+                const sample_place at = place_of(local, J->cam, 0);
+                const int64_t k = at.pass; // the item's chunk within the step
                 const int q = static_cast<int>(local - k * J->padded_pixels);
-                const int tile = q >> 5;
-                const int l = q & 31;
-                px = (tile % J->tiles_x) * 8 + (l & 7);
-                py = (tile / J->tiles_x) * 4 + (l >> 3);
+                px = at.x;
+                py = at.y;
                 if (px >= J->cam.width || py >= J->cam.height)
                 {
                     continue;
@@ -2173,13 +2241,15 @@ __global__ void __launch_bounds__(render_block, render_min_blocks<true, FLAT, FE
         const camera_params& cam = J->cam;
         if (start)
         {
-            const int64_t round = pass / J->round_passes;
+            const int64_t round = round_of(pass, cam);
             const int in_round = static_cast<int>(pass - round * J->round_passes);
             const uint64_t key = J->seed + (static_cast<uint64_t>(round) << 32);
             rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
             rng.pass = static_cast<uint32_t>(in_round);
             const float4 u = rng.draw(0, 0);
-            camera_ray(cam, px, py, in_round % cam.sqrt_spp, in_round / cam.sqrt_spp, u, ps.o, ps.d);
+            int s_i, s_j;
+            stratum_of(cam, in_round, s_i, s_j);
+            camera_ray(cam, px, py, s_i, s_j, u, ps.o, ps.d);
             ps.time = FEATURES && J->scene.has_motion ? rng.draw(0, block_time).x : 0.0f;
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
             ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
@@ -2365,36 +2435,6 @@ constexpr int wave_shade_min_blocks()
     return RTB_WAVE_SHADE_MIN_BLOCKS > 0 ? RTB_WAVE_SHADE_MIN_BLOCKS : render_min_blocks<QUALITY, false, FEATURES>();
 }
 
-// Where sample number `local` of a launch (or of a batch job) lies: pass-major, then the pixels in 8x4 tiles (a
-// warp's worth); x may fall past the image's right edge or y past its bottom in the last tiles
-struct sample_place
-{
-    int64_t pass;
-    int x, y;
-};
-
-__device__ __forceinline__ sample_place place_of(int64_t local, int padded, int tiles_x, int64_t pass_begin)
-{
-    const int64_t j = local / padded;
-    const int q = static_cast<int>(local - j * padded);
-    const int tile = q >> 5;
-    const int l = q & 31;
-    return {pass_begin + j, (tile % tiles_x) * 8 + (l & 7), (tile / tiles_x) * 4 + (l >> 3)};
-}
-
-// A sample's random-number stream: its pixel, its pass within its round of strata, and the round's key
-// (seed + round * 2^32), as the persistent kernel sets them when it starts the sample
-__device__ __forceinline__ int sample_rng(const sample_place& at, int width, int round_passes, uint64_t seed,
-                                          sampler& rng)
-{
-    const int64_t round = at.pass / round_passes;
-    const int round_pass = static_cast<int>(at.pass - round * round_passes);
-    const uint64_t key = seed + (static_cast<uint64_t>(round) << 32);
-    rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
-    rng.pass = static_cast<uint32_t>(round_pass);
-    rng.pixel = static_cast<uint32_t>(at.y) * static_cast<uint32_t>(width) + static_cast<uint32_t>(at.x);
-    return round_pass;
-}
 
 // A slot's step: the last walk's answers, the shading, the sample's end, a new sample, the next rays queued.
 // BATCH: the slots render the samples of a group of batch jobs (W), each slot its job's scene, camera and integrator
@@ -2518,10 +2558,8 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             {
                 // the sample's stream, from its number
                 const int64_t local = sample_index + (BATCH ? J->local_begin : 0);
-                const sample_place at = place_of(local, BATCH ? J->padded_pixels : P.padded_pixels,
-                                                 BATCH ? J->tiles_x : P.tiles_x, BATCH ? J->pass_begin : P.pass_begin);
-                sample_rng(at, camera().width, BATCH ? J->round_passes : P.round_passes, BATCH ? J->seed : P.seed,
-                           rng);
+                const sample_place at = place_of(local, camera(), BATCH ? J->pass_begin : P.pass_begin);
+                sample_rng(at, camera(), BATCH ? J->seed : P.seed, rng);
             }
             bool finished = false;
             float3 sample = make_float3(0.0f, 0.0f, 0.0f);
@@ -2677,9 +2715,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
                 atomicOr(B.control + 3, 1u);
                 return false;
             }
-            const sample_place at = place_of(index + (BATCH ? K->local_begin : 0),
-                                             BATCH ? K->padded_pixels : P.padded_pixels, BATCH ? K->tiles_x : P.tiles_x,
-                                             BATCH ? K->pass_begin : P.pass_begin);
+            const sample_place at = place_of(index + (BATCH ? K->local_begin : 0), c, BATCH ? K->pass_begin : P.pass_begin);
             if (!(at.x < c.width && at.y < c.height))
             {
                 if (stream_run)
@@ -2756,8 +2792,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         {
             // A new sample, as the persistent kernel starts one
             const camera_params& cam = camera();
-            round_pass = sample_rng({pass, px, py}, cam.width, BATCH ? J->round_passes : P.round_passes,
-                                    BATCH ? J->seed : P.seed, rng);
+            round_pass = sample_rng({pass, px, py}, cam, BATCH ? J->seed : P.seed, rng);
             // Under a tree walk and the heavier shading (NEE/MIS, the second book's features) the trace kernel makes
             // the camera ray, a warp's 32 at once, instead of this warp for its few new samples: the mesh +3.6%, the
             // second book's final scene +3.7%. The books' plain sphere scenes (-2%) and the flat searches (-3% to
@@ -2766,7 +2801,9 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             if (!primary)
             {
                 const float4 u = rng.draw(0, 0);
-                camera_ray(cam, px, py, round_pass % cam.sqrt_spp, round_pass / cam.sqrt_spp, u, ps.o, ps.d);
+                int s_i, s_j;
+                stratum_of(cam, round_pass, s_i, s_j);
+                camera_ray(cam, px, py, s_i, s_j, u, ps.o, ps.d);
                 ps.time = FEATURES && scene().has_motion ? rng.draw(0, block_time).x : 0.0f;
             }
             ps.throughput = make_float3(1.0f, 1.0f, 1.0f);
@@ -2905,7 +2942,9 @@ __device__ __forceinline__ void wave_camera_query(const wave_buffers& B, const w
         rng.pass = static_cast<uint32_t>(round_pass);
         rng.job = BATCH ? J->job : B.job;
         float3 o, d;
-        camera_ray(cam, px, py, round_pass % cam.sqrt_spp, round_pass / cam.sqrt_spp, rng.draw(0, 0), o, d);
+        int s_i, s_j;
+        stratum_of(cam, round_pass, s_i, s_j);
+        camera_ray(cam, px, py, s_i, s_j, rng.draw(0, 0), o, d);
         const float time = FEATURES && S.has_motion ? rng.draw(0, block_time).x : 0.0f;
         float4* rows = static_cast<float4*>(B.slots);
         stream_store(rows + qm.w, make_float4(o.x, o.y, o.z, time));

@@ -516,6 +516,15 @@ camera_params to_camera(const rt_camera_desc& d)
     c.sky_bottom = to_f3(d.sky_bottom);
     c.sky_top = to_f3(d.sky_top);
     c.sampling = d.sampling;
+    if (d.image_width > 0 && d.image_height > 0 && d.sqrt_spp > 0)
+    {
+        const auto tiles_x = static_cast<uint32_t>((d.image_width + 7) / 8);
+        const auto tiles_y = static_cast<uint32_t>((d.image_height + 3) / 4);
+        c.div_sqrt_spp = make_fast_divisor(static_cast<uint32_t>(d.sqrt_spp));
+        c.div_round_passes = make_fast_divisor(static_cast<uint32_t>(d.sqrt_spp) * static_cast<uint32_t>(d.sqrt_spp));
+        c.div_tiles_x = make_fast_divisor(tiles_x);
+        c.div_padded = make_fast_divisor(tiles_x * tiles_y * 32u);
+    }
     return c;
 }
 
