@@ -607,28 +607,43 @@ rt_server_step_report render_server::step_continuous()
     std::vector<std::pair<const resident_scene*, double>> step_samples;
     std::vector<int64_t> firsts;
     double planned = 0;
-    while (!first_queue_.empty())
+    // The waiting first frames, cheapest first (shortest job first, equal costs in arrival order): a 1080p frame
+    // waits for no 4K frame that arrived before it, only for the cheaper ones and the step in flight
+    std::vector<std::pair<double, int64_t>> waiting;
+    for (const int64_t id : first_queue_)
     {
-        const int64_t id = first_queue_.front();
         const auto it = requests_.find(id);
-        if (it == requests_.end() || it->second.first_handle < 0)
+        if (it != requests_.end() && it->second.first_handle >= 0)
         {
-            first_queue_.pop_front();
-            continue;
+            const request& r = it->second;
+            waiting.emplace_back(double(r.camera.image_width) * r.camera.image_height * cost_of(r.scene.get()), id);
         }
-        request& r = it->second;
-        const double pixels = double(r.camera.image_width) * r.camera.image_height;
-        if (!work.empty() && planned + pixels * cost_of(r.scene.get()) > std::max(first_frame_seconds,
-                                                                                     options_.step_seconds))
+    }
+    std::stable_sort(waiting.begin(), waiting.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (const auto& [cost, id] : waiting)
+    {
+        request& r = requests_.at(id);
+        if (!work.empty() && planned + cost > std::max(first_frame_seconds, options_.step_seconds))
         {
             break;
         }
         work.push_back({r.first_handle, 1});
-        step_samples.emplace_back(r.scene.get(), pixels);
-        planned += pixels * cost_of(r.scene.get());
+        step_samples.emplace_back(r.scene.get(), double(r.camera.image_width) * r.camera.image_height);
+        planned += cost;
         firsts.push_back(id);
-        first_queue_.pop_front();
     }
+    // what stays queued: the frames not taken, in arrival order (entries of requests gone or handed over drop out)
+    std::deque<int64_t> left;
+    for (const int64_t id : first_queue_)
+    {
+        const auto it = requests_.find(id);
+        if (it != requests_.end() && it->second.first_handle >= 0 &&
+            std::find(firsts.begin(), firsts.end(), id) == firsts.end())
+        {
+            left.push_back(id);
+        }
+    }
+    first_queue_.swap(left);
     if (!work.empty())
     {
         const double seconds = engine_->step(std::move(work));
@@ -739,25 +754,32 @@ rt_server_step_report render_server::step()
         queue_.pop_front();
         ++report.admitted;
     }
-    // First frames, in arrival order, while the step's time allows (at least one): a burst of large first frames
+    // First frames, cheapest first (shortest job first, equal costs in arrival order: a 1080p frame waits for no 4K
+    // frame that arrived before it), while the step's time allows (at least one): a burst of large first frames
     // spreads over steps rather than holding up the ones behind it for a long step
     std::vector<batch_engine::assignment> work;
     std::vector<std::pair<const resident_scene*, double>> step_samples; // each job's scene and pixel passes
     double planned = 0;
+    std::vector<std::pair<double, request*>> waiting;
     for (auto& [id, r] : requests_)
     {
         if (r.state == RT_REQUEST_ACTIVE && engine_->passes(r.handle) == 0)
         {
-            const double pixels = double(r.camera.image_width) * r.camera.image_height;
-            if (report.first_frames > 0 && planned + pixels * cost_of(r.scene.get()) > options_.step_seconds)
-            {
-                break;
-            }
-            work.push_back({r.handle, 1});
-            step_samples.emplace_back(r.scene.get(), pixels);
-            planned += pixels * cost_of(r.scene.get());
-            ++report.first_frames;
+            waiting.emplace_back(double(r.camera.image_width) * r.camera.image_height * cost_of(r.scene.get()), &r);
         }
+    }
+    std::stable_sort(waiting.begin(), waiting.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (auto& [cost, rp] : waiting)
+    {
+        request& r = *rp;
+        if (report.first_frames > 0 && planned + cost > options_.step_seconds)
+        {
+            break;
+        }
+        work.push_back({r.handle, 1});
+        step_samples.emplace_back(r.scene.get(), double(r.camera.image_width) * r.camera.image_height);
+        planned += cost;
+        ++report.first_frames;
     }
     // Refinement: the others, least remaining work first (shortest remaining processing time, which minimises the
     // mean time to target), while the step's time allows. A step with first frames carries nothing else: a first
