@@ -1930,13 +1930,12 @@ __device__ __forceinline__ int64_t round_of(int64_t pass, const camera_params& c
 // (seed + round * 2^32), as the persistent kernel sets them when it starts the sample
 __device__ __forceinline__ int sample_rng(const sample_place& at, const camera_params& cam, uint64_t seed, sampler& rng)
 {
-    const int width = cam.width;
     const int64_t round = round_of(at.pass, cam);
     const int round_pass = static_cast<int>(at.pass - round * static_cast<int64_t>(cam.div_round_passes.d));
     const uint64_t key = seed + (static_cast<uint64_t>(round) << 32);
     rng.key = make_uint2(static_cast<uint32_t>(key), static_cast<uint32_t>(key >> 32));
     rng.pass = static_cast<uint32_t>(round_pass);
-    rng.pixel = static_cast<uint32_t>(at.y) * static_cast<uint32_t>(width) + static_cast<uint32_t>(at.x);
+    rng.pixel = static_cast<uint32_t>(at.y) * static_cast<uint32_t>(cam.width) + static_cast<uint32_t>(at.x);
     return round_pass;
 }
 
