@@ -892,7 +892,8 @@ def run_b200(args):
     if not args.no_e2e:
         e2e_steps = max(1, args.steps)
         out = np.empty((scene.height, scene.width, 3), dtype=np.float64)
-        rt.render(scene_desc, seed=seed, passes=passes, launch_seconds=0.5, out=out)  # warm-up
+        for w in range(max(1, args.warmup)):  # warm-up calls, as the timed steps have theirs
+            rt.render(scene_desc, seed=seed + 100 + w, passes=passes, launch_seconds=0.5, out=out)
         e_seconds = 0.0
         e_rays = 0
         e_each = []
