@@ -145,18 +145,34 @@ def read_peaks() -> dict:
 
 
 # The wavefront's state per unit of work, by the layout of its slots and queues (raytracing_b200/csrc/kernels.cu): what
-# the shade kernel must move through HBM for each segment (the slot's five 16-byte rows in and out, the walk's answer,
-# the next query of 48 bytes), for each shadow ray (its answer, its three rows out and back in, its query) and for each
-# sample (its value). These are the bytes that bind the shade kernel: the scene itself (a few KB) is read from L1.
-SHADE_BYTES_PER_SEGMENT = 2 * 5 * 16 + 16 + 48
+# the shade kernel must move through HBM for each segment (the slot's 16-byte rows in and out: five, or four for the
+# books' scenes without the second book's features, whose paths carry no NEE radiance; the walk's answer; the next
+# query of 48 bytes), for each shadow ray (its answer, its three rows out and back in, its query) and for each sample
+# (its value). These are the bytes that bind the shade kernel: the scene itself (a few KB) is read from L1.
+def shade_bytes_per_segment(slot_rows: int) -> int:
+    return 2 * slot_rows * 16 + 16 + 48
+
+
 SHADE_BYTES_PER_SHADOW_RAY = 4 + 2 * 3 * 16 + 48
 SHADE_BYTES_PER_SAMPLE = 16
+
+
+def slot_rows_of(desc, kernel_name: str) -> int:
+    """The rows of a session's wavefront slot: four for a books' scene without moving spheres, textures or smoke
+    (kernels.cu books_slots), five otherwise."""
+    d = desc.contents
+    moving = any(d.spheres[i].displacement.x or d.spheres[i].displacement.y or d.spheres[i].displacement.z
+                 for i in range(d.sphere_count))
+    textured = any(d.materials[i].kind in (0, 3, 4) and d.textures[d.materials[i].texture].kind != 0
+                   for i in range(d.material_count))
+    features = moving or textured or d.medium_count > 0
+    return 4 if kernel_name == "wavefront books" and not features else 5
 # FP32 operations per primitive test and per node visit (slab test: 6 FMA + 6 min/max), the trace kernels' arithmetic
 FLOPS_PER_NODE, FLOPS_PER_SPHERE, FLOPS_PER_QUAD, FLOPS_PER_TRIANGLE = 12, 20, 25, 30
 
 
 def roofline_of(times: dict, counts: dict, samples: int, fetched: dict, counted: int, scene_bytes_per_query: float,
-                peaks: dict, fp32_peak: float, render_seconds: float) -> dict:
+                peaks: dict, fp32_peak: float, render_seconds: float, slot_rows: int = 5) -> dict:
     """The roofline of the render's dominant kernel, from per-kernel CUDA-event times of one render of the workload.
     The wavefront's shade kernel is bound by HBM on the slot state it streams; the trace kernel (and the persistent
     kernel) by FP32 arithmetic on the scene's primitives, which sit in L1."""
@@ -178,7 +194,8 @@ def roofline_of(times: dict, counts: dict, samples: int, fetched: dict, counted:
                 "peak_source": "measured here: FP32 GEMM through cuBLAS, TF32 off"}
 
     if dominant == "shade":
-        state = rays * SHADE_BYTES_PER_SEGMENT + shadow * SHADE_BYTES_PER_SHADOW_RAY + samples * SHADE_BYTES_PER_SAMPLE
+        state = (rays * shade_bytes_per_segment(slot_rows) + shadow * SHADE_BYTES_PER_SHADOW_RAY +
+                 samples * SHADE_BYTES_PER_SAMPLE)
         sec = active["shade"][0]
         achieved = state / sec / 1e9
         out = {"bound": "hbm", "kernel": "wave_shade_kernel", "achieved": achieved, "peak": peaks["hbm_gbs"],
@@ -873,7 +890,8 @@ def run_b200(args):
     peaks = read_peaks()
     fp32_peak = fp32_peak_tflops(torch)
     roofline = roofline_of(kernel_times, prof_counts, passes * scene.width * scene.height, fetched,
-                           segments_counted, bytes_per_segment, peaks, fp32_peak, profiled["gpu_seconds"])
+                           segments_counted, bytes_per_segment, peaks, fp32_peak, profiled["gpu_seconds"],
+                           slot_rows=slot_rows_of(scene_desc.desc, session.kernel()["name"]))
 
     line = None
     if rank == 0:

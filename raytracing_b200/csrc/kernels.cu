@@ -2455,11 +2455,18 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     // has work); once every sample is claimed (the drain) the flags first, and the rest only for a slot with work
     float4 r0, r1, r2, r3;
     int4 r5, answer; // r5: the flags row
+    // The books' plain scenes in a session's launch keep four rows: their paths carry no NEE radiance and no NEE
+    // density, so the direction row's last word holds `from` and the rays left are max_depth - depth; the fourth row
+    // (radiance, from, rays left) is neither read nor written
+    constexpr bool books_slots = !QUALITY && !BATCH && !FEATURES;
     const auto load_rest = [&] {
         r0 = stream_load(rows + own);
         r1 = stream_load(rows + n + own);
         r2 = stream_load(rows + 2 * n + own);
-        r3 = stream_load(rows + 3 * n + own);
+        if constexpr (!books_slots)
+        {
+            r3 = stream_load(rows + 3 * n + own);
+        }
         answer = stream_load(B.ext_result + own);
     };
     if (!B.draining)
@@ -2544,12 +2551,22 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             ps.o = make_float3(r0.x, r0.y, r0.z);
             ps.time = r0.w;
             ps.d = make_float3(r1.x, r1.y, r1.z);
-            ps.bsdf_pdf = r1.w;
             ps.throughput = make_float3(r2.x, r2.y, r2.z);
-            ps.radiance = make_float3(r2.w, r3.x, r3.y);
-            ps.from = __float_as_int(r3.z);
-            ps.rays_left = __float_as_int(r3.w);
             ps.depth = r5.x;
+            if constexpr (books_slots)
+            {
+                ps.bsdf_pdf = 0.0f;
+                ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
+                ps.from = __float_as_int(r1.w);
+                ps.rays_left = camera().max_depth - ps.depth;
+            }
+            else
+            {
+                ps.bsdf_pdf = r1.w;
+                ps.radiance = make_float3(r2.w, r3.x, r3.y);
+                ps.from = __float_as_int(r3.z);
+                ps.rays_left = __float_as_int(r3.w);
+            }
             ps.specular = (flags & wave_specular) != 0u;
             ps.inward = (flags & wave_inward) != 0u;
             sample_index = static_cast<int64_t>(static_cast<uint32_t>(r5.z));
@@ -2903,11 +2920,15 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             else
             {
                 stream_store(rows + i, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time));
-                stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf));
+                stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z,
+                                                       books_slots ? __int_as_float(ps.from) : ps.bsdf_pdf));
                 stream_store(rows + 2 * n + i,
                              make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x));
-                stream_store(rows + 3 * n + i, make_float4(ps.radiance.y, ps.radiance.z, __int_as_float(ps.from),
-                                                           __int_as_float(ps.rays_left)));
+                if constexpr (!books_slots)
+                {
+                    stream_store(rows + 3 * n + i, make_float4(ps.radiance.y, ps.radiance.z, __int_as_float(ps.from),
+                                                               __int_as_float(ps.rays_left)));
+                }
                 stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
                              make_int4(ps.depth, static_cast<int>(flags), static_cast<int>(static_cast<uint32_t>(
                                                                               sample_index)),
