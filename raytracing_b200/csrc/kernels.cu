@@ -2455,16 +2455,32 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     // has work); once every sample is claimed (the drain) the flags first, and the rest only for a slot with work
     float4 r0, r1, r2, r3;
     int4 r5, answer; // r5: the flags row
-    // The books' plain scenes in a session's launch keep four rows: their paths carry no NEE radiance and no NEE
-    // density, so the direction row's last word holds `from` and the rays left are max_depth - depth; the fourth row
-    // (radiance, from, rays left) is neither read nor written
+    // The books' plain scenes in a session's launch keep three rows: their paths carry no NEE radiance or density,
+    // no time (nothing moves) and no job, and use three flags, so a slot is (origin, throughput x), (direction,
+    // throughput y) and the flags row (depth << 3 | ext | exhausted | inward, sample, from, throughput z); the rays
+    // left are max_depth - depth. Rows 2 and 3 are neither read nor written.
     constexpr bool books_slots = !QUALITY && !BATCH && !FEATURES;
+    int books_from = -1;
+    float books_tz = 0.0f;
+    const auto load_flags = [&] {
+        r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + own);
+        if constexpr (books_slots)
+        {
+            // into the five-row form's (depth, flags, sample, job)
+            const auto w = static_cast<uint32_t>(r5.x);
+            books_from = r5.z;
+            books_tz = __int_as_float(r5.w);
+            const uint32_t f = ((w & 1u) ? wave_ext : 0u) | ((w & 2u) ? wave_exhausted : 0u) |
+                               ((w & 4u) ? wave_inward : 0u);
+            r5 = make_int4(static_cast<int>(w >> 3), static_cast<int>(f), r5.y, 0);
+        }
+    };
     const auto load_rest = [&] {
         r0 = stream_load(rows + own);
         r1 = stream_load(rows + n + own);
-        r2 = stream_load(rows + 2 * n + own);
         if constexpr (!books_slots)
         {
+            r2 = stream_load(rows + 2 * n + own);
             r3 = stream_load(rows + 3 * n + own);
         }
         answer = stream_load(B.ext_result + own);
@@ -2472,11 +2488,11 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     if (!B.draining)
     {
         load_rest();
-        r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + own);
+        load_flags();
     }
     else
     {
-        r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + own);
+        load_flags();
         if ((static_cast<uint32_t>(r5.y) & wave_exhausted) == 0u)
         {
             load_rest();
@@ -2551,17 +2567,19 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             ps.o = make_float3(r0.x, r0.y, r0.z);
             ps.time = r0.w;
             ps.d = make_float3(r1.x, r1.y, r1.z);
-            ps.throughput = make_float3(r2.x, r2.y, r2.z);
             ps.depth = r5.x;
             if constexpr (books_slots)
             {
+                ps.time = 0.0f;
+                ps.throughput = make_float3(r0.w, r1.w, books_tz);
                 ps.bsdf_pdf = 0.0f;
                 ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
-                ps.from = __float_as_int(r1.w);
+                ps.from = books_from;
                 ps.rays_left = camera().max_depth - ps.depth;
             }
             else
             {
+                ps.throughput = make_float3(r2.x, r2.y, r2.z);
                 ps.bsdf_pdf = r1.w;
                 ps.radiance = make_float3(r2.w, r3.x, r3.y);
                 ps.from = __float_as_int(r3.z);
@@ -2912,23 +2930,32 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         {
             flags = (flags & ~(wave_specular | wave_inward)) | (ps.specular ? wave_specular : 0u) |
                     (ps.inward ? wave_inward : 0u);
+            // the books' three-row form's flags word (depth << 3 | ext | exhausted | inward)
+            const auto books_word = [&](int depth) {
+                return static_cast<int>((static_cast<uint32_t>(depth) << 3) | ((flags & wave_ext) ? 1u : 0u) |
+                                        ((flags & wave_exhausted) ? 2u : 0u) | ((flags & wave_inward) ? 4u : 0u));
+            };
             if (flags & wave_exhausted)
             {
                 stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
-                             make_int4(0, static_cast<int>(flags), 0, 0));
+                             books_slots ? make_int4(books_word(0), 0, 0, 0) : make_int4(0, static_cast<int>(flags), 0, 0));
+            }
+            else if constexpr (books_slots)
+            {
+                stream_store(rows + i, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.throughput.x));
+                stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z, ps.throughput.y));
+                stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
+                             make_int4(books_word(ps.depth), static_cast<int>(static_cast<uint32_t>(sample_index)),
+                                       ps.from, __float_as_int(ps.throughput.z)));
             }
             else
             {
                 stream_store(rows + i, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.time));
-                stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z,
-                                                       books_slots ? __int_as_float(ps.from) : ps.bsdf_pdf));
+                stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z, ps.bsdf_pdf));
                 stream_store(rows + 2 * n + i,
                              make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.x));
-                if constexpr (!books_slots)
-                {
-                    stream_store(rows + 3 * n + i, make_float4(ps.radiance.y, ps.radiance.z, __int_as_float(ps.from),
-                                                               __int_as_float(ps.rays_left)));
-                }
+                stream_store(rows + 3 * n + i, make_float4(ps.radiance.y, ps.radiance.z, __int_as_float(ps.from),
+                                                           __int_as_float(ps.rays_left)));
                 stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
                              make_int4(ps.depth, static_cast<int>(flags), static_cast<int>(static_cast<uint32_t>(
                                                                               sample_index)),
