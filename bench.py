@@ -145,9 +145,9 @@ def read_peaks() -> dict:
 
 
 # The wavefront's state per unit of work, by the layout of its slots and queues (raytracing_b200/csrc/kernels.cu): what
-# the shade kernel must move through HBM for each segment (the slot's 16-byte rows in and out: five, or three for the
-# books' scenes without the second book's features, whose paths carry no NEE radiance, time or job; the walk's answer;
-# the next query of 48 bytes), for each shadow ray (its answer, its three rows out and back in, its query) and for each sample
+# the shade kernel must move through HBM for each segment (the slot's 16-byte rows in and out: five, or for a scene
+# without the second book's features, whose paths carry no time or job, three for the books' integrator and four for
+# NEE/MIS; the walk's answer; the next query of 48 bytes), for each shadow ray (its answer, its three rows out and back in, its query) and for each sample
 # (its value). These are the bytes that bind the shade kernel: the scene itself (a few KB) is read from L1.
 def shade_bytes_per_segment(slot_rows: int) -> int:
     return 2 * slot_rows * 16 + 16 + 48
@@ -158,15 +158,17 @@ SHADE_BYTES_PER_SAMPLE = 16
 
 
 def slot_rows_of(desc, kernel_name: str) -> int:
-    """The rows of a session's wavefront slot: three for a books' scene without moving spheres, textures or smoke
-    (kernels.cu books_slots), five otherwise."""
+    """The rows of a session's wavefront slot for a scene without moving spheres, textures or smoke (kernels.cu
+    compact_slots): three for the books' integrator, four for NEE/MIS; five otherwise."""
     d = desc.contents
     moving = any(d.spheres[i].displacement.x or d.spheres[i].displacement.y or d.spheres[i].displacement.z
                  for i in range(d.sphere_count))
     textured = any(d.materials[i].kind in (0, 3, 4) and d.textures[d.materials[i].texture].kind != 0
                    for i in range(d.material_count))
     features = moving or textured or d.medium_count > 0
-    return 3 if kernel_name == "wavefront books" and not features else 5
+    if features:
+        return 5
+    return {"wavefront books": 3, "wavefront nee-mis": 4}.get(kernel_name, 5)
 # FP32 operations per primitive test and per node visit (slab test: 6 FMA + 6 min/max), the trace kernels' arithmetic
 FLOPS_PER_NODE, FLOPS_PER_SPHERE, FLOPS_PER_QUAD, FLOPS_PER_TRIANGLE = 12, 20, 25, 30
 

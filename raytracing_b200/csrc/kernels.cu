@@ -2455,24 +2455,29 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
     // has work); once every sample is claimed (the drain) the flags first, and the rest only for a slot with work
     float4 r0, r1, r2, r3;
     int4 r5, answer; // r5: the flags row
-    // The books' plain scenes in a session's launch keep three rows: their paths carry no NEE radiance or density,
-    // no time (nothing moves) and no job, and use three flags, so a slot is (origin, throughput x), (direction,
-    // throughput y) and the flags row (depth << 3 | ext | exhausted | inward, sample, from, throughput z); the rays
-    // left are max_depth - depth. Rows 2 and 3 are neither read nor written.
-    constexpr bool books_slots = !QUALITY && !BATCH && !FEATURES;
-    int books_from = -1;
-    float books_tz = 0.0f;
+    // Compact slots, in a session's launch of a scene without the second book's features (nothing moves, so no time;
+    // no job; the rays left are max_depth - depth): the depth and the six flags in one word of the flags row, which
+    // also holds the sample's number, the primitive left and one more value. The books' paths carry no NEE radiance
+    // or density: three rows, (origin, throughput x), (direction, throughput y), flags row (..., throughput z). The
+    // NEE/MIS paths: four, (origin, NEE density), (direction, radiance r), (throughput, radiance g), flags row (...,
+    // radiance b). A camera ray the trace kernel writes into rows 0 and 1 leaves their last words 0: no density, no
+    // radiance. Row 3 (and for the books row 2) is neither read nor written.
+    constexpr bool compact_slots = !BATCH && !FEATURES;
+    constexpr bool books_slots = compact_slots && !QUALITY;
+    int compact_from = -1;
+    float compact_last = 0.0f; // the flags row's last word: throughput z (books) or radiance b (NEE/MIS)
     const auto load_flags = [&] {
         r5 = stream_load(reinterpret_cast<const int4*>(rows) + wave_flags_row * n + own);
-        if constexpr (books_slots)
+        if constexpr (compact_slots)
         {
             // into the five-row form's (depth, flags, sample, job)
             const auto w = static_cast<uint32_t>(r5.x);
-            books_from = r5.z;
-            books_tz = __int_as_float(r5.w);
+            compact_from = r5.z;
+            compact_last = __int_as_float(r5.w);
             const uint32_t f = ((w & 1u) ? wave_ext : 0u) | ((w & 2u) ? wave_exhausted : 0u) |
-                               ((w & 4u) ? wave_inward : 0u);
-            r5 = make_int4(static_cast<int>(w >> 3), static_cast<int>(f), r5.y, 0);
+                               ((w & 4u) ? wave_inward : 0u) | ((w & 8u) ? wave_specular : 0u) |
+                               ((w & 16u) ? wave_shadow : 0u) | ((w & 32u) ? wave_finish : 0u);
+            r5 = make_int4(static_cast<int>(w >> 6), static_cast<int>(f), r5.y, 0);
         }
     };
     const auto load_rest = [&] {
@@ -2481,6 +2486,9 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         if constexpr (!books_slots)
         {
             r2 = stream_load(rows + 2 * n + own);
+        }
+        if constexpr (!compact_slots)
+        {
             r3 = stream_load(rows + 3 * n + own);
         }
         answer = stream_load(B.ext_result + own);
@@ -2571,10 +2579,19 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
             if constexpr (books_slots)
             {
                 ps.time = 0.0f;
-                ps.throughput = make_float3(r0.w, r1.w, books_tz);
+                ps.throughput = make_float3(r0.w, r1.w, compact_last);
                 ps.bsdf_pdf = 0.0f;
                 ps.radiance = make_float3(0.0f, 0.0f, 0.0f);
-                ps.from = books_from;
+                ps.from = compact_from;
+                ps.rays_left = camera().max_depth - ps.depth;
+            }
+            else if constexpr (compact_slots)
+            {
+                ps.time = 0.0f;
+                ps.bsdf_pdf = r0.w;
+                ps.throughput = make_float3(r2.x, r2.y, r2.z);
+                ps.radiance = make_float3(r1.w, r2.w, compact_last);
+                ps.from = compact_from;
                 ps.rays_left = camera().max_depth - ps.depth;
             }
             else
@@ -2930,23 +2947,36 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         {
             flags = (flags & ~(wave_specular | wave_inward)) | (ps.specular ? wave_specular : 0u) |
                     (ps.inward ? wave_inward : 0u);
-            // the books' three-row form's flags word (depth << 3 | ext | exhausted | inward)
-            const auto books_word = [&](int depth) {
-                return static_cast<int>((static_cast<uint32_t>(depth) << 3) | ((flags & wave_ext) ? 1u : 0u) |
-                                        ((flags & wave_exhausted) ? 2u : 0u) | ((flags & wave_inward) ? 4u : 0u));
+            // the compact forms' flags word: depth << 6 and the six flags
+            const auto compact_word = [&](int depth) {
+                return static_cast<int>((static_cast<uint32_t>(depth) << 6) | ((flags & wave_ext) ? 1u : 0u) |
+                                        ((flags & wave_exhausted) ? 2u : 0u) | ((flags & wave_inward) ? 4u : 0u) |
+                                        ((flags & wave_specular) ? 8u : 0u) | ((flags & wave_shadow) ? 16u : 0u) |
+                                        ((flags & wave_finish) ? 32u : 0u));
             };
             if (flags & wave_exhausted)
             {
                 stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
-                             books_slots ? make_int4(books_word(0), 0, 0, 0) : make_int4(0, static_cast<int>(flags), 0, 0));
+                             compact_slots ? make_int4(compact_word(0), 0, 0, 0)
+                                           : make_int4(0, static_cast<int>(flags), 0, 0));
             }
             else if constexpr (books_slots)
             {
                 stream_store(rows + i, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.throughput.x));
                 stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z, ps.throughput.y));
                 stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
-                             make_int4(books_word(ps.depth), static_cast<int>(static_cast<uint32_t>(sample_index)),
+                             make_int4(compact_word(ps.depth), static_cast<int>(static_cast<uint32_t>(sample_index)),
                                        ps.from, __float_as_int(ps.throughput.z)));
+            }
+            else if constexpr (compact_slots)
+            {
+                stream_store(rows + i, make_float4(ps.o.x, ps.o.y, ps.o.z, ps.bsdf_pdf));
+                stream_store(rows + n + i, make_float4(ps.d.x, ps.d.y, ps.d.z, ps.radiance.x));
+                stream_store(rows + 2 * n + i,
+                             make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.radiance.y));
+                stream_store(reinterpret_cast<int4*>(rows) + wave_flags_row * n + i,
+                             make_int4(compact_word(ps.depth), static_cast<int>(static_cast<uint32_t>(sample_index)),
+                                       ps.from, __float_as_int(ps.radiance.z)));
             }
             else
             {
