@@ -48,7 +48,7 @@ batch_engine::batch_engine(size_t partial_budget_bytes, bool use_graph, bool hig
     work_counter_.allocate(batch_groups);
     header_.allocate(1);
     retain_pool_memory(); // what the jobs free stays in the pool for the next jobs
-    check(cudaMallocHost(reinterpret_cast<void**>(&header_host_), sizeof(batch_header)), "allocating pinned memory");
+    header_host_ = static_cast<batch_header*>(acquire_pinned(sizeof(batch_header)));
 }
 
 batch_engine::~batch_engine()
@@ -59,14 +59,9 @@ batch_engine::~batch_engine()
     table_.release();
     rgba_.release();
     release_graph();
-    if (table_host_)
-    {
-        cudaFreeHost(table_host_);
-    }
-    if (header_host_)
-    {
-        cudaFreeHost(header_host_);
-    }
+    cudaStreamSynchronize(stream_); // no copy from the pinned tables is in flight when they go back to the cache
+    release_pinned(table_host_, capacity_ * sizeof(batch_job));
+    release_pinned(header_host_, sizeof(batch_header));
     if (start_)
     {
         cudaEventDestroy(start_);
@@ -159,13 +154,9 @@ void batch_engine::ensure_capacity(size_t jobs, size_t partial_doubles)
             capacity *= 2;
         }
         table_.allocate_async(capacity, stream_);
-        if (table_host_)
-        {
-            cudaFreeHost(table_host_);
-            table_host_ = nullptr;
-        }
-        check(cudaMallocHost(reinterpret_cast<void**>(&table_host_), capacity * sizeof(batch_job)),
-              "allocating pinned memory");
+        check(cudaStreamSynchronize(stream_), "finishing the batch's copies"); // of the old table, before it is reused
+        release_pinned(table_host_, capacity_ * sizeof(batch_job));
+        table_host_ = static_cast<batch_job*>(acquire_pinned(capacity * sizeof(batch_job)));
         capacity_ = capacity;
         moved = true;
     }

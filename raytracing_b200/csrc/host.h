@@ -213,6 +213,13 @@ environment_tables build_environment(const rt_environment_desc& env);
 // pool): the scratch that comes and goes with renders, views and requests is mapped once, not on every allocation
 void retain_pool_memory();
 
+// Page-locked host memory for what the host writes for kernels or reads back while they run (queue lengths, counters,
+// job tables), from a process-wide cache: a block given back is kept for the next request of its size, never freed,
+// because cudaFreeHost can hold the calling thread for hundreds of milliseconds (measured on the B200: 200-270 ms in
+// some session teardowns, the end of a render() call)
+void* acquire_pinned(size_t bytes);
+void release_pinned(void* block, size_t bytes);
+
 // The wavefront's host side: its buffers, sized to a launch's samples (slots: at most max_slots) and kept for the next,
 // and the loop of steps, in groups of `group` with two groups in flight, until a step queues no ray
 class wave_runner

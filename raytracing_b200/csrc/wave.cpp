@@ -2,6 +2,9 @@
 // and the loop of steps that ends when a step queues no ray.
 #include <algorithm>
 #include <functional>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "host.h"
 
@@ -17,35 +20,65 @@ void retain_pool_memory()
     check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "setting the memory pool");
 }
 
+namespace
+{
+std::mutex pinned_mutex;
+std::map<size_t, std::vector<void*>>& pinned_free()
+{
+    static auto* blocks = new std::map<size_t, std::vector<void*>>(); // lives to the process's end, as the blocks do
+    return *blocks;
+}
+} // namespace
+
+void* acquire_pinned(size_t bytes)
+{
+    {
+        const std::lock_guard<std::mutex> lock(pinned_mutex);
+        auto& list = pinned_free()[bytes];
+        if (!list.empty())
+        {
+            void* block = list.back();
+            list.pop_back();
+            return block;
+        }
+    }
+    void* block = nullptr;
+    check(cudaHostAlloc(&block, bytes, cudaHostAllocDefault), "allocating pinned memory");
+    return block;
+}
+
+void release_pinned(void* block, size_t bytes)
+{
+    if (block)
+    {
+        const std::lock_guard<std::mutex> lock(pinned_mutex);
+        pinned_free()[bytes].push_back(block);
+    }
+}
+
 wave_runner::wave_runner(int max_slots_, int group_) : max_slots(max_slots_), group(group_) { retain_pool_memory(); }
 
 wave_runner::~wave_runner()
 {
+    // the blocks go back to the cache once no copy into them is in flight (each group's readback records done_)
     for (auto& e : done_)
     {
         if (e)
         {
+            cudaEventSynchronize(e);
             cudaEventDestroy(e);
         }
     }
-    if (queued_)
-    {
-        cudaFreeHost(queued_);
-    }
-    if (claimed_)
-    {
-        cudaFreeHost(claimed_);
-    }
+    release_pinned(queued_, 8 * sizeof(unsigned));
+    release_pinned(claimed_, 2 * sizeof(unsigned long long));
 }
 
 wave_buffers wave_runner::setup(int64_t samples, cudaStream_t stream)
 {
     if (!queued_)
     {
-        check(cudaHostAlloc(reinterpret_cast<void**>(&queued_), 8 * sizeof(unsigned), cudaHostAllocDefault),
-              "allocating pinned memory");
-        check(cudaHostAlloc(reinterpret_cast<void**>(&claimed_), 2 * sizeof(unsigned long long), cudaHostAllocDefault),
-              "allocating pinned memory");
+        queued_ = static_cast<unsigned*>(acquire_pinned(8 * sizeof(unsigned)));
+        claimed_ = static_cast<unsigned long long*>(acquire_pinned(2 * sizeof(unsigned long long)));
         for (auto& e : done_)
         {
             check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating a CUDA event");
