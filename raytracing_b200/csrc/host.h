@@ -30,6 +30,12 @@ void check(cudaError_t e, const char* what);
 // Keeps a message for rt_last_error_message() on this thread
 void remember_error(const char* message);
 
+// The library's own stream on the current device (created once per device, non-blocking), from which arrays that
+// belong to no session's or batch's stream (a scene's tables, counters) take their memory: the device's memory pool,
+// which keeps what is freed. A synchronous cudaMalloc / cudaFree pair per array (a scene has about thirty) held the
+// host for hundreds of milliseconds now and then on the B200 machines; the pool maps its memory once.
+cudaStream_t allocation_stream();
+
 // Device memory owned by one object, freed with it
 template <class T>
 class device_array
@@ -40,7 +46,8 @@ public:
     ~device_array() { release(); }
     device_array(const device_array&) = delete;
     device_array& operator=(const device_array&) = delete;
-    device_array(device_array&& o) noexcept : data_(o.data_), count_(o.count_), stream_(o.stream_)
+    device_array(device_array&& o) noexcept
+        : data_(o.data_), count_(o.count_), stream_(o.stream_), device_(o.device_)
     {
         o.data_ = nullptr;
         o.count_ = 0;
@@ -53,18 +60,23 @@ public:
             data_ = o.data_;
             count_ = o.count_;
             stream_ = o.stream_;
+            device_ = o.device_;
             o.data_ = nullptr;
             o.count_ = 0;
         }
         return *this;
     }
 
+    // Usable by any stream of the current device on return (as cudaMalloc's), from the memory pool
     void allocate(size_t count)
     {
         release();
         if (count > 0)
         {
-            check(cudaMalloc(reinterpret_cast<void**>(&data_), count * sizeof(T)), "allocating device memory");
+            const cudaStream_t s = allocation_stream();
+            check(cudaGetDevice(&device_), "querying the device");
+            check(cudaMallocAsync(reinterpret_cast<void**>(&data_), count * sizeof(T), s), "allocating device memory");
+            check(cudaStreamSynchronize(s), "allocating device memory");
         }
         count_ = count;
     }
@@ -100,7 +112,19 @@ public:
             }
             else
             {
-                cudaFree(data_);
+                // as cudaFree: once the array's device has finished every kernel that may read it
+                int current = 0;
+                cudaGetDevice(&current);
+                if (current != device_)
+                {
+                    cudaSetDevice(device_);
+                }
+                cudaDeviceSynchronize();
+                cudaFreeAsync(data_, allocation_stream());
+                if (current != device_)
+                {
+                    cudaSetDevice(current);
+                }
             }
         }
         data_ = nullptr;
@@ -114,7 +138,8 @@ public:
 private:
     T* data_ = nullptr;
     size_t count_ = 0;
-    cudaStream_t stream_ = nullptr; // set when allocated stream-ordered
+    cudaStream_t stream_ = nullptr; // set when allocated stream-ordered on a caller's stream
+    int device_ = 0;                // where allocate() took it
 };
 
 // The display transform (display.cu): the options' check (renderer.cu:1204-1220) and the kernel over an image's sums

@@ -56,6 +56,25 @@ void release_pinned(void* block, size_t bytes)
     }
 }
 
+cudaStream_t allocation_stream()
+{
+    static std::mutex mutex;
+    static auto* streams = new std::map<int, cudaStream_t>(); // one per device, to the process's end
+    int device = 0;
+    check(cudaGetDevice(&device), "querying the device");
+    const std::lock_guard<std::mutex> lock(mutex);
+    const auto it = streams->find(device);
+    if (it != streams->end())
+    {
+        return it->second;
+    }
+    cudaStream_t s = nullptr;
+    check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "creating a CUDA stream");
+    retain_pool_memory();
+    (*streams)[device] = s;
+    return s;
+}
+
 wave_runner::wave_runner(int max_slots_, int group_) : max_slots(max_slots_), group(group_) { retain_pool_memory(); }
 
 wave_runner::~wave_runner()
