@@ -363,15 +363,17 @@ double batch_engine::step(std::vector<assignment> work)
         const bool flat = g == wave_batch_group(true, false) || g == wave_batch_group(true, true);
         const bool features = g == wave_batch_group(flat, true);
         bool wide = true;
+        bool quality = false;
         for (int32_t i = header.group_jobs[g]; i < header.group_jobs[g + 1]; ++i)
         {
             wide = wide && table_host_[i].scene.wide_nodes != nullptr;
+            quality = quality || table_host_[i].quality != 0;
         }
         const wave_buffers b = wave_->setup(group_samples[g], stream_);
         const int64_t steps = wave_->run(
             b, group_depth[g], stream_,
             [&](bool draining) {
-                return launch_wave_batch_step(w, flat, features, wide, b, trace_grid_, stream_, draining);
+                return launch_wave_batch_step(w, flat, features, wide, quality, b, trace_grid_, stream_, draining);
             },
             work_counter_.data() + g);
         check(launch_wave_batch_partials(w, b, stream_), "launching the wavefront's partials");

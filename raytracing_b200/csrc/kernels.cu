@@ -2550,7 +2550,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         const auto quality = [&]() -> bool {
             if constexpr (BATCH)
             {
-                return J->quality != 0;
+                return QUALITY && J->quality != 0; // a group of books' jobs only: no NEE/MIS code
             }
             else
             {
@@ -2870,7 +2870,7 @@ __global__ void __launch_bounds__(render_block, wave_shade_min_blocks<QUALITY ||
         // The slot's queries: one atomic per warp for its next rays and its shadow rays from the bottom of the queue,
         // one for its new samples' camera rays (primary queries) from the top down
         const bool ext = (flags & wave_ext) != 0u && !primary;
-        const bool shadow = (QUALITY || BATCH) && (flags & wave_shadow) != 0u;
+        const bool shadow = QUALITY && (flags & wave_shadow) != 0u;
         const unsigned ext_lanes = __ballot_sync(full_warp, ext);
         const unsigned shadow_lanes = __ballot_sync(full_warp, shadow);
         const unsigned primary_lanes = __ballot_sync(full_warp, primary);
@@ -3829,8 +3829,8 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
     return e;
 }
 
-cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, const wave_buffers& b,
-                                   int trace_grid, cudaStream_t stream, bool draining)
+cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, bool quality,
+                                   const wave_buffers& b, int trace_grid, cudaStream_t stream, bool draining)
 {
     cudaError_t e = cudaMemsetAsync(b.control, 0, 3 * sizeof(unsigned), stream);
     if (e != cudaSuccess)
@@ -3838,7 +3838,8 @@ cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features
         return e;
     }
     const launch_params none{};
-    const auto shade = features ? wave_shade_kernel<false, true, true> : wave_shade_kernel<false, false, true>;
+    const auto shade = quality ? (features ? wave_shade_kernel<true, true, true> : wave_shade_kernel<true, false, true>)
+                               : (features ? wave_shade_kernel<false, true, true> : wave_shade_kernel<false, false, true>);
     wave_buffers bd = b;
     bd.draining = draining ? 1 : 0;
     shade<<<b.slot_count / render_block, render_block, 0, stream>>>(none, bd, w);
@@ -3857,6 +3858,8 @@ cudaError_t preload_wave_batch()
     cudaFuncAttributes a{};
     const void* kernels[] = {reinterpret_cast<const void*>(wave_shade_kernel<false, false, true>),
                              reinterpret_cast<const void*>(wave_shade_kernel<false, true, true>),
+                             reinterpret_cast<const void*>(wave_shade_kernel<true, false, true>),
+                             reinterpret_cast<const void*>(wave_shade_kernel<true, true, true>),
                              reinterpret_cast<const void*>(wave_trace_variant<true>(false, false)),
                              reinterpret_cast<const void*>(wave_trace_variant<true>(false, true)),
                              reinterpret_cast<const void*>(wave_trace_variant<true>(true, false)),

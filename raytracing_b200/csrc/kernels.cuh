@@ -233,10 +233,11 @@ cudaError_t launch_wave_step(const launch_params& p, bool quality, const wave_bu
 cudaError_t launch_wave_reduce(const reduce_params& r, const wave_buffers& b, int64_t pass_begin, int64_t pass_end,
                                int32_t chunk, cudaStream_t stream);
 // The same for a group of batch jobs (flat: the group's scenes are searched flat; features: its kernels compile the
-// second book's features; wide: every job's tree is four wide), and the group's samples into its jobs' chunk
-// partials (then the batch's reduction adds them into the sums)
-cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, const wave_buffers& b,
-                                   int trace_grid, cudaStream_t stream,
+// second book's features; wide: every job's tree is four wide; quality: some job uses the NEE/MIS integrator, which
+// the shade kernel then picks per job, where a group of books' jobs only gets a kernel without that code), and the
+// group's samples into its jobs' chunk partials (then the batch's reduction adds them into the sums)
+cudaError_t launch_wave_batch_step(const wave_batch& w, bool flat, bool features, bool wide, bool quality,
+                                   const wave_buffers& b, int trace_grid, cudaStream_t stream,
                                    bool draining = false);
 cudaError_t launch_wave_batch_partials(const wave_batch& w, const wave_buffers& b, cudaStream_t stream);
 // Loads the batch wavefront's kernels (every variant) now, so that no step pays for loading them

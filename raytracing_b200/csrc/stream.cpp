@@ -425,7 +425,8 @@ cudaGraphExec_t stream_engine::group_graph(int k)
                                     stream_);
     for (int s = 0; s < group_steps_ && e == cudaSuccess; ++s)
     {
-        e = launch_wave_batch_step(w, false, features_, wide_, buffers_, trace_grid_, stream_, false);
+        // requests of either integrator share the pool: the kernel that picks it per request
+        e = launch_wave_batch_step(w, false, features_, wide_, true, buffers_, trace_grid_, stream_, false);
     }
     if (e == cudaSuccess)
     {
