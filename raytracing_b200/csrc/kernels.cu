@@ -2437,7 +2437,9 @@ constexpr int wave_shade_min_blocks()
 
 // A slot's step: the last walk's answers, the shading, the sample's end, a new sample, the next rays queued.
 // BATCH: the slots render the samples of a group of batch jobs (W), each slot its job's scene, camera and integrator
-// (QUALITY is then the job's own); otherwise the launch's one view (P).
+// (with QUALITY each job's own, picked at run time; without, a group of books' jobs only, compiled without the NEE/MIS
+// code); otherwise the launch's one view (P). A batch kernel keeps the NEE/MIS kernels' register budget either way:
+// at the books' tighter one its per-job loads spill.
 // Every load of the slot's rows and answer is issued at the start, before any of them is needed, so the step waits
 // for one round trip to memory, not one for the flags and another for what they say to read.
 template <bool QUALITY, bool FEATURES, bool BATCH>
