@@ -334,6 +334,15 @@ def config_errors(rt, seed: int) -> dict:
     return out
 
 
+def row_band(height: int, threads: int, per_thread: int) -> tuple[int, int]:
+    """(first row, rows) of the CPU legs' band of rows about the image's middle: `per_thread` rows a thread where the
+    image has them, and always a whole number of rows a thread when the image has at least one a thread (rows are the
+    unit of threading, so no thread idles in the last round)."""
+    per_thread = max(1, per_thread)
+    rows = threads * min(per_thread, height // threads) if height >= threads else height
+    return max(0, height // 2 - rows // 2), rows
+
+
 def cpu_baseline(scene, args, threads: int) -> dict:
     """The reference's CPU renderer (restated as the oracle) on a bounded band of rows of the same workload."""
     from oracle import binding as oracle
@@ -344,8 +353,7 @@ def cpu_baseline(scene, args, threads: int) -> dict:
     # threads
     _, probe = oracle.render(scene.desc, scene.width, h, seed=11, passes=args.spp, threads=threads,
                              row_begin=mid, row_end=mid + 1)
-    rows = int(min(h, threads * max(1, int(args.cpu_seconds / max(probe["seconds"], 1e-3)))))
-    begin = max(0, mid - rows // 2)
+    begin, rows = row_band(h, threads, int(args.cpu_seconds / max(probe["seconds"], 1e-3)))
     _, stats = oracle.render(scene.desc, scene.width, h, seed=12, passes=args.spp, threads=threads,
                              row_begin=begin, row_end=begin + rows)
     value = stats["rays"] / stats["seconds"]
@@ -774,10 +782,7 @@ def run_reference(args):
                              row_end=mid + 1)
     # Each step is a band of rows of about 2 s on all threads (one row per thread at a time), so that warm-up +
     # steps end within a few minutes
-    # A whole number of rows per thread (rows are the unit of threading), so no thread idles in the last round
-    per_thread = max(1, int(2.0 / max(probe["seconds"], 1e-3)))
-    rows = int(min(h, threads * per_thread))
-    begin = max(0, mid - rows // 2)
+    begin, rows = row_band(h, threads, int(2.0 / max(probe["seconds"], 1e-3)))
     for w in range(args.warmup):
         oracle.render(scene.desc, scene.width, h, seed=100 + w, passes=args.spp, threads=threads, row_begin=begin,
                       row_end=begin + rows)
