@@ -145,8 +145,45 @@ private:
         return leaf_link(start, end - begin, kind);
     }
 
-    // Returns the subtree's link: an inner node's index, or a leaf
-    int32_t build(int begin, int end, int depth, box& bounds)
+    // ceil(log2(n)) for n >= 1
+    static int ceil_log2(int n)
+    {
+        int levels = 0;
+        while ((int64_t{1} << levels) < n)
+        {
+            ++levels;
+        }
+        return levels;
+    }
+
+    // The object median on the longest axis of the centroids' box (the reference's only split, bvh.ixx:53-73 and
+    // bvh.cuh:425-432, there on where the boxes start): the range sorted by (centroid, index), a total order, so the
+    // tree does not depend on the sort's implementation, and cut in the middle
+    int median_split(int begin, int end, const box& centroids)
+    {
+        int axis = 0;
+        for (int a = 1; a < 3; ++a)
+        {
+            if (centroids.hi[a] - centroids.lo[a] > centroids.hi[axis] - centroids.lo[axis])
+            {
+                axis = a;
+            }
+        }
+        std::sort(index_.begin() + begin, index_.begin() + end, [&](int32_t p, int32_t q) {
+            const double cp = centroid_[3 * static_cast<size_t>(p) + static_cast<size_t>(axis)];
+            const double cq = centroid_[3 * static_cast<size_t>(q) + static_cast<size_t>(axis)];
+            return cp < cq || (cp == cq && p < q);
+        });
+        return begin + (end - begin) / 2;
+    }
+
+    // Returns the subtree's link: an inner node's index, or a leaf. `median`: the subtree is cut at object medians.
+    // The SAH can peel one primitive a level off some inputs (centroids spaced geometrically: 400 spheres at 1.5^i
+    // make a chain deeper than the traversal stack), so a subtree whose median cuts would only just fit the stack
+    // from here takes them all the way down: halving n primitives takes ceil(log2 n) levels and a leaf-sized range of
+    // two or three kinds at most two more, so no leaf lies deeper than max_bvh_depth. Trees of the usual scenes (the
+    // 1.31M-triangle mesh is 24 levels deep) never come near that point and are pure SAH.
+    int32_t build(int begin, int end, int depth, box& bounds, bool median = false)
     {
         bounds = box{};
         box centroids;
@@ -168,6 +205,7 @@ private:
         }
 
         int split = -1;
+        median = median || depth + ceil_log2(n) + 2 >= max_bvh_depth;
         if (!one_kind && n <= max_leaf)
         {
             // Few enough for one leaf but of several kinds: split off the first kind (stable, as bvh.cuh:404-410)
@@ -175,6 +213,14 @@ private:
                 return prims_[static_cast<size_t>(p)].kind == first_kind;
             });
             split = static_cast<int>(middle - index_.begin());
+        }
+        else if (median)
+        {
+            if (one_kind && n <= max_leaf)
+            {
+                return make_leaf(begin, end);
+            }
+            split = median_split(begin, end, centroids);
         }
         else
         {
@@ -265,8 +311,8 @@ private:
         out_.nodes.push_back(bvh_node{});
         box left_box;
         box right_box;
-        const int32_t left = build(begin, split, depth + 1, left_box);
-        const int32_t right = build(split, end, depth + 1, right_box);
+        const int32_t left = build(begin, split, depth + 1, left_box, median);
+        const int32_t right = build(split, end, depth + 1, right_box, median);
         bvh_node& node = out_.nodes[static_cast<size_t>(index)];
         set_child(node, 0, left, left_box);
         set_child(node, 1, right, right_box);
