@@ -947,8 +947,12 @@ def run_b200(args):
                            "path": "raytracing_b200.render -> rt_render (validate, BVH build, upload, launches, "
                                    "download of width*height*3 doubles)"}
 
+    # The other workloads' legs (NEE/MIS, the FP64 errors, the mesh, the served streams, the CPU baseline) run on rank 0
+    # of a one-GPU run only: under torchrun they would hold the other ranks' GPUs idle in the closing barrier for
+    # minutes, and the scaled metric is the image's alone
+    single = world == 1
     mis = mis_image = mis_desc = None
-    if rank == 0 and not args.no_mis:
+    if rank == 0 and single and not args.no_mis:
         mis, mis_image, mis_desc, mis_passes = mis_measurement(rt, torch, args, max(1, min(args.steps, 3)), seed)
         line["nee_mis"] = mis
 
@@ -978,15 +982,15 @@ def run_b200(args):
                                                                mis_image, seeds=(8, 9)),
                     "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": mis_image,
                                                                 "reference_gpu": mis_ref})}
-    if rank == 0 and not args.no_reference_gpu:
+    if rank == 0 and single and not args.no_reference_gpu:
         line["error_vs_fp64_by_config"] = config_errors(rt, seed)
-    if rank == 0 and not args.no_mesh:
+    if rank == 0 and single and not args.no_mesh:
         line["mesh"] = mesh_measurement(rt, torch, peaks)
     if not args.no_batched:
         batched = batched_measurement(rt, torch, rank, world)  # every rank: its share of the 64 jobs
         if rank == 0:
             line["batched"] = batched
-    if rank == 0 and not args.no_served:
+    if rank == 0 and single and not args.no_served:
         line["served"] = served_measurement(rt, torch, args)
         if args.served_long_window > 0:
             line["served"]["long_stream"] = served_first_frames(rt, args)
@@ -996,8 +1000,11 @@ def run_b200(args):
                                              "reached_target", "time_to_target_p50_s", "gpu_s", "wall_s", "steps",
                                              "longest_steps")}
 
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and single and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene_desc, args, os.cpu_count() or 1)
+    if rank == 0 and not single:
+        line["single_gpu_legs"] = "nee_mis, error_vs_fp64_by_config, mesh, served and cpu_baseline are measured in the " \
+                                  "one-GPU run"
 
     if rank == 0:
         print(json.dumps(line), flush=True)
