@@ -5,9 +5,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <future>
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <thread>
 
 namespace rtb
 {
@@ -26,6 +28,9 @@ float round_up(double x)
 namespace
 {
 constexpr double inf = std::numeric_limits<double>::infinity();
+constexpr int max_bins = 256;
+// Ranges of at least this many primitives split their two subtrees across threads
+constexpr int parallel_min = 1 << 14;
 
 struct box
 {
@@ -39,12 +44,12 @@ struct box
             hi[a] = std::max(hi[a], b.hi[a]);
         }
     }
-    void grow(const double* p)
+    void grow(const double* l, const double* h)
     {
         for (int a = 0; a < 3; ++a)
         {
-            lo[a] = std::min(lo[a], p[a]);
-            hi[a] = std::max(hi[a], p[a]);
+            lo[a] = std::min(lo[a], l[a]);
+            hi[a] = std::max(hi[a], h[a]);
         }
     }
     double area() const
@@ -56,32 +61,166 @@ struct box
     }
 };
 
-class builder
+// A primitive as the builder moves it: its box, centroid, kind and source index in one 80-byte record, so that the
+// passes over a range read memory in order and a partition moves the records themselves
+struct item
 {
-public:
-    builder(std::vector<build_prim>& prims, const bvh_options& options, bvh_result& out)
-        : prims_(prims), options_(options), out_(out), index_(prims.size()), centroid_(prims.size() * 3),
-          bin_of_(prims.size())
+    double lo[3];
+    double hi[3];
+    double c[3];
+    int32_t kind;
+    int32_t source;
+};
+
+// A subtree built on its own: nodes numbered from 0 and each kind's leaf order from 0, spliced into its parent's
+// arrays where a depth-first build would have written it
+struct fragment
+{
+    std::vector<bvh_node> nodes;
+    std::vector<int32_t> order[3];
+    int32_t depth = 0;
+    int64_t leaves = 0;
+};
+
+// The SAH's best binned split of a range: axis and last bin of the left side (axis -1: none), and its cost
+struct sah_split
+{
+    int axis = -1;
+    int bin = -1;
+    double cost = inf;
+};
+
+inline int bin_of(double c, double lo, double scale, int bins)
+{
+    return std::min(bins - 1, static_cast<int>((c - lo) * scale));
+}
+
+// Every axis with a nonzero centroid extent binned in one pass over the range; the cost sweeps as before, axis by
+// axis and bin by bin, the first strictly cheapest split winning
+sah_split choose_sah_split(const item* first, int n, const box& centroids, int bins)
+{
+    // Only the `bins` entries of an axis in use are set up (small ranges, most of a tree, would pay more for clearing
+    // every bin than for binning)
+    struct bin
     {
-        for (size_t i = 0; i < prims.size(); ++i)
+        double lo[3], hi[3];
+        int count;
+    };
+    bin bin_box[3][max_bins];
+    double scale[3] = {0, 0, 0};
+    bool binned[3] = {false, false, false};
+    for (int axis = 0; axis < 3; ++axis)
+    {
+        const double extent = centroids.hi[axis] - centroids.lo[axis];
+        if (extent > 0)
         {
-            index_[i] = static_cast<int32_t>(i);
-            for (int a = 0; a < 3; ++a)
+            binned[axis] = true;
+            scale[axis] = bins / extent;
+            for (int b = 0; b < bins; ++b)
             {
-                centroid_[3 * i + a] = 0.5 * (prims[i].lo[a] + prims[i].hi[a]);
+                bin_box[axis][b] = {{inf, inf, inf}, {-inf, -inf, -inf}, 0};
             }
         }
     }
-
-    void run()
+    for (int i = 0; i < n; ++i)
     {
-        const int n = static_cast<int>(prims_.size());
+        const item& it = first[i];
+        for (int axis = 0; axis < 3; ++axis)
+        {
+            if (binned[axis])
+            {
+                bin& into = bin_box[axis][bin_of(it.c[axis], centroids.lo[axis], scale[axis], bins)];
+                for (int a = 0; a < 3; ++a)
+                {
+                    into.lo[a] = std::min(into.lo[a], it.lo[a]);
+                    into.hi[a] = std::max(into.hi[a], it.hi[a]);
+                }
+                ++into.count;
+            }
+        }
+    }
+    sah_split best;
+    double right_area[max_bins];
+    int right_count[max_bins];
+    for (int axis = 0; axis < 3; ++axis)
+    {
+        if (!binned[axis])
+        {
+            continue;
+        }
+        box acc;
+        int count = 0;
+        for (int b = bins - 1; b > 0; --b)
+        {
+            acc.grow(bin_box[axis][b].lo, bin_box[axis][b].hi);
+            count += bin_box[axis][b].count;
+            right_area[b] = acc.area();
+            right_count[b] = count;
+        }
+        acc = box{};
+        count = 0;
+        for (int b = 0; b < bins - 1; ++b)
+        {
+            acc.grow(bin_box[axis][b].lo, bin_box[axis][b].hi);
+            count += bin_box[axis][b].count;
+            const int rc = right_count[b + 1];
+            if (count == 0 || rc == 0)
+            {
+                continue;
+            }
+            const double cost = acc.area() * count + right_area[b + 1] * rc;
+            if (cost < best.cost)
+            {
+                best = {axis, b, cost};
+            }
+        }
+    }
+    return best;
+}
+
+class builder
+{
+public:
+    builder(const std::vector<build_prim>& prims, const bvh_options& options) : options_(options), items_(prims.size())
+    {
+        for (size_t i = 0; i < prims.size(); ++i)
+        {
+            item& it = items_[i];
+            for (int a = 0; a < 3; ++a)
+            {
+                it.lo[a] = prims[i].lo[a];
+                it.hi[a] = prims[i].hi[a];
+                it.c[a] = 0.5 * (prims[i].lo[a] + prims[i].hi[a]);
+            }
+            it.kind = prims[i].kind;
+            it.source = prims[i].source;
+        }
+        // Threads for the subtrees: each split of a large range hands one side to a new thread, to this depth
+        const unsigned threads = options.threads > 0 ? static_cast<unsigned>(options.threads)
+                                                     : std::max(1u, std::thread::hardware_concurrency());
+        while ((1u << spawn_levels_) < std::min(threads, 64u))
+        {
+            ++spawn_levels_;
+        }
+    }
+
+    void run(bvh_result& out)
+    {
+        const int n = static_cast<int>(items_.size());
         if (n == 0)
         {
             return;
         }
         box bounds;
-        const int32_t root = build(0, n, 1, bounds);
+        fragment tree;
+        const int32_t root = build(0, n, 1, bounds, false, tree, spawn_levels_);
+        out.nodes = std::move(tree.nodes);
+        for (int k = 0; k < 3; ++k)
+        {
+            out.order[k] = std::move(tree.order[k]);
+        }
+        out.depth = tree.depth;
+        out.leaves = tree.leaves;
         if (root < 0)
         {
             // A scene that is one leaf: a root node whose second child is the empty leaf, boxed at +infinity so that
@@ -94,17 +233,14 @@ public:
                 far.lo[a] = far.hi[a] = inf;
             }
             set_child(node, 1, leaf_link(0, 0, 0), far);
-            out_.nodes.insert(out_.nodes.begin(), node);
+            out.nodes.insert(out.nodes.begin(), node);
         }
     }
 
 private:
-    std::vector<build_prim>& prims_;
     const bvh_options& options_;
-    bvh_result& out_;
-    std::vector<int32_t> index_;
-    std::vector<double> centroid_;
-    std::vector<int32_t> bin_of_;
+    std::vector<item> items_;
+    int spawn_levels_ = 0;
 
     static void set_child(bvh_node& node, int c, int32_t link, const box& b)
     {
@@ -117,32 +253,62 @@ private:
         node.link[c] = link;
     }
 
-    box prim_box(int32_t i) const
+    static void check_leaf_start(size_t start)
     {
-        box b;
-        for (int a = 0; a < 3; ++a)
-        {
-            b.lo[a] = prims_[static_cast<size_t>(i)].lo[a];
-            b.hi[a] = prims_[static_cast<size_t>(i)].hi[a];
-        }
-        return b;
-    }
-
-    int32_t make_leaf(int begin, int end)
-    {
-        const int32_t kind = prims_[static_cast<size_t>(index_[static_cast<size_t>(begin)])].kind;
-        std::vector<int32_t>& order = out_.order[kind];
-        const auto start = static_cast<int32_t>(order.size());
-        if (start >= (1 << (31 - leaf_start_shift)))
+        if (start >= (size_t{1} << (31 - leaf_start_shift)))
         {
             throw std::runtime_error("too many primitives of one kind for the leaf encoding (2^26)");
         }
+    }
+
+    int32_t make_leaf(int begin, int end, fragment& out) const
+    {
+        const int32_t kind = items_[static_cast<size_t>(begin)].kind;
+        std::vector<int32_t>& order = out.order[kind];
+        const size_t start = order.size();
+        check_leaf_start(start);
         for (int i = begin; i < end; ++i)
         {
-            order.push_back(prims_[static_cast<size_t>(index_[static_cast<size_t>(i)])].source);
+            order.push_back(items_[static_cast<size_t>(i)].source);
         }
-        ++out_.leaves;
-        return leaf_link(start, end - begin, kind);
+        ++out.leaves;
+        return leaf_link(static_cast<int32_t>(start), end - begin, kind);
+    }
+
+    // `f` (a subtree built on its own, whose root is `link`) appended to `out`: its nodes after out's, its leaves after
+    // out's leaves of each kind; returns the root's link in out's numbering
+    static int32_t splice(fragment& out, const fragment& f, int32_t link)
+    {
+        const auto base = static_cast<int32_t>(out.nodes.size());
+        size_t offset[3];
+        for (int k = 0; k < 3; ++k)
+        {
+            offset[k] = out.order[k].size();
+        }
+        const auto moved = [&](int32_t l) {
+            if (l >= 0)
+            {
+                return l + base;
+            }
+            const int32_t kind = leaf_kind(l);
+            const size_t start = static_cast<size_t>(leaf_start(l)) + offset[kind];
+            check_leaf_start(start);
+            return leaf_link(static_cast<int32_t>(start), leaf_count(l), kind);
+        };
+        out.nodes.reserve(out.nodes.size() + f.nodes.size());
+        for (bvh_node node : f.nodes)
+        {
+            node.link[0] = moved(node.link[0]);
+            node.link[1] = moved(node.link[1]);
+            out.nodes.push_back(node);
+        }
+        for (int k = 0; k < 3; ++k)
+        {
+            out.order[k].insert(out.order[k].end(), f.order[k].begin(), f.order[k].end());
+        }
+        out.depth = std::max(out.depth, f.depth);
+        out.leaves += f.leaves;
+        return moved(link);
     }
 
     // ceil(log2(n)) for n >= 1
@@ -157,8 +323,8 @@ private:
     }
 
     // The object median on the longest axis of the centroids' box (the reference's only split, bvh.ixx:53-73 and
-    // bvh.cuh:425-432, there on where the boxes start): the range sorted by (centroid, index), a total order, so the
-    // tree does not depend on the sort's implementation, and cut in the middle
+    // bvh.cuh:425-432, there on where the boxes start): the range sorted by (centroid, kind, source), a total order,
+    // so the tree does not depend on the sort's implementation, and cut in the middle
     int median_split(int begin, int end, const box& centroids)
     {
         int axis = 0;
@@ -169,39 +335,42 @@ private:
                 axis = a;
             }
         }
-        std::sort(index_.begin() + begin, index_.begin() + end, [&](int32_t p, int32_t q) {
-            const double cp = centroid_[3 * static_cast<size_t>(p) + static_cast<size_t>(axis)];
-            const double cq = centroid_[3 * static_cast<size_t>(q) + static_cast<size_t>(axis)];
-            return cp < cq || (cp == cq && p < q);
+        std::sort(items_.begin() + begin, items_.begin() + end, [axis](const item& p, const item& q) {
+            if (p.c[axis] != q.c[axis])
+            {
+                return p.c[axis] < q.c[axis];
+            }
+            return p.kind != q.kind ? p.kind < q.kind : p.source < q.source;
         });
         return begin + (end - begin) / 2;
     }
 
-    // Returns the subtree's link: an inner node's index, or a leaf. `median`: the subtree is cut at object medians.
-    // The SAH can peel one primitive a level off some inputs (centroids spaced geometrically: 400 spheres at 1.5^i
-    // make a chain deeper than the traversal stack), so a subtree whose median cuts would only just fit the stack
-    // from here takes them all the way down: halving n primitives takes ceil(log2 n) levels and a leaf-sized range of
-    // two or three kinds at most two more, so no leaf lies deeper than max_bvh_depth. Trees of the usual scenes (the
-    // 1.31M-triangle mesh is 24 levels deep) never come near that point and are pure SAH.
-    int32_t build(int begin, int end, int depth, box& bounds, bool median = false)
+    // Returns the subtree's link in `out`: an inner node's index, or a leaf. `median`: the subtree is cut at object
+    // medians. The SAH can peel one primitive a level off some inputs (centroids spaced geometrically: 400 spheres at
+    // 1.5^i make a chain deeper than the traversal stack), so a subtree whose median cuts would only just fit the
+    // stack from here takes them all the way down: halving n primitives takes ceil(log2 n) levels and a leaf-sized
+    // range of two or three kinds at most two more, so no leaf lies deeper than max_bvh_depth. Trees of the usual
+    // scenes (the 1.31M-triangle mesh is 24 levels deep) never come near that point and are pure SAH. `spawn`: levels
+    // below this one that may still hand a subtree to a new thread; the tree is the same whichever threads build it.
+    int32_t build(int begin, int end, int depth, box& bounds, bool median, fragment& out, int spawn)
     {
         bounds = box{};
         box centroids;
         bool one_kind = true;
-        const int32_t first_kind = prims_[static_cast<size_t>(index_[static_cast<size_t>(begin)])].kind;
+        const int32_t first_kind = items_[static_cast<size_t>(begin)].kind;
         for (int i = begin; i < end; ++i)
         {
-            const int32_t p = index_[static_cast<size_t>(i)];
-            bounds.grow(prim_box(p));
-            centroids.grow(&centroid_[3 * static_cast<size_t>(p)]);
-            one_kind = one_kind && prims_[static_cast<size_t>(p)].kind == first_kind;
+            const item& it = items_[static_cast<size_t>(i)];
+            bounds.grow(it.lo, it.hi);
+            centroids.grow(it.c, it.c);
+            one_kind = one_kind && it.kind == first_kind;
         }
-        out_.depth = std::max(out_.depth, depth);
+        out.depth = std::max(out.depth, depth);
         const int n = end - begin;
         const int max_leaf = std::clamp(options_.max_leaf_size, 1, max_leaf_size);
         if (n == 1)
         {
-            return make_leaf(begin, end);
+            return make_leaf(begin, end, out);
         }
 
         int split = -1;
@@ -209,92 +378,38 @@ private:
         if (!one_kind && n <= max_leaf)
         {
             // Few enough for one leaf but of several kinds: split off the first kind (stable, as bvh.cuh:404-410)
-            auto middle = std::stable_partition(index_.begin() + begin, index_.begin() + end, [&](int32_t p) {
-                return prims_[static_cast<size_t>(p)].kind == first_kind;
-            });
-            split = static_cast<int>(middle - index_.begin());
+            auto middle = std::stable_partition(items_.begin() + begin, items_.begin() + end,
+                                                [&](const item& it) { return it.kind == first_kind; });
+            split = static_cast<int>(middle - items_.begin());
         }
         else if (median)
         {
             if (one_kind && n <= max_leaf)
             {
-                return make_leaf(begin, end);
+                return make_leaf(begin, end, out);
             }
             split = median_split(begin, end, centroids);
         }
         else
         {
-            double best_cost = inf;
-            int best_axis = -1;
-            int best_bin = -1;
-            const int bins = std::clamp(options_.bins, 2, 256);
-            std::vector<box> bin_box(static_cast<size_t>(bins));
-            std::vector<int> bin_count(static_cast<size_t>(bins));
-            std::vector<double> right_area(static_cast<size_t>(bins));
-            std::vector<int> right_count(static_cast<size_t>(bins));
-            for (int axis = 0; axis < 3; ++axis)
-            {
-                const double lo = centroids.lo[axis];
-                const double extent = centroids.hi[axis] - lo;
-                if (!(extent > 0))
-                {
-                    continue;
-                }
-                std::fill(bin_box.begin(), bin_box.end(), box{});
-                std::fill(bin_count.begin(), bin_count.end(), 0);
-                const double scale = bins / extent;
-                for (int i = begin; i < end; ++i)
-                {
-                    const int32_t p = index_[static_cast<size_t>(i)];
-                    const int b = std::min(bins - 1, static_cast<int>((centroid_[3 * static_cast<size_t>(p) + axis] - lo) * scale));
-                    bin_box[static_cast<size_t>(b)].grow(prim_box(p));
-                    ++bin_count[static_cast<size_t>(b)];
-                }
-                box acc;
-                int count = 0;
-                for (int b = bins - 1; b > 0; --b)
-                {
-                    acc.grow(bin_box[static_cast<size_t>(b)]);
-                    count += bin_count[static_cast<size_t>(b)];
-                    right_area[static_cast<size_t>(b)] = acc.area();
-                    right_count[static_cast<size_t>(b)] = count;
-                }
-                acc = box{};
-                count = 0;
-                for (int b = 0; b < bins - 1; ++b)
-                {
-                    acc.grow(bin_box[static_cast<size_t>(b)]);
-                    count += bin_count[static_cast<size_t>(b)];
-                    const int rc = right_count[static_cast<size_t>(b + 1)];
-                    if (count == 0 || rc == 0)
-                    {
-                        continue;
-                    }
-                    const double cost = acc.area() * count + right_area[static_cast<size_t>(b + 1)] * rc;
-                    if (cost < best_cost)
-                    {
-                        best_cost = cost;
-                        best_axis = axis;
-                        best_bin = b;
-                    }
-                }
-            }
+            const int bins = std::clamp(options_.bins, 2, max_bins);
+            const sah_split best = choose_sah_split(items_.data() + begin, n, centroids, bins);
             const double parent_area = bounds.area();
             const double split_cost =
-                best_axis >= 0 && parent_area > 0 ? options_.node_cost + best_cost / parent_area : inf;
+                best.axis >= 0 && parent_area > 0 ? options_.node_cost + best.cost / parent_area : inf;
             if (one_kind && n <= max_leaf && static_cast<double>(n) <= split_cost)
             {
-                return make_leaf(begin, end);
+                return make_leaf(begin, end, out);
             }
-            if (best_axis >= 0)
+            if (best.axis >= 0)
             {
-                const double lo = centroids.lo[best_axis];
-                const double scale = bins / (centroids.hi[best_axis] - lo);
-                auto middle = std::partition(index_.begin() + begin, index_.begin() + end, [&](int32_t p) {
-                    const int b = std::min(bins - 1, static_cast<int>((centroid_[3 * static_cast<size_t>(p) + best_axis] - lo) * scale));
-                    return b <= best_bin;
+                const int axis = best.axis;
+                const double lo = centroids.lo[axis];
+                const double scale = bins / (centroids.hi[axis] - lo);
+                auto middle = std::partition(items_.begin() + begin, items_.begin() + end, [&](const item& it) {
+                    return bin_of(it.c[axis], lo, scale, bins) <= best.bin;
                 });
-                split = static_cast<int>(middle - index_.begin());
+                split = static_cast<int>(middle - items_.begin());
             }
             if (split <= begin || split >= end)
             {
@@ -307,13 +422,41 @@ private:
             throw std::runtime_error("the BVH is deeper than the traversal stack (" + std::to_string(max_bvh_depth) +
                                      " levels)");
         }
-        const auto index = static_cast<int32_t>(out_.nodes.size());
-        out_.nodes.push_back(bvh_node{});
+        const auto index = static_cast<int32_t>(out.nodes.size());
+        out.nodes.push_back(bvh_node{});
         box left_box;
         box right_box;
-        const int32_t left = build(begin, split, depth + 1, left_box, median);
-        const int32_t right = build(split, end, depth + 1, right_box, median);
-        bvh_node& node = out_.nodes[static_cast<size_t>(index)];
+        int32_t left = 0;
+        int32_t right = 0;
+        if (spawn > 0 && n >= parallel_min)
+        {
+            // The left subtree on another thread, the right on this one, each into a fragment of its own, spliced in
+            // the depth-first order: the same nodes, links and leaf order as one thread's build
+            fragment left_part;
+            fragment right_part;
+            auto pending = std::async(std::launch::async, [&] {
+                return build(begin, split, depth + 1, left_box, median, left_part, spawn - 1);
+            });
+            int32_t right_root = 0;
+            try
+            {
+                right_root = build(split, end, depth + 1, right_box, median, right_part, spawn - 1);
+            }
+            catch (...)
+            {
+                pending.wait();
+                throw;
+            }
+            const int32_t left_root = pending.get();
+            left = splice(out, left_part, left_root);
+            right = splice(out, right_part, right_root);
+        }
+        else
+        {
+            left = build(begin, split, depth + 1, left_box, median, out, spawn);
+            right = build(split, end, depth + 1, right_box, median, out, spawn);
+        }
+        bvh_node& node = out.nodes[static_cast<size_t>(index)];
         set_child(node, 0, left, left_box);
         set_child(node, 1, right, right_box);
         return index;
@@ -324,10 +467,13 @@ private:
 bvh_result build_bvh(std::vector<build_prim> prims, const bvh_options& options)
 {
     bvh_result out;
-    builder b(prims, options, out);
-    b.run();
+    builder b(prims, options);
+    prims.clear();
+    prims.shrink_to_fit();
+    b.run(out);
     return out;
 }
+
 namespace
 {
 // A child of a binary node: its box and link

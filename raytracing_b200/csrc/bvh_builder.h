@@ -25,6 +25,7 @@ struct bvh_options
     int max_leaf_size = 1;   // 1..7
     int bins = 32;
     double node_cost = 1.0;  // the SAH's cost of a node fetch, in primitive tests
+    int threads = 0;         // host threads for the subtrees (0: every hardware thread); the tree is the same for any
 };
 
 struct bvh_result

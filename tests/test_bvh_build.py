@@ -10,7 +10,8 @@ src/bvh.ixx:53-73, src/gpu/bvh.cuh:425-432). For every tree, at leaf sizes 1, 4 
 * a leaf holds 1..max_leaf primitives of one kind, and its float box (rounded outward) contains each of their double
   boxes; an inner node's child box contains both of that child's own child boxes;
 * no leaf is deeper than the traversal stack (64 levels; the reference throws at its own limit, bvh.cuh:384-387),
-  the reported depth is the walked depth, and building twice gives the same nodes and orders byte for byte.
+  the reported depth is the walked depth, and the tree built on every hardware thread, on one and on three is the
+  same, nodes and orders byte for byte (ranges of 16,384 primitives or more hand a subtree to another thread).
 """
 import shutil
 import subprocess
@@ -93,12 +94,19 @@ static int check(const std::string& name, int n, int seed, int leaf)
         std::printf("%s %d %d %d threw %s\n", name.c_str(), n, leaf, seed, ex.what());
         return 1;
     }
-    const bvh_result again = build_bvh(prims, o);
     int errors = 0;
-    errors += again.nodes.size() != tree.nodes.size() ||
-              (!tree.nodes.empty() &&
-               std::memcmp(again.nodes.data(), tree.nodes.data(), tree.nodes.size() * sizeof(bvh_node)) != 0);
-    for (int k = 0; k < 3; ++k) { errors += again.order[k] != tree.order[k]; }
+    // the same tree from one thread and from three (the default build uses every hardware thread)
+    for (int threads : {1, 3})
+    {
+        bvh_options t = o;
+        t.threads = threads;
+        const bvh_result again = build_bvh(prims, t);
+        errors += again.nodes.size() != tree.nodes.size() ||
+                  (!tree.nodes.empty() &&
+                   std::memcmp(again.nodes.data(), tree.nodes.data(), tree.nodes.size() * sizeof(bvh_node)) != 0);
+        for (int k = 0; k < 3; ++k) { errors += again.order[k] != tree.order[k]; }
+        errors += again.depth != tree.depth || again.leaves != tree.leaves;
+    }
 
     std::map<std::pair<int, int>, const build_prim*> by_source;
     for (const build_prim& p : prims) { by_source[{p.kind, p.source}] = &p; }
@@ -172,7 +180,8 @@ int main()
 {
     int failures = 0;
     const std::pair<const char*, int> cases[] = {
-        {"random", 1}, {"random", 2}, {"random", 100}, {"random", 5000}, {"one-kind", 3000}, {"identical", 1000},
+        {"random", 1}, {"random", 2}, {"random", 100}, {"random", 5000}, {"random", 60000}, {"one-kind", 40000},
+        {"identical", 1000}, {"identical", 40000},
         {"cluster", 2000}, {"geometric", 40}, {"geometric", 400}, {"geometric", 1500}, {"geometric-spheres", 1500},
         {"random", 0}};
     for (const auto& [name, n] : cases)
@@ -204,7 +213,7 @@ def test_binary_tree_holds_every_primitive_within_the_stack(tmp_path):
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     rows = [line.split() for line in run.stdout.split("\n") if line.strip()]
     assert run.returncode == 0, run.stdout
-    assert len(rows) == 36 and not any("threw" in r for r in rows), run.stdout
+    assert len(rows) == 42 and not any("threw" in r for r in rows), run.stdout
     for name, n, leaf, _seed, depth, nodes, errors in rows:
         n, leaf, depth, errors = int(n), int(leaf), int(depth), int(errors)
         assert errors == 0, (name, n, leaf)
