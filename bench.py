@@ -387,11 +387,16 @@ def mesh_measurement(rt, torch, peaks: dict) -> dict:
     in both forms of a session: the wavefront (its default on a tree-searched scene) and the persistent kernel.
     Timed on the GPU by the session's own events; the scene is far larger than L2."""
     desc = rt.builtin_scene("mesh-ggx")
-    scene = rt.Scene(desc)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    scene = rt.Scene(desc)  # validation, the BVH build on the host's threads, the upload
+    torch.cuda.synchronize()
+    create_s = time.perf_counter() - t0
     passes = desc.round_passes  # sqrt_spp^2: 256
     out = {"workload": f"mesh-ggx {desc.width}x{desc.height}, {passes} spp, depth {desc.camera.max_depth}, "
                        f"{scene.stats()['triangles']} triangles, NEE/MIS with the environment map",
-           "scene_stats": scene.stats()}
+           "scene_stats": scene.stats(),
+           "scene_create_s": create_s, "host_threads": os.cpu_count()}
     # The tree's algorithmic bytes per query: node visits (64 B) and triangle tests (48 B) counted on the workload's
     # own rays by the counting build (the binary walk; the four-wide walk reads 128-B nodes about half as often)
     counting = rt.Session(scene, seed=4, launch_seconds=0.5)
