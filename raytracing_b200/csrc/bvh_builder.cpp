@@ -95,6 +95,85 @@ inline int bin_of(double c, double lo, double scale, int bins)
     return std::min(bins - 1, static_cast<int>((c - lo) * scale));
 }
 
+// The same choice for a range of at most sparse_max primitives, over its occupied bins only (a tree's many small
+// ranges would spend more on sweeping every bin than on binning). The dense sweep's candidates between two occupied
+// bins all cut the range in the same place at the same cost, so the first of them, the left side's last occupied bin,
+// is the one that can win; the same boxes are merged into the same unions, so the costs compare the same and the
+// split is the dense sweep's bit for bit.
+constexpr int sparse_max = 32;
+
+sah_split choose_sparse_sah_split(const item* first, int n, const box& centroids, int bins)
+{
+    sah_split best;
+    for (int axis = 0; axis < 3; ++axis)
+    {
+        const double lo = centroids.lo[axis];
+        const double extent = centroids.hi[axis] - lo;
+        if (!(extent > 0))
+        {
+            continue;
+        }
+        const double scale = bins / extent;
+        // the occupied bins in increasing order, each with its box and count (an insertion into a short sorted list)
+        int key[sparse_max];
+        box group[sparse_max];
+        int count[sparse_max];
+        int groups = 0;
+        for (int i = 0; i < n; ++i)
+        {
+            const int b = bin_of(first[i].c[axis], lo, scale, bins);
+            int g = groups;
+            while (g > 0 && key[g - 1] > b)
+            {
+                --g;
+            }
+            if (g > 0 && key[g - 1] == b)
+            {
+                --g;
+            }
+            else
+            {
+                for (int j = groups; j > g; --j)
+                {
+                    key[j] = key[j - 1];
+                    group[j] = group[j - 1];
+                    count[j] = count[j - 1];
+                }
+                key[g] = b;
+                group[g] = box{};
+                count[g] = 0;
+                ++groups;
+            }
+            group[g].grow(first[i].lo, first[i].hi);
+            ++count[g];
+        }
+        double right_area[sparse_max];
+        int right_count[sparse_max];
+        box acc;
+        int total = 0;
+        for (int g = groups - 1; g > 0; --g)
+        {
+            acc.grow(group[g]);
+            total += count[g];
+            right_area[g] = acc.area();
+            right_count[g] = total;
+        }
+        acc = box{};
+        total = 0;
+        for (int g = 0; g + 1 < groups; ++g)
+        {
+            acc.grow(group[g]);
+            total += count[g];
+            const double cost = acc.area() * total + right_area[g + 1] * right_count[g + 1];
+            if (cost < best.cost)
+            {
+                best = {axis, key[g], cost};
+            }
+        }
+    }
+    return best;
+}
+
 // Every axis with a nonzero centroid extent binned in one pass over the range; the cost sweeps as before, axis by
 // axis and bin by bin, the first strictly cheapest split winning
 sah_split choose_sah_split(const item* first, int n, const box& centroids, int bins)
@@ -393,7 +472,8 @@ private:
         else
         {
             const int bins = std::clamp(options_.bins, 2, max_bins);
-            const sah_split best = choose_sah_split(items_.data() + begin, n, centroids, bins);
+            const sah_split best = n <= sparse_max ? choose_sparse_sah_split(items_.data() + begin, n, centroids, bins)
+                                                   : choose_sah_split(items_.data() + begin, n, centroids, bins);
             const double parent_area = bounds.area();
             const double split_cost =
                 best.axis >= 0 && parent_area > 0 ? options_.node_cost + best.cost / parent_area : inf;
