@@ -9,6 +9,7 @@
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <system_error>
 #include <thread>
 
 namespace rtb
@@ -514,20 +515,39 @@ private:
             // the depth-first order: the same nodes, links and leaf order as one thread's build
             fragment left_part;
             fragment right_part;
-            auto pending = std::async(std::launch::async, [&] {
-                return build(begin, split, depth + 1, left_box, median, left_part, spawn - 1);
-            });
+            std::future<int32_t> pending;
+            try
+            {
+                pending = std::async(std::launch::async, [&] {
+                    return build(begin, split, depth + 1, left_box, median, left_part, spawn - 1);
+                });
+            }
+            catch (const std::system_error&)
+            {
+                // no thread to be had: this one builds both sides, into the same fragments
+            }
+            int32_t left_root = 0;
+            if (!pending.valid())
+            {
+                left_root = build(begin, split, depth + 1, left_box, median, left_part, 0);
+            }
             int32_t right_root = 0;
             try
             {
-                right_root = build(split, end, depth + 1, right_box, median, right_part, spawn - 1);
+                right_root = build(split, end, depth + 1, right_box, median, right_part, pending.valid() ? spawn - 1 : 0);
             }
             catch (...)
             {
-                pending.wait();
+                if (pending.valid())
+                {
+                    pending.wait();
+                }
                 throw;
             }
-            const int32_t left_root = pending.get();
+            if (pending.valid())
+            {
+                left_root = pending.get();
+            }
             left = splice(out, left_part, left_root);
             right = splice(out, right_part, right_root);
         }
