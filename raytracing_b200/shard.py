@@ -7,6 +7,9 @@ slowest rank's, the work is the sum. Nothing else crosses between GPUs.
 
 * `assign` splits units of given costs over the ranks, longest first to the least loaded rank (LPT), the same on
   every rank (a pure function of the costs), so no rank needs to hear the others' choices.
+* `route` sends a stream's requests, as they arrive, each to the rank with the least outstanding work at its
+  arrival: the online counterpart of `assign` for a request server on every GPU, again a pure function (of the
+  arrival times and the costs), so each rank admits exactly its own requests without a message between ranks.
 * `combine` reduces one rank's (seconds, units) over the process group: max of the seconds, sum of the units.
 """
 from __future__ import annotations
@@ -34,6 +37,39 @@ def assign(costs: Sequence[float], world: int) -> list[list[int]]:
 
 def my_units(costs: Sequence[float], world: int, rank: int) -> list[int]:
     return assign(costs, world)[rank]
+
+
+def route(arrivals: Sequence[float], costs: Sequence[float], world: int, rate: float) -> list[int]:
+    """The rank of each request of a stream: requests taken in arrival order (equal times in index order), each sent
+    to the rank whose backlog is the least when it arrives (ties to the lowest rank), where a rank's backlog is the
+    cost it was sent less what it can have worked off since, at `rate` cost units a second, never below zero. With
+    costs in samples (pixels x target passes) and `rate` one GPU's samples a second, a burst of large requests spreads
+    over the GPUs instead of queueing behind one. Every rank computes the same list from the same arrivals."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    if len(arrivals) != len(costs):
+        raise ValueError("one arrival time per cost")
+    if not rate > 0:
+        raise ValueError("rate must be positive")
+    order = sorted(range(len(costs)), key=lambda i: (float(arrivals[i]), i))
+    backlog = [0.0] * world
+    now = None
+    ranks = [0] * len(costs)
+    for i in order:
+        t = float(arrivals[i])
+        if now is not None:
+            worked = rate * (t - now)
+            backlog = [max(0.0, b - worked) for b in backlog]
+        now = t
+        r = min(range(world), key=lambda k: (backlog[k], k))
+        ranks[i] = r
+        backlog[r] += float(costs[i])
+    return ranks
+
+
+def my_requests(arrivals: Sequence[float], costs: Sequence[float], world: int, rank: int, rate: float) -> list[int]:
+    """The indices of the requests `route` sends to `rank`, in index order."""
+    return [i for i, r in enumerate(route(arrivals, costs, world, rate)) if r == rank]
 
 
 def combine(seconds: float, units: float, group=None) -> tuple[float, float]:
