@@ -334,6 +334,15 @@ def config_errors(rt, seed: int) -> dict:
     return out
 
 
+def leg(line, key: str, run) -> None:
+    """line[key] = run(), or, when the leg raises, the error in its place: one workload's failure is recorded in the
+    line instead of ending the run before the line is printed."""
+    try:
+        line[key] = run()
+    except Exception as e:  # noqa: BLE001 - any failure of an auxiliary leg
+        line[key] = {"error": f"{type(e).__name__}: {e}"}
+
+
 def row_band(height: int, threads: int, per_thread: int) -> tuple[int, int]:
     """(first row, rows) of the CPU legs' band of rows about the image's middle: `per_thread` rows a thread where the
     image has them, and always a whole number of rows a thread when the image has at least one a thread (rows are the
@@ -957,56 +966,74 @@ def run_b200(args):
     # minutes, and the scaled metric is the image's alone
     single = world == 1
     mis = mis_image = mis_desc = None
+    mis_passes = 0
     if rank == 0 and single and not args.no_mis:
-        mis, mis_image, mis_desc, mis_passes = mis_measurement(rt, torch, args, max(1, min(args.steps, 3)), seed)
-        line["nee_mis"] = mis
+        def run_mis():
+            nonlocal mis, mis_image, mis_desc, mis_passes
+            mis, mis_image, mis_desc, mis_passes = mis_measurement(rt, torch, args, max(1, min(args.steps, 3)), seed)
+            return mis
+
+        leg(line, "nee_mis", run_mis)
 
     if rank == 0 and not args.no_reference_gpu:
-        ref = reference_gpu_measurement(scene_desc, passes, line["value"])
-        ref_image = ref.pop("image", None)
-        line["reference_gpu"] = ref
-        # Parity of the timed image at its full size: ImageCompare against the reference's own renderer (the same
-        # scene tables, spp and strategy, another seed), and both images' error against the FP64 oracle render
-        if ref_image is not None:
-            from oracle import ref_gpu
+        def run_reference_gpu():
+            ref = reference_gpu_measurement(scene_desc, passes, line["value"])
+            ref_image = ref.pop("image", None)
+            # Parity of the timed image at its full size: ImageCompare against the reference's own renderer (the
+            # same scene tables, spp and strategy, another seed), and both images' error against the FP64 oracle
+            if ref_image is not None:
+                from oracle import ref_gpu
 
-            w, h = scene.width, scene.height
-            line["parity"] = {
-                "workload": line["config"]["workload"],
-                "image_compare_vs_reference": image_parity(
-                    lambda sd: ref_image if sd == 6 else ref_gpu.render(scene_desc.desc, w, h, seed=sd,
-                                                                         passes=passes)[0], timed_image),
-                "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": timed_image,
-                                                            "reference_gpu": ref_image})}
-            if mis is not None:
-                mis_ref_fn = lambda sd: ref_gpu.render(mis_desc.desc, mis_desc.width, mis_desc.height,  # noqa: E731
-                                                       seed=sd, passes=mis_passes)[0]
-                mis_ref = mis_ref_fn(8)
-                mis["parity"] = {
-                    "image_compare_vs_reference": image_parity(lambda sd: mis_ref if sd == 8 else mis_ref_fn(sd),
-                                                               mis_image, seeds=(8, 9)),
-                    "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": mis_image,
-                                                                "reference_gpu": mis_ref})}
+                w, h = scene.width, scene.height
+                leg(line, "parity", lambda: {
+                    "workload": line["config"]["workload"],
+                    "image_compare_vs_reference": image_parity(
+                        lambda sd: ref_image if sd == 6 else ref_gpu.render(scene_desc.desc, w, h, seed=sd,
+                                                                             passes=passes)[0], timed_image),
+                    "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": timed_image,
+                                                                "reference_gpu": ref_image})})
+                if mis is not None and mis_image is not None:
+                    def run_mis_parity():
+                        mis_ref_fn = lambda sd: ref_gpu.render(mis_desc.desc, mis_desc.width,  # noqa: E731
+                                                               mis_desc.height, seed=sd, passes=mis_passes)[0]
+                        mis_ref = mis_ref_fn(8)
+                        return {"image_compare_vs_reference": image_parity(
+                                    lambda sd: mis_ref if sd == 8 else mis_ref_fn(sd), mis_image, seeds=(8, 9)),
+                                "error_vs_fp64": error_vs_fp64(args.scene, {"this_library": mis_image,
+                                                                            "reference_gpu": mis_ref})}
+
+                    leg(mis, "parity", run_mis_parity)
+            return ref
+
+        leg(line, "reference_gpu", run_reference_gpu)
     if rank == 0 and single and not args.no_reference_gpu:
-        line["error_vs_fp64_by_config"] = config_errors(rt, seed)
+        leg(line, "error_vs_fp64_by_config", lambda: config_errors(rt, seed))
     if rank == 0 and single and not args.no_mesh:
-        line["mesh"] = mesh_measurement(rt, torch, peaks)
+        leg(line, "mesh", lambda: mesh_measurement(rt, torch, peaks))
     if not args.no_batched:
-        batched = batched_measurement(rt, torch, rank, world)  # every rank: its share of the 64 jobs
-        if rank == 0:
-            line["batched"] = batched
+        if single:
+            leg(line, "batched", lambda: batched_measurement(rt, torch, rank, world))
+        else:
+            # every rank its share of the 64 jobs, with collectives inside: not guarded, so that no rank leaves them
+            batched = batched_measurement(rt, torch, rank, world)
+            if rank == 0:
+                line["batched"] = batched
     if rank == 0 and single and not args.no_served:
-        line["served"] = served_measurement(rt, torch, args)
-        if args.served_long_window > 0:
-            line["served"]["long_stream"] = served_first_frames(rt, args)
-            batched_long = served_first_frames(rt, args, continuous=False)
-            line["served"]["long_stream"]["batched_server"] = {
-                k: batched_long[k] for k in ("ttff_p50_s", "ttff_p99_s", "ttff_max_s", "ttff_by_resolution",
-                                             "reached_target", "time_to_target_p50_s", "gpu_s", "wall_s", "steps",
-                                             "longest_steps")}
+        def run_served():
+            served = served_measurement(rt, torch, args)
+            if args.served_long_window > 0:
+                served["long_stream"] = served_first_frames(rt, args)
+                batched_long = served_first_frames(rt, args, continuous=False)
+                served["long_stream"]["batched_server"] = {
+                    k: batched_long[k] for k in ("ttff_p50_s", "ttff_p99_s", "ttff_max_s", "ttff_by_resolution",
+                                                 "reached_target", "time_to_target_p50_s", "gpu_s", "wall_s",
+                                                 "steps", "longest_steps")}
+            return served
+
+        leg(line, "served", run_served)
 
     if rank == 0 and single and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(scene_desc, args, os.cpu_count() or 1)
+        leg(line, "cpu_baseline", lambda: cpu_baseline(scene_desc, args, os.cpu_count() or 1))
     if rank == 0 and not single:
         line["single_gpu_legs"] = "nee_mis, error_vs_fp64_by_config, mesh, served and cpu_baseline are measured in the " \
                                   "one-GPU run"

@@ -1,6 +1,6 @@
 """bench.py's own logic without a GPU: the roofline's arithmetic, the slot layout it counts bytes by, the CPU legs'
-band of rows, the error statistic, the batched and served workloads' generators, and the reference arm's JSON line
-(the oracle on a small image, on the CPU)."""
+band of rows, the error statistic, the batched and served workloads' generators, the reference arm's JSON line
+(the oracle on a small image, on the CPU), and a failing auxiliary leg recorded in the line instead of ending the run."""
 import json
 import os
 import subprocess
@@ -161,3 +161,16 @@ def test_reference_arm_other_ranks_exit_without_work():
     out = _run_reference({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert out.returncode == 0, out.stderr
     assert not [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_a_failing_leg_is_recorded_and_the_rest_still_run():
+    line = {"value": 1.0}
+
+    def broken():
+        raise RuntimeError("the reference renderer is not built")
+
+    bench.leg(line, "reference_gpu", broken)
+    bench.leg(line, "mesh", lambda: {"segments_per_s": 2.0})
+    assert line["reference_gpu"] == {"error": "RuntimeError: the reference renderer is not built"}
+    assert line["mesh"] == {"segments_per_s": 2.0}
+    assert json.loads(json.dumps(line)) == line  # the line still prints as JSON
