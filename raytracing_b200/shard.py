@@ -44,7 +44,9 @@ def route(arrivals: Sequence[float], costs: Sequence[float], world: int, rate: f
     to the rank whose backlog is the least when it arrives (ties to the lowest rank), where a rank's backlog is the
     cost it was sent less what it can have worked off since, at `rate` cost units a second, never below zero. With
     costs in samples (pixels x target passes) and `rate` one GPU's samples a second, a burst of large requests spreads
-    over the GPUs instead of queueing behind one. Every rank computes the same list from the same arrivals."""
+    over the GPUs instead of queueing behind one. Every rank computes the same list from the same arrivals, and a
+    request's rank depends only on the requests that arrived before it, so routing the stream seen so far gives the
+    ranks of its earlier requests unchanged: a process can route each request the moment it arrives."""
     if world < 1:
         raise ValueError("world must be at least 1")
     if len(arrivals) != len(costs):

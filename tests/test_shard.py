@@ -107,6 +107,8 @@ def test_route_spreads_a_burst_and_matches_its_rule():
         assert ranks == _brute_route(arrivals, costs, world, 20.0)
         mine = [shard.my_requests(arrivals, costs, world, k, 20.0) for k in range(world)]
         assert sorted(i for m in mine for i in m) == list(range(60))
+        for cut in (1, 17, 59):  # online: the stream seen so far routes its requests as the whole stream does
+            assert shard.route(arrivals[:cut], costs[:cut], world, rate=20.0) == ranks[:cut]
     # a burst at one instant goes round the ranks; requests spaced wider than their work all go to the first
     assert shard.route([0.0] * 6, [5.0] * 6, 3, rate=1.0) == [0, 1, 2, 0, 1, 2]
     assert shard.route([0.0, 10.0, 20.0], [5.0] * 3, 3, rate=1.0) == [0, 0, 0]
